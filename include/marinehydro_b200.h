@@ -1,0 +1,145 @@
+/*
+ * marinehydro_b200 -- C ABI of the B200 (sm_100a) boundary-element library.
+ *
+ * Drop-in for the hot path of MarineHydro.jl: influence-matrix assembly of the
+ * Rankine / reflected-Rankine / Wu / exact Guevel-Delhommeau Green functions,
+ * the dense complex solve (direct or indirect formulation), the pressure
+ * integration that gives added mass, radiation damping and diffraction force,
+ * and their adjoints.  The reference is pure Julia; its per-pair multiple
+ * dispatch (`integral` / `integral_gradient` on `GreensFunction` subtypes,
+ * src/green_functions/abstract_greens_function.jl:47-83) is too fine-grained
+ * for a foreign call, so this boundary sits at matrix level
+ * (`assemble_matrices`, `solve`) and at output level
+ * (`calculate_radiation_forces`, `DiffractionForce`, the batched
+ * hydrodynamic-coefficient driver and its gradients).
+ *
+ * Conventions (all follow the reference's Julia storage):
+ *  - matrices and N x 3 arrays are column-major; complex numbers are
+ *    interleaved (re, im) float64 pairs, i.e. Julia's ComplexF64;
+ *  - faces are 0-based vertex indices, N x 4 int64 (src/meshes.jl:179 adds 1);
+ *  - every function returns MH_OK (0) or an MH_ERR_* code and never aborts;
+ *    mh_last_error() gives the message;
+ *  - host pointers are caller-owned and only read/written during the call;
+ *  - one mh_ctx owns one CUDA stream; calls on one ctx must not overlap.
+ */
+#ifndef MARINEHYDRO_B200_H
+#define MARINEHYDRO_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define MH_OK                 0
+#define MH_ERR_ARG            1 /* bad shape / NULL / out-of-range, mirrors the reference's @assert checks (src/meshes.jl:28-34) */
+#define MH_ERR_CUDA           2 /* a CUDA runtime / library call failed */
+#define MH_ERR_NOT_CONVERGED  3 /* iterative refinement hit its iteration cap */
+#define MH_ERR_TIMEOUT        4 /* a bounded device-side wait gave up */
+#define MH_ERR_OOM            5 /* device allocation failed */
+#define MH_ERR_NO_DEVICE      6 /* no CUDA device / requested device absent */
+#define MH_ERR_SINGULAR       7 /* zero pivot in the LU factorisation */
+
+/* Green-function terms, summed like the reference's tuples
+ * (abstract_greens_function.jl:18,34,49,65,83).  RANKINE_REFLECTED and
+ * RANKINE_REFLECTED_NEGATIVE together cancel, as +G - G does in Julia. */
+#define MH_GF_RANKINE                     1u  /* Rankine()                  src/green_functions/rankine.jl */
+#define MH_GF_RANKINE_REFLECTED           2u  /* RankineReflected()         src/green_functions/rankine_reflected.jl */
+#define MH_GF_RANKINE_REFLECTED_NEGATIVE  4u  /* RankineReflectedNegative() src/green_functions/rankine_reflected_negative.jl */
+#define MH_GF_WU                          8u  /* GFWu()                     src/green_functions/wu.jl */
+#define MH_GF_DELHOMMEAU                 16u  /* ExactGuevelDelhommeau()    src/green_functions/exact_Guevel_Delhommeau.jl */
+
+/* precision of a solve */
+#define MH_PRECISION_FP64   0  /* FP64 assembly + FP64 LU (cuSOLVER zgetrf/zgetrs) */
+#define MH_PRECISION_MIXED  1  /* FP64-accurate matrices, low-precision LU, FP64 iterative refinement */
+
+typedef struct mh_ctx mh_ctx;
+typedef struct mh_mesh mh_mesh;
+
+/* ---- library / context ------------------------------------------------ */
+
+/* ABI version (major*10000 + minor*100 + patch). */
+int mh_version(void);
+
+/* Number of visible CUDA devices (0 on a machine without a GPU). */
+int mh_device_count(int* count);
+
+/* Create a context bound to `device`: one CUDA stream, library handles and a
+ * grow-only workspace.  No reference counterpart (the reference is
+ * single-process Julia); it replaces Julia's implicit global state. */
+int mh_ctx_create(int device, mh_ctx** out);
+int mh_ctx_destroy(mh_ctx* ctx);
+
+/* Message of the last error on this context (ctx == NULL: last error of
+ * mh_ctx_create on this thread).  Valid until the next call on the ctx. */
+const char* mh_last_error(const mh_ctx* ctx);
+
+/* Number of this library's own kernels launched on the ctx so far. */
+int mh_ctx_kernel_launches(const mh_ctx* ctx, int64_t* count);
+
+/* ---- meshes ------------------------------------------------------------ */
+
+/* Upload a panel mesh; replaces `Mesh(vertices, faces, centers, normals,
+ * areas, radii, nvertices, nfaces)` (src/meshes.jl:21-36) on the device.
+ *   vertices  nvertices x 3, column-major float64
+ *   faces     nfaces x 4, column-major int64, 0-based
+ *   centers, normals  nfaces x 3 column-major; areas, radii  nfaces   */
+int mh_mesh_create(mh_ctx* ctx, int64_t nfaces, int64_t nvertices,
+                   const double* vertices, const int64_t* faces,
+                   const double* centers, const double* normals,
+                   const double* areas, const double* radii,
+                   mh_mesh** out);
+int mh_mesh_destroy(mh_ctx* ctx, mh_mesh* mesh);
+int mh_mesh_nfaces(const mh_mesh* mesh, int64_t* nfaces);
+
+/* ---- matrix level ------------------------------------------------------ */
+
+/* S and D (direct) or S and K (indirect), FP64, written to HOST buffers of
+ * nfaces*nfaces complex128 (column-major); either may be NULL.
+ * Replaces `assemble_matrices(green_functions, mesh, wavenumber; direct)`
+ * (src/matrix_assembly.jl:4-42, :97). */
+int mh_assemble_matrices(mh_ctx* ctx, const mh_mesh* mesh, double wavenumber,
+                         uint32_t gf_mask, int direct,
+                         double* S_out, double* D_out);
+
+/* Same, into DEVICE buffers (nfaces*nfaces complex128 each, may be NULL). */
+int mh_assemble_matrices_device(mh_ctx* ctx, const mh_mesh* mesh, double wavenumber,
+                                uint32_t gf_mask, int direct,
+                                void* S_dev, void* D_dev);
+
+/* phi = D \ (S bc) (direct) or phi = S (K \ bc) (indirect), FP64, host
+ * buffers; D, S: n x n complex128, bc and phi_out: n x nrhs complex128.
+ * Replaces `solve(D, S, bc; direct)` (src/matrix_assembly.jl:105-133). */
+int mh_solve(mh_ctx* ctx, int64_t n, const double* D, const double* S,
+             const double* bc, int64_t nrhs, int direct, double* phi_out);
+
+/* ---- output level ------------------------------------------------------ */
+
+/* [added mass, radiation damping] for one rigid-body motion `dof` at
+ * frequency omega: k = omega^2/g, assembly, bc = -i omega (n . dof), solve,
+ * p = i rho omega phi, F = sum p (-(n . dof)) area, out = [Re F/omega^2,
+ * Im F/omega].  `dof` is a 3-vector (dof_rows = 1) or an nfaces x 3
+ * column-major matrix (dof_rows = nfaces).
+ * Replaces `calculate_radiation_forces(mesh, dof, omega)` (src/waves.jl:29-37);
+ * the reference hard-codes gf = Rankine+RankineReflected+GFWu and direct=true,
+ * which are the values a drop-in caller passes. */
+int mh_calculate_radiation_forces(mh_ctx* ctx, const mh_mesh* mesh,
+                                  const double* dof, int64_t dof_rows,
+                                  double omega, double rho, double g,
+                                  uint32_t gf_mask, int direct, int precision,
+                                  double out[2]);
+
+/* Complex diffraction force (re, im) for incident Airy waves of heading beta:
+ * bc = -(v_inc . n) (src/waves.jl:121-142), solve, p = i rho phi omega,
+ * F = sum p (-(n . dof)) area.
+ * Replaces `DiffractionForce(mesh, omega, dof)` (src/waves.jl:40-59). */
+int mh_diffraction_force(mh_ctx* ctx, const mh_mesh* mesh, double omega,
+                         const double* dof, int64_t dof_rows, double beta,
+                         double rho, double g, uint32_t gf_mask, int direct,
+                         int precision, double out[2]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

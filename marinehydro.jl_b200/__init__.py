@@ -1,0 +1,21 @@
+"""marinehydro_b200 -- B200 (sm_100a) implementation of MarineHydro.jl's
+boundary-element hot path: Green-function influence-matrix assembly, the
+dense complex solve and the outputs built on it (added mass, radiation
+damping, diffraction force).
+
+The compute runs in ``lib/libmarinehydro_b200.so`` (hand-written CUDA for
+sm_100a behind the C ABI in ``include/marinehydro_b200.h``).  This package is
+the host-side mirror of the reference's public API for that path.
+"""
+from .meshes import Mesh, combine_meshes, mesh_hemisphere, mesh_two_hemispheres, panel_geometry
+from .api import (SETTINGS, set_g, set_rho, GreensFunction, Rankine, RankineReflected,
+                  RankineReflectedNegative, GFWu, ExactGuevelDelhommeau, gf_mask,
+                  DEFAULT_GREEN_FUNCTIONS, DeviceMesh, device_mesh, assemble_matrices,
+                  assemble_matrix_wu, solve, calculate_radiation_forces, DiffractionForce,
+                  radiation_bc, AiryBC, airy_waves_potential, airy_waves_velocity,
+                  airy_waves_pressure, integrate_pressure, FroudeKrylovForce)
+from ._native import (Context, MarineHydroError, ArgumentError, NotConvergedError,
+                      SingularMatrixError, device_count, default_context)
+from . import _native as native
+
+__all__ = [n for n in dir() if not n.startswith("_")]

@@ -1,0 +1,173 @@
+"""ctypes binding of ``lib/libmarinehydro_b200.so`` (declared in
+``include/marinehydro_b200.h``).
+
+There is no fallback: if the shared library is missing this module raises,
+and every compute call surfaces the library's status code as an exception.
+"""
+from __future__ import annotations
+
+import ctypes
+import pathlib
+import threading
+
+import numpy as np
+
+PKG = pathlib.Path(__file__).resolve().parent
+LIB_PATH = PKG / "lib" / "libmarinehydro_b200.so"
+
+MH_OK = 0
+MH_ERR_ARG = 1
+MH_ERR_CUDA = 2
+MH_ERR_NOT_CONVERGED = 3
+MH_ERR_TIMEOUT = 4
+MH_ERR_OOM = 5
+MH_ERR_NO_DEVICE = 6
+MH_ERR_SINGULAR = 7
+
+MH_PRECISION_FP64 = 0
+MH_PRECISION_MIXED = 1
+
+_NAMES = {MH_ERR_ARG: "MH_ERR_ARG", MH_ERR_CUDA: "MH_ERR_CUDA",
+          MH_ERR_NOT_CONVERGED: "MH_ERR_NOT_CONVERGED", MH_ERR_TIMEOUT: "MH_ERR_TIMEOUT",
+          MH_ERR_OOM: "MH_ERR_OOM", MH_ERR_NO_DEVICE: "MH_ERR_NO_DEVICE",
+          MH_ERR_SINGULAR: "MH_ERR_SINGULAR"}
+
+
+class MarineHydroError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+class ArgumentError(MarineHydroError, ValueError):
+    """Bad shapes or values (the reference raises from its @assert checks)."""
+
+
+class NotConvergedError(MarineHydroError):
+    pass
+
+
+class SingularMatrixError(MarineHydroError):
+    pass
+
+
+_P = ctypes.c_void_p
+_D = ctypes.POINTER(ctypes.c_double)
+_I64 = ctypes.POINTER(ctypes.c_int64)
+
+# name -> (restype, argtypes); every symbol include/marinehydro_b200.h declares.
+SIGNATURES = {
+    "mh_version": (ctypes.c_int, []),
+    "mh_device_count": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
+    "mh_ctx_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_P)]),
+    "mh_ctx_destroy": (ctypes.c_int, [_P]),
+    "mh_last_error": (ctypes.c_char_p, [_P]),
+    "mh_ctx_kernel_launches": (ctypes.c_int, [_P, _I64]),
+    "mh_mesh_create": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_int64, _D, _I64, _D, _D, _D, _D,
+                                      ctypes.POINTER(_P)]),
+    "mh_mesh_destroy": (ctypes.c_int, [_P, _P]),
+    "mh_mesh_nfaces": (ctypes.c_int, [_P, _I64]),
+    "mh_assemble_matrices": (ctypes.c_int, [_P, _P, ctypes.c_double, ctypes.c_uint32, ctypes.c_int,
+                                            _D, _D]),
+    "mh_assemble_matrices_device": (ctypes.c_int, [_P, _P, ctypes.c_double, ctypes.c_uint32,
+                                                   ctypes.c_int, _P, _P]),
+    "mh_solve": (ctypes.c_int, [_P, ctypes.c_int64, _D, _D, _D, ctypes.c_int64, ctypes.c_int, _D]),
+    "mh_calculate_radiation_forces": (ctypes.c_int, [_P, _P, _D, ctypes.c_int64, ctypes.c_double,
+                                                     ctypes.c_double, ctypes.c_double,
+                                                     ctypes.c_uint32, ctypes.c_int, ctypes.c_int,
+                                                     _D]),
+    "mh_diffraction_force": (ctypes.c_int, [_P, _P, ctypes.c_double, _D, ctypes.c_int64,
+                                            ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                            ctypes.c_uint32, ctypes.c_int, ctypes.c_int, _D]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def lib():
+    """Load the shared library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not LIB_PATH.exists():
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python marinehydro.jl_b200/build.py` "
+                "(there is no CPU fallback)")
+        L = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+        return L
+
+
+def dptr(a: np.ndarray):
+    return a.ctypes.data_as(_D) if a is not None else None
+
+
+def i64ptr(a: np.ndarray):
+    return a.ctypes.data_as(_I64)
+
+
+def check(rc: int, ctx=None):
+    if rc == MH_OK:
+        return
+    msg = lib().mh_last_error(ctx)
+    msg = msg.decode() if msg else ""
+    if rc == MH_ERR_ARG:
+        raise ArgumentError(rc, msg)
+    if rc == MH_ERR_NOT_CONVERGED:
+        raise NotConvergedError(rc, msg)
+    if rc == MH_ERR_SINGULAR:
+        raise SingularMatrixError(rc, msg)
+    raise MarineHydroError(rc, msg)
+
+
+def device_count() -> int:
+    c = ctypes.c_int(0)
+    check(lib().mh_device_count(ctypes.byref(c)))
+    return int(c.value)
+
+
+class Context:
+    """One device, one CUDA stream, one workspace (``mh_ctx``)."""
+
+    def __init__(self, device: int = 0):
+        self._h = _P()
+        check(lib().mh_ctx_create(int(device), ctypes.byref(self._h)), None)
+        self.device = int(device)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def kernel_launches(self) -> int:
+        c = ctypes.c_int64(0)
+        check(lib().mh_ctx_kernel_launches(self._h, ctypes.byref(c)), self._h)
+        return int(c.value)
+
+    def close(self):
+        if self._h:
+            lib().mh_ctx_destroy(self._h)
+            self._h = _P()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx

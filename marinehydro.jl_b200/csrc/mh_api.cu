@@ -1,0 +1,447 @@
+// C ABI of libmarinehydro_b200: contexts, meshes, matrix-level and
+// output-level entry points.  Every entry point validates its arguments,
+// returns an MH_* status and records a message on the context.
+#include <cuComplex.h>
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+
+#include <cmath>
+#include <new>
+#include <string>
+
+#include "mh_internal.h"
+
+namespace {
+thread_local std::string g_create_err;
+
+bool finite_array(const double* a, int64_t count)
+{
+    for (int64_t i = 0; i < count; ++i)
+        if (!std::isfinite(a[i])) return false;
+    return true;
+}
+}  // namespace
+
+namespace mh {
+
+int set_err(mh_ctx* ctx, int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (ctx) ctx->err = buf;
+    else g_create_err = buf;
+    return code;
+}
+
+void* ws_get(mh_ctx* ctx, int slot, size_t bytes)
+{
+    if (bytes == 0) bytes = 16;
+    if (ctx->ws_bytes[slot] >= bytes) return ctx->ws[slot];
+    if (ctx->ws[slot]) {
+        cudaStreamSynchronize(ctx->stream);
+        cudaFree(ctx->ws[slot]);
+        ctx->ws[slot] = nullptr;
+        ctx->ws_bytes[slot] = 0;
+    }
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_err(ctx, MH_ERR_OOM, "device allocation of %zu bytes failed: %s", bytes,
+                cudaGetErrorString(e));
+        return nullptr;
+    }
+    ctx->ws[slot] = p;
+    ctx->ws_bytes[slot] = bytes;
+    return p;
+}
+
+}  // namespace mh
+
+using mh::set_err;
+using mh::ws_get;
+
+namespace {
+
+int check_ctx(mh_ctx* ctx)
+{
+    if (!ctx) return MH_ERR_ARG;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess)
+        return set_err(ctx, MH_ERR_CUDA, "cudaSetDevice(%d): %s", ctx->device, cudaGetErrorString(e));
+    ctx->err.clear();
+    return MH_OK;
+}
+
+int check_mesh(mh_ctx* ctx, const mh_mesh* m)
+{
+    if (!m || !m->geom || m->n <= 0) return set_err(ctx, MH_ERR_ARG, "mesh is NULL or empty");
+    if (m->device != ctx->device)
+        return set_err(ctx, MH_ERR_ARG, "mesh lives on device %d, context on device %d", m->device,
+                       ctx->device);
+    return MH_OK;
+}
+
+int valid_mask(mh_ctx* ctx, uint32_t mask)
+{
+    const uint32_t all = MH_GF_RANKINE | MH_GF_RANKINE_REFLECTED | MH_GF_RANKINE_REFLECTED_NEGATIVE |
+                         MH_GF_WU | MH_GF_DELHOMMEAU;
+    if (mask == 0 || (mask & ~all))
+        return set_err(ctx, MH_ERR_ARG, "invalid Green-function mask 0x%x", mask);
+    return MH_OK;
+}
+
+int sync_status(mh_ctx* ctx, const char* what)
+{
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return set_err(ctx, MH_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    return MH_OK;
+}
+
+// LU-factorise A (n x n, device, overwritten) and solve A X = B in place
+// (B: n x nrhs, device) with cuSOLVER zgetrf/zgetrs.
+int lu_solve_fp64(mh_ctx* ctx, int64_t n, double2* A, double2* B, int64_t nrhs)
+{
+    int lwork = 0;
+    cusolverStatus_t st = cusolverDnZgetrf_bufferSize(ctx->cusolver, (int)n, (int)n,
+                                                      (cuDoubleComplex*)A, (int)n, &lwork);
+    if (st != CUSOLVER_STATUS_SUCCESS)
+        return set_err(ctx, MH_ERR_CUDA, "cusolverDnZgetrf_bufferSize failed (%d)", (int)st);
+    auto* work = (cuDoubleComplex*)ws_get(ctx, WS_LWORK, sizeof(cuDoubleComplex) * (size_t)lwork);
+    auto* piv = (int*)ws_get(ctx, WS_PIV, sizeof(int) * (size_t)n);
+    auto* info = (int*)ws_get(ctx, WS_INFO, sizeof(int) * 2);
+    if (!work || !piv || !info) return MH_ERR_OOM;
+    st = cusolverDnZgetrf(ctx->cusolver, (int)n, (int)n, (cuDoubleComplex*)A, (int)n, work, piv, info);
+    if (st != CUSOLVER_STATUS_SUCCESS)
+        return set_err(ctx, MH_ERR_CUDA, "cusolverDnZgetrf failed (%d)", (int)st);
+    st = cusolverDnZgetrs(ctx->cusolver, CUBLAS_OP_N, (int)n, (int)nrhs, (const cuDoubleComplex*)A,
+                          (int)n, piv, (cuDoubleComplex*)B, (int)n, info + 1);
+    if (st != CUSOLVER_STATUS_SUCCESS)
+        return set_err(ctx, MH_ERR_CUDA, "cusolverDnZgetrs failed (%d)", (int)st);
+    int h_info[2] = {0, 0};
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(h_info, info, sizeof(h_info), cudaMemcpyDeviceToHost, ctx->stream));
+    int rc = sync_status(ctx, "LU solve");
+    if (rc) return rc;
+    if (h_info[0] > 0) return set_err(ctx, MH_ERR_SINGULAR, "zero pivot at column %d", h_info[0]);
+    if (h_info[0] < 0 || h_info[1] < 0)
+        return set_err(ctx, MH_ERR_ARG, "LAPACK argument %d invalid", -(h_info[0] ? h_info[0] : h_info[1]));
+    return MH_OK;
+}
+
+// C = A B for n x n A and n x nrhs B (device, complex128).
+int zgemm_nn(mh_ctx* ctx, int64_t n, int64_t nrhs, const double2* A, const double2* B, double2* C)
+{
+    const cuDoubleComplex one = make_cuDoubleComplex(1.0, 0.0), zero = make_cuDoubleComplex(0.0, 0.0);
+    cublasStatus_t st = cublasZgemm(ctx->cublas, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, (int)nrhs, (int)n,
+                                    &one, (const cuDoubleComplex*)A, (int)n,
+                                    (const cuDoubleComplex*)B, (int)n, &zero, (cuDoubleComplex*)C,
+                                    (int)n);
+    if (st != CUBLAS_STATUS_SUCCESS) return set_err(ctx, MH_ERR_CUDA, "cublasZgemm failed (%d)", (int)st);
+    return MH_OK;
+}
+
+// phi = D \ (S bc)  or  phi = S (K \ bc), all device; D is overwritten by its
+// LU factors, bc by intermediate results.  (src/matrix_assembly.jl:105-133)
+int solve_fp64_device(mh_ctx* ctx, int64_t n, double2* D, const double2* S, double2* bc,
+                      int64_t nrhs, int direct, double2* phi)
+{
+    int rc;
+    if (direct) {
+        if ((rc = zgemm_nn(ctx, n, nrhs, S, bc, phi))) return rc;
+        return lu_solve_fp64(ctx, n, D, phi, nrhs);
+    }
+    if ((rc = lu_solve_fp64(ctx, n, D, bc, nrhs))) return rc;
+    return zgemm_nn(ctx, n, nrhs, S, bc, phi);
+}
+
+int dof_upload(mh_ctx* ctx, const mh_mesh* m, const double* dof, int64_t dof_rows, double** d_dof)
+{
+    if (!dof) return set_err(ctx, MH_ERR_ARG, "dof is NULL");
+    if (dof_rows != 1 && dof_rows != m->n)
+        return set_err(ctx, MH_ERR_ARG, "dof must be a 3-vector or an nfaces x 3 matrix (got %lld rows)",
+                       (long long)dof_rows);
+    size_t bytes = sizeof(double) * 3 * (size_t)dof_rows;
+    double* p = (double*)ws_get(ctx, WS_DOF, bytes);
+    if (!p) return MH_ERR_OOM;
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(p, dof, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    *d_dof = p;
+    return MH_OK;
+}
+
+// Shared pipeline of the two front doors: assembly, bc, solve, force.
+int front_door(mh_ctx* ctx, const mh_mesh* m, const double* dof, int64_t dof_rows, double omega,
+               double rho, double g, uint32_t gf_mask, int direct, int precision, bool diffraction,
+               double beta, double2* F_host)
+{
+    int rc;
+    if ((rc = check_ctx(ctx))) return rc;
+    if ((rc = check_mesh(ctx, m))) return rc;
+    if ((rc = valid_mask(ctx, gf_mask))) return rc;
+    if (!(omega > 0.0) || !std::isfinite(omega) || !(g > 0.0) || !std::isfinite(rho))
+        return set_err(ctx, MH_ERR_ARG, "omega and g must be positive and finite");
+    if (precision != MH_PRECISION_FP64)
+        return set_err(ctx, MH_ERR_ARG, "precision %d is not available on this entry point", precision);
+    const int64_t n = m->n;
+    const size_t mat = sizeof(double2) * (size_t)n * (size_t)n;
+    auto* S = (double2*)ws_get(ctx, WS_S, mat);
+    auto* D = (double2*)ws_get(ctx, WS_D, mat);
+    auto* bc = (double2*)ws_get(ctx, WS_RHS, sizeof(double2) * (size_t)n);
+    auto* phi = (double2*)ws_get(ctx, WS_PHI, sizeof(double2) * (size_t)n);
+    auto* F = (double2*)ws_get(ctx, WS_OUT, sizeof(double2));
+    if (!S || !D || !bc || !phi || !F) return MH_ERR_OOM;
+    double* d_dof = nullptr;
+    if ((rc = dof_upload(ctx, m, dof, dof_rows, &d_dof))) return rc;
+    const double k = omega * omega / g;
+    MH_CUDA_TRY(ctx, mh::launch_assemble_f64(ctx, m, k, gf_mask, direct, S, D));
+    if (diffraction) MH_CUDA_TRY(ctx, mh::launch_airy_bc(ctx, m, omega, beta, g, bc));
+    else MH_CUDA_TRY(ctx, mh::launch_radiation_bc(ctx, m, d_dof, dof_rows, omega, bc));
+    if ((rc = solve_fp64_device(ctx, n, D, S, bc, 1, direct, phi))) return rc;
+    MH_CUDA_TRY(ctx, mh::launch_force(ctx, m, phi, d_dof, dof_rows, rho, omega, F));
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(F_host, F, sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
+    return sync_status(ctx, "front door");
+}
+
+}  // namespace
+
+extern "C" {
+
+int mh_version(void) { return 100; }
+
+int mh_device_count(int* count)
+{
+    if (!count) return MH_ERR_ARG;
+    int c = 0;
+    cudaError_t e = cudaGetDeviceCount(&c);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        c = 0;
+    }
+    *count = c;
+    return MH_OK;
+}
+
+int mh_ctx_create(int device, mh_ctx** out)
+{
+    if (!out) return set_err(nullptr, MH_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return set_err(nullptr, MH_ERR_NO_DEVICE, "no CUDA device is visible");
+    }
+    if (device < 0 || device >= count)
+        return set_err(nullptr, MH_ERR_NO_DEVICE, "device %d out of range (%d visible)", device, count);
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess)
+        return set_err(nullptr, MH_ERR_CUDA, "cudaSetDevice(%d): %s", device, cudaGetErrorString(e));
+    auto* ctx = new (std::nothrow) mh_ctx();
+    if (!ctx) return set_err(nullptr, MH_ERR_OOM, "host allocation failed");
+    ctx->device = device;
+    if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+        delete ctx;
+        return set_err(nullptr, MH_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+    }
+    if (cublasCreate(&ctx->cublas) != CUBLAS_STATUS_SUCCESS ||
+        cusolverDnCreate(&ctx->cusolver) != CUSOLVER_STATUS_SUCCESS) {
+        mh_ctx_destroy(ctx);
+        return set_err(nullptr, MH_ERR_CUDA, "cuBLAS / cuSOLVER handle creation failed");
+    }
+    cublasSetStream(ctx->cublas, ctx->stream);
+    cusolverDnSetStream(ctx->cusolver, ctx->stream);
+    *out = ctx;
+    return MH_OK;
+}
+
+int mh_ctx_destroy(mh_ctx* ctx)
+{
+    if (!ctx) return MH_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (int s = 0; s < WS_NSLOTS; ++s)
+        if (ctx->ws[s]) cudaFree(ctx->ws[s]);
+    if (ctx->cusolver) cusolverDnDestroy(ctx->cusolver);
+    if (ctx->cublas) cublasDestroy(ctx->cublas);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return MH_OK;
+}
+
+const char* mh_last_error(const mh_ctx* ctx)
+{
+    return ctx ? ctx->err.c_str() : g_create_err.c_str();
+}
+
+int mh_ctx_kernel_launches(const mh_ctx* ctx, int64_t* count)
+{
+    if (!ctx || !count) return MH_ERR_ARG;
+    *count = ctx->launches;
+    return MH_OK;
+}
+
+int mh_mesh_create(mh_ctx* ctx, int64_t nfaces, int64_t nvertices, const double* vertices,
+                   const int64_t* faces, const double* centers, const double* normals,
+                   const double* areas, const double* radii, mh_mesh** out)
+{
+    int rc;
+    if ((rc = check_ctx(ctx))) return rc;
+    if (!out) return set_err(ctx, MH_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (nfaces <= 0 || nvertices <= 0)
+        return set_err(ctx, MH_ERR_ARG, "nfaces and nvertices must be positive");
+    if (!vertices || !faces || !centers || !normals || !areas || !radii)
+        return set_err(ctx, MH_ERR_ARG, "a mesh array is NULL");
+    for (int64_t q = 0; q < 4 * nfaces; ++q)
+        if (faces[q] < 0 || faces[q] >= nvertices)
+            return set_err(ctx, MH_ERR_ARG, "face vertex index %lld out of range [0, %lld)",
+                           (long long)faces[q], (long long)nvertices);
+    if (!finite_array(vertices, 3 * nvertices) || !finite_array(centers, 3 * nfaces) ||
+        !finite_array(normals, 3 * nfaces) || !finite_array(areas, nfaces) ||
+        !finite_array(radii, nfaces))
+        return set_err(ctx, MH_ERR_ARG, "mesh arrays must be finite");
+    // Host-side staging of the structure-of-arrays geometry.
+    const int64_t n = nfaces;
+    double* h = new (std::nothrow) double[(size_t)G_NFIELDS * (size_t)n];
+    if (!h) return set_err(ctx, MH_ERR_OOM, "host allocation failed");
+    for (int64_t i = 0; i < n; ++i) {
+        for (int c = 0; c < 3; ++c) {
+            h[(G_CX + c) * n + i] = centers[c * n + i];
+            h[(G_NX + c) * n + i] = normals[c * n + i];
+        }
+        h[G_AREA * n + i] = areas[i];
+        h[G_RADIUS * n + i] = radii[i];
+        for (int a = 0; a < 4; ++a) {
+            int64_t v = faces[a * n + i];
+            for (int c = 0; c < 3; ++c) h[(G_V + 3 * a + c) * n + i] = vertices[c * nvertices + v];
+        }
+    }
+    auto* m = new (std::nothrow) mh_mesh();
+    if (!m) {
+        delete[] h;
+        return set_err(ctx, MH_ERR_OOM, "host allocation failed");
+    }
+    m->n = n;
+    m->nv = nvertices;
+    m->device = ctx->device;
+    size_t bytes = sizeof(double) * (size_t)G_NFIELDS * (size_t)n;
+    cudaError_t e = cudaMalloc(&m->geom, bytes);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(m->geom, h, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    delete[] h;
+    if (e != cudaSuccess) {
+        if (m->geom) cudaFree(m->geom);
+        delete m;
+        return set_err(ctx, e == cudaErrorMemoryAllocation ? MH_ERR_OOM : MH_ERR_CUDA,
+                       "mesh upload failed: %s", cudaGetErrorString(e));
+    }
+    *out = m;
+    return MH_OK;
+}
+
+int mh_mesh_destroy(mh_ctx* ctx, mh_mesh* mesh)
+{
+    if (!mesh) return MH_OK;
+    if (ctx) {
+        cudaSetDevice(ctx->device);
+        cudaStreamSynchronize(ctx->stream);
+    }
+    if (mesh->geom) cudaFree(mesh->geom);
+    delete mesh;
+    return MH_OK;
+}
+
+int mh_mesh_nfaces(const mh_mesh* mesh, int64_t* nfaces)
+{
+    if (!mesh || !nfaces) return MH_ERR_ARG;
+    *nfaces = mesh->n;
+    return MH_OK;
+}
+
+int mh_assemble_matrices_device(mh_ctx* ctx, const mh_mesh* mesh, double wavenumber,
+                                uint32_t gf_mask, int direct, void* S_dev, void* D_dev)
+{
+    int rc;
+    if ((rc = check_ctx(ctx))) return rc;
+    if ((rc = check_mesh(ctx, mesh))) return rc;
+    if ((rc = valid_mask(ctx, gf_mask))) return rc;
+    if (!std::isfinite(wavenumber) || wavenumber < 0.0)
+        return set_err(ctx, MH_ERR_ARG, "wavenumber must be finite and non-negative");
+    if ((gf_mask & (MH_GF_WU | MH_GF_DELHOMMEAU)) && !(wavenumber > 0.0))
+        return set_err(ctx, MH_ERR_ARG, "wave terms need a positive wavenumber");
+    if (!S_dev && !D_dev) return MH_OK;
+    MH_CUDA_TRY(ctx, mh::launch_assemble_f64(ctx, mesh, wavenumber, gf_mask, direct, (double2*)S_dev,
+                                             (double2*)D_dev));
+    return sync_status(ctx, "assembly");
+}
+
+int mh_assemble_matrices(mh_ctx* ctx, const mh_mesh* mesh, double wavenumber, uint32_t gf_mask,
+                         int direct, double* S_out, double* D_out)
+{
+    int rc;
+    if ((rc = check_ctx(ctx))) return rc;
+    if ((rc = check_mesh(ctx, mesh))) return rc;
+    const int64_t n = mesh->n;
+    const size_t mat = sizeof(double2) * (size_t)n * (size_t)n;
+    void* S = S_out ? ws_get(ctx, WS_S, mat) : nullptr;
+    void* D = D_out ? ws_get(ctx, WS_D, mat) : nullptr;
+    if ((S_out && !S) || (D_out && !D)) return MH_ERR_OOM;
+    if ((rc = mh_assemble_matrices_device(ctx, mesh, wavenumber, gf_mask, direct, S, D))) return rc;
+    if (S_out) MH_CUDA_TRY(ctx, cudaMemcpyAsync(S_out, S, mat, cudaMemcpyDeviceToHost, ctx->stream));
+    if (D_out) MH_CUDA_TRY(ctx, cudaMemcpyAsync(D_out, D, mat, cudaMemcpyDeviceToHost, ctx->stream));
+    return sync_status(ctx, "copy of S/D to host");
+}
+
+int mh_solve(mh_ctx* ctx, int64_t n, const double* D, const double* S, const double* bc,
+             int64_t nrhs, int direct, double* phi_out)
+{
+    int rc;
+    if ((rc = check_ctx(ctx))) return rc;
+    if (n <= 0 || nrhs <= 0) return set_err(ctx, MH_ERR_ARG, "n and nrhs must be positive");
+    if (!D || !S || !bc || !phi_out) return set_err(ctx, MH_ERR_ARG, "a solve argument is NULL");
+    const size_t mat = sizeof(double2) * (size_t)n * (size_t)n;
+    const size_t vec = sizeof(double2) * (size_t)n * (size_t)nrhs;
+    auto* dD = (double2*)ws_get(ctx, WS_D, mat);
+    auto* dS = (double2*)ws_get(ctx, WS_S, mat);
+    auto* dB = (double2*)ws_get(ctx, WS_RHS, vec);
+    auto* dP = (double2*)ws_get(ctx, WS_PHI, vec);
+    if (!dD || !dS || !dB || !dP) return MH_ERR_OOM;
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(dD, D, mat, cudaMemcpyHostToDevice, ctx->stream));
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(dS, S, mat, cudaMemcpyHostToDevice, ctx->stream));
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(dB, bc, vec, cudaMemcpyHostToDevice, ctx->stream));
+    if ((rc = solve_fp64_device(ctx, n, dD, dS, dB, nrhs, direct, dP))) return rc;
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(phi_out, dP, vec, cudaMemcpyDeviceToHost, ctx->stream));
+    return sync_status(ctx, "solve");
+}
+
+int mh_calculate_radiation_forces(mh_ctx* ctx, const mh_mesh* mesh, const double* dof,
+                                  int64_t dof_rows, double omega, double rho, double g,
+                                  uint32_t gf_mask, int direct, int precision, double out[2])
+{
+    if (!out) return ctx ? set_err(ctx, MH_ERR_ARG, "out is NULL") : MH_ERR_ARG;
+    double2 F;
+    int rc = front_door(ctx, mesh, dof, dof_rows, omega, rho, g, gf_mask, direct, precision, false,
+                        0.0, &F);
+    if (rc) return rc;
+    out[0] = F.x / (omega * omega);  // src/waves.jl:36
+    out[1] = F.y / omega;
+    return MH_OK;
+}
+
+int mh_diffraction_force(mh_ctx* ctx, const mh_mesh* mesh, double omega, const double* dof,
+                         int64_t dof_rows, double beta, double rho, double g, uint32_t gf_mask,
+                         int direct, int precision, double out[2])
+{
+    if (!out) return ctx ? set_err(ctx, MH_ERR_ARG, "out is NULL") : MH_ERR_ARG;
+    double2 F;
+    int rc = front_door(ctx, mesh, dof, dof_rows, omega, rho, g, gf_mask, direct, precision, true,
+                        beta, &F);
+    if (rc) return rc;
+    out[0] = F.x;
+    out[1] = F.y;
+    return MH_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,74 @@
+// Internal declarations shared by the library's translation units.
+#pragma once
+#include <cublas_v2.h>
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "marinehydro_b200.h"
+
+// Device geometry of one mesh: 20 arrays of n doubles (structure of arrays,
+// so a warp reading one field of consecutive panels is one coalesced load).
+enum GeomField : int {
+    G_CX = 0, G_CY, G_CZ,      // panel centres
+    G_NX, G_NY, G_NZ,          // unit normals
+    G_AREA, G_RADIUS,          // areas, radii
+    G_V = 8,                   // vertex a, coord c at field G_V + 3*a + c (a<4, c<3)
+    G_NFIELDS = 20
+};
+
+struct mh_mesh {
+    int64_t n = 0;
+    int64_t nv = 0;
+    int device = 0;
+    double* geom = nullptr;  // device, G_NFIELDS * n doubles
+};
+
+// Workspace slots of a context; each is a grow-only device buffer.
+enum WsSlot : int {
+    WS_S = 0, WS_D, WS_RHS, WS_PHI, WS_TMP, WS_PIV, WS_INFO, WS_LWORK,
+    WS_DOF, WS_OUT, WS_NSLOTS
+};
+
+struct mh_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cublasHandle_t cublas = nullptr;
+    cusolverDnHandle_t cusolver = nullptr;
+    std::string err;
+    int64_t launches = 0;
+    void* ws[WS_NSLOTS] = {};
+    size_t ws_bytes[WS_NSLOTS] = {};
+};
+
+namespace mh {
+
+int set_err(mh_ctx* ctx, int code, const char* fmt, ...);
+// Returns a device buffer of at least `bytes` for `slot` (nullptr + error set on failure).
+void* ws_get(mh_ctx* ctx, int slot, size_t bytes);
+
+// ---- kernels (mh_kernels.cu) ----
+// S, D: n x n complex128 column-major device buffers (either may be null).
+cudaError_t launch_assemble_f64(mh_ctx* ctx, const mh_mesh* m, double k, uint32_t mask,
+                                int direct, double2* S, double2* D);
+// bc[i] = -i omega (n_i . dof_i); dof is a device 3-vector (dof_rows==1) or n x 3 col-major.
+cudaError_t launch_radiation_bc(mh_ctx* ctx, const mh_mesh* m, const double* dof, int64_t dof_rows,
+                                double omega, double2* bc);
+// bc[i] = -(v_inc(x_i) . n_i) for Airy waves (src/waves.jl:121-142).
+cudaError_t launch_airy_bc(mh_ctx* ctx, const mh_mesh* m, double omega, double beta, double g,
+                           double2* bc);
+// F = sum_j (i rho omega phi_j) * (-(n_j . dof_j)) * area_j, written to F_out (device, 1 complex).
+cudaError_t launch_force(mh_ctx* ctx, const mh_mesh* m, const double2* phi, const double* dof,
+                         int64_t dof_rows, double rho, double omega, double2* F_out);
+
+}  // namespace mh
+
+#define MH_CUDA_TRY(ctx, expr)                                                             \
+    do {                                                                                   \
+        cudaError_t _e = (expr);                                                           \
+        if (_e != cudaSuccess)                                                             \
+            return mh::set_err((ctx), MH_ERR_CUDA, "%s failed: %s", #expr,                 \
+                               cudaGetErrorString(_e));                                    \
+    } while (0)
