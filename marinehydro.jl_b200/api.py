@@ -198,8 +198,8 @@ def assemble_matrices(green_functions, mesh: Mesh, wavenumber: float, direct: bo
     S = np.empty((n, n), dtype=np.complex128, order="F")
     D = np.empty((n, n), dtype=np.complex128, order="F")
     N.check(N.lib().mh_assemble_matrices(dm.ctx.handle, dm.handle, float(wavenumber), mask,
-                                         int(bool(direct)), N.dptr(S.view(np.float64)),
-                                         N.dptr(D.view(np.float64))), dm.ctx.handle)
+                                         int(bool(direct)), N.dptr(S),
+                                         N.dptr(D)), dm.ctx.handle)
     return S, D
 
 
@@ -221,9 +221,9 @@ def solve(D, S, bc, direct: bool = True, ctx: N.Context | None = None):
     if D.shape != (n, n) or S.shape != (n, n) or b2.shape[0] != n:
         raise ValueError("solve: D and S must be n x n and bc must have n rows")
     phi = np.empty_like(b2, order="F")
-    N.check(N.lib().mh_solve(ctx.handle, n, N.dptr(D.view(np.float64)), N.dptr(S.view(np.float64)),
-                             N.dptr(b2.view(np.float64)), b2.shape[1], int(bool(direct)),
-                             N.dptr(phi.view(np.float64))), ctx.handle)
+    N.check(N.lib().mh_solve(ctx.handle, n, N.dptr(D), N.dptr(S),
+                             N.dptr(b2), b2.shape[1], int(bool(direct)),
+                             N.dptr(phi)), ctx.handle)
     return phi[:, 0].copy() if vec else phi
 
 

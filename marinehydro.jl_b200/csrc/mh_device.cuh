@@ -434,9 +434,11 @@ __device__ __noinline__ void delh_dimless(double r, double z, cplx out[3])
         for (int q = 0; q < 4; ++q) acc[q] = est[q];
     } else {
         constexpr int kStack = 52;
+        constexpr int kMaxIntervals = 4096;
         double sa[kStack], sb[kStack];
         int sd[kStack];
         int sp = 0;
+        int processed = 0;  // hard cap: a NaN error estimate must not bisect forever
         double m = 0.5 * half_pi;
         sa[sp] = m; sb[sp] = half_pi; sd[sp] = 1; ++sp;
         sa[sp] = 0.0; sb[sp] = m; sd[sp] = 1; ++sp;
@@ -446,7 +448,7 @@ __device__ __noinline__ void delh_dimless(double r, double z, cplx out[3])
             int d = sd[sp];
             double res[4], e;
             delh_gk15(a, b, r, z, res, e);
-            if (e <= tol * (b - a) || d >= 48 || sp + 2 > kStack) {
+            if (e <= tol * (b - a) || d >= 48 || sp + 2 > kStack || ++processed > kMaxIntervals) {
 #pragma unroll
                 for (int q = 0; q < 4; ++q) acc[q] += res[q];
             } else {

@@ -15,10 +15,11 @@ from typing import Sequence
 import numpy as np
 
 
-@dataclass
+@dataclass(eq=False)
 class Mesh:
     """Panel mesh (src/meshes.jl:12-37).  The constructor checks the same
-    shapes as the reference's inner constructor (src/meshes.jl:27-34)."""
+    shapes as the reference's inner constructor (src/meshes.jl:27-34).
+    Meshes compare and hash by identity (device uploads are cached per object)."""
 
     vertices: np.ndarray
     faces: np.ndarray

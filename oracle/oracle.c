@@ -462,18 +462,20 @@ static void gk15(double a, double b, double r, double z, double res[4], double* 
     *err = e;
 }
 
+/* Depth-first bisection; *budget caps the number of intervals processed so
+ * that a NaN error estimate cannot bisect forever. */
 static void adapt(double a, double b, double r, double z, double tol_per_len,
-                  int depth, double acc[4])
+                  int depth, double acc[4], int* budget)
 {
     double res[4], err;
     gk15(a, b, r, z, res, &err);
-    if (err <= tol_per_len * (b - a) || depth >= 48) {
+    if (err <= tol_per_len * (b - a) || depth >= 48 || --(*budget) < 0) {
         for (int q = 0; q < 4; ++q) acc[q] += res[q];
         return;
     }
     double m = 0.5 * (a + b);
-    adapt(a, m, r, z, tol_per_len, depth + 1, acc);
-    adapt(m, b, r, z, tol_per_len, depth + 1, acc);
+    adapt(a, m, r, z, tol_per_len, depth + 1, acc, budget);
+    adapt(m, b, r, z, tol_per_len, depth + 1, acc, budget);
 }
 
 /* exact_Guevel_Delhommeau.jl:15-26 (G), :35-46 (dG/dr), :52-59 (dG/dz) */
@@ -486,7 +488,8 @@ void orc_delhommeau_dimless(double r, double z, double out[6])
         if (fabs(est[q]) > scale) scale = fabs(est[q]);
     double tol = fmax(1e-15, 1e-13 * scale) / (0.5 * PI);
     double acc[4] = {0, 0, 0, 0};
-    adapt(0.0, 0.5 * PI, r, z, tol, 0, acc);
+    int budget = 4097;
+    adapt(0.0, 0.5 * PI, r, z, tol, 0, acc, &budget);
     out[0] = 4.0 * acc[0];
     out[1] = 4.0 * acc[1];
     out[2] = 4.0 * acc[2];

@@ -114,3 +114,15 @@ def test_host_helpers_match_oracle(mh, oracle):
                       oracle.integrate_pressure(m.normals, m.areas, p, [0, 0, 1.0]), rtol=1e-14)
     assert np.isclose(mh.FroudeKrylovForce(m, w, [0, 0, 1.0]),
                       oracle.froude_krylov_force(m, w, [0, 0, 1.0]), rtol=1e-14)
+
+
+def test_mesh_is_hashable_and_digest_tracks_changes(mh):
+    import weakref
+
+    m = mh.mesh_hemisphere(1.0, (0, 0, 0), (4, 6))
+    d = weakref.WeakKeyDictionary()
+    d[m] = 1
+    assert d[m] == 1
+    dig = mh.api._mesh_digest(m)
+    m.centers[0, 0] += 1e-3
+    assert mh.api._mesh_digest(m) != dig
