@@ -54,8 +54,19 @@ extern "C" {
 #define MH_PRECISION_FP64   0  /* FP64 assembly + FP64 LU (cuSOLVER zgetrf/zgetrs) */
 #define MH_PRECISION_MIXED  1  /* FP64-accurate matrices, low-precision LU, FP64 iterative refinement */
 
+/* evaluation of the ExactGuevelDelhommeau wave term */
+#define MH_DELHOMMEAU_TABLE  0  /* 2-D Chebyshev table built on the device from the FP64 quadrature (default) */
+#define MH_DELHOMMEAU_EXACT  1  /* adaptive Gauss-Kronrod quadrature per panel pair, as the reference */
+
 typedef struct mh_ctx mh_ctx;
 typedef struct mh_mesh mh_mesh;
+
+/* Diagnostics of a batched solve. */
+typedef struct mh_batch_info {
+    int32_t refine_iterations; /* mixed: largest number of refinement sweeps used */
+    int32_t n_fallback;        /* mixed: problems re-solved with the pivoted FP64 LU */
+    double max_rel_residual;   /* mixed: largest final max|b - A x| / max|b| per right-hand side */
+} mh_batch_info;
 
 /* ---- library / context ------------------------------------------------ */
 
@@ -77,6 +88,19 @@ const char* mh_last_error(const mh_ctx* ctx);
 
 /* Number of this library's own kernels launched on the ctx so far. */
 int mh_ctx_kernel_launches(const mh_ctx* ctx, int64_t* count);
+
+/* How ExactGuevelDelhommeau() is evaluated on this ctx: MH_DELHOMMEAU_TABLE
+ * (default) or MH_DELHOMMEAU_EXACT (per-pair adaptive quadrature, the
+ * reference's method, src/green_functions/exact_Guevel_Delhommeau.jl:8-26). */
+int mh_ctx_set_delhommeau_method(mh_ctx* ctx, int method);
+
+/* Dimensionless wave term at n points (r[i], z[i]), z < 0, on the device:
+ * out[6*i .. 6*i+5] = (G, dG/dr, dG/dz) as (re, im) pairs.  `which` is
+ * MH_GF_WU (wu.jl:19-30) or MH_GF_DELHOMMEAU (exact_Guevel_Delhommeau.jl:15-59
+ * through the ctx's method).  Replaces the reference's test hooks
+ * `_dimless_wave_term` / `_d_dimless_wave_term_dr`. */
+int mh_wave_term(mh_ctx* ctx, uint32_t which, int64_t n, const double* r, const double* z,
+                 double* out);
 
 /* ---- meshes ------------------------------------------------------------ */
 
@@ -138,6 +162,37 @@ int mh_diffraction_force(mh_ctx* ctx, const mh_mesh* mesh, double omega,
                          const double* dof, int64_t dof_rows, double beta,
                          double rho, double g, uint32_t gf_mask, int direct,
                          int precision, double out[2]);
+
+/* ---- batched driver ---------------------------------------------------- */
+
+/* Hydrodynamic coefficients of one mesh over n_omega frequencies, every
+ * degree of freedom radiating and influenced, and n_beta incident-wave
+ * headings.  Replaces `compute_hydrodynamic_coefficients(parameters, body)`
+ * (src/problems_and_results.jl:231-236) with parameters = (wave_frequencies,
+ * radiating_dofs = influenced_dofs = all dofs, wave_directions): the
+ * reference solves one problem per (omega, dof) and (omega, beta)
+ * re-assembling each time (src/solve.jl:4-13); here each frequency is
+ * assembled once and all its right-hand sides share one factorisation.
+ *   dofs          n_dof motion fields, each nfaces x 3 column-major
+ *                 (FloatingBody dofs, src/bodies.jl:63-89), concatenated
+ *   n_dof + n_beta <= 16
+ *   added_mass, damping      n_dof x n_dof x n_omega  ([influenced, radiating, omega])
+ *   diffraction, froude_krylov  complex n_dof x n_omega x n_beta ([dof, omega, beta])
+ *   (any output may be NULL)
+ *   precision     MH_PRECISION_FP64 or MH_PRECISION_MIXED
+ *   tol, max_iter mixed only: refinement stops when max|b - A x|/max|b| <= tol
+ *                 for every right-hand side; problems that do not get there in
+ *                 max_iter sweeps are re-solved in FP64 (info->n_fallback).
+ * The mixed path accepts at most one wave term (GFWu or Delhommeau). */
+int mh_hydro_batch(mh_ctx* ctx, const mh_mesh* mesh,
+                   int64_t n_omega, const double* omegas,
+                   int64_t n_dof, const double* dofs,
+                   int64_t n_beta, const double* betas,
+                   double rho, double g, uint32_t gf_mask, int direct, int precision,
+                   double tol, int max_iter,
+                   double* added_mass, double* damping,
+                   double* diffraction, double* froude_krylov,
+                   mh_batch_info* info);
 
 #ifdef __cplusplus
 }

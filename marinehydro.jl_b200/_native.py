@@ -24,6 +24,9 @@ MH_ERR_OOM = 5
 MH_ERR_NO_DEVICE = 6
 MH_ERR_SINGULAR = 7
 
+MH_DELHOMMEAU_TABLE = 0
+MH_DELHOMMEAU_EXACT = 1
+
 MH_PRECISION_FP64 = 0
 MH_PRECISION_MIXED = 1
 
@@ -63,6 +66,8 @@ SIGNATURES = {
     "mh_ctx_destroy": (ctypes.c_int, [_P]),
     "mh_last_error": (ctypes.c_char_p, [_P]),
     "mh_ctx_kernel_launches": (ctypes.c_int, [_P, _I64]),
+    "mh_ctx_set_delhommeau_method": (ctypes.c_int, [_P, ctypes.c_int]),
+    "mh_wave_term": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_int64, _D, _D, _D]),
     "mh_mesh_create": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_int64, _D, _I64, _D, _D, _D, _D,
                                       ctypes.POINTER(_P)]),
     "mh_mesh_destroy": (ctypes.c_int, [_P, _P]),
@@ -145,6 +150,21 @@ class Context:
     @property
     def handle(self):
         return self._h
+
+    def set_delhommeau_method(self, method: str):
+        """'table' (default) or 'exact' (per-pair adaptive quadrature)."""
+        code = {"table": MH_DELHOMMEAU_TABLE, "exact": MH_DELHOMMEAU_EXACT}[method]
+        check(lib().mh_ctx_set_delhommeau_method(self._h, code), self._h)
+
+    def wave_term(self, which: int, r, z):
+        """Dimensionless (G, dG/dr, dG/dz) at points (r, z) on the device."""
+        r = np.ascontiguousarray(r, dtype=np.float64).reshape(-1)
+        z = np.ascontiguousarray(z, dtype=np.float64).reshape(-1)
+        out = np.empty((r.shape[0], 6))
+        check(lib().mh_wave_term(self._h, int(which), r.shape[0], dptr(r), dptr(z), dptr(out)),
+              self._h)
+        c = out[:, 0::2] + 1j * out[:, 1::2]
+        return c[:, 0], c[:, 1], c[:, 2]
 
     def kernel_launches(self) -> int:
         c = ctypes.c_int64(0)

@@ -196,7 +196,9 @@ int front_door(mh_ctx* ctx, const mh_mesh* m, const double* dof, int64_t dof_row
     double* d_dof = nullptr;
     if ((rc = dof_upload(ctx, m, dof, dof_rows, &d_dof))) return rc;
     const double k = omega * omega / g;
-    MH_CUDA_TRY(ctx, mh::launch_assemble_f64(ctx, m, k, gf_mask, direct, S, D));
+    const double* tab = mh::delh_table_for(ctx, gf_mask, &rc);
+    if (rc) return rc;
+    MH_CUDA_TRY(ctx, mh::launch_assemble_f64(ctx, m, k, gf_mask, direct, tab, S, D));
     if (diffraction) MH_CUDA_TRY(ctx, mh::launch_airy_bc(ctx, m, omega, beta, g, bc));
     else MH_CUDA_TRY(ctx, mh::launch_radiation_bc(ctx, m, d_dof, dof_rows, omega, bc));
     if ((rc = solve_fp64_device(ctx, n, D, S, bc, 1, direct, phi))) return rc;
@@ -263,6 +265,7 @@ int mh_ctx_destroy(mh_ctx* ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     for (int s = 0; s < WS_NSLOTS; ++s)
         if (ctx->ws[s]) cudaFree(ctx->ws[s]);
+    if (ctx->delh_table) cudaFree(ctx->delh_table);
     if (ctx->cusolver) cusolverDnDestroy(ctx->cusolver);
     if (ctx->cublas) cublasDestroy(ctx->cublas);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -280,6 +283,36 @@ int mh_ctx_kernel_launches(const mh_ctx* ctx, int64_t* count)
     if (!ctx || !count) return MH_ERR_ARG;
     *count = ctx->launches;
     return MH_OK;
+}
+
+int mh_ctx_set_delhommeau_method(mh_ctx* ctx, int method)
+{
+    int rc;
+    if ((rc = check_ctx(ctx))) return rc;
+    if (method != MH_DELHOMMEAU_TABLE && method != MH_DELHOMMEAU_EXACT)
+        return set_err(ctx, MH_ERR_ARG, "unknown Delhommeau method %d", method);
+    ctx->delh_method = method;
+    return MH_OK;
+}
+
+int mh_wave_term(mh_ctx* ctx, uint32_t which, int64_t n, const double* r, const double* z,
+                 double* out)
+{
+    int rc;
+    if ((rc = check_ctx(ctx))) return rc;
+    if (which != MH_GF_WU && which != MH_GF_DELHOMMEAU)
+        return set_err(ctx, MH_ERR_ARG, "mh_wave_term evaluates MH_GF_WU or MH_GF_DELHOMMEAU");
+    if (n <= 0 || !r || !z || !out) return set_err(ctx, MH_ERR_ARG, "bad point arrays");
+    const double* tab = mh::delh_table_for(ctx, which, &rc);
+    if (rc) return rc;
+    size_t b = sizeof(double) * (size_t)n;
+    auto* d = (double*)ws_get(ctx, WS_TMP, b * 8);
+    if (!d) return MH_ERR_OOM;
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(d, r, b, cudaMemcpyHostToDevice, ctx->stream));
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(d + n, z, b, cudaMemcpyHostToDevice, ctx->stream));
+    MH_CUDA_TRY(ctx, mh::launch_wave_term(ctx, tab, which, n, d, d + n, d + 2 * n));
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(out, d + 2 * n, 6 * b, cudaMemcpyDeviceToHost, ctx->stream));
+    return sync_status(ctx, "wave term");
 }
 
 int mh_mesh_create(mh_ctx* ctx, int64_t nfaces, int64_t nvertices, const double* vertices,
@@ -372,8 +405,10 @@ int mh_assemble_matrices_device(mh_ctx* ctx, const mh_mesh* mesh, double wavenum
     if ((gf_mask & (MH_GF_WU | MH_GF_DELHOMMEAU)) && !(wavenumber > 0.0))
         return set_err(ctx, MH_ERR_ARG, "wave terms need a positive wavenumber");
     if (!S_dev && !D_dev) return MH_OK;
-    MH_CUDA_TRY(ctx, mh::launch_assemble_f64(ctx, mesh, wavenumber, gf_mask, direct, (double2*)S_dev,
-                                             (double2*)D_dev));
+    const double* tab = mh::delh_table_for(ctx, gf_mask, &rc);
+    if (rc) return rc;
+    MH_CUDA_TRY(ctx, mh::launch_assemble_f64(ctx, mesh, wavenumber, gf_mask, direct, tab,
+                                             (double2*)S_dev, (double2*)D_dev));
     return sync_status(ctx, "assembly");
 }
 
@@ -442,6 +477,40 @@ int mh_diffraction_force(mh_ctx* ctx, const mh_mesh* mesh, double omega, const d
     out[0] = F.x;
     out[1] = F.y;
     return MH_OK;
+}
+
+int mh_hydro_batch(mh_ctx* ctx, const mh_mesh* mesh, int64_t n_omega, const double* omegas,
+                   int64_t n_dof, const double* dofs, int64_t n_beta, const double* betas,
+                   double rho, double g, uint32_t gf_mask, int direct, int precision, double tol,
+                   int max_iter, double* added_mass, double* damping, double* diffraction,
+                   double* froude_krylov, mh_batch_info* info)
+{
+    int rc;
+    if ((rc = check_ctx(ctx))) return rc;
+    if ((rc = check_mesh(ctx, mesh))) return rc;
+    if ((rc = valid_mask(ctx, gf_mask))) return rc;
+    if (n_omega <= 0 || !omegas) return set_err(ctx, MH_ERR_ARG, "need at least one frequency");
+    for (int64_t z = 0; z < n_omega; ++z)
+        if (!(omegas[z] > 0.0) || !std::isfinite(omegas[z]))
+            return set_err(ctx, MH_ERR_ARG, "frequencies must be positive and finite");
+    if (n_dof < 1 || n_beta < 0 || n_dof + n_beta > kMaxRhs)
+        return set_err(ctx, MH_ERR_ARG, "need 1 <= n_dof and n_dof + n_beta <= %d", kMaxRhs);
+    if (!dofs || (n_beta > 0 && !betas)) return set_err(ctx, MH_ERR_ARG, "dofs / betas is NULL");
+    if (!finite_array(dofs, 3 * mesh->n * n_dof) || (n_beta && !finite_array(betas, n_beta)))
+        return set_err(ctx, MH_ERR_ARG, "dofs and betas must be finite");
+    if (!(g > 0.0) || !std::isfinite(g) || !std::isfinite(rho))
+        return set_err(ctx, MH_ERR_ARG, "g must be positive and rho finite");
+    if (precision != MH_PRECISION_FP64 && precision != MH_PRECISION_MIXED)
+        return set_err(ctx, MH_ERR_ARG, "unknown precision %d", precision);
+    if (precision == MH_PRECISION_MIXED) {
+        if (!(tol > 0.0) || max_iter < 1 || max_iter > 100)
+            return set_err(ctx, MH_ERR_ARG, "mixed precision needs tol > 0 and 1 <= max_iter <= 100");
+        if ((gf_mask & MH_GF_WU) && (gf_mask & MH_GF_DELHOMMEAU))
+            return set_err(ctx, MH_ERR_ARG, "the mixed path takes one wave term (GFWu or Delhommeau)");
+    }
+    return mh::hydro_batch(ctx, mesh, n_omega, omegas, n_dof, dofs, n_beta, betas, rho, g, gf_mask,
+                           direct, precision, tol, max_iter, added_mass, damping, diffraction,
+                           froude_krylov, info);
 }
 
 }  // extern "C"

@@ -1,0 +1,572 @@
+// Batched hydrodynamic coefficients: many frequencies of one mesh, every
+// radiating degree of freedom and every incident-wave heading at once.
+//
+// Replaces the reference's problem loop (src/solve.jl:4-21 over
+// src/problems_and_results.jl:70-100, assembled per problem) with one call:
+//
+//   FP64 (MH_PRECISION_FP64): per frequency, FP64 assembly of S and D (or K),
+//     S*BC with cuBLAS, zgetrf/zgetrs from cuSOLVER, force reduction.
+//   mixed (MH_PRECISION_MIXED): the frequency-independent Rankine part of S
+//     and D once per call; per frequency the wave part is added in FP64 and
+//     written twice, an FP64 master copy for residuals and an FP32 copy that
+//     is LU-factorised without pivoting (batched over frequencies); FP64
+//     iterative refinement r = b - D x, x += LU^-1 r until
+//     max|r|/max|b| <= tol per right-hand side.  A problem whose FP32 LU
+//     meets a bad pivot or does not converge is re-solved with the pivoted
+//     FP64 LU (counted in mh_batch_info.n_fallback).
+#include <cuComplex.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "mh_device.cuh"
+#include "mh_internal.h"
+
+namespace mh {
+namespace {
+
+constexpr int kRows = 128;
+constexpr int kCols = 16;
+constexpr double kInv4Pi = 1.0 / (4.0 * kPi);
+constexpr size_t kBatchBytes = 16ull << 30;  // device memory budget of one frequency chunk
+
+__device__ __forceinline__ void load_panel_field(Panel& p, int f, double v)
+{
+    if (f < 3) p.c[f] = v;
+    else if (f < 6) p.n[f - 3] = v;
+    else if (f == G_AREA) p.area = v;
+    else if (f == G_RADIUS) p.radius = v;
+    else p.v[f - G_V] = v;
+}
+
+__device__ __forceinline__ void stage_panels(Panel* sp, const double* __restrict__ geom, int64_t n,
+                                             int64_t j0)
+{
+    for (int t = threadIdx.x; t < kCols * G_NFIELDS; t += blockDim.x) {
+        int f = t / kCols, jj = t % kCols;
+        int64_t j = j0 + jj;
+        load_panel_field(sp[jj], f, (j < n) ? geom[(int64_t)f * n + j] : 0.0);
+    }
+}
+
+// Rankine / reflected terms (real, frequency independent), with the -1/(4 pi)
+// factor and the 1/2 diagonal of D already applied.
+__global__ void __launch_bounds__(kRows)
+k_rankine_real(const double* __restrict__ geom, int64_t n, uint32_t mask, int direct,
+               double* __restrict__ SR, double* __restrict__ DR)
+{
+    __shared__ Panel sp[kCols];
+    const int64_t j0 = (int64_t)blockIdx.y * kCols;
+    stage_panels(sp, geom, n, j0);
+    __syncthreads();
+    const int64_t i = (int64_t)blockIdx.x * kRows + threadIdx.x;
+    if (i >= n) return;
+    const double x[3] = {geom[G_CX * n + i], geom[G_CY * n + i], geom[G_CZ * n + i]};
+    const double ni[3] = {geom[G_NX * n + i], geom[G_NY * n + i], geom[G_NZ * n + i]};
+    const int jend = (int)min((int64_t)kCols, n - j0);
+    for (int jj = 0; jj < jend; ++jj) {
+        const Panel& p = sp[jj];
+        const int64_t j = j0 + jj;
+        cplx s, g[3];
+        pair_integrals(x, p, 0.0, mask, !direct, nullptr, s, g);
+        const double* nn = direct ? p.n : ni;
+        const int64_t o = j * n + i;
+        SR[o] = -kInv4Pi * s.re;
+        DR[o] = (i == j ? 0.5 : 0.0) - kInv4Pi * (nn[0] * g[0].re + nn[1] * g[1].re + nn[2] * g[2].re);
+    }
+}
+
+// Per frequency z = blockIdx.z: S = SR + wave, D = DR + wave, written as FP64
+// complex (S64, D64) and the FP32 LU copy of D (Dlo).
+template <bool kDelh>
+__global__ void __launch_bounds__(kRows)
+k_wave_batch(const double* __restrict__ geom, int64_t n, int direct, const double* __restrict__ tab,
+             const double* __restrict__ kvec, const double* __restrict__ SR,
+             const double* __restrict__ DR, double2* __restrict__ S64, double2* __restrict__ D64,
+             float2* __restrict__ Dlo)
+{
+    __shared__ Panel sp[kCols];
+    const int64_t j0 = (int64_t)blockIdx.y * kCols;
+    stage_panels(sp, geom, n, j0);
+    __syncthreads();
+    const int64_t i = (int64_t)blockIdx.x * kRows + threadIdx.x;
+    if (i >= n) return;
+    const double k = kvec[blockIdx.z];
+    const int64_t mat = (int64_t)blockIdx.z * n * n;
+    const double x[3] = {geom[G_CX * n + i], geom[G_CY * n + i], geom[G_CZ * n + i]};
+    const double ni[3] = {geom[G_NX * n + i], geom[G_NY * n + i], geom[G_NZ * n + i]};
+    const int jend = (int)min((int64_t)kCols, n - j0);
+    for (int jj = 0; jj < jend; ++jj) {
+        const Panel& p = sp[jj];
+        const int64_t j = j0 + jj;
+        cplx s, g[3];
+        wave_pair<kDelh>(x, p, k, !direct, tab, s, g);
+        const double* nn = direct ? p.n : ni;
+        const int64_t o = j * n + i;
+        double sr = SR[o] - kInv4Pi * s.re, si = -kInv4Pi * s.im;
+        double dr = DR[o] - kInv4Pi * (nn[0] * g[0].re + nn[1] * g[1].re + nn[2] * g[2].re);
+        double di = -kInv4Pi * (nn[0] * g[0].im + nn[1] * g[1].im + nn[2] * g[2].im);
+        S64[mat + o] = make_double2(sr, si);
+        D64[mat + o] = make_double2(dr, di);
+        Dlo[mat + o] = make_float2((float)dr, (float)di);
+    }
+}
+
+// Copies of the Rankine part when the Green-function tuple has no wave term.
+__global__ void k_no_wave_batch(int64_t nn, const double* __restrict__ SR,
+                                const double* __restrict__ DR, double2* __restrict__ S64,
+                                double2* __restrict__ D64, float2* __restrict__ Dlo)
+{
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nn) return;
+    const int64_t mat = (int64_t)blockIdx.y * nn;
+    S64[mat + t] = make_double2(SR[t], 0.0);
+    D64[mat + t] = make_double2(DR[t], 0.0);
+    Dlo[mat + t] = make_float2((float)DR[t], 0.f);
+}
+
+// Boundary conditions of every right-hand side of frequency blockIdx.y:
+// q < ndof: radiation -i omega (n . dof_q) (src/waves.jl:89-101);
+// q >= ndof: incident Airy wave of heading beta_{q-ndof} (src/waves.jl:121-142).
+__global__ void k_bc_batch(const double* __restrict__ geom, int64_t n, const double* __restrict__ dofs,
+                           int ndof, const double* __restrict__ betas, int nbeta,
+                           const double* __restrict__ omegas, double gacc, double2* __restrict__ BC)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int nrhs = ndof + nbeta;
+    const double w = omegas[blockIdx.y];
+    double2* out = BC + (int64_t)blockIdx.y * n * nrhs;
+    const double nx = geom[G_NX * n + i], ny = geom[G_NY * n + i], nz = geom[G_NZ * n + i];
+    for (int q = 0; q < ndof; ++q) {
+        const double* d = dofs + (int64_t)q * 3 * n;
+        double nd = nx * d[i] + ny * d[n + i] + nz * d[2 * n + i];
+        out[(int64_t)q * n + i] = make_double2(0.0, -w * nd);
+    }
+    const double k = w * w / gacc;
+    const double x = geom[G_CX * n + i], y = geom[G_CY * n + i], z = geom[G_CZ * n + i];
+    const double cih = exp(k * z), f = gacc * k / w;
+    for (int b = 0; b < nbeta; ++b) {
+        double cb, sb, cw, sw;
+        sincos(betas[b], &sb, &cb);
+        sincos(k * (x * cb + y * sb), &sw, &cw);
+        cplx e = mk(f * cw, f * sw);
+        cplx vn = e * (cb * cih * nx) + e * (sb * cih * ny) + e * mk(0.0, -cih * nz);
+        out[(int64_t)(ndof + b) * n + i] = make_double2(-vn.re, -vn.im);
+    }
+}
+
+// Forces of right-hand side q of frequency z (blockIdx.x = z*nrhs + q):
+// F_i = sum_j (i rho omega phi_j) * (-(n_j . dof_i,j)) * area_j for every
+// influenced dof i (src/waves.jl:72-85); for diffraction right-hand sides
+// also the Froude-Krylov force of the same heading (src/waves.jl:157-163).
+__global__ void __launch_bounds__(256)
+k_forces_batch(const double* __restrict__ geom, int64_t n, const double* __restrict__ dofs, int ndof,
+               const double* __restrict__ betas, int nbeta, const double* __restrict__ omegas,
+               double rho, double gacc, const double2* __restrict__ phi, double2* __restrict__ F,
+               double2* __restrict__ FK)
+{
+    const int nrhs = ndof + nbeta;
+    const int z = blockIdx.x / nrhs, q = blockIdx.x % nrhs;
+    const double w = omegas[z];
+    const double2* ph = phi + ((int64_t)z * nrhs + q) * n;
+    const bool diff = q >= ndof;
+    double fr[kMaxRhs], fi[kMaxRhs], kr[kMaxRhs], ki[kMaxRhs];
+    for (int d = 0; d < ndof; ++d) fr[d] = fi[d] = kr[d] = ki[d] = 0.0;
+    double k = w * w / gacc, cb = 1.0, sb = 0.0;
+    if (diff) sincos(betas[q - ndof], &sb, &cb);
+    for (int64_t j = threadIdx.x; j < n; j += blockDim.x) {
+        const double nx = geom[G_NX * n + j], ny = geom[G_NY * n + j], nz = geom[G_NZ * n + j];
+        const double a = geom[G_AREA * n + j];
+        // i rho omega phi
+        const double pr = -rho * w * ph[j].y, pi = rho * w * ph[j].x;
+        double ar = 0.0, ai = 0.0;
+        if (diff) {  // airy pressure i omega rho phi_inc = rho g e^{kz} e^{i k wbar}
+            const double x = geom[G_CX * n + j], y = geom[G_CY * n + j], zz = geom[G_CZ * n + j];
+            double sw, cw;
+            sincos(k * (x * cb + y * sb), &sw, &cw);
+            const double m = rho * gacc * exp(k * zz);
+            ar = m * cw;
+            ai = m * sw;
+        }
+        for (int d = 0; d < ndof; ++d) {
+            const double* dd = dofs + (int64_t)d * 3 * n;
+            const double wgt = -(nx * dd[j] + ny * dd[n + j] + nz * dd[2 * n + j]) * a;
+            fr[d] += pr * wgt;
+            fi[d] += pi * wgt;
+            kr[d] += ar * wgt;
+            ki[d] += ai * wgt;
+        }
+    }
+    __shared__ double red[8][4 * kMaxRhs];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int d = 0; d < ndof; ++d) {
+        double v[4] = {fr[d], fi[d], kr[d], ki[d]};
+        for (int c = 0; c < 4; ++c) {
+            double s = v[c];
+            for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+            if (lane == 0) red[warp][4 * d + c] = s;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 4 * ndof) {
+        double s = 0.0;
+        for (int wp = 0; wp < (int)(blockDim.x >> 5); ++wp) s += red[wp][threadIdx.x];
+        red[0][threadIdx.x] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < ndof) {
+        const int d = threadIdx.x;
+        F[((int64_t)z * nrhs + q) * ndof + d] = make_double2(red[0][4 * d], red[0][4 * d + 1]);
+        if (diff)
+            FK[((int64_t)z * nbeta + (q - ndof)) * ndof + d] =
+                make_double2(red[0][4 * d + 2], red[0][4 * d + 3]);
+    }
+}
+
+__global__ void k_to_f32(const double2* __restrict__ a, float2* __restrict__ b, int64_t count)
+{
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < count) b[t] = make_float2((float)a[t].x, (float)a[t].y);
+}
+
+__global__ void k_add_f32(double2* __restrict__ x, const float2* __restrict__ d, int64_t count)
+{
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < count) x[t] = make_double2(x[t].x + (double)d[t].x, x[t].y + (double)d[t].y);
+}
+
+// Per (frequency z = blockIdx.x): max over right-hand sides of
+// max_i |r_iq| / max_i |b_iq|.
+__global__ void __launch_bounds__(256)
+k_rel_residual(const double2* __restrict__ r, const double2* __restrict__ b, int64_t n, int nrhs,
+               double* __restrict__ out)
+{
+    __shared__ double sr[256], sb[256];
+    double worst = 0.0;
+    for (int q = 0; q < nrhs; ++q) {
+        const int64_t off = ((int64_t)blockIdx.x * nrhs + q) * n;
+        double mr = 0.0, mb = 0.0;
+        for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+            mr = fmax(mr, hypot(r[off + i].x, r[off + i].y));
+            mb = fmax(mb, hypot(b[off + i].x, b[off + i].y));
+        }
+        sr[threadIdx.x] = mr;
+        sb[threadIdx.x] = mb;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+            if (threadIdx.x < s) {
+                sr[threadIdx.x] = fmax(sr[threadIdx.x], sr[threadIdx.x + s]);
+                sb[threadIdx.x] = fmax(sb[threadIdx.x], sb[threadIdx.x + s]);
+            }
+            __syncthreads();
+        }
+        if (sb[0] > 0.0) worst = fmax(worst, sr[0] / sb[0]);
+        else if (sr[0] > 0.0 || sr[0] != sr[0]) worst = INFINITY;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = (worst == worst) ? worst : INFINITY;
+}
+
+// ---------------------------------------------------------------------------
+// host orchestration
+// ---------------------------------------------------------------------------
+
+struct Batch {
+    mh_ctx* ctx;
+    const mh_mesh* m;
+    int64_t n;
+    int ndof, nbeta, nrhs;
+    const double* d_dofs;
+    const double* d_betas;
+    double rho, g;
+    uint32_t mask;
+    int direct;
+};
+
+unsigned blocks(int64_t count, int threads) { return (unsigned)((count + threads - 1) / threads); }
+
+int zgemm_strided(mh_ctx* ctx, int64_t n, int nrhs, const double2* A, const double2* B, double2* C,
+                  int nb, double alpha_re, double beta_re)
+{
+    const cuDoubleComplex alpha = make_cuDoubleComplex(alpha_re, 0.0);
+    const cuDoubleComplex beta = make_cuDoubleComplex(beta_re, 0.0);
+    cublasStatus_t st = cublasZgemmStridedBatched(
+        ctx->cublas, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, nrhs, (int)n, &alpha,
+        (const cuDoubleComplex*)A, (int)n, n * n, (const cuDoubleComplex*)B, (int)n, n * nrhs, &beta,
+        (cuDoubleComplex*)C, (int)n, n * nrhs, nb);
+    if (st != CUBLAS_STATUS_SUCCESS)
+        return set_err(ctx, MH_ERR_CUDA, "cublasZgemmStridedBatched failed (%d)", (int)st);
+    return MH_OK;
+}
+
+int fp64_lu_solve(mh_ctx* ctx, int64_t n, double2* A, double2* B, int nrhs)
+{
+    int lwork = 0;
+    cusolverStatus_t st = cusolverDnZgetrf_bufferSize(ctx->cusolver, (int)n, (int)n,
+                                                      (cuDoubleComplex*)A, (int)n, &lwork);
+    if (st != CUSOLVER_STATUS_SUCCESS)
+        return set_err(ctx, MH_ERR_CUDA, "cusolverDnZgetrf_bufferSize failed (%d)", (int)st);
+    auto* work = (cuDoubleComplex*)ws_get(ctx, WS_LWORK, sizeof(cuDoubleComplex) * (size_t)lwork);
+    auto* piv = (int*)ws_get(ctx, WS_PIV, sizeof(int) * (size_t)n);
+    auto* info = (int*)ws_get(ctx, WS_INFO, sizeof(int) * 2);
+    if (!work || !piv || !info) return MH_ERR_OOM;
+    st = cusolverDnZgetrf(ctx->cusolver, (int)n, (int)n, (cuDoubleComplex*)A, (int)n, work, piv, info);
+    if (st != CUSOLVER_STATUS_SUCCESS)
+        return set_err(ctx, MH_ERR_CUDA, "cusolverDnZgetrf failed (%d)", (int)st);
+    st = cusolverDnZgetrs(ctx->cusolver, CUBLAS_OP_N, (int)n, nrhs, (const cuDoubleComplex*)A, (int)n,
+                          piv, (cuDoubleComplex*)B, (int)n, info + 1);
+    if (st != CUSOLVER_STATUS_SUCCESS)
+        return set_err(ctx, MH_ERR_CUDA, "cusolverDnZgetrs failed (%d)", (int)st);
+    int h[2] = {0, 0};
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(h, info, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    MH_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (h[0] > 0) return set_err(ctx, MH_ERR_SINGULAR, "zero pivot at column %d", h[0]);
+    return MH_OK;
+}
+
+// FP64 path: one frequency at a time.
+int run_fp64(const Batch& bt, const double* d_omegas, int nomega, double2* d_F, double2* d_FK)
+{
+    mh_ctx* ctx = bt.ctx;
+    const int64_t n = bt.n;
+    const size_t mat = sizeof(double2) * (size_t)n * (size_t)n;
+    const size_t vec = sizeof(double2) * (size_t)n * (size_t)bt.nrhs;
+    auto* S = (double2*)ws_get(ctx, WS_S, mat);
+    auto* D = (double2*)ws_get(ctx, WS_D, mat);
+    auto* BC = (double2*)ws_get(ctx, WS_RHS, vec);
+    auto* X = (double2*)ws_get(ctx, WS_PHI, vec);
+    if (!S || !D || !BC || !X) return MH_ERR_OOM;
+    int rc;
+    const double* tab = delh_table_for(ctx, bt.mask, &rc);
+    if (rc) return rc;
+    std::vector<double> h_w(nomega);
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(h_w.data(), d_omegas, sizeof(double) * nomega,
+                                     cudaMemcpyDeviceToHost, ctx->stream));
+    MH_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int z = 0; z < nomega; ++z) {
+        const double k = h_w[z] * h_w[z] / bt.g;
+        MH_CUDA_TRY(ctx, launch_assemble_f64(ctx, bt.m, k, bt.mask, bt.direct, tab, S, D));
+        k_bc_batch<<<dim3(blocks(n, 256), 1), 256, 0, ctx->stream>>>(
+            bt.m->geom, n, bt.d_dofs, bt.ndof, bt.d_betas, bt.nbeta, d_omegas + z, bt.g, BC);
+        ctx->launches += 1;
+        if (bt.direct) {
+            if ((rc = zgemm_strided(ctx, n, bt.nrhs, S, BC, X, 1, 1.0, 0.0))) return rc;
+            if ((rc = fp64_lu_solve(ctx, n, D, X, bt.nrhs))) return rc;
+        } else {
+            if ((rc = fp64_lu_solve(ctx, n, D, BC, bt.nrhs))) return rc;
+            if ((rc = zgemm_strided(ctx, n, bt.nrhs, S, BC, X, 1, 1.0, 0.0))) return rc;
+        }
+        k_forces_batch<<<bt.nrhs, 256, 0, ctx->stream>>>(
+            bt.m->geom, n, bt.d_dofs, bt.ndof, bt.d_betas, bt.nbeta, d_omegas + z, bt.rho, bt.g, X,
+            d_F + (int64_t)z * bt.nrhs * bt.ndof, d_FK + (int64_t)z * bt.nbeta * bt.ndof);
+        ctx->launches += 1;
+        MH_CUDA_TRY(ctx, cudaGetLastError());
+    }
+    return MH_OK;
+}
+
+// Mixed path for one chunk of `nb` frequencies.
+int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, int nb,
+                    const double* SR, const double* DR, double tol, int max_iter, double2* d_F,
+                    double2* d_FK, mh_batch_info* info)
+{
+    mh_ctx* ctx = bt.ctx;
+    const int64_t n = bt.n, nn = n * n;
+    const int nrhs = bt.nrhs;
+    const int64_t nv = n * nrhs;
+    auto* S64 = (double2*)ws_get(ctx, WS_S, sizeof(double2) * nn * nb);
+    auto* D64 = (double2*)ws_get(ctx, WS_D, sizeof(double2) * nn * nb);
+    auto* Dlo = (float2*)ws_get(ctx, WS_LO, sizeof(float2) * nn * nb);
+    auto* Dinv = (float2*)ws_get(ctx, WS_DINV, sizeof(float2) * lu_dinv_stride(n) * nb);
+    auto* BC = (double2*)ws_get(ctx, WS_RHS, sizeof(double2) * nv * nb);
+    auto* X = (double2*)ws_get(ctx, WS_PHI, sizeof(double2) * nv * nb);
+    auto* R = (double2*)ws_get(ctx, WS_TMP, sizeof(double2) * nv * nb * 2);
+    auto* R32 = (float2*)ws_get(ctx, WS_TMP32, sizeof(float2) * nv * nb);
+    auto* misc = (char*)ws_get(ctx, WS_MISC, (sizeof(double) + sizeof(int)) * nb + 64);
+    if (!S64 || !D64 || !Dlo || !Dinv || !BC || !X || !R || !R32 || !misc) return MH_ERR_OOM;
+    double2* RHS = R + nv * nb;  // right-hand side of the D (or K) system
+    auto* d_res = (double*)misc;
+    auto* d_bad = (int*)(misc + sizeof(double) * nb);
+    int rc;
+    const double* tab = delh_table_for(ctx, bt.mask, &rc);
+    if (rc) return rc;
+    // matrices
+    const uint32_t wave = bt.mask & (MH_GF_WU | MH_GF_DELHOMMEAU);
+    dim3 grid(blocks(n, kRows), blocks(n, kCols), (unsigned)nb);
+    if (wave == MH_GF_WU)
+        k_wave_batch<false><<<grid, kRows, 0, ctx->stream>>>(bt.m->geom, n, bt.direct, nullptr, d_k, SR,
+                                                            DR, S64, D64, Dlo);
+    else if (wave == MH_GF_DELHOMMEAU)
+        k_wave_batch<true><<<grid, kRows, 0, ctx->stream>>>(bt.m->geom, n, bt.direct, tab, d_k, SR, DR,
+                                                           S64, D64, Dlo);
+    else if (wave == 0)
+        k_no_wave_batch<<<dim3(blocks(nn, 256), nb), 256, 0, ctx->stream>>>(nn, SR, DR, S64, D64, Dlo);
+    else
+        return set_err(ctx, MH_ERR_ARG, "the mixed path takes one wave term (GFWu or Delhommeau)");
+    ctx->launches += 1;
+    k_bc_batch<<<dim3(blocks(n, 256), nb), 256, 0, ctx->stream>>>(
+        bt.m->geom, n, bt.d_dofs, bt.ndof, bt.d_betas, bt.nbeta, d_omegas, bt.g, BC);
+    ctx->launches += 1;
+    MH_CUDA_TRY(ctx, cudaGetLastError());
+    if (bt.direct) {
+        if ((rc = zgemm_strided(ctx, n, nrhs, S64, BC, RHS, nb, 1.0, 0.0))) return rc;
+    } else {
+        MH_CUDA_TRY(ctx, cudaMemcpyAsync(RHS, BC, sizeof(double2) * nv * nb, cudaMemcpyDeviceToDevice,
+                                         ctx->stream));
+    }
+    // FP32 LU of every D (or K)
+    MH_CUDA_TRY(ctx, cudaMemsetAsync(d_bad, 0, sizeof(int) * nb, ctx->stream));
+    MH_CUDA_TRY(ctx, launch_lu_f32(ctx, Dlo, n, nn, nb, Dinv, d_bad));
+    // refinement: x = 0, r = rhs
+    MH_CUDA_TRY(ctx, cudaMemsetAsync(X, 0, sizeof(double2) * nv * nb, ctx->stream));
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(R, RHS, sizeof(double2) * nv * nb, cudaMemcpyDeviceToDevice,
+                                     ctx->stream));
+    std::vector<double> h_res(nb);
+    std::vector<int> h_bad(nb);
+    const int64_t cnt = nv * nb;
+    int it = 0;
+    double worst = INFINITY;
+    for (it = 1; it <= max_iter; ++it) {
+        k_to_f32<<<blocks(cnt, 256), 256, 0, ctx->stream>>>(R, R32, cnt);
+        ctx->launches += 1;
+        MH_CUDA_TRY(ctx, launch_lu_solve_f32(ctx, Dlo, n, nn, nb, Dinv, R32, nv, nrhs));
+        k_add_f32<<<blocks(cnt, 256), 256, 0, ctx->stream>>>(X, R32, cnt);
+        ctx->launches += 1;
+        // R = RHS - D X
+        MH_CUDA_TRY(ctx, cudaMemcpyAsync(R, RHS, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice,
+                                         ctx->stream));
+        if ((rc = zgemm_strided(ctx, n, nrhs, D64, X, R, nb, -1.0, 1.0))) return rc;
+        k_rel_residual<<<nb, 256, 0, ctx->stream>>>(R, RHS, n, nrhs, d_res);
+        ctx->launches += 1;
+        MH_CUDA_TRY(ctx, cudaMemcpyAsync(h_res.data(), d_res, sizeof(double) * nb,
+                                         cudaMemcpyDeviceToHost, ctx->stream));
+        MH_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        worst = 0.0;
+        for (int z = 0; z < nb; ++z) worst = std::max(worst, std::isfinite(h_res[z]) ? h_res[z] : INFINITY);
+        if (worst <= tol) break;
+    }
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(h_bad.data(), d_bad, sizeof(int) * nb, cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+    MH_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    info->refine_iterations = std::max(info->refine_iterations, std::min(it, max_iter));
+    // FP64 fallback for bad or unconverged problems
+    for (int z = 0; z < nb; ++z) {
+        if (!(h_bad[z] || !(h_res[z] <= tol))) {
+            info->max_rel_residual = std::max(info->max_rel_residual, h_res[z]);
+            continue;
+        }
+        info->n_fallback += 1;
+        double2* Xz = X + (int64_t)z * nv;
+        MH_CUDA_TRY(ctx, cudaMemcpyAsync(Xz, RHS + (int64_t)z * nv, sizeof(double2) * nv,
+                                         cudaMemcpyDeviceToDevice, ctx->stream));
+        if ((rc = fp64_lu_solve(ctx, n, D64 + (int64_t)z * nn, Xz, nrhs))) return rc;
+    }
+    // indirect: phi = S sigma
+    double2* PHI = X;
+    if (!bt.direct) {
+        if ((rc = zgemm_strided(ctx, n, nrhs, S64, X, R, nb, 1.0, 0.0))) return rc;
+        PHI = R;
+    }
+    k_forces_batch<<<nb * nrhs, 256, 0, ctx->stream>>>(bt.m->geom, n, bt.d_dofs, bt.ndof, bt.d_betas,
+                                                        bt.nbeta, d_omegas, bt.rho, bt.g, PHI, d_F, d_FK);
+    ctx->launches += 1;
+    MH_CUDA_TRY(ctx, cudaGetLastError());
+    return MH_OK;
+}
+
+}  // namespace
+
+int hydro_batch(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double* omegas, int64_t ndof,
+                const double* dofs, int64_t nbeta, const double* betas, double rho, double g,
+                uint32_t mask, int direct, int precision, double tol, int max_iter,
+                double* added_mass, double* damping, double* diffraction, double* froude_krylov,
+                mh_batch_info* info)
+{
+    const int64_t n = m->n;
+    const int nrhs = (int)(ndof + nbeta);
+    mh_batch_info local{};
+    // inputs to the device
+    const size_t dof_bytes = sizeof(double) * 3 * (size_t)n * (size_t)ndof;
+    const size_t in_bytes = dof_bytes + sizeof(double) * (size_t)(2 * nomega + nbeta) + 64;
+    auto* in = (char*)ws_get(ctx, WS_DOF, in_bytes);
+    const size_t out_count = (size_t)nomega * (size_t)(nrhs * ndof + nbeta * ndof);
+    auto* d_out = (double2*)ws_get(ctx, WS_OUT, sizeof(double2) * out_count + 16);
+    if (!in || !d_out) return MH_ERR_OOM;
+    auto* d_dofs = (double*)in;
+    auto* d_omegas = (double*)(in + dof_bytes);
+    auto* d_k = d_omegas + nomega;
+    auto* d_betas = d_k + nomega;
+    std::vector<double> hk(nomega);
+    for (int64_t z = 0; z < nomega; ++z) hk[z] = omegas[z] * omegas[z] / g;
+    if (ndof) MH_CUDA_TRY(ctx, cudaMemcpyAsync(d_dofs, dofs, dof_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(d_omegas, omegas, sizeof(double) * nomega, cudaMemcpyHostToDevice,
+                                     ctx->stream));
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(d_k, hk.data(), sizeof(double) * nomega, cudaMemcpyHostToDevice,
+                                     ctx->stream));
+    if (nbeta)
+        MH_CUDA_TRY(ctx, cudaMemcpyAsync(d_betas, betas, sizeof(double) * nbeta, cudaMemcpyHostToDevice,
+                                         ctx->stream));
+    double2* d_F = d_out;
+    double2* d_FK = d_out + (size_t)nomega * nrhs * ndof;
+    Batch bt{ctx, m, n, (int)ndof, (int)nbeta, nrhs, d_dofs, d_betas, rho, g, mask, direct};
+    int rc = MH_OK;
+    if (precision == MH_PRECISION_FP64) {
+        rc = run_fp64(bt, d_omegas, (int)nomega, d_F, d_FK);
+    } else {
+        const size_t nn = (size_t)n * (size_t)n;
+        auto* SR = (double*)ws_get(ctx, WS_SR, sizeof(double) * nn * 2);
+        if (!SR) return MH_ERR_OOM;
+        double* DR = SR + nn;
+        k_rankine_real<<<dim3(blocks(n, kRows), blocks(n, kCols)), kRows, 0, ctx->stream>>>(
+            m->geom, n, mask & (MH_GF_RANKINE | MH_GF_RANKINE_REFLECTED |
+                                MH_GF_RANKINE_REFLECTED_NEGATIVE), direct, SR, DR);
+        ctx->launches += 1;
+        MH_CUDA_TRY(ctx, cudaGetLastError());
+        const size_t per = nn * (2 * sizeof(double2) + sizeof(float2)) +
+                           (size_t)n * nrhs * (5 * sizeof(double2) + sizeof(float2));
+        const int chunk = (int)std::max<int64_t>(1, std::min<int64_t>(nomega, kBatchBytes / per));
+        for (int64_t z0 = 0; z0 < nomega && rc == MH_OK; z0 += chunk) {
+            const int nb = (int)std::min<int64_t>(chunk, nomega - z0);
+            rc = run_mixed_chunk(bt, d_omegas + z0, d_k + z0, nb, SR, DR, tol, max_iter,
+                                 d_F + z0 * nrhs * ndof, d_FK + z0 * nbeta * ndof, &local);
+        }
+    }
+    if (rc) return rc;
+    std::vector<double2> h(out_count);
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), d_out, sizeof(double2) * out_count,
+                                     cudaMemcpyDeviceToHost, ctx->stream));
+    MH_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    // outputs in the reference's layout (src/problems_and_results.jl:137-165):
+    // added_mass[i, j, w] (i influenced, j radiating), diffraction[i, w, b]
+    for (int64_t z = 0; z < nomega; ++z) {
+        const double w = omegas[z];
+        for (int64_t jq = 0; jq < ndof; ++jq)
+            for (int64_t i = 0; i < ndof; ++i) {
+                double2 F = h[((size_t)z * nrhs + jq) * ndof + i];
+                size_t o = (size_t)i + (size_t)ndof * ((size_t)jq + (size_t)ndof * (size_t)z);
+                if (added_mass) added_mass[o] = F.x / (w * w);
+                if (damping) damping[o] = F.y / w;
+            }
+        for (int64_t b = 0; b < nbeta; ++b)
+            for (int64_t i = 0; i < ndof; ++i) {
+                double2 F = h[((size_t)z * nrhs + ndof + b) * ndof + i];
+                double2 K = h[(size_t)nomega * nrhs * ndof + ((size_t)z * nbeta + b) * ndof + i];
+                size_t o = (size_t)i + (size_t)ndof * ((size_t)z + (size_t)nomega * (size_t)b);
+                if (diffraction) {
+                    diffraction[2 * o] = F.x;
+                    diffraction[2 * o + 1] = F.y;
+                }
+                if (froude_krylov) {
+                    froude_krylov[2 * o] = K.x;
+                    froude_krylov[2 * o + 1] = K.y;
+                }
+            }
+    }
+    if (info) *info = local;
+    return MH_OK;
+}
+
+}  // namespace mh

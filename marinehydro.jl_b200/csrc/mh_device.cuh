@@ -61,7 +61,7 @@ __device__ __forceinline__ cplx clog_(cplx a) { return {log(cabs_(a)), atan2(a.i
 // ---------------------------------------------------------------------------
 
 // A&S 5.1.11: E1(z) = -gamma - log z - sum_{n>=1} (-z)^n / (n n!)
-__device__ __noinline__ cplx e1_series(cplx z)
+static __device__ __noinline__ cplx e1_series(cplx z)
 {
     cplx term = mk(1.0, 0.0), sum = mk(0.0, 0.0);
     cplx mz = -z;
@@ -75,7 +75,7 @@ __device__ __noinline__ cplx e1_series(cplx z)
 }
 
 // A&S 5.1.22 contracted form, modified Lentz.
-__device__ __noinline__ cplx e1_cfrac(cplx z)
+static __device__ __noinline__ cplx e1_cfrac(cplx z)
 {
     const double tiny = 1e-300;
     cplx b = z + mk(1.0, 0.0);
@@ -421,7 +421,7 @@ __device__ __forceinline__ void delh_gk15(double a, double b, double r, double z
 
 // (G, dG/dr, dG/dz) of the exact wave term; the theta-integral is adaptive
 // Gauss-Kronrod bisection with the same acceptance rule as the CPU oracle.
-__device__ __noinline__ void delh_dimless(double r, double z, cplx out[3])
+static __device__ __noinline__ void delh_dimless(double r, double z, cplx out[3])
 {
     const double half_pi = 0.5 * kPi;
     double est[4], err;
@@ -463,6 +463,12 @@ __device__ __noinline__ void delh_dimless(double r, double z, cplx out[3])
     out[2] = mk(out[0].re + 2.0 / hypot(r, z), out[0].im);
 }
 
+}  // namespace mh
+
+#include "mh_table.cuh"
+
+namespace mh {
+
 // ---------------------------------------------------------------------------
 // reduced coordinates and the per-pair sum over Green-function terms
 // ---------------------------------------------------------------------------
@@ -471,7 +477,7 @@ __device__ __noinline__ void delh_dimless(double r, double z, cplx out[3])
 // one-point rule wu.jl:33-47 / exact_Guevel_Delhommeau.jl:61-75).
 template <bool kDelh>
 __device__ __forceinline__ void wave_pair(const double x[3], const Panel& p, double k,
-                                          bool wrt_first, cplx& s, cplx g[3])
+                                          bool wrt_first, const double* tab, cplx& s, cplx g[3])
 {
     double dx = x[0] - p.c[0], dy = x[1] - p.c[1];
     double dis2 = dx * dx + dy * dy;
@@ -480,10 +486,12 @@ __device__ __forceinline__ void wave_pair(const double x[3], const Panel& p, dou
     double r = k * dis;
     double z = k * (x[2] + p.c[2]);
     cplx o[3];
-    if (kDelh)
-        delh_dimless(r, z, o);
-    else
+    if (kDelh) {
+        if (tab) delh_dimless_table(tab, r, z, o);
+        else delh_dimless(r, z, o);
+    } else {
         wu_dimless(r, z, o);
+    }
     double d1 = 0.0, d2 = 0.0;
     if (fabs(r) > 1e-6) {
         double f = k * k / r;
@@ -499,8 +507,8 @@ __device__ __forceinline__ void wave_pair(const double x[3], const Panel& p, dou
 
 // Sum over the Green-function tuple of integral / integral_gradient.
 __device__ __forceinline__ void pair_integrals(const double x[3], const Panel& p, double k,
-                                               uint32_t mask, bool wrt_first, cplx& s,
-                                               cplx g[3])
+                                               uint32_t mask, bool wrt_first, const double* tab,
+                                               cplx& s, cplx g[3])
 {
     s = mk(0.0, 0.0);
     g[0] = g[1] = g[2] = mk(0.0, 0.0);
@@ -528,7 +536,7 @@ __device__ __forceinline__ void pair_integrals(const double x[3], const Panel& p
     }
     if (mask & MH_GF_WU) {
         cplx sw, gw[3];
-        wave_pair<false>(x, p, k, wrt_first, sw, gw);
+        wave_pair<false>(x, p, k, wrt_first, tab, sw, gw);
         s = s + sw;
         g[0] = g[0] + gw[0];
         g[1] = g[1] + gw[1];
@@ -536,7 +544,7 @@ __device__ __forceinline__ void pair_integrals(const double x[3], const Panel& p
     }
     if (mask & MH_GF_DELHOMMEAU) {
         cplx sw, gw[3];
-        wave_pair<true>(x, p, k, wrt_first, sw, gw);
+        wave_pair<true>(x, p, k, wrt_first, tab, sw, gw);
         s = s + sw;
         g[0] = g[0] + gw[0];
         g[1] = g[1] + gw[1];

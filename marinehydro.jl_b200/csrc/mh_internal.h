@@ -29,8 +29,11 @@ struct mh_mesh {
 // Workspace slots of a context; each is a grow-only device buffer.
 enum WsSlot : int {
     WS_S = 0, WS_D, WS_RHS, WS_PHI, WS_TMP, WS_PIV, WS_INFO, WS_LWORK,
-    WS_DOF, WS_OUT, WS_NSLOTS
+    WS_DOF, WS_OUT, WS_LO, WS_DINV, WS_TMP32, WS_MISC, WS_SR, WS_NSLOTS
 };
+
+// Largest number of right-hand sides (radiating dofs + headings) per frequency.
+constexpr int kMaxRhs = 16;
 
 struct mh_ctx {
     int device = 0;
@@ -39,6 +42,8 @@ struct mh_ctx {
     cusolverDnHandle_t cusolver = nullptr;
     std::string err;
     int64_t launches = 0;
+    int delh_method = MH_DELHOMMEAU_TABLE;
+    double* delh_table = nullptr;  // device, kTabWords doubles (built on first use)
     void* ws[WS_NSLOTS] = {};
     size_t ws_bytes[WS_NSLOTS] = {};
 };
@@ -50,9 +55,10 @@ int set_err(mh_ctx* ctx, int code, const char* fmt, ...);
 void* ws_get(mh_ctx* ctx, int slot, size_t bytes);
 
 // ---- kernels (mh_kernels.cu) ----
-// S, D: n x n complex128 column-major device buffers (either may be null).
+// S, D: n x n complex128 column-major device buffers (either may be null);
+// tab: Delhommeau table or null (adaptive quadrature).
 cudaError_t launch_assemble_f64(mh_ctx* ctx, const mh_mesh* m, double k, uint32_t mask,
-                                int direct, double2* S, double2* D);
+                                int direct, const double* tab, double2* S, double2* D);
 // bc[i] = -i omega (n_i . dof_i); dof is a device 3-vector (dof_rows==1) or n x 3 col-major.
 cudaError_t launch_radiation_bc(mh_ctx* ctx, const mh_mesh* m, const double* dof, int64_t dof_rows,
                                 double omega, double2* bc);
@@ -62,6 +68,31 @@ cudaError_t launch_airy_bc(mh_ctx* ctx, const mh_mesh* m, double omega, double b
 // F = sum_j (i rho omega phi_j) * (-(n_j . dof_j)) * area_j, written to F_out (device, 1 complex).
 cudaError_t launch_force(mh_ctx* ctx, const mh_mesh* m, const double2* phi, const double* dof,
                          int64_t dof_rows, double rho, double omega, double2* F_out);
+
+// ---- batched FP32 LU (mh_lu.cu) ----
+// Elements of the inverse-diagonal-block buffer per matrix.
+int64_t lu_dinv_stride(int64_t n);
+// Pivot-free LU of nbatch n x n float2 matrices (stride elements apart), in
+// place; bad[b] is set when matrix b meets a zero/non-finite pivot.
+cudaError_t launch_lu_f32(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int nbatch,
+                          float2* Dinv, int* bad);
+// X <- (LU)^-1 X for nrhs <= kMaxRhs right-hand sides per matrix.
+cudaError_t launch_lu_solve_f32(mh_ctx* ctx, const float2* A, int64_t n, int64_t stride, int nbatch,
+                                const float2* Dinv, float2* X, int64_t xstride, int nrhs);
+
+// ---- batched driver (mh_batch.cu) ----
+int hydro_batch(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double* omegas, int64_t ndof,
+                const double* dofs, int64_t nbeta, const double* betas, double rho, double g,
+                uint32_t mask, int direct, int precision, double tol, int max_iter,
+                double* added_mass, double* damping, double* diffraction, double* froude_krylov,
+                mh_batch_info* info);
+
+// ---- Delhommeau table (mh_table.cu) ----
+int ensure_delh_table(mh_ctx* ctx);
+// Table to use for `mask` on this ctx (null: no Delhommeau term or exact quadrature).
+const double* delh_table_for(mh_ctx* ctx, uint32_t mask, int* status);
+cudaError_t launch_wave_term(mh_ctx* ctx, const double* tab, uint32_t which, int64_t n,
+                             const double* r, const double* z, double* out);
 
 }  // namespace mh
 

@@ -33,7 +33,7 @@ __device__ __forceinline__ void load_panel_field(Panel& p, int f, double v)
 
 __global__ void __launch_bounds__(kRows)
 k_assemble_f64(const double* __restrict__ geom, int64_t n, double k, uint32_t mask, int direct,
-               double2* __restrict__ S, double2* __restrict__ D)
+               const double* __restrict__ tab, double2* __restrict__ S, double2* __restrict__ D)
 {
     __shared__ Panel sp[kCols];
     const int64_t j0 = (int64_t)blockIdx.y * kCols;
@@ -54,7 +54,7 @@ k_assemble_f64(const double* __restrict__ geom, int64_t n, double k, uint32_t ma
         const Panel& p = sp[jj];
         const int64_t j = j0 + jj;
         cplx s, g[3];
-        pair_integrals(x, p, k, mask, wrt_first, s, g);
+        pair_integrals(x, p, k, mask, wrt_first, tab, s, g);
         const int64_t o = j * n + i;
         if (S) S[o] = make_double2(-kInv4Pi * s.re, -kInv4Pi * s.im);
         if (D) {
@@ -151,11 +151,11 @@ k_force(const double* __restrict__ geom, int64_t n, const double2* __restrict__ 
 }  // namespace
 
 cudaError_t launch_assemble_f64(mh_ctx* ctx, const mh_mesh* m, double k, uint32_t mask, int direct,
-                                double2* S, double2* D)
+                                const double* tab, double2* S, double2* D)
 {
     const int64_t n = m->n;
     dim3 grid((unsigned)((n + kRows - 1) / kRows), (unsigned)((n + kCols - 1) / kCols));
-    k_assemble_f64<<<grid, kRows, 0, ctx->stream>>>(m->geom, n, k, mask, direct, S, D);
+    k_assemble_f64<<<grid, kRows, 0, ctx->stream>>>(m->geom, n, k, mask, direct, tab, S, D);
     ctx->launches += 1;
     return cudaGetLastError();
 }

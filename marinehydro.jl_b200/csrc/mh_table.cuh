@@ -1,0 +1,104 @@
+// Tabulated Guevel-Delhommeau wave term.
+//
+// The reference evaluates the dimensionless wave term of the infinite-depth
+// Green function by adaptive quadrature per panel pair
+// (src/green_functions/exact_Guevel_Delhommeau.jl:15-59).  With
+// R = sqrt(r^2 + z^2), z < 0, the term separates into closed-form parts and
+// one smooth remainder:
+//
+//   Im G    =  2 pi e^z J0(r)
+//   Re G    = -2 e^z J0(r) log((R + |z|)/2) + B(r, z)
+//   Im dG/dr = -2 pi e^z J1(r)
+//   Re dG/dr =  2 e^z J1(r) log((R+|z|)/2) - 2 e^z J0(r) r / (R (R+|z|)) + C(r, z)
+//   dG/dz   =  G + 2/R                              (exact_Guevel_Delhommeau.jl:56)
+//
+// (the log coefficient is the generating function sum_m (-R)^m P_m(|z|/R)/m!
+// = e^z J0(r) of the log-moments of e^zeta E1(zeta)).  B and C are smooth
+// in polar coordinates (R, alpha = atan2(r, |z|)) near the origin and in
+// (r, |z|) away from it, so they are tabulated as 2-D Chebyshev series:
+//   - one polar patch, R in [0, 1.5), alpha in [0, pi/2], degree 20 x 20;
+//   - Cartesian cells of 0.5 x 0.5 over r, |z| in [0, 16), degree 12 x 12
+//     (every cell touching R < 1 lies inside the polar patch).
+// Points outside the table fall back to the adaptive quadrature.  The node
+// values are computed on the device with the FP64 quadrature; the table's
+// error against it is ~1e-12 absolute.
+#pragma once
+// Included from mh_device.cuh after the quadrature routines it falls back to.
+
+namespace mh {
+
+constexpr int kTabNP = 20;          // polar patch degree (per direction)
+constexpr int kTabNC = 12;          // Cartesian cell degree
+constexpr double kTabRPolar = 1.5;  // polar patch radius
+constexpr double kTabH = 0.5;       // Cartesian cell size
+constexpr int kTabNCell = 32;       // cells per direction -> extent 16
+constexpr double kTabExtent = kTabH * kTabNCell;
+constexpr int kTabPolarWords = 2 * kTabNP * kTabNP;            // B then C
+constexpr int kTabCellWords = 2 * kTabNC * kTabNC;             // B then C
+constexpr int kTabWords = kTabPolarWords + kTabNCell * kTabNCell * kTabCellWords;
+
+// sum_i sum_j c[i*N + j] T_i(u) T_j(v)
+template <int N>
+__device__ __forceinline__ double cheb2d(const double* __restrict__ c, double u, double v)
+{
+    double tu[N], tv[N];
+    tu[0] = 1.0;
+    tu[1] = u;
+    tv[0] = 1.0;
+    tv[1] = v;
+#pragma unroll
+    for (int j = 2; j < N; ++j) {
+        tu[j] = 2.0 * u * tu[j - 1] - tu[j - 2];
+        tv[j] = 2.0 * v * tv[j - 1] - tv[j - 2];
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        double row = 0.0;
+#pragma unroll
+        for (int j = 0; j < N; ++j) row = fma(__ldg(c + i * N + j), tv[j], row);
+        s = fma(tu[i], row, s);
+    }
+    return s;
+}
+
+// (G, dG/dr, dG/dz) from the table (falls back to quadrature outside it).
+__device__ __forceinline__ void delh_dimless_table(const double* __restrict__ tab, double r, double z,
+                                                   cplx out[3])
+{
+    const double az = -z;
+    const double R = hypot(r, z);
+    double B, C;
+    if (!(az >= 0.0)) {  // above the free surface or NaN: not tabulated
+        delh_dimless(r, z, out);
+        return;
+    }
+    if (R < kTabRPolar) {
+        double alpha = atan2(r, az);
+        double u = 2.0 * R / kTabRPolar - 1.0;
+        double v = 4.0 * alpha / kPi - 1.0;
+        B = cheb2d<kTabNP>(tab, u, v);
+        C = cheb2d<kTabNP>(tab + kTabNP * kTabNP, u, v);
+    } else if (r < kTabExtent && az < kTabExtent) {
+        int ir = min((int)(r / kTabH), kTabNCell - 1);
+        int iz = min((int)(az / kTabH), kTabNCell - 1);
+        const double* c = tab + kTabPolarWords + (iz * kTabNCell + ir) * kTabCellWords;
+        double u = 2.0 * (r - ir * kTabH) / kTabH - 1.0;
+        double v = 2.0 * (az - iz * kTabH) / kTabH - 1.0;
+        B = cheb2d<kTabNC>(c, u, v);
+        C = cheb2d<kTabNC>(c + kTabNC * kTabNC, u, v);
+    } else {
+        delh_dimless(r, z, out);
+        return;
+    }
+    const double e = exp(z);
+    const double J0 = j0(r), J1 = j1(r);
+    const double L = log(0.5 * (R + az));
+    const double G_re = -2.0 * e * J0 * L + B;
+    const double G_im = 2.0 * kPi * e * J0;
+    out[0] = mk(G_re, G_im);
+    out[1] = mk(2.0 * e * J1 * L - 2.0 * e * J0 * r / (R * (R + az)) + C, -2.0 * kPi * e * J1);
+    out[2] = mk(G_re + 2.0 / R, G_im);
+}
+
+}  // namespace mh
