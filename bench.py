@@ -1,0 +1,437 @@
+#!/usr/bin/env python
+"""Benchmark: batched BEM solves/s at N=2048 panels on B200.
+
+Workload (one "step" = one pass of the hot path over one batch): a
+hemisphere of radius 1 m meshed with 32 x 64 panels (2048), 64 frequencies
+omega = linspace(0.3, 3.0), heave and surge radiating/influenced, one
+incident heading (beta = 0), Rankine + reflected Rankine + tabulated
+Guevel-Delhommeau wave term, direct formulation; mixed precision (FP32 LU,
+FP64 refinement to max|r|/max|b| <= 1e-10).  A solve is one (mesh,
+frequency) problem with all its right-hand sides and outputs (A, B, F, FK).
+
+  value  solves/s with the mesh already resident on the device
+  e2e    the same through the C ABI from pinned host buffers: mesh upload,
+         batch call, outputs back to the host, every step
+
+Also reported: the plain FP64 GPU path (cuSOLVER zgetrf) on a frequency
+subsample, the relative error of the mixed outputs against it, per-phase
+times measured with CUDA events on the library's stream, clocks sampled
+during the timed region, and the CPU oracle baseline.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import datetime
+import importlib.util
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+METRIC = "BEM solves/s + adjoint grads/s, N=2048 panels: mixed vs FP64 GPU at 1e-6 err"
+WORKLOAD = "hemisphere_2048p_64omega_heave_surge_diffraction_delhommeau_direct"
+
+
+def load_package():
+    name = "marinehydro_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    pkg_dir = ROOT / "marinehydro.jl_b200"
+    spec = importlib.util.spec_from_file_location(
+        name, pkg_dir / "__init__.py", submodule_search_locations=[str(pkg_dir)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def workload(mh, res, n_omega):
+    mesh = mh.mesh_hemisphere(1.0, (0.0, 0.0, 0.0), tuple(res))
+    body = mh.FloatingBody.rigid(mesh, ["Heave", "Surge"])
+    dofs = list(body.dofs.values())
+    omegas = np.linspace(0.3, 3.0, n_omega)
+    betas = [0.0]
+    gfs = (mh.Rankine(), mh.RankineReflected(), mh.ExactGuevelDelhommeau())
+    return mesh, dofs, omegas, betas, gfs
+
+
+def config_dict(mesh, omegas, args):
+    return {"workload": WORKLOAD, "panels": int(mesh.nfaces), "resolution": list(args.res),
+            "n_omega": int(len(omegas)), "omega_range": [float(omegas[0]), float(omegas[-1])],
+            "dofs": ["Heave", "Surge"], "headings": [0.0],
+            "green_functions": "Rankine+RankineReflected+ExactGuevelDelhommeau(table)",
+            "formulation": "direct", "precision": "mixed (FP32 LU, FP64 refinement)",
+            "tol": args.tol, "solve": "one (mesh, omega) problem, 3 right-hand sides",
+            "l2": "working set ~11 GB per step, larger than the 126 MB L2 (no flush needed)"}
+
+
+# --------------------------------------------------------------------------
+# clocks during the timed region
+# --------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: str):
+        self.proc = None
+        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", gpu_index], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        rows = [r.split(",") for r in self.path.read_text().splitlines() if r.strip()]
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------
+# CPU baseline (the FP64 CPU oracle; test infrastructure, timed as the baseline)
+# --------------------------------------------------------------------------
+
+def cpu_baseline(mh, mesh, dofs, omegas, betas, columns: int):
+    sys.path.insert(0, str(ROOT))
+    import oracle
+    import scipy.linalg as sla
+
+    oracle.lib()
+    n = mesh.nfaces
+    w = float(omegas[len(omegas) // 2])
+    k = w * w / 9.81
+    mask = oracle.GF_RANKINE | oracle.GF_RANKINE_REFLECTED | oracle.GF_DELHOMMEAU
+    t0 = time.perf_counter()
+    S, D = oracle.assemble(mesh, k, mask, True, columns=(0, columns))
+    t_asm = (time.perf_counter() - t0) * n / columns
+    # LU and solves on a full FP64 matrix of the same size (Wu assembly is cheap)
+    S, D = oracle.assemble(mesh, k, oracle.GF_RANKINE | oracle.GF_RANKINE_REFLECTED | oracle.GF_WU,
+                           True)
+    t0 = time.perf_counter()
+    lu = sla.lu_factor(D, check_finite=False)
+    bcs = [oracle.radiation_bc(mesh.normals, d, w) for d in dofs]
+    bcs += [oracle.airy_bc(mesh.centers, mesh.normals, w, b) for b in betas]
+    phi = sla.lu_solve(lu, S @ np.stack(bcs, axis=1), check_finite=False)
+    for q in range(phi.shape[1]):
+        for d in dofs:
+            oracle.integrate_pressure(mesh.normals, mesh.areas, 1j * 1000.0 * w * phi[:, q], d)
+    t_lu = time.perf_counter() - t0
+    per_solve = t_asm + t_lu
+    return {"value": 1.0 / per_solve, "unit": "solves/s", "cores": oracle.max_threads(),
+            "kind": "port",
+            "sample": (f"1 frequency (omega={w:.3f}): exact-quadrature Delhommeau assembly of "
+                       f"{columns} of {n} columns scaled x{n / columns:g} ({t_asm:.2f} s), plus "
+                       f"LAPACK zgetrf/zgetrs + 3 right-hand sides + forces ({t_lu:.3f} s)")}
+
+
+# --------------------------------------------------------------------------
+# reference arm: the CPU implementation of the path (oracle port)
+# --------------------------------------------------------------------------
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    mh = load_package()
+    mesh, dofs, omegas, betas, gfs = workload(mh, args.res, args.n_omega)
+    times = []
+    base = None
+    for step in range(args.warmup + args.steps):
+        base = cpu_baseline(mh, mesh, dofs, omegas, betas, args.cpu_columns)
+        if step >= args.warmup:
+            times.append(1.0 / base["value"])
+    per = float(np.mean(times))
+    v = 1.0 / per
+    line = {"metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": config_dict(mesh, omegas, args), "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": base["cores"],
+                             "kind": "port", "sample": base["sample"]},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------
+# our arm
+# --------------------------------------------------------------------------
+
+def _pinned(a: np.ndarray, torch):
+    t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    return t
+
+
+def e2e_step(mh, ctx, host, omegas_p, dofs_p, betas_p, out_p, args, mask, info):
+    """Mesh upload + batch + outputs to host through the C ABI."""
+    N = mh.native
+    L = N.lib()
+    h = N._P()
+    dp = lambda t: ctypes.cast(t.data_ptr(), N._D)
+    N.check(L.mh_mesh_create(ctx.handle, host["n"], host["nv"], dp(host["vertices"]),
+                             ctypes.cast(host["faces"].data_ptr(), N._I64), dp(host["centers"]),
+                             dp(host["normals"]), dp(host["areas"]), dp(host["radii"]),
+                             ctypes.byref(h)), ctx.handle)
+    try:
+        N.check(L.mh_hydro_batch(ctx.handle, h, omegas_p.numel(), dp(omegas_p), args.n_dof,
+                                 dp(dofs_p), betas_p.numel(), dp(betas_p), 1000.0, 9.81, mask, 1,
+                                 N.MH_PRECISION_MIXED, args.tol, args.max_iter, dp(out_p[0]),
+                                 dp(out_p[1]), dp(out_p[2]), dp(out_p[3]), ctypes.byref(info)),
+                ctx.handle)
+    finally:
+        L.mh_mesh_destroy(ctx.handle, h)
+
+
+def run_ours(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(local)
+    mh = load_package()
+    ctx = mh.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    mesh, dofs, omegas, betas, gfs = workload(mh, args.res, args.n_omega)
+    mask = mh.gf_mask(gfs)
+    args.n_dof = len(dofs)
+    dm = mh.device_mesh(mesh, ctx)
+
+    def step():
+        return mh.hydro_batch(mesh, omegas, dofs, betas, green_functions=gfs, precision="mixed",
+                              tol=args.tol, max_iter=args.max_iter, ctx=ctx)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        out = step()
+    # ---- timed region (resident inputs) ----
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    gpu_index = vis.split(",")[local] if vis and vis.split(",")[local].strip().isdigit() else str(local)
+    sampler = ClockSampler(gpu_index)
+    ctx.set_profiling(True)
+    launches0 = ctx.kernel_launches()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        out = step()
+    ev1.record(stream)
+    barrier()
+    launches = ctx.kernel_launches() - launches0
+    phases = ctx.phase_times()
+    ctx.set_profiling(False)
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * args.n_omega * args.steps / (ms / 1e3)
+    A, B, Fd, Fk, info = out
+
+    # ---- e2e through the C ABI from pinned host buffers ----
+    host = {"n": mesh.nfaces, "nv": mesh.nvertices,
+            "vertices": _pinned(np.asfortranarray(mesh.vertices).reshape(-1, order="F"), torch),
+            "faces": _pinned(np.asfortranarray(mesh.faces).reshape(-1, order="F"), torch),
+            "centers": _pinned(np.asfortranarray(mesh.centers).reshape(-1, order="F"), torch),
+            "normals": _pinned(np.asfortranarray(mesh.normals).reshape(-1, order="F"), torch),
+            "areas": _pinned(mesh.areas, torch), "radii": _pinned(mesh.radii, torch)}
+    omegas_p = _pinned(omegas, torch)
+    betas_p = _pinned(np.asarray(betas, dtype=np.float64), torch)
+    dofs_p = _pinned(np.concatenate([np.asfortranarray(d).reshape(-1, order="F") for d in dofs]),
+                     torch)
+    nd, nw, nb = len(dofs), len(omegas), len(betas)
+    out_p = [torch.zeros(nd * nd * nw, dtype=torch.float64).pin_memory(),
+             torch.zeros(nd * nd * nw, dtype=torch.float64).pin_memory(),
+             torch.zeros(2 * nd * nw * nb, dtype=torch.float64).pin_memory(),
+             torch.zeros(2 * nd * nw * nb, dtype=torch.float64).pin_memory()]
+    cinfo = mh.bodies._Info()
+    e2e_step(mh, ctx, host, omegas_p, dofs_p, betas_p, out_p, args, mask, cinfo)
+    barrier()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        e2e_step(mh, ctx, host, omegas_p, dofs_p, betas_p, out_p, args, mask, cinfo)
+    ev1.record(stream)
+    barrier()
+    ms_e2e = ev0.elapsed_time(ev1)
+    if dist is not None:
+        t = torch.tensor([ms_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    h2d = sum(int(v.numel() * v.element_size()) for k, v in host.items() if k not in ("n", "nv"))
+    h2d += int(omegas_p.numel() * 8 * 2 + betas_p.numel() * 8 + dofs_p.numel() * 8)
+    d2h = sum(int(t.numel() * t.element_size()) for t in out_p)
+    e2e = {"value": world * args.n_omega * args.steps / (ms_e2e / 1e3), "unit": "solves/s",
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+           "ms_per_step": ms_e2e / args.steps}
+
+    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64+f32 (FP64 matrices and residuals, FP32 LU)", "data": "synthetic",
+            "config": config_dict(mesh, omegas, args), "e2e": e2e, "gpu_launches": launches,
+            "refinement": {"iterations": info.refine_iterations, "fallbacks": info.n_fallback,
+                           "max_rel_residual": info.max_rel_residual}}
+    if clocks:
+        line["clocks"] = clocks
+    per_phase = {k: v[0] / args.steps for k, v in phases.items() if v[1]}
+    line["phases_ms_per_step"] = per_phase
+    line["roofline"] = roofline(per_phase, mesh.nfaces, args)
+
+    if rank == 0 and not args.no_fp64:
+        line["fp64_gpu"], line["accuracy"] = fp64_baseline(mh, ctx, mesh, dofs, omegas, betas, gfs,
+                                                           (A, B, Fd), args)
+        if line["fp64_gpu"]["table"]["value"] > 0:
+            line["speedup_vs_fp64_gpu"] = value / line["fp64_gpu"]["table"]["value"]
+    if rank == 0 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(mh, mesh, dofs, omegas, betas, args.cpu_columns)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    ctx.close()
+    return 0
+
+
+def roofline(per_phase, n, args):
+    """Dominant phase against the measured HBM copy bandwidth.  Algorithmic
+    bytes per frequency of the wave pass: read the FP64 Rankine part of S and
+    D (16 B/pair), write S and D in FP64 complex (32 B/pair) and the FP32 LU
+    copy (8 B/pair); of the LU: the FP32 complex trailing updates read and
+    write each trailing block once per step, sum_k 16 B (n - k*32)^2."""
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        hbm, src = float(peaks["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        hbm, src = 6650.0, "fallback"
+    if not per_phase:
+        return None
+    dom = max(per_phase, key=per_phase.get)
+    ms = per_phase[dom]
+    nn = float(n) * n
+    if dom == "wave":
+        traffic_alg = 56.0 * nn * args.n_omega
+    elif dom == "lu":
+        traffic_alg = sum(16.0 * (n - k) ** 2 for k in range(32, n, 32)) * args.n_omega
+    elif dom == "refine":
+        traffic_alg = 16.0 * nn * args.n_omega * 3
+    else:
+        traffic_alg = 16.0 * nn * args.n_omega
+    achieved = traffic_alg / (ms / 1e3) / 1e9
+    return {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+            "frac": achieved / hbm, "peak_source": src, "traffic": None,
+            "ms_per_step": ms, "algorithmic_bytes_per_step": traffic_alg}
+
+
+def fp64_baseline(mh, ctx, mesh, dofs, omegas, betas, gfs, mixed, args):
+    """Plain FP64 GPU path on a frequency subsample: FP64 assembly (table and
+    exact quadrature), cuSOLVER zgetrf/zgetrs, one frequency at a time; timed
+    with CUDA events on the library's stream."""
+    import torch
+
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    sub = np.arange(0, len(omegas), max(1, len(omegas) // args.fp64_omegas))[:args.fp64_omegas]
+    res = {}
+    out64 = None
+    for method in ("table", "exact"):
+        ctx.set_delhommeau_method(method)
+        om = omegas[sub] if method == "table" else omegas[sub[:2]]
+        mh.hydro_batch(mesh, om[:1], dofs, betas, green_functions=gfs, precision="fp64", ctx=ctx)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        o = mh.hydro_batch(mesh, om, dofs, betas, green_functions=gfs, precision="fp64", ctx=ctx)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        dt = ev0.elapsed_time(ev1) / 1e3
+        res[method] = {"value": len(om) / dt, "unit": "solves/s", "omegas": int(len(om)),
+                       "ms_per_solve": dt / len(om) * 1e3}
+        if method == "table":
+            out64 = o
+    ctx.set_delhommeau_method("table")
+    A, B, Fd = mixed
+    acc = {}
+    for name, a, b in (("A", A[:, :, sub], out64[0]), ("B", B[:, :, sub], out64[1]),
+                       ("F", Fd[:, sub], out64[2])):
+        acc[name] = float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+    acc["note"] = "max abs difference / max abs value, mixed vs FP64 GPU path, same frequencies"
+    return res, acc
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--res", type=int, nargs=2, default=[64, 64])
+    ap.add_argument("--n-omega", type=int, default=64)
+    ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--max-iter", type=int, default=30)
+    ap.add_argument("--fp64-omegas", type=int, default=8)
+    ap.add_argument("--cpu-columns", type=int, default=64)
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -89,6 +89,17 @@ const char* mh_last_error(const mh_ctx* ctx);
 /* Number of this library's own kernels launched on the ctx so far. */
 int mh_ctx_kernel_launches(const mh_ctx* ctx, int64_t* count);
 
+/* The ctx's CUDA stream (a cudaStream_t), e.g. to record timing events. */
+int mh_ctx_stream(const mh_ctx* ctx, void** stream);
+
+/* Phase timing with CUDA events on the ctx stream (off by default; turning it
+ * on or off resets the totals).  Phases, in order: 0 Rankine part, 1 wave
+ * part + FP32 copy, 2 right-hand sides S*BC, 3 FP32 LU, 4 refinement,
+ * 5 forces, 6 FP64 assembly, 7 FP64 LU (cuSOLVER).  No reference
+ * counterpart (instrumentation). */
+int mh_ctx_set_profiling(mh_ctx* ctx, int enable);
+int mh_ctx_phase_times(mh_ctx* ctx, int nphases, double* ms, int64_t* calls);
+
 /* How ExactGuevelDelhommeau() is evaluated on this ctx: MH_DELHOMMEAU_TABLE
  * (default) or MH_DELHOMMEAU_EXACT (per-pair adaptive quadrature, the
  * reference's method, src/green_functions/exact_Guevel_Delhommeau.jl:8-26). */

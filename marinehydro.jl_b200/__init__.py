@@ -14,6 +14,9 @@ from .api import (SETTINGS, set_g, set_rho, GreensFunction, Rankine, RankineRefl
                   assemble_matrix_wu, solve, calculate_radiation_forces, DiffractionForce,
                   radiation_bc, AiryBC, airy_waves_potential, airy_waves_velocity,
                   airy_waves_pressure, integrate_pressure, FroudeKrylovForce)
+from .bodies import (FloatingBody, combine_floatingbodies, make_body_name_list_unique,
+                     translational_dofs, rotational_dofs, hydro_batch, BatchInfo,
+                     compute_hydrodynamic_coefficients)
 from ._native import (Context, MarineHydroError, ArgumentError, NotConvergedError,
                       SingularMatrixError, device_count, default_context)
 from . import _native as native

@@ -67,6 +67,9 @@ SIGNATURES = {
     "mh_last_error": (ctypes.c_char_p, [_P]),
     "mh_ctx_kernel_launches": (ctypes.c_int, [_P, _I64]),
     "mh_ctx_set_delhommeau_method": (ctypes.c_int, [_P, ctypes.c_int]),
+    "mh_ctx_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
+    "mh_ctx_set_profiling": (ctypes.c_int, [_P, ctypes.c_int]),
+    "mh_ctx_phase_times": (ctypes.c_int, [_P, ctypes.c_int, _D, _I64]),
     "mh_wave_term": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_int64, _D, _D, _D]),
     "mh_mesh_create": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_int64, _D, _I64, _D, _D, _D, _D,
                                       ctypes.POINTER(_P)]),
@@ -84,6 +87,10 @@ SIGNATURES = {
     "mh_diffraction_force": (ctypes.c_int, [_P, _P, ctypes.c_double, _D, ctypes.c_int64,
                                             ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                             ctypes.c_uint32, ctypes.c_int, ctypes.c_int, _D]),
+    "mh_hydro_batch": (ctypes.c_int, [_P, _P, ctypes.c_int64, _D, ctypes.c_int64, _D,
+                                      ctypes.c_int64, _D, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_uint32, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                      ctypes.c_int, _D, _D, _D, _D, ctypes.c_void_p]),
 }
 
 _lib = None
@@ -165,6 +172,25 @@ class Context:
               self._h)
         c = out[:, 0::2] + 1j * out[:, 1::2]
         return c[:, 0], c[:, 1], c[:, 2]
+
+    PHASES = ("rankine", "wave", "rhs", "lu", "refine", "forces", "fp64_assembly", "fp64_lu")
+
+    def stream(self) -> int:
+        """The ctx's cudaStream_t as an integer handle."""
+        p = _P()
+        check(lib().mh_ctx_stream(self._h, ctypes.byref(p)), self._h)
+        return int(p.value or 0)
+
+    def set_profiling(self, enable: bool):
+        check(lib().mh_ctx_set_profiling(self._h, int(bool(enable))), self._h)
+
+    def phase_times(self) -> dict:
+        """name -> (total ms, number of timed occurrences) since profiling was enabled."""
+        n = len(self.PHASES)
+        ms = np.zeros(n)
+        calls = np.zeros(n, dtype=np.int64)
+        check(lib().mh_ctx_phase_times(self._h, n, dptr(ms), i64ptr(calls)), self._h)
+        return {name: (float(ms[q]), int(calls[q])) for q, name in enumerate(self.PHASES)}
 
     def kernel_launches(self) -> int:
         c = ctypes.c_int64(0)

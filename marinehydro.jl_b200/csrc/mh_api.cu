@@ -60,6 +60,36 @@ void* ws_get(mh_ctx* ctx, int slot, size_t bytes)
     return p;
 }
 
+void phase_begin(mh_ctx* ctx, int ph)
+{
+    if (!ctx->profile) return;
+    if (ctx->ev_pending[ph]) phase_collect(ctx);
+    cudaEventRecord(ctx->ev[2 * ph], ctx->stream);
+}
+
+void phase_end(mh_ctx* ctx, int ph)
+{
+    if (!ctx->profile) return;
+    cudaEventRecord(ctx->ev[2 * ph + 1], ctx->stream);
+    ctx->ev_pending[ph] = true;
+}
+
+void phase_collect(mh_ctx* ctx)
+{
+    if (!ctx->profile) return;
+    cudaStreamSynchronize(ctx->stream);
+    for (int ph = 0; ph < PH_N; ++ph) {
+        if (!ctx->ev_pending[ph]) continue;
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, ctx->ev[2 * ph], ctx->ev[2 * ph + 1]) == cudaSuccess) {
+            ctx->phase_ms[ph] += ms;
+            ctx->phase_calls[ph] += 1;
+        }
+        ctx->ev_pending[ph] = false;
+    }
+    cudaGetLastError();
+}
+
 }  // namespace mh
 
 using mh::set_err;
@@ -266,6 +296,8 @@ int mh_ctx_destroy(mh_ctx* ctx)
     for (int s = 0; s < WS_NSLOTS; ++s)
         if (ctx->ws[s]) cudaFree(ctx->ws[s]);
     if (ctx->delh_table) cudaFree(ctx->delh_table);
+    for (int q = 0; q < 2 * PH_N; ++q)
+        if (ctx->ev[q]) cudaEventDestroy(ctx->ev[q]);
     if (ctx->cusolver) cusolverDnDestroy(ctx->cusolver);
     if (ctx->cublas) cublasDestroy(ctx->cublas);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -282,6 +314,43 @@ int mh_ctx_kernel_launches(const mh_ctx* ctx, int64_t* count)
 {
     if (!ctx || !count) return MH_ERR_ARG;
     *count = ctx->launches;
+    return MH_OK;
+}
+
+int mh_ctx_stream(const mh_ctx* ctx, void** stream)
+{
+    if (!ctx || !stream) return MH_ERR_ARG;
+    *stream = (void*)ctx->stream;
+    return MH_OK;
+}
+
+int mh_ctx_set_profiling(mh_ctx* ctx, int enable)
+{
+    int rc;
+    if ((rc = check_ctx(ctx))) return rc;
+    if (enable && !ctx->ev[0]) {
+        for (int q = 0; q < 2 * PH_N; ++q)
+            if (cudaEventCreate(&ctx->ev[q]) != cudaSuccess)
+                return set_err(ctx, MH_ERR_CUDA, "cudaEventCreate failed");
+    }
+    mh::phase_collect(ctx);
+    ctx->profile = enable != 0;
+    for (int q = 0; q < PH_N; ++q) {
+        ctx->phase_ms[q] = 0.0;
+        ctx->phase_calls[q] = 0;
+        ctx->ev_pending[q] = false;
+    }
+    return MH_OK;
+}
+
+int mh_ctx_phase_times(mh_ctx* ctx, int nphases, double* ms, int64_t* calls)
+{
+    if (!ctx || nphases < 0 || (nphases && (!ms || !calls))) return MH_ERR_ARG;
+    mh::phase_collect(ctx);
+    for (int q = 0; q < nphases; ++q) {
+        ms[q] = q < PH_N ? ctx->phase_ms[q] : 0.0;
+        calls[q] = q < PH_N ? ctx->phase_calls[q] : 0;
+    }
     return MH_OK;
 }
 

@@ -348,15 +348,21 @@ int run_fp64(const Batch& bt, const double* d_omegas, int nomega, double2* d_F, 
     MH_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     for (int z = 0; z < nomega; ++z) {
         const double k = h_w[z] * h_w[z] / bt.g;
+        phase_begin(ctx, PH_FP64_ASSEMBLY);
         MH_CUDA_TRY(ctx, launch_assemble_f64(ctx, bt.m, k, bt.mask, bt.direct, tab, S, D));
+        phase_end(ctx, PH_FP64_ASSEMBLY);
         k_bc_batch<<<dim3(blocks(n, 256), 1), 256, 0, ctx->stream>>>(
             bt.m->geom, n, bt.d_dofs, bt.ndof, bt.d_betas, bt.nbeta, d_omegas + z, bt.g, BC);
         ctx->launches += 1;
         if (bt.direct) {
             if ((rc = zgemm_strided(ctx, n, bt.nrhs, S, BC, X, 1, 1.0, 0.0))) return rc;
+            phase_begin(ctx, PH_FP64_LU);
             if ((rc = fp64_lu_solve(ctx, n, D, X, bt.nrhs))) return rc;
+            phase_end(ctx, PH_FP64_LU);
         } else {
+            phase_begin(ctx, PH_FP64_LU);
             if ((rc = fp64_lu_solve(ctx, n, D, BC, bt.nrhs))) return rc;
+            phase_end(ctx, PH_FP64_LU);
             if ((rc = zgemm_strided(ctx, n, bt.nrhs, S, BC, X, 1, 1.0, 0.0))) return rc;
         }
         k_forces_batch<<<bt.nrhs, 256, 0, ctx->stream>>>(
@@ -396,6 +402,7 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
     // matrices
     const uint32_t wave = bt.mask & (MH_GF_WU | MH_GF_DELHOMMEAU);
     dim3 grid(blocks(n, kRows), blocks(n, kCols), (unsigned)nb);
+    phase_begin(ctx, PH_WAVE);
     if (wave == MH_GF_WU)
         k_wave_batch<false><<<grid, kRows, 0, ctx->stream>>>(bt.m->geom, n, bt.direct, nullptr, d_k, SR,
                                                             DR, S64, D64, Dlo);
@@ -407,6 +414,8 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
     else
         return set_err(ctx, MH_ERR_ARG, "the mixed path takes one wave term (GFWu or Delhommeau)");
     ctx->launches += 1;
+    phase_end(ctx, PH_WAVE);
+    phase_begin(ctx, PH_RHS);
     k_bc_batch<<<dim3(blocks(n, 256), nb), 256, 0, ctx->stream>>>(
         bt.m->geom, n, bt.d_dofs, bt.ndof, bt.d_betas, bt.nbeta, d_omegas, bt.g, BC);
     ctx->launches += 1;
@@ -417,9 +426,13 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
         MH_CUDA_TRY(ctx, cudaMemcpyAsync(RHS, BC, sizeof(double2) * nv * nb, cudaMemcpyDeviceToDevice,
                                          ctx->stream));
     }
+    phase_end(ctx, PH_RHS);
     // FP32 LU of every D (or K)
     MH_CUDA_TRY(ctx, cudaMemsetAsync(d_bad, 0, sizeof(int) * nb, ctx->stream));
+    phase_begin(ctx, PH_LU);
     MH_CUDA_TRY(ctx, launch_lu_f32(ctx, Dlo, n, nn, nb, Dinv, d_bad));
+    phase_end(ctx, PH_LU);
+    phase_begin(ctx, PH_REFINE);
     // refinement: x = 0, r = rhs
     MH_CUDA_TRY(ctx, cudaMemsetAsync(X, 0, sizeof(double2) * nv * nb, ctx->stream));
     MH_CUDA_TRY(ctx, cudaMemcpyAsync(R, RHS, sizeof(double2) * nv * nb, cudaMemcpyDeviceToDevice,
@@ -448,6 +461,7 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
         for (int z = 0; z < nb; ++z) worst = std::max(worst, std::isfinite(h_res[z]) ? h_res[z] : INFINITY);
         if (worst <= tol) break;
     }
+    phase_end(ctx, PH_REFINE);
     MH_CUDA_TRY(ctx, cudaMemcpyAsync(h_bad.data(), d_bad, sizeof(int) * nb, cudaMemcpyDeviceToHost,
                                      ctx->stream));
     MH_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
@@ -470,9 +484,11 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
         if ((rc = zgemm_strided(ctx, n, nrhs, S64, X, R, nb, 1.0, 0.0))) return rc;
         PHI = R;
     }
+    phase_begin(ctx, PH_FORCES);
     k_forces_batch<<<nb * nrhs, 256, 0, ctx->stream>>>(bt.m->geom, n, bt.d_dofs, bt.ndof, bt.d_betas,
                                                         bt.nbeta, d_omegas, bt.rho, bt.g, PHI, d_F, d_FK);
     ctx->launches += 1;
+    phase_end(ctx, PH_FORCES);
     MH_CUDA_TRY(ctx, cudaGetLastError());
     return MH_OK;
 }
@@ -520,10 +536,12 @@ int hydro_batch(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double* ome
         auto* SR = (double*)ws_get(ctx, WS_SR, sizeof(double) * nn * 2);
         if (!SR) return MH_ERR_OOM;
         double* DR = SR + nn;
+        phase_begin(ctx, PH_RANKINE);
         k_rankine_real<<<dim3(blocks(n, kRows), blocks(n, kCols)), kRows, 0, ctx->stream>>>(
             m->geom, n, mask & (MH_GF_RANKINE | MH_GF_RANKINE_REFLECTED |
                                 MH_GF_RANKINE_REFLECTED_NEGATIVE), direct, SR, DR);
         ctx->launches += 1;
+        phase_end(ctx, PH_RANKINE);
         MH_CUDA_TRY(ctx, cudaGetLastError());
         const size_t per = nn * (2 * sizeof(double2) + sizeof(float2)) +
                            (size_t)n * nrhs * (5 * sizeof(double2) + sizeof(float2));
@@ -535,6 +553,7 @@ int hydro_batch(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double* ome
         }
     }
     if (rc) return rc;
+    phase_collect(ctx);
     std::vector<double2> h(out_count);
     MH_CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), d_out, sizeof(double2) * out_count,
                                      cudaMemcpyDeviceToHost, ctx->stream));

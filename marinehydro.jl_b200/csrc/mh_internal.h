@@ -35,6 +35,12 @@ enum WsSlot : int {
 // Largest number of right-hand sides (radiating dofs + headings) per frequency.
 constexpr int kMaxRhs = 16;
 
+// Phases timed with CUDA events when profiling is on (mh_ctx_set_profiling).
+enum Phase : int {
+    PH_RANKINE = 0, PH_WAVE, PH_RHS, PH_LU, PH_REFINE, PH_FORCES, PH_FP64_ASSEMBLY, PH_FP64_LU,
+    PH_N
+};
+
 struct mh_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -44,6 +50,11 @@ struct mh_ctx {
     int64_t launches = 0;
     int delh_method = MH_DELHOMMEAU_TABLE;
     double* delh_table = nullptr;  // device, kTabWords doubles (built on first use)
+    bool profile = false;
+    cudaEvent_t ev[2 * PH_N] = {};
+    bool ev_pending[PH_N] = {};
+    double phase_ms[PH_N] = {};
+    int64_t phase_calls[PH_N] = {};
     void* ws[WS_NSLOTS] = {};
     size_t ws_bytes[WS_NSLOTS] = {};
 };
@@ -51,6 +62,11 @@ struct mh_ctx {
 namespace mh {
 
 int set_err(mh_ctx* ctx, int code, const char* fmt, ...);
+// Phase timing (no-ops unless ctx->profile): begin/end record events on the
+// ctx stream; collect() adds the elapsed times of completed phases.
+void phase_begin(mh_ctx* ctx, int ph);
+void phase_end(mh_ctx* ctx, int ph);
+void phase_collect(mh_ctx* ctx);
 // Returns a device buffer of at least `bytes` for `slot` (nullptr + error set on failure).
 void* ws_get(mh_ctx* ctx, int slot, size_t bytes);
 

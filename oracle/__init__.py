@@ -285,6 +285,43 @@ def froude_krylov_force(mesh, omega, dof, beta=0.0, rho=1000.0, g=9.81):
     return integrate_pressure(mesh.normals, mesh.areas, p, dof)
 
 
+def hydro_coefficients(mesh, omegas, dofs, betas=(), rho=1000.0, g=9.81,
+                       gf_mask=GF_RANKINE | GF_RANKINE_REFLECTED | GF_WU, direct=True, nthreads=0):
+    """Per-problem restatement of compute_hydrodynamic_coefficients
+    (src/problems_and_results.jl:70-181, src/solve.jl:4-21): one radiation
+    problem per (omega, dof), one diffraction problem per (omega, beta), all
+    dofs influenced.  Returns added_mass[i, j, w], damping[i, j, w],
+    diffraction[i, w, b], froude_krylov[i, w, b]."""
+    omegas = np.atleast_1d(np.asarray(omegas, dtype=np.float64))
+    nd, nw, nb = len(dofs), len(omegas), len(betas)
+    A = np.zeros((nd, nd, nw))
+    B = np.zeros((nd, nd, nw))
+    Fd = np.zeros((nd, nw, nb), dtype=np.complex128)
+    Fk = np.zeros((nd, nw, nb), dtype=np.complex128)
+    for w_i, w in enumerate(omegas):
+        k = w * w / g
+        S, D = assemble(mesh, k, gf_mask, direct, nthreads)
+        import scipy.linalg as sla
+        lu = sla.lu_factor(D, check_finite=False)
+        for j, dj in enumerate(dofs):
+            bc = radiation_bc(mesh.normals, dj, w)
+            phi = sla.lu_solve(lu, S @ bc) if direct else S @ sla.lu_solve(lu, bc)
+            p = 1j * rho * w * phi
+            for i, di in enumerate(dofs):
+                F = integrate_pressure(mesh.normals, mesh.areas, p, di)
+                A[i, j, w_i] = F.real / w ** 2
+                B[i, j, w_i] = F.imag / w
+        for b_i, beta in enumerate(betas):
+            bc = airy_bc(mesh.centers, mesh.normals, w, beta, g)
+            phi = sla.lu_solve(lu, S @ bc) if direct else S @ sla.lu_solve(lu, bc)
+            p = 1j * rho * phi * w
+            pk = airy_waves_pressure(mesh.centers, w, beta, rho, g)
+            for i, di in enumerate(dofs):
+                Fd[i, w_i, b_i] = integrate_pressure(mesh.normals, mesh.areas, p, di)
+                Fk[i, w_i, b_i] = integrate_pressure(mesh.normals, mesh.areas, pk, di)
+    return A, B, Fd, Fk
+
+
 def threads_env() -> int:
     v = os.environ.get("OMP_NUM_THREADS")
     return int(v) if v else 0

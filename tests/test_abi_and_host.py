@@ -126,3 +126,30 @@ def test_mesh_is_hashable_and_digest_tracks_changes(mh):
     dig = mh.api._mesh_digest(m)
     m.centers[0, 0] += 1e-3
     assert mh.api._mesh_digest(m) != dig
+
+
+def test_rigid_dofs_follow_reference(mh):
+    """src/bodies.jl:63-89: translations are unit fields, rotations axis x (x - c)."""
+    m = mh.mesh_hemisphere(1.0, (0, 0, 0), (6, 8))
+    b = mh.FloatingBody.rigid(m, ["Surge", "Heave", "Pitch", "Yaw"], (1.0, 1.0, 0.0))
+    assert np.array_equal(b.dofs["Surge"], np.tile([1.0, 0, 0], (m.nfaces, 1)))
+    assert np.array_equal(b.dofs["Heave"], np.tile([0, 0, 1.0], (m.nfaces, 1)))
+    pos = m.centers - np.array([1.0, 1.0, 0.0])
+    assert np.allclose(b.dofs["Pitch"], np.cross([0, 1.0, 0], pos))
+    assert np.allclose(b.dofs["Yaw"], np.cross([0, 0, 1.0], pos))
+    with pytest.raises(ValueError):
+        mh.FloatingBody.rigid(m, ["Wobble"])
+
+
+def test_combine_floatingbodies_names(mh):
+    """src/bodies.jl:102-170: unique names and zero-padded dof fields."""
+    assert mh.make_body_name_list_unique(["a", "a", "a_2", "b"]) == ["a", "a_3", "a_2", "b"]
+    m = mh.mesh_hemisphere(1.0, (0, 0, 0), (4, 6))
+    b1 = mh.FloatingBody.rigid(m, ["Heave"], body_name="my body")
+    b2 = mh.FloatingBody.rigid(m.translated((3, 0, 0)), ["Heave", "Surge"], body_name="my body")
+    c = b1 + b2
+    assert c.body_name == "my_body+my_body_2"
+    assert list(c.dofs) == ["my_body__Heave", "my_body_2__Heave", "my_body_2__Surge"]
+    assert np.all(c.dofs["my_body__Heave"][m.nfaces:] == 0)
+    assert np.all(c.dofs["my_body_2__Heave"][:m.nfaces] == 0)
+    assert np.all(c.dofs["my_body_2__Heave"][m.nfaces:, 2] == 1)
