@@ -83,7 +83,8 @@ int mh_ctx_create(int device, mh_ctx** out);
 int mh_ctx_destroy(mh_ctx* ctx);
 
 /* Message of the last error on this context (ctx == NULL: last error of
- * mh_ctx_create on this thread).  Valid until the next call on the ctx. */
+ * mh_ctx_create or of mh_solve_mixed_noalloc on this thread).  Valid until
+ * the next call on the ctx (or on this thread, for NULL). */
 const char* mh_last_error(const mh_ctx* ctx);
 
 /* Number of this library's own kernels launched on the ctx so far. */
@@ -204,6 +205,35 @@ int mh_hydro_batch(mh_ctx* ctx, const mh_mesh* mesh,
                    double* added_mass, double* damping,
                    double* diffraction, double* froude_krylov,
                    mh_batch_info* info);
+
+/* ---- allocation-free mixed-precision solve ------------------------------ */
+
+#define MH_NOALLOC_MAX_N    1024
+#define MH_NOALLOC_MAX_RHS  16
+
+/* X = A^-1 B for a dense complex128 A (n x n) and B (n x nrhs), all three
+ * column-major DEVICE buffers owned by the caller, by the same method as the
+ * batched mixed path (pivot-free FP32 LU of A, FP64 refinement until
+ * max|B - A X| / max|B| <= tol per column, at most max_iter sweeps), WITHOUT
+ * allocating any device memory: its scratch is one static device array of
+ * fixed size, so it serves callers that cannot call cudaMalloc (a memory
+ * pool that owns the whole device, a fixed-footprint real-time loop, a host
+ * thread that must not block on the allocator).  No counterpart in the
+ * reference.
+ * Limits: n <= MH_NOALLOC_MAX_N, nrhs <= MH_NOALLOC_MAX_RHS (beyond them:
+ * MH_ERR_ARG); the static array (~9 MiB) is held by every GPU that loads the
+ * library until the process exits.  Runs on the calling thread's current
+ * device, on `stream` (a cudaStream_t; NULL = default stream), and returns
+ * after the work is done.  All calls on a device share the array: calls that
+ * overlap on the GPU race, so serialise them.  The first call on a device
+ * looks up the array's address (cudaGetSymbolAddress) and should come before
+ * any stream capture.  A bad FP32 pivot or no convergence within max_iter
+ * gives MH_ERR_NOT_CONVERGED (X then holds the last iterate).
+ * iterations / rel_residual (host, may be NULL) report the sweeps used and
+ * the final residual ratio; errors go to mh_last_error(NULL). */
+int mh_solve_mixed_noalloc(int64_t n, const void* A, const void* B, int64_t nrhs, void* X,
+                           double tol, int max_iter, void* stream,
+                           int32_t* iterations, double* rel_residual);
 
 #ifdef __cplusplus
 }

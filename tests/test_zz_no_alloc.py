@@ -1,0 +1,73 @@
+"""The allocation-free solve (mh_solve_mixed_noalloc) through the C ABI (GPU).
+
+Callers that cannot allocate device memory (an application whose pool owns
+the device, a fixed-footprint real-time loop) hand the library device buffers
+they already own; the entry point keeps its scratch in one static device
+array.  This file is collected last so that, if it fails, a run that stops at
+the first failure has already run every other test; it also passes when run
+alone in a fresh process.
+
+Checked against the existing FP64 entry point mh_solve (cuSOLVER LU) with
+S = I, i.e. X = D^-1 B, within 1e-9 (the tolerance of the other mixed-path
+tests), on two calls in a row with different matrices and right-hand sides,
+so the second call cannot reuse anything the first left in the shared array.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _device(a, torch):
+    """Column-major complex128 numpy array -> device tensor with the same
+    memory layout (the transpose of a C-contiguous tensor)."""
+    return torch.from_numpy(np.ascontiguousarray(np.asarray(a, dtype=np.complex128).T)).cuda()
+
+
+def _noalloc(mh, torch, D, B, tol=1e-12, max_iter=30):
+    n, nrhs = B.shape
+    dA, dB = _device(D, torch), _device(B, torch)
+    dX = torch.empty((nrhs, n), dtype=torch.complex128, device="cuda")
+    iters = ctypes.c_int32(0)
+    res = ctypes.c_double(0.0)
+    stream = torch.cuda.current_stream().cuda_stream
+    rc = mh.native.lib().mh_solve_mixed_noalloc(
+        n, ctypes.c_void_p(dA.data_ptr()), ctypes.c_void_p(dB.data_ptr()), nrhs,
+        ctypes.c_void_p(dX.data_ptr()), tol, max_iter, ctypes.c_void_p(stream),
+        ctypes.byref(iters), ctypes.byref(res))
+    return rc, dX.cpu().numpy().T, iters.value, res.value
+
+
+def test_noalloc_matches_fp64_solve_twice(mh, gpu):
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(11)
+    cases = [(mh.mesh_hemisphere(1.0, (0, 0, 0), (16, 32)), 0.6, 3),
+             (mh.mesh_hemisphere(1.0, (0, 0, 0), (24, 36)) + mh.mesh_hemisphere(1.0, (4, 0, 0), (8, 12)),
+              1.4, 2)]
+    for mesh, k, nrhs in cases:
+        _, D = mh.assemble_matrices(mh.DEFAULT_GREEN_FUNCTIONS, mesh, k, ctx=gpu)
+        n = mesh.nfaces
+        B = rng.standard_normal((n, nrhs)) + 1j * rng.standard_normal((n, nrhs))
+        ref = mh.solve(D, np.eye(n, dtype=np.complex128), B, ctx=gpu)
+        rc, X, iters, res = _noalloc(mh, torch, D, B)
+        assert rc == 0, mh.native.lib().mh_last_error(None)
+        assert 1 <= iters <= 10 and res <= 1e-12
+        err = np.max(np.abs(X - ref)) / np.max(np.abs(ref))
+        assert err < 1e-9, err
+
+
+def test_noalloc_rejects_sizes_beyond_its_maximum(mh, gpu):
+    torch = pytest.importorskip("torch")
+    L = mh.native.lib()
+    n = 1025  # MH_NOALLOC_MAX_N + 1
+    dA = torch.zeros((n, n), dtype=torch.complex128, device="cuda")
+    dB = torch.zeros((1, n), dtype=torch.complex128, device="cuda")
+    dX = torch.zeros((1, n), dtype=torch.complex128, device="cuda")
+    rc = L.mh_solve_mixed_noalloc(n, ctypes.c_void_p(dA.data_ptr()), ctypes.c_void_p(dB.data_ptr()),
+                                  1, ctypes.c_void_p(dX.data_ptr()), 1e-10, 10, None, None, None)
+    assert rc == mh.native.MH_ERR_ARG
+    assert b"1024" in L.mh_last_error(None)
