@@ -69,7 +69,10 @@ def config_dict(mesh, omegas, args):
             "n_omega": int(len(omegas)), "omega_range": [float(omegas[0]), float(omegas[-1])],
             "dofs": ["Heave", "Surge"], "headings": [0.0],
             "green_functions": "Rankine+RankineReflected+ExactGuevelDelhommeau(table)",
-            "formulation": "direct", "precision": "mixed (FP32 LU, FP64 refinement)",
+            "formulation": "direct",
+            "precision": ("mixed: FP16 tcgen05 trailing update / FP32 LU, FP64 refinement"
+                          if args.lu == "tcgen05" else "mixed: FP32 LU, FP64 refinement"),
+            "lu_backend": args.lu,
             "tol": args.tol, "solve": "one (mesh, omega) problem, 3 right-hand sides",
             "l2": "working set ~11 GB per step, larger than the 126 MB L2 (no flush needed)"}
 
@@ -238,6 +241,7 @@ def run_ours(args):
         torch.cuda.set_device(local)
     mh = load_package()
     ctx = mh.Context(local)
+    ctx.set_lu_backend(args.lu)
     stream = torch.cuda.ExternalStream(ctx.stream())
     mesh, dofs, omegas, betas, gfs = workload(mh, args.res, args.n_omega)
     mask = mh.gf_mask(gfs)
@@ -320,7 +324,8 @@ def run_ours(args):
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64+f32 (FP64 matrices and residuals, FP32 LU)", "data": "synthetic",
+            "dtype": ("f64+f32+f16 (FP64 matrices and residuals, FP32 LU panels, FP16 tensor-core "
+                      "updates)" if args.lu == "tcgen05" else "f64+f32"), "data": "synthetic",
             "config": config_dict(mesh, omegas, args), "e2e": e2e, "gpu_launches": launches,
             "refinement": {"iterations": info.refine_iterations, "fallbacks": info.n_fallback,
                            "max_rel_residual": info.max_rel_residual}}
@@ -425,6 +430,7 @@ def main():
     ap.add_argument("--max-iter", type=int, default=30)
     ap.add_argument("--fp64-omegas", type=int, default=8)
     ap.add_argument("--cpu-columns", type=int, default=64)
+    ap.add_argument("--lu", default="tcgen05", choices=["tcgen05", "simt"])
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()

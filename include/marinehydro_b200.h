@@ -58,6 +58,10 @@ extern "C" {
 #define MH_DELHOMMEAU_TABLE  0  /* 2-D Chebyshev table built on the device from the FP64 quadrature (default) */
 #define MH_DELHOMMEAU_EXACT  1  /* adaptive Gauss-Kronrod quadrature per panel pair, as the reference */
 
+/* low-precision LU of the mixed path */
+#define MH_LU_SIMT_F32     0  /* FP32 complex blocked LU on the CUDA cores (block 32) */
+#define MH_LU_TCGEN05_F16  1  /* block-64 LU, trailing update as FP16 tcgen05 MMA with FP32 accumulation in tensor memory */
+
 typedef struct mh_ctx mh_ctx;
 typedef struct mh_mesh mh_mesh;
 
@@ -105,6 +109,20 @@ int mh_ctx_phase_times(mh_ctx* ctx, int nphases, double* ms, int64_t* calls);
  * (default) or MH_DELHOMMEAU_EXACT (per-pair adaptive quadrature, the
  * reference's method, src/green_functions/exact_Guevel_Delhommeau.jl:8-26). */
 int mh_ctx_set_delhommeau_method(mh_ctx* ctx, int method);
+
+/* Low-precision LU backend of the mixed path on this ctx (MH_LU_*).  No
+ * reference counterpart (the reference factors in FP64 with LAPACK). */
+int mh_ctx_set_lu_backend(mh_ctx* ctx, int backend);
+
+/* Pivot-free low-precision LU of nbatch n x n complex matrices as the mixed
+ * path computes it: A_host is nbatch x n x n complex128 column-major, LU_host
+ * receives the factors (unit-lower L below the diagonal, U on and above) as
+ * complex64 (interleaved float32), bad_host[b] != 0 flags a matrix with a bad
+ * pivot or a timed-out tensor-core wait.  Test and diagnostic hook of the
+ * factorisation that replaces LAPACK's getrf in `solve`
+ * (src/matrix_assembly.jl:105-133). */
+int mh_lu_factor_lowp(mh_ctx* ctx, int backend, int64_t n, int64_t nbatch, const double* A_host,
+                      float* LU_host, int* bad_host);
 
 /* Dimensionless wave term at n points (r[i], z[i]), z < 0, on the device:
  * out[6*i .. 6*i+5] = (G, dG/dr, dG/dz) as (re, im) pairs.  `which` is

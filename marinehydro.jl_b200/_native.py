@@ -27,6 +27,9 @@ MH_ERR_SINGULAR = 7
 MH_DELHOMMEAU_TABLE = 0
 MH_DELHOMMEAU_EXACT = 1
 
+MH_LU_SIMT_F32 = 0
+MH_LU_TCGEN05_F16 = 1
+
 MH_PRECISION_FP64 = 0
 MH_PRECISION_MIXED = 1
 
@@ -68,6 +71,10 @@ SIGNATURES = {
     "mh_ctx_kernel_launches": (ctypes.c_int, [_P, _I64]),
     "mh_ctx_set_delhommeau_method": (ctypes.c_int, [_P, ctypes.c_int]),
     "mh_ctx_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
+    "mh_ctx_set_lu_backend": (ctypes.c_int, [_P, ctypes.c_int]),
+    "mh_lu_factor_lowp": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int64, ctypes.c_int64, _D,
+                                         ctypes.POINTER(ctypes.c_float),
+                                         ctypes.POINTER(ctypes.c_int)]),
     "mh_ctx_set_profiling": (ctypes.c_int, [_P, ctypes.c_int]),
     "mh_ctx_phase_times": (ctypes.c_int, [_P, ctypes.c_int, _D, _I64]),
     "mh_wave_term": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_int64, _D, _D, _D]),
@@ -178,6 +185,28 @@ class Context:
         return c[:, 0], c[:, 1], c[:, 2]
 
     PHASES = ("rankine", "wave", "rhs", "lu", "refine", "forces", "fp64_assembly", "fp64_lu")
+
+    def set_lu_backend(self, backend: str):
+        """'simt' (FP32 CUDA cores) or 'tcgen05' (FP16 tensor-core trailing update)."""
+        code = {"simt": MH_LU_SIMT_F32, "tcgen05": MH_LU_TCGEN05_F16}[backend]
+        check(lib().mh_ctx_set_lu_backend(self._h, code), self._h)
+
+    def lu_factor_lowp(self, A, backend: str = "tcgen05"):
+        """Pivot-free low-precision LU of a batch (nbatch, n, n) of complex
+        matrices; returns (LU as complex64 (nbatch, n, n), bad flags)."""
+        A = np.asarray(A, dtype=np.complex128)
+        if A.ndim == 2:
+            A = A[None]
+        nb, n, _ = A.shape
+        # column-major per matrix: the transpose of each C-ordered matrix
+        Af = np.ascontiguousarray(np.transpose(A, (0, 2, 1)))
+        LU = np.empty((nb, n, n), dtype=np.complex64)
+        bad = np.zeros(nb, dtype=np.int32)
+        code = {"simt": MH_LU_SIMT_F32, "tcgen05": MH_LU_TCGEN05_F16}[backend]
+        check(lib().mh_lu_factor_lowp(self._h, code, n, nb, dptr(Af),
+                                      LU.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                      bad.ctypes.data_as(ctypes.POINTER(ctypes.c_int))), self._h)
+        return np.transpose(LU, (0, 2, 1)), bad
 
     def stream(self) -> int:
         """The ctx's cudaStream_t as an integer handle."""

@@ -364,6 +364,47 @@ int mh_ctx_set_delhommeau_method(mh_ctx* ctx, int method)
     return MH_OK;
 }
 
+int mh_ctx_set_lu_backend(mh_ctx* ctx, int backend)
+{
+    int rc;
+    if ((rc = check_ctx(ctx))) return rc;
+    if (backend != MH_LU_SIMT_F32 && backend != MH_LU_TCGEN05_F16)
+        return set_err(ctx, MH_ERR_ARG, "unknown LU backend %d", backend);
+    ctx->lu_backend = backend;
+    return MH_OK;
+}
+
+int mh_lu_factor_lowp(mh_ctx* ctx, int backend, int64_t n, int64_t nbatch, const double* A_host,
+                      float* LU_host, int* bad_host)
+{
+    int rc;
+    if ((rc = check_ctx(ctx))) return rc;
+    if (backend != MH_LU_SIMT_F32 && backend != MH_LU_TCGEN05_F16)
+        return set_err(ctx, MH_ERR_ARG, "unknown LU backend %d", backend);
+    if (n < 1 || nbatch < 1 || !A_host || !LU_host || !bad_host)
+        return set_err(ctx, MH_ERR_ARG, "bad arguments to mh_lu_factor_lowp");
+    const size_t nn = (size_t)n * (size_t)n, cnt = nn * (size_t)nbatch;
+    auto* d64 = (double2*)ws_get(ctx, WS_D, sizeof(double2) * cnt);
+    auto* lo = (float2*)ws_get(ctx, WS_LO, sizeof(float2) * cnt);
+    const int64_t dst = backend == MH_LU_TCGEN05_F16 ? mh::lu_dinv_stride_tc(n) : mh::lu_dinv_stride(n);
+    auto* dinv = (float2*)ws_get(ctx, WS_DINV, sizeof(float2) * (size_t)dst * (size_t)nbatch);
+    auto* bad = (int*)ws_get(ctx, WS_MISC, sizeof(int) * (size_t)nbatch);
+    if (!d64 || !lo || !dinv || !bad) return MH_ERR_OOM;
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(d64, A_host, sizeof(double2) * cnt, cudaMemcpyHostToDevice,
+                                     ctx->stream));
+    MH_CUDA_TRY(ctx, mh::launch_to_f32(ctx, d64, lo, (int64_t)cnt));
+    MH_CUDA_TRY(ctx, cudaMemsetAsync(bad, 0, sizeof(int) * (size_t)nbatch, ctx->stream));
+    if (backend == MH_LU_TCGEN05_F16)
+        MH_CUDA_TRY(ctx, mh::launch_lu_tc(ctx, lo, n, (int64_t)nn, (int)nbatch, dinv, bad));
+    else
+        MH_CUDA_TRY(ctx, mh::launch_lu_f32(ctx, lo, n, (int64_t)nn, (int)nbatch, dinv, bad));
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(LU_host, lo, sizeof(float2) * cnt, cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(bad_host, bad, sizeof(int) * (size_t)nbatch,
+                                     cudaMemcpyDeviceToHost, ctx->stream));
+    return sync_status(ctx, "low-precision LU");
+}
+
 int mh_wave_term(mh_ctx* ctx, uint32_t which, int64_t n, const double* r, const double* z,
                  double* out)
 {

@@ -31,6 +31,7 @@ constexpr int kRows = 128;
 constexpr int kCols = 16;
 constexpr double kInv4Pi = 1.0 / (4.0 * kPi);
 constexpr size_t kBatchBytes = 16ull << 30;  // device memory budget of one frequency chunk
+constexpr int kAllwMinFreqs = 6;  // chunks this large use the frequency-batched Delhommeau pass
 
 __device__ __forceinline__ void load_panel_field(Panel& p, int f, double v)
 {
@@ -111,6 +112,126 @@ k_wave_batch(const double* __restrict__ geom, int64_t n, int direct, const doubl
         S64[mat + o] = make_double2(sr, si);
         D64[mat + o] = make_double2(dr, di);
         Dlo[mat + o] = make_float2((float)dr, (float)di);
+    }
+}
+
+// Frequency-batched tabulated Delhommeau term.  Every frequency of the chunk
+// sees the same panel pair, so the pair's polar angle alpha is fixed and only
+// R = k d moves: the alpha direction of the four polar tables (B, C,
+// E0 = e^z J0(r), E1 = e^z J1(r)) is contracted once per pair into
+// w_q[i] = sum_j c_q[i][j] T_j(v(alpha)) (shared memory), and each frequency
+// then evaluates four 1-D Chebyshev series in R (Clenshaw) with no
+// transcendental calls; the log term splits as log(k) + log((d + |zeta|)/2).
+// Frequencies at which the pair leaves the polar patch use the full table.
+// Same arithmetic as wave_pair<true> up to reassociation (~1e-16).
+constexpr int kWT = 128;  // threads (rows) per CTA of k_wave_delh_allw
+constexpr size_t kWaveAllwSmem = sizeof(double) * (4 * kTabNP * kTabNP + 4 * kTabNP * kWT);
+
+__global__ void __launch_bounds__(kWT, 2)
+k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const double* __restrict__ tab,
+                 const double* __restrict__ kvec, int nb, const double* __restrict__ SR,
+                 const double* __restrict__ DR, double2* __restrict__ S64, double2* __restrict__ D64,
+                 float2* __restrict__ Dlo)
+{
+    extern __shared__ double wsm[];
+    double* coef = wsm;                           // 4 polar tables, NP x NP each
+    double* w = wsm + 4 * kTabNP * kTabNP;         // [4*NP][kWT]
+    __shared__ Panel sp[kCols];
+    const int64_t j0 = (int64_t)blockIdx.y * kCols;
+    stage_panels(sp, geom, n, j0);
+    for (int t = threadIdx.x; t < 4 * kTabNP * kTabNP; t += blockDim.x) coef[t] = tab[t];
+    __syncthreads();
+    const int tid = threadIdx.x;
+    const int64_t i = (int64_t)blockIdx.x * kWT + tid;
+    if (i >= n) return;
+    const int64_t nn = n * n;
+    const double x[3] = {geom[G_CX * n + i], geom[G_CY * n + i], geom[G_CZ * n + i]};
+    const double ni[3] = {geom[G_NX * n + i], geom[G_NY * n + i], geom[G_NZ * n + i]};
+    const bool wrt_first = !direct;
+    const int jend = (int)min((int64_t)kCols, n - j0);
+    for (int jj = 0; jj < jend; ++jj) {
+        const Panel& p = sp[jj];
+        const int64_t j = j0 + jj;
+        const int64_t o = j * n + i;
+        const double* nn3 = direct ? p.n : ni;
+        // pair geometry (abstract_greens_function.jl:111-131 at k = 1)
+        const double dx = x[0] - p.c[0], dy = x[1] - p.c[1];
+        const double dis2 = dx * dx + dy * dy;
+        const double purt = 1e-18;
+        const double rho = (dis2 == 0.0) ? sqrt(dis2 + purt * purt) - purt : sqrt(dis2);
+        const double zeta = x[2] + p.c[2];
+        const double az = -zeta;
+        const double d = hypot(rho, zeta);
+        const bool polar_ok = az >= 0.0;
+        const double v = 4.0 * atan2(rho, az) / kPi - 1.0;
+        const double lp = log(0.5 * (d + az));
+        const double gp = rho / (d * (d + az));
+        const double sr = SR[o], dr = DR[o];
+        // contract alpha: w_q[row] = sum_j c_q[row][j] T_j(v)
+        if (polar_ok) {
+#pragma unroll 1
+            for (int q = 0; q < 4; ++q) {
+                const double* c = coef + q * kTabNP * kTabNP;
+#pragma unroll 1
+                for (int row = 0; row < kTabNP; ++row) {
+                    const double* cr = c + row * kTabNP;
+                    double b1 = 0.0, b2 = 0.0;
+#pragma unroll
+                    for (int col = kTabNP - 1; col >= 1; --col) {
+                        const double t = fma(2.0 * v, b1, cr[col] - b2);
+                        b2 = b1;
+                        b1 = t;
+                    }
+                    w[(q * kTabNP + row) * kWT + tid] = fma(v, b1, cr[0] - b2);
+                }
+            }
+        }
+        for (int z = 0; z < nb; ++z) {
+            const double k = kvec[z];
+            const double r = k * rho, zz = k * zeta;
+            const double R = k * d;
+            cplx o3[3];
+            if (polar_ok && R < kTabRPolar) {
+                const double u = 2.0 * R / kTabRPolar - 1.0;
+                double val[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const double* wq = w + q * kTabNP * kWT + tid;
+                    double b1 = 0.0, b2 = 0.0;
+#pragma unroll
+                    for (int row = kTabNP - 1; row >= 1; --row) {
+                        const double t = fma(2.0 * u, b1, wq[row * kWT] - b2);
+                        b2 = b1;
+                        b1 = t;
+                    }
+                    val[q] = fma(u, b1, wq[0] - b2);
+                }
+                const double B = val[0], C = val[1], E0 = val[2], E1 = val[3];
+                const double L = log(k) + lp;
+                const double G_re = -2.0 * E0 * L + B, G_im = 2.0 * kPi * E0;
+                o3[0] = mk(G_re, G_im);
+                o3[1] = mk(2.0 * E1 * L - 2.0 * E0 * gp / k + C, -2.0 * kPi * E1);
+                o3[2] = mk(G_re + 2.0 / R, G_im);
+            } else {
+                delh_dimless_table(tab, r, zz, o3);
+            }
+            double d1 = 0.0, d2 = 0.0;
+            if (fabs(r) > 1e-6) {
+                const double f = k * k / r;
+                d1 = wrt_first ? f * dx : -f * dx;
+                d2 = wrt_first ? f * dy : -f * dy;
+            }
+            const double ka = k * p.area;
+            const cplx s = ka * o3[0];
+            const cplx g0 = (ka * d1) * o3[1], g1 = (ka * d2) * o3[1], g2 = (ka * k) * o3[2];
+            const double Sr = sr - kInv4Pi * s.re, Si = -kInv4Pi * s.im;
+            const double Dr = dr - kInv4Pi * (nn3[0] * g0.re + nn3[1] * g1.re + nn3[2] * g2.re);
+            const double Di = -kInv4Pi * (nn3[0] * g0.im + nn3[1] * g1.im + nn3[2] * g2.im);
+            const int64_t m = (int64_t)z * nn + o;
+            S64[m] = make_double2(Sr, Si);
+            D64[m] = make_double2(Dr, Di);
+            Dlo[m] = make_float2((float)Dr, (float)Di);
+        }
     }
 }
 
@@ -386,13 +507,16 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
     auto* S64 = (double2*)ws_get(ctx, WS_S, sizeof(double2) * nn * nb);
     auto* D64 = (double2*)ws_get(ctx, WS_D, sizeof(double2) * nn * nb);
     auto* Dlo = (float2*)ws_get(ctx, WS_LO, sizeof(float2) * nn * nb);
-    auto* Dinv = (float2*)ws_get(ctx, WS_DINV, sizeof(float2) * lu_dinv_stride(n) * nb);
+    const bool tc = ctx->lu_backend == MH_LU_TCGEN05_F16;
+    const int64_t dinv_stride = tc ? lu_dinv_stride_tc(n) : lu_dinv_stride(n);
+    auto* Dinv = (float2*)ws_get(ctx, WS_DINV, sizeof(float2) * dinv_stride * nb);
+    auto* T32 = (float2*)ws_get(ctx, WS_TMP32B, sizeof(float2) * n * nrhs * nb);
     auto* BC = (double2*)ws_get(ctx, WS_RHS, sizeof(double2) * nv * nb);
     auto* X = (double2*)ws_get(ctx, WS_PHI, sizeof(double2) * nv * nb);
     auto* R = (double2*)ws_get(ctx, WS_TMP, sizeof(double2) * nv * nb * 2);
     auto* R32 = (float2*)ws_get(ctx, WS_TMP32, sizeof(float2) * nv * nb);
     auto* misc = (char*)ws_get(ctx, WS_MISC, (sizeof(double) + sizeof(int)) * nb + 64);
-    if (!S64 || !D64 || !Dlo || !Dinv || !BC || !X || !R || !R32 || !misc) return MH_ERR_OOM;
+    if (!S64 || !D64 || !Dlo || !Dinv || !T32 || !BC || !X || !R || !R32 || !misc) return MH_ERR_OOM;
     double2* RHS = R + nv * nb;  // right-hand side of the D (or K) system
     auto* d_res = (double*)misc;
     auto* d_bad = (int*)(misc + sizeof(double) * nb);
@@ -406,7 +530,13 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
     if (wave == MH_GF_WU)
         k_wave_batch<false><<<grid, kRows, 0, ctx->stream>>>(bt.m->geom, n, bt.direct, nullptr, d_k, SR,
                                                             DR, S64, D64, Dlo);
-    else if (wave == MH_GF_DELHOMMEAU)
+    else if (wave == MH_GF_DELHOMMEAU && tab && nb >= kAllwMinFreqs) {
+        MH_CUDA_TRY(ctx, cudaFuncSetAttribute(k_wave_delh_allw,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)kWaveAllwSmem));
+        k_wave_delh_allw<<<dim3(blocks(n, kWT), blocks(n, kCols)), kWT, kWaveAllwSmem, ctx->stream>>>(
+            bt.m->geom, n, bt.direct, tab, d_k, nb, SR, DR, S64, D64, Dlo);
+    } else if (wave == MH_GF_DELHOMMEAU)
         k_wave_batch<true><<<grid, kRows, 0, ctx->stream>>>(bt.m->geom, n, bt.direct, tab, d_k, SR, DR,
                                                            S64, D64, Dlo);
     else if (wave == 0)
@@ -430,7 +560,8 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
     // FP32 LU of every D (or K)
     MH_CUDA_TRY(ctx, cudaMemsetAsync(d_bad, 0, sizeof(int) * nb, ctx->stream));
     phase_begin(ctx, PH_LU);
-    MH_CUDA_TRY(ctx, launch_lu_f32(ctx, Dlo, n, nn, nb, Dinv, d_bad));
+    if (tc) MH_CUDA_TRY(ctx, launch_lu_tc(ctx, Dlo, n, nn, nb, Dinv, d_bad));
+    else MH_CUDA_TRY(ctx, launch_lu_f32(ctx, Dlo, n, nn, nb, Dinv, d_bad));
     phase_end(ctx, PH_LU);
     phase_begin(ctx, PH_REFINE);
     // refinement: x = 0, r = rhs
@@ -445,7 +576,8 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
     for (it = 1; it <= max_iter; ++it) {
         k_to_f32<<<blocks(cnt, 256), 256, 0, ctx->stream>>>(R, R32, cnt);
         ctx->launches += 1;
-        MH_CUDA_TRY(ctx, launch_lu_solve_f32(ctx, Dlo, n, nn, nb, Dinv, R32, nv, nrhs));
+        if (tc) MH_CUDA_TRY(ctx, launch_lu_solve_tc(ctx, Dlo, n, nn, nb, Dinv, R32, T32, nv, nrhs));
+        else MH_CUDA_TRY(ctx, launch_lu_solve_blocks32(ctx, Dlo, n, nn, nb, Dinv, R32, T32, nv, nrhs));
         k_add_f32<<<blocks(cnt, 256), 256, 0, ctx->stream>>>(X, R32, cnt);
         ctx->launches += 1;
         // R = RHS - D X
@@ -494,6 +626,13 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
 }
 
 }  // namespace
+
+cudaError_t launch_to_f32(mh_ctx* ctx, const double2* a, float2* b, int64_t count)
+{
+    k_to_f32<<<blocks(count, 256), 256, 0, ctx->stream>>>(a, b, count);
+    ctx->launches += 1;
+    return cudaGetLastError();
+}
 
 int hydro_batch(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double* omegas, int64_t ndof,
                 const double* dofs, int64_t nbeta, const double* betas, double rho, double g,

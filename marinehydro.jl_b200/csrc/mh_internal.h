@@ -29,7 +29,7 @@ struct mh_mesh {
 // Workspace slots of a context; each is a grow-only device buffer.
 enum WsSlot : int {
     WS_S = 0, WS_D, WS_RHS, WS_PHI, WS_TMP, WS_PIV, WS_INFO, WS_LWORK,
-    WS_DOF, WS_OUT, WS_LO, WS_DINV, WS_TMP32, WS_MISC, WS_SR, WS_NSLOTS
+    WS_DOF, WS_OUT, WS_LO, WS_DINV, WS_TMP32, WS_MISC, WS_SR, WS_TMP32B, WS_NSLOTS
 };
 
 // Largest number of right-hand sides (radiating dofs + headings) per frequency.
@@ -49,6 +49,7 @@ struct mh_ctx {
     std::string err;
     int64_t launches = 0;
     int delh_method = MH_DELHOMMEAU_TABLE;
+    int lu_backend = MH_LU_TCGEN05_F16;
     double* delh_table = nullptr;  // device, kTabWords doubles (built on first use)
     bool profile = false;
     cudaEvent_t ev[2 * PH_N] = {};
@@ -96,7 +97,20 @@ cudaError_t launch_lu_f32(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int
 cudaError_t launch_lu_solve_f32(mh_ctx* ctx, const float2* A, int64_t n, int64_t stride, int nbatch,
                                 const float2* Dinv, float2* X, int64_t xstride, int nrhs);
 
+// ---- tensor-core LU (mh_lu_tc.cu), block size 64 ----
+int64_t lu_dinv_stride_tc(int64_t n);
+cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int nbatch, float2* Dinv,
+                         int* bad);
+// Block-parallel (LU)^-1 X in place; T: scratch of the same size as X.
+cudaError_t launch_lu_solve_tc(mh_ctx* ctx, const float2* A, int64_t n, int64_t stride, int nbatch,
+                               const float2* Dinv, float2* X, float2* T, int64_t xstride, int nrhs);
+// The same block-parallel solve for the block-size-32 factors of launch_lu_f32.
+cudaError_t launch_lu_solve_blocks32(mh_ctx* ctx, const float2* A, int64_t n, int64_t stride,
+                                     int nbatch, const float2* Dinv, float2* X, float2* T,
+                                     int64_t xstride, int nrhs);
+
 // ---- batched driver (mh_batch.cu) ----
+cudaError_t launch_to_f32(mh_ctx* ctx, const double2* a, float2* b, int64_t count);
 int hydro_batch(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double* omegas, int64_t ndof,
                 const double* dofs, int64_t nbeta, const double* betas, double rho, double g,
                 uint32_t mask, int direct, int precision, double tol, int max_iter,

@@ -17,146 +17,12 @@
 #include <cuda_runtime.h>
 
 #include "mh_internal.h"
+#include "mh_lu_kernels.cuh"
 
 namespace mh {
 namespace {
 
 constexpr int NB = 32;
-
-__device__ __forceinline__ float2 cmulf(float2 a, float2 b)
-{
-    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ float2 csubf(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-// a - b*c
-__device__ __forceinline__ float2 cfms(float2 a, float2 b, float2 c)
-{
-    return make_float2(a.x - (b.x * c.x - b.y * c.y), a.y - (b.x * c.y + b.y * c.x));
-}
-__device__ __forceinline__ float2 cdivf(float2 a, float2 b)
-{
-    float d = b.x * b.x + b.y * b.y;
-    return make_float2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
-}
-
-// Factor the diagonal block [k0, k0+kb) of every matrix in place, and store
-// inv(L11) (unit lower) and inv(U11) in Dinv (per matrix: n/NB blocks of
-// 2 x NB x NB, column-major) for the triangular solves.
-__global__ void __launch_bounds__(256)
-k_lu_diag(float2* __restrict__ A, int64_t n, int64_t stride, int64_t k0, float2* __restrict__ Dinv,
-          int64_t dstride, int* __restrict__ bad)
-{
-    __shared__ float2 s[NB][NB + 1];   // s[row][col]
-    __shared__ float2 w[NB][NB + 1];   // inverse being built, w[row][col]
-    const int64_t b = blockIdx.x;
-    float2* M = A + b * stride;
-    const int kb = (int)min((int64_t)NB, n - k0);
-    for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) {
-        int r = t % NB, c = t / NB;
-        s[r][c] = (r < kb && c < kb) ? M[(k0 + c) * n + k0 + r]
-                                     : make_float2(r == c ? 1.f : 0.f, 0.f);
-    }
-    __syncthreads();
-    for (int c = 0; c < kb; ++c) {
-        float2 piv = s[c][c];
-        float mag = piv.x * piv.x + piv.y * piv.y;
-        if (threadIdx.x == 0 && !(mag > 1e-30f && mag < 3e38f)) atomicExch(bad + b, 1);
-        for (int r = c + 1 + threadIdx.x; r < kb; r += blockDim.x) s[r][c] = cdivf(s[r][c], piv);
-        __syncthreads();
-        int m = kb - c - 1;
-        for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
-            int r = c + 1 + t % m, q = c + 1 + t / m;
-            s[r][q] = cfms(s[r][q], s[r][c], s[c][q]);
-        }
-        __syncthreads();
-    }
-    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
-        int r = t % kb, c = t / kb;
-        M[(k0 + c) * n + k0 + r] = s[r][c];
-    }
-    float2* out = Dinv + b * dstride + (k0 / NB) * 2 * NB * NB;
-    // inv(L11): column c solves L y = e_c (unit lower), one thread per column
-    if (threadIdx.x < NB) {
-        const int c = threadIdx.x;
-        for (int r = 0; r < NB; ++r) {
-            float2 acc = make_float2(r == c ? 1.f : 0.f, 0.f);
-            for (int t = c; t < r; ++t) acc = cfms(acc, s[r][t], w[t][c]);
-            w[r][c] = (r < c) ? make_float2(0.f, 0.f) : acc;
-        }
-    }
-    __syncthreads();
-    for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) out[t] = w[t % NB][t / NB];
-    __syncthreads();
-    // inv(U11): column c solves U y = e_c, backward, one thread per column
-    if (threadIdx.x < NB) {
-        const int c = threadIdx.x;
-        for (int r = NB - 1; r >= 0; --r) {
-            float2 acc = make_float2(r == c ? 1.f : 0.f, 0.f);
-            if (r <= c) {
-                for (int t = r + 1; t <= c; ++t) acc = cfms(acc, s[r][t], w[t][c]);
-                acc = cdivf(acc, s[r][r]);
-            } else {
-                acc = make_float2(0.f, 0.f);
-            }
-            w[r][c] = acc;
-        }
-    }
-    __syncthreads();
-    for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) out[NB * NB + t] = w[t % NB][t / NB];
-}
-
-// blockIdx.y == 0: rows of L21 = A21 U11^-1; blockIdx.y == 1: columns of
-// U12 = L11^-1 A12.  blockIdx.z = matrix.
-__global__ void __launch_bounds__(128)
-k_lu_trsm(float2* __restrict__ A, int64_t n, int64_t stride, int64_t k0)
-{
-    __shared__ float2 s[NB][NB + 1];
-    float2* M = A + (int64_t)blockIdx.z * stride;
-    const int kb = (int)min((int64_t)NB, n - k0);
-    for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) {
-        int r = t % NB, c = t / NB;
-        s[r][c] = (r < kb && c < kb) ? M[(k0 + c) * n + k0 + r] : make_float2(0.f, 0.f);
-    }
-    __syncthreads();
-    const int64_t idx = k0 + kb + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= n) return;
-    float2 v[NB];
-    if (blockIdx.y == 0) {
-        // row idx: x U11 = a  ->  x_c = (a_c - sum_{t<c} x_t u_tc) / u_cc
-#pragma unroll
-        for (int c = 0; c < NB; ++c) v[c] = (c < kb) ? M[(k0 + c) * n + idx] : make_float2(0.f, 0.f);
-#pragma unroll
-        for (int c = 0; c < NB; ++c) {
-            if (c < kb) {
-                float2 acc = v[c];
-#pragma unroll
-                for (int t = 0; t < c; ++t) acc = cfms(acc, v[t], s[t][c]);
-                v[c] = cdivf(acc, s[c][c]);
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < NB; ++c)
-            if (c < kb) M[(k0 + c) * n + idx] = v[c];
-    } else {
-        // column idx: L11 y = a (unit lower)  ->  y_r = a_r - sum_{t<r} l_rt y_t
-        const float2* col = M + idx * n + k0;
-#pragma unroll
-        for (int r = 0; r < NB; ++r) v[r] = (r < kb) ? col[r] : make_float2(0.f, 0.f);
-#pragma unroll
-        for (int r = 0; r < NB; ++r) {
-            if (r < kb) {
-                float2 acc = v[r];
-#pragma unroll
-                for (int t = 0; t < r; ++t) acc = cfms(acc, s[r][t], v[t]);
-                v[r] = acc;
-            }
-        }
-        float2* colw = M + idx * n + k0;
-#pragma unroll
-        for (int r = 0; r < NB; ++r)
-            if (r < kb) colw[r] = v[r];
-    }
-}
 
 // A22 -= L21 U12 over rows/cols [k0+NB, n); 64 x 64 tile per CTA, 256 threads,
 // 4 x 4 complex outputs per thread.
@@ -307,12 +173,13 @@ cudaError_t launch_lu_f32(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int
 {
     const int64_t dstride = lu_dinv_stride(n);
     for (int64_t k0 = 0; k0 < n; k0 += NB) {
-        k_lu_diag<<<nbatch, 256, 0, ctx->stream>>>(A, n, stride, k0, Dinv, dstride, bad);
+        k_lu_diag<NB><<<nbatch, 256, lu_diag_smem_bytes<NB>(), ctx->stream>>>(A, n, stride, k0, Dinv,
+                                                                               dstride, bad);
         ctx->launches += 1;
         const int64_t rest = n - k0 - NB;
         if (rest > 0) {
             dim3 g1((unsigned)((rest + 127) / 128), 2, (unsigned)nbatch);
-            k_lu_trsm<<<g1, 128, 0, ctx->stream>>>(A, n, stride, k0);
+            k_lu_trsm<NB><<<g1, 128, 0, ctx->stream>>>(A, n, stride, k0);
             dim3 g2((unsigned)((rest + 63) / 64), (unsigned)((rest + 63) / 64), (unsigned)nbatch);
             k_lu_update<<<g2, 256, 0, ctx->stream>>>(A, n, stride, k0);
             ctx->launches += 2;

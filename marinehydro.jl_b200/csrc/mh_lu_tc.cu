@@ -1,0 +1,392 @@
+// Batched pivot-free complex LU with the trailing update on the 5th-generation
+// tensor cores (tcgen05), and block-parallel triangular solves.
+//
+// Block size NB = 64 complex.  Per step k0:
+//   k_lu_diag<64>      factor the 64 x 64 diagonal block (shared memory),
+//                      store inv(L11), inv(U11);
+//   k_lu_trsm<64>      L21 = A21 U11^-1, U12 = L11^-1 A12 (FP32, per row/column);
+//   k_lu_update_tc     A22 -= L21 U12.
+//
+// The trailing update is one real GEMM per 128 x 128 complex tile of A22:
+// with A = [Re L21 | Im L21] (128 x 128) and
+//   B = [ Re U12^T  -Im U12^T ]   (rows 0..127: real part of the product)
+//       [ Im U12^T   Re U12^T ]   (rows 128..255: imaginary part)
+// D = A B^T (128 x 256) holds Re(L21 U12) in columns 0..127 and Im in
+// 128..255.  Operands are rounded to FP16 and staged by the threads in shared
+// memory in the UMMA K-major no-swizzle layout (8-row x 16-byte core
+// matrices; SBO = 128 B between 8-row groups, LBO = one K chunk of 8
+// elements); one thread issues eight tcgen05.mma.kind::f16 (M=128, N=256,
+// K=16) into a 256-column FP32 accumulator in tensor memory and commits
+// them to an mbarrier; the four warps read their 32 TMEM lanes back with
+// tcgen05.ld and subtract from A22 in FP32.  Every wait is bounded: a
+// timeout marks the matrix bad (the host then re-solves it with the FP64
+// pivoted LU) instead of spinning.
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "mh_internal.h"
+#include "mh_lu_kernels.cuh"
+
+namespace mh {
+namespace {
+
+constexpr int TC_NB = 64;                 // complex K of the trailing update
+constexpr int TC_TM = 128;                // C rows per CTA (UMMA M)
+constexpr int TC_TN = 128;                // C complex columns per CTA (UMMA N = 256)
+constexpr int TC_KR = 2 * TC_NB;          // real K = 128 (8 UMMA K-steps of 16)
+constexpr uint32_t kSmemA = TC_TM * TC_KR * 2;          // 32 KiB of FP16
+constexpr uint32_t kSmemB = 2 * TC_TN * TC_KR * 2;      // 64 KiB of FP16
+constexpr uint32_t kTmemCols = 2 * TC_TN;               // 256 FP32 columns
+constexpr uint32_t kLboA = (TC_TM / 8) * 128;           // bytes between K chunks of A
+constexpr uint32_t kLboB = (2 * TC_TN / 8) * 128;       // bytes between K chunks of B
+constexpr uint32_t kSbo = 128;                          // bytes between 8-row groups
+// Instruction descriptor: F32 accumulator (bits 4-5 = 1), A and B F16
+// (bits 7-9, 10-12 = 0), both K-major (bits 15, 16 = 0), N >> 3 at bit 17,
+// M >> 4 at bit 24.
+constexpr uint32_t kIdesc = (1u << 4) | ((uint32_t)(2 * TC_TN) >> 3 << 17) | ((uint32_t)TC_TM >> 4 << 24);
+constexpr int kWaitPolls = 4096;          // bounded mbarrier polls ...
+constexpr uint32_t kWaitHintNs = 1000;    // ... each suspending at most ~1 us
+
+// Dynamic shared memory of k_lu_update_tc: the two operand tiles (96 KiB), so
+// two CTAs share an SM and its 512 TMEM columns.
+constexpr uint32_t kTcSmemBytes = kSmemA + kSmemB;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Shared-memory matrix descriptor, no swizzle, Blackwell version field = 1.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Byte offset of (row, K chunk kc) in a K-major no-swizzle tile with `rows` rows.
+__device__ __forceinline__ uint32_t core_off(int row, int kc, int rows)
+{
+    return (uint32_t)((kc * (rows / 8) + row / 8) * 128 + (row % 8) * 16);
+}
+
+__device__ __forceinline__ uint32_t pack_h2(float a, float b)
+{
+    __half2 h = __floats2half2_rn(a, b);
+    return *reinterpret_cast<uint32_t*>(&h);
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t phase)
+{
+    for (int it = 0; it < kWaitPolls; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(addr), "r"(phase), "r"(kWaitHintNs)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+          "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+          "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+}
+
+__global__ void __launch_bounds__(128, 2)
+k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0, int* __restrict__ bad)
+{
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    __shared__ uint64_t mbar;
+    __shared__ uint32_t tmem_slot;
+    unsigned char* sA = tc_smem;
+    unsigned char* sB = tc_smem + kSmemA;
+    const int b = blockIdx.z;
+    float2* M = Ab + (int64_t)b * stride;
+    const int64_t base = k0 + TC_NB;
+    const int64_t r0 = base + (int64_t)blockIdx.x * TC_TM;
+    const int64_t c0 = base + (int64_t)blockIdx.y * TC_TN;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(&tmem_slot)), "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&mbar)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+
+    // A tile: row tid of L21 -> 8 K chunks of Re, 8 of Im
+    {
+        const int64_t gi = r0 + tid;
+        const bool ok = gi < n;
+#pragma unroll 1
+        for (int c = 0; c < 8; ++c) {
+            float2 v[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                v[q] = ok ? M[(k0 + 8 * c + q) * n + gi] : make_float2(0.f, 0.f);
+            uint4 re = make_uint4(pack_h2(v[0].x, v[1].x), pack_h2(v[2].x, v[3].x),
+                                  pack_h2(v[4].x, v[5].x), pack_h2(v[6].x, v[7].x));
+            uint4 im = make_uint4(pack_h2(v[0].y, v[1].y), pack_h2(v[2].y, v[3].y),
+                                  pack_h2(v[4].y, v[5].y), pack_h2(v[6].y, v[7].y));
+            *reinterpret_cast<uint4*>(sA + core_off(tid, c, TC_TM)) = re;
+            *reinterpret_cast<uint4*>(sA + core_off(tid, 8 + c, TC_TM)) = im;
+        }
+    }
+    // B tile: column tid of U12 -> rows tid (real part) and 128 + tid (imaginary part)
+    {
+        const int64_t gj = c0 + tid;
+        const bool ok = gj < n;
+#pragma unroll 1
+        for (int c = 0; c < 8; ++c) {
+            float2 u[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                u[q] = ok ? M[gj * n + k0 + 8 * c + q] : make_float2(0.f, 0.f);
+            uint4 re = make_uint4(pack_h2(u[0].x, u[1].x), pack_h2(u[2].x, u[3].x),
+                                  pack_h2(u[4].x, u[5].x), pack_h2(u[6].x, u[7].x));
+            uint4 im = make_uint4(pack_h2(u[0].y, u[1].y), pack_h2(u[2].y, u[3].y),
+                                  pack_h2(u[4].y, u[5].y), pack_h2(u[6].y, u[7].y));
+            uint4 nim = make_uint4(pack_h2(-u[0].y, -u[1].y), pack_h2(-u[2].y, -u[3].y),
+                                   pack_h2(-u[4].y, -u[5].y), pack_h2(-u[6].y, -u[7].y));
+            *reinterpret_cast<uint4*>(sB + core_off(tid, c, 2 * TC_TN)) = re;
+            *reinterpret_cast<uint4*>(sB + core_off(tid, 8 + c, 2 * TC_TN)) = nim;
+            *reinterpret_cast<uint4*>(sB + core_off(TC_TN + tid, c, 2 * TC_TN)) = im;
+            *reinterpret_cast<uint4*>(sB + core_off(TC_TN + tid, 8 + c, 2 * TC_TN)) = re;
+        }
+    }
+    // make the generic-proxy shared stores visible to the tensor cores
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+    const uint32_t mbar_addr = smem_u32(&mbar);
+
+    if (tid == 0) {
+        const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+#pragma unroll
+        for (int s = 0; s < TC_KR / 16; ++s) {
+            const uint64_t da = umma_desc(a0 + 2 * s * kLboA, kLboA, kSbo);
+            const uint64_t db = umma_desc(b0 + 2 * s * kLboB, kLboB, kSbo);
+            const uint32_t acc = s > 0 ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+                :: "r"(tmem), "l"(da), "l"(db), "r"(kIdesc), "r"(acc),
+                   "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                     :: "r"(mbar_addr) : "memory");
+    }
+    // CTA-uniform: tcgen05.ld below is warp-collective and must not diverge
+    const bool done = __syncthreads_and(mbar_wait(mbar_addr, 0)) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (done) {
+        const int64_t gi = r0 + warp * 32 + lane;
+        const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+        for (int cc = 0; cc < TC_TN / 32; ++cc) {
+            uint32_t re[32], im[32];
+            tmem_ld32(lane_base + (uint32_t)(cc * 32), re);
+            tmem_ld32(lane_base + (uint32_t)(TC_TN + cc * 32), im);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (gi < n) {
+#pragma unroll 4
+                for (int q = 0; q < 32; ++q) {
+                    const int64_t gj = c0 + cc * 32 + q;
+                    if (gj < n) {
+                        float2 v = M[gj * n + gi];
+                        v.x -= __uint_as_float(re[q]);
+                        v.y -= __uint_as_float(im[q]);
+                        M[gj * n + gi] = v;
+                    }
+                }
+            }
+        }
+    } else {
+        if (lane == 0) atomicExch(bad + b, 2);
+        mbar_wait(mbar_addr, 0);  // bounded second wait for the MMAs still in flight
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kTmemCols));
+}
+
+// ---------------------------------------------------------------------------
+// block-parallel triangular solves, one launch per diagonal block
+// ---------------------------------------------------------------------------
+
+// Forward step of L y = x for diagonal block `blk`: y_blk = inv(L11) x_blk
+// (written to Y by CTA 0), then x_i -= L_i,blk y_blk for the rows below,
+// 128 rows per CTA.
+template <int NB>
+__global__ void __launch_bounds__(128)
+k_trsv_fwd(const float2* __restrict__ A, int64_t n, int64_t stride, const float2* __restrict__ Dinv,
+           int64_t dstride, float2* __restrict__ X, float2* __restrict__ Y, int64_t xstride, int nrhs,
+           int blk)
+{
+    __shared__ float2 ys[kMaxRhs * NB];
+    const int b = blockIdx.y;
+    const float2* M = A + (int64_t)b * stride;
+    const float2* Li = Dinv + (int64_t)b * dstride + (int64_t)blk * 2 * NB * NB;
+    float2* x = X + (int64_t)b * xstride;
+    float2* y = Y + (int64_t)b * xstride;
+    const int64_t k0 = (int64_t)blk * NB;
+    const int kb = (int)min((int64_t)NB, n - k0);
+    for (int t = threadIdx.x; t < NB * nrhs; t += blockDim.x) {
+        const int r = t % NB, q = t / NB;
+        float2 acc = make_float2(0.f, 0.f);
+        if (r < kb)
+            for (int c = 0; c <= r; ++c) {
+                const float2 l = Li[c * NB + r], v = x[(int64_t)q * n + k0 + c];
+                acc.x += l.x * v.x - l.y * v.y;
+                acc.y += l.x * v.y + l.y * v.x;
+            }
+        ys[q * NB + r] = acc;
+    }
+    __syncthreads();
+    if (blockIdx.x == 0)
+        for (int t = threadIdx.x; t < kb * nrhs; t += blockDim.x) {
+            const int r = t % kb, q = t / kb;
+            y[(int64_t)q * n + k0 + r] = ys[q * NB + r];
+        }
+    const int64_t i = k0 + kb + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int q = 0; q < nrhs; ++q) {
+        float2 acc = x[(int64_t)q * n + i];
+        for (int t = 0; t < kb; ++t) acc = cfms(acc, M[(k0 + t) * n + i], ys[q * NB + t]);
+        x[(int64_t)q * n + i] = acc;
+    }
+}
+
+// Backward step of U z = y for block `blk`: z_blk = inv(U11) y_blk (written
+// to Z by CTA 0), then y_i -= U_i,blk z_blk for the rows above.
+template <int NB>
+__global__ void __launch_bounds__(128)
+k_trsv_bwd(const float2* __restrict__ A, int64_t n, int64_t stride, const float2* __restrict__ Dinv,
+           int64_t dstride, float2* __restrict__ Y, float2* __restrict__ Z, int64_t xstride, int nrhs,
+           int blk)
+{
+    __shared__ float2 zs[kMaxRhs * NB];
+    const int b = blockIdx.y;
+    const float2* M = A + (int64_t)b * stride;
+    const float2* Ui = Dinv + (int64_t)b * dstride + (int64_t)blk * 2 * NB * NB + NB * NB;
+    float2* y = Y + (int64_t)b * xstride;
+    float2* z = Z + (int64_t)b * xstride;
+    const int64_t k0 = (int64_t)blk * NB;
+    const int kb = (int)min((int64_t)NB, n - k0);
+    for (int t = threadIdx.x; t < NB * nrhs; t += blockDim.x) {
+        const int r = t % NB, q = t / NB;
+        float2 acc = make_float2(0.f, 0.f);
+        if (r < kb)
+            for (int c = r; c < kb; ++c) {
+                const float2 u = Ui[c * NB + r], v = y[(int64_t)q * n + k0 + c];
+                acc.x += u.x * v.x - u.y * v.y;
+                acc.y += u.x * v.y + u.y * v.x;
+            }
+        zs[q * NB + r] = acc;
+    }
+    __syncthreads();
+    if (blockIdx.x == 0)
+        for (int t = threadIdx.x; t < kb * nrhs; t += blockDim.x) {
+            const int r = t % kb, q = t / kb;
+            z[(int64_t)q * n + k0 + r] = zs[q * NB + r];
+        }
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= k0) return;
+    for (int q = 0; q < nrhs; ++q) {
+        float2 acc = y[(int64_t)q * n + i];
+        for (int t = 0; t < kb; ++t) acc = cfms(acc, M[(k0 + t) * n + i], zs[q * NB + t]);
+        y[(int64_t)q * n + i] = acc;
+    }
+}
+
+unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
+
+}  // namespace
+
+int64_t lu_dinv_stride_tc(int64_t n) { return ((n + TC_NB - 1) / TC_NB) * 2 * TC_NB * TC_NB; }
+
+cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int nbatch, float2* Dinv,
+                         int* bad)
+{
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k_lu_diag<TC_NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)lu_diag_smem_bytes<TC_NB>())) != cudaSuccess)
+        return e;
+    if ((e = cudaFuncSetAttribute(k_lu_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kTcSmemBytes)) != cudaSuccess)
+        return e;
+    const int64_t dstride = lu_dinv_stride_tc(n);
+    for (int64_t k0 = 0; k0 < n; k0 += TC_NB) {
+        k_lu_diag<TC_NB><<<nbatch, 256, lu_diag_smem_bytes<TC_NB>(), ctx->stream>>>(A, n, stride, k0,
+                                                                                  Dinv, dstride, bad);
+        ctx->launches += 1;
+        const int64_t rest = n - k0 - TC_NB;
+        if (rest > 0) {
+            k_lu_trsm<TC_NB><<<dim3(cdiv(rest, 128), 2, (unsigned)nbatch), 128, 0, ctx->stream>>>(
+                A, n, stride, k0);
+            k_lu_update_tc<<<dim3(cdiv(rest, TC_TM), cdiv(rest, TC_TN), (unsigned)nbatch), 128,
+                             kTcSmemBytes, ctx->stream>>>(A, n, stride, k0, bad);
+            ctx->launches += 2;
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+namespace {
+template <int NB>
+cudaError_t solve_blocks(mh_ctx* ctx, const float2* A, int64_t n, int64_t stride, int nbatch,
+                         const float2* Dinv, int64_t dstride, float2* X, float2* T, int64_t xstride,
+                         int nrhs)
+{
+    if (nrhs < 1 || nrhs > kMaxRhs) return cudaErrorInvalidValue;
+    const int nblk = (int)((n + NB - 1) / NB);
+    for (int blk = 0; blk < nblk; ++blk) {
+        const int64_t below = n - (int64_t)(blk + 1) * NB;
+        dim3 g(below > 0 ? cdiv(below, 128) : 1u, (unsigned)nbatch);
+        k_trsv_fwd<NB><<<g, 128, 0, ctx->stream>>>(A, n, stride, Dinv, dstride, X, T, xstride, nrhs, blk);
+    }
+    for (int blk = nblk - 1; blk >= 0; --blk) {
+        const int64_t above = (int64_t)blk * NB;
+        dim3 g(above > 0 ? cdiv(above, 128) : 1u, (unsigned)nbatch);
+        k_trsv_bwd<NB><<<g, 128, 0, ctx->stream>>>(A, n, stride, Dinv, dstride, T, X, xstride, nrhs, blk);
+    }
+    ctx->launches += 2 * nblk;
+    return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_lu_solve_tc(mh_ctx* ctx, const float2* A, int64_t n, int64_t stride, int nbatch,
+                               const float2* Dinv, float2* X, float2* T, int64_t xstride, int nrhs)
+{
+    return solve_blocks<TC_NB>(ctx, A, n, stride, nbatch, Dinv, lu_dinv_stride_tc(n), X, T, xstride,
+                               nrhs);
+}
+
+cudaError_t launch_lu_solve_blocks32(mh_ctx* ctx, const float2* A, int64_t n, int64_t stride,
+                                     int nbatch, const float2* Dinv, float2* X, float2* T,
+                                     int64_t xstride, int nrhs)
+{
+    return solve_blocks<32>(ctx, A, n, stride, nbatch, Dinv, lu_dinv_stride(n), X, T, xstride, nrhs);
+}
+
+}  // namespace mh

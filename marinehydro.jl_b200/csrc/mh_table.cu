@@ -13,7 +13,8 @@ namespace {
 
 // B and C at the table nodes, from the FP64 adaptive quadrature.
 __global__ void k_table_nodes(const double* __restrict__ rr, const double* __restrict__ zz, int n,
-                              double* __restrict__ B, double* __restrict__ C)
+                              double* __restrict__ B, double* __restrict__ C,
+                              double* __restrict__ E0, double* __restrict__ E1)
 {
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
@@ -25,6 +26,8 @@ __global__ void k_table_nodes(const double* __restrict__ rr, const double* __res
     double L = log(0.5 * (R + az));
     B[t] = o[0].re + 2.0 * e * J0 * L;
     C[t] = o[1].re - (2.0 * e * J1 * L - 2.0 * e * J0 * r / (R * (R + az)));
+    E0[t] = e * J0;
+    E1[t] = e * J1;
 }
 
 // Dimensionless (G, dG/dr, dG/dz) at arbitrary points.
@@ -98,41 +101,49 @@ int ensure_delh_table(mh_ctx* ctx)
                 }
         }
     const int n = (int)r.size();
-    double *d_r = nullptr, *d_z = nullptr, *d_B = nullptr, *d_C = nullptr, *d_tab = nullptr;
+    double *d_r = nullptr, *d_z = nullptr, *d_B = nullptr, *d_C = nullptr, *d_E0 = nullptr,
+           *d_E1 = nullptr, *d_tab = nullptr;
     auto cleanup = [&]() {
         cudaFree(d_r);
         cudaFree(d_z);
         cudaFree(d_B);
         cudaFree(d_C);
+        cudaFree(d_E0);
+        cudaFree(d_E1);
     };
     size_t bytes = sizeof(double) * (size_t)n;
     if (cudaMalloc(&d_r, bytes) != cudaSuccess || cudaMalloc(&d_z, bytes) != cudaSuccess ||
         cudaMalloc(&d_B, bytes) != cudaSuccess || cudaMalloc(&d_C, bytes) != cudaSuccess ||
+        cudaMalloc(&d_E0, bytes) != cudaSuccess || cudaMalloc(&d_E1, bytes) != cudaSuccess ||
         cudaMalloc(&d_tab, sizeof(double) * kTabWords) != cudaSuccess) {
         cudaGetLastError();
         cleanup();
         cudaFree(d_tab);
         return set_err(ctx, MH_ERR_OOM, "allocation of the Delhommeau table failed");
     }
-    std::vector<double> hB(n), hC(n), tab(kTabWords);
+    std::vector<double> hB(n), hC(n), hE0(n), hE1(n), tab(kTabWords);
     cudaError_t e = cudaMemcpyAsync(d_r, r.data(), bytes, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_z, z.data(), bytes, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) {
-        k_table_nodes<<<(n + 127) / 128, 128, 0, ctx->stream>>>(d_r, d_z, n, d_B, d_C);
+        k_table_nodes<<<(n + 127) / 128, 128, 0, ctx->stream>>>(d_r, d_z, n, d_B, d_C, d_E0, d_E1);
         ctx->launches += 1;
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(hB.data(), d_B, bytes, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(hC.data(), d_C, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hE0.data(), d_E0, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hE1.data(), d_E1, bytes, cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) {
         cleanup();
         cudaFree(d_tab);
         return set_err(ctx, MH_ERR_CUDA, "Delhommeau table nodes: %s", cudaGetErrorString(e));
     }
-    // polar block
+    // polar block: B, C, E0, E1
     cheb_coeffs(kTabNP, hB.data(), tab.data());
     cheb_coeffs(kTabNP, hC.data(), tab.data() + kTabNP * kTabNP);
+    cheb_coeffs(kTabNP, hE0.data(), tab.data() + 2 * kTabNP * kTabNP);
+    cheb_coeffs(kTabNP, hE1.data(), tab.data() + 3 * kTabNP * kTabNP);
     // cells
     const int np = kTabNP * kTabNP, nc = kTabNC * kTabNC;
     for (int c = 0; c < kTabNCell * kTabNCell; ++c) {

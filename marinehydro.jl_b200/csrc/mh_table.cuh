@@ -16,7 +16,10 @@
 // = e^z J0(r) of the log-moments of e^zeta E1(zeta)).  B and C are smooth
 // in polar coordinates (R, alpha = atan2(r, |z|)) near the origin and in
 // (r, |z|) away from it, so they are tabulated as 2-D Chebyshev series:
-//   - one polar patch, R in [0, 1.5), alpha in [0, pi/2], degree 20 x 20;
+//   - one polar patch, R in [0, 1.5), alpha in [0, pi/2], degree 20 x 20,
+//     holding B, C and also E0 = e^z J0(r), E1 = e^z J1(r) (smooth; used by
+//     the frequency-batched evaluation, which contracts the alpha direction
+//     once per panel pair and then needs only 1-D series in R per frequency);
 //   - Cartesian cells of 0.5 x 0.5 over r, |z| in [0, 16), degree 12 x 12
 //     (every cell touching R < 1 lies inside the polar patch).
 // Points outside the table fall back to the adaptive quadrature.  The node
@@ -33,37 +36,40 @@ constexpr double kTabRPolar = 1.5;  // polar patch radius
 constexpr double kTabH = 0.5;       // Cartesian cell size
 constexpr int kTabNCell = 32;       // cells per direction -> extent 16
 constexpr double kTabExtent = kTabH * kTabNCell;
-constexpr int kTabPolarWords = 2 * kTabNP * kTabNP;            // B then C
+constexpr int kTabPolarWords = 4 * kTabNP * kTabNP;            // B, C, E0, E1
 constexpr int kTabCellWords = 2 * kTabNC * kTabNC;             // B then C
 constexpr int kTabWords = kTabPolarWords + kTabNCell * kTabNCell * kTabCellWords;
 
-// sum_i sum_j c[i*N + j] T_i(u) T_j(v)
+// sum_i sum_j c[i*N + j] T_i(u) T_j(v) by nested Clenshaw recurrences (rows
+// in v, then the row sums in u); a few registers instead of 2N basis values.
 template <int N>
 __device__ __forceinline__ double cheb2d(const double* __restrict__ c, double u, double v)
 {
-    double tu[N], tv[N];
-    tu[0] = 1.0;
-    tu[1] = u;
-    tv[0] = 1.0;
-    tv[1] = v;
+    double a1 = 0.0, a2 = 0.0, s0 = 0.0;
+#pragma unroll 1
+    for (int i = N - 1; i >= 0; --i) {
+        const double* ci = c + i * N;
+        double b1 = 0.0, b2 = 0.0;
 #pragma unroll
-    for (int j = 2; j < N; ++j) {
-        tu[j] = 2.0 * u * tu[j - 1] - tu[j - 2];
-        tv[j] = 2.0 * v * tv[j - 1] - tv[j - 2];
+        for (int j = N - 1; j >= 1; --j) {
+            const double t = fma(2.0 * v, b1, __ldg(ci + j) - b2);
+            b2 = b1;
+            b1 = t;
+        }
+        const double si = fma(v, b1, __ldg(ci) - b2);
+        if (i >= 1) {
+            const double t = fma(2.0 * u, a1, si - a2);
+            a2 = a1;
+            a1 = t;
+        } else {
+            s0 = fma(u, a1, si - a2);
+        }
     }
-    double s = 0.0;
-#pragma unroll
-    for (int i = 0; i < N; ++i) {
-        double row = 0.0;
-#pragma unroll
-        for (int j = 0; j < N; ++j) row = fma(__ldg(c + i * N + j), tv[j], row);
-        s = fma(tu[i], row, s);
-    }
-    return s;
+    return s0;
 }
 
 // (G, dG/dr, dG/dz) from the table (falls back to quadrature outside it).
-__device__ __forceinline__ void delh_dimless_table(const double* __restrict__ tab, double r, double z,
+__device__ __noinline__ static void delh_dimless_table(const double* __restrict__ tab, double r, double z,
                                                    cplx out[3])
 {
     const double az = -z;

@@ -110,3 +110,22 @@ def test_batch_argument_errors(mh, gpu, body):
         mh.hydro_batch(body.mesh, [1.0], dofs, precision="mixed",
                        green_functions=(mh.Rankine(), mh.GFWu(), mh.ExactGuevelDelhommeau()),
                        ctx=gpu)
+
+
+@pytest.mark.parametrize("direct", [True, False])
+def test_frequency_batched_delhommeau(mh, oracle, gpu, direct):
+    """Chunks of >= 6 frequencies take the frequency-batched Delhommeau pass
+    (alpha contraction once per pair); across [0.3, 4.0] rad/s pairs move from
+    the polar patch into the Cartesian cells, so both branches run."""
+    mesh = mh.mesh_hemisphere(1.3, (0, 0, 0), (10, 14))
+    body = mh.FloatingBody.rigid(mesh, ["Heave", "Surge"])
+    dofs = list(body.dofs.values())
+    om = np.linspace(0.3, 4.0, 9)
+    gfs = (mh.Rankine(), mh.RankineReflected(), mh.ExactGuevelDelhommeau())
+    A, B, Fd, _, info = mh.hydro_batch(mesh, om, dofs, [0.3], green_functions=gfs, direct=direct,
+                                       precision="mixed", tol=1e-12, ctx=gpu)
+    Ao, Bo, Fdo, _ = oracle.hydro_coefficients(mesh, om, dofs, [0.3], gf_mask=DELH, direct=direct)
+    assert _rel(A, Ao) < 1e-9 and _rel(B, Bo) < 1e-9 and _rel(Fd, Fdo) < 1e-9
+    A64, B64, _, _, _ = mh.hydro_batch(mesh, om, dofs, [0.3], green_functions=gfs, direct=direct,
+                                       precision="fp64", ctx=gpu)
+    assert _rel(A, A64) < 1e-10 and _rel(B, B64) < 1e-10

@@ -1,0 +1,94 @@
+"""The low-precision LU of the mixed path (GPU).
+
+Backends: FP32 on the CUDA cores (block 32) and the block-64 LU whose
+trailing update runs on tcgen05 with FP16 operands and FP32 accumulation.
+Checked by reconstruction, ||L U - A||_max / ||A||_max: <= 2e-6 for FP32,
+<= 4e-3 for the FP16 tensor-core update (operands rounded to 11 significant
+bits), on sizes that are not multiples of the tiles; and end to end through
+the batch driver, whose FP64 refinement must still reach the FP64 result.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _bem_like(rng, nb, n):
+    """Matrices shaped like the BEM D: 1/2 on the diagonal plus a smooth,
+    decaying complex kernel (well conditioned, no pivoting needed)."""
+    x = rng.uniform(-1, 1, (nb, n, 3))
+    d = np.linalg.norm(x[:, :, None, :] - x[:, None, :, :], axis=-1) + 0.3
+    A = (0.8 / n) * (np.exp(-d) * (np.cos(2 * d) + 1j * np.sin(3 * d))) / d
+    A += 0.5 * np.eye(n)[None]
+    return A
+
+
+def _reconstruct(LU):
+    n = LU.shape[-1]
+    L = np.tril(LU, -1) + np.eye(n)
+    U = np.triu(LU)
+    return L @ U
+
+
+@pytest.mark.parametrize("backend,tol", [("simt", 2e-6), ("tcgen05", 4e-3)])
+@pytest.mark.parametrize("n", [64, 200, 320])
+def test_lowp_lu_reconstructs(mh, gpu, backend, tol, n):
+    rng = np.random.default_rng(n)
+    A = _bem_like(rng, 3, n)
+    LU, bad = gpu.lu_factor_lowp(A, backend)
+    assert not bad.any()
+    for b in range(A.shape[0]):
+        R = _reconstruct(LU[b].astype(np.complex128))
+        err = np.max(np.abs(R - A[b])) / np.max(np.abs(A[b]))
+        assert err <= tol, (backend, n, b, err)
+
+
+def test_tcgen05_factors_track_fp32(mh, gpu):
+    rng = np.random.default_rng(5)
+    A = _bem_like(rng, 2, 300)
+    LU32, _ = gpu.lu_factor_lowp(A, "simt")
+    LU16, _ = gpu.lu_factor_lowp(A, "tcgen05")
+    err = np.max(np.abs(LU16 - LU32)) / np.max(np.abs(LU32))
+    assert err < 4e-3
+
+
+def test_singular_block_flagged(mh, gpu):
+    n = 96
+    A = np.eye(n, dtype=np.complex128)[None].repeat(2, axis=0)
+    A[1, 70, 70] = 0.0
+    for backend in ("simt", "tcgen05"):
+        _, bad = gpu.lu_factor_lowp(A, backend)
+        assert bad[0] == 0 and bad[1] != 0
+
+
+@pytest.mark.parametrize("direct", [True, False])
+def test_batch_with_tensor_core_lu(mh, oracle, gpu, direct):
+    """tcgen05 is the default backend; set explicitly to be independent of order."""
+    mesh = mh.mesh_hemisphere(1.0, (0, 0, 0), (14, 20))
+    body = mh.FloatingBody.rigid(mesh, ["Heave", "Surge"])
+    dofs = list(body.dofs.values())
+    om = [0.5, 1.2, 2.5]
+    gpu.set_lu_backend("tcgen05")
+    A, B, Fd, _, info = mh.hydro_batch(mesh, om, dofs, [0.0], direct=direct, precision="mixed",
+                                       tol=1e-12, ctx=gpu)
+    Ao, Bo, Fdo, _ = oracle.hydro_coefficients(mesh, om, dofs, [0.0], direct=direct)
+    for got, ref in ((A, Ao), (B, Bo), (Fd, Fdo)):
+        assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) < 1e-9
+    assert info.n_fallback == 0
+    assert info.refine_iterations <= 12
+
+
+def test_batch_with_fp32_lu(mh, oracle, gpu):
+    mesh = mh.mesh_hemisphere(1.0, (0, 0, 0), (12, 16))
+    dofs = [mh.translational_dofs(mesh, "Heave")]
+    gpu.set_lu_backend("simt")
+    try:
+        A, B, _, _, info = mh.hydro_batch(mesh, [0.7, 1.9], dofs, precision="mixed", tol=1e-12,
+                                          ctx=gpu)
+    finally:
+        gpu.set_lu_backend("tcgen05")
+    Ao, Bo, _, _ = oracle.hydro_coefficients(mesh, [0.7, 1.9], dofs)
+    assert np.max(np.abs(A - Ao)) / np.max(np.abs(Ao)) < 1e-9
+    assert info.refine_iterations <= 4
