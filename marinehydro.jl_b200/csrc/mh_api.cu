@@ -394,8 +394,12 @@ int mh_lu_factor_lowp(mh_ctx* ctx, int backend, int64_t n, int64_t nbatch, const
                                      ctx->stream));
     MH_CUDA_TRY(ctx, mh::launch_to_f32(ctx, d64, lo, (int64_t)cnt));
     MH_CUDA_TRY(ctx, cudaMemsetAsync(bad, 0, sizeof(int) * (size_t)nbatch, ctx->stream));
-    if (backend == MH_LU_TCGEN05_F16)
-        MH_CUDA_TRY(ctx, mh::launch_lu_tc(ctx, lo, n, (int64_t)nn, (int)nbatch, dinv, bad));
+    if (backend == MH_LU_TCGEN05_F16) {
+        auto* panels = (unsigned char*)ws_get(ctx, WS_PANEL,
+                                              (size_t)mh::lu_panel_bytes_tc(n) * (size_t)nbatch);
+        if (!panels) return MH_ERR_OOM;
+        MH_CUDA_TRY(ctx, mh::launch_lu_tc(ctx, lo, n, (int64_t)nn, (int)nbatch, dinv, panels, bad));
+    }
     else
         MH_CUDA_TRY(ctx, mh::launch_lu_f32(ctx, lo, n, (int64_t)nn, (int)nbatch, dinv, bad));
     MH_CUDA_TRY(ctx, cudaMemcpyAsync(LU_host, lo, sizeof(float2) * cnt, cudaMemcpyDeviceToHost,

@@ -560,7 +560,11 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
     // FP32 LU of every D (or K)
     MH_CUDA_TRY(ctx, cudaMemsetAsync(d_bad, 0, sizeof(int) * nb, ctx->stream));
     phase_begin(ctx, PH_LU);
-    if (tc) MH_CUDA_TRY(ctx, launch_lu_tc(ctx, Dlo, n, nn, nb, Dinv, d_bad));
+    if (tc) {
+        auto* panels = (unsigned char*)ws_get(ctx, WS_PANEL, (size_t)lu_panel_bytes_tc(n) * nb);
+        if (!panels) return MH_ERR_OOM;
+        MH_CUDA_TRY(ctx, launch_lu_tc(ctx, Dlo, n, nn, nb, Dinv, panels, d_bad));
+    }
     else MH_CUDA_TRY(ctx, launch_lu_f32(ctx, Dlo, n, nn, nb, Dinv, d_bad));
     phase_end(ctx, PH_LU);
     phase_begin(ctx, PH_REFINE);

@@ -29,7 +29,7 @@ struct mh_mesh {
 // Workspace slots of a context; each is a grow-only device buffer.
 enum WsSlot : int {
     WS_S = 0, WS_D, WS_RHS, WS_PHI, WS_TMP, WS_PIV, WS_INFO, WS_LWORK,
-    WS_DOF, WS_OUT, WS_LO, WS_DINV, WS_TMP32, WS_MISC, WS_SR, WS_TMP32B, WS_NSLOTS
+    WS_DOF, WS_OUT, WS_LO, WS_DINV, WS_TMP32, WS_MISC, WS_SR, WS_TMP32B, WS_PANEL, WS_NSLOTS
 };
 
 // Largest number of right-hand sides (radiating dofs + headings) per frequency.
@@ -99,8 +99,10 @@ cudaError_t launch_lu_solve_f32(mh_ctx* ctx, const float2* A, int64_t n, int64_t
 
 // ---- tensor-core LU (mh_lu_tc.cu), block size 64 ----
 int64_t lu_dinv_stride_tc(int64_t n);
+// Bytes of packed FP16 operand panels per matrix (scratch of launch_lu_tc).
+int64_t lu_panel_bytes_tc(int64_t n);
 cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int nbatch, float2* Dinv,
-                         int* bad);
+                         unsigned char* panels, int* bad);
 // Block-parallel (LU)^-1 X in place; T: scratch of the same size as X.
 cudaError_t launch_lu_solve_tc(mh_ctx* ctx, const float2* A, int64_t n, int64_t stride, int nbatch,
                                const float2* Dinv, float2* X, float2* T, int64_t xstride, int nrhs);

@@ -31,8 +31,8 @@ __device__ __forceinline__ float2 cdivf(float2 a, float2 b)
 // Factor the diagonal block [k0, k0+kb) of every matrix in place, and store
 // inv(L11) (unit lower) and inv(U11) in Dinv (per matrix: n/NB blocks of
 // 2 x NB x NB, column-major) for the triangular solves.
-template <int NB>
-__global__ void __launch_bounds__(256)
+template <int NB, int THREADS = 256>
+__global__ void __launch_bounds__(THREADS)
 k_lu_diag(float2* __restrict__ A, int64_t n, int64_t stride, int64_t k0, float2* __restrict__ Dinv,
           int64_t dstride, int* __restrict__ bad)
 {

@@ -4,8 +4,12 @@
 // Block size NB = 64 complex.  Per step k0:
 //   k_lu_diag<64>      factor the 64 x 64 diagonal block (shared memory),
 //                      store inv(L11), inv(U11);
-//   k_lu_trsm<64>      L21 = A21 U11^-1, U12 = L11^-1 A12 (FP32, per row/column);
-//   k_lu_update_tc     A22 -= L21 U12.
+//   k_lu_trsm_tc       L21 = A21 inv(U11) and U12^T = A12^T inv(L11)^T as
+//                      tcgen05 GEMMs (M=128, N=128, K=128); writes the FP32
+//                      factors into the matrix and the FP16 operand panels of
+//                      the update, pre-packed as their shared-memory images;
+//   k_lu_update_tc     A22 -= L21 U12: the two packed panels arrive by
+//                      cp.async.bulk (no register staging), eight MMAs.
 //
 // The trailing update is one real GEMM per 128 x 128 complex tile of A22:
 // with A = [Re L21 | Im L21] (128 x 128) and
@@ -44,6 +48,10 @@ constexpr uint32_t kSbo = 128;                          // bytes between 8-row g
 // (bits 7-9, 10-12 = 0), both K-major (bits 15, 16 = 0), N >> 3 at bit 17,
 // M >> 4 at bit 24.
 constexpr uint32_t kIdesc = (1u << 4) | ((uint32_t)(2 * TC_TN) >> 3 << 17) | ((uint32_t)TC_TM >> 4 << 24);
+constexpr uint32_t kIdescN128 = (1u << 4) | (128u >> 3 << 17) | ((uint32_t)TC_TM >> 4 << 24);
+constexpr uint32_t kLboB128 = (128 / 8) * 128;          // B of the TRSM GEMM: 128 rows
+constexpr uint32_t kPanelL = kSmemA;                    // packed L21 tile (A image), bytes
+constexpr uint32_t kPanelU = kSmemB;                    // packed U12 tile (B image), bytes
 constexpr int kWaitPolls = 4096;          // bounded mbarrier polls ...
 constexpr uint32_t kWaitHintNs = 1000;    // ... each suspending at most ~1 us
 
@@ -105,11 +113,179 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
         : "r"(taddr));
 }
 
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols)
+{
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(smem_u32(slot)), "r"(ncols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(taddr), "r"(ncols));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Eight K=16 MMAs over a K=128 (real) operand pair, then commit to `bar`.
+__device__ __forceinline__ void mma_k128(uint32_t tmem, uint32_t a0, uint32_t lbo_a, uint32_t b0,
+                                        uint32_t lbo_b, uint32_t idesc, uint32_t bar)
+{
+#pragma unroll
+    for (int s = 0; s < TC_KR / 16; ++s) {
+        const uint64_t da = umma_desc(a0 + 2 * s * lbo_a, lbo_a, kSbo);
+        const uint64_t db = umma_desc(b0 + 2 * s * lbo_b, lbo_b, kSbo);
+        const uint32_t acc = s > 0 ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+            :: "r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :: "r"(bar) : "memory");
+}
+
+__device__ __forceinline__ uint4 pack8(const float2* v, bool imag, float sign)
+{
+    if (imag)
+        return make_uint4(pack_h2(sign * v[0].y, sign * v[1].y), pack_h2(sign * v[2].y, sign * v[3].y),
+                          pack_h2(sign * v[4].y, sign * v[5].y), pack_h2(sign * v[6].y, sign * v[7].y));
+    return make_uint4(pack_h2(sign * v[0].x, sign * v[1].x), pack_h2(sign * v[2].x, sign * v[3].x),
+                      pack_h2(sign * v[4].x, sign * v[5].x), pack_h2(sign * v[6].x, sign * v[7].x));
+}
+
+// Panel TRSMs of step k0 on the tensor cores.  blockIdx.x < ntile: a 128-row
+// tile of L21 = A21 inv(U11); otherwise a 128-column tile of U12 = inv(L11)
+// A12, computed as U12^T = A12^T inv(L11)^T.  blockIdx.y = matrix.  Writes the
+// FP32 factors back and the packed FP16 panels Lp (A image of the update) and
+// Up (B image: rows j = [Re U12(:, j) | -Im], rows 128 + j = [Im | Re]).
 __global__ void __launch_bounds__(128, 2)
-k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0, int* __restrict__ bad)
+k_lu_trsm_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
+             const float2* __restrict__ Dinv, int64_t dstride, unsigned char* __restrict__ Lp,
+             unsigned char* __restrict__ Up, int64_t pstride, int ntile, int* __restrict__ bad)
 {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
     __shared__ uint64_t mbar;
+    __shared__ uint32_t tmem_slot;
+    unsigned char* sA = tc_smem;             // 128 x 128 FP16 (32 KiB)
+    unsigned char* sB = tc_smem + kSmemA;    // 128 x 128 FP16 (32 KiB)
+    const int b = blockIdx.y;
+    float2* M = Ab + (int64_t)b * stride;
+    const int64_t blk = k0 / TC_NB;
+    const float2* Li = Dinv + (int64_t)b * dstride + blk * 2 * TC_NB * TC_NB;  // column-major
+    const float2* Ui = Li + TC_NB * TC_NB;
+    const bool lower = (int)blockIdx.x < ntile;
+    const int tile = lower ? blockIdx.x : blockIdx.x - ntile;
+    const int64_t base = k0 + TC_NB;
+    const int64_t g = base + (int64_t)tile * TC_TM + threadIdx.x;  // row of L21 or column of U12
+    const bool ok = g < n;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (warp == 0) tmem_alloc(&tmem_slot, 128);
+    if (tid == 0) mbar_init(&mbar);
+    // A operand: row tid = A21(g, :) or A12(:, g)^T, 64 complex -> Re chunks 0..7, Im 8..15
+#pragma unroll 1
+    for (int c = 0; c < 8; ++c) {
+        float2 v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int64_t t = k0 + 8 * c + q;
+            v[q] = !ok ? make_float2(0.f, 0.f) : (lower ? M[t * n + g] : M[g * n + t]);
+        }
+        *reinterpret_cast<uint4*>(sA + core_off(tid, c, TC_TM)) = pack8(v, false, 1.f);
+        *reinterpret_cast<uint4*>(sA + core_off(tid, 8 + c, TC_TM)) = pack8(v, true, 1.f);
+    }
+    // B operand (N = 128): rows r < 64 give the real part of the product,
+    // rows 64 + r the imaginary part.  Complex row r of B is column r of
+    // inv(U11) (L21) or row r of inv(L11) (U12).
+    {
+        const int r = tid & 63;
+        const bool im_row = tid >= 64;
+#pragma unroll 1
+        for (int c = 0; c < 8; ++c) {
+            float2 v[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int t = 8 * c + q;
+                v[q] = lower ? Ui[r * TC_NB + t] : Li[t * TC_NB + r];
+            }
+            // rows r: [Re | -Im], rows 64 + r: [Im | Re]
+            *reinterpret_cast<uint4*>(sB + core_off(tid, c, 128)) = pack8(v, im_row, 1.f);
+            *reinterpret_cast<uint4*>(sB + core_off(tid, 8 + c, 128)) =
+                im_row ? pack8(v, false, 1.f) : pack8(v, true, -1.f);
+        }
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+    const uint32_t bar = smem_u32(&mbar);
+    if (tid == 0) mma_k128(tmem, smem_u32(sA), kLboA, smem_u32(sB), kLboB128, kIdescN128, bar);
+    const bool done = __syncthreads_and(mbar_wait(bar, 0)) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (done) {
+        const int row = warp * 32 + lane;  // TMEM lane = A row = tid of the loader above
+        const int64_t gg = base + (int64_t)tile * TC_TM + row;
+        const bool okr = gg < n;
+        const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+        unsigned char* panel = lower ? Lp + (int64_t)b * pstride + (int64_t)tile * kPanelL
+                                     : Up + (int64_t)b * pstride + (int64_t)tile * kPanelU;
+#pragma unroll 1
+        for (int half = 0; half < 2; ++half) {
+            uint32_t re[32], im[32];
+            tmem_ld32(lane_base + (uint32_t)(half * 32), re);
+            tmem_ld32(lane_base + (uint32_t)(64 + half * 32), im);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            float2 v[32];
+#pragma unroll
+            for (int q = 0; q < 32; ++q)
+                v[q] = okr ? make_float2(__uint_as_float(re[q]), __uint_as_float(im[q]))
+                           : make_float2(0.f, 0.f);
+            if (okr) {
+#pragma unroll 8
+                for (int q = 0; q < 32; ++q) {
+                    const int64_t t = k0 + half * 32 + q;
+                    if (lower) M[t * n + gg] = v[q];
+                    else M[gg * n + t] = v[q];
+                }
+            }
+#pragma unroll
+            for (int c4 = 0; c4 < 4; ++c4) {
+                const int c = half * 4 + c4;
+                const float2* w8 = v + 8 * c4;
+                if (lower) {
+                    *reinterpret_cast<uint4*>(panel + core_off(row, c, TC_TM)) = pack8(w8, false, 1.f);
+                    *reinterpret_cast<uint4*>(panel + core_off(row, 8 + c, TC_TM)) = pack8(w8, true, 1.f);
+                } else {
+                    *reinterpret_cast<uint4*>(panel + core_off(row, c, 2 * TC_TN)) = pack8(w8, false, 1.f);
+                    *reinterpret_cast<uint4*>(panel + core_off(row, 8 + c, 2 * TC_TN)) = pack8(w8, true, -1.f);
+                    *reinterpret_cast<uint4*>(panel + core_off(TC_TN + row, c, 2 * TC_TN)) = pack8(w8, true, 1.f);
+                    *reinterpret_cast<uint4*>(panel + core_off(TC_TN + row, 8 + c, 2 * TC_TN)) = pack8(w8, false, 1.f);
+                }
+            }
+        }
+    } else {
+        if (lane == 0) atomicExch(bad + b, 2);
+        mbar_wait(bar, 0);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, 128);
+}
+
+// A22 -= L21 U12 for one 128 x 128 complex tile; operands are the packed
+// panels of k_lu_trsm_tc, fetched by cp.async.bulk into shared memory.
+__global__ void __launch_bounds__(128, 2)
+k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
+               const unsigned char* __restrict__ Lp, const unsigned char* __restrict__ Up,
+               int64_t pstride, int* __restrict__ bad)
+{
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    __shared__ uint64_t mbar[2];
     __shared__ uint32_t tmem_slot;
     unsigned char* sA = tc_smem;
     unsigned char* sB = tc_smem + kSmemA;
@@ -119,83 +295,32 @@ k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0, i
     const int64_t r0 = base + (int64_t)blockIdx.x * TC_TM;
     const int64_t c0 = base + (int64_t)blockIdx.y * TC_TN;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                     :: "r"(smem_u32(&tmem_slot)), "r"(kTmemCols));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-    }
+    if (warp == 0) tmem_alloc(&tmem_slot, kTmemCols);
+    const uint32_t bar_ld = smem_u32(&mbar[0]), bar_mma = smem_u32(&mbar[1]);
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&mbar)), "r"(1));
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-
-    // A tile: row tid of L21 -> 8 K chunks of Re, 8 of Im
-    {
-        const int64_t gi = r0 + tid;
-        const bool ok = gi < n;
+        mbar_init(&mbar[0]);
+        mbar_init(&mbar[1]);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                     :: "r"(bar_ld), "r"(kPanelL + kPanelU) : "memory");
+        const unsigned char* srcA = Lp + (int64_t)b * pstride + (int64_t)blockIdx.x * kPanelL;
+        const unsigned char* srcB = Up + (int64_t)b * pstride + (int64_t)blockIdx.y * kPanelU;
+        constexpr uint32_t kChunk = 16384;
 #pragma unroll 1
-        for (int c = 0; c < 8; ++c) {
-            float2 v[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q)
-                v[q] = ok ? M[(k0 + 8 * c + q) * n + gi] : make_float2(0.f, 0.f);
-            uint4 re = make_uint4(pack_h2(v[0].x, v[1].x), pack_h2(v[2].x, v[3].x),
-                                  pack_h2(v[4].x, v[5].x), pack_h2(v[6].x, v[7].x));
-            uint4 im = make_uint4(pack_h2(v[0].y, v[1].y), pack_h2(v[2].y, v[3].y),
-                                  pack_h2(v[4].y, v[5].y), pack_h2(v[6].y, v[7].y));
-            *reinterpret_cast<uint4*>(sA + core_off(tid, c, TC_TM)) = re;
-            *reinterpret_cast<uint4*>(sA + core_off(tid, 8 + c, TC_TM)) = im;
-        }
-    }
-    // B tile: column tid of U12 -> rows tid (real part) and 128 + tid (imaginary part)
-    {
-        const int64_t gj = c0 + tid;
-        const bool ok = gj < n;
+        for (uint32_t off = 0; off < kPanelL; off += kChunk)
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                         :: "r"(smem_u32(sA + off)), "l"(srcA + off), "r"(kChunk), "r"(bar_ld) : "memory");
 #pragma unroll 1
-        for (int c = 0; c < 8; ++c) {
-            float2 u[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q)
-                u[q] = ok ? M[gj * n + k0 + 8 * c + q] : make_float2(0.f, 0.f);
-            uint4 re = make_uint4(pack_h2(u[0].x, u[1].x), pack_h2(u[2].x, u[3].x),
-                                  pack_h2(u[4].x, u[5].x), pack_h2(u[6].x, u[7].x));
-            uint4 im = make_uint4(pack_h2(u[0].y, u[1].y), pack_h2(u[2].y, u[3].y),
-                                  pack_h2(u[4].y, u[5].y), pack_h2(u[6].y, u[7].y));
-            uint4 nim = make_uint4(pack_h2(-u[0].y, -u[1].y), pack_h2(-u[2].y, -u[3].y),
-                                   pack_h2(-u[4].y, -u[5].y), pack_h2(-u[6].y, -u[7].y));
-            *reinterpret_cast<uint4*>(sB + core_off(tid, c, 2 * TC_TN)) = re;
-            *reinterpret_cast<uint4*>(sB + core_off(tid, 8 + c, 2 * TC_TN)) = nim;
-            *reinterpret_cast<uint4*>(sB + core_off(TC_TN + tid, c, 2 * TC_TN)) = im;
-            *reinterpret_cast<uint4*>(sB + core_off(TC_TN + tid, 8 + c, 2 * TC_TN)) = re;
-        }
+        for (uint32_t off = 0; off < kPanelU; off += kChunk)
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                         :: "r"(smem_u32(sB + off)), "l"(srcB + off), "r"(kChunk), "r"(bar_ld) : "memory");
     }
-    // make the generic-proxy shared stores visible to the tensor cores
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_slot;
-    const uint32_t mbar_addr = smem_u32(&mbar);
-
-    if (tid == 0) {
-        const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
-#pragma unroll
-        for (int s = 0; s < TC_KR / 16; ++s) {
-            const uint64_t da = umma_desc(a0 + 2 * s * kLboA, kLboA, kSbo);
-            const uint64_t db = umma_desc(b0 + 2 * s * kLboB, kLboB, kSbo);
-            const uint32_t acc = s > 0 ? 1u : 0u;
-            asm volatile(
-                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
-                :: "r"(tmem), "l"(da), "l"(db), "r"(kIdesc), "r"(acc),
-                   "r"(0u), "r"(0u), "r"(0u), "r"(0u));
-        }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                     :: "r"(mbar_addr) : "memory");
-    }
-    // CTA-uniform: tcgen05.ld below is warp-collective and must not diverge
-    const bool done = __syncthreads_and(mbar_wait(mbar_addr, 0)) != 0;
+    bool ok = __syncthreads_and(mbar_wait(bar_ld, 0)) != 0;
+    if (ok && tid == 0) mma_k128(tmem, smem_u32(sA), kLboA, smem_u32(sB), kLboB, kIdesc, bar_mma);
+    const bool done = ok && __syncthreads_and(mbar_wait(bar_mma, 0)) != 0;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (done) {
         const int64_t gi = r0 + warp * 32 + lane;
@@ -207,26 +332,29 @@ k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0, i
             tmem_ld32(lane_base + (uint32_t)(TC_TN + cc * 32), im);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (gi < n) {
-#pragma unroll 4
+                float2 v[32];
+#pragma unroll
                 for (int q = 0; q < 32; ++q) {
                     const int64_t gj = c0 + cc * 32 + q;
-                    if (gj < n) {
-                        float2 v = M[gj * n + gi];
-                        v.x -= __uint_as_float(re[q]);
-                        v.y -= __uint_as_float(im[q]);
-                        M[gj * n + gi] = v;
-                    }
+                    v[q] = gj < n ? M[gj * n + gi] : make_float2(0.f, 0.f);
+                }
+#pragma unroll
+                for (int q = 0; q < 32; ++q) {
+                    const int64_t gj = c0 + cc * 32 + q;
+                    if (gj < n)
+                        M[gj * n + gi] = make_float2(v[q].x - __uint_as_float(re[q]),
+                                                     v[q].y - __uint_as_float(im[q]));
                 }
             }
         }
     } else {
         if (lane == 0) atomicExch(bad + b, 2);
-        mbar_wait(mbar_addr, 0);  // bounded second wait for the MMAs still in flight
+        if (!ok) mbar_wait(bar_ld, 0);   // bounded: copies still in flight
+        mbar_wait(bar_mma, 0);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(kTmemCols));
+    if (warp == 0) tmem_dealloc(tmem, kTmemCols);
 }
 
 // ---------------------------------------------------------------------------
@@ -324,27 +452,39 @@ unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
 
 int64_t lu_dinv_stride_tc(int64_t n) { return ((n + TC_NB - 1) / TC_NB) * 2 * TC_NB * TC_NB; }
 
+int64_t lu_panel_bytes_tc(int64_t n) { return ((n + TC_TM - 1) / TC_TM) * (int64_t)(kPanelL + kPanelU); }
+
 cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int nbatch, float2* Dinv,
-                         int* bad)
+                         unsigned char* panels, int* bad)
 {
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(k_lu_diag<TC_NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    constexpr int kDiagThreads = 1024;
+    if ((e = cudaFuncSetAttribute(k_lu_diag<TC_NB, kDiagThreads>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)lu_diag_smem_bytes<TC_NB>())) != cudaSuccess)
         return e;
     if ((e = cudaFuncSetAttribute(k_lu_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kTcSmemBytes)) != cudaSuccess)
         return e;
+    if ((e = cudaFuncSetAttribute(k_lu_trsm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(kSmemA + kSmemA))) != cudaSuccess)
+        return e;
     const int64_t dstride = lu_dinv_stride_tc(n);
+    const int64_t pstride = lu_panel_bytes_tc(n);
+    const int64_t ntiles = (n + TC_TM - 1) / TC_TM;
+    unsigned char* Lp = panels;
+    unsigned char* Up = panels + ntiles * kPanelL;
     for (int64_t k0 = 0; k0 < n; k0 += TC_NB) {
-        k_lu_diag<TC_NB><<<nbatch, 256, lu_diag_smem_bytes<TC_NB>(), ctx->stream>>>(A, n, stride, k0,
-                                                                                  Dinv, dstride, bad);
+        k_lu_diag<TC_NB, kDiagThreads><<<nbatch, kDiagThreads, lu_diag_smem_bytes<TC_NB>(),
+                                         ctx->stream>>>(A, n, stride, k0, Dinv, dstride, bad);
         ctx->launches += 1;
         const int64_t rest = n - k0 - TC_NB;
         if (rest > 0) {
-            k_lu_trsm<TC_NB><<<dim3(cdiv(rest, 128), 2, (unsigned)nbatch), 128, 0, ctx->stream>>>(
-                A, n, stride, k0);
-            k_lu_update_tc<<<dim3(cdiv(rest, TC_TM), cdiv(rest, TC_TN), (unsigned)nbatch), 128,
-                             kTcSmemBytes, ctx->stream>>>(A, n, stride, k0, bad);
+            const unsigned nt = cdiv(rest, TC_TM);
+            k_lu_trsm_tc<<<dim3(2 * nt, (unsigned)nbatch), 128, kSmemA + kSmemA, ctx->stream>>>(
+                A, n, stride, k0, Dinv, dstride, Lp, Up, pstride, (int)nt, bad);
+            k_lu_update_tc<<<dim3(nt, nt, (unsigned)nbatch), 128, kTcSmemBytes, ctx->stream>>>(
+                A, n, stride, k0, Lp, Up, pstride, bad);
             ctx->launches += 2;
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
