@@ -224,6 +224,41 @@ int mh_hydro_batch(mh_ctx* ctx, const mh_mesh* mesh,
                    double* diffraction, double* froude_krylov,
                    mh_batch_info* info);
 
+/* ---- adjoint gradients -------------------------------------------------- */
+
+/* Reverse-mode derivative of mh_hydro_batch: runs the same forward batch
+ * (outputs as mh_hydro_batch, each may be NULL) and, for the cotangents of
+ * its outputs (bar_*, same layouts; NULL = zero), returns the cotangents of
+ * every input: the mesh fields as given to mh_mesh_create
+ *   d_vertices  n_vertices x 3,  d_centers, d_normals  nfaces x 3,
+ *   d_areas, d_radii  nfaces  (radii only select branches: zero),
+ * d_omegas (n_omega) and d_dofs (same layout as dofs); any may be NULL.
+ * For J(A, B, F, FK) the result is dJ/dx = sum bar_A dA/dx + bar_B dB/dx
+ * + Re(conj(bar_F) dF/dx) + Re(conj(bar_FK) dFK/dx) for the real and
+ * imaginary parts of complex outputs given as (re, im) pairs.
+ * Replaces Zygote's pullback through compute_hydrodynamic_coefficients /
+ * calculate_radiation_forces / DiffractionForce: the ImplicitAD adjoint of
+ * `solve` (src/matrix_assembly.jl:105-133, implicit_linear at :120) and the
+ * pullbacks of the pair integrals (src/green_functions/*.jl) that the
+ * reference's tests check (test/outputs_differentiation.jl:59-68, :21-35).
+ * The adjoint solve reuses the forward factors (FP64: conjugate-transposed
+ * zgetrs; mixed: the low-precision factors with FP64 refinement of
+ * D^H x = r to tol, FP64 fallback as in the forward).  Arguments and errors
+ * as mh_hydro_batch; non-finite cotangents are MH_ERR_ARG. */
+int mh_hydro_batch_vjp(mh_ctx* ctx, const mh_mesh* mesh,
+                       int64_t n_omega, const double* omegas,
+                       int64_t n_dof, const double* dofs,
+                       int64_t n_beta, const double* betas,
+                       double rho, double g, uint32_t gf_mask, int direct, int precision,
+                       double tol, int max_iter,
+                       const double* bar_added_mass, const double* bar_damping,
+                       const double* bar_diffraction, const double* bar_froude_krylov,
+                       double* added_mass, double* damping,
+                       double* diffraction, double* froude_krylov,
+                       double* d_vertices, double* d_centers, double* d_normals,
+                       double* d_areas, double* d_radii, double* d_omegas, double* d_dofs,
+                       mh_batch_info* info);
+
 /* ---- allocation-free mixed-precision solve ------------------------------ */
 
 #define MH_NOALLOC_MAX_N    1024

@@ -1,0 +1,1076 @@
+// Adjoint (reverse-mode) gradients of the batched hydrodynamic coefficients.
+//
+// Replaces the reference's differentiation of this path: Zygote through the
+// assembly, ImplicitAD's implicit_linear for the solve
+// (src/matrix_assembly.jl:105-133) and the ForwardDiff branch (:108-114).
+// For output cotangents (of added mass, damping, diffraction and
+// Froude-Krylov forces) it returns the cotangents of every mesh field
+// (vertices, centres, normals, areas, radii), of every frequency and of the
+// dof arrays, i.e. the Tangent{Mesh} plus omega-bar of an rrule.
+//
+// Per frequency, with S, D (K when indirect), boundary conditions b and
+// output cotangent phi-bar (from the force sums):
+//   direct   D phi = S b:    lambda = D^-H phi-bar, b-bar = S^H lambda,
+//            S-bar = lambda b^H, D-bar = -lambda phi^H;
+//   indirect K sigma = b, phi = S sigma: mu = K^-H S^H phi-bar, b-bar = mu,
+//            S-bar = phi-bar sigma^H, K-bar = -mu sigma^H.
+// The adjoint solve reuses the forward factors: FP64 (zgetrs with
+// conjugate transpose) or the low-precision factors with FP64 refinement of
+// D^H x = r.  S-bar and D-bar are never formed: the pair kernels form
+// sum_q a_iq conj(b_jq) on the fly.  The Rankine terms are frequency
+// independent, so their contraction runs once per call against
+// Re sum_w S-bar(w) and Re sum_w D-bar(w), accumulated by ZGEMM; the wave
+// term runs per frequency, with exact derivatives of the table or Wu
+// formulas (dual numbers in (r, z)) chained by hand to the panel geometry
+// and k.  The near-field Rankine integral is differentiated with 6-way dual
+// numbers (three passes over centre+normal and the four vertices).
+#include <cuComplex.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "mh_device.cuh"
+#include "mh_internal.h"
+
+namespace mh {
+namespace {
+
+constexpr int kAR = 128;  // rows (threads) per CTA of the pair kernels
+constexpr int kAC = 16;   // columns (panels in shared memory) per CTA
+constexpr double kI4P = 1.0 / (4.0 * kPi);
+
+// Per-panel cotangent fields (device array gbar[GB_NF][n]).
+enum GbarField : int { GB_C = 0, GB_N = 3, GB_A = 6, GB_V = 7, GB_NF = 19 };
+constexpr int kRowF = 6;   // row partials: centre (3), normal (3)
+constexpr int kWaveF = 7;  // wave column partials: centre, normal, area
+
+using d2 = dualn<2>;
+using d6 = dualn<6>;
+
+unsigned nblk(int64_t count, int threads) { return (unsigned)((count + threads - 1) / threads); }
+
+__device__ __forceinline__ double re_mul(const cplx& a, const cplx& b) { return a.re * b.re - a.im * b.im; }
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    return v;
+}
+
+__device__ __forceinline__ void stage(Panel* sp, const double* __restrict__ geom, int64_t n, int64_t j0)
+{
+    for (int t = threadIdx.x; t < kAC * G_NFIELDS; t += blockDim.x) {
+        const int f = t / kAC, jj = t % kAC;
+        const int64_t j = j0 + jj;
+        const double v = (j < n) ? geom[(int64_t)f * n + j] : 0.0;
+        Panel& p = sp[jj];
+        if (f < 3) p.c[f] = v;
+        else if (f < 6) p.n[f - 3] = v;
+        else if (f == G_AREA) p.area = v;
+        else if (f == G_RADIUS) p.radius = v;
+        else p.v[f - G_V] = v;
+    }
+}
+
+// Sum over the block of one value per thread; result valid in thread 0.
+__device__ __forceinline__ double block_sum(double v, double* red)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// wave term
+// ---------------------------------------------------------------------------
+
+// Dimensionless wave term and its (r, z) derivatives: o[m].{re,im}.d[0] =
+// d/dr, .d[1] = d/dz of (G, G_r, G_z).  kind 1: Wu; 2: Delhommeau (table
+// when tab != null, else the quadrature with analytic second derivatives).
+__device__ __noinline__ void wave_dimless_d2(int kind, const double* __restrict__ tab, double r, double z,
+                                             cx<d2>* o)
+{
+    d2 rd, zd;
+    rd.v = r;
+    rd.d[0] = 1.0;
+    rd.d[1] = 0.0;
+    zd.v = z;
+    zd.d[0] = 0.0;
+    zd.d[1] = 1.0;
+    if (kind == 1) wu_dimless(rd, zd, o);
+    else if (tab) delh_table_t(tab, rd, zd, o);
+    else delh_exact_t(rd, zd, o);
+}
+
+struct WaveBar {
+    double dx, dy, zs, area, k;
+    double n[3];
+};
+
+// Reverse of wave_pair for one pair (abstract_greens_function.jl:88-155 with
+// the one-point rule): L = Re(cs s + cw (nD . g)), with s = k A G(r, z),
+// g = (sg k^2 A u_x G_r, sg k^2 A u_y G_r, k^2 A G_z), r = k |dx, dy|,
+// z = k zs, u = (dx, dy)/|dx, dy|, sg = +1 for the gradient with respect to
+// the first variable.  Returns dL/d(dx, dy, zs, area, k) and dL/dnD.
+__device__ __forceinline__ void wave_pair_vjp(int kind, const double x[3], const Panel& p, double k,
+                                              bool wrt_first, const double* __restrict__ tab, cplx cs,
+                                              cplx cw, const double nD[3], WaveBar& wb)
+{
+    const double dx = x[0] - p.c[0], dy = x[1] - p.c[1], zs = x[2] + p.c[2];
+    const double dis2 = dx * dx + dy * dy;
+    const double purt = 1e-18;
+    const double dis = (dis2 == 0.0) ? sqrt(dis2 + purt * purt) - purt : sqrt(dis2);
+    const double r = k * dis, z = k * zs;
+    cx<d2> o[3];
+    wave_dimless_d2(kind, tab, r, z, o);
+    const cplx G0 = mk(o[0].re.v, o[0].im.v), G1 = mk(o[1].re.v, o[1].im.v), G2 = mk(o[2].re.v, o[2].im.v);
+    const bool rad = fabs(r) > 1e-6;
+    const double invd = dis > 0.0 ? 1.0 / dis : 0.0;
+    const double u0 = dx * invd, u1 = dy * invd;
+    const double sg = wrt_first ? 1.0 : -1.0;
+    const double A = p.area, k2 = k * k;
+    const cplx c0 = cw * nD[0], c1 = cw * nD[1], c2 = cw * nD[2];  // conj of the g cotangents
+    const cplx P1 = rad ? sg * (c0 * u0 + c1 * u1) : mk(0.0, 0.0);
+    double Lr = 0.0, Lz = 0.0;
+    {
+        const cplx a0 = cs * k, a1 = P1 * k2, a2 = c2 * k2;
+        Lr = A * (re_mul(a0, mk(o[0].re.d[0], o[0].im.d[0])) + re_mul(a1, mk(o[1].re.d[0], o[1].im.d[0])) +
+                  re_mul(a2, mk(o[2].re.d[0], o[2].im.d[0])));
+        Lz = A * (re_mul(a0, mk(o[0].re.d[1], o[0].im.d[1])) + re_mul(a1, mk(o[1].re.d[1], o[1].im.d[1])) +
+                  re_mul(a2, mk(o[2].re.d[1], o[2].im.d[1])));
+    }
+    const double U0 = rad ? sg * k2 * A * re_mul(c0, G1) : 0.0;
+    const double U1 = rad ? sg * k2 * A * re_mul(c1, G1) : 0.0;
+    wb.dx = Lr * k * u0 + (U0 * (1.0 - u0 * u0) - U1 * u0 * u1) * invd;
+    wb.dy = Lr * k * u1 + (U1 * (1.0 - u1 * u1) - U0 * u0 * u1) * invd;
+    wb.zs = Lz * k;
+    const double e0 = re_mul(cs, G0), e12 = re_mul(P1, G1) + re_mul(c2, G2);
+    wb.area = k * e0 + k2 * e12;
+    wb.k = Lr * dis + Lz * zs + A * e0 + 2.0 * k * A * e12;
+    const double gr = rad ? sg * k2 * A : 0.0;
+    const cplx g0 = (gr * u0) * G1, g1 = (gr * u1) * G1, g2 = (k2 * A) * G2;
+    wb.n[0] = re_mul(cw, g0);
+    wb.n[1] = re_mul(cw, g1);
+    wb.n[2] = re_mul(cw, g2);
+}
+
+// Wave-term contraction over the pairs of a 128-row x 16-column tile for
+// every frequency of the chunk.  S-bar_ij(z) = sum_q VA_iq conj(VB_jq),
+// D-bar_ij(z) = -sum_q VC_iq conj(VD_jq) (vectors [z][q][n]).
+// rowpart[colblock][kRowF][n], colpart[rowblock][kWaveF][n],
+// kpart[z][block]: deterministic partial sums.
+__global__ void __launch_bounds__(kAR)
+k_adj_wave(int kind, const double* __restrict__ geom, int64_t n, int direct, const double* __restrict__ tab,
+           const double* __restrict__ kvec, int nb, int nrhs, const double2* __restrict__ VA,
+           const double2* __restrict__ VB, const double2* __restrict__ VC, const double2* __restrict__ VD,
+           double* __restrict__ rowpart, double* __restrict__ colpart, double* __restrict__ kpart)
+{
+    extern __shared__ double ksm[];  // [4 warps][nb]
+    __shared__ Panel sp[kAC];
+    __shared__ double csm[kAR / 32][kAC][kWaveF];
+    const int64_t j0 = (int64_t)blockIdx.y * kAC;
+    stage(sp, geom, n, j0);
+    for (int t = threadIdx.x; t < (kAR / 32) * nb; t += blockDim.x) ksm[t] = 0.0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t i = (int64_t)blockIdx.x * kAR + threadIdx.x;
+    const bool live = i < n;
+    const int64_t ii = live ? i : 0;
+    const double x[3] = {geom[G_CX * n + ii], geom[G_CY * n + ii], geom[G_CZ * n + ii]};
+    const double ni[3] = {geom[G_NX * n + ii], geom[G_NY * n + ii], geom[G_NZ * n + ii]};
+    const int jend = (int)min((int64_t)kAC, n - j0);
+    const int64_t nv = n * nrhs;
+    double xb[3] = {0.0, 0.0, 0.0}, nbi[3] = {0.0, 0.0, 0.0};
+    for (int jj = 0; jj < jend; ++jj) {
+        const Panel& p = sp[jj];
+        const int64_t j = j0 + jj;
+        const double* nD = direct ? p.n : ni;
+        double cacc[kWaveF] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int z = 0; z < nb; ++z) {
+            const int64_t base = (int64_t)z * nv;
+            double sr = 0.0, si = 0.0, dr = 0.0, di = 0.0;
+            for (int q = 0; q < nrhs; ++q) {
+                const double2 a = VA[base + q * n + ii], b = VB[base + q * n + j];
+                const double2 c = VC[base + q * n + ii], d = VD[base + q * n + j];
+                sr += a.x * b.x + a.y * b.y;
+                si += a.y * b.x - a.x * b.y;
+                dr -= c.x * d.x + c.y * d.y;
+                di -= c.y * d.x - c.x * d.y;
+            }
+            // cs = conj(-S-bar / 4pi), cw = conj(-D-bar / 4pi)
+            const cplx cs = mk(-kI4P * sr, kI4P * si), cw = mk(-kI4P * dr, kI4P * di);
+            double bk = 0.0;
+            if (live) {
+                WaveBar wb;
+                wave_pair_vjp(kind, x, p, kvec[z], !direct, tab, cs, cw, nD, wb);
+                xb[0] += wb.dx;
+                xb[1] += wb.dy;
+                xb[2] += wb.zs;
+                cacc[0] -= wb.dx;
+                cacc[1] -= wb.dy;
+                cacc[2] += wb.zs;
+                if (direct) {
+                    cacc[3] += wb.n[0];
+                    cacc[4] += wb.n[1];
+                    cacc[5] += wb.n[2];
+                } else {
+                    nbi[0] += wb.n[0];
+                    nbi[1] += wb.n[1];
+                    nbi[2] += wb.n[2];
+                }
+                cacc[6] += wb.area;
+                bk = wb.k;
+            }
+            bk = warp_sum(bk);
+            if (lane == 0) ksm[warp * nb + z] += bk;
+        }
+#pragma unroll
+        for (int f = 0; f < kWaveF; ++f) {
+            const double v = warp_sum(cacc[f]);
+            if (lane == 0) csm[warp][jj][f] = v;
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < jend * kWaveF; t += blockDim.x) {
+        const int jj = t / kWaveF, f = t % kWaveF;
+        double s = 0.0;
+        for (int w = 0; w < kAR / 32; ++w) s += csm[w][jj][f];
+        colpart[((int64_t)blockIdx.x * kWaveF + f) * n + j0 + jj] = s;
+    }
+    if (live) {
+        for (int c = 0; c < 3; ++c) {
+            rowpart[((int64_t)blockIdx.y * kRowF + c) * n + i] = xb[c];
+            rowpart[((int64_t)blockIdx.y * kRowF + 3 + c) * n + i] = nbi[c];
+        }
+    }
+    const int64_t P = (int64_t)gridDim.x * gridDim.y;
+    const int64_t blk = (int64_t)blockIdx.y * gridDim.x + blockIdx.x;
+    for (int z = threadIdx.x; z < nb; z += blockDim.x) {
+        double s = 0.0;
+        for (int w = 0; w < kAR / 32; ++w) s += ksm[w * nb + z];
+        kpart[(int64_t)z * P + blk] = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Rankine terms
+// ---------------------------------------------------------------------------
+
+// Near field (rankine.jl:36-61, 65-123): derivatives along the panel centre,
+// normal and the four vertices by 6-way dual numbers, three passes.  The
+// integrals depend on y - c, y - v_a and n only, so dL/dy = -(dL/dc + sum_a
+// dL/dv_a).  Accumulates into pb (gbar field order); gr = forward gradient.
+__device__ __noinline__ void rankine_near_vjp(const double* y, const Panel& p, double ibar,
+                                              const double* gb, double* yb, double* pb, double* gr)
+{
+    double cb[3], nbv[3], vb[12];
+    for (int pass = 0; pass < 3; ++pass) {
+        PanelT<d6> q;
+        for (int a = 0; a < 3; ++a) {
+            q.c[a] = dconst<6>(p.c[a]);
+            q.n[a] = dconst<6>(p.n[a]);
+        }
+        for (int t = 0; t < 12; ++t) q.v[t] = dconst<6>(p.v[t]);
+        q.area = dconst<6>(p.area);
+        q.radius = dconst<6>(p.radius);
+        if (pass == 0) {
+            for (int a = 0; a < 3; ++a) {
+                q.c[a].d[a] = 1.0;
+                q.n[a].d[3 + a] = 1.0;
+            }
+        } else {
+            const int v0 = 2 * (pass - 1);
+            for (int c = 0; c < 3; ++c) {
+                q.v[3 * v0 + c].d[c] = 1.0;
+                q.v[3 * (v0 + 1) + c].d[3 + c] = 1.0;
+            }
+        }
+        const d6 yd[3] = {dconst<6>(y[0]), dconst<6>(y[1]), dconst<6>(y[2])};
+        d6 I, g[3];
+        rankine_pair(yd, q, I, g);
+        double t[6];
+        for (int k = 0; k < 6; ++k) t[k] = ibar * I.d[k] + gb[0] * g[0].d[k] + gb[1] * g[1].d[k] + gb[2] * g[2].d[k];
+        if (pass == 0) {
+            for (int a = 0; a < 3; ++a) {
+                cb[a] = t[a];
+                nbv[a] = t[3 + a];
+                gr[a] = g[a].v;
+            }
+        } else {
+            for (int k = 0; k < 6; ++k) vb[6 * (pass - 1) + k] = t[k];
+        }
+    }
+    for (int a = 0; a < 3; ++a) {
+        yb[a] = -(cb[a] + vb[a] + vb[3 + a] + vb[6 + a] + vb[9 + a]);
+        pb[GB_C + a] += cb[a];
+        pb[GB_N + a] += nbv[a];
+    }
+    for (int t = 0; t < 12; ++t) pb[GB_V + t] += vb[t];
+}
+
+// Reverse of rankine_pair at point y: L = ibar * I + gb . grad.
+__device__ __forceinline__ void rankine_vjp(const double y[3], const Panel& p, double ibar, const double gb[3],
+                                            double yb[3], double pb[GB_NF], double gr[3])
+{
+    const double rb[3] = {y[0] - p.c[0], y[1] - p.c[1], y[2] - p.c[2]};
+    const double r = sqrt(rb[0] * rb[0] + rb[1] * rb[1] + rb[2] * rb[2]);
+    if (r > 7.0 * p.radius) {  // far field: I = A/r, grad = A rb / r^3 (rankine.jl:33-34)
+        const double ir = 1.0 / r, ir3 = ir * ir * ir, ir5 = ir3 * ir * ir;
+        const double A = p.area;
+        const double gdr = gb[0] * rb[0] + gb[1] * rb[1] + gb[2] * rb[2];
+        for (int a = 0; a < 3; ++a) {
+            gr[a] = rb[a] * ir3 * A;
+            const double d = A * (-ibar * rb[a] * ir3 + gb[a] * ir3 - 3.0 * gdr * rb[a] * ir5);
+            yb[a] = d;
+            pb[GB_C + a] -= d;
+        }
+        pb[GB_A] += ibar * ir + gdr * ir3;
+        return;
+    }
+    rankine_near_vjp(y, p, ibar, gb, yb, pb, gr);
+}
+
+// Rankine-term contraction against the frequency sums WS = sum_w S-bar(w),
+// WD = sum_w D-bar(w) (real parts used).  Layout as k_adj_wave with
+// GB_NF column fields.
+__global__ void __launch_bounds__(kAR)
+k_adj_rankine(const double* __restrict__ geom, int64_t n, uint32_t mask, int direct,
+              const double2* __restrict__ WS, const double2* __restrict__ WD, double* __restrict__ rowpart,
+              double* __restrict__ colpart)
+{
+    __shared__ Panel sp[kAC];
+    __shared__ double csm[kAR / 32][kAC][GB_NF];
+    const int64_t j0 = (int64_t)blockIdx.y * kAC;
+    stage(sp, geom, n, j0);
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t i = (int64_t)blockIdx.x * kAR + threadIdx.x;
+    const bool live = i < n;
+    const int64_t ii = live ? i : 0;
+    const double x[3] = {geom[G_CX * n + ii], geom[G_CY * n + ii], geom[G_CZ * n + ii]};
+    const double ni[3] = {geom[G_NX * n + ii], geom[G_NY * n + ii], geom[G_NZ * n + ii]};
+    const int jend = (int)min((int64_t)kAC, n - j0);
+    const bool wrt_first = !direct;
+    const double sg = wrt_first ? -1.0 : 1.0, sz = wrt_first ? -1.0 : 1.0;
+    const uint32_t refl = mask & (MH_GF_RANKINE_REFLECTED | MH_GF_RANKINE_REFLECTED_NEGATIVE);
+    const bool has_refl = refl == MH_GF_RANKINE_REFLECTED || refl == MH_GF_RANKINE_REFLECTED_NEGATIVE;
+    const double sgn = (refl == MH_GF_RANKINE_REFLECTED) ? 1.0 : -1.0;
+    double xb[3] = {0.0, 0.0, 0.0}, nbi[3] = {0.0, 0.0, 0.0};
+    for (int jj = 0; jj < jend; ++jj) {
+        const Panel& p = sp[jj];
+        const int64_t j = j0 + jj;
+        const double* nD = direct ? p.n : ni;
+        double pb[GB_NF];
+#pragma unroll
+        for (int f = 0; f < GB_NF; ++f) pb[f] = 0.0;
+        if (live) {
+            const double ws = WS[j * n + i].x, wd = WD[j * n + i].x;
+            const double ibar = -kI4P * ws;
+            const double gbar[3] = {-kI4P * wd * nD[0], -kI4P * wd * nD[1], -kI4P * wd * nD[2]};
+            double gt[3] = {0.0, 0.0, 0.0};
+            if (mask & MH_GF_RANKINE) {
+                const double gb[3] = {sg * gbar[0], sg * gbar[1], sg * gbar[2]};
+                double yb[3], gr[3];
+                rankine_vjp(x, p, ibar, gb, yb, pb, gr);
+                for (int a = 0; a < 3; ++a) {
+                    xb[a] += yb[a];
+                    gt[a] += sg * gr[a];
+                }
+            }
+            if (has_refl) {
+                const double xr[3] = {x[0], x[1], -x[2]};
+                const double m[3] = {sgn * sg, sgn * sg, sgn * sg * sz};
+                const double gb[3] = {m[0] * gbar[0], m[1] * gbar[1], m[2] * gbar[2]};
+                double yb[3], gr[3];
+                rankine_vjp(xr, p, sgn * ibar, gb, yb, pb, gr);
+                xb[0] += yb[0];
+                xb[1] += yb[1];
+                xb[2] -= yb[2];
+                for (int a = 0; a < 3; ++a) gt[a] += m[a] * gr[a];
+            }
+            for (int a = 0; a < 3; ++a) {
+                const double nb_a = -kI4P * wd * gt[a];
+                if (direct) pb[GB_N + a] += nb_a;
+                else nbi[a] += nb_a;
+            }
+        }
+#pragma unroll
+        for (int f = 0; f < GB_NF; ++f) {
+            const double v = warp_sum(pb[f]);
+            if (lane == 0) csm[warp][jj][f] = v;
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < jend * GB_NF; t += blockDim.x) {
+        const int jj = t / GB_NF, f = t % GB_NF;
+        double s = 0.0;
+        for (int w = 0; w < kAR / 32; ++w) s += csm[w][jj][f];
+        colpart[((int64_t)blockIdx.x * GB_NF + f) * n + j0 + jj] = s;
+    }
+    if (live) {
+        for (int c = 0; c < 3; ++c) {
+            rowpart[((int64_t)blockIdx.y * kRowF + c) * n + i] = xb[c];
+            rowpart[((int64_t)blockIdx.y * kRowF + 3 + c) * n + i] = nbi[c];
+        }
+    }
+}
+
+// gbar[f][i] += sum over row partials (fields 0..kRowF) and column partials
+// (fields 0..colF), in a fixed order.
+__global__ void k_adj_reduce(int64_t n, const double* __restrict__ rowpart, int nrow, const double* __restrict__ colpart,
+                             int ncol, int colF, double* __restrict__ gbar)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int f = 0; f < kRowF; ++f) {
+        double s = 0.0;
+        for (int p = 0; p < nrow; ++p) s += rowpart[((int64_t)p * kRowF + f) * n + i];
+        gbar[(int64_t)f * n + i] += s;
+    }
+    for (int f = 0; f < colF; ++f) {
+        double s = 0.0;
+        for (int p = 0; p < ncol; ++p) s += colpart[((int64_t)p * colF + f) * n + i];
+        gbar[(int64_t)f * n + i] += s;
+    }
+}
+
+// out[z] += sum_p part[z][p] (one CTA per z, fixed-order tree).
+__global__ void __launch_bounds__(256) k_sum_parts(const double* __restrict__ part, int64_t P, double* __restrict__ out)
+{
+    __shared__ double red[256];
+    const int z = blockIdx.x;
+    double s = 0.0;
+    for (int64_t p = threadIdx.x; p < P; p += blockDim.x) s += part[(int64_t)z * P + p];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[z] += red[0];
+}
+
+// ---------------------------------------------------------------------------
+// O(n) terms: forces, Froude-Krylov, boundary conditions
+// ---------------------------------------------------------------------------
+
+// Reverse of the force sums (src/waves.jl:72-85, 157-163) for the nb
+// frequencies of a chunk; thread = panel.  CF[z][q][d]: complex cotangent of
+// F_dq; CK[z][b][d]: of the Froude-Krylov force.  Writes phi-bar
+// PB[z][q][n] and accumulates panel and dof cotangents; kpart[z][block]
+// gets the k cotangents of the incident pressure.
+__global__ void __launch_bounds__(256)
+k_adj_forces(const double* __restrict__ geom, int64_t n, const double* __restrict__ dofs, int ndof,
+             const double* __restrict__ betas, int nbeta, const double* __restrict__ omegas, int nb,
+             double rho, double gacc, const double2* __restrict__ PHI, const double2* __restrict__ CF,
+             const double2* __restrict__ CK, double2* __restrict__ PB, double* __restrict__ gbar,
+             double* __restrict__ dofbar, double* __restrict__ kpart)
+{
+    __shared__ double red[8];
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < n;
+    const int64_t ii = live ? i : 0;
+    const int nrhs = ndof + nbeta;
+    const double x = geom[G_CX * n + ii], y = geom[G_CY * n + ii], zc = geom[G_CZ * n + ii];
+    const double nx = geom[G_NX * n + ii], ny = geom[G_NY * n + ii], nz = geom[G_NZ * n + ii];
+    const double a = geom[G_AREA * n + ii];
+    double gc[3] = {0.0, 0.0, 0.0}, gn[3] = {0.0, 0.0, 0.0}, ga = 0.0;
+    double zb[kMaxRhs][3];
+    double nzd[kMaxRhs], md[kMaxRhs];
+    for (int d = 0; d < ndof; ++d) {
+        const double* dd = dofs + (int64_t)d * 3 * n;
+        zb[d][0] = zb[d][1] = zb[d][2] = 0.0;
+        nzd[d] = nx * dd[ii] + ny * dd[n + ii] + nz * dd[2 * n + ii];
+        md[d] = -nzd[d] * a;
+    }
+    for (int z = 0; z < nb; ++z) {
+        const double w = omegas[z], k = w * w / gacc;
+        const double2* cf = CF + (int64_t)z * nrhs * ndof;
+        double mb[kMaxRhs];
+        for (int d = 0; d < ndof; ++d) mb[d] = 0.0;
+        for (int q = 0; q < nrhs; ++q) {
+            double ar = 0.0, ai = 0.0;
+            for (int d = 0; d < ndof; ++d) {
+                ar += md[d] * cf[q * ndof + d].x;
+                ai += md[d] * cf[q * ndof + d].y;
+            }
+            const double2 ph = PHI[((int64_t)z * nrhs + q) * n + ii];
+            if (live) PB[((int64_t)z * nrhs + q) * n + i] = make_double2(rho * w * ai, -rho * w * ar);
+            // m-bar_d += Re(conj(c) i rho w phi) = -rho w Im(conj(c) phi)
+            for (int d = 0; d < ndof; ++d) {
+                const double2 c = cf[q * ndof + d];
+                mb[d] -= rho * w * (c.x * ph.y - c.y * ph.x);
+            }
+        }
+        double kb = 0.0;
+        for (int b = 0; b < nbeta; ++b) {
+            double sb, cb, sw, cw;
+            sincos(betas[b], &sb, &cb);
+            const double wv = x * cb + y * sb;
+            sincos(k * wv, &sw, &cw);
+            const double m = rho * gacc * exp(k * zc);
+            const double pr = m * cw, pi = m * sw;
+            const double2* ck = CK + ((int64_t)z * nbeta + b) * ndof;
+            double pbr = 0.0, pbi = 0.0;
+            for (int d = 0; d < ndof; ++d) {
+                mb[d] += ck[d].x * pr + ck[d].y * pi;
+                pbr += ck[d].x * md[d];
+                pbi += ck[d].y * md[d];
+            }
+            // cpp = conj(p-bar) p
+            const double cr = pbr * pr + pbi * pi, ci = pbr * pi - pbi * pr;
+            gc[2] += cr * k;
+            gc[0] -= ci * k * cb;
+            gc[1] -= ci * k * sb;
+            kb += cr * zc - ci * wv;
+        }
+        for (int d = 0; d < ndof; ++d) {
+            const double* dd = dofs + (int64_t)d * 3 * n;
+            const double zeta[3] = {dd[ii], dd[n + ii], dd[2 * n + ii]};
+            gn[0] -= mb[d] * zeta[0] * a;
+            gn[1] -= mb[d] * zeta[1] * a;
+            gn[2] -= mb[d] * zeta[2] * a;
+            ga -= mb[d] * nzd[d];
+            zb[d][0] -= mb[d] * nx * a;
+            zb[d][1] -= mb[d] * ny * a;
+            zb[d][2] -= mb[d] * nz * a;
+        }
+        const double s = block_sum(live ? kb : 0.0, red);
+        if (threadIdx.x == 0) kpart[(int64_t)z * gridDim.x + blockIdx.x] = s;
+    }
+    if (!live) return;
+    for (int c = 0; c < 3; ++c) {
+        gbar[(GB_C + c) * n + i] += gc[c];
+        gbar[(GB_N + c) * n + i] += gn[c];
+    }
+    gbar[GB_A * n + i] += ga;
+    for (int d = 0; d < ndof; ++d)
+        for (int c = 0; c < 3; ++c) dofbar[((int64_t)d * 3 + c) * n + i] += zb[d][c];
+}
+
+// Reverse of the boundary conditions (src/waves.jl:89-101, 121-142) for
+// b-bar BB[z][q][n]: radiation -i w (n . dof_q); diffraction
+// -(g k / w) e^{k z} e^{i k (x cos b + y sin b)} (n_x cos b + n_y sin b - i n_z).
+// kpart/wpart[z][block]: k and explicit omega cotangents.
+__global__ void __launch_bounds__(256)
+k_adj_bc(const double* __restrict__ geom, int64_t n, const double* __restrict__ dofs, int ndof,
+         const double* __restrict__ betas, int nbeta, const double* __restrict__ omegas, int nb, double gacc,
+         const double2* __restrict__ BB, double* __restrict__ gbar, double* __restrict__ dofbar,
+         double* __restrict__ kpart, double* __restrict__ wpart)
+{
+    __shared__ double red[8];
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < n;
+    const int64_t ii = live ? i : 0;
+    const int nrhs = ndof + nbeta;
+    const double x = geom[G_CX * n + ii], y = geom[G_CY * n + ii], zc = geom[G_CZ * n + ii];
+    const double nv[3] = {geom[G_NX * n + ii], geom[G_NY * n + ii], geom[G_NZ * n + ii]};
+    double gc[3] = {0.0, 0.0, 0.0}, gn[3] = {0.0, 0.0, 0.0};
+    for (int z = 0; z < nb; ++z) {
+        const double w = omegas[z], k = w * w / gacc;
+        double kb = 0.0, wb = 0.0;
+        for (int q = 0; q < ndof; ++q) {
+            const double* dd = dofs + (int64_t)q * 3 * n;
+            const double zeta[3] = {dd[ii], dd[n + ii], dd[2 * n + ii]};
+            const double s = -BB[((int64_t)z * nrhs + q) * n + ii].y;  // Re(conj(b-bar) (-i))
+            for (int c = 0; c < 3; ++c) {
+                gn[c] += w * s * zeta[c];
+                if (live) dofbar[((int64_t)q * 3 + c) * n + i] += w * s * nv[c];
+            }
+            wb += s * (nv[0] * zeta[0] + nv[1] * zeta[1] + nv[2] * zeta[2]);
+        }
+        const double f = gacc * k / w, ez = exp(k * zc);
+        for (int b = 0; b < nbeta; ++b) {
+            double sb, cb, sw, cw;
+            sincos(betas[b], &sb, &cb);
+            const double wv = x * cb + y * sb;
+            sincos(k * wv, &sw, &cw);
+            const cplx E = mk(f * ez * cw, f * ez * sw);
+            const cplx h = mk(nv[0] * cb + nv[1] * sb, -nv[2]);
+            const cplx bv = -(E * h);
+            const double2 bbar = BB[((int64_t)z * nrhs + ndof + b) * n + ii];
+            const cplx cbb = mk(bbar.x, -bbar.y);  // conj(b-bar)
+            const cplx cb_ = cbb * bv;
+            gc[2] += cb_.re * k;
+            gc[0] -= cb_.im * k * cb;
+            gc[1] -= cb_.im * k * sb;
+            kb += cb_.re * zc - cb_.im * wv + cb_.re / k;
+            wb -= cb_.re / w;
+            const cplx Ep = cbb * (-E);
+            gn[0] += Ep.re * cb;
+            gn[1] += Ep.re * sb;
+            gn[2] += Ep.im;
+        }
+        double s = block_sum(live ? kb : 0.0, red);
+        if (threadIdx.x == 0) kpart[(int64_t)z * gridDim.x + blockIdx.x] = s;
+        s = block_sum(live ? wb : 0.0, red);
+        if (threadIdx.x == 0) wpart[(int64_t)z * gridDim.x + blockIdx.x] = s;
+    }
+    if (!live) return;
+    for (int c = 0; c < 3; ++c) {
+        gbar[(GB_C + c) * n + i] += gc[c];
+        gbar[(GB_N + c) * n + i] += gn[c];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+
+// C = alpha A^H B + beta C for nb strided n x n by n x nrhs products.
+int zgemm_ct_strided(mh_ctx* ctx, int64_t n, int nrhs, const double2* A, const double2* B, double2* C, int nb,
+                     double alpha_re, double beta_re)
+{
+    const cuDoubleComplex alpha = make_cuDoubleComplex(alpha_re, 0.0);
+    const cuDoubleComplex beta = make_cuDoubleComplex(beta_re, 0.0);
+    cublasStatus_t st = cublasZgemmStridedBatched(
+        ctx->cublas, CUBLAS_OP_C, CUBLAS_OP_N, (int)n, nrhs, (int)n, &alpha, (const cuDoubleComplex*)A,
+        (int)n, n * n, (const cuDoubleComplex*)B, (int)n, n * nrhs, &beta, (cuDoubleComplex*)C, (int)n,
+        n * nrhs, nb);
+    if (st != CUBLAS_STATUS_SUCCESS)
+        return set_err(ctx, MH_ERR_CUDA, "cublasZgemmStridedBatched (conjugate transpose) failed (%d)", (int)st);
+    return MH_OK;
+}
+
+// W += alpha U V^H, U and V n x K.
+int zgemm_outer(mh_ctx* ctx, int64_t n, int64_t K, const double2* U, const double2* V, double2* W, double alpha_re)
+{
+    const cuDoubleComplex alpha = make_cuDoubleComplex(alpha_re, 0.0);
+    const cuDoubleComplex beta = make_cuDoubleComplex(1.0, 0.0);
+    cublasStatus_t st = cublasZgemm(ctx->cublas, CUBLAS_OP_N, CUBLAS_OP_C, (int)n, (int)n, (int)K, &alpha,
+                                    (const cuDoubleComplex*)U, (int)n, (const cuDoubleComplex*)V, (int)n,
+                                    &beta, (cuDoubleComplex*)W, (int)n);
+    if (st != CUBLAS_STATUS_SUCCESS)
+        return set_err(ctx, MH_ERR_CUDA, "cublasZgemm (outer product) failed (%d)", (int)st);
+    return MH_OK;
+}
+
+// Device state of one vjp call.
+struct Vjp {
+    double* gbar;    // [GB_NF][n]
+    double* dofbar;  // [ndof][3][n]
+    double* kbar;    // [nomega]
+    double* wbar;    // [nomega] explicit omega cotangent
+    double2* WS;     // n x n, sum over frequencies of S-bar (Rankine contraction)
+    double2* WD;
+    double2* CF;     // [nomega][nrhs][ndof]
+    double2* CK;     // [nomega][nbeta][ndof]
+    double* part;    // partial sums
+    size_t part_words;
+    bool rankine;
+    int wave_kinds[2];
+    int nwave;
+};
+
+size_t part_words_needed(int64_t n, int nb)
+{
+    const int64_t rb = nblk(n, kAR), cb = nblk(n, kAC);
+    const int64_t pair = rb * cb;
+    const size_t pairs = (size_t)cb * kRowF * n + (size_t)rb * GB_NF * n + (size_t)nb * pair;
+    const size_t lin = (size_t)2 * nb * nblk(n, 256);
+    return std::max(pairs, lin);
+}
+
+// Contraction of the pair kernels for the vectors of nb frequencies.
+int contract_pairs_wave(const Batch& bt, Vjp& vj, const double* d_k, int nb, int z0, const double* tab,
+                        const double2* VA, const double2* VB, const double2* VC, const double2* VD)
+{
+    mh_ctx* ctx = bt.ctx;
+    const int64_t n = bt.n;
+    const unsigned rb = nblk(n, kAR), cb = nblk(n, kAC);
+    double* rowpart = vj.part;
+    double* colpart = rowpart + (size_t)cb * kRowF * n;
+    double* kpart = colpart + (size_t)rb * kWaveF * n;
+    for (int w = 0; w < vj.nwave; ++w) {
+        const int kind = vj.wave_kinds[w];
+        const size_t smem = sizeof(double) * (kAR / 32) * nb;
+        k_adj_wave<<<dim3(rb, cb), kAR, smem, ctx->stream>>>(kind, bt.m->geom, n, bt.direct,
+                                                             kind == 2 ? tab : nullptr, d_k, nb, bt.nrhs,
+                                                             VA, VB, VC, VD, rowpart, colpart, kpart);
+        k_adj_reduce<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, rowpart, (int)cb, colpart, (int)rb, kWaveF,
+                                                            vj.gbar);
+        k_sum_parts<<<nb, 256, 0, ctx->stream>>>(kpart, (int64_t)rb * cb, vj.kbar + z0);
+        ctx->launches += 3;
+        MH_CUDA_TRY(ctx, cudaGetLastError());
+    }
+    return MH_OK;
+}
+
+// Everything after the adjoint solve for nb frequencies: Rankine sums,
+// wave contraction, boundary-condition reverse.
+int adjoint_tail(const Batch& bt, Vjp& vj, const double* d_omegas, const double* d_k, int nb, int z0,
+                 const double* tab, const double2* VA, const double2* VB, const double2* VC,
+                 const double2* VD, const double2* BB)
+{
+    mh_ctx* ctx = bt.ctx;
+    const int64_t n = bt.n;
+    int rc;
+    if (vj.rankine) {
+        const int64_t K = (int64_t)nb * bt.nrhs;
+        if ((rc = zgemm_outer(ctx, n, K, VA, VB, vj.WS, 1.0))) return rc;
+        if ((rc = zgemm_outer(ctx, n, K, VC, VD, vj.WD, -1.0))) return rc;
+    }
+    if ((rc = contract_pairs_wave(bt, vj, d_k, nb, z0, tab, VA, VB, VC, VD))) return rc;
+    const unsigned lb = nblk(n, 256);
+    double* kpart = vj.part;
+    double* wpart = kpart + (size_t)nb * lb;
+    k_adj_bc<<<lb, 256, 0, ctx->stream>>>(bt.m->geom, n, bt.d_dofs, bt.ndof, bt.d_betas, bt.nbeta, d_omegas,
+                                          nb, bt.g, BB, vj.gbar, vj.dofbar, kpart, wpart);
+    k_sum_parts<<<nb, 256, 0, ctx->stream>>>(kpart, lb, vj.kbar + z0);
+    k_sum_parts<<<nb, 256, 0, ctx->stream>>>(wpart, lb, vj.wbar + z0);
+    ctx->launches += 3;
+    MH_CUDA_TRY(ctx, cudaGetLastError());
+    return MH_OK;
+}
+
+int seed_forces(const Batch& bt, Vjp& vj, const double* d_omegas, int nb, int z0, const double2* PHI,
+                double2* PB)
+{
+    mh_ctx* ctx = bt.ctx;
+    const int64_t n = bt.n;
+    const unsigned lb = nblk(n, 256);
+    double* kpart = vj.part;
+    k_adj_forces<<<lb, 256, 0, ctx->stream>>>(bt.m->geom, n, bt.d_dofs, bt.ndof, bt.d_betas, bt.nbeta,
+                                              d_omegas, nb, bt.rho, bt.g, PHI,
+                                              vj.CF + (int64_t)z0 * bt.nrhs * bt.ndof,
+                                              vj.CK + (int64_t)z0 * bt.nbeta * bt.ndof, PB, vj.gbar,
+                                              vj.dofbar, kpart);
+    k_sum_parts<<<nb, 256, 0, ctx->stream>>>(kpart, lb, vj.kbar + z0);
+    ctx->launches += 2;
+    MH_CUDA_TRY(ctx, cudaGetLastError());
+    return MH_OK;
+}
+
+// Mixed adjoint of one chunk: the forward state of run_mixed_chunk is in
+// the workspace.  Solves D^H x = rhs with the low-precision factors and FP64
+// refinement; problems that left the mixed path in the forward solve, or
+// whose adjoint refinement does not converge, use FP64 factors.
+int adjoint_mixed_chunk(const Batch& bt, Vjp& vj, const double* d_omegas, const double* d_k, int nb, int z0,
+                        double tol, int max_iter, FallbackStore& fb, mh_batch_info* info)
+{
+    mh_ctx* ctx = bt.ctx;
+    const int64_t n = bt.n, nn = n * n;
+    const int nrhs = bt.nrhs;
+    const int64_t nv = n * nrhs, cnt = nv * nb;
+    const bool tc = ctx->lu_backend == MH_LU_TCGEN05_F16;
+    auto* S64 = (double2*)ctx->ws[WS_S];
+    auto* D64 = (double2*)ctx->ws[WS_D];
+    auto* Dlo = (float2*)ctx->ws[WS_LO];
+    auto* Dinv = (float2*)ctx->ws[WS_DINV];
+    auto* BC = (double2*)ctx->ws[WS_RHS];
+    auto* X = (double2*)ctx->ws[WS_PHI];
+    auto* PHIi = (double2*)ctx->ws[WS_TMP];  // phi = S sigma (indirect)
+    auto* adj = (double2*)ws_get(ctx, WS_ADJ, sizeof(double2) * cnt * 5);
+    auto* R32 = (float2*)ws_get(ctx, WS_TMP32, sizeof(float2) * cnt);
+    auto* T32 = (float2*)ws_get(ctx, WS_TMP32B, sizeof(float2) * cnt);
+    auto* misc = (double*)ws_get(ctx, WS_MISC, (sizeof(double) + sizeof(int)) * nb + 64);
+    if (!adj || !R32 || !T32 || !misc) return MH_ERR_OOM;
+    double2* PB = adj;
+    double2* LAM = adj + cnt;
+    double2* BB = adj + 2 * cnt;
+    double2* RHS = adj + 3 * cnt;
+    double2* R = adj + 4 * cnt;
+    int rc;
+    const double* tab = delh_table_for(ctx, bt.mask, &rc);
+    if (rc) return rc;
+    if ((rc = seed_forces(bt, vj, d_omegas, nb, z0, bt.direct ? X : PHIi, PB))) return rc;
+    if (bt.direct) {
+        MH_CUDA_TRY(ctx, cudaMemcpyAsync(RHS, PB, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, ctx->stream));
+    } else if ((rc = zgemm_ct_strided(ctx, n, nrhs, S64, PB, RHS, nb, 1.0, 0.0))) {
+        return rc;
+    }
+    // refinement of D^H lam = RHS
+    MH_CUDA_TRY(ctx, cudaMemsetAsync(LAM, 0, sizeof(double2) * cnt, ctx->stream));
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(R, RHS, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, ctx->stream));
+    std::vector<double> h_res(nb, INFINITY);
+    for (int it = 1; it <= max_iter; ++it) {
+        MH_CUDA_TRY(ctx, launch_to_f32(ctx, R, R32, cnt));
+        MH_CUDA_TRY(ctx, launch_lu_solve_ct(ctx, tc ? MH_LU_TCGEN05_F16 : MH_LU_SIMT_F32, Dlo, n, nn, nb, Dinv,
+                                            R32, T32, nv, nrhs));
+        MH_CUDA_TRY(ctx, launch_add_f32(ctx, LAM, R32, cnt));
+        MH_CUDA_TRY(ctx, cudaMemcpyAsync(R, RHS, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, ctx->stream));
+        if ((rc = zgemm_ct_strided(ctx, n, nrhs, D64, LAM, R, nb, -1.0, 1.0))) return rc;
+        MH_CUDA_TRY(ctx, launch_rel_residual(ctx, R, RHS, n, nrhs, nb, misc));
+        MH_CUDA_TRY(ctx, cudaMemcpyAsync(h_res.data(), misc, sizeof(double) * nb, cudaMemcpyDeviceToHost,
+                                         ctx->stream));
+        MH_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        double worst = 0.0;
+        for (int z = 0; z < nb; ++z)
+            if (!fb.used[z]) worst = std::max(worst, std::isfinite(h_res[z]) ? h_res[z] : INFINITY);
+        info->refine_iterations = std::max(info->refine_iterations, it);
+        if (worst <= tol) break;
+    }
+    for (int z = 0; z < nb; ++z) {
+        if (!fb.used[z] && h_res[z] <= tol) {
+            info->max_rel_residual = std::max(info->max_rel_residual, h_res[z]);
+            continue;
+        }
+        if (!fb.used[z]) {
+            info->n_fallback += 1;
+            if ((rc = fallback_factor(ctx, &fb, n, nb, z, D64 + (int64_t)z * nn))) return rc;
+        }
+        double2* Lz = LAM + (int64_t)z * nv;
+        MH_CUDA_TRY(ctx, cudaMemcpyAsync(Lz, RHS + (int64_t)z * nv, sizeof(double2) * nv,
+                                         cudaMemcpyDeviceToDevice, ctx->stream));
+        if ((rc = fp64_getrs(ctx, true, n, fb.lu + (int64_t)z * nn, fb.piv + (int64_t)z * n, Lz, nrhs)))
+            return rc;
+    }
+    if (bt.direct) {
+        if ((rc = zgemm_ct_strided(ctx, n, nrhs, S64, LAM, BB, nb, 1.0, 0.0))) return rc;
+        return adjoint_tail(bt, vj, d_omegas, d_k, nb, z0, tab, LAM, BC, LAM, X, BB);
+    }
+    return adjoint_tail(bt, vj, d_omegas, d_k, nb, z0, tab, PB, X, LAM, X, LAM);
+}
+
+// FP64 forward + adjoint of one frequency (pivoted cuSOLVER LU, kept for
+// the conjugate-transposed solve).
+int fp64_vjp_one(const Batch& bt, Vjp& vj, const double* d_omega, const double* d_k, double k, int z,
+                 double2* d_F, double2* d_FK)
+{
+    mh_ctx* ctx = bt.ctx;
+    const int64_t n = bt.n;
+    const int nrhs = bt.nrhs;
+    const int64_t nv = n * nrhs;
+    const size_t mat = sizeof(double2) * (size_t)n * (size_t)n;
+    auto* S = (double2*)ws_get(ctx, WS_S, mat);
+    auto* D = (double2*)ws_get(ctx, WS_D, mat);
+    auto* BC = (double2*)ws_get(ctx, WS_RHS, sizeof(double2) * nv);
+    auto* X = (double2*)ws_get(ctx, WS_PHI, sizeof(double2) * nv);
+    auto* piv = (int*)ws_get(ctx, WS_PIV, sizeof(int) * (size_t)n);
+    auto* adj = (double2*)ws_get(ctx, WS_ADJ, sizeof(double2) * nv * 5);
+    if (!S || !D || !BC || !X || !piv || !adj) return MH_ERR_OOM;
+    double2* PB = adj;
+    double2* LAM = adj + nv;
+    double2* BB = adj + 2 * nv;
+    double2* PHI = adj + 3 * nv;
+    int rc;
+    const double* tab = delh_table_for(ctx, bt.mask, &rc);
+    if (rc) return rc;
+    phase_begin(ctx, PH_FP64_ASSEMBLY);
+    MH_CUDA_TRY(ctx, launch_assemble_f64(ctx, bt.m, k, bt.mask, bt.direct, tab, S, D));
+    phase_end(ctx, PH_FP64_ASSEMBLY);
+    MH_CUDA_TRY(ctx, launch_bc_batch(bt, d_omega, 1, BC));
+    phase_begin(ctx, PH_FP64_LU);
+    if ((rc = fp64_lu_factor(ctx, n, D, piv))) return rc;
+    if (bt.direct) {
+        if ((rc = zgemm_strided(ctx, n, nrhs, S, BC, X, 1, 1.0, 0.0))) return rc;
+        if ((rc = fp64_getrs(ctx, false, n, D, piv, X, nrhs))) return rc;
+        MH_CUDA_TRY(ctx, cudaMemcpyAsync(PHI, X, sizeof(double2) * nv, cudaMemcpyDeviceToDevice, ctx->stream));
+    } else {
+        MH_CUDA_TRY(ctx, cudaMemcpyAsync(X, BC, sizeof(double2) * nv, cudaMemcpyDeviceToDevice, ctx->stream));
+        if ((rc = fp64_getrs(ctx, false, n, D, piv, X, nrhs))) return rc;
+        if ((rc = zgemm_strided(ctx, n, nrhs, S, X, PHI, 1, 1.0, 0.0))) return rc;
+    }
+    phase_end(ctx, PH_FP64_LU);
+    MH_CUDA_TRY(ctx, launch_forces_batch(bt, d_omega, 1, PHI, d_F, d_FK));
+    if ((rc = seed_forces(bt, vj, d_omega, 1, z, PHI, PB))) return rc;
+    if (bt.direct) {
+        MH_CUDA_TRY(ctx, cudaMemcpyAsync(LAM, PB, sizeof(double2) * nv, cudaMemcpyDeviceToDevice, ctx->stream));
+    } else if ((rc = zgemm_ct_strided(ctx, n, nrhs, S, PB, LAM, 1, 1.0, 0.0))) {
+        return rc;
+    }
+    if ((rc = fp64_getrs(ctx, true, n, D, piv, LAM, nrhs))) return rc;
+    if (bt.direct) {
+        if ((rc = zgemm_ct_strided(ctx, n, nrhs, S, LAM, BB, 1, 1.0, 0.0))) return rc;
+        return adjoint_tail(bt, vj, d_omega, d_k, 1, z, tab, LAM, BC, LAM, X, BB);
+    }
+    return adjoint_tail(bt, vj, d_omega, d_k, 1, z, tab, PB, X, LAM, X, LAM);
+}
+
+}  // namespace
+
+int hydro_batch_vjp(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double* omegas, int64_t ndof,
+                    const double* dofs, int64_t nbeta, const double* betas, double rho, double g,
+                    uint32_t mask, int direct, int precision, double tol, int max_iter,
+                    const double* bar_added_mass, const double* bar_damping, const double* bar_diffraction,
+                    const double* bar_froude_krylov, double* added_mass, double* damping,
+                    double* diffraction, double* froude_krylov, double* d_vertices, double* d_centers,
+                    double* d_normals, double* d_areas, double* d_radii, double* d_omegas_out,
+                    double* d_dofs_out, mh_batch_info* info)
+{
+    const int64_t n = m->n;
+    const int nrhs = (int)(ndof + nbeta);
+    mh_batch_info local{};
+    // ---- inputs and cotangents to the device ----
+    const size_t dof_bytes = sizeof(double) * 3 * (size_t)n * (size_t)ndof;
+    const size_t in_bytes = dof_bytes + sizeof(double) * (size_t)(2 * nomega + nbeta) + 64;
+    auto* in = (char*)ws_get(ctx, WS_DOF, in_bytes);
+    const size_t out_count = (size_t)nomega * (size_t)(nrhs * ndof + nbeta * ndof);
+    auto* d_out = (double2*)ws_get(ctx, WS_OUT, sizeof(double2) * out_count * 2 + 16);
+    const size_t gb_words = (size_t)GB_NF * n + 3 * (size_t)n * ndof + 2 * (size_t)nomega;
+    auto* gb = (double*)ws_get(ctx, WS_GBAR, sizeof(double) * gb_words);
+    if (!in || !d_out || !gb) return MH_ERR_OOM;
+    auto* d_dofs = (double*)in;
+    auto* d_om = (double*)(in + dof_bytes);
+    auto* d_k = d_om + nomega;
+    auto* d_betas = d_k + nomega;
+    std::vector<double> hk(nomega);
+    for (int64_t z = 0; z < nomega; ++z) hk[z] = omegas[z] * omegas[z] / g;
+    if (ndof) MH_CUDA_TRY(ctx, cudaMemcpyAsync(d_dofs, dofs, dof_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(d_om, omegas, sizeof(double) * nomega, cudaMemcpyHostToDevice, ctx->stream));
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(d_k, hk.data(), sizeof(double) * nomega, cudaMemcpyHostToDevice, ctx->stream));
+    if (nbeta)
+        MH_CUDA_TRY(ctx, cudaMemcpyAsync(d_betas, betas, sizeof(double) * nbeta, cudaMemcpyHostToDevice,
+                                         ctx->stream));
+    // complex force cotangents: c = A-bar / w^2 + i B-bar / w (radiation), F-bar (diffraction)
+    std::vector<double2> hcf((size_t)nomega * nrhs * ndof), hck((size_t)nomega * nbeta * ndof);
+    for (int64_t z = 0; z < nomega; ++z) {
+        const double w = omegas[z];
+        for (int64_t q = 0; q < ndof; ++q)
+            for (int64_t i = 0; i < ndof; ++i) {
+                const size_t o = (size_t)i + (size_t)ndof * ((size_t)q + (size_t)ndof * (size_t)z);
+                const double ab = bar_added_mass ? bar_added_mass[o] : 0.0;
+                const double bb = bar_damping ? bar_damping[o] : 0.0;
+                hcf[((size_t)z * nrhs + q) * ndof + i] = make_double2(ab / (w * w), bb / w);
+            }
+        for (int64_t b = 0; b < nbeta; ++b)
+            for (int64_t i = 0; i < ndof; ++i) {
+                const size_t o = (size_t)i + (size_t)ndof * ((size_t)z + (size_t)nomega * (size_t)b);
+                hcf[((size_t)z * nrhs + ndof + b) * ndof + i] =
+                    bar_diffraction ? make_double2(bar_diffraction[2 * o], bar_diffraction[2 * o + 1])
+                                    : make_double2(0.0, 0.0);
+                hck[((size_t)z * nbeta + b) * ndof + i] =
+                    bar_froude_krylov ? make_double2(bar_froude_krylov[2 * o], bar_froude_krylov[2 * o + 1])
+                                      : make_double2(0.0, 0.0);
+            }
+    }
+    double2* d_F = d_out;
+    double2* d_FK = d_out + (size_t)nomega * nrhs * ndof;
+    double2* d_CF = d_out + out_count;
+    double2* d_CK = d_CF + (size_t)nomega * nrhs * ndof;
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(d_CF, hcf.data(), sizeof(double2) * hcf.size(), cudaMemcpyHostToDevice,
+                                     ctx->stream));
+    if (!hck.empty())
+        MH_CUDA_TRY(ctx, cudaMemcpyAsync(d_CK, hck.data(), sizeof(double2) * hck.size(), cudaMemcpyHostToDevice,
+                                         ctx->stream));
+    MH_CUDA_TRY(ctx, cudaMemsetAsync(gb, 0, sizeof(double) * gb_words, ctx->stream));
+    Vjp vj{};
+    vj.gbar = gb;
+    vj.dofbar = gb + (size_t)GB_NF * n;
+    vj.kbar = vj.dofbar + 3 * (size_t)n * ndof;
+    vj.wbar = vj.kbar + nomega;
+    vj.CF = d_CF;
+    vj.CK = d_CK;
+    vj.rankine = (mask & (MH_GF_RANKINE | MH_GF_RANKINE_REFLECTED | MH_GF_RANKINE_REFLECTED_NEGATIVE)) != 0;
+    vj.nwave = 0;
+    if (mask & MH_GF_WU) vj.wave_kinds[vj.nwave++] = 1;
+    if (mask & MH_GF_DELHOMMEAU) vj.wave_kinds[vj.nwave++] = 2;
+    const size_t nn = (size_t)n * (size_t)n;
+    if (vj.rankine) {
+        vj.WS = (double2*)ws_get(ctx, WS_WSD, sizeof(double2) * nn * 2);
+        if (!vj.WS) return MH_ERR_OOM;
+        vj.WD = vj.WS + nn;
+        MH_CUDA_TRY(ctx, cudaMemsetAsync(vj.WS, 0, sizeof(double2) * nn * 2, ctx->stream));
+    }
+    Batch bt{ctx, m, n, (int)ndof, (int)nbeta, nrhs, d_dofs, d_betas, rho, g, mask, direct};
+    int rc = MH_OK;
+    if (precision == MH_PRECISION_FP64) {
+        vj.part_words = part_words_needed(n, 1);
+        vj.part = (double*)ws_get(ctx, WS_PART, sizeof(double) * vj.part_words);
+        if (!vj.part) return MH_ERR_OOM;
+        for (int64_t z = 0; z < nomega && rc == MH_OK; ++z)
+            rc = fp64_vjp_one(bt, vj, d_om + z, d_k + z, hk[z], (int)z, d_F + z * nrhs * ndof,
+                              d_FK + z * nbeta * ndof);
+    } else {
+        auto* SR = (double*)ws_get(ctx, WS_SR, sizeof(double) * nn * 2);
+        if (!SR) return MH_ERR_OOM;
+        double* DR = SR + nn;
+        if ((rc = rankine_real(bt, SR, DR))) return rc;
+        const size_t per = nn * (2 * sizeof(double2) + sizeof(float2)) +
+                           (size_t)n * nrhs * (10 * sizeof(double2) + 2 * sizeof(float2));
+        constexpr size_t kVjpBatchBytes = 16ull << 30;
+        const int64_t fit = std::min<int64_t>(1024, (int64_t)(kVjpBatchBytes / per));
+        const int chunk = (int)std::max<int64_t>(1, std::min<int64_t>(nomega, fit));
+        vj.part_words = part_words_needed(n, chunk);
+        vj.part = (double*)ws_get(ctx, WS_PART, sizeof(double) * vj.part_words);
+        if (!vj.part) return MH_ERR_OOM;
+        FallbackStore fb;
+        for (int64_t z0 = 0; z0 < nomega && rc == MH_OK; z0 += chunk) {
+            const int nb = (int)std::min<int64_t>(chunk, nomega - z0);
+            fb.lu = nullptr;
+            fb.piv = nullptr;
+            fb.used.assign(nb, 0);
+            rc = run_mixed_chunk(bt, d_om + z0, d_k + z0, nb, SR, DR, tol, max_iter, d_F + z0 * nrhs * ndof,
+                                 d_FK + z0 * nbeta * ndof, &local, &fb);
+            if (rc == MH_OK)
+                rc = adjoint_mixed_chunk(bt, vj, d_om + z0, d_k + z0, nb, (int)z0, tol, max_iter, fb, &local);
+        }
+    }
+    if (rc) return rc;
+    if (vj.rankine) {
+        const unsigned rb = nblk(n, kAR), cb = nblk(n, kAC);
+        double* rowpart = vj.part;
+        double* colpart = rowpart + (size_t)cb * kRowF * n;
+        k_adj_rankine<<<dim3(rb, cb), kAR, 0, ctx->stream>>>(m->geom, n, mask, direct, vj.WS, vj.WD, rowpart,
+                                                             colpart);
+        k_adj_reduce<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, rowpart, (int)cb, colpart, (int)rb, GB_NF,
+                                                            vj.gbar);
+        ctx->launches += 2;
+        MH_CUDA_TRY(ctx, cudaGetLastError());
+    }
+    // ---- results to the host ----
+    std::vector<double2> h(out_count);
+    std::vector<double> hg(gb_words);
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), d_out, sizeof(double2) * out_count, cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(hg.data(), gb, sizeof(double) * gb_words, cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+    MH_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    unpack_outputs(h.data(), nomega, omegas, ndof, nbeta, added_mass, damping, diffraction, froude_krylov);
+    const double* G = hg.data();
+    if (d_centers)
+        for (int c = 0; c < 3; ++c)
+            for (int64_t i = 0; i < n; ++i) d_centers[c * n + i] = G[(GB_C + c) * n + i];
+    if (d_normals)
+        for (int c = 0; c < 3; ++c)
+            for (int64_t i = 0; i < n; ++i) d_normals[c * n + i] = G[(GB_N + c) * n + i];
+    if (d_areas)
+        for (int64_t i = 0; i < n; ++i) d_areas[i] = G[GB_A * n + i];
+    if (d_radii)
+        for (int64_t i = 0; i < n; ++i) d_radii[i] = 0.0;  // radii only select branches
+    if (d_vertices) {
+        const int64_t nvtx = m->nv;
+        std::fill(d_vertices, d_vertices + 3 * nvtx, 0.0);
+        for (int64_t i = 0; i < n; ++i)
+            for (int a = 0; a < 4; ++a) {
+                const int64_t v = m->faces[(size_t)a * n + i];
+                for (int c = 0; c < 3; ++c) d_vertices[c * nvtx + v] += G[(GB_V + 3 * a + c) * n + i];
+            }
+    }
+    if (d_dofs_out)
+        for (int64_t t = 0; t < 3 * n * ndof; ++t) d_dofs_out[t] = G[GB_NF * n + t];
+    if (d_omegas_out) {
+        const double* kb = G + (size_t)GB_NF * n + 3 * (size_t)n * ndof;
+        const double* wb = kb + nomega;
+        for (int64_t z = 0; z < nomega; ++z) {
+            const double w = omegas[z];
+            double s = wb[z] + kb[z] * 2.0 * w / g;
+            // explicit omega of the outputs: A = Re F / w^2, B = Im F / w, F = i rho w sum(...)
+            for (int64_t q = 0; q < nrhs; ++q)
+                for (int64_t i = 0; i < ndof; ++i) {
+                    const double2 F = h[((size_t)z * nrhs + q) * ndof + i];
+                    const double2 c = hcf[((size_t)z * nrhs + q) * ndof + i];
+                    s += (c.x * F.x + c.y * F.y) / w;
+                    if (q < ndof) {
+                        const size_t o = (size_t)i + (size_t)ndof * ((size_t)q + (size_t)ndof * (size_t)z);
+                        const double ab = bar_added_mass ? bar_added_mass[o] : 0.0;
+                        const double bb = bar_damping ? bar_damping[o] : 0.0;
+                        s += ab * (-2.0 * F.x / (w * w * w)) + bb * (-F.y / (w * w));
+                    }
+                }
+            d_omegas_out[z] = s;
+        }
+    }
+    if (info) *info = local;
+    return MH_OK;
+}
+
+}  // namespace mh

@@ -473,6 +473,13 @@ int mh_mesh_create(mh_ctx* ctx, int64_t nfaces, int64_t nvertices, const double*
     m->n = n;
     m->nv = nvertices;
     m->device = ctx->device;
+    try {
+        m->faces.assign(faces, faces + 4 * n);
+    } catch (...) {
+        delete[] h;
+        delete m;
+        return set_err(ctx, MH_ERR_OOM, "host allocation failed");
+    }
     size_t bytes = sizeof(double) * (size_t)G_NFIELDS * (size_t)n;
     cudaError_t e = cudaMalloc(&m->geom, bytes);
     if (e == cudaSuccess) e = cudaMemcpyAsync(m->geom, h, bytes, cudaMemcpyHostToDevice, ctx->stream);
@@ -593,11 +600,13 @@ int mh_diffraction_force(mh_ctx* ctx, const mh_mesh* mesh, double omega, const d
     return MH_OK;
 }
 
-int mh_hydro_batch(mh_ctx* ctx, const mh_mesh* mesh, int64_t n_omega, const double* omegas,
-                   int64_t n_dof, const double* dofs, int64_t n_beta, const double* betas,
-                   double rho, double g, uint32_t gf_mask, int direct, int precision, double tol,
-                   int max_iter, double* added_mass, double* damping, double* diffraction,
-                   double* froude_krylov, mh_batch_info* info)
+}  // extern "C"
+
+namespace {
+
+int check_batch(mh_ctx* ctx, const mh_mesh* mesh, int64_t n_omega, const double* omegas, int64_t n_dof,
+                const double* dofs, int64_t n_beta, const double* betas, double rho, double g,
+                uint32_t gf_mask, int precision, double tol, int max_iter)
 {
     int rc;
     if ((rc = check_ctx(ctx))) return rc;
@@ -622,9 +631,53 @@ int mh_hydro_batch(mh_ctx* ctx, const mh_mesh* mesh, int64_t n_omega, const doub
         if ((gf_mask & MH_GF_WU) && (gf_mask & MH_GF_DELHOMMEAU))
             return set_err(ctx, MH_ERR_ARG, "the mixed path takes one wave term (GFWu or Delhommeau)");
     }
+    return MH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mh_hydro_batch(mh_ctx* ctx, const mh_mesh* mesh, int64_t n_omega, const double* omegas,
+                   int64_t n_dof, const double* dofs, int64_t n_beta, const double* betas,
+                   double rho, double g, uint32_t gf_mask, int direct, int precision, double tol,
+                   int max_iter, double* added_mass, double* damping, double* diffraction,
+                   double* froude_krylov, mh_batch_info* info)
+{
+    int rc;
+    if ((rc = check_batch(ctx, mesh, n_omega, omegas, n_dof, dofs, n_beta, betas, rho, g, gf_mask,
+                          precision, tol, max_iter)))
+        return rc;
     return mh::hydro_batch(ctx, mesh, n_omega, omegas, n_dof, dofs, n_beta, betas, rho, g, gf_mask,
                            direct, precision, tol, max_iter, added_mass, damping, diffraction,
                            froude_krylov, info);
+}
+
+int mh_hydro_batch_vjp(mh_ctx* ctx, const mh_mesh* mesh, int64_t n_omega, const double* omegas,
+                       int64_t n_dof, const double* dofs, int64_t n_beta, const double* betas,
+                       double rho, double g, uint32_t gf_mask, int direct, int precision, double tol,
+                       int max_iter, const double* bar_added_mass, const double* bar_damping,
+                       const double* bar_diffraction, const double* bar_froude_krylov,
+                       double* added_mass, double* damping, double* diffraction,
+                       double* froude_krylov, double* d_vertices, double* d_centers,
+                       double* d_normals, double* d_areas, double* d_radii, double* d_omegas,
+                       double* d_dofs, mh_batch_info* info)
+{
+    int rc;
+    if ((rc = check_batch(ctx, mesh, n_omega, omegas, n_dof, dofs, n_beta, betas, rho, g, gf_mask,
+                          precision, tol, max_iter)))
+        return rc;
+    const int64_t nrad = n_dof * n_dof * n_omega, ndif = 2 * n_dof * n_omega * n_beta;
+    if ((bar_added_mass && !finite_array(bar_added_mass, nrad)) ||
+        (bar_damping && !finite_array(bar_damping, nrad)) ||
+        (bar_diffraction && !finite_array(bar_diffraction, ndif)) ||
+        (bar_froude_krylov && !finite_array(bar_froude_krylov, ndif)))
+        return set_err(ctx, MH_ERR_ARG, "output cotangents must be finite");
+    return mh::hydro_batch_vjp(ctx, mesh, n_omega, omegas, n_dof, dofs, n_beta, betas, rho, g, gf_mask,
+                               direct, precision, tol, max_iter, bar_added_mass, bar_damping,
+                               bar_diffraction, bar_froude_krylov, added_mass, damping, diffraction,
+                               froude_krylov, d_vertices, d_centers, d_normals, d_areas, d_radii,
+                               d_omegas, d_dofs, info);
 }
 
 }  // extern "C"

@@ -395,19 +395,9 @@ k_rel_residual(const double2* __restrict__ r, const double2* __restrict__ b, int
 // host orchestration
 // ---------------------------------------------------------------------------
 
-struct Batch {
-    mh_ctx* ctx;
-    const mh_mesh* m;
-    int64_t n;
-    int ndof, nbeta, nrhs;
-    const double* d_dofs;
-    const double* d_betas;
-    double rho, g;
-    uint32_t mask;
-    int direct;
-};
-
 unsigned blocks(int64_t count, int threads) { return (unsigned)((count + threads - 1) / threads); }
+
+}  // namespace
 
 int zgemm_strided(mh_ctx* ctx, int64_t n, int nrhs, const double2* A, const double2* B, double2* C,
                   int nb, double alpha_re, double beta_re)
@@ -423,7 +413,7 @@ int zgemm_strided(mh_ctx* ctx, int64_t n, int nrhs, const double2* A, const doub
     return MH_OK;
 }
 
-int fp64_lu_solve(mh_ctx* ctx, int64_t n, double2* A, double2* B, int nrhs)
+int fp64_lu_factor(mh_ctx* ctx, int64_t n, double2* A, int* piv)
 {
     int lwork = 0;
     cusolverStatus_t st = cusolverDnZgetrf_bufferSize(ctx->cusolver, (int)n, (int)n,
@@ -431,22 +421,41 @@ int fp64_lu_solve(mh_ctx* ctx, int64_t n, double2* A, double2* B, int nrhs)
     if (st != CUSOLVER_STATUS_SUCCESS)
         return set_err(ctx, MH_ERR_CUDA, "cusolverDnZgetrf_bufferSize failed (%d)", (int)st);
     auto* work = (cuDoubleComplex*)ws_get(ctx, WS_LWORK, sizeof(cuDoubleComplex) * (size_t)lwork);
-    auto* piv = (int*)ws_get(ctx, WS_PIV, sizeof(int) * (size_t)n);
     auto* info = (int*)ws_get(ctx, WS_INFO, sizeof(int) * 2);
-    if (!work || !piv || !info) return MH_ERR_OOM;
+    if (!work || !info) return MH_ERR_OOM;
     st = cusolverDnZgetrf(ctx->cusolver, (int)n, (int)n, (cuDoubleComplex*)A, (int)n, work, piv, info);
     if (st != CUSOLVER_STATUS_SUCCESS)
         return set_err(ctx, MH_ERR_CUDA, "cusolverDnZgetrf failed (%d)", (int)st);
-    st = cusolverDnZgetrs(ctx->cusolver, CUBLAS_OP_N, (int)n, nrhs, (const cuDoubleComplex*)A, (int)n,
-                          piv, (cuDoubleComplex*)B, (int)n, info + 1);
-    if (st != CUSOLVER_STATUS_SUCCESS)
-        return set_err(ctx, MH_ERR_CUDA, "cusolverDnZgetrs failed (%d)", (int)st);
-    int h[2] = {0, 0};
-    MH_CUDA_TRY(ctx, cudaMemcpyAsync(h, info, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    int h = 0;
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(&h, info, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
     MH_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-    if (h[0] > 0) return set_err(ctx, MH_ERR_SINGULAR, "zero pivot at column %d", h[0]);
+    if (h > 0) return set_err(ctx, MH_ERR_SINGULAR, "zero pivot at column %d", h);
     return MH_OK;
 }
+
+int fp64_getrs(mh_ctx* ctx, bool conj_trans, int64_t n, const double2* LU, const int* piv, double2* B,
+               int nrhs)
+{
+    auto* info = (int*)ws_get(ctx, WS_INFO, sizeof(int) * 2);
+    if (!info) return MH_ERR_OOM;
+    cusolverStatus_t st = cusolverDnZgetrs(ctx->cusolver, conj_trans ? CUBLAS_OP_C : CUBLAS_OP_N,
+                                           (int)n, nrhs, (const cuDoubleComplex*)LU, (int)n, piv,
+                                           (cuDoubleComplex*)B, (int)n, info + 1);
+    if (st != CUSOLVER_STATUS_SUCCESS)
+        return set_err(ctx, MH_ERR_CUDA, "cusolverDnZgetrs failed (%d)", (int)st);
+    return MH_OK;
+}
+
+int fp64_lu_solve(mh_ctx* ctx, int64_t n, double2* A, double2* B, int nrhs)
+{
+    auto* piv = (int*)ws_get(ctx, WS_PIV, sizeof(int) * (size_t)n);
+    if (!piv) return MH_ERR_OOM;
+    int rc = fp64_lu_factor(ctx, n, A, piv);
+    if (rc) return rc;
+    return fp64_getrs(ctx, false, n, A, piv, B, nrhs);
+}
+
+namespace {
 
 // FP64 path: one frequency at a time.
 int run_fp64(const Batch& bt, const double* d_omegas, int nomega, double2* d_F, double2* d_FK)
@@ -495,10 +504,12 @@ int run_fp64(const Batch& bt, const double* d_omegas, int nomega, double2* d_F, 
     return MH_OK;
 }
 
+}  // namespace
+
 // Mixed path for one chunk of `nb` frequencies.
 int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, int nb,
                     const double* SR, const double* DR, double tol, int max_iter, double2* d_F,
-                    double2* d_FK, mh_batch_info* info)
+                    double2* d_FK, mh_batch_info* info, FallbackStore* fb)
 {
     mh_ctx* ctx = bt.ctx;
     const int64_t n = bt.n, nn = n * n;
@@ -612,7 +623,13 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
         double2* Xz = X + (int64_t)z * nv;
         MH_CUDA_TRY(ctx, cudaMemcpyAsync(Xz, RHS + (int64_t)z * nv, sizeof(double2) * nv,
                                          cudaMemcpyDeviceToDevice, ctx->stream));
-        if ((rc = fp64_lu_solve(ctx, n, D64 + (int64_t)z * nn, Xz, nrhs))) return rc;
+        if (fb) {  // keep D: factor a copy and keep its pivots for the adjoint solve
+            if ((rc = fallback_factor(ctx, fb, n, nb, z, D64 + (int64_t)z * nn))) return rc;
+            if ((rc = fp64_getrs(ctx, false, n, fb->lu + (int64_t)z * nn, fb->piv + z * n, Xz, nrhs)))
+                return rc;
+        } else if ((rc = fp64_lu_solve(ctx, n, D64 + (int64_t)z * nn, Xz, nrhs))) {
+            return rc;
+        }
     }
     // indirect: phi = S sigma
     double2* PHI = X;
@@ -629,13 +646,104 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
     return MH_OK;
 }
 
-}  // namespace
+int fallback_factor(mh_ctx* ctx, FallbackStore* fb, int64_t n, int nb, int z, const double2* D)
+{
+    const int64_t nn = n * n;
+    if (!fb->lu) {
+        fb->lu = (double2*)ws_get(ctx, WS_FB, sizeof(double2) * nn * nb + sizeof(int) * n * nb);
+        if (!fb->lu) return MH_ERR_OOM;
+        fb->piv = (int*)(fb->lu + nn * nb);
+    }
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(fb->lu + (int64_t)z * nn, D, sizeof(double2) * nn,
+                                     cudaMemcpyDeviceToDevice, ctx->stream));
+    fb->used[z] = 1;
+    return fp64_lu_factor(ctx, n, fb->lu + (int64_t)z * nn, fb->piv + (int64_t)z * n);
+}
+
+int rankine_real(const Batch& bt, double* SR, double* DR)
+{
+    mh_ctx* ctx = bt.ctx;
+    const int64_t n = bt.n;
+    phase_begin(ctx, PH_RANKINE);
+    k_rankine_real<<<dim3(blocks(n, kRows), blocks(n, kCols)), kRows, 0, ctx->stream>>>(
+        bt.m->geom, n, bt.mask & (MH_GF_RANKINE | MH_GF_RANKINE_REFLECTED |
+                                  MH_GF_RANKINE_REFLECTED_NEGATIVE), bt.direct, SR, DR);
+    ctx->launches += 1;
+    phase_end(ctx, PH_RANKINE);
+    MH_CUDA_TRY(ctx, cudaGetLastError());
+    return MH_OK;
+}
+
+cudaError_t launch_bc_batch(const Batch& bt, const double* d_omegas, int nb, double2* BC)
+{
+    k_bc_batch<<<dim3(blocks(bt.n, 256), (unsigned)nb), 256, 0, bt.ctx->stream>>>(
+        bt.m->geom, bt.n, bt.d_dofs, bt.ndof, bt.d_betas, bt.nbeta, d_omegas, bt.g, BC);
+    bt.ctx->launches += 1;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_forces_batch(const Batch& bt, const double* d_omegas, int nb, const double2* PHI,
+                                double2* d_F, double2* d_FK)
+{
+    k_forces_batch<<<nb * bt.nrhs, 256, 0, bt.ctx->stream>>>(bt.m->geom, bt.n, bt.d_dofs, bt.ndof,
+                                                             bt.d_betas, bt.nbeta, d_omegas, bt.rho,
+                                                             bt.g, PHI, d_F, d_FK);
+    bt.ctx->launches += 1;
+    return cudaGetLastError();
+}
 
 cudaError_t launch_to_f32(mh_ctx* ctx, const double2* a, float2* b, int64_t count)
 {
     k_to_f32<<<blocks(count, 256), 256, 0, ctx->stream>>>(a, b, count);
     ctx->launches += 1;
     return cudaGetLastError();
+}
+
+cudaError_t launch_add_f32(mh_ctx* ctx, double2* x, const float2* d, int64_t count)
+{
+    k_add_f32<<<blocks(count, 256), 256, 0, ctx->stream>>>(x, d, count);
+    ctx->launches += 1;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rel_residual(mh_ctx* ctx, const double2* r, const double2* b, int64_t n, int nrhs,
+                                int nb, double* out)
+{
+    k_rel_residual<<<nb, 256, 0, ctx->stream>>>(r, b, n, nrhs, out);
+    ctx->launches += 1;
+    return cudaGetLastError();
+}
+
+void unpack_outputs(const double2* h, int64_t nomega, const double* omegas, int64_t ndof, int64_t nbeta,
+                    double* added_mass, double* damping, double* diffraction, double* froude_krylov)
+{
+    const int64_t nrhs = ndof + nbeta;
+    // outputs in the reference's layout (src/problems_and_results.jl:137-165):
+    // added_mass[i, j, w] (i influenced, j radiating), diffraction[i, w, b]
+    for (int64_t z = 0; z < nomega; ++z) {
+        const double w = omegas[z];
+        for (int64_t jq = 0; jq < ndof; ++jq)
+            for (int64_t i = 0; i < ndof; ++i) {
+                double2 F = h[((size_t)z * nrhs + jq) * ndof + i];
+                size_t o = (size_t)i + (size_t)ndof * ((size_t)jq + (size_t)ndof * (size_t)z);
+                if (added_mass) added_mass[o] = F.x / (w * w);
+                if (damping) damping[o] = F.y / w;
+            }
+        for (int64_t b = 0; b < nbeta; ++b)
+            for (int64_t i = 0; i < ndof; ++i) {
+                double2 F = h[((size_t)z * nrhs + ndof + b) * ndof + i];
+                double2 K = h[(size_t)nomega * nrhs * ndof + ((size_t)z * nbeta + b) * ndof + i];
+                size_t o = (size_t)i + (size_t)ndof * ((size_t)z + (size_t)nomega * (size_t)b);
+                if (diffraction) {
+                    diffraction[2 * o] = F.x;
+                    diffraction[2 * o + 1] = F.y;
+                }
+                if (froude_krylov) {
+                    froude_krylov[2 * o] = K.x;
+                    froude_krylov[2 * o + 1] = K.y;
+                }
+            }
+    }
 }
 
 int hydro_batch(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double* omegas, int64_t ndof,
@@ -679,20 +787,14 @@ int hydro_batch(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double* ome
         auto* SR = (double*)ws_get(ctx, WS_SR, sizeof(double) * nn * 2);
         if (!SR) return MH_ERR_OOM;
         double* DR = SR + nn;
-        phase_begin(ctx, PH_RANKINE);
-        k_rankine_real<<<dim3(blocks(n, kRows), blocks(n, kCols)), kRows, 0, ctx->stream>>>(
-            m->geom, n, mask & (MH_GF_RANKINE | MH_GF_RANKINE_REFLECTED |
-                                MH_GF_RANKINE_REFLECTED_NEGATIVE), direct, SR, DR);
-        ctx->launches += 1;
-        phase_end(ctx, PH_RANKINE);
-        MH_CUDA_TRY(ctx, cudaGetLastError());
+        if ((rc = rankine_real(bt, SR, DR))) return rc;
         const size_t per = nn * (2 * sizeof(double2) + sizeof(float2)) +
                            (size_t)n * nrhs * (5 * sizeof(double2) + sizeof(float2));
         const int chunk = (int)std::max<int64_t>(1, std::min<int64_t>(nomega, kBatchBytes / per));
         for (int64_t z0 = 0; z0 < nomega && rc == MH_OK; z0 += chunk) {
             const int nb = (int)std::min<int64_t>(chunk, nomega - z0);
             rc = run_mixed_chunk(bt, d_omegas + z0, d_k + z0, nb, SR, DR, tol, max_iter,
-                                 d_F + z0 * nrhs * ndof, d_FK + z0 * nbeta * ndof, &local);
+                                 d_F + z0 * nrhs * ndof, d_FK + z0 * nbeta * ndof, &local, nullptr);
         }
     }
     if (rc) return rc;
@@ -701,32 +803,8 @@ int hydro_batch(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double* ome
     MH_CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), d_out, sizeof(double2) * out_count,
                                      cudaMemcpyDeviceToHost, ctx->stream));
     MH_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-    // outputs in the reference's layout (src/problems_and_results.jl:137-165):
-    // added_mass[i, j, w] (i influenced, j radiating), diffraction[i, w, b]
-    for (int64_t z = 0; z < nomega; ++z) {
-        const double w = omegas[z];
-        for (int64_t jq = 0; jq < ndof; ++jq)
-            for (int64_t i = 0; i < ndof; ++i) {
-                double2 F = h[((size_t)z * nrhs + jq) * ndof + i];
-                size_t o = (size_t)i + (size_t)ndof * ((size_t)jq + (size_t)ndof * (size_t)z);
-                if (added_mass) added_mass[o] = F.x / (w * w);
-                if (damping) damping[o] = F.y / w;
-            }
-        for (int64_t b = 0; b < nbeta; ++b)
-            for (int64_t i = 0; i < ndof; ++i) {
-                double2 F = h[((size_t)z * nrhs + ndof + b) * ndof + i];
-                double2 K = h[(size_t)nomega * nrhs * ndof + ((size_t)z * nbeta + b) * ndof + i];
-                size_t o = (size_t)i + (size_t)ndof * ((size_t)z + (size_t)nomega * (size_t)b);
-                if (diffraction) {
-                    diffraction[2 * o] = F.x;
-                    diffraction[2 * o + 1] = F.y;
-                }
-                if (froude_krylov) {
-                    froude_krylov[2 * o] = K.x;
-                    froude_krylov[2 * o + 1] = K.y;
-                }
-            }
-    }
+    unpack_outputs(h.data(), nomega, omegas, ndof, nbeta, added_mass, damping, diffraction,
+                   froude_krylov);
     if (info) *info = local;
     return MH_OK;
 }

@@ -15,30 +15,41 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "marinehydro_b200.h"
+#include "mh_dual.cuh"
 
 namespace mh {
 
 constexpr double kPi = 3.14159265358979323846264338327950288;
 constexpr double kEulerGamma = 0.57721566490153286060651209008240243;
 
-struct cplx {
-    double re, im;
+template <class T>
+struct cx {
+    T re, im;
 };
+using cplx = cx<double>;
 
 __device__ __forceinline__ cplx mk(double r, double i) { return cplx{r, i}; }
-__device__ __forceinline__ cplx operator+(cplx a, cplx b) { return {a.re + b.re, a.im + b.im}; }
-__device__ __forceinline__ cplx operator-(cplx a, cplx b) { return {a.re - b.re, a.im - b.im}; }
-__device__ __forceinline__ cplx operator-(cplx a) { return {-a.re, -a.im}; }
-__device__ __forceinline__ cplx operator*(cplx a, cplx b)
+template <class T>
+__device__ __forceinline__ cx<T> operator+(const cx<T>& a, const cx<T>& b) { return {a.re + b.re, a.im + b.im}; }
+template <class T>
+__device__ __forceinline__ cx<T> operator-(const cx<T>& a, const cx<T>& b) { return {a.re - b.re, a.im - b.im}; }
+template <class T>
+__device__ __forceinline__ cx<T> operator-(const cx<T>& a) { return {-a.re, -a.im}; }
+template <class T>
+__device__ __forceinline__ cx<T> operator*(const cx<T>& a, const cx<T>& b)
 {
     return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
 }
-__device__ __forceinline__ cplx operator*(double s, cplx a) { return {s * a.re, s * a.im}; }
-__device__ __forceinline__ cplx operator*(cplx a, double s) { return {s * a.re, s * a.im}; }
-__device__ __forceinline__ cplx operator/(cplx a, double s) { return {a.re / s, a.im / s}; }
+template <class T>
+__device__ __forceinline__ cx<T> operator*(T s, const cx<T>& a) { return {s * a.re, s * a.im}; }
+template <class T>
+__device__ __forceinline__ cx<T> operator*(const cx<T>& a, T s) { return {s * a.re, s * a.im}; }
+__device__ __forceinline__ cplx operator/(const cplx& a, double s) { return {a.re / s, a.im / s}; }
 // Smith's algorithm for complex division.
-__device__ __forceinline__ cplx operator/(cplx a, cplx b)
+__device__ __forceinline__ cplx operator/(const cplx& a, const cplx& b)
 {
     if (fabs(b.re) >= fabs(b.im)) {
         double r = b.im / b.re, d = b.re + b.im * r;
@@ -55,6 +66,18 @@ __device__ __forceinline__ cplx cexp_(cplx a)
     return {e * c, e * s};
 }
 __device__ __forceinline__ cplx clog_(cplx a) { return {log(cabs_(a)), atan2(a.im, a.re)}; }
+
+// constant of the scalar type (double or dual number)
+__device__ __forceinline__ void tset(double& r, double v) { r = v; }
+template <int ND>
+__device__ __forceinline__ void tset(dualn<ND>& r, double v) { r = dconst<ND>(v); }
+template <class T>
+__device__ __forceinline__ T tconst(double v)
+{
+    T r;
+    tset(r, v);
+    return r;
+}
 
 // ---------------------------------------------------------------------------
 // complex E1
@@ -108,15 +131,18 @@ __device__ __forceinline__ cplx expint_e1(cplx z)
 // Rankine panel integrals
 // ---------------------------------------------------------------------------
 
-struct Panel {
-    double c[3];   // centre
-    double n[3];   // unit normal
-    double v[12];  // 4 vertices, v[3*a + coord]
-    double area;
-    double radius;
+template <class T>
+struct PanelT {
+    T c[3];   // centre
+    T n[3];   // unit normal
+    T v[12];  // 4 vertices, v[3*a + coord]
+    T area;
+    T radius;
 };
+using Panel = PanelT<double>;
 
-__device__ __forceinline__ double dot3(const double* a, const double* b)
+template <class T>
+__device__ __forceinline__ T dot3(const T* a, const T* b)
 {
     return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
 }
@@ -126,27 +152,28 @@ __device__ __forceinline__ double signd(double v) { return (double)((v > 0) - (v
 // both_integral_and_integral_gradient(::Rankine) (rankine.jl:65-123),
 // computed in one pass over the panel edges.  The gradient is w.r.t. the
 // source point; callers negate it for with_respect_to_first_variable.
-__device__ __forceinline__ void rankine_pair(const double x[3], const Panel& p,
-                                             double& integral, double grad[3])
+template <class T>
+__device__ __forceinline__ void rankine_pair(const T x[3], const PanelT<T>& p, T& integral, T grad[3])
 {
-    double rb[3] = {x[0] - p.c[0], x[1] - p.c[1], x[2] - p.c[2]};
-    double r = sqrt(dot3(rb, rb));
-    if (r > 7.0 * p.radius) {
-        double inv3 = 1.0 / (r * r * r);
+    T rb[3] = {x[0] - p.c[0], x[1] - p.c[1], x[2] - p.c[2]};
+    T r = sqrt(dot3(rb, rb));
+    if (val(r) > 7.0 * val(p.radius)) {
+        T inv3 = 1.0 / (r * r * r);
         integral = p.area / r;
         grad[0] = rb[0] * inv3 * p.area;
         grad[1] = rb[1] * inv3 * p.area;
         grad[2] = rb[2] * inv3 * p.area;
         return;
     }
-    double I = 0.0, g0 = 0.0, g1 = 0.0, g2 = 0.0;
-    double GZ = dot3(rb, p.n);
-    double aGZ = fabs(GZ), sg = signd(GZ);
-    bool use_at = aGZ >= 1e-4 * p.radius;
-    double RR[4], DRX[4][3];
+    T I = tconst<T>(0.0), g0 = tconst<T>(0.0), g1 = tconst<T>(0.0), g2 = tconst<T>(0.0);
+    T GZ = dot3(rb, p.n);
+    T aGZ = fabs(GZ);
+    double sg = signd(val(GZ));
+    bool use_at = val(aGZ) >= 1e-4 * val(p.radius);
+    T RR[4], DRX[4][3];
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
-        double d0 = x[0] - p.v[3 * a], d1 = x[1] - p.v[3 * a + 1], d2 = x[2] - p.v[3 * a + 2];
+        T d0 = x[0] - p.v[3 * a], d1 = x[1] - p.v[3 * a + 1], d2 = x[2] - p.v[3 * a + 2];
         RR[a] = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
         DRX[a][0] = d0 / RR[a];
         DRX[a][1] = d1 / RR[a];
@@ -155,35 +182,35 @@ __device__ __forceinline__ void rankine_pair(const double x[3], const Panel& p,
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
         const int b = (a + 1) & 3;
-        double e0 = p.v[3 * b] - p.v[3 * a], e1 = p.v[3 * b + 1] - p.v[3 * a + 1],
-               e2 = p.v[3 * b + 2] - p.v[3 * a + 2];
-        double L = sqrt(e0 * e0 + e1 * e1 + e2 * e2);
-        if (L >= 1e-3 * p.radius) {
-            double u0 = e0 / L, u1 = e1 / L, u2 = e2 / L;
-            double GYX[3] = {p.n[1] * u2 - p.n[2] * u1, p.n[2] * u0 - p.n[0] * u2,
-                             p.n[0] * u1 - p.n[1] * u0};
-            double pa[3] = {x[0] - p.v[3 * a], x[1] - p.v[3 * a + 1], x[2] - p.v[3 * a + 2]};
-            double GY = dot3(pa, GYX);
-            double s = RR[b] + RR[a];
-            double ANT = 2.0 * GY * L;
-            double DNT = s * s - L * L + 2.0 * aGZ * s;
-            double ANL = s + L;
-            double DNL = s - L;
-            double ALDEN = log(ANL / DNL);
-            double AT = use_at ? atan2(ANT, DNT) : 0.0;
+        T e0 = p.v[3 * b] - p.v[3 * a], e1 = p.v[3 * b + 1] - p.v[3 * a + 1],
+          e2 = p.v[3 * b + 2] - p.v[3 * a + 2];
+        T L = sqrt(e0 * e0 + e1 * e1 + e2 * e2);
+        if (val(L) >= 1e-3 * val(p.radius)) {
+            T u0 = e0 / L, u1 = e1 / L, u2 = e2 / L;
+            T GYX[3] = {p.n[1] * u2 - p.n[2] * u1, p.n[2] * u0 - p.n[0] * u2,
+                        p.n[0] * u1 - p.n[1] * u0};
+            T pa[3] = {x[0] - p.v[3 * a], x[1] - p.v[3 * a + 1], x[2] - p.v[3 * a + 2]};
+            T GY = dot3(pa, GYX);
+            T s = RR[b] + RR[a];
+            T ANT = 2.0 * GY * L;
+            T DNT = s * s - L * L + 2.0 * aGZ * s;
+            T ANL = s + L;
+            T DNL = s - L;
+            T ALDEN = log(ANL / DNL);
+            T AT = use_at ? atan2(ANT, DNT) : tconst<T>(0.0);
             // integral(): solid-angle term and log term with their own guards
             if (use_at) I -= 2.0 * aGZ * AT;
-            if (fabs(GY) > 1e-5) I += GY * ALDEN;
+            if (fabs(val(GY)) > 1e-5) I += GY * ALDEN;
             // gradient (rankine.jl:97-110)
-            double q = GY * (DNL - ANL) / (ANL * DNL);
-            double den = ANT * ANT + DNT * DNT;
-            double gg[3];
+            T q = GY * (DNL - ANL) / (ANL * DNL);
+            T den = ANT * ANT + DNT * DNT;
+            T gg[3];
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                double ANLX = DRX[b][c] + DRX[a][c];
-                double ANTX = 2.0 * L * GYX[c];
-                double DNTX = 2.0 * (s + aGZ) * ANLX + 2.0 * sg * s * p.n[c];
-                gg[c] = ALDEN * GYX[c] - 2.0 * sg * AT * p.n[c] + q * ANLX
+                T ANLX = DRX[b][c] + DRX[a][c];
+                T ANTX = 2.0 * L * GYX[c];
+                T DNTX = 2.0 * (s + aGZ) * ANLX + (2.0 * sg) * s * p.n[c];
+                gg[c] = ALDEN * GYX[c] - (2.0 * sg) * AT * p.n[c] + q * ANLX
                         - 2.0 * aGZ * (ANTX * DNT - DNTX * ANT) / den;
             }
             g0 -= gg[0];
@@ -201,17 +228,19 @@ __device__ __forceinline__ void rankine_pair(const double x[3], const Panel& p,
 // Wu et al. wave term (wu.jl)
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ double wu_dFuncC(double t)  // wu.jl:51-66
+template <class T>
+__device__ __forceinline__ T wu_dFuncC(const T& t)  // wu.jl:51-66
 {
-    double g = (3168.35 + -1590.27 * t) * t;
+    T g = (3168.35 + -1590.27 * t) * t;
     g = (-2318.58 + g) * t;
     g = (847.8 + g) * t;
     g = (-148.24 + g) * t;
     return 14.19 + g;
 }
-__device__ __forceinline__ double wu_dFuncB(double t)  // wu.jl:69-92
+template <class T>
+__device__ __forceinline__ T wu_dFuncB(const T& t)  // wu.jl:69-92
 {
-    double g = (-76209.82 + 19923.28 * t) * t;
+    T g = (-76209.82 + 19923.28 * t) * t;
     g = (118879.26 + g) * t;
     g = (-97014.11 + g) * t;
     g = (44270.15 + g) * t;
@@ -221,9 +250,10 @@ __device__ __forceinline__ double wu_dFuncB(double t)  // wu.jl:69-92
     g = (2.894 + g) * t;
     return 1.11 + g;
 }
-__device__ __forceinline__ double wu_dFuncA(double t)  // wu.jl:94-117
+template <class T>
+__device__ __forceinline__ T wu_dFuncA(const T& t)  // wu.jl:94-117
 {
-    double g = (-46688.0 + 12622.25 * t) * t;
+    T g = (-46688.0 + 12622.25 * t) * t;
     g = (68220.87 + g) * t;
     g = (-48811.41 + g) * t;
     g = (16370.75 + g) * t;
@@ -233,9 +263,10 @@ __device__ __forceinline__ double wu_dFuncA(double t)  // wu.jl:94-117
     g = (-24.53 + g) * t;
     return 2.948 + g;
 }
-__device__ __forceinline__ double wu_FuncD(double t)  // wu.jl:159-182
+template <class T>
+__device__ __forceinline__ T wu_FuncD(const T& t)  // wu.jl:159-182
 {
-    double g = (128170.2 + -33744.6 * t) * t;
+    T g = (128170.2 + -33744.6 * t) * t;
     g = (-205690.43 + g) * t;
     g = (181856.75 + g) * t;
     g = (-96293.05 + g) * t;
@@ -245,9 +276,10 @@ __device__ __forceinline__ double wu_FuncD(double t)  // wu.jl:159-182
     g = (-40.97 + g) * t;
     return 0.632 + g;
 }
-__device__ __forceinline__ double wu_FuncC(double t)  // wu.jl:184-203
+template <class T>
+__device__ __forceinline__ T wu_FuncC(const T& t)  // wu.jl:184-203
 {
-    double g = (9136.4 + -3272.62 * t) * t;
+    T g = (9136.4 + -3272.62 * t) * t;
     g = (-9844.35 + g) * t;
     g = (5155.67 + g) * t;
     g = (-1397.89 + g) * t;
@@ -255,9 +287,10 @@ __device__ __forceinline__ double wu_FuncC(double t)  // wu.jl:184-203
     g = (-9.747 + g) * t;
     return 1.268 + g;
 }
-__device__ __forceinline__ double wu_FuncB(double t)  // wu.jl:205-228
+template <class T>
+__device__ __forceinline__ T wu_FuncB(const T& t)  // wu.jl:205-228
 {
-    double g = (-29030.24 + 7671.22 * t) * t;
+    T g = (-29030.24 + 7671.22 * t) * t;
     g = (44894.06 + g) * t;
     g = (-36618.81 + g) * t;
     g = (17137.74 + g) * t;
@@ -267,9 +300,10 @@ __device__ __forceinline__ double wu_FuncB(double t)  // wu.jl:205-228
     g = (5.737 + g) * t;
     return 0.938 + g;
 }
-__device__ __forceinline__ double wu_FuncA(double t)  // wu.jl:230-253
+template <class T>
+__device__ __forceinline__ T wu_FuncA(const T& t)  // wu.jl:230-253
 {
-    double g = (21859.0 + -4838.6 * t) * t;
+    T g = (21859.0 + -4838.6 * t) * t;
     g = (-41592.9 + g) * t;
     g = (42002.57 + g) * t;
     g = (-24314.21 + g) * t;
@@ -280,72 +314,75 @@ __device__ __forceinline__ double wu_FuncA(double t)  // wu.jl:230-253
     return 1.21 + g;
 }
 
-__device__ __forceinline__ double struve_h0(double xx)  // wu.jl:295-327
+template <class T>
+__device__ __forceinline__ T struve_h0(const T& xx)  // wu.jl:295-327
 {
-    if (xx <= 3.0) {
-        double yy = (xx / 3.0) * (xx / 3.0);
-        double h = 1.909859164 + (-1.909855001 + (0.687514637 + (-0.126164557
+    if (val(xx) <= 3.0) {
+        T yy = (xx / 3.0) * (xx / 3.0);
+        T h = 1.909859164 + (-1.909855001 + (0.687514637 + (-0.126164557
                    + (0.013828813 + -0.000876918 * yy) * yy) * yy) * yy) * yy;
         return h * (xx / 3.0);
     }
-    double yy = (3.0 / xx) * (3.0 / xx);
-    double c1 = 2.0 * (0.99999906 + (4.77228920 + (3.85542044 + 0.32303607 * yy) * yy) * yy);
-    double c2 = kPi * xx * (1.0 + (4.88331068 + (4.28957333 + 0.52120508 * yy) * yy) * yy);
+    T yy = (3.0 / xx) * (3.0 / xx);
+    T c1 = 2.0 * (0.99999906 + (4.77228920 + (3.85542044 + 0.32303607 * yy) * yy) * yy);
+    T c2 = kPi * xx * (1.0 + (4.88331068 + (4.28957333 + 0.52120508 * yy) * yy) * yy);
     return c1 / c2 + y0(xx);
 }
 
-__device__ __forceinline__ double struve_h1(double xx)  // wu.jl:331-362
+template <class T>
+__device__ __forceinline__ T struve_h1(const T& xx)  // wu.jl:331-362
 {
-    if (xx <= 3.0) {
-        double yy = (xx / 3.0) * (xx / 3.0);
+    if (val(xx) <= 3.0) {
+        T yy = (xx / 3.0) * (xx / 3.0);
         return (1.909859286 + (-1.145914713 + (0.294656958 + (-0.042070508
                 + (0.003785727 + -0.000207183 * yy) * yy) * yy) * yy) * yy) * yy;
     }
-    double yy = (3.0 / xx) * (3.0 / xx);
-    double c1 = 2.0 * (1.00000004 + (3.92205313 + (2.64893033 + 0.27450895 * yy) * yy) * yy);
-    double c2 = kPi * (1.0 + (3.81095112 + (2.26216956 + 0.10885141 * yy) * yy) * yy);
+    T yy = (3.0 / xx) * (3.0 / xx);
+    T c1 = 2.0 * (1.00000004 + (3.92205313 + (2.64893033 + 0.27450895 * yy) * yy) * yy);
+    T c2 = kPi * (1.0 + (3.81095112 + (2.26216956 + 0.10885141 * yy) * yy) * yy);
     return c1 / c2 + y1(xx);
 }
 
 // (G, dG/dh, dG/dv) of the Wu wave term, wu.jl:19-30; out = 3 complex.
-__device__ __forceinline__ void wu_dimless(double hh, double vv, cplx out[3])
+template <class T>
+__device__ __forceinline__ void wu_dimless(const T& hh, const T& vv, cx<T> out[3])
 {
-    double dd = sqrt(hh * hh + vv * vv);
-    double alpha = -vv / dd;
-    double beta = hh / dd;
-    double rho = dd / (1.0 + dd);
-    double ev = exp(vv);
-    double om = 1.0 - rho;
-    double om3 = om * om * om;
-    double dd3 = dd * dd * dd;
+    T dd = sqrt(hh * hh + vv * vv);
+    T alpha = -vv / dd;
+    T beta = hh / dd;
+    T rho = dd / (1.0 + dd);
+    T ev = exp(vv);
+    T om = 1.0 - rho;
+    T om3 = om * om * om;
+    T dd3 = dd * dd * dd;
     // GF_Func_Lp / GF_Func_L0 (wu.jl:266-293)
-    double RR = (1.0 - beta) * wu_FuncA(rho);
+    T RR = (1.0 - beta) * wu_FuncA(rho);
     RR -= beta * wu_FuncB(rho);
     RR -= alpha * wu_FuncC(rho) / (1.0 + 6.0 * alpha * rho * (1.0 - rho));
     RR += beta * (1.0 - beta) * wu_FuncD(rho);
-    double Lp = rho * om3 * RR;
+    T Lp = rho * om3 * RR;
     const double gama = 0.5772156649;
-    double PP = log(0.5 * (dd - vv)) + gama - 2.0 * dd * dd;
+    T PP = log(0.5 * (dd - vv)) + gama - 2.0 * dd * dd;
     PP = ev * PP;
     PP = PP + dd * dd - vv;
-    double L0 = 2.0 * PP / (1.0 + dd3) + 2.0 * Lp;
+    T L0 = 2.0 * PP / (1.0 + dd3) + 2.0 * Lp;
     // GF_Func_Lsp / GF_Func_Ls (wu.jl:131-157)
-    double RS = beta * wu_dFuncA(rho);
+    T RS = beta * wu_dFuncA(rho);
     RS -= (1.0 - alpha) * wu_dFuncB(rho);
     RS += beta * (1.0 - beta) * rho * (1.0 - 2.0 * rho) * wu_dFuncC(rho);
-    double Lsp = rho * om3 * RS;
-    double PS = (beta + hh) / (dd - vv);
+    T Lsp = rho * om3 * RS;
+    T PS = (beta + hh) / (dd - vv);
     PS = PS - 2.0 * beta + 2.0 * ev * dd - hh;
-    double QS = exp(-dd) * (1.0 - beta);
+    T QS = exp(-dd) * (1.0 - beta);
     QS = QS * (1.0 + dd / (1.0 + dd3));
-    double Ls = 2.0 * PS / (1.0 + dd3) - 4.0 * QS + 2.0 * Lsp;
+    T Ls = 2.0 * PS / (1.0 + dd3) - 4.0 * QS + 2.0 * Lsp;
     // W, Wh (wu.jl:122-129, :257-264)
-    double H0 = struve_h0(hh), J0 = j0(hh), H1 = struve_h1(hh), J1 = j1(hh);
-    double G_re = -L0 - 2.0 * kPi * H0 * ev;
-    double G_im = 2.0 * kPi * J0 * ev;
-    out[0] = mk(G_re, G_im);
-    out[1] = mk(-Ls - 2.0 * kPi * (2.0 / kPi - H1) * ev, -2.0 * kPi * J1 * ev);
-    out[2] = mk(G_re + 2.0 / dd, G_im);
+    T H0 = struve_h0(hh), J0 = j0(hh), H1 = struve_h1(hh), J1 = j1(hh);
+    T G_re = -L0 - (2.0 * kPi) * H0 * ev;
+    T G_im = (2.0 * kPi) * J0 * ev;
+    out[0] = cx<T>{G_re, G_im};
+    out[1] = cx<T>{-Ls - (2.0 * kPi) * (2.0 / kPi - H1) * ev, (-2.0 * kPi) * J1 * ev};
+    out[2] = cx<T>{G_re + 2.0 / dd, G_im};
 }
 
 // ---------------------------------------------------------------------------
@@ -473,32 +510,136 @@ namespace mh {
 // reduced coordinates and the per-pair sum over Green-function terms
 // ---------------------------------------------------------------------------
 
+// Exact wave term in the T arithmetic: the double quadrature, or for dual
+// numbers its value with derivatives from dG/dr, dG/dz = G + 2/R and, for
+// the second derivatives, G_zz = G_z - 2z/R^3, G_rz = G_r - 2r/R^3 and the
+// harmonic identity G_rr = -G_r/r - G_zz (the wave part solves Laplace's
+// equation), G_rr(0, z) = -G_zz/2.
+__device__ __forceinline__ void delh_exact_t(const double& r, const double& z, cplx out[3])
+{
+    delh_dimless(r, z, out);
+}
+template <int ND>
+__device__ __forceinline__ void delh_exact_t(const dualn<ND>& r, const dualn<ND>& z,
+                                             cx<dualn<ND>> out[3])
+{
+    cplx o[3];
+    delh_dimless(r.v, z.v, o);
+    const double R = hypot(r.v, z.v), R3 = R * R * R;
+    cplx gzz = o[2] - mk(2.0 * z.v / R3, 0.0);
+    cplx grz = o[1] - mk(2.0 * r.v / R3, 0.0);
+    cplx grr = (r.v > 0.0) ? -(o[1] / r.v) - gzz : mk(-0.5 * gzz.re, -0.5 * gzz.im);
+    const cplx d[3][2] = {{o[1], o[2]}, {grr, grz}, {grz, gzz}};  // (d/dr, d/dz) of G, G_r, G_z
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        out[q].re.v = o[q].re;
+        out[q].im.v = o[q].im;
+#pragma unroll
+        for (int k = 0; k < ND; ++k) {
+            out[q].re.d[k] = d[q][0].re * r.d[k] + d[q][1].re * z.d[k];
+            out[q].im.d[k] = d[q][0].im * r.d[k] + d[q][1].im * z.d[k];
+        }
+    }
+}
+
+// Table evaluation in the T arithmetic (the double version is
+// delh_dimless_table); derivatives are those of the Chebyshev interpolant.
+template <int N, class T>
+__device__ __forceinline__ T cheb2d_t(const double* __restrict__ c, const T& u, const T& v)
+{
+    T a1 = tconst<T>(0.0), a2 = tconst<T>(0.0), s0 = tconst<T>(0.0);
+#pragma unroll 1
+    for (int i = N - 1; i >= 0; --i) {
+        const double* ci = c + i * N;
+        T b1 = tconst<T>(0.0), b2 = tconst<T>(0.0);
+#pragma unroll 4
+        for (int j = N - 1; j >= 1; --j) {
+            T t = 2.0 * v * b1 + (__ldg(ci + j) - b2);
+            b2 = b1;
+            b1 = t;
+        }
+        T si = v * b1 + (__ldg(ci) - b2);
+        if (i >= 1) {
+            T t = 2.0 * u * a1 + (si - a2);
+            a2 = a1;
+            a1 = t;
+        } else {
+            s0 = u * a1 + (si - a2);
+        }
+    }
+    return s0;
+}
+
+template <class T>
+__device__ __forceinline__ void delh_table_t(const double* __restrict__ tab, const T& r, const T& z,
+                                             cx<T> out[3])
+{
+    const T az = -z;
+    const T R = hypot(r, z);
+    T B, C;
+    if (!(val(az) >= 0.0)) {
+        delh_exact_t(r, z, out);
+        return;
+    }
+    if (val(R) < kTabRPolar) {
+        T alpha = atan2(r, az);
+        T u = R * (2.0 / kTabRPolar) - 1.0;
+        T v = alpha * (4.0 / kPi) - 1.0;
+        B = cheb2d_t<kTabNP>(tab, u, v);
+        C = cheb2d_t<kTabNP>(tab + kTabNP * kTabNP, u, v);
+    } else if (val(r) < kTabExtent && val(az) < kTabExtent) {
+        int ir = min((int)(val(r) / kTabH), kTabNCell - 1);
+        int iz = min((int)(val(az) / kTabH), kTabNCell - 1);
+        const double* c = tab + kTabPolarWords + (iz * kTabNCell + ir) * kTabCellWords;
+        T u = (r - ir * kTabH) * (2.0 / kTabH) - 1.0;
+        T v = (az - iz * kTabH) * (2.0 / kTabH) - 1.0;
+        B = cheb2d_t<kTabNC>(c, u, v);
+        C = cheb2d_t<kTabNC>(c + kTabNC * kTabNC, u, v);
+    } else {
+        delh_exact_t(r, z, out);
+        return;
+    }
+    const T e = exp(z);
+    const T J0 = j0(r), J1 = j1(r);
+    const T L = log(0.5 * (R + az));
+    const T G_re = -2.0 * e * J0 * L + B;
+    const T G_im = (2.0 * kPi) * e * J0;
+    out[0] = cx<T>{G_re, G_im};
+    out[1] = cx<T>{2.0 * e * J1 * L - 2.0 * e * J0 * r / (R * (R + az)) + C, (-2.0 * kPi) * e * J1};
+    out[2] = cx<T>{G_re + 2.0 / R, G_im};
+}
+
 // k*G*area and the k-scaled gradient * area (abstract_greens_function.jl:88-155,
 // one-point rule wu.jl:33-47 / exact_Guevel_Delhommeau.jl:61-75).
-template <bool kDelh>
-__device__ __forceinline__ void wave_pair(const double x[3], const Panel& p, double k,
-                                          bool wrt_first, const double* tab, cplx& s, cplx g[3])
+template <bool kDelh, class T>
+__device__ __forceinline__ void wave_pair(const T x[3], const PanelT<T>& p, const T& k, bool wrt_first,
+                                          const double* tab, cx<T>& s, cx<T> g[3])
 {
-    double dx = x[0] - p.c[0], dy = x[1] - p.c[1];
-    double dis2 = dx * dx + dy * dy;
+    T dx = x[0] - p.c[0], dy = x[1] - p.c[1];
+    T dis2 = dx * dx + dy * dy;
     const double purt = 1e-18;
-    double dis = (dis2 == 0.0) ? sqrt(dis2 + purt * purt) - purt : sqrt(dis2);
-    double r = k * dis;
-    double z = k * (x[2] + p.c[2]);
-    cplx o[3];
+    T dis = (val(dis2) == 0.0) ? sqrt(dis2 + purt * purt) - purt : sqrt(dis2);
+    T r = k * dis;
+    T z = k * (x[2] + p.c[2]);
+    cx<T> o[3];
     if (kDelh) {
-        if (tab) delh_dimless_table(tab, r, z, o);
-        else delh_dimless(r, z, o);
+        if constexpr (std::is_same<T, double>::value) {
+            if (tab) delh_dimless_table(tab, r, z, o);
+            else delh_dimless(r, z, o);
+        } else {
+            if (tab) delh_table_t(tab, r, z, o);
+            else delh_exact_t(r, z, o);
+        }
     } else {
         wu_dimless(r, z, o);
     }
-    double d1 = 0.0, d2 = 0.0;
-    if (fabs(r) > 1e-6) {
-        double f = k * k / r;
-        d1 = wrt_first ? f * dx : -f * dx;
-        d2 = wrt_first ? f * dy : -f * dy;
+    T d1 = tconst<T>(0.0), d2 = tconst<T>(0.0);
+    if (fabs(val(r)) > 1e-6) {
+        T f = k * k / r;
+        d1 = wrt_first ? f * dx : -(f * dx);
+        d2 = wrt_first ? f * dy : -(f * dy);
     }
-    double ka = k * p.area;
+    T ka = k * p.area;
     s = ka * o[0];
     g[0] = (ka * d1) * o[1];
     g[1] = (ka * d2) * o[1];
@@ -506,14 +647,16 @@ __device__ __forceinline__ void wave_pair(const double x[3], const Panel& p, dou
 }
 
 // Sum over the Green-function tuple of integral / integral_gradient.
-__device__ __forceinline__ void pair_integrals(const double x[3], const Panel& p, double k,
+template <class T>
+__device__ __forceinline__ void pair_integrals(const T x[3], const PanelT<T>& p, const T& k,
                                                uint32_t mask, bool wrt_first, const double* tab,
-                                               cplx& s, cplx g[3])
+                                               cx<T>& s, cx<T> g[3])
 {
-    s = mk(0.0, 0.0);
-    g[0] = g[1] = g[2] = mk(0.0, 0.0);
+    const T zero = tconst<T>(0.0);
+    s = cx<T>{zero, zero};
+    g[0] = g[1] = g[2] = cx<T>{zero, zero};
     if (mask & MH_GF_RANKINE) {
-        double I, gr[3];
+        T I, gr[3];
         rankine_pair(x, p, I, gr);
         double sg = wrt_first ? -1.0 : 1.0;
         s.re += I;
@@ -524,18 +667,18 @@ __device__ __forceinline__ void pair_integrals(const double x[3], const Panel& p
     uint32_t refl = mask & (MH_GF_RANKINE_REFLECTED | MH_GF_RANKINE_REFLECTED_NEGATIVE);
     if (refl == MH_GF_RANKINE_REFLECTED || refl == MH_GF_RANKINE_REFLECTED_NEGATIVE) {
         double sgn = (refl == MH_GF_RANKINE_REFLECTED) ? 1.0 : -1.0;
-        double xr[3] = {x[0], x[1], -x[2]};
-        double I, gr[3];
+        T xr[3] = {x[0], x[1], -x[2]};
+        T I, gr[3];
         rankine_pair(xr, p, I, gr);
         double sg = wrt_first ? -1.0 : 1.0;
         double sz = wrt_first ? -1.0 : 1.0;  // vertical_reflection for wrt_first
         s.re += sgn * I;
-        g[0].re += sgn * sg * gr[0];
-        g[1].re += sgn * sg * gr[1];
-        g[2].re += sgn * sg * sz * gr[2];
+        g[0].re += (sgn * sg) * gr[0];
+        g[1].re += (sgn * sg) * gr[1];
+        g[2].re += (sgn * sg * sz) * gr[2];
     }
     if (mask & MH_GF_WU) {
-        cplx sw, gw[3];
+        cx<T> sw, gw[3];
         wave_pair<false>(x, p, k, wrt_first, tab, sw, gw);
         s = s + sw;
         g[0] = g[0] + gw[0];
@@ -543,7 +686,7 @@ __device__ __forceinline__ void pair_integrals(const double x[3], const Panel& p
         g[2] = g[2] + gw[2];
     }
     if (mask & MH_GF_DELHOMMEAU) {
-        cplx sw, gw[3];
+        cx<T> sw, gw[3];
         wave_pair<true>(x, p, k, wrt_first, tab, sw, gw);
         s = s + sw;
         g[0] = g[0] + gw[0];

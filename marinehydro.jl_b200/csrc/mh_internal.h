@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "marinehydro_b200.h"
 
@@ -23,13 +24,15 @@ struct mh_mesh {
     int64_t n = 0;
     int64_t nv = 0;
     int device = 0;
-    double* geom = nullptr;  // device, G_NFIELDS * n doubles
+    double* geom = nullptr;      // device, G_NFIELDS * n doubles
+    std::vector<int64_t> faces;  // host copy, 4 x n column-major (vertex cotangent scatter)
 };
 
 // Workspace slots of a context; each is a grow-only device buffer.
 enum WsSlot : int {
     WS_S = 0, WS_D, WS_RHS, WS_PHI, WS_TMP, WS_PIV, WS_INFO, WS_LWORK,
-    WS_DOF, WS_OUT, WS_LO, WS_DINV, WS_TMP32, WS_MISC, WS_SR, WS_TMP32B, WS_PANEL, WS_NSLOTS
+    WS_DOF, WS_OUT, WS_LO, WS_DINV, WS_TMP32, WS_MISC, WS_SR, WS_TMP32B, WS_PANEL, WS_FB,
+    WS_ADJ, WS_WSD, WS_PART, WS_GBAR, WS_NSLOTS
 };
 
 // Largest number of right-hand sides (radiating dofs + headings) per frequency.
@@ -111,13 +114,73 @@ cudaError_t launch_lu_solve_blocks32(mh_ctx* ctx, const float2* A, int64_t n, in
                                      int nbatch, const float2* Dinv, float2* X, float2* T,
                                      int64_t xstride, int nrhs);
 
+// Conjugate-transposed solve D^H X = X with the factors of launch_lu_tc
+// (backend MH_LU_TCGEN05_F16) or launch_lu_f32 (MH_LU_SIMT_F32).
+cudaError_t launch_lu_solve_ct(mh_ctx* ctx, int backend, const float2* A, int64_t n, int64_t stride,
+                               int nbatch, const float2* Dinv, float2* X, float2* T, int64_t xstride,
+                               int nrhs);
+
 // ---- batched driver (mh_batch.cu) ----
+struct Batch {
+    mh_ctx* ctx;
+    const mh_mesh* m;
+    int64_t n;
+    int ndof, nbeta, nrhs;
+    const double* d_dofs;
+    const double* d_betas;
+    double rho, g;
+    uint32_t mask;
+    int direct;
+};
+// FP64 factors of the problems of a chunk that left the mixed path, kept for
+// the adjoint solve (lu: nb matrices, piv: nb x n, used[z] != 0 when set).
+struct FallbackStore {
+    double2* lu = nullptr;
+    int* piv = nullptr;
+    std::vector<int> used;
+};
 cudaError_t launch_to_f32(mh_ctx* ctx, const double2* a, float2* b, int64_t count);
+cudaError_t launch_add_f32(mh_ctx* ctx, double2* x, const float2* d, int64_t count);
+// out[z] = max over right-hand sides of max|r| / max|b| for nb problems of n x nrhs.
+cudaError_t launch_rel_residual(mh_ctx* ctx, const double2* r, const double2* b, int64_t n, int nrhs,
+                                int nb, double* out);
+// Device force layout (F then FK, see hydro_batch) to the reference's output arrays.
+void unpack_outputs(const double2* h, int64_t nomega, const double* omegas, int64_t ndof, int64_t nbeta,
+                    double* added_mass, double* damping, double* diffraction, double* froude_krylov);
+// C = alpha A B + beta C for nb strided n x n by n x nrhs complex products.
+int zgemm_strided(mh_ctx* ctx, int64_t n, int nrhs, const double2* A, const double2* B, double2* C,
+                  int nb, double alpha_re, double beta_re);
+int fp64_lu_factor(mh_ctx* ctx, int64_t n, double2* A, int* piv);
+int fp64_getrs(mh_ctx* ctx, bool conj_trans, int64_t n, const double2* LU, const int* piv, double2* B,
+               int nrhs);
+int fp64_lu_solve(mh_ctx* ctx, int64_t n, double2* A, double2* B, int nrhs);
+int fallback_factor(mh_ctx* ctx, FallbackStore* fb, int64_t n, int nb, int z, const double2* D);
+// Frequency-independent Rankine parts SR, DR (n x n real) of the mixed path.
+int rankine_real(const Batch& bt, double* SR, double* DR);
+// One chunk of the mixed path; leaves S (WS_S), D (WS_D), the low-precision
+// factors (WS_LO, WS_DINV), the boundary conditions (WS_RHS), the solution
+// (WS_PHI: phi, or sigma when indirect; phi = S sigma in WS_TMP) in place.
+int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, int nb,
+                    const double* SR, const double* DR, double tol, int max_iter, double2* d_F,
+                    double2* d_FK, mh_batch_info* info, FallbackStore* fb);
+cudaError_t launch_bc_batch(const Batch& bt, const double* d_omegas, int nb, double2* BC);
+cudaError_t launch_forces_batch(const Batch& bt, const double* d_omegas, int nb, const double2* PHI,
+                                double2* d_F, double2* d_FK);
 int hydro_batch(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double* omegas, int64_t ndof,
                 const double* dofs, int64_t nbeta, const double* betas, double rho, double g,
                 uint32_t mask, int direct, int precision, double tol, int max_iter,
                 double* added_mass, double* damping, double* diffraction, double* froude_krylov,
                 mh_batch_info* info);
+
+// ---- adjoint (mh_adjoint.cu) ----
+int hydro_batch_vjp(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double* omegas, int64_t ndof,
+                    const double* dofs, int64_t nbeta, const double* betas, double rho, double g,
+                    uint32_t mask, int direct, int precision, double tol, int max_iter,
+                    const double* bar_added_mass, const double* bar_damping, const double* bar_diffraction,
+                    const double* bar_froude_krylov, double* added_mass, double* damping,
+                    double* diffraction, double* froude_krylov, double* d_vertices, double* d_centers,
+                    double* d_normals, double* d_areas, double* d_radii, double* d_omegas_out,
+                    double* d_dofs_out, mh_batch_info* info);
 
 // ---- Delhommeau table (mh_table.cu) ----
 int ensure_delh_table(mh_ctx* ctx);

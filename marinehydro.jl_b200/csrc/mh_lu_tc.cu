@@ -446,6 +446,128 @@ k_trsv_bwd(const float2* __restrict__ A, int64_t n, int64_t stride, const float2
     }
 }
 
+// Conjugate-transposed solves with the same factors, D^H x = r = U^H L^H x:
+// U^H y = r by blocks in increasing order, then L^H x = y in decreasing
+// order.  Row i of U^H (or L^H) is column i of the stored factor, so the
+// update of row i reads NB consecutive entries of column i: 8 lanes per
+// row, each lane every 8th entry, reduced with three shuffles.
+__device__ __forceinline__ float2 cconjmul(float2 a, float2 b)  // conj(a) * b
+{
+    return make_float2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+
+template <int NB>
+__global__ void __launch_bounds__(128)
+k_trsv_ct_fwd(const float2* __restrict__ A, int64_t n, int64_t stride, const float2* __restrict__ Dinv,
+              int64_t dstride, float2* __restrict__ X, float2* __restrict__ Y, int64_t xstride, int nrhs,
+              int blk)
+{
+    __shared__ float2 ys[kMaxRhs * NB];
+    const int b = blockIdx.y;
+    const float2* M = A + (int64_t)b * stride;
+    const float2* Ui = Dinv + (int64_t)b * dstride + (int64_t)blk * 2 * NB * NB + NB * NB;
+    float2* x = X + (int64_t)b * xstride;
+    float2* y = Y + (int64_t)b * xstride;
+    const int64_t k0 = (int64_t)blk * NB;
+    const int kb = (int)min((int64_t)NB, n - k0);
+    // y_blk = inv(U11)^H x_blk; inv(U11)^H[r][c] = conj(inv(U11)[c][r]), c <= r
+    for (int t = threadIdx.x; t < NB * nrhs; t += blockDim.x) {
+        const int r = t % NB, q = t / NB;
+        float2 acc = make_float2(0.f, 0.f);
+        if (r < kb)
+            for (int c = 0; c <= r; ++c) {
+                const float2 v = cconjmul(Ui[r * NB + c], x[(int64_t)q * n + k0 + c]);
+                acc.x += v.x;
+                acc.y += v.y;
+            }
+        ys[q * NB + r] = acc;
+    }
+    __syncthreads();
+    if (blockIdx.x == 0)
+        for (int t = threadIdx.x; t < kb * nrhs; t += blockDim.x) {
+            const int r = t % kb, q = t / kb;
+            y[(int64_t)q * n + k0 + r] = ys[q * NB + r];
+        }
+    // x_i -= sum_t conj(U[k0+t][i]) y_t for the rows below, 16 rows per CTA
+    const int sub = threadIdx.x & 7;
+    const int64_t i = k0 + kb + (int64_t)blockIdx.x * 16 + (threadIdx.x >> 3);
+    const bool live = i < n;
+    const float2* col = M + (live ? i : 0) * n + k0;
+    for (int q = 0; q < nrhs; ++q) {
+        float ax = 0.f, ay = 0.f;
+        if (live)
+            for (int t = sub; t < kb; t += 8) {
+                const float2 v = cconjmul(col[t], ys[q * NB + t]);
+                ax += v.x;
+                ay += v.y;
+            }
+        for (int off = 4; off > 0; off >>= 1) {
+            ax += __shfl_down_sync(0xffffffffu, ax, off, 8);
+            ay += __shfl_down_sync(0xffffffffu, ay, off, 8);
+        }
+        if (live && sub == 0) {
+            float2 v = x[(int64_t)q * n + i];
+            x[(int64_t)q * n + i] = make_float2(v.x - ax, v.y - ay);
+        }
+    }
+}
+
+template <int NB>
+__global__ void __launch_bounds__(128)
+k_trsv_ct_bwd(const float2* __restrict__ A, int64_t n, int64_t stride, const float2* __restrict__ Dinv,
+              int64_t dstride, float2* __restrict__ Y, float2* __restrict__ Z, int64_t xstride, int nrhs,
+              int blk)
+{
+    __shared__ float2 zs[kMaxRhs * NB];
+    const int b = blockIdx.y;
+    const float2* M = A + (int64_t)b * stride;
+    const float2* Li = Dinv + (int64_t)b * dstride + (int64_t)blk * 2 * NB * NB;
+    float2* y = Y + (int64_t)b * xstride;
+    float2* z = Z + (int64_t)b * xstride;
+    const int64_t k0 = (int64_t)blk * NB;
+    const int kb = (int)min((int64_t)NB, n - k0);
+    // z_blk = inv(L11)^H y_blk; inv(L11)^H[r][c] = conj(inv(L11)[c][r]), c >= r
+    for (int t = threadIdx.x; t < NB * nrhs; t += blockDim.x) {
+        const int r = t % NB, q = t / NB;
+        float2 acc = make_float2(0.f, 0.f);
+        if (r < kb)
+            for (int c = r; c < kb; ++c) {
+                const float2 v = cconjmul(Li[r * NB + c], y[(int64_t)q * n + k0 + c]);
+                acc.x += v.x;
+                acc.y += v.y;
+            }
+        zs[q * NB + r] = acc;
+    }
+    __syncthreads();
+    if (blockIdx.x == 0)
+        for (int t = threadIdx.x; t < kb * nrhs; t += blockDim.x) {
+            const int r = t % kb, q = t / kb;
+            z[(int64_t)q * n + k0 + r] = zs[q * NB + r];
+        }
+    // y_i -= sum_t conj(L[k0+t][i]) z_t for the rows above
+    const int sub = threadIdx.x & 7;
+    const int64_t i = (int64_t)blockIdx.x * 16 + (threadIdx.x >> 3);
+    const bool live = i < k0;
+    const float2* col = M + (live ? i : 0) * n + k0;
+    for (int q = 0; q < nrhs; ++q) {
+        float ax = 0.f, ay = 0.f;
+        if (live)
+            for (int t = sub; t < kb; t += 8) {
+                const float2 v = cconjmul(col[t], zs[q * NB + t]);
+                ax += v.x;
+                ay += v.y;
+            }
+        for (int off = 4; off > 0; off >>= 1) {
+            ax += __shfl_down_sync(0xffffffffu, ax, off, 8);
+            ay += __shfl_down_sync(0xffffffffu, ay, off, 8);
+        }
+        if (live && sub == 0) {
+            float2 v = y[(int64_t)q * n + i];
+            y[(int64_t)q * n + i] = make_float2(v.x - ax, v.y - ay);
+        }
+    }
+}
+
 unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
 
 }  // namespace
@@ -513,7 +635,40 @@ cudaError_t solve_blocks(mh_ctx* ctx, const float2* A, int64_t n, int64_t stride
     ctx->launches += 2 * nblk;
     return cudaGetLastError();
 }
+
+template <int NB>
+cudaError_t solve_blocks_ct(mh_ctx* ctx, const float2* A, int64_t n, int64_t stride, int nbatch,
+                            const float2* Dinv, int64_t dstride, float2* X, float2* T, int64_t xstride,
+                            int nrhs)
+{
+    if (nrhs < 1 || nrhs > kMaxRhs) return cudaErrorInvalidValue;
+    const int nblk = (int)((n + NB - 1) / NB);
+    for (int blk = 0; blk < nblk; ++blk) {
+        const int64_t below = n - (int64_t)(blk + 1) * NB;
+        dim3 g(below > 0 ? cdiv(below, 16) : 1u, (unsigned)nbatch);
+        k_trsv_ct_fwd<NB><<<g, 128, 0, ctx->stream>>>(A, n, stride, Dinv, dstride, X, T, xstride, nrhs,
+                                                       blk);
+    }
+    for (int blk = nblk - 1; blk >= 0; --blk) {
+        const int64_t above = (int64_t)blk * NB;
+        dim3 g(above > 0 ? cdiv(above, 16) : 1u, (unsigned)nbatch);
+        k_trsv_ct_bwd<NB><<<g, 128, 0, ctx->stream>>>(A, n, stride, Dinv, dstride, T, X, xstride, nrhs,
+                                                       blk);
+    }
+    ctx->launches += 2 * nblk;
+    return cudaGetLastError();
+}
 }  // namespace
+
+cudaError_t launch_lu_solve_ct(mh_ctx* ctx, int backend, const float2* A, int64_t n, int64_t stride,
+                               int nbatch, const float2* Dinv, float2* X, float2* T, int64_t xstride,
+                               int nrhs)
+{
+    if (backend == MH_LU_TCGEN05_F16)
+        return solve_blocks_ct<TC_NB>(ctx, A, n, stride, nbatch, Dinv, lu_dinv_stride_tc(n), X, T,
+                                      xstride, nrhs);
+    return solve_blocks_ct<32>(ctx, A, n, stride, nbatch, Dinv, lu_dinv_stride(n), X, T, xstride, nrhs);
+}
 
 cudaError_t launch_lu_solve_tc(mh_ctx* ctx, const float2* A, int64_t n, int64_t stride, int nbatch,
                                const float2* Dinv, float2* X, float2* T, int64_t xstride, int nrhs)
