@@ -100,8 +100,10 @@ int mh_ctx_stream(const mh_ctx* ctx, void** stream);
 /* Phase timing with CUDA events on the ctx stream (off by default; turning it
  * on or off resets the totals).  Phases, in order: 0 Rankine part, 1 wave
  * part + FP32 copy, 2 right-hand sides S*BC, 3 FP32 LU, 4 refinement,
- * 5 forces, 6 FP64 assembly, 7 FP64 LU (cuSOLVER).  No reference
- * counterpart (instrumentation). */
+ * 5 forces, 6 FP64 assembly, 7 FP64 LU (cuSOLVER), and of the adjoint
+ * (mh_hydro_batch_vjp): 8 adjoint solve, 9 wave-term contraction,
+ * 10 Rankine contraction, 11 force / boundary-condition reverse and
+ * frequency sums.  No reference counterpart (instrumentation). */
 int mh_ctx_set_profiling(mh_ctx* ctx, int enable);
 int mh_ctx_phase_times(mh_ctx* ctx, int nphases, double* ms, int64_t* calls);
 

@@ -189,7 +189,8 @@ class Context:
         c = out[:, 0::2] + 1j * out[:, 1::2]
         return c[:, 0], c[:, 1], c[:, 2]
 
-    PHASES = ("rankine", "wave", "rhs", "lu", "refine", "forces", "fp64_assembly", "fp64_lu")
+    PHASES = ("rankine", "wave", "rhs", "lu", "refine", "forces", "fp64_assembly", "fp64_lu",
+              "adj_solve", "adj_wave", "adj_rankine", "adj_linear")
 
     def set_lu_backend(self, backend: str):
         """'simt' (FP32 CUDA cores) or 'tcgen05' (FP16 tensor-core trailing update)."""

@@ -45,6 +45,7 @@ constexpr double kI4P = 1.0 / (4.0 * kPi);
 enum GbarField : int { GB_C = 0, GB_N = 3, GB_A = 6, GB_V = 7, GB_NF = 19 };
 constexpr int kRowF = 6;   // row partials: centre (3), normal (3)
 constexpr int kWaveF = 7;  // wave column partials: centre, normal, area
+constexpr int kAdjAllwMinFreqs = 4;  // chunks this large use the frequency-batched Delhommeau adjoint
 
 using d2 = dualn<2>;
 using d6 = dualn<6>;
@@ -92,11 +93,26 @@ __device__ __forceinline__ double block_sum(double v, double* red)
 // wave term
 // ---------------------------------------------------------------------------
 
-// Dimensionless wave term and its (r, z) derivatives: o[m].{re,im}.d[0] =
-// d/dr, .d[1] = d/dz of (G, G_r, G_z).  kind 1: Wu; 2: Delhommeau (table
-// when tab != null, else the quadrature with analytic second derivatives).
-__device__ __noinline__ void wave_dimless_d2(int kind, const double* __restrict__ tab, double r, double z,
-                                             cx<d2>* o)
+// Dimensionless wave term (G, G_r, G_z) with its r and z derivatives.
+struct GDer {
+    cplx G[3];
+    cplx Gr[3];
+    cplx Gz[3];
+};
+
+__device__ __forceinline__ void from_duals(const cx<d2>* o, GDer& g)
+{
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        g.G[m] = mk(o[m].re.v, o[m].im.v);
+        g.Gr[m] = mk(o[m].re.d[0], o[m].im.d[0]);
+        g.Gz[m] = mk(o[m].re.d[1], o[m].im.d[1]);
+    }
+}
+
+// (r, z) derivatives by 2-way dual numbers: Wu's formulas (kind 1) or the
+// Delhommeau quadrature with the second derivatives from its identities.
+__device__ __noinline__ void wave_dimless_dual(int kind, double r, double z, GDer* g)
 {
     d2 rd, zd;
     rd.v = r;
@@ -105,9 +121,143 @@ __device__ __noinline__ void wave_dimless_d2(int kind, const double* __restrict_
     zd.v = z;
     zd.d[0] = 0.0;
     zd.d[1] = 1.0;
+    cx<d2> o[3];
     if (kind == 1) wu_dimless(rd, zd, o);
-    else if (tab) delh_table_t(tab, rd, zd, o);
     else delh_exact_t(rd, zd, o);
+    from_duals(o, *g);
+}
+
+// Value and gradient of a 2-D Chebyshev series sum c[i*N+j] T_i(u) T_j(v)
+// (nested Clenshaw; the derivative recurrences d b_k = 2 b_{k+1} +
+// 2x d b_{k+1} - d b_{k+2} run beside the values).
+template <int N>
+__device__ __forceinline__ void cheb2d_grad(const double* __restrict__ c, double u, double v, double& f,
+                                            double& fu, double& fv)
+{
+    double a1 = 0.0, a2 = 0.0, da1 = 0.0, da2 = 0.0, e1 = 0.0, e2 = 0.0;
+#pragma unroll 1
+    for (int i = N - 1; i >= 0; --i) {
+        const double* ci = c + i * N;
+        double b1 = 0.0, b2 = 0.0, db1 = 0.0, db2 = 0.0;
+#pragma unroll 4
+        for (int j = N - 1; j >= 1; --j) {
+            const double t = fma(2.0 * v, b1, __ldg(ci + j) - b2);
+            const double dt = fma(2.0 * v, db1, fma(2.0, b1, -db2));
+            b2 = b1;
+            b1 = t;
+            db2 = db1;
+            db1 = dt;
+        }
+        const double si = fma(v, b1, __ldg(ci) - b2);
+        const double dsi = fma(v, db1, b1 - db2);
+        if (i >= 1) {
+            const double t = fma(2.0 * u, a1, si - a2);
+            const double dt = fma(2.0 * u, da1, fma(2.0, a1, -da2));
+            const double et = fma(2.0 * u, e1, dsi - e2);
+            a2 = a1;
+            a1 = t;
+            da2 = da1;
+            da1 = dt;
+            e2 = e1;
+            e1 = et;
+        } else {
+            f = fma(u, a1, si - a2);
+            fu = fma(u, da1, a1 - da2);
+            fv = fma(u, e1, dsi - e2);
+        }
+    }
+}
+
+// G, G_r, G_z and their r, z derivatives from the tabulated smooth parts
+// (B, C with their r, z derivatives), E0 = e^z J0(r), E1 = e^z J1(r) and
+// L = log((R + |z|)/2): G = -2 E0 L + B + 2 pi i E0,
+// G_r = 2 E1 L - 2 E0 r / (R (R + |z|)) + C - 2 pi i E1, G_z = G + 2/R;
+// dE0/dr = -E1, dE1/dr = E0 - E1/r, d/dz e^z = e^z.
+__device__ __forceinline__ void delh_grad_from_parts(double B, double Br, double Bz, double C, double Cr, double Cz,
+                                                     double E0, double E1, double r, double R, double az,
+                                                     double L, GDer& o)
+{
+    const double iR = 1.0 / R;
+    const double sr = r * iR, sz = -az * iR;
+    const double D1 = 1.0 / (R + az);
+    const double Lr = sr * D1, Lz = (sz - 1.0) * D1;
+    const double iM = iR * D1;  // 1 / (R (R + |z|))
+    const double Q = r * iM;
+    const double Mr = sr * (2.0 * R + az), Mz = sz * (2.0 * R + az) - R;
+    const double Qr = (1.0 - Q * Mr) * iM, Qz = -Q * Mz * iM;
+    const double E1r = (r > 1e-3) ? E0 - E1 / r : 0.5 * E0;
+    const double tp = 2.0 * kPi;
+    const double G0 = -2.0 * E0 * L + B;
+    const double G0r = 2.0 * E1 * L - 2.0 * E0 * Lr + Br;
+    const double G0z = -2.0 * E0 * L - 2.0 * E0 * Lz + Bz;
+    o.G[0] = mk(G0, tp * E0);
+    o.Gr[0] = mk(G0r, -tp * E1);
+    o.Gz[0] = mk(G0z, tp * E0);
+    o.G[1] = mk(2.0 * E1 * L - 2.0 * E0 * Q + C, -tp * E1);
+    o.Gr[1] = mk(2.0 * E1r * L + 2.0 * E1 * Lr + 2.0 * E1 * Q - 2.0 * E0 * Qr + Cr, -tp * E1r);
+    o.Gz[1] = mk(2.0 * E1 * L + 2.0 * E1 * Lz - 2.0 * E0 * Q - 2.0 * E0 * Qz + Cz, -tp * E1);
+    const double iR2 = iR * iR;
+    o.G[2] = mk(G0 + 2.0 * iR, tp * E0);
+    o.Gr[2] = mk(G0r - 2.0 * sr * iR2, -tp * E1);
+    o.Gz[2] = mk(G0z - 2.0 * sz * iR2, tp * E0);
+}
+
+// Tabulated Delhommeau term with its r, z derivatives at one point, the
+// derivative of exactly what delh_dimless_table evaluates; outside the
+// table, the quadrature path.
+__device__ __noinline__ void delh_point_grad(const double* __restrict__ tab, double r, double z, GDer* out)
+{
+    const double az = -z;
+    const double R = hypot(r, z);
+    double B, Br, Bz, C, Cr, Cz;
+    if (!(az >= 0.0)) {
+        wave_dimless_dual(2, r, z, out);
+        return;
+    }
+    if (R < kTabRPolar) {
+        const double alpha = atan2(r, az);
+        const double u = 2.0 * R / kTabRPolar - 1.0;
+        const double v = 4.0 * alpha / kPi - 1.0;
+        double fu, fv;
+        const double sr = r / R, sz = z / R;
+        cheb2d_grad<kTabNP>(tab, u, v, B, fu, fv);
+        double BR = fu * (2.0 / kTabRPolar), Ba = fv * (4.0 / kPi);
+        Br = BR * sr - Ba * sz / R;
+        Bz = BR * sz + Ba * sr / R;
+        cheb2d_grad<kTabNP>(tab + kTabNP * kTabNP, u, v, C, fu, fv);
+        BR = fu * (2.0 / kTabRPolar);
+        Ba = fv * (4.0 / kPi);
+        Cr = BR * sr - Ba * sz / R;
+        Cz = BR * sz + Ba * sr / R;
+    } else if (r < kTabExtent && az < kTabExtent) {
+        const int ir = min((int)(r / kTabH), kTabNCell - 1);
+        const int iz = min((int)(az / kTabH), kTabNCell - 1);
+        const double* c = tab + kTabPolarWords + (iz * kTabNCell + ir) * kTabCellWords;
+        const double u = 2.0 * (r - ir * kTabH) / kTabH - 1.0;
+        const double v = 2.0 * (az - iz * kTabH) / kTabH - 1.0;
+        double fu, fv;
+        cheb2d_grad<kTabNC>(c, u, v, B, fu, fv);
+        Br = fu * (2.0 / kTabH);
+        Bz = -fv * (2.0 / kTabH);
+        cheb2d_grad<kTabNC>(c + kTabNC * kTabNC, u, v, C, fu, fv);
+        Cr = fu * (2.0 / kTabH);
+        Cz = -fv * (2.0 / kTabH);
+    } else {
+        wave_dimless_dual(2, r, z, out);
+        return;
+    }
+    const double e = exp(z);
+    const double E0 = e * j0(r), E1 = e * j1(r);
+    const double L = log(0.5 * (R + az));
+    delh_grad_from_parts(B, Br, Bz, C, Cr, Cz, E0, E1, r, R, az, L, *out);
+}
+
+// kind 1: Wu; kind 2: Delhommeau (table when tab != null, else quadrature).
+__device__ __forceinline__ void wave_dimless_grad(int kind, const double* __restrict__ tab, double r, double z,
+                                                  GDer& g)
+{
+    if (kind == 2 && tab) delh_point_grad(tab, r, z, &g);
+    else wave_dimless_dual(kind, r, z, &g);
 }
 
 struct WaveBar {
@@ -115,51 +265,65 @@ struct WaveBar {
     double n[3];
 };
 
-// Reverse of wave_pair for one pair (abstract_greens_function.jl:88-155 with
-// the one-point rule): L = Re(cs s + cw (nD . g)), with s = k A G(r, z),
-// g = (sg k^2 A u_x G_r, sg k^2 A u_y G_r, k^2 A G_z), r = k |dx, dy|,
-// z = k zs, u = (dx, dy)/|dx, dy|, sg = +1 for the gradient with respect to
-// the first variable.  Returns dL/d(dx, dy, zs, area, k) and dL/dnD.
+// Pair geometry of the wave term (abstract_greens_function.jl:88-155 at k = 1).
+struct WaveGeom {
+    double dx, dy, zs, dis, u0, u1, invd;
+};
+
+__device__ __forceinline__ WaveGeom wave_geom(const double x[3], const Panel& p)
+{
+    WaveGeom w;
+    w.dx = x[0] - p.c[0];
+    w.dy = x[1] - p.c[1];
+    w.zs = x[2] + p.c[2];
+    const double dis2 = w.dx * w.dx + w.dy * w.dy;
+    const double purt = 1e-18;
+    w.dis = (dis2 == 0.0) ? sqrt(dis2 + purt * purt) - purt : sqrt(dis2);
+    w.invd = w.dis > 0.0 ? 1.0 / w.dis : 0.0;
+    w.u0 = w.dx * w.invd;
+    w.u1 = w.dy * w.invd;
+    return w;
+}
+
+// Reverse of wave_pair for one pair and one k, given the dimensionless term
+// and its derivatives at (r, z) = k (dis, zs): L = Re(cs s + cw (nD . g)),
+// s = k A G, g = (sg k^2 A u_x G_r, sg k^2 A u_y G_r, k^2 A G_z),
+// sg = +1 for the gradient with respect to the first variable.  Returns
+// dL/d(dx, dy, zs, area, k) and dL/dnD.
+__device__ __forceinline__ void wave_chain(const GDer& o, const WaveGeom& w, double k, double A, bool wrt_first,
+                                           cplx cs, cplx cw, const double nD[3], WaveBar& wb)
+{
+    const bool rad = fabs(k * w.dis) > 1e-6;
+    const double sg = wrt_first ? 1.0 : -1.0;
+    const double k2 = k * k;
+    const cplx c0 = cw * nD[0], c1 = cw * nD[1], c2 = cw * nD[2];  // conj of the g cotangents
+    const cplx P1 = rad ? sg * (c0 * w.u0 + c1 * w.u1) : mk(0.0, 0.0);
+    const cplx a0 = cs * k, a1 = P1 * k2, a2 = c2 * k2;
+    const double Lr = A * (re_mul(a0, o.Gr[0]) + re_mul(a1, o.Gr[1]) + re_mul(a2, o.Gr[2]));
+    const double Lz = A * (re_mul(a0, o.Gz[0]) + re_mul(a1, o.Gz[1]) + re_mul(a2, o.Gz[2]));
+    const double U0 = rad ? sg * k2 * A * re_mul(c0, o.G[1]) : 0.0;
+    const double U1 = rad ? sg * k2 * A * re_mul(c1, o.G[1]) : 0.0;
+    wb.dx = Lr * k * w.u0 + (U0 * (1.0 - w.u0 * w.u0) - U1 * w.u0 * w.u1) * w.invd;
+    wb.dy = Lr * k * w.u1 + (U1 * (1.0 - w.u1 * w.u1) - U0 * w.u0 * w.u1) * w.invd;
+    wb.zs = Lz * k;
+    const double e0 = re_mul(cs, o.G[0]), e12 = re_mul(P1, o.G[1]) + re_mul(c2, o.G[2]);
+    wb.area = k * e0 + k2 * e12;
+    wb.k = Lr * w.dis + Lz * w.zs + A * e0 + 2.0 * k * A * e12;
+    const double gr = rad ? sg * k2 * A : 0.0;
+    const cplx g0 = (gr * w.u0) * o.G[1], g1 = (gr * w.u1) * o.G[1], g2 = (k2 * A) * o.G[2];
+    wb.n[0] = re_mul(cw, g0);
+    wb.n[1] = re_mul(cw, g1);
+    wb.n[2] = re_mul(cw, g2);
+}
+
 __device__ __forceinline__ void wave_pair_vjp(int kind, const double x[3], const Panel& p, double k,
                                               bool wrt_first, const double* __restrict__ tab, cplx cs,
                                               cplx cw, const double nD[3], WaveBar& wb)
 {
-    const double dx = x[0] - p.c[0], dy = x[1] - p.c[1], zs = x[2] + p.c[2];
-    const double dis2 = dx * dx + dy * dy;
-    const double purt = 1e-18;
-    const double dis = (dis2 == 0.0) ? sqrt(dis2 + purt * purt) - purt : sqrt(dis2);
-    const double r = k * dis, z = k * zs;
-    cx<d2> o[3];
-    wave_dimless_d2(kind, tab, r, z, o);
-    const cplx G0 = mk(o[0].re.v, o[0].im.v), G1 = mk(o[1].re.v, o[1].im.v), G2 = mk(o[2].re.v, o[2].im.v);
-    const bool rad = fabs(r) > 1e-6;
-    const double invd = dis > 0.0 ? 1.0 / dis : 0.0;
-    const double u0 = dx * invd, u1 = dy * invd;
-    const double sg = wrt_first ? 1.0 : -1.0;
-    const double A = p.area, k2 = k * k;
-    const cplx c0 = cw * nD[0], c1 = cw * nD[1], c2 = cw * nD[2];  // conj of the g cotangents
-    const cplx P1 = rad ? sg * (c0 * u0 + c1 * u1) : mk(0.0, 0.0);
-    double Lr = 0.0, Lz = 0.0;
-    {
-        const cplx a0 = cs * k, a1 = P1 * k2, a2 = c2 * k2;
-        Lr = A * (re_mul(a0, mk(o[0].re.d[0], o[0].im.d[0])) + re_mul(a1, mk(o[1].re.d[0], o[1].im.d[0])) +
-                  re_mul(a2, mk(o[2].re.d[0], o[2].im.d[0])));
-        Lz = A * (re_mul(a0, mk(o[0].re.d[1], o[0].im.d[1])) + re_mul(a1, mk(o[1].re.d[1], o[1].im.d[1])) +
-                  re_mul(a2, mk(o[2].re.d[1], o[2].im.d[1])));
-    }
-    const double U0 = rad ? sg * k2 * A * re_mul(c0, G1) : 0.0;
-    const double U1 = rad ? sg * k2 * A * re_mul(c1, G1) : 0.0;
-    wb.dx = Lr * k * u0 + (U0 * (1.0 - u0 * u0) - U1 * u0 * u1) * invd;
-    wb.dy = Lr * k * u1 + (U1 * (1.0 - u1 * u1) - U0 * u0 * u1) * invd;
-    wb.zs = Lz * k;
-    const double e0 = re_mul(cs, G0), e12 = re_mul(P1, G1) + re_mul(c2, G2);
-    wb.area = k * e0 + k2 * e12;
-    wb.k = Lr * dis + Lz * zs + A * e0 + 2.0 * k * A * e12;
-    const double gr = rad ? sg * k2 * A : 0.0;
-    const cplx g0 = (gr * u0) * G1, g1 = (gr * u1) * G1, g2 = (k2 * A) * G2;
-    wb.n[0] = re_mul(cw, g0);
-    wb.n[1] = re_mul(cw, g1);
-    wb.n[2] = re_mul(cw, g2);
+    const WaveGeom w = wave_geom(x, p);
+    GDer o;
+    wave_dimless_grad(kind, tab, k * w.dis, k * w.zs, o);
+    wave_chain(o, w, k, p.area, wrt_first, cs, cw, nD, wb);
 }
 
 // Wave-term contraction over the pairs of a 128-row x 16-column tile for
@@ -256,6 +420,222 @@ k_adj_wave(int kind, const double* __restrict__ geom, int64_t n, int direct, con
     for (int z = threadIdx.x; z < nb; z += blockDim.x) {
         double s = 0.0;
         for (int w = 0; w < kAR / 32; ++w) s += ksm[w * nb + z];
+        kpart[(int64_t)z * P + blk] = s;
+    }
+}
+
+// Frequency-batched adjoint of the tabulated Delhommeau term (the reverse
+// of the forward's frequency-batched pass).  A pair keeps its polar angle
+// alpha at every frequency, so the alpha direction of the polar tables is
+// contracted once per pair into six series in R (shared memory, one column
+// per thread): B and C with their alpha derivatives, E0 = e^z J0(r) and
+// E1 = e^z J1(r).  Each frequency then runs 1-D Clenshaw recurrences in
+// u(R) for the values and u-derivatives, two frequencies at a time, and the
+// r, z derivatives follow from dR = (r dr + z dz)/R, dalpha = (|z| dr +
+// r dz)/R^2.  Frequencies at which the pair leaves the polar patch take the
+// per-point table gradient.  Partial sums as k_adj_wave.
+constexpr int kAW = 64;  // rows (threads) per CTA
+constexpr int kZC = 2;   // frequencies per Clenshaw pass
+constexpr int kNS = 6;   // series: B, dB/dalpha, C, dC/dalpha, E0, E1
+
+size_t adj_allw_smem(int nb)
+{
+    return sizeof(double) * ((size_t)kNS * kTabNP * kAW + (size_t)(kAW / 32) * nb + nb);
+}
+
+__global__ void __launch_bounds__(kAW, 3)
+k_adj_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const double* __restrict__ tab,
+                const double* __restrict__ kvec, int nb, int nrhs, const double2* __restrict__ VA,
+                const double2* __restrict__ VB, const double2* __restrict__ VC, const double2* __restrict__ VD,
+                double* __restrict__ rowpart, double* __restrict__ colpart, double* __restrict__ kpart)
+{
+    extern __shared__ double dsm[];
+    double* w = dsm;                              // [kNS * kTabNP][kAW]
+    double* ksm = w + kNS * kTabNP * kAW;         // [kAW / 32][nb]
+    double* logk = ksm + (kAW / 32) * nb;         // [nb]
+    __shared__ Panel sp[kAC];
+    __shared__ double csm[kAW / 32][kAC][kWaveF];
+    const int64_t j0 = (int64_t)blockIdx.y * kAC;
+    stage(sp, geom, n, j0);
+    for (int t = threadIdx.x; t < (kAW / 32) * nb; t += blockDim.x) ksm[t] = 0.0;
+    for (int t = threadIdx.x; t < nb; t += blockDim.x) logk[t] = log(kvec[t]);
+    __syncthreads();
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int64_t i = (int64_t)blockIdx.x * kAW + tid;
+    const bool live = i < n;
+    const int64_t ii = live ? i : 0;
+    const double x[3] = {geom[G_CX * n + ii], geom[G_CY * n + ii], geom[G_CZ * n + ii]};
+    const double ni[3] = {geom[G_NX * n + ii], geom[G_NY * n + ii], geom[G_NZ * n + ii]};
+    const int jend = (int)min((int64_t)kAC, n - j0);
+    const int64_t nv = n * nrhs;
+    double* wt = w + tid;
+    double xb[3] = {0.0, 0.0, 0.0}, nbi[3] = {0.0, 0.0, 0.0};
+    for (int jj = 0; jj < jend; ++jj) {
+        const Panel& p = sp[jj];
+        const int64_t j = j0 + jj;
+        const double* nD = direct ? p.n : ni;
+        const WaveGeom wg = wave_geom(x, p);
+        const double az1 = -wg.zs;
+        const double rho = hypot(wg.dis, wg.zs);
+        const bool polar_ok = az1 >= 0.0 && rho > 0.0;
+        const double sr = polar_ok ? wg.dis / rho : 0.0, sz = polar_ok ? wg.zs / rho : 0.0;
+        const double lp = log(0.5 * (rho + az1));
+        if (polar_ok) {  // contract alpha: values (and alpha derivatives of B, C)
+            const double v = 4.0 * atan2(wg.dis, az1) / kPi - 1.0;
+#pragma unroll 1
+            for (int q = 0; q < 4; ++q) {
+                const double* c = tab + q * kTabNP * kTabNP;
+                const int slot = (q < 2) ? 2 * q : q + 2;
+#pragma unroll 1
+                for (int row = 0; row < kTabNP; ++row) {
+                    const double* cr = c + row * kTabNP;
+                    double b1 = 0.0, b2 = 0.0, d1 = 0.0, d2 = 0.0;
+#pragma unroll
+                    for (int col = kTabNP - 1; col >= 1; --col) {
+                        const double t = fma(2.0 * v, b1, __ldg(cr + col) - b2);
+                        const double dt = fma(2.0 * v, d1, fma(2.0, b1, -d2));
+                        b2 = b1;
+                        b1 = t;
+                        d2 = d1;
+                        d1 = dt;
+                    }
+                    wt[(slot * kTabNP + row) * kAW] = fma(v, b1, __ldg(cr) - b2);
+                    if (q < 2) wt[((slot + 1) * kTabNP + row) * kAW] = (4.0 / kPi) * fma(v, d1, b1 - d2);
+                }
+            }
+        }
+        double cacc[kWaveF] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int zc = 0; zc < nb; zc += kZC) {
+            double kk[kZC], uu[kZC];
+            bool pol[kZC];
+#pragma unroll
+            for (int t = 0; t < kZC; ++t) {
+                const int z = min(zc + t, nb - 1);
+                kk[t] = kvec[z];
+                const double R = kk[t] * rho;
+                pol[t] = polar_ok && (zc + t < nb) && R < kTabRPolar;
+                uu[t] = 2.0 * R / kTabRPolar - 1.0;
+            }
+            // series values (sv) and u-derivatives of B, C (su), Clenshaw in u
+            double sv[kZC][kNS], su[kZC][2];
+            if (pol[0] || pol[kZC - 1]) {
+                double b1[kZC][kNS], b2[kZC][kNS], e1[kZC][2], e2[kZC][2];
+#pragma unroll
+                for (int t = 0; t < kZC; ++t) {
+#pragma unroll
+                    for (int q = 0; q < kNS; ++q) b1[t][q] = b2[t][q] = 0.0;
+                    e1[t][0] = e1[t][1] = e2[t][0] = e2[t][1] = 0.0;
+                }
+#pragma unroll 2
+                for (int row = kTabNP - 1; row >= 1; --row) {
+                    double cq[kNS];
+#pragma unroll
+                    for (int q = 0; q < kNS; ++q) cq[q] = wt[(q * kTabNP + row) * kAW];
+#pragma unroll
+                    for (int t = 0; t < kZC; ++t) {
+                        const double u2 = 2.0 * uu[t];
+                        // derivatives of the B (q = 0) and C (q = 2) series
+                        const double dB = fma(u2, e1[t][0], fma(2.0, b1[t][0], -e2[t][0]));
+                        const double dC = fma(u2, e1[t][1], fma(2.0, b1[t][2], -e2[t][1]));
+                        e2[t][0] = e1[t][0];
+                        e1[t][0] = dB;
+                        e2[t][1] = e1[t][1];
+                        e1[t][1] = dC;
+#pragma unroll
+                        for (int q = 0; q < kNS; ++q) {
+                            const double nt = fma(u2, b1[t][q], cq[q] - b2[t][q]);
+                            b2[t][q] = b1[t][q];
+                            b1[t][q] = nt;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int t = 0; t < kZC; ++t) {
+#pragma unroll
+                    for (int q = 0; q < kNS; ++q) sv[t][q] = fma(uu[t], b1[t][q], wt[q * kTabNP * kAW] - b2[t][q]);
+                    su[t][0] = fma(uu[t], e1[t][0], b1[t][0] - e2[t][0]);
+                    su[t][1] = fma(uu[t], e1[t][1], b1[t][2] - e2[t][1]);
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < kZC; ++t) {
+                const int z = zc + t;
+                if (z >= nb) break;
+                const double k = kk[t];
+                const int64_t base = (int64_t)z * nv;
+                double sr_ = 0.0, si_ = 0.0, dr_ = 0.0, di_ = 0.0;
+                for (int q = 0; q < nrhs; ++q) {
+                    const double2 a = VA[base + q * n + ii], b = VB[base + q * n + j];
+                    const double2 c = VC[base + q * n + ii], d = VD[base + q * n + j];
+                    sr_ += a.x * b.x + a.y * b.y;
+                    si_ += a.y * b.x - a.x * b.y;
+                    dr_ -= c.x * d.x + c.y * d.y;
+                    di_ -= c.y * d.x - c.x * d.y;
+                }
+                const cplx cs = mk(-kI4P * sr_, kI4P * si_), cw = mk(-kI4P * dr_, kI4P * di_);
+                double bk = 0.0;
+                if (live) {
+                    GDer o;
+                    if (pol[t]) {
+                        const double R = k * rho, r = k * wg.dis, azk = k * az1;
+                        const double iR = 1.0 / R;
+                        const double BR = su[t][0] * (2.0 / kTabRPolar), CR = su[t][1] * (2.0 / kTabRPolar);
+                        const double Ba = sv[t][1], Ca = sv[t][3];
+                        const double Br = BR * sr - Ba * sz * iR, Bz = BR * sz + Ba * sr * iR;
+                        const double Cr = CR * sr - Ca * sz * iR, Cz = CR * sz + Ca * sr * iR;
+                        delh_grad_from_parts(sv[t][0], Br, Bz, sv[t][2], Cr, Cz, sv[t][4], sv[t][5], r, R, azk,
+                                             logk[z] + lp, o);
+                    } else {
+                        delh_point_grad(tab, k * wg.dis, k * wg.zs, &o);
+                    }
+                    WaveBar wb;
+                    wave_chain(o, wg, k, p.area, !direct, cs, cw, nD, wb);
+                    xb[0] += wb.dx;
+                    xb[1] += wb.dy;
+                    xb[2] += wb.zs;
+                    cacc[0] -= wb.dx;
+                    cacc[1] -= wb.dy;
+                    cacc[2] += wb.zs;
+                    if (direct) {
+                        cacc[3] += wb.n[0];
+                        cacc[4] += wb.n[1];
+                        cacc[5] += wb.n[2];
+                    } else {
+                        nbi[0] += wb.n[0];
+                        nbi[1] += wb.n[1];
+                        nbi[2] += wb.n[2];
+                    }
+                    cacc[6] += wb.area;
+                    bk = wb.k;
+                }
+                bk = warp_sum(bk);
+                if (lane == 0) ksm[warp * nb + z] += bk;
+            }
+        }
+#pragma unroll
+        for (int f = 0; f < kWaveF; ++f) {
+            const double v = warp_sum(cacc[f]);
+            if (lane == 0) csm[warp][jj][f] = v;
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < jend * kWaveF; t += blockDim.x) {
+        const int jj = t / kWaveF, f = t % kWaveF;
+        double s = 0.0;
+        for (int w2 = 0; w2 < kAW / 32; ++w2) s += csm[w2][jj][f];
+        colpart[((int64_t)blockIdx.x * kWaveF + f) * n + j0 + jj] = s;
+    }
+    if (live) {
+        for (int c = 0; c < 3; ++c) {
+            rowpart[((int64_t)blockIdx.y * kRowF + c) * n + i] = xb[c];
+            rowpart[((int64_t)blockIdx.y * kRowF + 3 + c) * n + i] = nbi[c];
+        }
+    }
+    const int64_t P = (int64_t)gridDim.x * gridDim.y;
+    const int64_t blk = (int64_t)blockIdx.y * gridDim.x + blockIdx.x;
+    for (int z = threadIdx.x; z < nb; z += blockDim.x) {
+        double s = 0.0;
+        for (int w2 = 0; w2 < kAW / 32; ++w2) s += ksm[w2 * nb + z];
         kpart[(int64_t)z * P + blk] = s;
     }
 }
@@ -672,7 +1052,7 @@ struct Vjp {
 
 size_t part_words_needed(int64_t n, int nb)
 {
-    const int64_t rb = nblk(n, kAR), cb = nblk(n, kAC);
+    const int64_t rb = nblk(n, std::min(kAR, kAW)), cb = nblk(n, kAC);
     const int64_t pair = rb * cb;
     const size_t pairs = (size_t)cb * kRowF * n + (size_t)rb * GB_NF * n + (size_t)nb * pair;
     const size_t lin = (size_t)2 * nb * nblk(n, 256);
@@ -685,22 +1065,35 @@ int contract_pairs_wave(const Batch& bt, Vjp& vj, const double* d_k, int nb, int
 {
     mh_ctx* ctx = bt.ctx;
     const int64_t n = bt.n;
-    const unsigned rb = nblk(n, kAR), cb = nblk(n, kAC);
-    double* rowpart = vj.part;
-    double* colpart = rowpart + (size_t)cb * kRowF * n;
-    double* kpart = colpart + (size_t)rb * kWaveF * n;
+    const unsigned cb = nblk(n, kAC);
+    phase_begin(ctx, PH_ADJ_WAVE);
     for (int w = 0; w < vj.nwave; ++w) {
         const int kind = vj.wave_kinds[w];
-        const size_t smem = sizeof(double) * (kAR / 32) * nb;
-        k_adj_wave<<<dim3(rb, cb), kAR, smem, ctx->stream>>>(kind, bt.m->geom, n, bt.direct,
-                                                             kind == 2 ? tab : nullptr, d_k, nb, bt.nrhs,
-                                                             VA, VB, VC, VD, rowpart, colpart, kpart);
-        k_adj_reduce<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, rowpart, (int)cb, colpart, (int)rb, kWaveF,
+        const bool allw = kind == 2 && tab && nb >= kAdjAllwMinFreqs;
+        const unsigned nrb = nblk(n, allw ? kAW : kAR);
+        double* rowpart = vj.part;
+        double* colpart = rowpart + (size_t)cb * kRowF * n;
+        double* kpart = colpart + (size_t)nrb * kWaveF * n;
+        if (allw) {
+            const size_t smem = adj_allw_smem(nb);
+            MH_CUDA_TRY(ctx, cudaFuncSetAttribute(k_adj_delh_allw, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)smem));
+            k_adj_delh_allw<<<dim3(nrb, cb), kAW, smem, ctx->stream>>>(bt.m->geom, n, bt.direct, tab, d_k, nb,
+                                                                       bt.nrhs, VA, VB, VC, VD, rowpart, colpart,
+                                                                       kpart);
+        } else {
+            const size_t smem = sizeof(double) * (kAR / 32) * nb;
+            k_adj_wave<<<dim3(nrb, cb), kAR, smem, ctx->stream>>>(kind, bt.m->geom, n, bt.direct,
+                                                                 kind == 2 ? tab : nullptr, d_k, nb, bt.nrhs,
+                                                                 VA, VB, VC, VD, rowpart, colpart, kpart);
+        }
+        k_adj_reduce<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, rowpart, (int)cb, colpart, (int)nrb, kWaveF,
                                                             vj.gbar);
-        k_sum_parts<<<nb, 256, 0, ctx->stream>>>(kpart, (int64_t)rb * cb, vj.kbar + z0);
+        k_sum_parts<<<nb, 256, 0, ctx->stream>>>(kpart, (int64_t)nrb * cb, vj.kbar + z0);
         ctx->launches += 3;
         MH_CUDA_TRY(ctx, cudaGetLastError());
     }
+    phase_end(ctx, PH_ADJ_WAVE);
     return MH_OK;
 }
 
@@ -714,11 +1107,14 @@ int adjoint_tail(const Batch& bt, Vjp& vj, const double* d_omegas, const double*
     const int64_t n = bt.n;
     int rc;
     if (vj.rankine) {
+        phase_begin(ctx, PH_ADJ_RANKINE);
         const int64_t K = (int64_t)nb * bt.nrhs;
         if ((rc = zgemm_outer(ctx, n, K, VA, VB, vj.WS, 1.0))) return rc;
         if ((rc = zgemm_outer(ctx, n, K, VC, VD, vj.WD, -1.0))) return rc;
+        phase_end(ctx, PH_ADJ_RANKINE);
     }
     if ((rc = contract_pairs_wave(bt, vj, d_k, nb, z0, tab, VA, VB, VC, VD))) return rc;
+    phase_begin(ctx, PH_ADJ_LINEAR);
     const unsigned lb = nblk(n, 256);
     double* kpart = vj.part;
     double* wpart = kpart + (size_t)nb * lb;
@@ -727,6 +1123,7 @@ int adjoint_tail(const Batch& bt, Vjp& vj, const double* d_omegas, const double*
     k_sum_parts<<<nb, 256, 0, ctx->stream>>>(kpart, lb, vj.kbar + z0);
     k_sum_parts<<<nb, 256, 0, ctx->stream>>>(wpart, lb, vj.wbar + z0);
     ctx->launches += 3;
+    phase_end(ctx, PH_ADJ_LINEAR);
     MH_CUDA_TRY(ctx, cudaGetLastError());
     return MH_OK;
 }
@@ -738,6 +1135,7 @@ int seed_forces(const Batch& bt, Vjp& vj, const double* d_omegas, int nb, int z0
     const int64_t n = bt.n;
     const unsigned lb = nblk(n, 256);
     double* kpart = vj.part;
+    phase_begin(ctx, PH_ADJ_LINEAR);
     k_adj_forces<<<lb, 256, 0, ctx->stream>>>(bt.m->geom, n, bt.d_dofs, bt.ndof, bt.d_betas, bt.nbeta,
                                               d_omegas, nb, bt.rho, bt.g, PHI,
                                               vj.CF + (int64_t)z0 * bt.nrhs * bt.ndof,
@@ -745,6 +1143,7 @@ int seed_forces(const Batch& bt, Vjp& vj, const double* d_omegas, int nb, int z0
                                               vj.dofbar, kpart);
     k_sum_parts<<<nb, 256, 0, ctx->stream>>>(kpart, lb, vj.kbar + z0);
     ctx->launches += 2;
+    phase_end(ctx, PH_ADJ_LINEAR);
     MH_CUDA_TRY(ctx, cudaGetLastError());
     return MH_OK;
 }
@@ -782,6 +1181,7 @@ int adjoint_mixed_chunk(const Batch& bt, Vjp& vj, const double* d_omegas, const 
     const double* tab = delh_table_for(ctx, bt.mask, &rc);
     if (rc) return rc;
     if ((rc = seed_forces(bt, vj, d_omegas, nb, z0, bt.direct ? X : PHIi, PB))) return rc;
+    phase_begin(ctx, PH_ADJ_SOLVE);
     if (bt.direct) {
         MH_CUDA_TRY(ctx, cudaMemcpyAsync(RHS, PB, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, ctx->stream));
     } else if ((rc = zgemm_ct_strided(ctx, n, nrhs, S64, PB, RHS, nb, 1.0, 0.0))) {
@@ -823,10 +1223,9 @@ int adjoint_mixed_chunk(const Batch& bt, Vjp& vj, const double* d_omegas, const 
         if ((rc = fp64_getrs(ctx, true, n, fb.lu + (int64_t)z * nn, fb.piv + (int64_t)z * n, Lz, nrhs)))
             return rc;
     }
-    if (bt.direct) {
-        if ((rc = zgemm_ct_strided(ctx, n, nrhs, S64, LAM, BB, nb, 1.0, 0.0))) return rc;
-        return adjoint_tail(bt, vj, d_omegas, d_k, nb, z0, tab, LAM, BC, LAM, X, BB);
-    }
+    if (bt.direct && (rc = zgemm_ct_strided(ctx, n, nrhs, S64, LAM, BB, nb, 1.0, 0.0))) return rc;
+    phase_end(ctx, PH_ADJ_SOLVE);
+    if (bt.direct) return adjoint_tail(bt, vj, d_omegas, d_k, nb, z0, tab, LAM, BC, LAM, X, BB);
     return adjoint_tail(bt, vj, d_omegas, d_k, nb, z0, tab, PB, X, LAM, X, LAM);
 }
 
@@ -872,16 +1271,16 @@ int fp64_vjp_one(const Batch& bt, Vjp& vj, const double* d_omega, const double* 
     phase_end(ctx, PH_FP64_LU);
     MH_CUDA_TRY(ctx, launch_forces_batch(bt, d_omega, 1, PHI, d_F, d_FK));
     if ((rc = seed_forces(bt, vj, d_omega, 1, z, PHI, PB))) return rc;
+    phase_begin(ctx, PH_ADJ_SOLVE);
     if (bt.direct) {
         MH_CUDA_TRY(ctx, cudaMemcpyAsync(LAM, PB, sizeof(double2) * nv, cudaMemcpyDeviceToDevice, ctx->stream));
     } else if ((rc = zgemm_ct_strided(ctx, n, nrhs, S, PB, LAM, 1, 1.0, 0.0))) {
         return rc;
     }
     if ((rc = fp64_getrs(ctx, true, n, D, piv, LAM, nrhs))) return rc;
-    if (bt.direct) {
-        if ((rc = zgemm_ct_strided(ctx, n, nrhs, S, LAM, BB, 1, 1.0, 0.0))) return rc;
-        return adjoint_tail(bt, vj, d_omega, d_k, 1, z, tab, LAM, BC, LAM, X, BB);
-    }
+    if (bt.direct && (rc = zgemm_ct_strided(ctx, n, nrhs, S, LAM, BB, 1, 1.0, 0.0))) return rc;
+    phase_end(ctx, PH_ADJ_SOLVE);
+    if (bt.direct) return adjoint_tail(bt, vj, d_omega, d_k, 1, z, tab, LAM, BC, LAM, X, BB);
     return adjoint_tail(bt, vj, d_omega, d_k, 1, z, tab, PB, X, LAM, X, LAM);
 }
 
@@ -1006,6 +1405,7 @@ int hydro_batch_vjp(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double*
     }
     if (rc) return rc;
     if (vj.rankine) {
+        phase_begin(ctx, PH_ADJ_RANKINE);
         const unsigned rb = nblk(n, kAR), cb = nblk(n, kAC);
         double* rowpart = vj.part;
         double* colpart = rowpart + (size_t)cb * kRowF * n;
@@ -1014,8 +1414,10 @@ int hydro_batch_vjp(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double*
         k_adj_reduce<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, rowpart, (int)cb, colpart, (int)rb, GB_NF,
                                                             vj.gbar);
         ctx->launches += 2;
+        phase_end(ctx, PH_ADJ_RANKINE);
         MH_CUDA_TRY(ctx, cudaGetLastError());
     }
+    phase_collect(ctx);
     // ---- results to the host ----
     std::vector<double2> h(out_count);
     std::vector<double> hg(gb_words);

@@ -41,7 +41,7 @@ constexpr int kMaxRhs = 16;
 // Phases timed with CUDA events when profiling is on (mh_ctx_set_profiling).
 enum Phase : int {
     PH_RANKINE = 0, PH_WAVE, PH_RHS, PH_LU, PH_REFINE, PH_FORCES, PH_FP64_ASSEMBLY, PH_FP64_LU,
-    PH_N
+    PH_ADJ_SOLVE, PH_ADJ_WAVE, PH_ADJ_RANKINE, PH_ADJ_LINEAR, PH_N
 };
 
 struct mh_ctx {

@@ -206,3 +206,29 @@ def test_rrule_pullback(mh, gpu, setup):
     assert np.allclose(mt.centers, r.mesh.centers, rtol=1e-12, atol=0)
     assert np.allclose(wbar, r.omegas, rtol=1e-12, atol=0)
     assert np.allclose(A, r.added_mass, rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("direct", [True, False])
+def test_vjp_frequency_batched_delhommeau(mh, gpu, direct):
+    """Chunks of >= 4 frequencies take the frequency-batched Delhommeau
+    adjoint (alpha contraction once per pair); over [0.3, 4.0] rad/s pairs
+    leave the polar patch, so the per-point path runs too.  Checked against
+    the per-frequency path (one frequency per call) and, for omega, against
+    central differences."""
+    mesh = mh.mesh_hemisphere(1.3, (0, 0, 0), (10, 14))
+    body = mh.FloatingBody.rigid(mesh, ["Heave", "Surge"])
+    dofs = list(body.dofs.values())
+    om = np.linspace(0.3, 4.0, 7)
+    w = _weights(2, len(om), 1, seed=4)
+    batched = _vjp(mh, gpu, mesh, om, dofs, [0.2], w, DELH, direct, "mixed")
+    wA, wB, wF, wK = w
+    acc = None
+    for z in range(len(om)):
+        r = mh.hydro_batch_vjp(mesh, om[z:z + 1], dofs, [0.2], wA[:, :, z:z + 1], wB[:, :, z:z + 1],
+                               wF[:, z:z + 1], wK[:, z:z + 1], green_functions=_gfs(mh, DELH),
+                               direct=direct, precision="fp64", ctx=gpu)
+        acc = r.mesh if acc is None else acc + r.mesh
+        assert abs(r.omegas[0] - batched.omegas[z]) <= 1e-8 * np.max(np.abs(batched.omegas))
+    for f in ("vertices", "centers", "normals", "areas"):
+        x, y = getattr(batched.mesh, f), getattr(acc, f)
+        assert np.max(np.abs(x - y)) <= 1e-8 * np.max(np.abs(y)), f
