@@ -110,8 +110,7 @@ __device__ __forceinline__ void from_duals(const cx<d2>* o, GDer& g)
     }
 }
 
-// (r, z) derivatives by 2-way dual numbers: Wu's formulas (kind 1) or the
-// Delhommeau quadrature with the second derivatives from its identities.
+// (r, z) derivatives of Wu's formulas by 2-way dual numbers.
 __device__ __noinline__ void wave_dimless_dual(int kind, double r, double z, GDer* g)
 {
     d2 rd, zd;
@@ -122,141 +121,49 @@ __device__ __noinline__ void wave_dimless_dual(int kind, double r, double z, GDe
     zd.d[0] = 0.0;
     zd.d[1] = 1.0;
     cx<d2> o[3];
-    if (kind == 1) wu_dimless(rd, zd, o);
-    else delh_exact_t(rd, zd, o);
+    (void)kind;
+    wu_dimless(rd, zd, o);
     from_duals(o, *g);
 }
 
-// Value and gradient of a 2-D Chebyshev series sum c[i*N+j] T_i(u) T_j(v)
-// (nested Clenshaw; the derivative recurrences d b_k = 2 b_{k+1} +
-// 2x d b_{k+1} - d b_{k+2} run beside the values).
-template <int N>
-__device__ __forceinline__ void cheb2d_grad(const double* __restrict__ c, double u, double v, double& f,
-                                            double& fu, double& fv)
+// r, z derivatives of the Delhommeau wave term from its values: with
+// G_r = G1 and G_z = G2 = G + 2/R (exact_Guevel_Delhommeau.jl:56), the wave
+// part is harmonic in the fluid, so G_zz = G_z - 2z/R^3, G_rz = G_r - 2r/R^3
+// and G_rr = -G_r/r - G_zz (-G_zz/2 as r -> 0).  These are the derivatives
+// of the function itself (what the reference's AD of its quadrature
+// gives), whichever way its values were obtained.
+__device__ __forceinline__ void gder_identities(const cplx G[3], double r, double z, double R, GDer& o)
 {
-    double a1 = 0.0, a2 = 0.0, da1 = 0.0, da2 = 0.0, e1 = 0.0, e2 = 0.0;
-#pragma unroll 1
-    for (int i = N - 1; i >= 0; --i) {
-        const double* ci = c + i * N;
-        double b1 = 0.0, b2 = 0.0, db1 = 0.0, db2 = 0.0;
-#pragma unroll 4
-        for (int j = N - 1; j >= 1; --j) {
-            const double t = fma(2.0 * v, b1, __ldg(ci + j) - b2);
-            const double dt = fma(2.0 * v, db1, fma(2.0, b1, -db2));
-            b2 = b1;
-            b1 = t;
-            db2 = db1;
-            db1 = dt;
-        }
-        const double si = fma(v, b1, __ldg(ci) - b2);
-        const double dsi = fma(v, db1, b1 - db2);
-        if (i >= 1) {
-            const double t = fma(2.0 * u, a1, si - a2);
-            const double dt = fma(2.0 * u, da1, fma(2.0, a1, -da2));
-            const double et = fma(2.0 * u, e1, dsi - e2);
-            a2 = a1;
-            a1 = t;
-            da2 = da1;
-            da1 = dt;
-            e2 = e1;
-            e1 = et;
-        } else {
-            f = fma(u, a1, si - a2);
-            fu = fma(u, da1, a1 - da2);
-            fv = fma(u, e1, dsi - e2);
-        }
-    }
+    const double iR = 1.0 / R, iR3 = iR * iR * iR;
+    const cplx Gzz = G[2] - mk(2.0 * z * iR3, 0.0);
+    const cplx Grz = G[1] - mk(2.0 * r * iR3, 0.0);
+    const cplx Grr = (r > 1e-3) ? -(G[1] / r) - Gzz : mk(-0.5 * Gzz.re, -0.5 * Gzz.im);
+#pragma unroll
+    for (int m = 0; m < 3; ++m) o.G[m] = G[m];
+    o.Gr[0] = G[1];
+    o.Gz[0] = G[2];
+    o.Gr[1] = Grr;
+    o.Gz[1] = Grz;
+    o.Gr[2] = Grz;
+    o.Gz[2] = Gzz;
 }
 
-// G, G_r, G_z and their r, z derivatives from the tabulated smooth parts
-// (B, C with their r, z derivatives), E0 = e^z J0(r), E1 = e^z J1(r) and
-// L = log((R + |z|)/2): G = -2 E0 L + B + 2 pi i E0,
-// G_r = 2 E1 L - 2 E0 r / (R (R + |z|)) + C - 2 pi i E1, G_z = G + 2/R;
-// dE0/dr = -E1, dE1/dr = E0 - E1/r, d/dz e^z = e^z.
-__device__ __forceinline__ void delh_grad_from_parts(double B, double Br, double Bz, double C, double Cr, double Cz,
-                                                     double E0, double E1, double r, double R, double az,
-                                                     double L, GDer& o)
-{
-    const double iR = 1.0 / R;
-    const double sr = r * iR, sz = -az * iR;
-    const double D1 = 1.0 / (R + az);
-    const double Lr = sr * D1, Lz = (sz - 1.0) * D1;
-    const double iM = iR * D1;  // 1 / (R (R + |z|))
-    const double Q = r * iM;
-    const double Mr = sr * (2.0 * R + az), Mz = sz * (2.0 * R + az) - R;
-    const double Qr = (1.0 - Q * Mr) * iM, Qz = -Q * Mz * iM;
-    const double E1r = (r > 1e-3) ? E0 - E1 / r : 0.5 * E0;
-    const double tp = 2.0 * kPi;
-    const double G0 = -2.0 * E0 * L + B;
-    const double G0r = 2.0 * E1 * L - 2.0 * E0 * Lr + Br;
-    const double G0z = -2.0 * E0 * L - 2.0 * E0 * Lz + Bz;
-    o.G[0] = mk(G0, tp * E0);
-    o.Gr[0] = mk(G0r, -tp * E1);
-    o.Gz[0] = mk(G0z, tp * E0);
-    o.G[1] = mk(2.0 * E1 * L - 2.0 * E0 * Q + C, -tp * E1);
-    o.Gr[1] = mk(2.0 * E1r * L + 2.0 * E1 * Lr + 2.0 * E1 * Q - 2.0 * E0 * Qr + Cr, -tp * E1r);
-    o.Gz[1] = mk(2.0 * E1 * L + 2.0 * E1 * Lz - 2.0 * E0 * Q - 2.0 * E0 * Qz + Cz, -tp * E1);
-    const double iR2 = iR * iR;
-    o.G[2] = mk(G0 + 2.0 * iR, tp * E0);
-    o.Gr[2] = mk(G0r - 2.0 * sr * iR2, -tp * E1);
-    o.Gz[2] = mk(G0z - 2.0 * sz * iR2, tp * E0);
-}
-
-// Tabulated Delhommeau term with its r, z derivatives at one point, the
-// derivative of exactly what delh_dimless_table evaluates; outside the
-// table, the quadrature path.
+// Delhommeau term and its r, z derivatives at one point: the forward's
+// value (table, or the quadrature outside it / without a table), then the
+// identities.
 __device__ __noinline__ void delh_point_grad(const double* __restrict__ tab, double r, double z, GDer* out)
 {
-    const double az = -z;
-    const double R = hypot(r, z);
-    double B, Br, Bz, C, Cr, Cz;
-    if (!(az >= 0.0)) {
-        wave_dimless_dual(2, r, z, out);
-        return;
-    }
-    if (R < kTabRPolar) {
-        const double alpha = atan2(r, az);
-        const double u = 2.0 * R / kTabRPolar - 1.0;
-        const double v = 4.0 * alpha / kPi - 1.0;
-        double fu, fv;
-        const double sr = r / R, sz = z / R;
-        cheb2d_grad<kTabNP>(tab, u, v, B, fu, fv);
-        double BR = fu * (2.0 / kTabRPolar), Ba = fv * (4.0 / kPi);
-        Br = BR * sr - Ba * sz / R;
-        Bz = BR * sz + Ba * sr / R;
-        cheb2d_grad<kTabNP>(tab + kTabNP * kTabNP, u, v, C, fu, fv);
-        BR = fu * (2.0 / kTabRPolar);
-        Ba = fv * (4.0 / kPi);
-        Cr = BR * sr - Ba * sz / R;
-        Cz = BR * sz + Ba * sr / R;
-    } else if (r < kTabExtent && az < kTabExtent) {
-        const int ir = min((int)(r / kTabH), kTabNCell - 1);
-        const int iz = min((int)(az / kTabH), kTabNCell - 1);
-        const double* c = tab + kTabPolarWords + (iz * kTabNCell + ir) * kTabCellWords;
-        const double u = 2.0 * (r - ir * kTabH) / kTabH - 1.0;
-        const double v = 2.0 * (az - iz * kTabH) / kTabH - 1.0;
-        double fu, fv;
-        cheb2d_grad<kTabNC>(c, u, v, B, fu, fv);
-        Br = fu * (2.0 / kTabH);
-        Bz = -fv * (2.0 / kTabH);
-        cheb2d_grad<kTabNC>(c + kTabNC * kTabNC, u, v, C, fu, fv);
-        Cr = fu * (2.0 / kTabH);
-        Cz = -fv * (2.0 / kTabH);
-    } else {
-        wave_dimless_dual(2, r, z, out);
-        return;
-    }
-    const double e = exp(z);
-    const double E0 = e * j0(r), E1 = e * j1(r);
-    const double L = log(0.5 * (R + az));
-    delh_grad_from_parts(B, Br, Bz, C, Cr, Cz, E0, E1, r, R, az, L, *out);
+    cplx G[3];
+    if (tab) delh_dimless_table(tab, r, z, G);
+    else delh_dimless(r, z, G);
+    gder_identities(G, r, z, hypot(r, z), *out);
 }
 
-// kind 1: Wu; kind 2: Delhommeau (table when tab != null, else quadrature).
+// kind 1: Wu (exact derivatives of its formulas); kind 2: Delhommeau.
 __device__ __forceinline__ void wave_dimless_grad(int kind, const double* __restrict__ tab, double r, double z,
                                                   GDer& g)
 {
-    if (kind == 2 && tab) delh_point_grad(tab, r, z, &g);
+    if (kind == 2) delh_point_grad(tab, r, z, &g);
     else wave_dimless_dual(kind, r, z, &g);
 }
 
@@ -424,26 +331,38 @@ k_adj_wave(int kind, const double* __restrict__ geom, int64_t n, int direct, con
     }
 }
 
+// One (pair, frequency) of the Delhommeau adjoint off the polar patch: the
+// per-point table gradient and the chain (out of line, so the polar path
+// keeps its state in registers).
+__device__ __noinline__ void delh_pair_vjp_point(const double* __restrict__ tab, const WaveGeom* wg, double k,
+                                                 double A, bool wrt_first, cplx cs, cplx cw, const double* nD,
+                                                 WaveBar* wb)
+{
+    GDer o;
+    delh_point_grad(tab, k * wg->dis, k * wg->zs, &o);
+    wave_chain(o, *wg, k, A, wrt_first, cs, cw, nD, *wb);
+}
+
 // Frequency-batched adjoint of the tabulated Delhommeau term (the reverse
-// of the forward's frequency-batched pass).  A pair keeps its polar angle
-// alpha at every frequency, so the alpha direction of the polar tables is
-// contracted once per pair into six series in R (shared memory, one column
-// per thread): B and C with their alpha derivatives, E0 = e^z J0(r) and
-// E1 = e^z J1(r).  Each frequency then runs 1-D Clenshaw recurrences in
-// u(R) for the values and u-derivatives, two frequencies at a time, and the
-// r, z derivatives follow from dR = (r dr + z dz)/R, dalpha = (|z| dr +
-// r dz)/R^2.  Frequencies at which the pair leaves the polar patch take the
-// per-point table gradient.  Partial sums as k_adj_wave.
+// of the forward's frequency-batched pass, same arithmetic for the values).
+// A pair keeps its polar angle alpha at every frequency, so the alpha
+// direction of the four polar tables (B, C, E0 = e^z J0(r), E1 = e^z J1(r))
+// is contracted once per pair into series in R (shared memory, one column
+// per thread); each frequency runs 1-D Clenshaw recurrences in u(R), two
+// frequencies at a time, forms (G, G_r, G_z) as the forward does and takes
+// the derivatives from the identities.  Frequencies at which the pair
+// leaves the polar patch use the per-point table.  Partial sums as
+// k_adj_wave.
 constexpr int kAW = 64;  // rows (threads) per CTA
 constexpr int kZC = 2;   // frequencies per Clenshaw pass
-constexpr int kNS = 6;   // series: B, dB/dalpha, C, dC/dalpha, E0, E1
+constexpr int kNS = 4;   // series: B, C, E0, E1
 
 size_t adj_allw_smem(int nb)
 {
     return sizeof(double) * ((size_t)kNS * kTabNP * kAW + (size_t)(kAW / 32) * nb + nb);
 }
 
-__global__ void __launch_bounds__(kAW, 3)
+__global__ void __launch_bounds__(kAW, 5)
 k_adj_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const double* __restrict__ tab,
                 const double* __restrict__ kvec, int nb, int nrhs, const double2* __restrict__ VA,
                 const double2* __restrict__ VB, const double2* __restrict__ VC, const double2* __restrict__ VD,
@@ -478,29 +397,24 @@ k_adj_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const do
         const double az1 = -wg.zs;
         const double rho = hypot(wg.dis, wg.zs);
         const bool polar_ok = az1 >= 0.0 && rho > 0.0;
-        const double sr = polar_ok ? wg.dis / rho : 0.0, sz = polar_ok ? wg.zs / rho : 0.0;
         const double lp = log(0.5 * (rho + az1));
-        if (polar_ok) {  // contract alpha: values (and alpha derivatives of B, C)
+        const double gp = wg.dis / (rho * (rho + az1));  // r / (R (R + |z|)) at k = 1
+        if (polar_ok) {  // contract alpha: w_q[row] = sum_col c_q[row][col] T_col(v)
             const double v = 4.0 * atan2(wg.dis, az1) / kPi - 1.0;
 #pragma unroll 1
-            for (int q = 0; q < 4; ++q) {
+            for (int q = 0; q < kNS; ++q) {
                 const double* c = tab + q * kTabNP * kTabNP;
-                const int slot = (q < 2) ? 2 * q : q + 2;
 #pragma unroll 1
                 for (int row = 0; row < kTabNP; ++row) {
                     const double* cr = c + row * kTabNP;
-                    double b1 = 0.0, b2 = 0.0, d1 = 0.0, d2 = 0.0;
+                    double b1 = 0.0, b2 = 0.0;
 #pragma unroll
                     for (int col = kTabNP - 1; col >= 1; --col) {
                         const double t = fma(2.0 * v, b1, __ldg(cr + col) - b2);
-                        const double dt = fma(2.0 * v, d1, fma(2.0, b1, -d2));
                         b2 = b1;
                         b1 = t;
-                        d2 = d1;
-                        d1 = dt;
                     }
-                    wt[(slot * kTabNP + row) * kAW] = fma(v, b1, __ldg(cr) - b2);
-                    if (q < 2) wt[((slot + 1) * kTabNP + row) * kAW] = (4.0 / kPi) * fma(v, d1, b1 - d2);
+                    wt[(q * kTabNP + row) * kAW] = fma(v, b1, __ldg(cr) - b2);
                 }
             }
         }
@@ -508,60 +422,10 @@ k_adj_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const do
         for (int zc = 0; zc < nb; zc += kZC) {
             double kk[kZC], uu[kZC];
             bool pol[kZC];
+            cplx csz[kZC], cwz[kZC];  // weights first: their loads overlap the recurrences
 #pragma unroll
             for (int t = 0; t < kZC; ++t) {
                 const int z = min(zc + t, nb - 1);
-                kk[t] = kvec[z];
-                const double R = kk[t] * rho;
-                pol[t] = polar_ok && (zc + t < nb) && R < kTabRPolar;
-                uu[t] = 2.0 * R / kTabRPolar - 1.0;
-            }
-            // series values (sv) and u-derivatives of B, C (su), Clenshaw in u
-            double sv[kZC][kNS], su[kZC][2];
-            if (pol[0] || pol[kZC - 1]) {
-                double b1[kZC][kNS], b2[kZC][kNS], e1[kZC][2], e2[kZC][2];
-#pragma unroll
-                for (int t = 0; t < kZC; ++t) {
-#pragma unroll
-                    for (int q = 0; q < kNS; ++q) b1[t][q] = b2[t][q] = 0.0;
-                    e1[t][0] = e1[t][1] = e2[t][0] = e2[t][1] = 0.0;
-                }
-#pragma unroll 2
-                for (int row = kTabNP - 1; row >= 1; --row) {
-                    double cq[kNS];
-#pragma unroll
-                    for (int q = 0; q < kNS; ++q) cq[q] = wt[(q * kTabNP + row) * kAW];
-#pragma unroll
-                    for (int t = 0; t < kZC; ++t) {
-                        const double u2 = 2.0 * uu[t];
-                        // derivatives of the B (q = 0) and C (q = 2) series
-                        const double dB = fma(u2, e1[t][0], fma(2.0, b1[t][0], -e2[t][0]));
-                        const double dC = fma(u2, e1[t][1], fma(2.0, b1[t][2], -e2[t][1]));
-                        e2[t][0] = e1[t][0];
-                        e1[t][0] = dB;
-                        e2[t][1] = e1[t][1];
-                        e1[t][1] = dC;
-#pragma unroll
-                        for (int q = 0; q < kNS; ++q) {
-                            const double nt = fma(u2, b1[t][q], cq[q] - b2[t][q]);
-                            b2[t][q] = b1[t][q];
-                            b1[t][q] = nt;
-                        }
-                    }
-                }
-#pragma unroll
-                for (int t = 0; t < kZC; ++t) {
-#pragma unroll
-                    for (int q = 0; q < kNS; ++q) sv[t][q] = fma(uu[t], b1[t][q], wt[q * kTabNP * kAW] - b2[t][q]);
-                    su[t][0] = fma(uu[t], e1[t][0], b1[t][0] - e2[t][0]);
-                    su[t][1] = fma(uu[t], e1[t][1], b1[t][2] - e2[t][1]);
-                }
-            }
-#pragma unroll
-            for (int t = 0; t < kZC; ++t) {
-                const int z = zc + t;
-                if (z >= nb) break;
-                const double k = kk[t];
                 const int64_t base = (int64_t)z * nv;
                 double sr_ = 0.0, si_ = 0.0, dr_ = 0.0, di_ = 0.0;
                 for (int q = 0; q < nrhs; ++q) {
@@ -572,24 +436,64 @@ k_adj_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const do
                     dr_ -= c.x * d.x + c.y * d.y;
                     di_ -= c.y * d.x - c.x * d.y;
                 }
-                const cplx cs = mk(-kI4P * sr_, kI4P * si_), cw = mk(-kI4P * dr_, kI4P * di_);
+                csz[t] = mk(-kI4P * sr_, kI4P * si_);
+                cwz[t] = mk(-kI4P * dr_, kI4P * di_);
+                kk[t] = kvec[z];
+                const double R = kk[t] * rho;
+                pol[t] = polar_ok && (zc + t < nb) && R < kTabRPolar;
+                uu[t] = 2.0 * R / kTabRPolar - 1.0;
+            }
+            double sv[kZC][kNS];
+            if (pol[0] || pol[kZC - 1]) {
+                double b1[kZC][kNS], b2[kZC][kNS];
+#pragma unroll
+                for (int t = 0; t < kZC; ++t)
+#pragma unroll
+                    for (int q = 0; q < kNS; ++q) b1[t][q] = b2[t][q] = 0.0;
+#pragma unroll 2
+                for (int row = kTabNP - 1; row >= 1; --row) {
+                    double cq[kNS];
+#pragma unroll
+                    for (int q = 0; q < kNS; ++q) cq[q] = wt[(q * kTabNP + row) * kAW];
+#pragma unroll
+                    for (int t = 0; t < kZC; ++t) {
+                        const double u2 = 2.0 * uu[t];
+#pragma unroll
+                        for (int q = 0; q < kNS; ++q) {
+                            const double nt = fma(u2, b1[t][q], cq[q] - b2[t][q]);
+                            b2[t][q] = b1[t][q];
+                            b1[t][q] = nt;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int t = 0; t < kZC; ++t)
+#pragma unroll
+                    for (int q = 0; q < kNS; ++q) sv[t][q] = fma(uu[t], b1[t][q], wt[q * kTabNP * kAW] - b2[t][q]);
+            }
+#pragma unroll
+            for (int t = 0; t < kZC; ++t) {
+                const int z = zc + t;
+                if (z >= nb) break;
+                const double k = kk[t];
                 double bk = 0.0;
                 if (live) {
-                    GDer o;
-                    if (pol[t]) {
-                        const double R = k * rho, r = k * wg.dis, azk = k * az1;
-                        const double iR = 1.0 / R;
-                        const double BR = su[t][0] * (2.0 / kTabRPolar), CR = su[t][1] * (2.0 / kTabRPolar);
-                        const double Ba = sv[t][1], Ca = sv[t][3];
-                        const double Br = BR * sr - Ba * sz * iR, Bz = BR * sz + Ba * sr * iR;
-                        const double Cr = CR * sr - Ca * sz * iR, Cz = CR * sz + Ca * sr * iR;
-                        delh_grad_from_parts(sv[t][0], Br, Bz, sv[t][2], Cr, Cz, sv[t][4], sv[t][5], r, R, azk,
-                                             logk[z] + lp, o);
-                    } else {
-                        delh_point_grad(tab, k * wg.dis, k * wg.zs, &o);
-                    }
                     WaveBar wb;
-                    wave_chain(o, wg, k, p.area, !direct, cs, cw, nD, wb);
+                    if (pol[t]) {
+                        const double R = k * rho;
+                        const double B = sv[t][0], C = sv[t][1], E0 = sv[t][2], E1 = sv[t][3];
+                        const double L = logk[z] + lp;
+                        cplx G[3];
+                        const double G_re = -2.0 * E0 * L + B, G_im = 2.0 * kPi * E0;
+                        G[0] = mk(G_re, G_im);
+                        G[1] = mk(2.0 * E1 * L - 2.0 * E0 * gp / k + C, -2.0 * kPi * E1);
+                        G[2] = mk(G_re + 2.0 / R, G_im);
+                        GDer o;
+                        gder_identities(G, k * wg.dis, k * wg.zs, R, o);
+                        wave_chain(o, wg, k, p.area, !direct, csz[t], cwz[t], nD, wb);
+                    } else {
+                        delh_pair_vjp_point(tab, &wg, k, p.area, !direct, csz[t], cwz[t], nD, &wb);
+                    }
                     xb[0] += wb.dx;
                     xb[1] += wb.dy;
                     xb[2] += wb.zs;
@@ -1053,8 +957,7 @@ struct Vjp {
 size_t part_words_needed(int64_t n, int nb)
 {
     const int64_t rb = nblk(n, std::min(kAR, kAW)), cb = nblk(n, kAC);
-    const int64_t pair = rb * cb;
-    const size_t pairs = (size_t)cb * kRowF * n + (size_t)rb * GB_NF * n + (size_t)nb * pair;
+    const size_t pairs = (size_t)cb * kRowF * n + (size_t)rb * GB_NF * n + (size_t)nb * rb * cb;
     const size_t lin = (size_t)2 * nb * nblk(n, 256);
     return std::max(pairs, lin);
 }
@@ -1070,26 +973,27 @@ int contract_pairs_wave(const Batch& bt, Vjp& vj, const double* d_k, int nb, int
     for (int w = 0; w < vj.nwave; ++w) {
         const int kind = vj.wave_kinds[w];
         const bool allw = kind == 2 && tab && nb >= kAdjAllwMinFreqs;
-        const unsigned nrb = nblk(n, allw ? kAW : kAR);
+        const unsigned nrb = allw ? nblk(n, kAW) : nblk(n, kAR);
+        const unsigned ncb = cb;
         double* rowpart = vj.part;
-        double* colpart = rowpart + (size_t)cb * kRowF * n;
+        double* colpart = rowpart + (size_t)ncb * kRowF * n;
         double* kpart = colpart + (size_t)nrb * kWaveF * n;
         if (allw) {
             const size_t smem = adj_allw_smem(nb);
             MH_CUDA_TRY(ctx, cudaFuncSetAttribute(k_adj_delh_allw, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                   (int)smem));
-            k_adj_delh_allw<<<dim3(nrb, cb), kAW, smem, ctx->stream>>>(bt.m->geom, n, bt.direct, tab, d_k, nb,
-                                                                       bt.nrhs, VA, VB, VC, VD, rowpart, colpart,
-                                                                       kpart);
+            k_adj_delh_allw<<<dim3(nrb, ncb), kAW, smem, ctx->stream>>>(bt.m->geom, n, bt.direct, tab, d_k, nb,
+                                                                        bt.nrhs, VA, VB, VC, VD, rowpart, colpart,
+                                                                        kpart);
         } else {
             const size_t smem = sizeof(double) * (kAR / 32) * nb;
             k_adj_wave<<<dim3(nrb, cb), kAR, smem, ctx->stream>>>(kind, bt.m->geom, n, bt.direct,
                                                                  kind == 2 ? tab : nullptr, d_k, nb, bt.nrhs,
                                                                  VA, VB, VC, VD, rowpart, colpart, kpart);
         }
-        k_adj_reduce<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, rowpart, (int)cb, colpart, (int)nrb, kWaveF,
+        k_adj_reduce<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, rowpart, (int)ncb, colpart, (int)nrb, kWaveF,
                                                             vj.gbar);
-        k_sum_parts<<<nb, 256, 0, ctx->stream>>>(kpart, (int64_t)nrb * cb, vj.kbar + z0);
+        k_sum_parts<<<nb, 256, 0, ctx->stream>>>(kpart, (int64_t)nrb * ncb, vj.kbar + z0);
         ctx->launches += 3;
         MH_CUDA_TRY(ctx, cudaGetLastError());
     }
@@ -1193,11 +1097,10 @@ int adjoint_mixed_chunk(const Batch& bt, Vjp& vj, const double* d_omegas, const 
     std::vector<double> h_res(nb, INFINITY);
     for (int it = 1; it <= max_iter; ++it) {
         MH_CUDA_TRY(ctx, launch_to_f32(ctx, R, R32, cnt));
-        MH_CUDA_TRY(ctx, launch_lu_solve_ct(ctx, tc ? MH_LU_TCGEN05_F16 : MH_LU_SIMT_F32, Dlo, n, nn, nb, Dinv,
-                                            R32, T32, nv, nrhs));
+        MH_CUDA_TRY(ctx, launch_lu_solve_persist(ctx, tc ? MH_LU_TCGEN05_F16 : MH_LU_SIMT_F32, true, Dlo, n, nn,
+                                                 nb, Dinv, R32, nv, nrhs));
         MH_CUDA_TRY(ctx, launch_add_f32(ctx, LAM, R32, cnt));
-        MH_CUDA_TRY(ctx, cudaMemcpyAsync(R, RHS, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, ctx->stream));
-        if ((rc = zgemm_ct_strided(ctx, n, nrhs, D64, LAM, R, nb, -1.0, 1.0))) return rc;
+        MH_CUDA_TRY(ctx, launch_residual(ctx, true, D64, n, nb, LAM, RHS, R, nrhs));
         MH_CUDA_TRY(ctx, launch_rel_residual(ctx, R, RHS, n, nrhs, nb, misc));
         MH_CUDA_TRY(ctx, cudaMemcpyAsync(h_res.data(), misc, sizeof(double) * nb, cudaMemcpyDeviceToHost,
                                          ctx->stream));

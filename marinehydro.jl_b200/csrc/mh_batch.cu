@@ -359,6 +359,82 @@ __global__ void k_add_f32(double2* __restrict__ x, const float2* __restrict__ d,
     if (t < count) x[t] = make_double2(x[t].x + (double)d[t].x, x[t].y + (double)d[t].y);
 }
 
+// Refinement residuals in FP64, bandwidth-bound reads of the n x n complex
+// matrices (column-major, nb of them, n*n apart), nrhs <= kMaxRhs:
+// k_resid_n: R = B - A X, one thread per row i, coalesced down the columns;
+// k_resid_c: R = B - A^H X, one warp per output j reading column j.
+// Q >= nrhs: accumulators per thread (4, 8 or 16, picked by the launcher).
+template <int Q>
+__global__ void __launch_bounds__(256)
+k_resid_n(const double2* __restrict__ A, const double2* __restrict__ X, const double2* __restrict__ B,
+          double2* __restrict__ R, int64_t n, int nrhs)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t b = blockIdx.y;
+    if (i >= n) return;
+    const double2* M = A + b * n * n;
+    const double2* x = X + b * n * nrhs;
+    double ar[Q], ai[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) ar[q] = ai[q] = 0.0;
+#pragma unroll 4
+    for (int64_t j = 0; j < n; ++j) {
+        const double2 m = M[j * n + i];
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+            if (q < nrhs) {
+                const double2 v = __ldg(x + (int64_t)q * n + j);
+                ar[q] = fma(m.x, v.x, fma(-m.y, v.y, ar[q]));
+                ai[q] = fma(m.x, v.y, fma(m.y, v.x, ai[q]));
+            }
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+        if (q < nrhs) {
+            const int64_t o = b * n * nrhs + (int64_t)q * n + i;
+            R[o] = make_double2(B[o].x - ar[q], B[o].y - ai[q]);
+        }
+}
+
+template <int Q>
+__global__ void __launch_bounds__(256)
+k_resid_c(const double2* __restrict__ A, const double2* __restrict__ X, const double2* __restrict__ B,
+          double2* __restrict__ R, int64_t n, int nrhs)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t j = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int64_t b = blockIdx.y;
+    if (j >= n) return;  // whole warps leave together
+    const double2* col = A + b * n * n + j * n;
+    const double2* x = X + b * n * nrhs;
+    double ar[Q], ai[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) ar[q] = ai[q] = 0.0;
+#pragma unroll 4
+    for (int64_t i = lane; i < n; i += 32) {
+        const double2 m = col[i];  // conj(m) * x
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+            if (q < nrhs) {
+                const double2 v = __ldg(x + (int64_t)q * n + i);
+                ar[q] = fma(m.x, v.x, fma(m.y, v.y, ar[q]));
+                ai[q] = fma(m.x, v.y, fma(-m.y, v.x, ai[q]));
+            }
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q)
+        if (q < nrhs) {
+            for (int off = 16; off > 0; off >>= 1) {
+                ar[q] += __shfl_down_sync(0xffffffffu, ar[q], off);
+                ai[q] += __shfl_down_sync(0xffffffffu, ai[q], off);
+            }
+            if (lane == 0) {
+                const int64_t o = b * n * nrhs + (int64_t)q * n + j;
+                R[o] = make_double2(B[o].x - ar[q], B[o].y - ai[q]);
+            }
+        }
+}
+
 // Per (frequency z = blockIdx.x): max over right-hand sides of
 // max_i |r_iq| / max_i |b_iq|.
 __global__ void __launch_bounds__(256)
@@ -591,14 +667,12 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
     for (it = 1; it <= max_iter; ++it) {
         k_to_f32<<<blocks(cnt, 256), 256, 0, ctx->stream>>>(R, R32, cnt);
         ctx->launches += 1;
-        if (tc) MH_CUDA_TRY(ctx, launch_lu_solve_tc(ctx, Dlo, n, nn, nb, Dinv, R32, T32, nv, nrhs));
-        else MH_CUDA_TRY(ctx, launch_lu_solve_blocks32(ctx, Dlo, n, nn, nb, Dinv, R32, T32, nv, nrhs));
+        MH_CUDA_TRY(ctx, launch_lu_solve_persist(ctx, ctx->lu_backend, false, Dlo, n, nn, nb, Dinv, R32, nv,
+                                                 nrhs));
         k_add_f32<<<blocks(cnt, 256), 256, 0, ctx->stream>>>(X, R32, cnt);
         ctx->launches += 1;
         // R = RHS - D X
-        MH_CUDA_TRY(ctx, cudaMemcpyAsync(R, RHS, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice,
-                                         ctx->stream));
-        if ((rc = zgemm_strided(ctx, n, nrhs, D64, X, R, nb, -1.0, 1.0))) return rc;
+        MH_CUDA_TRY(ctx, launch_residual(ctx, false, D64, n, nb, X, RHS, R, nrhs));
         k_rel_residual<<<nb, 256, 0, ctx->stream>>>(R, RHS, n, nrhs, d_res);
         ctx->launches += 1;
         MH_CUDA_TRY(ctx, cudaMemcpyAsync(h_res.data(), d_res, sizeof(double) * nb,
@@ -702,6 +776,24 @@ cudaError_t launch_to_f32(mh_ctx* ctx, const double2* a, float2* b, int64_t coun
 cudaError_t launch_add_f32(mh_ctx* ctx, double2* x, const float2* d, int64_t count)
 {
     k_add_f32<<<blocks(count, 256), 256, 0, ctx->stream>>>(x, d, count);
+    ctx->launches += 1;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_residual(mh_ctx* ctx, bool conj_trans, const double2* A, int64_t n, int nb, const double2* X,
+                            const double2* B, double2* R, int nrhs)
+{
+    if (nrhs < 1 || nrhs > kMaxRhs) return cudaErrorInvalidValue;
+    const dim3 gc(blocks(n, 8), (unsigned)nb), gn(blocks(n, 256), (unsigned)nb);
+    if (conj_trans) {
+        if (nrhs <= 4) k_resid_c<4><<<gc, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs);
+        else if (nrhs <= 8) k_resid_c<8><<<gc, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs);
+        else k_resid_c<kMaxRhs><<<gc, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs);
+    } else {
+        if (nrhs <= 4) k_resid_n<4><<<gn, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs);
+        else if (nrhs <= 8) k_resid_n<8><<<gn, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs);
+        else k_resid_n<kMaxRhs><<<gn, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs);
+    }
     ctx->launches += 1;
     return cudaGetLastError();
 }

@@ -114,6 +114,11 @@ cudaError_t launch_lu_solve_blocks32(mh_ctx* ctx, const float2* A, int64_t n, in
                                      int nbatch, const float2* Dinv, float2* X, float2* T,
                                      int64_t xstride, int nrhs);
 
+// Persistent (one CTA per matrix, one launch) solve with the factors of
+// launch_lu_tc / launch_lu_f32: X <- (LU)^-1 X, or (LU)^-H X when conj_trans.
+cudaError_t launch_lu_solve_persist(mh_ctx* ctx, int backend, bool conj_trans, const float2* A, int64_t n,
+                                    int64_t stride, int nbatch, const float2* Dinv, float2* X, int64_t xstride,
+                                    int nrhs);
 // Conjugate-transposed solve D^H X = X with the factors of launch_lu_tc
 // (backend MH_LU_TCGEN05_F16) or launch_lu_f32 (MH_LU_SIMT_F32).
 cudaError_t launch_lu_solve_ct(mh_ctx* ctx, int backend, const float2* A, int64_t n, int64_t stride,
@@ -141,6 +146,9 @@ struct FallbackStore {
 };
 cudaError_t launch_to_f32(mh_ctx* ctx, const double2* a, float2* b, int64_t count);
 cudaError_t launch_add_f32(mh_ctx* ctx, double2* x, const float2* d, int64_t count);
+// R = B - op(A) X for nb n x n complex matrices (op = identity or ^H).
+cudaError_t launch_residual(mh_ctx* ctx, bool conj_trans, const double2* A, int64_t n, int nb, const double2* X,
+                            const double2* B, double2* R, int nrhs);
 // out[z] = max over right-hand sides of max|r| / max|b| for nb problems of n x nrhs.
 cudaError_t launch_rel_residual(mh_ctx* ctx, const double2* r, const double2* b, int64_t n, int nrhs,
                                 int nb, double* out);

@@ -568,6 +568,209 @@ k_trsv_ct_bwd(const float2* __restrict__ A, int64_t n, int64_t stride, const flo
     }
 }
 
+// Persistent substitution: one thread-block cluster of kSolveCluster CTAs
+// per matrix runs every block step of both triangles in one launch,
+// streaming each triangle of the factors once.  Rows are owned block-
+// cyclically (row block rb by CTA rb % kSolveCluster); at each step every
+// CTA forms the diagonal block's solution redundantly from x (global), the
+// owner writes it back, each CTA updates the rows it owns, and one cluster
+// barrier (release/acquire) orders the steps.
+// kCT = false: L U x = b (L unit lower; right-looking, one thread per row,
+// coalesced down the columns).  kCT = true: U^H L^H x = b (row i of U^H is
+// column i of U: 8 lanes per row read its NB-long segment).  The diagonal
+// blocks use the stored inverses.  Right-hand sides in groups of 4.
+constexpr int kSolveThreads = 512;
+constexpr int kSolveCluster = 4;
+
+template <int NB>
+constexpr size_t persist_smem_bytes()
+{
+    return sizeof(float2) * (3 * kMaxRhs * NB + NB * (NB + 1));
+}
+
+// ys = op(T11^-1) x_blk with T11^-1 (column-major NB x NB, op = identity or
+// conjugate transpose; staged with a padded leading dimension NB + 1) and
+// x_blk staged in shared memory first.
+template <int NB, bool kCT>
+__device__ __forceinline__ void persist_diag(const float2* __restrict__ Ti, bool lower, const float2* __restrict__ x,
+                                             int64_t n, int64_t k0, int kb, int nrhs, float2* ys, float2* ts,
+                                             float2* xs)
+{
+    for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) ts[(t / NB) * (NB + 1) + t % NB] = Ti[t];
+    for (int t = threadIdx.x; t < NB * nrhs; t += blockDim.x) {
+        const int r = t % NB, q = t / NB;
+        xs[t] = r < kb ? x[(int64_t)q * n + k0 + r] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < NB * nrhs; t += blockDim.x) {
+        const int r = t % NB, q = t / NB;
+        float2 acc = make_float2(0.f, 0.f);
+        if (r < kb) {
+            const int c0 = lower ? 0 : r, c1 = lower ? r : kb - 1;
+            const float2* xq = xs + q * NB;
+            for (int c = c0; c <= c1; ++c) {
+                const float2 v = xq[c];
+                if (!kCT) {
+                    const float2 l = ts[c * (NB + 1) + r];
+                    acc.x += l.x * v.x - l.y * v.y;
+                    acc.y += l.x * v.y + l.y * v.x;
+                } else {
+                    const float2 l = ts[r * (NB + 1) + c];  // conj(T[c][r])
+                    acc.x += l.x * v.x + l.y * v.y;
+                    acc.y += l.x * v.y - l.y * v.x;
+                }
+            }
+        }
+        ys[q * NB + r] = acc;
+    }
+    __syncthreads();
+}
+
+// x_blk = ys, by the block's owner one step later: every CTA of the cluster
+// reads x_blk during the step that solves it.
+template <int NB>
+__device__ __forceinline__ void persist_writeback(float2* __restrict__ x, int64_t n, int64_t k0, int kb, int nrhs,
+                                                  const float2* ys)
+{
+    for (int t = threadIdx.x; t < kb * nrhs; t += blockDim.x) {
+        const int r = t % kb, q = t / kb;
+        x[(int64_t)q * n + k0 + r] = ys[q * NB + r];
+    }
+}
+
+// Rows [r0, r1) owned by this CTA: x_i -= sum_t op(M)[i][k0 + t] ys_t.
+template <int NB, bool kCT>
+__device__ __forceinline__ void persist_update(const float2* __restrict__ M, float2* __restrict__ x, int64_t n,
+                                               int64_t k0, int kb, int nrhs, const float2* ys, int64_t r0,
+                                               int64_t r1, int rank)
+{
+    if (r1 <= r0) return;
+    // owned row blocks intersecting [r0, r1): rb = rb0, rb0 + C, ...
+    const int64_t first = r0 / NB;
+    const int64_t rb0 = first + ((rank - first % kSolveCluster) + kSolveCluster) % kSolveCluster;
+    const int64_t nown = rb0 * NB < r1 ? ((r1 - 1) / NB - rb0) / kSolveCluster + 1 : 0;
+    if (!kCT) {
+        for (int64_t it = threadIdx.x; it < nown * NB; it += blockDim.x) {
+            const int64_t i = (rb0 + (it / NB) * kSolveCluster) * NB + it % NB;
+            if (i < r0 || i >= r1) continue;
+            for (int q0 = 0; q0 < nrhs; q0 += 4) {
+                const int nq = min(4, nrhs - q0);
+                float ax[4] = {0.f, 0.f, 0.f, 0.f}, ay[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll 8
+                for (int t = 0; t < kb; ++t) {
+                    const float2 m = M[(k0 + t) * n + i];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const float2 y = ys[(q0 + (q < nq ? q : 0)) * NB + t];
+                        ax[q] += m.x * y.x - m.y * y.y;
+                        ay[q] += m.x * y.y + m.y * y.x;
+                    }
+                }
+                for (int q = 0; q < nq; ++q) {
+                    const float2 v = x[(int64_t)(q0 + q) * n + i];
+                    x[(int64_t)(q0 + q) * n + i] = make_float2(v.x - ax[q], v.y - ay[q]);
+                }
+            }
+        }
+    } else {
+        const int sub = threadIdx.x & 7;
+        const int per = blockDim.x >> 3;
+        for (int64_t ib = 0; ib < nown * NB; ib += per) {
+            const int64_t it = ib + (threadIdx.x >> 3);
+            const int64_t i = (rb0 + (it / NB) * kSolveCluster) * NB + it % NB;
+            const bool live = it < nown * NB && i >= r0 && i < r1;
+            const float2* col = M + (live ? i : 0) * n + k0;
+            for (int q0 = 0; q0 < nrhs; q0 += 4) {
+                const int nq = min(4, nrhs - q0);
+                float ax[4] = {0.f, 0.f, 0.f, 0.f}, ay[4] = {0.f, 0.f, 0.f, 0.f};
+                if (live)
+#pragma unroll 4
+                    for (int t = sub; t < kb; t += 8) {
+                        const float2 m = col[t];  // conj(m) * y
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const float2 y = ys[(q0 + (q < nq ? q : 0)) * NB + t];
+                            ax[q] += m.x * y.x + m.y * y.y;
+                            ay[q] += m.x * y.y - m.y * y.x;
+                        }
+                    }
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    for (int off = 4; off > 0; off >>= 1) {
+                        ax[q] += __shfl_down_sync(0xffffffffu, ax[q], off, 8);
+                        ay[q] += __shfl_down_sync(0xffffffffu, ay[q], off, 8);
+                    }
+                if (live && sub == 0)
+                    for (int q = 0; q < nq; ++q) {
+                        const float2 v = x[(int64_t)(q0 + q) * n + i];
+                        x[(int64_t)(q0 + q) * n + i] = make_float2(v.x - ax[q], v.y - ay[q]);
+                    }
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void cluster_sync_all()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ unsigned cluster_rank()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+template <int NB, bool kCT>
+__global__ void __cluster_dims__(kSolveCluster, 1, 1) __launch_bounds__(kSolveThreads)
+k_lu_solve_persist(const float2* __restrict__ A, int64_t n, int64_t stride, const float2* __restrict__ Dinv,
+                   int64_t dstride, float2* __restrict__ X, int64_t xstride, int nrhs)
+{
+    extern __shared__ float2 psm[];
+    float2* ys[2] = {psm, psm + kMaxRhs * NB};
+    float2* xs = psm + 2 * kMaxRhs * NB;
+    float2* ts = psm + 3 * kMaxRhs * NB;  // NB x (NB + 1)
+    const int64_t b = blockIdx.x / kSolveCluster;
+    const int rank = (int)cluster_rank();
+    const float2* M = A + b * stride;
+    const float2* Dv = Dinv + b * dstride;
+    float2* x = X + b * xstride;
+    const int nblk = (int)((n + NB - 1) / NB);
+    // first triangle, blocks ascending: L (unit lower) or U^H (lower)
+    for (int blk = 0; blk < nblk; ++blk) {
+        const int64_t k0 = (int64_t)blk * NB;
+        const int kb = (int)min((int64_t)NB, n - k0);
+        const float2* Ti = Dv + (int64_t)blk * 2 * NB * NB + (kCT ? NB * NB : 0);
+        float2* cur = ys[blk & 1];
+        persist_diag<NB, kCT>(Ti, true, x, n, k0, kb, nrhs, cur, ts, xs);
+        if (blk > 0 && (blk - 1) % kSolveCluster == rank)  // rows above: untouched this step
+            persist_writeback<NB>(x, n, k0 - NB, NB, nrhs, ys[(blk - 1) & 1]);
+        persist_update<NB, kCT>(M, x, n, k0, kb, nrhs, cur, k0 + kb, n, rank);
+        cluster_sync_all();
+    }
+    {
+        const int blk = nblk - 1;
+        const int64_t k0 = (int64_t)blk * NB;
+        if (blk % kSolveCluster == rank)
+            persist_writeback<NB>(x, n, k0, (int)min((int64_t)NB, n - k0), nrhs, ys[blk & 1]);
+        cluster_sync_all();
+    }
+    // second triangle, blocks descending: U (upper) or L^H (unit upper)
+    for (int blk = nblk - 1; blk >= 0; --blk) {
+        const int64_t k0 = (int64_t)blk * NB;
+        const int kb = (int)min((int64_t)NB, n - k0);
+        const float2* Ti = Dv + (int64_t)blk * 2 * NB * NB + (kCT ? 0 : NB * NB);
+        const int par = (nblk - 1 - blk) & 1;
+        persist_diag<NB, kCT>(Ti, false, x, n, k0, kb, nrhs, ys[par], ts, xs);
+        if (blk < nblk - 1 && (blk + 1) % kSolveCluster == rank)  // rows below: untouched this step
+            persist_writeback<NB>(x, n, k0 + NB, (int)min((int64_t)NB, n - k0 - NB), nrhs, ys[par ^ 1]);
+        persist_update<NB, kCT>(M, x, n, k0, kb, nrhs, ys[par], 0, k0, rank);
+        cluster_sync_all();
+    }
+    if (0 % kSolveCluster == rank) persist_writeback<NB>(x, n, 0, (int)min((int64_t)NB, n), nrhs, ys[(nblk - 1) & 1]);
+}
+
 unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
 
 }  // namespace
@@ -659,6 +862,43 @@ cudaError_t solve_blocks_ct(mh_ctx* ctx, const float2* A, int64_t n, int64_t str
     return cudaGetLastError();
 }
 }  // namespace
+
+cudaError_t launch_lu_solve_persist(mh_ctx* ctx, int backend, bool conj_trans, const float2* A, int64_t n,
+                                    int64_t stride, int nbatch, const float2* Dinv, float2* X, int64_t xstride,
+                                    int nrhs)
+{
+    if (nrhs < 1 || nrhs > kMaxRhs) return cudaErrorInvalidValue;
+    const dim3 g((unsigned)nbatch * kSolveCluster);
+    cudaError_t e;
+    if (backend == MH_LU_TCGEN05_F16) {
+        const int64_t ds = lu_dinv_stride_tc(n);
+        const size_t sm = persist_smem_bytes<TC_NB>();
+        if (conj_trans) {
+            if ((e = cudaFuncSetAttribute(k_lu_solve_persist<TC_NB, true>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) != cudaSuccess)
+                return e;
+            k_lu_solve_persist<TC_NB, true><<<g, kSolveThreads, sm, ctx->stream>>>(A, n, stride, Dinv, ds, X,
+                                                                                    xstride, nrhs);
+        } else {
+            if ((e = cudaFuncSetAttribute(k_lu_solve_persist<TC_NB, false>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) != cudaSuccess)
+                return e;
+            k_lu_solve_persist<TC_NB, false><<<g, kSolveThreads, sm, ctx->stream>>>(A, n, stride, Dinv, ds, X,
+                                                                                     xstride, nrhs);
+        }
+    } else {
+        const int64_t ds = lu_dinv_stride(n);
+        const size_t sm = persist_smem_bytes<32>();
+        if (conj_trans)
+            k_lu_solve_persist<32, true><<<g, kSolveThreads, sm, ctx->stream>>>(A, n, stride, Dinv, ds, X,
+                                                                                 xstride, nrhs);
+        else
+            k_lu_solve_persist<32, false><<<g, kSolveThreads, sm, ctx->stream>>>(A, n, stride, Dinv, ds, X,
+                                                                                  xstride, nrhs);
+    }
+    ctx->launches += 1;
+    return cudaGetLastError();
+}
 
 cudaError_t launch_lu_solve_ct(mh_ctx* ctx, int backend, const float2* A, int64_t n, int64_t stride,
                                int nbatch, const float2* Dinv, float2* X, float2* T, int64_t xstride,
