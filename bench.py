@@ -12,6 +12,12 @@ frequency) problem with all its right-hand sides and outputs (A, B, F, FK).
   value  solves/s with the mesh already resident on the device
   e2e    the same through the C ABI from pinned host buffers: mesh upload,
          batch call, outputs back to the host, every step
+  grads  adjoint grads/s: one grad = one (mesh, frequency) problem solved
+         forward, its adjoint solve and the tangent contraction, giving the
+         cotangents of every mesh field and of omega for a scalar objective
+         J = sum(wA A) + sum(wB B) + Re sum(conj(wF) F) (seeded weights), and
+         from them dJ/dR through the exact mesh tangent; mixed path, with
+         the FP64 GPU path and the gradient agreement beside it
 
 Also reported: the plain FP64 GPU path (cuSOLVER zgetrf) on a frequency
 subsample, the relative error of the mixed outputs against it, per-phase
@@ -224,6 +230,151 @@ def e2e_step(mh, ctx, host, omegas_p, dofs_p, betas_p, out_p, args, mask, info):
         L.mh_mesh_destroy(ctx.handle, h)
 
 
+def e2e_grad_step(mh, ctx, host, omegas_p, dofs_p, betas_p, bars_p, grads_p, args, mask, info):
+    """Mesh upload + forward/adjoint batch + cotangents to host through the C ABI."""
+    N = mh.native
+    L = N.lib()
+    h = N._P()
+    dp = lambda t: ctypes.cast(t.data_ptr(), N._D) if t is not None else None
+    N.check(L.mh_mesh_create(ctx.handle, host["n"], host["nv"], dp(host["vertices"]),
+                             ctypes.cast(host["faces"].data_ptr(), N._I64), dp(host["centers"]),
+                             dp(host["normals"]), dp(host["areas"]), dp(host["radii"]),
+                             ctypes.byref(h)), ctx.handle)
+    try:
+        N.check(L.mh_hydro_batch_vjp(
+            ctx.handle, h, omegas_p.numel(), dp(omegas_p), args.n_dof, dp(dofs_p), betas_p.numel(),
+            dp(betas_p), 1000.0, 9.81, mask, 1, N.MH_PRECISION_MIXED, args.tol, args.max_iter,
+            dp(bars_p[0]), dp(bars_p[1]), dp(bars_p[2]), None, None, None, None, None,
+            dp(grads_p[0]), dp(grads_p[1]), dp(grads_p[2]), dp(grads_p[3]), None, dp(grads_p[4]),
+            None, ctypes.byref(info)), ctx.handle)
+    finally:
+        L.mh_mesh_destroy(ctx.handle, h)
+
+
+def grad_weights(nd, nw, nb):
+    rng = np.random.default_rng(2024)
+    return (rng.normal(size=(nd, nd, nw)), rng.normal(size=(nd, nd, nw)),
+            rng.normal(size=(nd, nw, nb)) + 1j * rng.normal(size=(nd, nw, nb)))
+
+
+def run_grads(mh, ctx, mesh, dofs, omegas, betas, gfs, args, stream, barrier, dist, world, torch):
+    """Adjoint grads/s (mixed) with the FP64 GPU path and the agreement of
+    the two; each step one mh_hydro_batch_vjp over all frequencies."""
+    nd, nw, nb = len(dofs), len(omegas), len(betas)
+    wA, wB, wF = grad_weights(nd, nw, nb)
+    tan = mh.hemisphere_tangents(1.0, (0.0, 0.0, 0.0), tuple(args.res))["radius"]
+
+    def gstep():
+        r = mh.hydro_batch_vjp(mesh, omegas, dofs, betas, wA, wB, wF, None, green_functions=gfs,
+                               precision="mixed", tol=args.tol, max_iter=args.max_iter, ctx=ctx)
+        return r, r.mesh.dot(tan)
+
+    for _ in range(args.warmup):
+        r, dR = gstep()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ctx.set_profiling(True)
+    l0 = ctx.kernel_launches()
+    barrier()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        r, dR = gstep()
+    ev1.record(stream)
+    barrier()
+    launches = ctx.kernel_launches() - l0
+    phases = ctx.phase_times()
+    ctx.set_profiling(False)
+    ms = ev0.elapsed_time(ev1)
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    out = {"value": world * nw * args.steps / (ms / 1e3), "unit": "grads/s",
+           "ms_per_step": ms / args.steps, "gpu_launches": launches,
+           "objective": "J = sum(wA A) + sum(wB B) + Re sum(conj(wF) Fd), seeded weights",
+           "outputs": "cotangents of vertices, centers, normals, areas, radii, omegas; dJ/dR",
+           "dJ_dR": dR, "phases_ms_per_step": {k: v[0] / args.steps for k, v in phases.items() if v[1]}}
+    # e2e through the C ABI
+    host = host_mesh(mesh, torch)
+    omegas_p = _pinned(omegas, torch)
+    betas_p = _pinned(np.asarray(betas, dtype=np.float64), torch)
+    dofs_p = _pinned(np.concatenate([np.asfortranarray(d).reshape(-1, order="F") for d in dofs]), torch)
+    bars_p = [_pinned(np.asfortranarray(wA).reshape(-1, order="F"), torch),
+              _pinned(np.asfortranarray(wB).reshape(-1, order="F"), torch),
+              _pinned(np.asfortranarray(wF).reshape(-1, order="F").view(np.float64), torch)]
+    grads_p = [torch.zeros(3 * mesh.nvertices, dtype=torch.float64).pin_memory(),
+               torch.zeros(3 * mesh.nfaces, dtype=torch.float64).pin_memory(),
+               torch.zeros(3 * mesh.nfaces, dtype=torch.float64).pin_memory(),
+               torch.zeros(mesh.nfaces, dtype=torch.float64).pin_memory(),
+               torch.zeros(nw, dtype=torch.float64).pin_memory()]
+    cinfo = mh.bodies._Info()
+    mask = mh.gf_mask(gfs)
+    e2e_grad_step(mh, ctx, host, omegas_p, dofs_p, betas_p, bars_p, grads_p, args, mask, cinfo)
+    barrier()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        e2e_grad_step(mh, ctx, host, omegas_p, dofs_p, betas_p, bars_p, grads_p, args, mask, cinfo)
+    ev1.record(stream)
+    barrier()
+    ms_e2e = ev0.elapsed_time(ev1)
+    if dist is not None:
+        t = torch.tensor([ms_e2e], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    h2d = sum(int(v.numel() * v.element_size()) for k, v in host.items() if k not in ("n", "nv"))
+    h2d += int(omegas_p.numel() * 8 + betas_p.numel() * 8 + dofs_p.numel() * 8)
+    h2d += sum(int(t.numel() * t.element_size()) for t in bars_p)
+    out["e2e"] = {"value": world * nw * args.steps / (ms_e2e / 1e3), "unit": "grads/s",
+                  "h2d_bytes_per_step": h2d,
+                  "d2h_bytes_per_step": sum(int(t.numel() * t.element_size()) for t in grads_p),
+                  "ms_per_step": ms_e2e / args.steps}
+    if args.no_fp64:
+        return out
+    # FP64 GPU path: per-call cost a + b * n_omega fitted on two subsample sizes
+    sub = np.arange(0, nw, max(1, nw // args.fp64_omegas))[:args.fp64_omegas]
+    mh.hydro_batch_vjp(mesh, omegas[sub[:1]], dofs, betas, wA[:, :, sub[:1]], wB[:, :, sub[:1]],
+                       wF[:, sub[:1]], None, green_functions=gfs, precision="fp64", ctx=ctx)  # warm-up
+    times = {}
+    res64 = resmx = None
+    for cnt in (2, len(sub)):
+        s_ = sub[:cnt]
+        call = lambda prec: mh.hydro_batch_vjp(mesh, omegas[s_], dofs, betas, wA[:, :, s_], wB[:, :, s_],
+                                               wF[:, s_], None, green_functions=gfs, precision=prec,
+                                               tol=args.tol, max_iter=args.max_iter, ctx=ctx)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        r64 = call("fp64")
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        times[cnt] = ev0.elapsed_time(ev1)
+        if cnt == len(sub):
+            res64, resmx = r64, call("mixed")
+    b = (times[len(sub)] - times[2]) / (len(sub) - 2)
+    a = times[2] - 2 * b
+    per = (a + nw * b) / nw
+    out["fp64_gpu"] = {"value": 1e3 / per, "unit": "grads/s", "ms_per_grad_at_n_omega": per,
+                       "fit_ms": {"per_call": a, "per_omega": b}, "omegas_timed": [2, int(len(sub))]}
+    out["speedup_vs_fp64_gpu"] = out["value"] / out["fp64_gpu"]["value"]
+    acc = {}
+    for f in ("vertices", "centers", "normals", "areas"):
+        x, y = getattr(resmx.mesh, f), getattr(res64.mesh, f)
+        acc[f] = float(np.max(np.abs(x - y)) / np.max(np.abs(y)))
+    acc["omegas"] = float(np.max(np.abs(resmx.omegas - res64.omegas)) / np.max(np.abs(res64.omegas)))
+    acc["dJ_dR"] = abs(resmx.mesh.dot(tan) - res64.mesh.dot(tan)) / abs(res64.mesh.dot(tan))
+    acc["note"] = "max abs difference / max abs value, mixed vs FP64 GPU gradients, same frequencies"
+    out["accuracy"] = acc
+    return out
+
+
+def host_mesh(mesh, torch):
+    return {"n": mesh.nfaces, "nv": mesh.nvertices,
+            "vertices": _pinned(np.asfortranarray(mesh.vertices).reshape(-1, order="F"), torch),
+            "faces": _pinned(np.asfortranarray(mesh.faces).reshape(-1, order="F"), torch),
+            "centers": _pinned(np.asfortranarray(mesh.centers).reshape(-1, order="F"), torch),
+            "normals": _pinned(np.asfortranarray(mesh.normals).reshape(-1, order="F"), torch),
+            "areas": _pinned(mesh.areas, torch), "radii": _pinned(mesh.radii, torch)}
+
+
 def run_ours(args):
     import torch
 
@@ -286,12 +437,7 @@ def run_ours(args):
     A, B, Fd, Fk, info = out
 
     # ---- e2e through the C ABI from pinned host buffers ----
-    host = {"n": mesh.nfaces, "nv": mesh.nvertices,
-            "vertices": _pinned(np.asfortranarray(mesh.vertices).reshape(-1, order="F"), torch),
-            "faces": _pinned(np.asfortranarray(mesh.faces).reshape(-1, order="F"), torch),
-            "centers": _pinned(np.asfortranarray(mesh.centers).reshape(-1, order="F"), torch),
-            "normals": _pinned(np.asfortranarray(mesh.normals).reshape(-1, order="F"), torch),
-            "areas": _pinned(mesh.areas, torch), "radii": _pinned(mesh.radii, torch)}
+    host = host_mesh(mesh, torch)
     omegas_p = _pinned(omegas, torch)
     betas_p = _pinned(np.asarray(betas, dtype=np.float64), torch)
     dofs_p = _pinned(np.concatenate([np.asfortranarray(d).reshape(-1, order="F") for d in dofs]),
@@ -335,6 +481,9 @@ def run_ours(args):
     line["phases_ms_per_step"] = per_phase
     line["roofline"] = roofline(per_phase, mesh.nfaces, args)
 
+    if not args.no_grads:
+        line["grads"] = run_grads(mh, ctx, mesh, dofs, omegas, betas, gfs, args, stream, barrier, dist,
+                                  world, torch)
     if rank == 0 and not args.no_fp64:
         line["fp64_gpu"], line["accuracy"] = fp64_baseline(mh, ctx, mesh, dofs, omegas, betas, gfs,
                                                            (A, B, Fd), args)
@@ -351,35 +500,52 @@ def run_ours(args):
     return 0
 
 
-def roofline(per_phase, n, args):
-    """Dominant phase against the measured HBM copy bandwidth.  Algorithmic
-    bytes per frequency of the wave pass: read the FP64 Rankine part of S and
-    D (16 B/pair), write S and D in FP64 complex (32 B/pair) and the FP32 LU
-    copy (8 B/pair); of the LU: the FP32 complex trailing updates read and
-    write each trailing block once per step, sum_k 16 B (n - k*32)^2."""
-    peaks = {}
+def _peaks():
     try:
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
-        hbm, src = float(peaks["hbm_gbs"]), "measured"
-    except (OSError, KeyError, ValueError):
-        hbm, src = 6650.0, "fallback"
-    if not per_phase:
+        return peaks, "measured"
+    except (OSError, ValueError):
+        return {}, "fallback"
+
+
+# DRAM bytes (read + write) per pair-frequency of k_wave_delh_allw from an
+# ncu capture (hemisphere 1024 panels, 16 frequencies: dram__bytes_read.sum +
+# dram__bytes_write.sum / (n^2 * 16)); traffic grows with the pairs and
+# frequencies a launch processes, so it is scaled by them.
+WAVE_DRAM_BYTES_PER_PAIR_FREQ = 37.6
+
+
+def roofline(per_phase, n, args):
+    """Dominant kernel of the solve step: the frequency-batched wave pass
+    k_wave_delh_allw (one launch per step, timed alone by its phase events).
+    Algorithmic bytes per launch: the FP64 Rankine parts of S and D read once
+    per pair (16 B), S and D written in FP64 complex and the FP32 LU copy of D
+    per pair and frequency (40 B).  The LU phase is given beside it against
+    the dense tensor peak, (8/3) n^3 real flops per matrix."""
+    peaks, src = _peaks()
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    tensor = float(peaks.get("bf16_tflops", 1590.0))
+    if "wave" not in per_phase:
         return None
-    dom = max(per_phase, key=per_phase.get)
-    ms = per_phase[dom]
+    ms = per_phase["wave"]
     nn = float(n) * n
-    if dom == "wave":
-        traffic_alg = 56.0 * nn * args.n_omega
-    elif dom == "lu":
-        traffic_alg = sum(16.0 * (n - k) ** 2 for k in range(32, n, 32)) * args.n_omega
-    elif dom == "refine":
-        traffic_alg = 16.0 * nn * args.n_omega * 3
-    else:
-        traffic_alg = 16.0 * nn * args.n_omega
-    achieved = traffic_alg / (ms / 1e3) / 1e9
-    return {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": achieved / hbm, "peak_source": src, "traffic": None,
-            "ms_per_step": ms, "algorithmic_bytes_per_step": traffic_alg}
+    alg = nn * (16.0 + 40.0 * args.n_omega)
+    achieved = alg / (ms / 1e3) / 1e9
+    traffic = None
+    if WAVE_DRAM_BYTES_PER_PAIR_FREQ is not None:
+        traffic = WAVE_DRAM_BYTES_PER_PAIR_FREQ * nn * args.n_omega
+    out = {"kernel": "k_wave_delh_allw", "bound": "hbm", "achieved": achieved, "peak": hbm,
+           "unit": "GB/s", "frac": achieved / hbm, "peak_source": src, "traffic": traffic,
+           "ms_per_launch": ms, "algorithmic_bytes_per_launch": alg,
+           "note": ("FP64-issue bound (table Clenshaw, log, complex arithmetic per pair and "
+                    "frequency); the HBM fraction shows the writes are not the limit")}
+    if "lu" in per_phase:
+        fl = 8.0 / 3.0 * float(n) ** 3 * args.n_omega
+        ach = fl / (per_phase["lu"] / 1e3) / 1e12
+        out["lu"] = {"kernels": "k_lu_diag + k_lu_trsm_tc + k_lu_update_tc", "bound": "tensor",
+                     "achieved": ach, "peak": tensor, "unit": "TFLOP/s", "frac": ach / tensor,
+                     "ms_per_step": per_phase["lu"], "algorithmic_flops_per_step": fl}
+    return out
 
 
 def fp64_baseline(mh, ctx, mesh, dofs, omegas, betas, gfs, mixed, args):
@@ -433,6 +599,7 @@ def main():
     ap.add_argument("--lu", default="tcgen05", choices=["tcgen05", "simt"])
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-grads", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
