@@ -548,83 +548,64 @@ k_adj_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const do
 // Rankine terms
 // ---------------------------------------------------------------------------
 
-// Near field (rankine.jl:36-61, 65-123): derivatives along the panel centre,
-// normal and the four vertices by 6-way dual numbers, three passes.  The
-// integrals depend on y - c, y - v_a and n only, so dL/dy = -(dL/dc + sum_a
-// dL/dv_a).  Accumulates into pb (gbar field order); gr = forward gradient.
-__device__ __noinline__ void rankine_near_vjp(const double* y, const Panel& p, double ibar,
-                                              const double* gb, double* yb, double* pb, double* gr)
+// One dual-number pass of the near-field reverse (rankine.jl:36-61, 65-123):
+// pass 0 gives dL/d(centre, normal) and the forward gradient, pass 1 dL/d
+// (vertex 0, vertex 1), pass 2 dL/d(vertex 2, vertex 3), L = ibar I + gb . grad.
+__device__ __noinline__ void rankine_near_pass(const double* y, const Panel& p, double ibar, const double* gb,
+                                               int pass, double* out, double* gr)
 {
-    double cb[3], nbv[3], vb[12];
-    for (int pass = 0; pass < 3; ++pass) {
-        PanelT<d6> q;
-        for (int a = 0; a < 3; ++a) {
-            q.c[a] = dconst<6>(p.c[a]);
-            q.n[a] = dconst<6>(p.n[a]);
-        }
-        for (int t = 0; t < 12; ++t) q.v[t] = dconst<6>(p.v[t]);
-        q.area = dconst<6>(p.area);
-        q.radius = dconst<6>(p.radius);
-        if (pass == 0) {
-            for (int a = 0; a < 3; ++a) {
-                q.c[a].d[a] = 1.0;
-                q.n[a].d[3 + a] = 1.0;
-            }
-        } else {
-            const int v0 = 2 * (pass - 1);
-            for (int c = 0; c < 3; ++c) {
-                q.v[3 * v0 + c].d[c] = 1.0;
-                q.v[3 * (v0 + 1) + c].d[3 + c] = 1.0;
-            }
-        }
-        const d6 yd[3] = {dconst<6>(y[0]), dconst<6>(y[1]), dconst<6>(y[2])};
-        d6 I, g[3];
-        rankine_pair(yd, q, I, g);
-        double t[6];
-        for (int k = 0; k < 6; ++k) t[k] = ibar * I.d[k] + gb[0] * g[0].d[k] + gb[1] * g[1].d[k] + gb[2] * g[2].d[k];
-        if (pass == 0) {
-            for (int a = 0; a < 3; ++a) {
-                cb[a] = t[a];
-                nbv[a] = t[3 + a];
-                gr[a] = g[a].v;
-            }
-        } else {
-            for (int k = 0; k < 6; ++k) vb[6 * (pass - 1) + k] = t[k];
-        }
-    }
+    PanelT<d6> q;
     for (int a = 0; a < 3; ++a) {
-        yb[a] = -(cb[a] + vb[a] + vb[3 + a] + vb[6 + a] + vb[9 + a]);
-        pb[GB_C + a] += cb[a];
-        pb[GB_N + a] += nbv[a];
+        q.c[a] = dconst<6>(p.c[a]);
+        q.n[a] = dconst<6>(p.n[a]);
     }
-    for (int t = 0; t < 12; ++t) pb[GB_V + t] += vb[t];
+    for (int t = 0; t < 12; ++t) q.v[t] = dconst<6>(p.v[t]);
+    q.area = dconst<6>(p.area);
+    q.radius = dconst<6>(p.radius);
+    if (pass == 0) {
+        for (int a = 0; a < 3; ++a) {
+            q.c[a].d[a] = 1.0;
+            q.n[a].d[3 + a] = 1.0;
+        }
+    } else {
+        const int v0 = 2 * (pass - 1);
+        for (int c = 0; c < 3; ++c) {
+            q.v[3 * v0 + c].d[c] = 1.0;
+            q.v[3 * (v0 + 1) + c].d[3 + c] = 1.0;
+        }
+    }
+    const d6 yd[3] = {dconst<6>(y[0]), dconst<6>(y[1]), dconst<6>(y[2])};
+    d6 I, g[3];
+    rankine_pair(yd, q, I, g);
+    for (int k = 0; k < 6; ++k) out[k] = ibar * I.d[k] + gb[0] * g[0].d[k] + gb[1] * g[1].d[k] + gb[2] * g[2].d[k];
+    if (pass == 0)
+        for (int a = 0; a < 3; ++a) gr[a] = g[a].v;
 }
 
-// Reverse of rankine_pair at point y: L = ibar * I + gb . grad.
-__device__ __forceinline__ void rankine_vjp(const double y[3], const Panel& p, double ibar, const double gb[3],
-                                            double yb[3], double pb[GB_NF], double gr[3])
+// Far field reverse (rankine.jl:33-34): I = A/r, grad = A rb / r^3,
+// L = ibar I + gb . grad; returns dL/dy (= -dL/dc) and adds dL/dA.
+__device__ __forceinline__ void rankine_far_vjp(const double rb[3], double r, double A, double ibar,
+                                                const double gb[3], double yb[3], double& ab, double gr[3])
 {
-    const double rb[3] = {y[0] - p.c[0], y[1] - p.c[1], y[2] - p.c[2]};
-    const double r = sqrt(rb[0] * rb[0] + rb[1] * rb[1] + rb[2] * rb[2]);
-    if (r > 7.0 * p.radius) {  // far field: I = A/r, grad = A rb / r^3 (rankine.jl:33-34)
-        const double ir = 1.0 / r, ir3 = ir * ir * ir, ir5 = ir3 * ir * ir;
-        const double A = p.area;
-        const double gdr = gb[0] * rb[0] + gb[1] * rb[1] + gb[2] * rb[2];
-        for (int a = 0; a < 3; ++a) {
-            gr[a] = rb[a] * ir3 * A;
-            const double d = A * (-ibar * rb[a] * ir3 + gb[a] * ir3 - 3.0 * gdr * rb[a] * ir5);
-            yb[a] = d;
-            pb[GB_C + a] -= d;
-        }
-        pb[GB_A] += ibar * ir + gdr * ir3;
-        return;
+    const double ir = 1.0 / r, ir3 = ir * ir * ir, ir5 = ir3 * ir * ir;
+    const double gdr = gb[0] * rb[0] + gb[1] * rb[1] + gb[2] * rb[2];
+    for (int a = 0; a < 3; ++a) {
+        gr[a] = rb[a] * ir3 * A;
+        yb[a] = A * (-ibar * rb[a] * ir3 + gb[a] * ir3 - 3.0 * gdr * rb[a] * ir5);
     }
-    rankine_near_vjp(y, p, ibar, gb, yb, pb, gr);
+    ab += ibar * ir + gdr * ir3;
 }
 
 // Rankine-term contraction against the frequency sums WS = sum_w S-bar(w),
-// WD = sum_w D-bar(w) (real parts used).  Layout as k_adj_wave with
-// GB_NF column fields.
+// WD = sum_w D-bar(w) (real parts used), 128 rows x 16 columns per CTA.
+// Far-field terms are reversed in place; near-field (row, column, term)
+// entries are listed per CTA in row-major order and their three dual passes
+// spread over all threads, 128 entries at a time; rows and columns then sum
+// their entries in list order.  Partials as k_adj_wave with GB_NF column
+// fields.
+constexpr int kNearChunk = 128;
+constexpr int kNearF = 21;  // per entry: pass outputs 18, normal cotangent 3
+
 __global__ void __launch_bounds__(kAR)
 k_adj_rankine(const double* __restrict__ geom, int64_t n, uint32_t mask, int direct,
               const double2* __restrict__ WS, const double2* __restrict__ WD, double* __restrict__ rowpart,
@@ -632,11 +613,17 @@ k_adj_rankine(const double* __restrict__ geom, int64_t n, uint32_t mask, int dir
 {
     __shared__ Panel sp[kAC];
     __shared__ double csm[kAR / 32][kAC][GB_NF];
+    __shared__ double cnear[kAC][GB_NF];
+    __shared__ double res[kNearChunk][kNearF];
+    __shared__ unsigned short list[kAR * kAC * 2];
+    __shared__ int offs[kAR + 1];
     const int64_t j0 = (int64_t)blockIdx.y * kAC;
     stage(sp, geom, n, j0);
+    for (int t = threadIdx.x; t < kAC * GB_NF; t += blockDim.x) (&cnear[0][0])[t] = 0.0;
     __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t i = (int64_t)blockIdx.x * kAR + threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int64_t i0 = (int64_t)blockIdx.x * kAR;
+    const int64_t i = i0 + tid;
     const bool live = i < n;
     const int64_t ii = live ? i : 0;
     const double x[3] = {geom[G_CX * n + ii], geom[G_CY * n + ii], geom[G_CZ * n + ii]};
@@ -646,57 +633,131 @@ k_adj_rankine(const double* __restrict__ geom, int64_t n, uint32_t mask, int dir
     const double sg = wrt_first ? -1.0 : 1.0, sz = wrt_first ? -1.0 : 1.0;
     const uint32_t refl = mask & (MH_GF_RANKINE_REFLECTED | MH_GF_RANKINE_REFLECTED_NEGATIVE);
     const bool has_refl = refl == MH_GF_RANKINE_REFLECTED || refl == MH_GF_RANKINE_REFLECTED_NEGATIVE;
+    const bool has_dir = (mask & MH_GF_RANKINE) != 0;
     const double sgn = (refl == MH_GF_RANKINE_REFLECTED) ? 1.0 : -1.0;
+    const double mref[3] = {sgn * sg, sgn * sg, sgn * sg * sz};
     double xb[3] = {0.0, 0.0, 0.0}, nbi[3] = {0.0, 0.0, 0.0};
+    uint32_t near = 0;
+    // ---- far field in place; near entries marked (bit 2 jj + term) ----
     for (int jj = 0; jj < jend; ++jj) {
         const Panel& p = sp[jj];
         const int64_t j = j0 + jj;
         const double* nD = direct ? p.n : ni;
-        double pb[GB_NF];
-#pragma unroll
-        for (int f = 0; f < GB_NF; ++f) pb[f] = 0.0;
+        double pb[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // centre, normal, area
         if (live) {
             const double ws = WS[j * n + i].x, wd = WD[j * n + i].x;
             const double ibar = -kI4P * ws;
             const double gbar[3] = {-kI4P * wd * nD[0], -kI4P * wd * nD[1], -kI4P * wd * nD[2]};
             double gt[3] = {0.0, 0.0, 0.0};
-            if (mask & MH_GF_RANKINE) {
-                const double gb[3] = {sg * gbar[0], sg * gbar[1], sg * gbar[2]};
-                double yb[3], gr[3];
-                rankine_vjp(x, p, ibar, gb, yb, pb, gr);
-                for (int a = 0; a < 3; ++a) {
-                    xb[a] += yb[a];
-                    gt[a] += sg * gr[a];
+            for (int term = 0; term < 2; ++term) {
+                if (term == 0 ? !has_dir : !has_refl) continue;
+                const double y[3] = {x[0], x[1], term ? -x[2] : x[2]};
+                const double f[3] = {term ? mref[0] : sg, term ? mref[1] : sg, term ? mref[2] : sg};
+                const double rb[3] = {y[0] - p.c[0], y[1] - p.c[1], y[2] - p.c[2]};
+                const double r = sqrt(rb[0] * rb[0] + rb[1] * rb[1] + rb[2] * rb[2]);
+                if (!(r > 7.0 * p.radius)) {
+                    near |= 1u << (2 * jj + term);
+                    continue;
                 }
-            }
-            if (has_refl) {
-                const double xr[3] = {x[0], x[1], -x[2]};
-                const double m[3] = {sgn * sg, sgn * sg, sgn * sg * sz};
-                const double gb[3] = {m[0] * gbar[0], m[1] * gbar[1], m[2] * gbar[2]};
+                const double gb[3] = {f[0] * gbar[0], f[1] * gbar[1], f[2] * gbar[2]};
                 double yb[3], gr[3];
-                rankine_vjp(xr, p, sgn * ibar, gb, yb, pb, gr);
+                rankine_far_vjp(rb, r, p.area, term ? sgn * ibar : ibar, gb, yb, pb[6], gr);
+                for (int a = 0; a < 3; ++a) {
+                    pb[a] -= yb[a];
+                    gt[a] += f[a] * gr[a];
+                }
                 xb[0] += yb[0];
                 xb[1] += yb[1];
-                xb[2] -= yb[2];
-                for (int a = 0; a < 3; ++a) gt[a] += m[a] * gr[a];
+                xb[2] += term ? -yb[2] : yb[2];
             }
             for (int a = 0; a < 3; ++a) {
                 const double nb_a = -kI4P * wd * gt[a];
-                if (direct) pb[GB_N + a] += nb_a;
+                if (direct) pb[3 + a] += nb_a;
                 else nbi[a] += nb_a;
             }
         }
 #pragma unroll
-        for (int f = 0; f < GB_NF; ++f) {
+        for (int f = 0; f < 7; ++f) {
             const double v = warp_sum(pb[f]);
             if (lane == 0) csm[warp][jj][f] = v;
         }
     }
+    // ---- near-field list (row-major: thread, then column, then term) ----
+    offs[tid + 1] = __popc(near);
+    if (tid == 0) offs[0] = 0;
+    __syncthreads();
+    if (tid == 0)
+        for (int t = 1; t <= kAR; ++t) offs[t] += offs[t - 1];
+    __syncthreads();
+    {
+        int o = offs[tid];
+        for (uint32_t m = near; m; m &= m - 1) {
+            const int bit = __ffs(m) - 1;
+            list[o++] = (unsigned short)((tid << 5) | bit);
+        }
+    }
+    const int total = offs[kAR];
+    __syncthreads();
+    double cl[GB_NF];  // this thread's column (tid < kAC) near sums
+    for (int f = 0; f < GB_NF; ++f) cl[f] = 0.0;
+    for (int c0 = 0; c0 < total; c0 += kNearChunk) {
+        const int m = min(kNearChunk, total - c0);
+        for (int w = tid; w < 3 * m; w += blockDim.x) {
+            const int e = w % m, pass = w / m;
+            const int code = list[c0 + e];
+            const int r = code >> 5, bit = code & 31, jj = bit >> 1, term = bit & 1;
+            const int64_t ie = i0 + r, j = j0 + jj;
+            const Panel& p = sp[jj];
+            const double xe[3] = {geom[G_CX * n + ie], geom[G_CY * n + ie], geom[G_CZ * n + ie]};
+            const double* nD = p.n;
+            double nie[3];
+            if (!direct) {
+                nie[0] = geom[G_NX * n + ie];
+                nie[1] = geom[G_NY * n + ie];
+                nie[2] = geom[G_NZ * n + ie];
+                nD = nie;
+            }
+            const double ws = WS[j * n + ie].x, wd = WD[j * n + ie].x;
+            const double f[3] = {term ? mref[0] : sg, term ? mref[1] : sg, term ? mref[2] : sg};
+            const double gb[3] = {-kI4P * wd * nD[0] * f[0], -kI4P * wd * nD[1] * f[1], -kI4P * wd * nD[2] * f[2]};
+            const double y[3] = {xe[0], xe[1], term ? -xe[2] : xe[2]};
+            double gr[3];
+            rankine_near_pass(y, p, (term ? sgn : 1.0) * (-kI4P * ws), gb, pass, &res[e][6 * pass], gr);
+            if (pass == 0)
+                for (int a = 0; a < 3; ++a) res[e][18 + a] = -kI4P * wd * f[a] * gr[a];
+        }
+        __syncthreads();
+        for (int e = 0; e < m; ++e) {
+            const int code = list[c0 + e];
+            const int r = code >> 5, bit = code & 31, jj = bit >> 1, term = bit & 1;
+            const double* q = res[e];
+            if (r == tid) {  // row: y-bar = -(c-bar + sum of vertex bars), mirrored back for the image
+                double yb[3];
+                for (int a = 0; a < 3; ++a) yb[a] = -(q[a] + q[6 + a] + q[9 + a] + q[12 + a] + q[15 + a]);
+                xb[0] += yb[0];
+                xb[1] += yb[1];
+                xb[2] += term ? -yb[2] : yb[2];
+                if (!direct)
+                    for (int a = 0; a < 3; ++a) nbi[a] += q[18 + a];
+            }
+            if (jj == tid) {  // column: centre, normal, vertices (+ normal cotangent when direct)
+                for (int a = 0; a < 3; ++a) {
+                    cl[GB_C + a] += q[a];
+                    cl[GB_N + a] += q[3 + a] + (direct ? q[18 + a] : 0.0);
+                }
+                for (int t = 0; t < 12; ++t) cl[GB_V + t] += q[6 + t];
+            }
+        }
+        __syncthreads();
+    }
+    if (tid < kAC)
+        for (int f = 0; f < GB_NF; ++f) cnear[tid][f] = cl[f];
     __syncthreads();
     for (int t = threadIdx.x; t < jend * GB_NF; t += blockDim.x) {
         const int jj = t / GB_NF, f = t % GB_NF;
-        double s = 0.0;
-        for (int w = 0; w < kAR / 32; ++w) s += csm[w][jj][f];
+        double s = cnear[jj][f];
+        if (f < 7)
+            for (int w = 0; w < kAR / 32; ++w) s += csm[w][jj][f];
         colpart[((int64_t)blockIdx.x * GB_NF + f) * n + j0 + jj] = s;
     }
     if (live) {
