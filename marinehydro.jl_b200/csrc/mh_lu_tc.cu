@@ -575,10 +575,9 @@ k_trsv_ct_bwd(const float2* __restrict__ A, int64_t n, int64_t stride, const flo
 // CTA forms the diagonal block's solution redundantly from x (global), the
 // owner writes it back, each CTA updates the rows it owns, and one cluster
 // barrier (release/acquire) orders the steps.
-// kCT = false: L U x = b (L unit lower; right-looking, one thread per row,
-// coalesced down the columns).  kCT = true: U^H L^H x = b (row i of U^H is
-// column i of U: 8 lanes per row read its NB-long segment).  The diagonal
-// blocks use the stored inverses.  Right-hand sides in groups of 4.
+// kCT = false: L U x = b (L unit lower, right-looking).  kCT = true:
+// U^H L^H x = b (row i of U^H is column i of U).  The diagonal blocks use
+// the stored inverses.  Right-hand sides in groups of 4.
 constexpr int kSolveThreads = 512;
 constexpr int kSolveCluster = 4;
 
@@ -639,6 +638,10 @@ __device__ __forceinline__ void persist_writeback(float2* __restrict__ x, int64_
 }
 
 // Rows [r0, r1) owned by this CTA: x_i -= sum_t op(M)[i][k0 + t] ys_t.
+// Four lanes per row, each loading its NB/4 entries of the row's panel
+// segment at once (entries t = lane + 4 s: M[i][k0 + t] down column k0 + t,
+// or for the conjugate transpose the NB-long piece of column i), then a
+// 2-step shuffle reduction.
 template <int NB, bool kCT>
 __device__ __forceinline__ void persist_update(const float2* __restrict__ M, float2* __restrict__ x, int64_t n,
                                                int64_t k0, int kb, int nrhs, const float2* ys, int64_t r0,
@@ -649,63 +652,50 @@ __device__ __forceinline__ void persist_update(const float2* __restrict__ M, flo
     const int64_t first = r0 / NB;
     const int64_t rb0 = first + ((rank - first % kSolveCluster) + kSolveCluster) % kSolveCluster;
     const int64_t nown = rb0 * NB < r1 ? ((r1 - 1) / NB - rb0) / kSolveCluster + 1 : 0;
-    if (!kCT) {
-        for (int64_t it = threadIdx.x; it < nown * NB; it += blockDim.x) {
-            const int64_t i = (rb0 + (it / NB) * kSolveCluster) * NB + it % NB;
-            if (i < r0 || i >= r1) continue;
-            for (int q0 = 0; q0 < nrhs; q0 += 4) {
-                const int nq = min(4, nrhs - q0);
-                float ax[4] = {0.f, 0.f, 0.f, 0.f}, ay[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll 8
-                for (int t = 0; t < kb; ++t) {
-                    const float2 m = M[(k0 + t) * n + i];
+    constexpr int CQ = NB / 4;
+    const int sub = threadIdx.x & 3;
+    const int per = blockDim.x >> 2;
+    for (int64_t ib = 0; ib < nown * NB; ib += per) {  // uniform trip count (shuffles below)
+        const int64_t it = ib + (threadIdx.x >> 2);
+        const int64_t i = (rb0 + (it / NB) * kSolveCluster) * NB + it % NB;
+        const bool live = it < nown * NB && i >= r0 && i < r1;
+        float2 m[CQ];
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const float2 y = ys[(q0 + (q < nq ? q : 0)) * NB + t];
-                        ax[q] += m.x * y.x - m.y * y.y;
-                        ay[q] += m.x * y.y + m.y * y.x;
+        for (int s = 0; s < CQ; ++s) {
+            const int t = sub + 4 * s;
+            m[s] = make_float2(0.f, 0.f);
+            if (live && t < kb) m[s] = kCT ? M[i * n + k0 + t] : M[(k0 + t) * n + i];
+        }
+        for (int q0 = 0; q0 < nrhs; q0 += 4) {
+            const int nq = min(4, nrhs - q0);
+            float ax[4] = {0.f, 0.f, 0.f, 0.f}, ay[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int s = 0; s < CQ; ++s) {
+                const int t = sub + 4 * s;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float2 y = ys[(q0 + (q < nq ? q : 0)) * NB + t];
+                    if (!kCT) {
+                        ax[q] += m[s].x * y.x - m[s].y * y.y;
+                        ay[q] += m[s].x * y.y + m[s].y * y.x;
+                    } else {  // conj(m) * y
+                        ax[q] += m[s].x * y.x + m[s].y * y.y;
+                        ay[q] += m[s].x * y.y - m[s].y * y.x;
                     }
                 }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                ax[q] += __shfl_xor_sync(0xffffffffu, ax[q], 1);
+                ay[q] += __shfl_xor_sync(0xffffffffu, ay[q], 1);
+                ax[q] += __shfl_xor_sync(0xffffffffu, ax[q], 2);
+                ay[q] += __shfl_xor_sync(0xffffffffu, ay[q], 2);
+            }
+            if (live && sub == 0)
                 for (int q = 0; q < nq; ++q) {
                     const float2 v = x[(int64_t)(q0 + q) * n + i];
                     x[(int64_t)(q0 + q) * n + i] = make_float2(v.x - ax[q], v.y - ay[q]);
                 }
-            }
-        }
-    } else {
-        const int sub = threadIdx.x & 7;
-        const int per = blockDim.x >> 3;
-        for (int64_t ib = 0; ib < nown * NB; ib += per) {
-            const int64_t it = ib + (threadIdx.x >> 3);
-            const int64_t i = (rb0 + (it / NB) * kSolveCluster) * NB + it % NB;
-            const bool live = it < nown * NB && i >= r0 && i < r1;
-            const float2* col = M + (live ? i : 0) * n + k0;
-            for (int q0 = 0; q0 < nrhs; q0 += 4) {
-                const int nq = min(4, nrhs - q0);
-                float ax[4] = {0.f, 0.f, 0.f, 0.f}, ay[4] = {0.f, 0.f, 0.f, 0.f};
-                if (live)
-#pragma unroll 4
-                    for (int t = sub; t < kb; t += 8) {
-                        const float2 m = col[t];  // conj(m) * y
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) {
-                            const float2 y = ys[(q0 + (q < nq ? q : 0)) * NB + t];
-                            ax[q] += m.x * y.x + m.y * y.y;
-                            ay[q] += m.x * y.y - m.y * y.x;
-                        }
-                    }
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    for (int off = 4; off > 0; off >>= 1) {
-                        ax[q] += __shfl_down_sync(0xffffffffu, ax[q], off, 8);
-                        ay[q] += __shfl_down_sync(0xffffffffu, ay[q], off, 8);
-                    }
-                if (live && sub == 0)
-                    for (int q = 0; q < nq; ++q) {
-                        const float2 v = x[(int64_t)(q0 + q) * n + i];
-                        x[(int64_t)(q0 + q) * n + i] = make_float2(v.x - ax[q], v.y - ay[q]);
-                    }
-            }
         }
     }
 }
@@ -723,7 +713,7 @@ __device__ __forceinline__ unsigned cluster_rank()
 }
 
 template <int NB, bool kCT>
-__global__ void __cluster_dims__(kSolveCluster, 1, 1) __launch_bounds__(kSolveThreads)
+__global__ void __cluster_dims__(kSolveCluster, 1, 1) __launch_bounds__(kSolveThreads, 2)
 k_lu_solve_persist(const float2* __restrict__ A, int64_t n, int64_t stride, const float2* __restrict__ Dinv,
                    int64_t dstride, float2* __restrict__ X, int64_t xstride, int nrhs)
 {
