@@ -19,6 +19,7 @@ from .bodies import (FloatingBody, combine_floatingbodies, make_body_name_list_u
                      compute_hydrodynamic_coefficients)
 from .gradients import (MeshTangent, VjpResult, hydro_batch_vjp, hydro_batch_rrule,
                         hemisphere_tangents, two_hemispheres_tangents)
+from .power import two_body_power
 from ._native import (Context, MarineHydroError, ArgumentError, NotConvergedError,
                       SingularMatrixError, device_count, default_context)
 from . import _native as native

@@ -1,0 +1,112 @@
+"""Mechanical power of two heaving hemispheres and its gradient
+(paper/Power.jl:13-83, the two-body design study).
+
+The reference computes, for spheres of radius r1 with centres (0, 0, 0) and
+(r1 + dx1, 0, 0), heave radiation on sphere 1 (A11, A12, B11, B12, assumed
+symmetric), the diffraction and Froude-Krylov heave forces on both, the 2x2
+equation of motion H Xi = F with H = w^2 (M + A) - i w (B + diag(B11)) + C,
+and J = sum(1/2 B11 |i w Xi|^2) / (2/3 pi r1^3).  Its hydrostatics come from
+Capytaine (paper/HydrostaticsRule.jl:7-15) and M = C there (Power.jl:18-19);
+Capytaine is absent, so both are restated as the heave stiffness of a
+hemisphere rho g pi r1^2 (rho = 1000, g = 9.81), keeping M = C.  As in the
+reference, the radiation pressure uses rho = 1000 (Power.jl:40) and the
+diffraction pressure rho = 1023 (:63), the Froude-Krylov pressure the default
+rho = 1000 (src/waves.jl:150-153).
+
+`two_body_power(..., grad=True)` returns dJ/d(r1, dx1, omega): the small
+2x2 algebra is differentiated with torch autograd on the host (exact), the
+boundary-element part with one `mh_hydro_batch_vjp` call and the exact mesh
+tangents of the generator.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .api import GFWu, Rankine, RankineReflected
+from .bodies import FloatingBody, hydro_batch
+from .gradients import MeshTangent, hemisphere_tangents, hydro_batch_vjp
+from .meshes import mesh_hemisphere
+
+RHO = 1000.0
+RHO_DIFFRACTION = 1023.0
+G = 9.81
+
+
+def _bodies(r1, dx1, resolution):
+    m1 = mesh_hemisphere(r1, (0.0, 0.0, 0.0), resolution)
+    m2 = mesh_hemisphere(r1, (r1 + dx1, 0.0, 0.0), resolution)
+    both = FloatingBody.rigid(m1, ["Heave"], body_name="sphere") + \
+        FloatingBody.rigid(m2, ["Heave"], body_name="sphere")
+    return both
+
+
+def _objective(A11, A12, B11, B12, F1r, F1i, F2r, F2i, K1r, K1i, K2r, K2i, w, r1):
+    """Power.jl:15-80 after the boundary-element outputs (torch scalars)."""
+    import torch
+
+    C = RHO * G * math.pi * r1 ** 2
+    M = C  # Power.jl:18-19
+    Am = torch.stack([torch.stack([A11, A12]), torch.stack([A12, A11])])
+    Bm = torch.stack([torch.stack([B11, B12]), torch.stack([B12, B11])])
+    eye = torch.eye(2, dtype=torch.float64)
+    inertia = M * eye + Am
+    pto = torch.stack([B11, B11])
+    resistance = Bm + torch.diag(pto)
+    H = (w ** 2 * inertia).to(torch.complex128) - 1j * w * resistance.to(torch.complex128) \
+        + (C * eye).to(torch.complex128)
+    scale = RHO_DIFFRACTION / RHO
+    F = torch.stack([torch.complex(scale * F1r + K1r, scale * F1i + K1i),
+                     torch.complex(scale * F2r + K2r, scale * F2i + K2i)])
+    Xi = torch.linalg.solve(H, F)
+    P = 0.5 * pto * torch.abs(1j * w * Xi) ** 2
+    return torch.sum(P) / ((2.0 / 3.0) * math.pi * r1 ** 3)
+
+
+def two_body_power(r1: float = 1.0, dx1: float = 4.0, omega: float = 1.03, *, resolution=(32, 64),
+                   green_functions=None, direct: bool = True, precision: str = "mixed",
+                   tol: float = 1e-10, grad: bool = False, ctx=None):
+    """J (and with grad=True a dict of dJ/dr1, dJ/ddx1, dJ/domega)."""
+    import torch
+
+    gfs = green_functions or (Rankine(), RankineReflected(), GFWu())
+    body = _bodies(r1, dx1, resolution)
+    dofs = list(body.dofs.values())
+    om = np.array([omega])
+    kw = dict(green_functions=gfs, direct=direct, precision=precision, tol=tol, rho=RHO, g=G, ctx=ctx)
+    A, B, Fd, Fk, _ = hydro_batch(body.mesh, om, dofs, [0.0], **kw)
+    # outputs used by Power.jl: radiation of sphere 1 (A[:, 0]), forces on both
+    leaves = [A[0, 0, 0], A[1, 0, 0], B[0, 0, 0], B[1, 0, 0],
+              Fd[0, 0, 0].real, Fd[0, 0, 0].imag, Fd[1, 0, 0].real, Fd[1, 0, 0].imag,
+              Fk[0, 0, 0].real, Fk[0, 0, 0].imag, Fk[1, 0, 0].real, Fk[1, 0, 0].imag, omega, r1]
+    t = [torch.tensor(float(v), dtype=torch.float64, requires_grad=grad) for v in leaves]
+    J = _objective(*t)
+    if not grad:
+        return float(J)
+    J.backward()
+    g = [float(x.grad) for x in t]
+    bA = np.zeros_like(A)
+    bB = np.zeros_like(B)
+    bF = np.zeros_like(Fd)
+    bK = np.zeros_like(Fk)
+    bA[0, 0, 0], bA[1, 0, 0], bB[0, 0, 0], bB[1, 0, 0] = g[0], g[1], g[2], g[3]
+    bF[0, 0, 0] = g[4] + 1j * g[5]
+    bF[1, 0, 0] = g[6] + 1j * g[7]
+    bK[0, 0, 0] = g[8] + 1j * g[9]
+    bK[1, 0, 0] = g[10] + 1j * g[11]
+    r = hydro_batch_vjp(body.mesh, om, dofs, [0.0], bA, bB, bF, bK, **kw)
+    t1 = hemisphere_tangents(r1, (0.0, 0.0, 0.0), resolution)
+    t2 = hemisphere_tangents(r1, (r1 + dx1, 0.0, 0.0), resolution)
+
+    def cat(a: MeshTangent, b: MeshTangent) -> MeshTangent:
+        return MeshTangent(np.concatenate([a.vertices, b.vertices]), np.concatenate([a.centers, b.centers]),
+                           np.concatenate([a.normals, b.normals]), np.concatenate([a.areas, b.areas]),
+                           np.concatenate([a.radii, b.radii]))
+
+    zero = MeshTangent.zeros_like(mesh_hemisphere(r1, (0.0, 0.0, 0.0), resolution))
+    # r1 scales both bodies and moves the second centre (x = r1 + dx1)
+    tan_r = cat(t1["radius"], t2["radius"] + t2["cx"])
+    tan_dx = cat(zero, t2["cx"])
+    grads = {"r1": g[13] + r.mesh.dot(tan_r), "dx1": r.mesh.dot(tan_dx), "omega": g[12] + float(r.omegas[0])}
+    return float(J.detach()), grads
