@@ -261,6 +261,32 @@ int mh_hydro_batch_vjp(mh_ctx* ctx, const mh_mesh* mesh,
                        double* d_areas, double* d_radii, double* d_omegas, double* d_dofs,
                        mh_batch_info* info);
 
+/* Forward-mode derivative of mh_hydro_batch along one direction of the
+ * inputs: the tangents of the mesh fields (t_vertices n_vertices x 3,
+ * t_centers and t_normals nfaces x 3, t_areas nfaces; radii only select
+ * branches and have none), of the frequencies (t_omegas) and of the dof
+ * fields (t_dofs, layout of dofs); any may be NULL (zero).  Returns the
+ * outputs (as mh_hydro_batch, each may be NULL) and their tangents
+ * d_added_mass, d_damping, d_diffraction, d_froude_krylov (same layouts).
+ * Replaces the reference's ForwardDiff path: Dual element types through
+ * assemble_matrices (src/matrix_assembly.jl:7-11) and `solve`
+ * (:108-114), as test/outputs_differentiation.jl:133-151 uses it.  The
+ * tangent solve reuses the forward factors.  One wave term at most
+ * (GFWu or Delhommeau); otherwise as mh_hydro_batch. */
+int mh_hydro_batch_jvp(mh_ctx* ctx, const mh_mesh* mesh,
+                       int64_t n_omega, const double* omegas,
+                       int64_t n_dof, const double* dofs,
+                       int64_t n_beta, const double* betas,
+                       double rho, double g, uint32_t gf_mask, int direct, int precision,
+                       double tol, int max_iter,
+                       const double* t_vertices, const double* t_centers, const double* t_normals,
+                       const double* t_areas, const double* t_omegas, const double* t_dofs,
+                       double* added_mass, double* damping,
+                       double* diffraction, double* froude_krylov,
+                       double* d_added_mass, double* d_damping,
+                       double* d_diffraction, double* d_froude_krylov,
+                       mh_batch_info* info);
+
 /* ---- allocation-free mixed-precision solve ------------------------------ */
 
 #define MH_NOALLOC_MAX_N    1024

@@ -17,7 +17,8 @@ from .api import (SETTINGS, set_g, set_rho, GreensFunction, Rankine, RankineRefl
 from .bodies import (FloatingBody, combine_floatingbodies, make_body_name_list_unique,
                      translational_dofs, rotational_dofs, hydro_batch, BatchInfo,
                      compute_hydrodynamic_coefficients)
-from .gradients import (MeshTangent, VjpResult, hydro_batch_vjp, hydro_batch_rrule,
+from .gradients import (MeshTangent, VjpResult, JvpResult, hydro_batch_vjp, hydro_batch_jvp,
+                        hydro_batch_rrule,
                         hemisphere_tangents, two_hemispheres_tangents)
 from .power import two_body_power
 from ._native import (Context, MarineHydroError, ArgumentError, NotConvergedError,

@@ -103,6 +103,11 @@ SIGNATURES = {
                                           ctypes.c_uint32, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_double, ctypes.c_int, _D, _D, _D, _D, _D, _D, _D,
                                           _D, _D, _D, _D, _D, _D, _D, _D, ctypes.c_void_p]),
+    "mh_hydro_batch_jvp": (ctypes.c_int, [_P, _P, ctypes.c_int64, _D, ctypes.c_int64, _D,
+                                          ctypes.c_int64, _D, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_uint32, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_double, ctypes.c_int, _D, _D, _D, _D, _D, _D, _D,
+                                          _D, _D, _D, _D, _D, _D, _D, ctypes.c_void_p]),
     "mh_solve_mixed_noalloc": (ctypes.c_int, [ctypes.c_int64, _P, _P, ctypes.c_int64, _P,
                                               ctypes.c_double, ctypes.c_int, _P,
                                               ctypes.POINTER(ctypes.c_int32),

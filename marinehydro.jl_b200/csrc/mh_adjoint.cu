@@ -38,7 +38,7 @@ namespace mh {
 namespace {
 
 constexpr int kAR = 128;  // rows (threads) per CTA of the pair kernels
-constexpr int kAC = 16;   // columns (panels in shared memory) per CTA
+constexpr int kAC = 16;   // columns (panels in shared memory) per CTA (kGradCols)
 constexpr double kI4P = 1.0 / (4.0 * kPi);
 
 // Per-panel cotangent fields (device array gbar[GB_NF][n]).
@@ -47,150 +47,15 @@ constexpr int kRowF = 6;   // row partials: centre (3), normal (3)
 constexpr int kWaveF = 7;  // wave column partials: centre, normal, area
 constexpr int kAdjAllwMinFreqs = 4;  // chunks this large use the frequency-batched Delhommeau adjoint
 
-using d2 = dualn<2>;
-using d6 = dualn<6>;
-
 unsigned nblk(int64_t count, int threads) { return (unsigned)((count + threads - 1) / threads); }
 
-__device__ __forceinline__ double re_mul(const cplx& a, const cplx& b) { return a.re * b.re - a.im * b.im; }
-
-__device__ __forceinline__ double warp_sum(double v)
-{
-    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-    return v;
-}
-
-__device__ __forceinline__ void stage(Panel* sp, const double* __restrict__ geom, int64_t n, int64_t j0)
-{
-    for (int t = threadIdx.x; t < kAC * G_NFIELDS; t += blockDim.x) {
-        const int f = t / kAC, jj = t % kAC;
-        const int64_t j = j0 + jj;
-        const double v = (j < n) ? geom[(int64_t)f * n + j] : 0.0;
-        Panel& p = sp[jj];
-        if (f < 3) p.c[f] = v;
-        else if (f < 6) p.n[f - 3] = v;
-        else if (f == G_AREA) p.area = v;
-        else if (f == G_RADIUS) p.radius = v;
-        else p.v[f - G_V] = v;
-    }
-}
-
-// Sum over the block of one value per thread; result valid in thread 0.
-__device__ __forceinline__ double block_sum(double v, double* red)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    v = warp_sum(v);
-    __syncthreads();
-    if (lane == 0) red[warp] = v;
-    __syncthreads();
-    double s = 0.0;
-    if (threadIdx.x == 0)
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
-    return s;
-}
-
-// ---------------------------------------------------------------------------
-// wave term
-// ---------------------------------------------------------------------------
-
-// Dimensionless wave term (G, G_r, G_z) with its r and z derivatives.
-struct GDer {
-    cplx G[3];
-    cplx Gr[3];
-    cplx Gz[3];
-};
-
-__device__ __forceinline__ void from_duals(const cx<d2>* o, GDer& g)
-{
-#pragma unroll
-    for (int m = 0; m < 3; ++m) {
-        g.G[m] = mk(o[m].re.v, o[m].im.v);
-        g.Gr[m] = mk(o[m].re.d[0], o[m].im.d[0]);
-        g.Gz[m] = mk(o[m].re.d[1], o[m].im.d[1]);
-    }
-}
-
-// (r, z) derivatives of Wu's formulas by 2-way dual numbers.
-__device__ __noinline__ void wave_dimless_dual(int kind, double r, double z, GDer* g)
-{
-    d2 rd, zd;
-    rd.v = r;
-    rd.d[0] = 1.0;
-    rd.d[1] = 0.0;
-    zd.v = z;
-    zd.d[0] = 0.0;
-    zd.d[1] = 1.0;
-    cx<d2> o[3];
-    (void)kind;
-    wu_dimless(rd, zd, o);
-    from_duals(o, *g);
-}
-
-// r, z derivatives of the Delhommeau wave term from its values: with
-// G_r = G1 and G_z = G2 = G + 2/R (exact_Guevel_Delhommeau.jl:56), the wave
-// part is harmonic in the fluid, so G_zz = G_z - 2z/R^3, G_rz = G_r - 2r/R^3
-// and G_rr = -G_r/r - G_zz (-G_zz/2 as r -> 0).  These are the derivatives
-// of the function itself (what the reference's AD of its quadrature
-// gives), whichever way its values were obtained.
-__device__ __forceinline__ void gder_identities(const cplx G[3], double r, double z, double R, GDer& o)
-{
-    const double iR = 1.0 / R, iR3 = iR * iR * iR;
-    const cplx Gzz = G[2] - mk(2.0 * z * iR3, 0.0);
-    const cplx Grz = G[1] - mk(2.0 * r * iR3, 0.0);
-    const cplx Grr = (r > 1e-3) ? -(G[1] / r) - Gzz : mk(-0.5 * Gzz.re, -0.5 * Gzz.im);
-#pragma unroll
-    for (int m = 0; m < 3; ++m) o.G[m] = G[m];
-    o.Gr[0] = G[1];
-    o.Gz[0] = G[2];
-    o.Gr[1] = Grr;
-    o.Gz[1] = Grz;
-    o.Gr[2] = Grz;
-    o.Gz[2] = Gzz;
-}
-
-// Delhommeau term and its r, z derivatives at one point: the forward's
-// value (table, or the quadrature outside it / without a table), then the
-// identities.
-__device__ __noinline__ void delh_point_grad(const double* __restrict__ tab, double r, double z, GDer* out)
-{
-    cplx G[3];
-    if (tab) delh_dimless_table(tab, r, z, G);
-    else delh_dimless(r, z, G);
-    gder_identities(G, r, z, hypot(r, z), *out);
-}
-
-// kind 1: Wu (exact derivatives of its formulas); kind 2: Delhommeau.
-__device__ __forceinline__ void wave_dimless_grad(int kind, const double* __restrict__ tab, double r, double z,
-                                                  GDer& g)
-{
-    if (kind == 2) delh_point_grad(tab, r, z, &g);
-    else wave_dimless_dual(kind, r, z, &g);
-}
+#include "mh_grad.cuh"
+static_assert(kAC == kGradCols, "pair kernels stage kGradCols panels");
 
 struct WaveBar {
     double dx, dy, zs, area, k;
     double n[3];
 };
-
-// Pair geometry of the wave term (abstract_greens_function.jl:88-155 at k = 1).
-struct WaveGeom {
-    double dx, dy, zs, dis, u0, u1, invd;
-};
-
-__device__ __forceinline__ WaveGeom wave_geom(const double x[3], const Panel& p)
-{
-    WaveGeom w;
-    w.dx = x[0] - p.c[0];
-    w.dy = x[1] - p.c[1];
-    w.zs = x[2] + p.c[2];
-    const double dis2 = w.dx * w.dx + w.dy * w.dy;
-    const double purt = 1e-18;
-    w.dis = (dis2 == 0.0) ? sqrt(dis2 + purt * purt) - purt : sqrt(dis2);
-    w.invd = w.dis > 0.0 ? 1.0 / w.dis : 0.0;
-    w.u0 = w.dx * w.invd;
-    w.u1 = w.dy * w.invd;
-    return w;
-}
 
 // Reverse of wave_pair for one pair and one k, given the dimensionless term
 // and its derivatives at (r, z) = k (dis, zs): L = Re(cs s + cw (nD . g)),
@@ -1134,9 +999,8 @@ int adjoint_mixed_chunk(const Batch& bt, Vjp& vj, const double* d_omegas, const 
     auto* PHIi = (double2*)ctx->ws[WS_TMP];  // phi = S sigma (indirect)
     auto* adj = (double2*)ws_get(ctx, WS_ADJ, sizeof(double2) * cnt * 5);
     auto* R32 = (float2*)ws_get(ctx, WS_TMP32, sizeof(float2) * cnt);
-    auto* T32 = (float2*)ws_get(ctx, WS_TMP32B, sizeof(float2) * cnt);
     auto* misc = (double*)ws_get(ctx, WS_MISC, (sizeof(double) + sizeof(int)) * nb + 64);
-    if (!adj || !R32 || !T32 || !misc) return MH_ERR_OOM;
+    if (!adj || !R32 || !misc) return MH_ERR_OOM;
     double2* PB = adj;
     double2* LAM = adj + cnt;
     double2* BB = adj + 2 * cnt;
@@ -1152,41 +1016,10 @@ int adjoint_mixed_chunk(const Batch& bt, Vjp& vj, const double* d_omegas, const 
     } else if ((rc = zgemm_ct_strided(ctx, n, nrhs, S64, PB, RHS, nb, 1.0, 0.0))) {
         return rc;
     }
-    // refinement of D^H lam = RHS
-    MH_CUDA_TRY(ctx, cudaMemsetAsync(LAM, 0, sizeof(double2) * cnt, ctx->stream));
-    MH_CUDA_TRY(ctx, cudaMemcpyAsync(R, RHS, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, ctx->stream));
-    std::vector<double> h_res(nb, INFINITY);
-    for (int it = 1; it <= max_iter; ++it) {
-        MH_CUDA_TRY(ctx, launch_to_f32(ctx, R, R32, cnt));
-        MH_CUDA_TRY(ctx, launch_lu_solve_persist(ctx, tc ? MH_LU_TCGEN05_F16 : MH_LU_SIMT_F32, true, Dlo, n, nn,
-                                                 nb, Dinv, R32, nv, nrhs));
-        MH_CUDA_TRY(ctx, launch_add_f32(ctx, LAM, R32, cnt));
-        MH_CUDA_TRY(ctx, launch_residual(ctx, true, D64, n, nb, LAM, RHS, R, nrhs));
-        MH_CUDA_TRY(ctx, launch_rel_residual(ctx, R, RHS, n, nrhs, nb, misc));
-        MH_CUDA_TRY(ctx, cudaMemcpyAsync(h_res.data(), misc, sizeof(double) * nb, cudaMemcpyDeviceToHost,
-                                         ctx->stream));
-        MH_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-        double worst = 0.0;
-        for (int z = 0; z < nb; ++z)
-            if (!fb.used[z]) worst = std::max(worst, std::isfinite(h_res[z]) ? h_res[z] : INFINITY);
-        info->refine_iterations = std::max(info->refine_iterations, it);
-        if (worst <= tol) break;
-    }
-    for (int z = 0; z < nb; ++z) {
-        if (!fb.used[z] && h_res[z] <= tol) {
-            info->max_rel_residual = std::max(info->max_rel_residual, h_res[z]);
-            continue;
-        }
-        if (!fb.used[z]) {
-            info->n_fallback += 1;
-            if ((rc = fallback_factor(ctx, &fb, n, nb, z, D64 + (int64_t)z * nn))) return rc;
-        }
-        double2* Lz = LAM + (int64_t)z * nv;
-        MH_CUDA_TRY(ctx, cudaMemcpyAsync(Lz, RHS + (int64_t)z * nv, sizeof(double2) * nv,
-                                         cudaMemcpyDeviceToDevice, ctx->stream));
-        if ((rc = fp64_getrs(ctx, true, n, fb.lu + (int64_t)z * nn, fb.piv + (int64_t)z * n, Lz, nrhs)))
-            return rc;
-    }
+    // D^H lam = RHS: low-precision factors + FP64 refinement, FP64 fallback
+    if ((rc = mixed_refine_solve(ctx, n, nb, nrhs, D64, Dlo, Dinv, RHS, LAM, R, R32, misc, true, tol, max_iter,
+                                 fb, info)))
+        return rc;
     if (bt.direct && (rc = zgemm_ct_strided(ctx, n, nrhs, S64, LAM, BB, nb, 1.0, 0.0))) return rc;
     phase_end(ctx, PH_ADJ_SOLVE);
     if (bt.direct) return adjoint_tail(bt, vj, d_omegas, d_k, nb, z0, tab, LAM, BC, LAM, X, BB);

@@ -680,4 +680,31 @@ int mh_hydro_batch_vjp(mh_ctx* ctx, const mh_mesh* mesh, int64_t n_omega, const 
                                d_omegas, d_dofs, info);
 }
 
+int mh_hydro_batch_jvp(mh_ctx* ctx, const mh_mesh* mesh, int64_t n_omega, const double* omegas,
+                       int64_t n_dof, const double* dofs, int64_t n_beta, const double* betas,
+                       double rho, double g, uint32_t gf_mask, int direct, int precision, double tol,
+                       int max_iter, const double* t_vertices, const double* t_centers,
+                       const double* t_normals, const double* t_areas, const double* t_omegas,
+                       const double* t_dofs, double* added_mass, double* damping, double* diffraction,
+                       double* froude_krylov, double* d_added_mass, double* d_damping,
+                       double* d_diffraction, double* d_froude_krylov, mh_batch_info* info)
+{
+    int rc;
+    if ((rc = check_batch(ctx, mesh, n_omega, omegas, n_dof, dofs, n_beta, betas, rho, g, gf_mask,
+                          precision, tol, max_iter)))
+        return rc;
+    if ((gf_mask & MH_GF_WU) && (gf_mask & MH_GF_DELHOMMEAU))
+        return set_err(ctx, MH_ERR_ARG, "the tangent path takes one wave term (GFWu or Delhommeau)");
+    const int64_t n = mesh->n;
+    if ((t_vertices && !finite_array(t_vertices, 3 * mesh->nv)) ||
+        (t_centers && !finite_array(t_centers, 3 * n)) || (t_normals && !finite_array(t_normals, 3 * n)) ||
+        (t_areas && !finite_array(t_areas, n)) || (t_omegas && !finite_array(t_omegas, n_omega)) ||
+        (t_dofs && !finite_array(t_dofs, 3 * n * n_dof)))
+        return set_err(ctx, MH_ERR_ARG, "tangents must be finite");
+    return mh::hydro_batch_jvp(ctx, mesh, n_omega, omegas, n_dof, dofs, n_beta, betas, rho, g, gf_mask,
+                               direct, precision, tol, max_iter, t_vertices, t_centers, t_normals, t_areas,
+                               t_omegas, t_dofs, added_mass, damping, diffraction, froude_krylov,
+                               d_added_mass, d_damping, d_diffraction, d_froude_krylov, info);
+}
+
 }  // extern "C"

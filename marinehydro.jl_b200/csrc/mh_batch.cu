@@ -720,6 +720,49 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
     return MH_OK;
 }
 
+int mixed_refine_solve(mh_ctx* ctx, int64_t n, int nb, int nrhs, const double2* D64, const float2* Dlo,
+                       const float2* Dinv, const double2* RHS, double2* X, double2* R, float2* R32, double* d_res,
+                       bool conj_trans, double tol, int max_iter, FallbackStore& fb, mh_batch_info* info)
+{
+    const int64_t nn = n * n, nv = n * nrhs, cnt = nv * nb;
+    int rc;
+    MH_CUDA_TRY(ctx, cudaMemsetAsync(X, 0, sizeof(double2) * cnt, ctx->stream));
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(R, RHS, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, ctx->stream));
+    std::vector<double> h_res(nb, INFINITY);
+    for (int it = 1; it <= max_iter; ++it) {
+        MH_CUDA_TRY(ctx, launch_to_f32(ctx, R, R32, cnt));
+        MH_CUDA_TRY(ctx, launch_lu_solve_persist(ctx, ctx->lu_backend, conj_trans, Dlo, n, nn, nb, Dinv, R32, nv,
+                                                 nrhs));
+        MH_CUDA_TRY(ctx, launch_add_f32(ctx, X, R32, cnt));
+        MH_CUDA_TRY(ctx, launch_residual(ctx, conj_trans, D64, n, nb, X, RHS, R, nrhs));
+        MH_CUDA_TRY(ctx, launch_rel_residual(ctx, R, RHS, n, nrhs, nb, d_res));
+        MH_CUDA_TRY(ctx, cudaMemcpyAsync(h_res.data(), d_res, sizeof(double) * nb, cudaMemcpyDeviceToHost,
+                                         ctx->stream));
+        MH_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        double worst = 0.0;
+        for (int z = 0; z < nb; ++z)
+            if (!fb.used[z]) worst = std::max(worst, std::isfinite(h_res[z]) ? h_res[z] : INFINITY);
+        info->refine_iterations = std::max(info->refine_iterations, it);
+        if (worst <= tol) break;
+    }
+    for (int z = 0; z < nb; ++z) {
+        if (!fb.used[z] && h_res[z] <= tol) {
+            info->max_rel_residual = std::max(info->max_rel_residual, h_res[z]);
+            continue;
+        }
+        if (!fb.used[z]) {
+            info->n_fallback += 1;
+            if ((rc = fallback_factor(ctx, &fb, n, nb, z, D64 + (int64_t)z * nn))) return rc;
+        }
+        double2* Xz = X + (int64_t)z * nv;
+        MH_CUDA_TRY(ctx, cudaMemcpyAsync(Xz, RHS + (int64_t)z * nv, sizeof(double2) * nv, cudaMemcpyDeviceToDevice,
+                                         ctx->stream));
+        if ((rc = fp64_getrs(ctx, conj_trans, n, fb.lu + (int64_t)z * nn, fb.piv + (int64_t)z * n, Xz, nrhs)))
+            return rc;
+    }
+    return MH_OK;
+}
+
 int fallback_factor(mh_ctx* ctx, FallbackStore* fb, int64_t n, int nb, int z, const double2* D)
 {
     const int64_t nn = n * n;

@@ -163,6 +163,13 @@ int fp64_getrs(mh_ctx* ctx, bool conj_trans, int64_t n, const double2* LU, const
                int nrhs);
 int fp64_lu_solve(mh_ctx* ctx, int64_t n, double2* A, double2* B, int nrhs);
 int fallback_factor(mh_ctx* ctx, FallbackStore* fb, int64_t n, int nb, int z, const double2* D);
+// X = op(D)^-1 RHS for nb problems (op = identity or ^H) with the low-precision
+// factors (Dlo, Dinv) and FP64 refinement against D64 to tol; problems whose
+// forward solve fell back (fb.used) or that do not converge use FP64 factors.
+// R (FP64) and R32 (FP32) are scratch of the size of RHS, d_res nb doubles.
+int mixed_refine_solve(mh_ctx* ctx, int64_t n, int nb, int nrhs, const double2* D64, const float2* Dlo,
+                       const float2* Dinv, const double2* RHS, double2* X, double2* R, float2* R32, double* d_res,
+                       bool conj_trans, double tol, int max_iter, FallbackStore& fb, mh_batch_info* info);
 // Frequency-independent Rankine parts SR, DR (n x n real) of the mixed path.
 int rankine_real(const Batch& bt, double* SR, double* DR);
 // One chunk of the mixed path; leaves S (WS_S), D (WS_D), the low-precision
@@ -189,6 +196,15 @@ int hydro_batch_vjp(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double*
                     double* diffraction, double* froude_krylov, double* d_vertices, double* d_centers,
                     double* d_normals, double* d_areas, double* d_radii, double* d_omegas_out,
                     double* d_dofs_out, mh_batch_info* info);
+
+// ---- forward mode (mh_jvp.cu) ----
+int hydro_batch_jvp(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double* omegas, int64_t ndof,
+                    const double* dofs, int64_t nbeta, const double* betas, double rho, double g, uint32_t mask,
+                    int direct, int precision, double tol, int max_iter, const double* t_vertices,
+                    const double* t_centers, const double* t_normals, const double* t_areas, const double* t_omegas,
+                    const double* t_dofs, double* added_mass, double* damping, double* diffraction,
+                    double* froude_krylov, double* d_added_mass, double* d_damping, double* d_diffraction,
+                    double* d_froude_krylov, mh_batch_info* info);
 
 // ---- Delhommeau table (mh_table.cu) ----
 int ensure_delh_table(mh_ctx* ctx);

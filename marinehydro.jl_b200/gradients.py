@@ -9,6 +9,10 @@ returns the cotangents of every input: the mesh fields (a ``MeshTangent``,
 the counterpart of the reference's ``Tangent{Mesh}``), the frequencies and
 the dof motion fields.
 
+``hydro_batch_jvp`` is the forward mode (the reference's ForwardDiff path):
+the tangents of all outputs along one input direction, e.g. dA/dR for every
+frequency at once.
+
 ``hydro_batch_rrule`` is the rrule / ``torch.autograd.Function`` shaped
 entry point: it returns the outputs and a pullback; the pullback recomputes
 the forward batch on the device (geometry and factors are recomputed rather
@@ -140,6 +144,65 @@ def hydro_batch_vjp(mesh: Mesh, omegas, dofs, betas=(), bar_added_mass=None, bar
              for q in range(nd)]
     return VjpResult(A, B, Fd, Fk, MeshTangent(np.ascontiguousarray(gv), np.ascontiguousarray(gc),
                                                np.ascontiguousarray(gn), ga, gr), gw, ddofs,
+                     BatchInfo(info.refine_iterations, info.n_fallback, info.max_rel_residual))
+
+
+@dataclass
+class JvpResult:
+    added_mass: np.ndarray
+    damping: np.ndarray
+    diffraction: np.ndarray
+    froude_krylov: np.ndarray
+    d_added_mass: np.ndarray
+    d_damping: np.ndarray
+    d_diffraction: np.ndarray
+    d_froude_krylov: np.ndarray
+    info: BatchInfo
+
+
+def hydro_batch_jvp(mesh: Mesh, omegas, dofs, betas=(), t_mesh: MeshTangent | None = None,
+                    t_omegas=None, t_dofs=None, *, green_functions=DEFAULT_GREEN_FUNCTIONS,
+                    direct: bool = True, precision="mixed", tol: float = 1e-10, max_iter: int = 30,
+                    rho=None, g=None, ctx=None) -> JvpResult:
+    """Forward batch (as ``hydro_batch``) plus the tangents of its outputs
+    along one direction of the inputs (``mh_hydro_batch_jvp``): the tangent
+    of the mesh fields (a ``MeshTangent``; radii have no effect), of the
+    frequencies and of the dof fields (None = zero)."""
+    mask = gf_mask(green_functions)
+    dm = device_mesh(mesh, ctx)
+    om = np.ascontiguousarray(np.asarray(omegas, dtype=np.float64).reshape(-1))
+    d = [np.asarray(x, dtype=np.float64) for x in dofs]
+    nd = len(d)
+    dof_arr = np.ascontiguousarray(
+        np.concatenate([np.asfortranarray(x).reshape(-1, order="F") for x in d]) if nd else np.zeros(1))
+    be = np.ascontiguousarray(np.asarray(betas, dtype=np.float64).reshape(-1))
+    nw, nb = om.shape[0], be.shape[0]
+    f = lambda a: None if a is None else np.ascontiguousarray(np.asfortranarray(np.asarray(a, dtype=np.float64))
+                                                                .reshape(-1, order="F"))
+    tv = tc = tn = ta = None
+    if t_mesh is not None:
+        tv, tc, tn, ta = f(t_mesh.vertices), f(t_mesh.centers), f(t_mesh.normals), f(t_mesh.areas)
+    tw = f(t_omegas)
+    td = None
+    if t_dofs is not None:
+        td = np.ascontiguousarray(np.concatenate([np.asfortranarray(np.asarray(x, dtype=np.float64))
+                                                  .reshape(-1, order="F") for x in t_dofs]))
+    A = np.zeros((nd, nd, nw), order="F")
+    B = np.zeros((nd, nd, nw), order="F")
+    Fd = np.zeros((nd, nw, nb), dtype=np.complex128, order="F")
+    Fk = np.zeros((nd, nw, nb), dtype=np.complex128, order="F")
+    dA, dB, dFd, dFk = np.zeros_like(A), np.zeros_like(B), np.zeros_like(Fd), np.zeros_like(Fk)
+    info = _Info()
+    nbp = (lambda a: N.dptr(a) if nb else None)
+    N.check(N.lib().mh_hydro_batch_jvp(
+        dm.ctx.handle, dm.handle, nw, N.dptr(om), nd, N.dptr(dof_arr), nb,
+        N.dptr(be) if nb else None,
+        float(SETTINGS.rho if rho is None else rho), float(SETTINGS.g if g is None else g), mask,
+        int(bool(direct)), _precision_code(precision), float(tol), int(max_iter),
+        N.dptr(tv), N.dptr(tc), N.dptr(tn), N.dptr(ta), N.dptr(tw), N.dptr(td),
+        N.dptr(A), N.dptr(B), nbp(Fd), nbp(Fk), N.dptr(dA), N.dptr(dB), nbp(dFd), nbp(dFk),
+        ctypes.byref(info)), dm.ctx.handle)
+    return JvpResult(A, B, Fd, Fk, dA, dB, dFd, dFk,
                      BatchInfo(info.refine_iterations, info.n_fallback, info.max_rel_residual))
 
 
