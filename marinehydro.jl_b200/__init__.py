@@ -21,6 +21,7 @@ from .gradients import (MeshTangent, VjpResult, JvpResult, hydro_batch_vjp, hydr
                         hydro_batch_rrule,
                         hemisphere_tangents, two_hemispheres_tangents)
 from .power import two_body_power
+from .design import SplitMix64, Design, designs, design_batch
 from ._native import (Context, MarineHydroError, ArgumentError, NotConvergedError,
                       SingularMatrixError, device_count, default_context)
 from . import _native as native
