@@ -1013,14 +1013,14 @@ int adjoint_mixed_chunk(const Batch& bt, Vjp& vj, const double* d_omegas, const 
     phase_begin(ctx, PH_ADJ_SOLVE);
     if (bt.direct) {
         MH_CUDA_TRY(ctx, cudaMemcpyAsync(RHS, PB, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, ctx->stream));
-    } else if ((rc = zgemm_ct_strided(ctx, n, nrhs, S64, PB, RHS, nb, 1.0, 0.0))) {
-        return rc;
+    } else {
+        MH_CUDA_TRY(ctx, launch_gemv(ctx, true, S64, n, nb, PB, nullptr, RHS, nrhs, 1.0, 0.0));
     }
     // D^H lam = RHS: low-precision factors + FP64 refinement, FP64 fallback
     if ((rc = mixed_refine_solve(ctx, n, nb, nrhs, D64, Dlo, Dinv, RHS, LAM, R, R32, misc, true, tol, max_iter,
                                  fb, info)))
         return rc;
-    if (bt.direct && (rc = zgemm_ct_strided(ctx, n, nrhs, S64, LAM, BB, nb, 1.0, 0.0))) return rc;
+    if (bt.direct) MH_CUDA_TRY(ctx, launch_gemv(ctx, true, S64, n, nb, LAM, nullptr, BB, nrhs, 1.0, 0.0));
     phase_end(ctx, PH_ADJ_SOLVE);
     if (bt.direct) return adjoint_tail(bt, vj, d_omegas, d_k, nb, z0, tab, LAM, BC, LAM, X, BB);
     return adjoint_tail(bt, vj, d_omegas, d_k, nb, z0, tab, PB, X, LAM, X, LAM);

@@ -359,15 +359,17 @@ __global__ void k_add_f32(double2* __restrict__ x, const float2* __restrict__ d,
     if (t < count) x[t] = make_double2(x[t].x + (double)d[t].x, x[t].y + (double)d[t].y);
 }
 
-// Refinement residuals in FP64, bandwidth-bound reads of the n x n complex
-// matrices (column-major, nb of them, n*n apart), nrhs <= kMaxRhs:
-// k_resid_n: R = B - A X, one thread per row i, coalesced down the columns;
-// k_resid_c: R = B - A^H X, one warp per output j reading column j.
+// Batched complex matrix products with few columns in FP64 (refinement
+// residuals, S b, S^H lambda), bandwidth-bound reads of the n x n matrices
+// (column-major, nb of them, n*n apart), nrhs <= kMaxRhs:
+// k_resid_n: R = beta B + alpha A X, one thread per row i, coalesced down the
+// columns; k_resid_c: R = beta B + alpha A^H X, one warp per output j reading
+// column j.  B may be R (read before written) or null when beta = 0.
 // Q >= nrhs: accumulators per thread (4, 8 or 16, picked by the launcher).
 template <int Q>
 __global__ void __launch_bounds__(256)
-k_resid_n(const double2* __restrict__ A, const double2* __restrict__ X, const double2* __restrict__ B,
-          double2* __restrict__ R, int64_t n, int nrhs)
+k_resid_n(const double2* __restrict__ A, const double2* __restrict__ X, const double2* B, double2* R, int64_t n,
+          int nrhs, double alpha, double beta)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t b = blockIdx.y;
@@ -392,14 +394,15 @@ k_resid_n(const double2* __restrict__ A, const double2* __restrict__ X, const do
     for (int q = 0; q < Q; ++q)
         if (q < nrhs) {
             const int64_t o = b * n * nrhs + (int64_t)q * n + i;
-            R[o] = make_double2(B[o].x - ar[q], B[o].y - ai[q]);
+            const double2 bo = B ? B[o] : make_double2(0.0, 0.0);
+            R[o] = make_double2(beta * bo.x + alpha * ar[q], beta * bo.y + alpha * ai[q]);
         }
 }
 
 template <int Q>
 __global__ void __launch_bounds__(256)
-k_resid_c(const double2* __restrict__ A, const double2* __restrict__ X, const double2* __restrict__ B,
-          double2* __restrict__ R, int64_t n, int nrhs)
+k_resid_c(const double2* __restrict__ A, const double2* __restrict__ X, const double2* B, double2* R, int64_t n,
+          int nrhs, double alpha, double beta)
 {
     const int lane = threadIdx.x & 31;
     const int64_t j = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -430,7 +433,8 @@ k_resid_c(const double2* __restrict__ A, const double2* __restrict__ X, const do
             }
             if (lane == 0) {
                 const int64_t o = b * n * nrhs + (int64_t)q * n + j;
-                R[o] = make_double2(B[o].x - ar[q], B[o].y - ai[q]);
+                const double2 bo = B ? B[o] : make_double2(0.0, 0.0);
+                R[o] = make_double2(beta * bo.x + alpha * ar[q], beta * bo.y + alpha * ai[q]);
             }
         }
 }
@@ -638,7 +642,7 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
     ctx->launches += 1;
     MH_CUDA_TRY(ctx, cudaGetLastError());
     if (bt.direct) {
-        if ((rc = zgemm_strided(ctx, n, nrhs, S64, BC, RHS, nb, 1.0, 0.0))) return rc;
+        MH_CUDA_TRY(ctx, launch_gemv(ctx, false, S64, n, nb, BC, nullptr, RHS, nrhs, 1.0, 0.0));
     } else {
         MH_CUDA_TRY(ctx, cudaMemcpyAsync(RHS, BC, sizeof(double2) * nv * nb, cudaMemcpyDeviceToDevice,
                                          ctx->stream));
@@ -708,7 +712,7 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
     // indirect: phi = S sigma
     double2* PHI = X;
     if (!bt.direct) {
-        if ((rc = zgemm_strided(ctx, n, nrhs, S64, X, R, nb, 1.0, 0.0))) return rc;
+        MH_CUDA_TRY(ctx, launch_gemv(ctx, false, S64, n, nb, X, nullptr, R, nrhs, 1.0, 0.0));
         PHI = R;
     }
     phase_begin(ctx, PH_FORCES);
@@ -823,22 +827,29 @@ cudaError_t launch_add_f32(mh_ctx* ctx, double2* x, const float2* d, int64_t cou
     return cudaGetLastError();
 }
 
-cudaError_t launch_residual(mh_ctx* ctx, bool conj_trans, const double2* A, int64_t n, int nb, const double2* X,
-                            const double2* B, double2* R, int nrhs)
+cudaError_t launch_gemv(mh_ctx* ctx, bool conj_trans, const double2* A, int64_t n, int nb, const double2* X,
+                        const double2* B, double2* R, int nrhs, double alpha, double beta)
 {
     if (nrhs < 1 || nrhs > kMaxRhs) return cudaErrorInvalidValue;
+    if (beta == 0.0) B = nullptr;
     const dim3 gc(blocks(n, 8), (unsigned)nb), gn(blocks(n, 256), (unsigned)nb);
     if (conj_trans) {
-        if (nrhs <= 4) k_resid_c<4><<<gc, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs);
-        else if (nrhs <= 8) k_resid_c<8><<<gc, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs);
-        else k_resid_c<kMaxRhs><<<gc, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs);
+        if (nrhs <= 4) k_resid_c<4><<<gc, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta);
+        else if (nrhs <= 8) k_resid_c<8><<<gc, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta);
+        else k_resid_c<kMaxRhs><<<gc, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta);
     } else {
-        if (nrhs <= 4) k_resid_n<4><<<gn, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs);
-        else if (nrhs <= 8) k_resid_n<8><<<gn, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs);
-        else k_resid_n<kMaxRhs><<<gn, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs);
+        if (nrhs <= 4) k_resid_n<4><<<gn, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta);
+        else if (nrhs <= 8) k_resid_n<8><<<gn, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta);
+        else k_resid_n<kMaxRhs><<<gn, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta);
     }
     ctx->launches += 1;
     return cudaGetLastError();
+}
+
+cudaError_t launch_residual(mh_ctx* ctx, bool conj_trans, const double2* A, int64_t n, int nb, const double2* X,
+                            const double2* B, double2* R, int nrhs)
+{
+    return launch_gemv(ctx, conj_trans, A, n, nb, X, B, R, nrhs, -1.0, 1.0);
 }
 
 cudaError_t launch_rel_residual(mh_ctx* ctx, const double2* r, const double2* b, int64_t n, int nrhs,

@@ -146,6 +146,10 @@ struct FallbackStore {
 };
 cudaError_t launch_to_f32(mh_ctx* ctx, const double2* a, float2* b, int64_t count);
 cudaError_t launch_add_f32(mh_ctx* ctx, double2* x, const float2* d, int64_t count);
+// R = beta B + alpha op(A) X for nb n x n complex matrices (op = identity or
+// ^H), X and B n x nrhs per matrix; B may be R, or null when beta = 0.
+cudaError_t launch_gemv(mh_ctx* ctx, bool conj_trans, const double2* A, int64_t n, int nb, const double2* X,
+                        const double2* B, double2* R, int nrhs, double alpha, double beta);
 // R = B - op(A) X for nb n x n complex matrices (op = identity or ^H).
 cudaError_t launch_residual(mh_ctx* ctx, bool conj_trans, const double2* A, int64_t n, int nb, const double2* X,
                             const double2* B, double2* R, int nrhs);

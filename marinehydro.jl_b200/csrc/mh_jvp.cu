@@ -17,9 +17,9 @@
 // the templated `rankine_pair` with 1-way dual numbers; the wave part per pair
 // and frequency from the r, z derivatives of the dimensionless term (Wu by
 // dual numbers, Delhommeau by its identities, frequency batched like the
-// forward pass).  The products with b, phi use the batched ZGEMM, the solve
-// reuses the forward factors (FP64 zgetrs, or the low-precision factors with
-// FP64 refinement).
+// forward pass).  The products with b, phi use the batched bandwidth-bound
+// GEMV (launch_gemv), the solve reuses the forward factors (FP64 zgetrs, or
+// the low-precision factors with FP64 refinement).
 #include <cuComplex.h>
 #include <cuda_runtime.h>
 
@@ -491,17 +491,15 @@ int tangent_chunk(const Batch& bt, const Jvp& jv, const double* d_om, const doub
     ctx->launches += 1;
     MH_CUDA_TRY(ctx, cudaGetLastError());
     if (bt.direct) {  // T = dS b + S db - dD phi; dphi = D^-1 T
-        if ((rc = zgemm_strided(ctx, n, nrhs, dS, BC, T, nb, 1.0, 0.0))) return rc;
-        if ((rc = zgemm_strided(ctx, n, nrhs, S64, dBC, T, nb, 1.0, 1.0))) return rc;
-        if ((rc = zgemm_strided(ctx, n, nrhs, dD, X, T, nb, -1.0, 1.0))) return rc;
+        MH_CUDA_TRY(ctx, launch_gemv(ctx, false, dS, n, nb, BC, nullptr, T, nrhs, 1.0, 0.0));
+        MH_CUDA_TRY(ctx, launch_gemv(ctx, false, S64, n, nb, dBC, T, T, nrhs, 1.0, 1.0));
+        MH_CUDA_TRY(ctx, launch_gemv(ctx, false, dD, n, nb, X, T, T, nrhs, -1.0, 1.0));
         if ((rc = solve(T, DPHI))) return rc;
     } else {  // T = db - dK sigma; dsigma = K^-1 T; dphi = dS sigma + S dsigma
-        MH_CUDA_TRY(ctx, cudaMemcpyAsync(T, dBC, sizeof(double2) * n * nrhs * nb, cudaMemcpyDeviceToDevice,
-                                         ctx->stream));
-        if ((rc = zgemm_strided(ctx, n, nrhs, dD, X, T, nb, -1.0, 1.0))) return rc;
+        MH_CUDA_TRY(ctx, launch_gemv(ctx, false, dD, n, nb, X, dBC, T, nrhs, -1.0, 1.0));
         if ((rc = solve(T, DX))) return rc;
-        if ((rc = zgemm_strided(ctx, n, nrhs, dS, X, DPHI, nb, 1.0, 0.0))) return rc;
-        if ((rc = zgemm_strided(ctx, n, nrhs, S64, DX, DPHI, nb, 1.0, 1.0))) return rc;
+        MH_CUDA_TRY(ctx, launch_gemv(ctx, false, dS, n, nb, X, nullptr, DPHI, nrhs, 1.0, 0.0));
+        MH_CUDA_TRY(ctx, launch_gemv(ctx, false, S64, n, nb, DX, DPHI, DPHI, nrhs, 1.0, 1.0));
     }
     k_forces_tangent<<<nb * nrhs, 256, 0, ctx->stream>>>(bt.m->geom, jv.tgeom, n, bt.d_dofs, jv.tdofs, bt.ndof,
                                                         bt.d_betas, bt.nbeta, d_om, d_dom, bt.rho, bt.g, PHI, DPHI,
