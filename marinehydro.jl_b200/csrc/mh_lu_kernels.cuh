@@ -66,34 +66,48 @@ k_lu_diag(float2* __restrict__ A, int64_t n, int64_t stride, int64_t k0, float2*
         M[(k0 + c) * n + k0 + r] = s[r][c];
     }
     float2* out = Dinv + b * dstride + (k0 / NB) * 2 * NB * NB;
-    // inv(L11): column c solves L y = e_c (unit lower), one thread per column
-    if (threadIdx.x < NB) {
-        const int c = threadIdx.x;
-        for (int r = 0; r < NB; ++r) {
-            float2 acc = make_float2(r == c ? 1.f : 0.f, 0.f);
-            for (int t = c; t < r; ++t) acc = cfms(acc, s[r][t], w[t][c]);
-            w[r][c] = (r < c) ? make_float2(0.f, 0.f) : acc;
-        }
+    // inv(L11), unit lower: W = I, then for t ascending the rows below t
+    // subtract L[r][t] W[t][:] (row t is final at step t); all threads per sweep.
+    for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) {
+        const int r = t % NB, c = t / NB;
+        w[r][c] = make_float2(r == c ? 1.f : 0.f, 0.f);
     }
     __syncthreads();
+    for (int t = 0; t + 1 < kb; ++t) {
+        const int wdt = t + 1, cnt = (kb - 1 - t) * wdt;
+        for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+            const int r = t + 1 + e / wdt, c = e % wdt;
+            w[r][c] = cfms(w[r][c], s[r][t], w[t][c]);
+        }
+        __syncthreads();
+    }
     for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) out[t] = w[t % NB][t / NB];
     __syncthreads();
-    // inv(U11): column c solves U y = e_c, backward, one thread per column
-    if (threadIdx.x < NB) {
-        const int c = threadIdx.x;
-        for (int r = NB - 1; r >= 0; --r) {
-            float2 acc = make_float2(r == c ? 1.f : 0.f, 0.f);
-            if (r <= c) {
-                for (int t = r + 1; t <= c; ++t) acc = cfms(acc, s[r][t], w[t][c]);
-                acc = cdivf(acc, s[r][r]);
-            } else {
-                acc = make_float2(0.f, 0.f);
-            }
-            w[r][c] = acc;
-        }
+    // inv(U11): W = I, then for t descending the rows above t subtract
+    // U[r][t] / U[t][t] W[t][:], and finally row r is scaled by 1 / U[r][r].
+    for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) {
+        const int r = t % NB, c = t / NB;
+        w[r][c] = make_float2(r == c ? 1.f : 0.f, 0.f);
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) out[NB * NB + t] = w[t % NB][t / NB];
+    if (threadIdx.x < NB) {  // the padding column of w holds 1 / U[r][r]
+        const int r = threadIdx.x;
+        w[r][NB] = r < kb ? cdivf(make_float2(1.f, 0.f), s[r][r]) : make_float2(1.f, 0.f);
+    }
+    __syncthreads();
+    for (int t = kb - 1; t >= 1; --t) {
+        const int wdt = kb - t, cnt = t * wdt;
+        const float2 f = w[t][NB];
+        for (int e = threadIdx.x; e < cnt; e += blockDim.x) {
+            const int r = e / wdt, c = t + e % wdt;
+            w[r][c] = cfms(w[r][c], cmulf(s[r][t], f), w[t][c]);
+        }
+        __syncthreads();
+    }
+    for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) {
+        const int r = t % NB, c = t / NB;
+        out[NB * NB + t] = (r < kb) ? cmulf(w[r][NB], w[r][c]) : w[r][c];
+    }
 }
 
 // blockIdx.y == 0: rows of L21 = A21 U11^-1; blockIdx.y == 1: columns of
