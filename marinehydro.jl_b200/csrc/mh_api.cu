@@ -273,9 +273,17 @@ int mh_ctx_create(int device, mh_ctx** out)
     auto* ctx = new (std::nothrow) mh_ctx();
     if (!ctx) return set_err(nullptr, MH_ERR_OOM, "host allocation failed");
     ctx->device = device;
-    if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if ((e = cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, greatest)) != cudaSuccess ||
+        (e = cudaStreamCreateWithPriority(&ctx->side, cudaStreamNonBlocking, least)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->ev_panel, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->ev_side, cudaEventDisableTiming)) != cudaSuccess) {
+        if (ctx->stream) cudaStreamDestroy(ctx->stream);
+        if (ctx->side) cudaStreamDestroy(ctx->side);
+        if (ctx->ev_panel) cudaEventDestroy(ctx->ev_panel);
         delete ctx;
-        return set_err(nullptr, MH_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+        return set_err(nullptr, MH_ERR_CUDA, "stream/event creation: %s", cudaGetErrorString(e));
     }
     if (cublasCreate(&ctx->cublas) != CUBLAS_STATUS_SUCCESS ||
         cusolverDnCreate(&ctx->cusolver) != CUSOLVER_STATUS_SUCCESS) {
@@ -293,6 +301,7 @@ int mh_ctx_destroy(mh_ctx* ctx)
     if (!ctx) return MH_OK;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->side) cudaStreamSynchronize(ctx->side);
     for (int s = 0; s < WS_NSLOTS; ++s)
         if (ctx->ws[s]) cudaFree(ctx->ws[s]);
     if (ctx->delh_table) cudaFree(ctx->delh_table);
@@ -300,6 +309,9 @@ int mh_ctx_destroy(mh_ctx* ctx)
         if (ctx->ev[q]) cudaEventDestroy(ctx->ev[q]);
     if (ctx->cusolver) cusolverDnDestroy(ctx->cusolver);
     if (ctx->cublas) cublasDestroy(ctx->cublas);
+    if (ctx->ev_panel) cudaEventDestroy(ctx->ev_panel);
+    if (ctx->ev_side) cudaEventDestroy(ctx->ev_side);
+    if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return MH_OK;

@@ -46,7 +46,9 @@ enum Phase : int {
 
 struct mh_ctx {
     int device = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;  // every call's work (highest priority)
+    cudaStream_t side = nullptr;    // concurrent work inside a call (lowest priority)
+    cudaEvent_t ev_panel = nullptr, ev_side = nullptr;
     cublasHandle_t cublas = nullptr;
     cusolverDnHandle_t cusolver = nullptr;
     std::string err;

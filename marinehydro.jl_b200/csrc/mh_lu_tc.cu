@@ -282,7 +282,7 @@ k_lu_trsm_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
 __global__ void __launch_bounds__(128, 2)
 k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
                const unsigned char* __restrict__ Lp, const unsigned char* __restrict__ Up,
-               int64_t pstride, int* __restrict__ bad)
+               int64_t pstride, int* __restrict__ bad, int mode, int ntile)
 {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
     __shared__ uint64_t mbar[2];
@@ -292,8 +292,19 @@ k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
     const int b = blockIdx.z;
     float2* M = Ab + (int64_t)b * stride;
     const int64_t base = k0 + TC_NB;
-    const int64_t r0 = base + (int64_t)blockIdx.x * TC_TM;
-    const int64_t c0 = base + (int64_t)blockIdx.y * TC_TN;
+    // mode 0: every tile (grid ntile x ntile); 1: tile row 0 and tile column 0
+    // (grid 2 ntile - 1, the part the next panel depends on); 2: the rest
+    // (grid (ntile - 1)^2)
+    int ti = blockIdx.x, tj = blockIdx.y;
+    if (mode == 1) {
+        ti = (int)blockIdx.x < ntile ? (int)blockIdx.x : 0;
+        tj = (int)blockIdx.x < ntile ? 0 : (int)blockIdx.x - ntile + 1;
+    } else if (mode == 2) {
+        ti = blockIdx.x + 1;
+        tj = blockIdx.y + 1;
+    }
+    const int64_t r0 = base + (int64_t)ti * TC_TM;
+    const int64_t c0 = base + (int64_t)tj * TC_TN;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (warp == 0) tmem_alloc(&tmem_slot, kTmemCols);
     const uint32_t bar_ld = smem_u32(&mbar[0]), bar_mma = smem_u32(&mbar[1]);
@@ -302,8 +313,8 @@ k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
         mbar_init(&mbar[1]);
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
                      :: "r"(bar_ld), "r"(kPanelL + kPanelU) : "memory");
-        const unsigned char* srcA = Lp + (int64_t)b * pstride + (int64_t)blockIdx.x * kPanelL;
-        const unsigned char* srcB = Up + (int64_t)b * pstride + (int64_t)blockIdx.y * kPanelU;
+        const unsigned char* srcA = Lp + (int64_t)b * pstride + (int64_t)ti * kPanelL;
+        const unsigned char* srcB = Up + (int64_t)b * pstride + (int64_t)tj * kPanelU;
         constexpr uint32_t kChunk = 16384;
 #pragma unroll 1
         for (uint32_t off = 0; off < kPanelL; off += kChunk)
@@ -767,13 +778,22 @@ unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
 
 int64_t lu_dinv_stride_tc(int64_t n) { return ((n + TC_NB - 1) / TC_NB) * 2 * TC_NB * TC_NB; }
 
-int64_t lu_panel_bytes_tc(int64_t n) { return ((n + TC_TM - 1) / TC_TM) * (int64_t)(kPanelL + kPanelU); }
+// Two panel buffers per matrix: the next step's panels are written while the
+// current step's interior update still reads its own.
+int64_t lu_panel_bytes_tc(int64_t n) { return 2 * ((n + TC_TM - 1) / TC_TM) * (int64_t)(kPanelL + kPanelU); }
 
+// Blocked LU with look-ahead: per step k the main (high-priority) stream runs
+// the diagonal block, the panel TRSM and the update of the tiles the next
+// panel needs (tile row 0 and column 0), then the next diagonal block; the
+// interior tiles of step k run concurrently on the side (low-priority)
+// stream.  Step k+1's edge update waits for step k's interior; the panel
+// buffers alternate between steps so a TRSM never overwrites panels an
+// interior update still reads.
 cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int nbatch, float2* Dinv,
                          unsigned char* panels, int* bad)
 {
     cudaError_t e;
-    constexpr int kDiagThreads = 1024;
+    constexpr int kDiagThreads = 512;
     if ((e = cudaFuncSetAttribute(k_lu_diag<TC_NB, kDiagThreads>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)lu_diag_smem_bytes<TC_NB>())) != cudaSuccess)
@@ -785,25 +805,45 @@ cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int 
                                   (int)(kSmemA + kSmemA))) != cudaSuccess)
         return e;
     const int64_t dstride = lu_dinv_stride_tc(n);
-    const int64_t pstride = lu_panel_bytes_tc(n);
+    const int64_t pstride = lu_panel_bytes_tc(n) / 2;  // one buffer, per matrix
     const int64_t ntiles = (n + TC_TM - 1) / TC_TM;
-    unsigned char* Lp = panels;
-    unsigned char* Up = panels + ntiles * kPanelL;
-    for (int64_t k0 = 0; k0 < n; k0 += TC_NB) {
-        k_lu_diag<TC_NB, kDiagThreads><<<nbatch, kDiagThreads, lu_diag_smem_bytes<TC_NB>(),
-                                         ctx->stream>>>(A, n, stride, k0, Dinv, dstride, bad);
-        ctx->launches += 1;
+    cudaStream_t main_s = ctx->stream, side_s = ctx->side;
+    if ((e = cudaEventRecord(ctx->ev_side, side_s)) != cudaSuccess) return e;
+    k_lu_diag<TC_NB, kDiagThreads><<<nbatch, kDiagThreads, lu_diag_smem_bytes<TC_NB>(), main_s>>>(
+        A, n, stride, 0, Dinv, dstride, bad);
+    ctx->launches += 1;
+    int step = 0;
+    for (int64_t k0 = 0; k0 < n; k0 += TC_NB, ++step) {
         const int64_t rest = n - k0 - TC_NB;
-        if (rest > 0) {
-            const unsigned nt = cdiv(rest, TC_TM);
-            k_lu_trsm_tc<<<dim3(2 * nt, (unsigned)nbatch), 128, kSmemA + kSmemA, ctx->stream>>>(
-                A, n, stride, k0, Dinv, dstride, Lp, Up, pstride, (int)nt, bad);
-            k_lu_update_tc<<<dim3(nt, nt, (unsigned)nbatch), 128, kTcSmemBytes, ctx->stream>>>(
-                A, n, stride, k0, Lp, Up, pstride, bad);
-            ctx->launches += 2;
+        if (rest <= 0) break;
+        unsigned char* buf = panels + (int64_t)(step & 1) * pstride * nbatch;
+        unsigned char* Lp = buf;
+        unsigned char* Up = buf + ntiles * kPanelL;
+        const unsigned nt = cdiv(rest, TC_TM);
+        k_lu_trsm_tc<<<dim3(2 * nt, (unsigned)nbatch), 128, kSmemA + kSmemA, main_s>>>(
+            A, n, stride, k0, Dinv, dstride, Lp, Up, pstride, (int)nt, bad);
+        // the previous interior update is done before this step's edge update
+        if ((e = cudaStreamWaitEvent(main_s, ctx->ev_side, 0)) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(ctx->ev_panel, main_s)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(side_s, ctx->ev_panel, 0)) != cudaSuccess) return e;
+        if (nt > 1) {
+            k_lu_update_tc<<<dim3(nt - 1, nt - 1, (unsigned)nbatch), 128, kTcSmemBytes, side_s>>>(
+                A, n, stride, k0, Lp, Up, pstride, bad, 2, (int)nt);
+            ctx->launches += 1;
+        }
+        if ((e = cudaEventRecord(ctx->ev_side, side_s)) != cudaSuccess) return e;
+        k_lu_update_tc<<<dim3(2 * nt - 1, 1, (unsigned)nbatch), 128, kTcSmemBytes, main_s>>>(
+            A, n, stride, k0, Lp, Up, pstride, bad, 1, (int)nt);
+        ctx->launches += 2;
+        if (k0 + TC_NB < n) {
+            k_lu_diag<TC_NB, kDiagThreads><<<nbatch, kDiagThreads, lu_diag_smem_bytes<TC_NB>(), main_s>>>(
+                A, n, stride, k0 + TC_NB, Dinv, dstride, bad);
+            ctx->launches += 1;
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
+    // join: everything of the side stream is done before the caller continues
+    if ((e = cudaStreamWaitEvent(main_s, ctx->ev_side, 0)) != cudaSuccess) return e;
     return cudaSuccess;
 }
 
