@@ -196,6 +196,118 @@ k_adj_wave(int kind, const double* __restrict__ geom, int64_t n, int direct, con
     }
 }
 
+// Delhommeau contraction from the forward's tape: the forward pass of the
+// same call stored the dimensionless (G, G_r) of every pair and frequency
+// (S layout, 32 B each), so no table is evaluated here; G_z = G + 2/R and
+// the second derivatives come from the identities.  Otherwise as k_adj_wave:  S-bar_ij(z) = sum_q VA_iq conj(VB_jq),
+// D-bar_ij(z) = -sum_q VC_iq conj(VD_jq) (vectors [z][q][n]).
+// rowpart[colblock][kRowF][n], colpart[rowblock][kWaveF][n],
+// kpart[z][block]: deterministic partial sums.
+__global__ void __launch_bounds__(kAR)
+k_adj_delh_tape(const double* __restrict__ geom, int64_t n, int direct, const double2* __restrict__ tape,
+                const double* __restrict__ kvec, int nb, int nrhs, const double2* __restrict__ VA,
+                const double2* __restrict__ VB, const double2* __restrict__ VC, const double2* __restrict__ VD,
+                double* __restrict__ rowpart, double* __restrict__ colpart, double* __restrict__ kpart)
+{
+    extern __shared__ double ksm[];  // [4 warps][nb]
+    __shared__ Panel sp[kAC];
+    __shared__ double csm[kAR / 32][kAC][kWaveF];
+    const int64_t j0 = (int64_t)blockIdx.y * kAC;
+    stage(sp, geom, n, j0);
+    for (int t = threadIdx.x; t < (kAR / 32) * nb; t += blockDim.x) ksm[t] = 0.0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t i = (int64_t)blockIdx.x * kAR + threadIdx.x;
+    const bool live = i < n;
+    const int64_t ii = live ? i : 0;
+    const double x[3] = {geom[G_CX * n + ii], geom[G_CY * n + ii], geom[G_CZ * n + ii]};
+    const double ni[3] = {geom[G_NX * n + ii], geom[G_NY * n + ii], geom[G_NZ * n + ii]};
+    const int jend = (int)min((int64_t)kAC, n - j0);
+    const int64_t nv = n * nrhs, nn = n * n;
+    double xb[3] = {0.0, 0.0, 0.0}, nbi[3] = {0.0, 0.0, 0.0};
+    for (int jj = 0; jj < jend; ++jj) {
+        const Panel& p = sp[jj];
+        const int64_t j = j0 + jj;
+        const double* nD = direct ? p.n : ni;
+        const WaveGeom wg = wave_geom(x, p);
+        const double rho = hypot(wg.dis, wg.zs);
+        double cacc[kWaveF] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (int z = 0; z < nb; ++z) {
+            const int64_t base = (int64_t)z * nv;
+            double sr = 0.0, si = 0.0, dr = 0.0, di = 0.0;
+            for (int q = 0; q < nrhs; ++q) {
+                const double2 a = VA[base + q * n + ii], b = VB[base + q * n + j];
+                const double2 c = VC[base + q * n + ii], d = VD[base + q * n + j];
+                sr += a.x * b.x + a.y * b.y;
+                si += a.y * b.x - a.x * b.y;
+                dr -= c.x * d.x + c.y * d.y;
+                di -= c.y * d.x - c.x * d.y;
+            }
+            // cs = conj(-S-bar / 4pi), cw = conj(-D-bar / 4pi)
+            const cplx cs = mk(-kI4P * sr, kI4P * si), cw = mk(-kI4P * dr, kI4P * di);
+            double bk = 0.0;
+            if (live) {
+                WaveBar wb;
+                const double k = kvec[z];
+                const int64_t m = (int64_t)z * nn + j * n + ii;
+                const double R = k * rho;
+                const double2 g0 = tape[2 * m], g1 = tape[2 * m + 1];
+                cplx G[3];
+                G[0] = mk(g0.x, g0.y);
+                G[1] = mk(g1.x, g1.y);
+                G[2] = mk(g0.x + 2.0 / R, g0.y);
+                GDer o;
+                gder_identities(G, k * wg.dis, k * wg.zs, R, o);
+                wave_chain(o, wg, k, p.area, !direct, cs, cw, nD, wb);
+                xb[0] += wb.dx;
+                xb[1] += wb.dy;
+                xb[2] += wb.zs;
+                cacc[0] -= wb.dx;
+                cacc[1] -= wb.dy;
+                cacc[2] += wb.zs;
+                if (direct) {
+                    cacc[3] += wb.n[0];
+                    cacc[4] += wb.n[1];
+                    cacc[5] += wb.n[2];
+                } else {
+                    nbi[0] += wb.n[0];
+                    nbi[1] += wb.n[1];
+                    nbi[2] += wb.n[2];
+                }
+                cacc[6] += wb.area;
+                bk = wb.k;
+            }
+            bk = warp_sum(bk);
+            if (lane == 0) ksm[warp * nb + z] += bk;
+        }
+#pragma unroll
+        for (int f = 0; f < kWaveF; ++f) {
+            const double v = warp_sum(cacc[f]);
+            if (lane == 0) csm[warp][jj][f] = v;
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < jend * kWaveF; t += blockDim.x) {
+        const int jj = t / kWaveF, f = t % kWaveF;
+        double s = 0.0;
+        for (int w = 0; w < kAR / 32; ++w) s += csm[w][jj][f];
+        colpart[((int64_t)blockIdx.x * kWaveF + f) * n + j0 + jj] = s;
+    }
+    if (live) {
+        for (int c = 0; c < 3; ++c) {
+            rowpart[((int64_t)blockIdx.y * kRowF + c) * n + i] = xb[c];
+            rowpart[((int64_t)blockIdx.y * kRowF + 3 + c) * n + i] = nbi[c];
+        }
+    }
+    const int64_t P = (int64_t)gridDim.x * gridDim.y;
+    const int64_t blk = (int64_t)blockIdx.y * gridDim.x + blockIdx.x;
+    for (int z = threadIdx.x; z < nb; z += blockDim.x) {
+        double s = 0.0;
+        for (int w = 0; w < kAR / 32; ++w) s += ksm[w * nb + z];
+        kpart[(int64_t)z * P + blk] = s;
+    }
+}
+
 // One (pair, frequency) of the Delhommeau adjoint off the polar patch: the
 // per-point table gradient and the chain (out of line, so the polar path
 // keeps its state in registers).
@@ -875,6 +987,7 @@ struct Vjp {
     double2* CK;     // [nomega][nbeta][ndof]
     double* part;    // partial sums
     size_t part_words;
+    double2* tape;   // forward (G, G_r) per pair and frequency of the chunk, or null
     bool rankine;
     int wave_kinds[2];
     int nwave;
@@ -898,13 +1011,19 @@ int contract_pairs_wave(const Batch& bt, Vjp& vj, const double* d_k, int nb, int
     phase_begin(ctx, PH_ADJ_WAVE);
     for (int w = 0; w < vj.nwave; ++w) {
         const int kind = vj.wave_kinds[w];
-        const bool allw = kind == 2 && tab && nb >= kAdjAllwMinFreqs;
+        const bool use_tape = kind == 2 && vj.tape;
+        const bool allw = !use_tape && kind == 2 && tab && nb >= kAdjAllwMinFreqs;
         const unsigned nrb = allw ? nblk(n, kAW) : nblk(n, kAR);
         const unsigned ncb = cb;
         double* rowpart = vj.part;
         double* colpart = rowpart + (size_t)ncb * kRowF * n;
         double* kpart = colpart + (size_t)nrb * kWaveF * n;
-        if (allw) {
+        if (use_tape) {
+            const size_t smem = sizeof(double) * (kAR / 32) * nb;
+            k_adj_delh_tape<<<dim3(nrb, cb), kAR, smem, ctx->stream>>>(bt.m->geom, n, bt.direct, vj.tape, d_k, nb,
+                                                                       bt.nrhs, VA, VB, VC, VD, rowpart, colpart,
+                                                                       kpart);
+        } else if (allw) {
             const size_t smem = adj_allw_smem(nb);
             MH_CUDA_TRY(ctx, cudaFuncSetAttribute(k_adj_delh_allw, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                   (int)smem));
@@ -1180,14 +1299,23 @@ int hydro_batch_vjp(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double*
         if (!SR) return MH_ERR_OOM;
         double* DR = SR + nn;
         if ((rc = rankine_real(bt, SR, DR))) return rc;
-        const size_t per = nn * (2 * sizeof(double2) + sizeof(float2)) +
+        // the Delhommeau table term keeps a tape of (G, G_r) per pair and frequency
+        int trc = MH_OK;
+        const bool tape = (mask & MH_GF_DELHOMMEAU) && delh_table_for(ctx, mask, &trc) != nullptr;
+        if (trc) return trc;
+        const size_t per = nn * (2 * sizeof(double2) + sizeof(float2) + (tape ? 2 * sizeof(double2) : 0)) +
                            (size_t)n * nrhs * (10 * sizeof(double2) + 2 * sizeof(float2));
-        constexpr size_t kVjpBatchBytes = 16ull << 30;
+        constexpr size_t kVjpBatchBytes = 32ull << 30;
         const int64_t fit = std::min<int64_t>(1024, (int64_t)(kVjpBatchBytes / per));
         const int chunk = (int)std::max<int64_t>(1, std::min<int64_t>(nomega, fit));
         vj.part_words = part_words_needed(n, chunk);
         vj.part = (double*)ws_get(ctx, WS_PART, sizeof(double) * vj.part_words);
         if (!vj.part) return MH_ERR_OOM;
+        if (tape) {
+            vj.tape = (double2*)ws_get(ctx, WS_TAPE, sizeof(double2) * 2 * nn * (size_t)chunk);
+            if (!vj.tape) return MH_ERR_OOM;
+            bt.tape = vj.tape;
+        }
         FallbackStore fb;
         for (int64_t z0 = 0; z0 < nomega && rc == MH_OK; z0 += chunk) {
             const int nb = (int)std::min<int64_t>(chunk, nomega - z0);

@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(kRows)
 k_wave_batch(const double* __restrict__ geom, int64_t n, int direct, const double* __restrict__ tab,
              const double* __restrict__ kvec, const double* __restrict__ SR,
              const double* __restrict__ DR, double2* __restrict__ S64, double2* __restrict__ D64,
-             float2* __restrict__ Dlo)
+             float2* __restrict__ Dlo, double2* __restrict__ tape)
 {
     __shared__ Panel sp[kCols];
     const int64_t j0 = (int64_t)blockIdx.y * kCols;
@@ -106,6 +106,15 @@ k_wave_batch(const double* __restrict__ geom, int64_t n, int direct, const doubl
         wave_pair<kDelh>(x, p, k, !direct, tab, s, g);
         const double* nn = direct ? p.n : ni;
         const int64_t o = j * n + i;
+        if (kDelh && tape) {  // (G, G_r) for the adjoint of the same call
+            const double dx = x[0] - p.c[0], dy = x[1] - p.c[1], dis2 = dx * dx + dy * dy;
+            const double dis = (dis2 == 0.0) ? sqrt(dis2 + 1e-36) - 1e-18 : sqrt(dis2);
+            cplx G[3];
+            if (tab) delh_dimless_table(tab, k * dis, k * (x[2] + p.c[2]), G);
+            else delh_dimless(k * dis, k * (x[2] + p.c[2]), G);
+            tape[2 * (mat + o)] = make_double2(G[0].re, G[0].im);
+            tape[2 * (mat + o) + 1] = make_double2(G[1].re, G[1].im);
+        }
         double sr = SR[o] - kInv4Pi * s.re, si = -kInv4Pi * s.im;
         double dr = DR[o] - kInv4Pi * (nn[0] * g[0].re + nn[1] * g[1].re + nn[2] * g[2].re);
         double di = -kInv4Pi * (nn[0] * g[0].im + nn[1] * g[1].im + nn[2] * g[2].im);
@@ -131,7 +140,7 @@ __global__ void __launch_bounds__(kWT, 2)
 k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const double* __restrict__ tab,
                  const double* __restrict__ kvec, int nb, const double* __restrict__ SR,
                  const double* __restrict__ DR, double2* __restrict__ S64, double2* __restrict__ D64,
-                 float2* __restrict__ Dlo)
+                 float2* __restrict__ Dlo, double2* __restrict__ tape)
 {
     extern __shared__ double wsm[];
     double* coef = wsm;                           // 4 polar tables, NP x NP each
@@ -231,6 +240,10 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
             S64[m] = make_double2(Sr, Si);
             D64[m] = make_double2(Dr, Di);
             Dlo[m] = make_float2((float)Dr, (float)Di);
+            if (tape) {  // (G, G_r) for the adjoint of the same call
+                tape[2 * m] = make_double2(o3[0].re, o3[0].im);
+                tape[2 * m + 1] = make_double2(o3[1].re, o3[1].im);
+            }
         }
     }
 }
@@ -620,16 +633,16 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
     phase_begin(ctx, PH_WAVE);
     if (wave == MH_GF_WU)
         k_wave_batch<false><<<grid, kRows, 0, ctx->stream>>>(bt.m->geom, n, bt.direct, nullptr, d_k, SR,
-                                                            DR, S64, D64, Dlo);
+                                                            DR, S64, D64, Dlo, nullptr);
     else if (wave == MH_GF_DELHOMMEAU && tab && nb >= kAllwMinFreqs) {
         MH_CUDA_TRY(ctx, cudaFuncSetAttribute(k_wave_delh_allw,
                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)kWaveAllwSmem));
         k_wave_delh_allw<<<dim3(blocks(n, kWT), blocks(n, kCols)), kWT, kWaveAllwSmem, ctx->stream>>>(
-            bt.m->geom, n, bt.direct, tab, d_k, nb, SR, DR, S64, D64, Dlo);
+            bt.m->geom, n, bt.direct, tab, d_k, nb, SR, DR, S64, D64, Dlo, bt.tape);
     } else if (wave == MH_GF_DELHOMMEAU)
         k_wave_batch<true><<<grid, kRows, 0, ctx->stream>>>(bt.m->geom, n, bt.direct, tab, d_k, SR, DR,
-                                                           S64, D64, Dlo);
+                                                           S64, D64, Dlo, bt.tape);
     else if (wave == 0)
         k_no_wave_batch<<<dim3(blocks(nn, 256), nb), 256, 0, ctx->stream>>>(nn, SR, DR, S64, D64, Dlo);
     else
