@@ -195,54 +195,84 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
                 }
             }
         }
-        for (int z = 0; z < nb; ++z) {
-            const double k = kvec[z];
-            const double r = k * rho, zz = k * zeta;
-            const double R = k * d;
-            cplx o3[3];
-            if (polar_ok && R < kTabRPolar) {
-                const double u = 2.0 * R / kTabRPolar - 1.0;
-                double val[4];
+        // two frequencies per Clenshaw pass: each series coefficient read from
+        // shared memory feeds both recurrences
+        for (int z0 = 0; z0 < nb; z0 += 2) {
+            const int nz = (z0 + 1 < nb) ? 2 : 1;
+            double kz[2], uz[2];
+            bool pz[2];
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+                kz[t] = kvec[z0 + (t < nz ? t : 0)];
+                const double R = kz[t] * d;
+                pz[t] = t < nz && polar_ok && R < kTabRPolar;
+                uz[t] = 2.0 * R / kTabRPolar - 1.0;
+            }
+            double val[2][4];
+            if (pz[0] || pz[1]) {
+                double b1[2][4], b2[2][4];
+#pragma unroll
+                for (int t = 0; t < 2; ++t)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) b1[t][q] = b2[t][q] = 0.0;
+#pragma unroll 4
+                for (int row = kTabNP - 1; row >= 1; --row) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const double c = w[(q * kTabNP + row) * kWT + tid];
+#pragma unroll
+                        for (int t = 0; t < 2; ++t) {
+                            const double nt = fma(2.0 * uz[t], b1[t][q], c - b2[t][q]);
+                            b2[t][q] = b1[t][q];
+                            b1[t][q] = nt;
+                        }
+                    }
+                }
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    const double* wq = w + q * kTabNP * kWT + tid;
-                    double b1 = 0.0, b2 = 0.0;
+                    const double c0 = w[q * kTabNP * kWT + tid];
 #pragma unroll
-                    for (int row = kTabNP - 1; row >= 1; --row) {
-                        const double t = fma(2.0 * u, b1, wq[row * kWT] - b2);
-                        b2 = b1;
-                        b1 = t;
-                    }
-                    val[q] = fma(u, b1, wq[0] - b2);
+                    for (int t = 0; t < 2; ++t) val[t][q] = fma(uz[t], b1[t][q], c0 - b2[t][q]);
                 }
-                const double B = val[0], C = val[1], E0 = val[2], E1 = val[3];
-                const double L = log(k) + lp;
-                const double G_re = -2.0 * E0 * L + B, G_im = 2.0 * kPi * E0;
-                o3[0] = mk(G_re, G_im);
-                o3[1] = mk(2.0 * E1 * L - 2.0 * E0 * gp / k + C, -2.0 * kPi * E1);
-                o3[2] = mk(G_re + 2.0 / R, G_im);
-            } else {
-                delh_dimless_table(tab, r, zz, o3);
             }
-            double d1 = 0.0, d2 = 0.0;
-            if (fabs(r) > 1e-6) {
-                const double f = k * k / r;
-                d1 = wrt_first ? f * dx : -f * dx;
-                d2 = wrt_first ? f * dy : -f * dy;
-            }
-            const double ka = k * p.area;
-            const cplx s = ka * o3[0];
-            const cplx g0 = (ka * d1) * o3[1], g1 = (ka * d2) * o3[1], g2 = (ka * k) * o3[2];
-            const double Sr = sr - kInv4Pi * s.re, Si = -kInv4Pi * s.im;
-            const double Dr = dr - kInv4Pi * (nn3[0] * g0.re + nn3[1] * g1.re + nn3[2] * g2.re);
-            const double Di = -kInv4Pi * (nn3[0] * g0.im + nn3[1] * g1.im + nn3[2] * g2.im);
-            const int64_t m = (int64_t)z * nn + o;
-            S64[m] = make_double2(Sr, Si);
-            D64[m] = make_double2(Dr, Di);
-            Dlo[m] = make_float2((float)Dr, (float)Di);
-            if (tape) {  // (G, G_r) for the adjoint of the same call
-                tape[2 * m] = make_double2(o3[0].re, o3[0].im);
-                tape[2 * m + 1] = make_double2(o3[1].re, o3[1].im);
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+                if (t >= nz) break;
+                const int z = z0 + t;
+                const double k = kz[t];
+                const double r = k * rho, zz = k * zeta;
+                const double R = k * d;
+                cplx o3[3];
+                if (pz[t]) {
+                    const double B = val[t][0], C = val[t][1], E0 = val[t][2], E1 = val[t][3];
+                    const double L = log(k) + lp;
+                    const double G_re = -2.0 * E0 * L + B, G_im = 2.0 * kPi * E0;
+                    o3[0] = mk(G_re, G_im);
+                    o3[1] = mk(2.0 * E1 * L - 2.0 * E0 * gp / k + C, -2.0 * kPi * E1);
+                    o3[2] = mk(G_re + 2.0 / R, G_im);
+                } else {
+                    delh_dimless_table(tab, r, zz, o3);
+                }
+                double d1 = 0.0, d2 = 0.0;
+                if (fabs(r) > 1e-6) {
+                    const double f = k * k / r;
+                    d1 = wrt_first ? f * dx : -f * dx;
+                    d2 = wrt_first ? f * dy : -f * dy;
+                }
+                const double ka = k * p.area;
+                const cplx s = ka * o3[0];
+                const cplx g0 = (ka * d1) * o3[1], g1 = (ka * d2) * o3[1], g2 = (ka * k) * o3[2];
+                const double Sr = sr - kInv4Pi * s.re, Si = -kInv4Pi * s.im;
+                const double Dr = dr - kInv4Pi * (nn3[0] * g0.re + nn3[1] * g1.re + nn3[2] * g2.re);
+                const double Di = -kInv4Pi * (nn3[0] * g0.im + nn3[1] * g1.im + nn3[2] * g2.im);
+                const int64_t m = (int64_t)z * nn + o;
+                S64[m] = make_double2(Sr, Si);
+                D64[m] = make_double2(Dr, Di);
+                Dlo[m] = make_float2((float)Dr, (float)Di);
+                if (tape) {  // (G, G_r) for the adjoint of the same call
+                    tape[2 * m] = make_double2(o3[0].re, o3[0].im);
+                    tape[2 * m + 1] = make_double2(o3[1].re, o3[1].im);
+                }
             }
         }
     }
