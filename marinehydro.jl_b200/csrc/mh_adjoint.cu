@@ -336,7 +336,7 @@ constexpr int kNS = 4;   // series: B, C, E0, E1
 
 size_t adj_allw_smem(int nb)
 {
-    return sizeof(double) * ((size_t)kNS * kTabNP * kAW + (size_t)(kAW / 32) * nb + nb);
+    return sizeof(double) * ((size_t)kNS * kTabNU * kAW + (size_t)(kAW / 32) * nb + nb);
 }
 
 __global__ void __launch_bounds__(kAW, 5)
@@ -346,8 +346,8 @@ k_adj_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const do
                 double* __restrict__ rowpart, double* __restrict__ colpart, double* __restrict__ kpart)
 {
     extern __shared__ double dsm[];
-    double* w = dsm;                              // [kNS * kTabNP][kAW]
-    double* ksm = w + kNS * kTabNP * kAW;         // [kAW / 32][nb]
+    double* w = dsm;                              // [kNS * kTabNU][kAW]
+    double* ksm = w + kNS * kTabNU * kAW;         // [kAW / 32][nb]
     double* logk = ksm + (kAW / 32) * nb;         // [nb]
     __shared__ Panel sp[kAC];
     __shared__ double csm[kAW / 32][kAC][kWaveF];
@@ -380,18 +380,18 @@ k_adj_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const do
             const double v = 4.0 * atan2(wg.dis, az1) / kPi - 1.0;
 #pragma unroll 1
             for (int q = 0; q < kNS; ++q) {
-                const double* c = tab + q * kTabNP * kTabNP;
+                const double* c = tab + q * kTabPolarFn;
 #pragma unroll 1
-                for (int row = 0; row < kTabNP; ++row) {
-                    const double* cr = c + row * kTabNP;
+                for (int row = 0; row < kTabNU; ++row) {
+                    const double* cr = c + row * kTabNV;
                     double b1 = 0.0, b2 = 0.0;
 #pragma unroll
-                    for (int col = kTabNP - 1; col >= 1; --col) {
+                    for (int col = kTabNV - 1; col >= 1; --col) {
                         const double t = fma(2.0 * v, b1, __ldg(cr + col) - b2);
                         b2 = b1;
                         b1 = t;
                     }
-                    wt[(q * kTabNP + row) * kAW] = fma(v, b1, __ldg(cr) - b2);
+                    wt[(q * kTabNU + row) * kAW] = fma(v, b1, __ldg(cr) - b2);
                 }
             }
         }
@@ -428,10 +428,10 @@ k_adj_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const do
 #pragma unroll
                     for (int q = 0; q < kNS; ++q) b1[t][q] = b2[t][q] = 0.0;
 #pragma unroll 2
-                for (int row = kTabNP - 1; row >= 1; --row) {
+                for (int row = kTabNU - 1; row >= 1; --row) {
                     double cq[kNS];
 #pragma unroll
-                    for (int q = 0; q < kNS; ++q) cq[q] = wt[(q * kTabNP + row) * kAW];
+                    for (int q = 0; q < kNS; ++q) cq[q] = wt[(q * kTabNU + row) * kAW];
 #pragma unroll
                     for (int t = 0; t < kZC; ++t) {
                         const double u2 = 2.0 * uu[t];
@@ -446,7 +446,7 @@ k_adj_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const do
 #pragma unroll
                 for (int t = 0; t < kZC; ++t)
 #pragma unroll
-                    for (int q = 0; q < kNS; ++q) sv[t][q] = fma(uu[t], b1[t][q], wt[q * kTabNP * kAW] - b2[t][q]);
+                    for (int q = 0; q < kNS; ++q) sv[t][q] = fma(uu[t], b1[t][q], wt[q * kTabNU * kAW] - b2[t][q]);
             }
 #pragma unroll
             for (int t = 0; t < kZC; ++t) {

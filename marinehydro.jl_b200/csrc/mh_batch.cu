@@ -134,9 +134,12 @@ k_wave_batch(const double* __restrict__ geom, int64_t n, int direct, const doubl
 // Frequencies at which the pair leaves the polar patch use the full table.
 // Same arithmetic as wave_pair<true> up to reassociation (~1e-16).
 constexpr int kWT = 128;  // threads (rows) per CTA of k_wave_delh_allw
-constexpr size_t kWaveAllwSmem = sizeof(double) * (4 * kTabNP * kTabNP + 4 * kTabNP * kWT);
+constexpr int kAllwMaxFreqs = 128;  // frequencies per launch of k_wave_delh_allw
+// polar tables, the contracted series of every row, log k and 1/k per frequency
+constexpr size_t kWaveAllwSmem =
+    sizeof(double) * (4 * kTabPolarFn + 4 * kTabNU * kWT + 2 * kAllwMaxFreqs);
 
-__global__ void __launch_bounds__(kWT, 2)
+__global__ void __launch_bounds__(kWT, 3)
 k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const double* __restrict__ tab,
                  const double* __restrict__ kvec, int nb, const double* __restrict__ SR,
                  const double* __restrict__ DR, double2* __restrict__ S64, double2* __restrict__ D64,
@@ -144,11 +147,17 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
 {
     extern __shared__ double wsm[];
     double* coef = wsm;                           // 4 polar tables, NP x NP each
-    double* w = wsm + 4 * kTabNP * kTabNP;         // [4*NP][kWT]
+    double* w = wsm + 4 * kTabPolarFn;         // [4 * NU][kWT]
+    double* logk = w + 4 * kTabNU * kWT;           // [nb]
+    double* invk = logk + kAllwMaxFreqs;           // [nb], nb <= kAllwMaxFreqs
     __shared__ Panel sp[kCols];
     const int64_t j0 = (int64_t)blockIdx.y * kCols;
     stage_panels(sp, geom, n, j0);
-    for (int t = threadIdx.x; t < 4 * kTabNP * kTabNP; t += blockDim.x) coef[t] = tab[t];
+    for (int t = threadIdx.x; t < 4 * kTabPolarFn; t += blockDim.x) coef[t] = tab[t];
+    for (int t = threadIdx.x; t < nb; t += blockDim.x) {
+        logk[t] = log(kvec[t]);
+        invk[t] = 1.0 / kvec[t];
+    }
     __syncthreads();
     const int tid = threadIdx.x;
     const int64_t i = (int64_t)blockIdx.x * kWT + tid;
@@ -175,23 +184,24 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
         const double v = 4.0 * atan2(rho, az) / kPi - 1.0;
         const double lp = log(0.5 * (d + az));
         const double gp = rho / (d * (d + az));
+        const double inv_d = 1.0 / d, inv_rho = rho > 0.0 ? 1.0 / rho : 0.0;
         const double sr = SR[o], dr = DR[o];
         // contract alpha: w_q[row] = sum_j c_q[row][j] T_j(v)
         if (polar_ok) {
 #pragma unroll 1
             for (int q = 0; q < 4; ++q) {
-                const double* c = coef + q * kTabNP * kTabNP;
+                const double* c = coef + q * kTabPolarFn;
 #pragma unroll 1
-                for (int row = 0; row < kTabNP; ++row) {
-                    const double* cr = c + row * kTabNP;
+                for (int row = 0; row < kTabNU; ++row) {
+                    const double* cr = c + row * kTabNV;
                     double b1 = 0.0, b2 = 0.0;
 #pragma unroll
-                    for (int col = kTabNP - 1; col >= 1; --col) {
+                    for (int col = kTabNV - 1; col >= 1; --col) {
                         const double t = fma(2.0 * v, b1, cr[col] - b2);
                         b2 = b1;
                         b1 = t;
                     }
-                    w[(q * kTabNP + row) * kWT + tid] = fma(v, b1, cr[0] - b2);
+                    w[(q * kTabNU + row) * kWT + tid] = fma(v, b1, cr[0] - b2);
                 }
             }
         }
@@ -215,11 +225,11 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
                 for (int t = 0; t < 2; ++t)
 #pragma unroll
                     for (int q = 0; q < 4; ++q) b1[t][q] = b2[t][q] = 0.0;
-#pragma unroll 4
-                for (int row = kTabNP - 1; row >= 1; --row) {
+#pragma unroll
+                for (int row = kTabNU - 1; row >= 1; --row) {
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        const double c = w[(q * kTabNP + row) * kWT + tid];
+                        const double c = w[(q * kTabNU + row) * kWT + tid];
 #pragma unroll
                         for (int t = 0; t < 2; ++t) {
                             const double nt = fma(2.0 * uz[t], b1[t][q], c - b2[t][q]);
@@ -230,7 +240,7 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
                 }
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    const double c0 = w[q * kTabNP * kWT + tid];
+                    const double c0 = w[q * kTabNU * kWT + tid];
 #pragma unroll
                     for (int t = 0; t < 2; ++t) val[t][q] = fma(uz[t], b1[t][q], c0 - b2[t][q]);
                 }
@@ -239,23 +249,22 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
             for (int t = 0; t < 2; ++t) {
                 if (t >= nz) break;
                 const int z = z0 + t;
-                const double k = kz[t];
+                const double k = kz[t], ik = invk[z];
                 const double r = k * rho, zz = k * zeta;
-                const double R = k * d;
                 cplx o3[3];
                 if (pz[t]) {
                     const double B = val[t][0], C = val[t][1], E0 = val[t][2], E1 = val[t][3];
-                    const double L = log(k) + lp;
+                    const double L = logk[z] + lp;
                     const double G_re = -2.0 * E0 * L + B, G_im = 2.0 * kPi * E0;
                     o3[0] = mk(G_re, G_im);
-                    o3[1] = mk(2.0 * E1 * L - 2.0 * E0 * gp / k + C, -2.0 * kPi * E1);
-                    o3[2] = mk(G_re + 2.0 / R, G_im);
+                    o3[1] = mk(2.0 * E1 * L - 2.0 * E0 * gp * ik + C, -2.0 * kPi * E1);
+                    o3[2] = mk(G_re + 2.0 * inv_d * ik, G_im);  // 2 / R, R = k d
                 } else {
                     delh_dimless_table(tab, r, zz, o3);
                 }
                 double d1 = 0.0, d2 = 0.0;
                 if (fabs(r) > 1e-6) {
-                    const double f = k * k / r;
+                    const double f = k * inv_rho;  // k^2 / r
                     d1 = wrt_first ? f * dx : -f * dx;
                     d2 = wrt_first ? f * dy : -f * dy;
                 }
@@ -668,8 +677,14 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
         MH_CUDA_TRY(ctx, cudaFuncSetAttribute(k_wave_delh_allw,
                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)kWaveAllwSmem));
-        k_wave_delh_allw<<<dim3(blocks(n, kWT), blocks(n, kCols)), kWT, kWaveAllwSmem, ctx->stream>>>(
-            bt.m->geom, n, bt.direct, tab, d_k, nb, SR, DR, S64, D64, Dlo, bt.tape);
+        for (int z = 0; z < nb; z += kAllwMaxFreqs) {
+            const int m = std::min(kAllwMaxFreqs, nb - z);
+            const int64_t off = (int64_t)z * nn;
+            k_wave_delh_allw<<<dim3(blocks(n, kWT), blocks(n, kCols)), kWT, kWaveAllwSmem, ctx->stream>>>(
+                bt.m->geom, n, bt.direct, tab, d_k + z, m, SR, DR, S64 + off, D64 + off, Dlo + off,
+                bt.tape ? bt.tape + 2 * off : nullptr);
+            ctx->launches += (z > 0);
+        }
     } else if (wave == MH_GF_DELHOMMEAU)
         k_wave_batch<true><<<grid, kRows, 0, ctx->stream>>>(bt.m->geom, n, bt.direct, tab, d_k, SR, DR,
                                                            S64, D64, Dlo, bt.tape);

@@ -544,16 +544,16 @@ __device__ __forceinline__ void delh_exact_t(const dualn<ND>& r, const dualn<ND>
 
 // Table evaluation in the T arithmetic (the double version is
 // delh_dimless_table); derivatives are those of the Chebyshev interpolant.
-template <int N, class T>
+template <int NU, int NV, class T>
 __device__ __forceinline__ T cheb2d_t(const double* __restrict__ c, const T& u, const T& v)
 {
     T a1 = tconst<T>(0.0), a2 = tconst<T>(0.0), s0 = tconst<T>(0.0);
 #pragma unroll 1
-    for (int i = N - 1; i >= 0; --i) {
-        const double* ci = c + i * N;
+    for (int i = NU - 1; i >= 0; --i) {
+        const double* ci = c + i * NV;
         T b1 = tconst<T>(0.0), b2 = tconst<T>(0.0);
 #pragma unroll 4
-        for (int j = N - 1; j >= 1; --j) {
+        for (int j = NV - 1; j >= 1; --j) {
             T t = 2.0 * v * b1 + (__ldg(ci + j) - b2);
             b2 = b1;
             b1 = t;
@@ -585,16 +585,16 @@ __device__ __forceinline__ void delh_table_t(const double* __restrict__ tab, con
         T alpha = atan2(r, az);
         T u = R * (2.0 / kTabRPolar) - 1.0;
         T v = alpha * (4.0 / kPi) - 1.0;
-        B = cheb2d_t<kTabNP>(tab, u, v);
-        C = cheb2d_t<kTabNP>(tab + kTabNP * kTabNP, u, v);
+        B = cheb2d_t<kTabNU, kTabNV>(tab, u, v);
+        C = cheb2d_t<kTabNU, kTabNV>(tab + kTabPolarFn, u, v);
     } else if (val(r) < kTabExtent && val(az) < kTabExtent) {
         int ir = min((int)(val(r) / kTabH), kTabNCell - 1);
         int iz = min((int)(val(az) / kTabH), kTabNCell - 1);
         const double* c = tab + kTabPolarWords + (iz * kTabNCell + ir) * kTabCellWords;
         T u = (r - ir * kTabH) * (2.0 / kTabH) - 1.0;
         T v = (az - iz * kTabH) * (2.0 / kTabH) - 1.0;
-        B = cheb2d_t<kTabNC>(c, u, v);
-        C = cheb2d_t<kTabNC>(c + kTabNC * kTabNC, u, v);
+        B = cheb2d_t<kTabNC, kTabNC>(c, u, v);
+        C = cheb2d_t<kTabNC, kTabNC>(c + kTabNC * kTabNC, u, v);
     } else {
         delh_exact_t(r, z, out);
         return;

@@ -209,7 +209,7 @@ k_wave_tangent(int kind, const double* __restrict__ geom, const double* __restri
 constexpr int kTW = 64;  // rows (threads) per CTA
 constexpr int kTS = 4;   // series: B, C, E0, E1
 
-size_t tan_allw_smem(int nb) { return sizeof(double) * ((size_t)kTS * kTabNP * kTW + nb); }
+size_t tan_allw_smem(int nb) { return sizeof(double) * ((size_t)kTS * kTabNU * kTW + nb); }
 
 __global__ void __launch_bounds__(kTW, 5)
 k_wave_tangent_allw(const double* __restrict__ geom, const double* __restrict__ tgeom, int64_t n, int direct,
@@ -218,8 +218,8 @@ k_wave_tangent_allw(const double* __restrict__ geom, const double* __restrict__ 
                     const double2* __restrict__ dDR, double2* __restrict__ dS, double2* __restrict__ dD)
 {
     extern __shared__ double dsm[];
-    double* w = dsm;                    // [kTS * kTabNP][kTW]
-    double* logk = w + kTS * kTabNP * kTW;  // [nb]
+    double* w = dsm;                    // [kTS * kTabNU][kTW]
+    double* logk = w + kTS * kTabNU * kTW;  // [nb]
     __shared__ Panel sp[kGradCols], tp[kGradCols];
     const int64_t j0 = (int64_t)blockIdx.y * kGradCols;
     stage(sp, geom, n, j0);
@@ -254,18 +254,18 @@ k_wave_tangent_allw(const double* __restrict__ geom, const double* __restrict__ 
             const double v = 4.0 * atan2(wg.dis, az1) / kPi - 1.0;
 #pragma unroll 1
             for (int q = 0; q < kTS; ++q) {
-                const double* c = tab + q * kTabNP * kTabNP;
+                const double* c = tab + q * kTabPolarFn;
 #pragma unroll 1
-                for (int row = 0; row < kTabNP; ++row) {
-                    const double* cr = c + row * kTabNP;
+                for (int row = 0; row < kTabNU; ++row) {
+                    const double* cr = c + row * kTabNV;
                     double b1 = 0.0, b2 = 0.0;
 #pragma unroll
-                    for (int col = kTabNP - 1; col >= 1; --col) {
+                    for (int col = kTabNV - 1; col >= 1; --col) {
                         const double t = fma(2.0 * v, b1, __ldg(cr + col) - b2);
                         b2 = b1;
                         b1 = t;
                     }
-                    wt[(q * kTabNP + row) * kTW] = fma(v, b1, __ldg(cr) - b2);
+                    wt[(q * kTabNU + row) * kTW] = fma(v, b1, __ldg(cr) - b2);
                 }
             }
         }
@@ -280,16 +280,16 @@ k_wave_tangent_allw(const double* __restrict__ geom, const double* __restrict__ 
 #pragma unroll
                 for (int q = 0; q < kTS; ++q) b1[q] = b2[q] = 0.0;
 #pragma unroll 4
-                for (int row = kTabNP - 1; row >= 1; --row)
+                for (int row = kTabNU - 1; row >= 1; --row)
 #pragma unroll
                     for (int q = 0; q < kTS; ++q) {
-                        const double nt = fma(u2, b1[q], wt[(q * kTabNP + row) * kTW] - b2[q]);
+                        const double nt = fma(u2, b1[q], wt[(q * kTabNU + row) * kTW] - b2[q]);
                         b2[q] = b1[q];
                         b1[q] = nt;
                     }
                 double sv[kTS];
 #pragma unroll
-                for (int q = 0; q < kTS; ++q) sv[q] = fma(u, b1[q], wt[q * kTabNP * kTW] - b2[q]);
+                for (int q = 0; q < kTS; ++q) sv[q] = fma(u, b1[q], wt[q * kTabNU * kTW] - b2[q]);
                 const double L = logk[z] + lp;
                 cplx G[3];
                 const double G_re = -2.0 * sv[2] * L + sv[0], G_im = 2.0 * kPi * sv[2];

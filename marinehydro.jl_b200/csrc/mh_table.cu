@@ -139,11 +139,18 @@ int ensure_delh_table(mh_ctx* ctx)
         cudaFree(d_tab);
         return set_err(ctx, MH_ERR_CUDA, "Delhommeau table nodes: %s", cudaGetErrorString(e));
     }
-    // polar block: B, C, E0, E1
-    cheb_coeffs(kTabNP, hB.data(), tab.data());
-    cheb_coeffs(kTabNP, hC.data(), tab.data() + kTabNP * kTabNP);
-    cheb_coeffs(kTabNP, hE0.data(), tab.data() + 2 * kTabNP * kTabNP);
-    cheb_coeffs(kTabNP, hE1.data(), tab.data() + 3 * kTabNP * kTabNP);
+    // polar block: B, C, E0, E1, fitted on kTabNP x kTabNP nodes; the first
+    // kTabNU rows (degrees in R) are kept
+    {
+        std::vector<double> full((size_t)kTabNP * kTabNP);
+        const double* src[4] = {hB.data(), hC.data(), hE0.data(), hE1.data()};
+        for (int q = 0; q < 4; ++q) {
+            cheb_coeffs(kTabNP, src[q], full.data());
+            for (int i = 0; i < kTabNU; ++i)
+                for (int j = 0; j < kTabNV; ++j)
+                    tab[(size_t)q * kTabPolarFn + i * kTabNV + j] = full[(size_t)i * kTabNP + j];
+        }
+    }
     // cells
     const int np = kTabNP * kTabNP, nc = kTabNC * kTabNC;
     for (int c = 0; c < kTabNCell * kTabNCell; ++c) {

@@ -16,10 +16,14 @@
 // = e^z J0(r) of the log-moments of e^zeta E1(zeta)).  B and C are smooth
 // in polar coordinates (R, alpha = atan2(r, |z|)) near the origin and in
 // (r, |z|) away from it, so they are tabulated as 2-D Chebyshev series:
-//   - one polar patch, R in [0, 1.5), alpha in [0, pi/2], degree 20 x 20,
-//     holding B, C and also E0 = e^z J0(r), E1 = e^z J1(r) (smooth; used by
-//     the frequency-batched evaluation, which contracts the alpha direction
-//     once per panel pair and then needs only 1-D series in R per frequency);
+//   - one polar patch, R in [0, 1.5), alpha in [0, pi/2], fitted at 20 x 20
+//     nodes, holding B, C and also E0 = e^z J0(r), E1 = e^z J1(r) (smooth;
+//     used by the frequency-batched evaluation, which contracts the alpha
+//     direction once per panel pair and then needs only 1-D series in R per
+//     frequency).  The R direction keeps degree 13: the fitted coefficients
+//     of degrees 14..19 in R are at the rounding level (|c| < 1e-14 for all
+//     four functions), so they are dropped and every series in R is 6 terms
+//     shorter;
 //   - Cartesian cells of 0.5 x 0.5 over r, |z| in [0, 16), degree 12 x 12
 //     (every cell touching R < 1 lies inside the polar patch).
 // Points outside the table fall back to the adaptive quadrature.  The node
@@ -30,28 +34,32 @@
 
 namespace mh {
 
-constexpr int kTabNP = 20;          // polar patch degree (per direction)
+constexpr int kTabNP = 20;          // polar patch nodes per direction (fit)
+constexpr int kTabNU = 14;          // polar coefficients kept in R (rows)
+constexpr int kTabNV = kTabNP;      // polar coefficients kept in alpha (columns)
 constexpr int kTabNC = 12;          // Cartesian cell degree
 constexpr double kTabRPolar = 1.5;  // polar patch radius
 constexpr double kTabH = 0.5;       // Cartesian cell size
 constexpr int kTabNCell = 32;       // cells per direction -> extent 16
 constexpr double kTabExtent = kTabH * kTabNCell;
-constexpr int kTabPolarWords = 4 * kTabNP * kTabNP;            // B, C, E0, E1
+constexpr int kTabPolarFn = kTabNU * kTabNV;                   // one polar function
+constexpr int kTabPolarWords = 4 * kTabPolarFn;                 // B, C, E0, E1
 constexpr int kTabCellWords = 2 * kTabNC * kTabNC;             // B then C
 constexpr int kTabWords = kTabPolarWords + kTabNCell * kTabNCell * kTabCellWords;
 
-// sum_i sum_j c[i*N + j] T_i(u) T_j(v) by nested Clenshaw recurrences (rows
-// in v, then the row sums in u); a few registers instead of 2N basis values.
-template <int N>
+// sum_i sum_j c[i*NV + j] T_i(u) T_j(v), i < NU, j < NV, by nested Clenshaw
+// recurrences (rows in v, then the row sums in u); a few registers instead
+// of NU + NV basis values.
+template <int NU, int NV>
 __device__ __forceinline__ double cheb2d(const double* __restrict__ c, double u, double v)
 {
     double a1 = 0.0, a2 = 0.0, s0 = 0.0;
 #pragma unroll 1
-    for (int i = N - 1; i >= 0; --i) {
-        const double* ci = c + i * N;
+    for (int i = NU - 1; i >= 0; --i) {
+        const double* ci = c + i * NV;
         double b1 = 0.0, b2 = 0.0;
 #pragma unroll
-        for (int j = N - 1; j >= 1; --j) {
+        for (int j = NV - 1; j >= 1; --j) {
             const double t = fma(2.0 * v, b1, __ldg(ci + j) - b2);
             b2 = b1;
             b1 = t;
@@ -83,16 +91,16 @@ __device__ __noinline__ static void delh_dimless_table(const double* __restrict_
         double alpha = atan2(r, az);
         double u = 2.0 * R / kTabRPolar - 1.0;
         double v = 4.0 * alpha / kPi - 1.0;
-        B = cheb2d<kTabNP>(tab, u, v);
-        C = cheb2d<kTabNP>(tab + kTabNP * kTabNP, u, v);
+        B = cheb2d<kTabNU, kTabNV>(tab, u, v);
+        C = cheb2d<kTabNU, kTabNV>(tab + kTabPolarFn, u, v);
     } else if (r < kTabExtent && az < kTabExtent) {
         int ir = min((int)(r / kTabH), kTabNCell - 1);
         int iz = min((int)(az / kTabH), kTabNCell - 1);
         const double* c = tab + kTabPolarWords + (iz * kTabNCell + ir) * kTabCellWords;
         double u = 2.0 * (r - ir * kTabH) / kTabH - 1.0;
         double v = 2.0 * (az - iz * kTabH) / kTabH - 1.0;
-        B = cheb2d<kTabNC>(c, u, v);
-        C = cheb2d<kTabNC>(c + kTabNC * kTabNC, u, v);
+        B = cheb2d<kTabNC, kTabNC>(c, u, v);
+        C = cheb2d<kTabNC, kTabNC>(c + kTabNC * kTabNC, u, v);
     } else {
         delh_dimless(r, z, out);
         return;

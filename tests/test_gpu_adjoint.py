@@ -232,3 +232,19 @@ def test_vjp_frequency_batched_delhommeau(mh, gpu, direct):
     for f in ("vertices", "centers", "normals", "areas"):
         x, y = getattr(batched.mesh, f), getattr(acc, f)
         assert np.max(np.abs(x - y)) <= 1e-8 * np.max(np.abs(y)), f
+
+
+def test_vjp_frequency_batched_many_slices(mh, gpu):
+    """A chunk of 150 frequencies: the forward writes the (G, G_r) tape in
+    slices of 128 frequencies, which the adjoint reads back at the same
+    offsets; mixed against FP64."""
+    mesh = mh.mesh_hemisphere(1.0, (0, 0, 0), (6, 8))
+    dofs = [mh.translational_dofs(mesh, "Heave"), mh.translational_dofs(mesh, "Surge")]
+    om = np.linspace(0.3, 4.0, 150)
+    w = _weights(2, len(om), 1, seed=9)
+    a = _vjp(mh, gpu, mesh, om, dofs, [0.1], w, DELH, True, "mixed")
+    b = _vjp(mh, gpu, mesh, om, dofs, [0.1], w, DELH, True, "fp64")
+    assert np.max(np.abs(a.omegas - b.omegas)) <= 1e-8 * np.max(np.abs(b.omegas))
+    for f in ("vertices", "centers", "normals", "areas"):
+        x, y = getattr(a.mesh, f), getattr(b.mesh, f)
+        assert np.max(np.abs(x - y)) <= 1e-8 * np.max(np.abs(y)), f

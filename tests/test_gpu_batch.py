@@ -129,3 +129,21 @@ def test_frequency_batched_delhommeau(mh, oracle, gpu, direct):
     A64, B64, _, _, _ = mh.hydro_batch(mesh, om, dofs, [0.3], green_functions=gfs, direct=direct,
                                        precision="fp64", ctx=gpu)
     assert _rel(A, A64) < 1e-10 and _rel(B, B64) < 1e-10
+
+
+def test_frequency_batched_delhommeau_many_slices(mh, oracle, gpu):
+    """More frequencies in one chunk than one launch of the batched pass
+    takes (128): the chunk runs in frequency slices whose outputs and tape
+    land at their own offsets."""
+    mesh = mh.mesh_hemisphere(1.0, (0, 0, 0), (6, 8))
+    dofs = [mh.translational_dofs(mesh, "Heave")]
+    om = np.linspace(0.3, 4.0, 150)
+    gfs = (mh.Rankine(), mh.RankineReflected(), mh.ExactGuevelDelhommeau())
+    A, B, Fd, _, _ = mh.hydro_batch(mesh, om, dofs, [0.0], green_functions=gfs, precision="mixed",
+                                    tol=1e-12, ctx=gpu)
+    A64, B64, Fd64, _, _ = mh.hydro_batch(mesh, om, dofs, [0.0], green_functions=gfs, precision="fp64",
+                                          ctx=gpu)
+    assert _rel(A, A64) < 1e-10 and _rel(B, B64) < 1e-10 and _rel(Fd, Fd64) < 1e-10
+    sel = [0, 127, 128, 149]
+    Ao, Bo, _, _ = oracle.hydro_coefficients(mesh, om[sel], dofs, [0.0], gf_mask=DELH)
+    assert _rel(A[..., sel], Ao) < 1e-9 and _rel(B[..., sel], Bo) < 1e-9
