@@ -199,22 +199,34 @@ k_adj_wave(int kind, const double* __restrict__ geom, int64_t n, int direct, con
 // Delhommeau contraction from the forward's tape: the forward pass of the
 // same call stored the dimensionless (G, G_r) of every pair and frequency
 // (S layout, 32 B each), so no table is evaluated here; G_z = G + 2/R and
-// the second derivatives come from the identities.  Otherwise as k_adj_wave:  S-bar_ij(z) = sum_q VA_iq conj(VB_jq),
-// D-bar_ij(z) = -sum_q VC_iq conj(VD_jq) (vectors [z][q][n]).
+// the second derivatives come from the identities.  Otherwise as k_adj_wave:
+// S-bar_ij(z) = sum_q VA_iq conj(VB_jq), D-bar_ij(z) = -sum_q VC_iq conj(VD_jq)
+// (vectors [z][q][n]).  Each sweep over the frequencies takes kTJ columns
+// at once, so the row vectors VA, VC are read once per kTJ pairs and the
+// k partial sums are reduced across the warp once per kTJ pairs.
 // rowpart[colblock][kRowF][n], colpart[rowblock][kWaveF][n],
 // kpart[z][block]: deterministic partial sums.
-__global__ void __launch_bounds__(kAR)
+constexpr int kTJ = 2;
+static_assert(kAC % kTJ == 0, "column blocks split into sweeps of kTJ pairs");
+
+__global__ void __launch_bounds__(kAR, 4)
 k_adj_delh_tape(const double* __restrict__ geom, int64_t n, int direct, const double2* __restrict__ tape,
                 const double* __restrict__ kvec, int nb, int nrhs, const double2* __restrict__ VA,
                 const double2* __restrict__ VB, const double2* __restrict__ VC, const double2* __restrict__ VD,
                 double* __restrict__ rowpart, double* __restrict__ colpart, double* __restrict__ kpart)
 {
-    extern __shared__ double ksm[];  // [4 warps][nb]
+    extern __shared__ double ksm[];  // [4 warps][nb], then k and 1/k [nb] each
+    double* ksh = ksm + (kAR / 32) * nb;
+    double* iksh = ksh + nb;
     __shared__ Panel sp[kAC];
     __shared__ double csm[kAR / 32][kAC][kWaveF];
     const int64_t j0 = (int64_t)blockIdx.y * kAC;
     stage(sp, geom, n, j0);
     for (int t = threadIdx.x; t < (kAR / 32) * nb; t += blockDim.x) ksm[t] = 0.0;
+    for (int t = threadIdx.x; t < nb; t += blockDim.x) {
+        ksh[t] = kvec[t];
+        iksh[t] = 1.0 / kvec[t];
+    }
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t i = (int64_t)blockIdx.x * kAR + threadIdx.x;
@@ -225,65 +237,88 @@ k_adj_delh_tape(const double* __restrict__ geom, int64_t n, int direct, const do
     const int jend = (int)min((int64_t)kAC, n - j0);
     const int64_t nv = n * nrhs, nn = n * n;
     double xb[3] = {0.0, 0.0, 0.0}, nbi[3] = {0.0, 0.0, 0.0};
-    for (int jj = 0; jj < jend; ++jj) {
-        const Panel& p = sp[jj];
-        const int64_t j = j0 + jj;
-        const double* nD = direct ? p.n : ni;
-        const WaveGeom wg = wave_geom(x, p);
-        const double rho = hypot(wg.dis, wg.zs);
-        double cacc[kWaveF] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int jb = 0; jb < jend; jb += kTJ) {
+        WaveGeom wg[kTJ];
+        double irho[kTJ];
+        double cacc[kTJ][kWaveF];
+#pragma unroll
+        for (int u = 0; u < kTJ; ++u) {
+            const int jj = min(jb + u, jend - 1);  // a short last sweep repeats its last pair, masked below
+            wg[u] = wave_geom(x, sp[jj]);
+            irho[u] = 1.0 / hypot(wg[u].dis, wg[u].zs);
+#pragma unroll
+            for (int f = 0; f < kWaveF; ++f) cacc[u][f] = 0.0;
+        }
         for (int z = 0; z < nb; ++z) {
             const int64_t base = (int64_t)z * nv;
-            double sr = 0.0, si = 0.0, dr = 0.0, di = 0.0;
-            for (int q = 0; q < nrhs; ++q) {
-                const double2 a = VA[base + q * n + ii], b = VB[base + q * n + j];
-                const double2 c = VC[base + q * n + ii], d = VD[base + q * n + j];
-                sr += a.x * b.x + a.y * b.y;
-                si += a.y * b.x - a.x * b.y;
-                dr -= c.x * d.x + c.y * d.y;
-                di -= c.y * d.x - c.x * d.y;
-            }
-            // cs = conj(-S-bar / 4pi), cw = conj(-D-bar / 4pi)
-            const cplx cs = mk(-kI4P * sr, kI4P * si), cw = mk(-kI4P * dr, kI4P * di);
+            const double k = ksh[z], ik = iksh[z];
             double bk = 0.0;
-            if (live) {
-                WaveBar wb;
-                const double k = kvec[z];
-                const int64_t m = (int64_t)z * nn + j * n + ii;
-                const double R = k * rho;
-                const double2 g0 = tape[2 * m], g1 = tape[2 * m + 1];
-                cplx G[3];
-                G[0] = mk(g0.x, g0.y);
-                G[1] = mk(g1.x, g1.y);
-                G[2] = mk(g0.x + 2.0 / R, g0.y);
-                GDer o;
-                gder_identities(G, k * wg.dis, k * wg.zs, R, o);
-                wave_chain(o, wg, k, p.area, !direct, cs, cw, nD, wb);
-                xb[0] += wb.dx;
-                xb[1] += wb.dy;
-                xb[2] += wb.zs;
-                cacc[0] -= wb.dx;
-                cacc[1] -= wb.dy;
-                cacc[2] += wb.zs;
-                if (direct) {
-                    cacc[3] += wb.n[0];
-                    cacc[4] += wb.n[1];
-                    cacc[5] += wb.n[2];
-                } else {
-                    nbi[0] += wb.n[0];
-                    nbi[1] += wb.n[1];
-                    nbi[2] += wb.n[2];
+            double sr[kTJ], si[kTJ], dr[kTJ], di[kTJ];
+#pragma unroll
+            for (int u = 0; u < kTJ; ++u) sr[u] = si[u] = dr[u] = di[u] = 0.0;
+            for (int q = 0; q < nrhs; ++q) {
+                const double2 a = VA[base + q * n + ii], c = VC[base + q * n + ii];
+#pragma unroll
+                for (int u = 0; u < kTJ; ++u) {
+                    const int64_t j = j0 + min(jb + u, jend - 1);
+                    const double2 b = VB[base + q * n + j], d = VD[base + q * n + j];
+                    sr[u] += a.x * b.x + a.y * b.y;
+                    si[u] += a.y * b.x - a.x * b.y;
+                    dr[u] -= c.x * d.x + c.y * d.y;
+                    di[u] -= c.y * d.x - c.x * d.y;
                 }
-                cacc[6] += wb.area;
-                bk = wb.k;
+            }
+#pragma unroll
+            for (int u = 0; u < kTJ; ++u) {
+                const int jj = jb + u;
+                if (jj >= jend) break;
+                const Panel& p = sp[jj];
+                const int64_t j = j0 + jj;
+                // cs = conj(-S-bar / 4pi), cw = conj(-D-bar / 4pi)
+                const cplx cs = mk(-kI4P * sr[u], kI4P * si[u]), cw = mk(-kI4P * dr[u], kI4P * di[u]);
+                if (live) {
+                    const double* nD = direct ? p.n : ni;
+                    WaveBar wb;
+                    const int64_t m = (int64_t)z * nn + j * n + ii;
+                    const double iR = ik * irho[u];  // 1 / R, R = k rho
+                    const double2 g0 = tape[2 * m], g1 = tape[2 * m + 1];
+                    cplx G[3];
+                    G[0] = mk(g0.x, g0.y);
+                    G[1] = mk(g1.x, g1.y);
+                    G[2] = mk(g0.x + 2.0 * iR, g0.y);
+                    GDer o;
+                    gder_identities_inv(G, k * wg[u].dis, k * wg[u].zs, iR, ik * wg[u].invd, o);
+                    wave_chain(o, wg[u], k, p.area, !direct, cs, cw, nD, wb);
+                    xb[0] += wb.dx;
+                    xb[1] += wb.dy;
+                    xb[2] += wb.zs;
+                    cacc[u][0] -= wb.dx;
+                    cacc[u][1] -= wb.dy;
+                    cacc[u][2] += wb.zs;
+                    if (direct) {
+                        cacc[u][3] += wb.n[0];
+                        cacc[u][4] += wb.n[1];
+                        cacc[u][5] += wb.n[2];
+                    } else {
+                        nbi[0] += wb.n[0];
+                        nbi[1] += wb.n[1];
+                        nbi[2] += wb.n[2];
+                    }
+                    cacc[u][6] += wb.area;
+                    bk += wb.k;
+                }
             }
             bk = warp_sum(bk);
             if (lane == 0) ksm[warp * nb + z] += bk;
         }
 #pragma unroll
-        for (int f = 0; f < kWaveF; ++f) {
-            const double v = warp_sum(cacc[f]);
-            if (lane == 0) csm[warp][jj][f] = v;
+        for (int u = 0; u < kTJ; ++u) {
+            if (jb + u >= jend) break;
+#pragma unroll
+            for (int f = 0; f < kWaveF; ++f) {
+                const double v = warp_sum(cacc[u][f]);
+                if (lane == 0) csm[warp][jb + u][f] = v;
+            }
         }
     }
     __syncthreads();
@@ -1019,7 +1054,7 @@ int contract_pairs_wave(const Batch& bt, Vjp& vj, const double* d_k, int nb, int
         double* colpart = rowpart + (size_t)ncb * kRowF * n;
         double* kpart = colpart + (size_t)nrb * kWaveF * n;
         if (use_tape) {
-            const size_t smem = sizeof(double) * (kAR / 32) * nb;
+            const size_t smem = sizeof(double) * (kAR / 32 + 2) * nb;
             k_adj_delh_tape<<<dim3(nrb, cb), kAR, smem, ctx->stream>>>(bt.m->geom, n, bt.direct, vj.tape, d_k, nb,
                                                                        bt.nrhs, VA, VB, VC, VD, rowpart, colpart,
                                                                        kpart);

@@ -105,6 +105,25 @@ __device__ __forceinline__ void gder_identities(const cplx G[3], double r, doubl
     o.Gz[2] = Gzz;
 }
 
+// The same with the reciprocals 1/R and 1/r given (hoisted out of a
+// frequency loop: R = k rho, r = k dis).
+__device__ __forceinline__ void gder_identities_inv(const cplx G[3], double r, double z, double iR, double ir,
+                                                    GDer& o)
+{
+    const double iR3 = iR * iR * iR;
+    const cplx Gzz = G[2] - mk(2.0 * z * iR3, 0.0);
+    const cplx Grz = G[1] - mk(2.0 * r * iR3, 0.0);
+    const cplx Grr = (r > 1e-3) ? -(G[1] * ir) - Gzz : mk(-0.5 * Gzz.re, -0.5 * Gzz.im);
+#pragma unroll
+    for (int m = 0; m < 3; ++m) o.G[m] = G[m];
+    o.Gr[0] = G[1];
+    o.Gz[0] = G[2];
+    o.Gr[1] = Grr;
+    o.Gz[1] = Grz;
+    o.Gr[2] = Grz;
+    o.Gz[2] = Gzz;
+}
+
 // Delhommeau term and its r, z derivatives at one point: the forward's
 // value (table, or the quadrature outside it / without a table), then the
 // identities.
