@@ -110,6 +110,116 @@ k_lu_diag(float2* __restrict__ A, int64_t n, int64_t stride, int64_t k0, float2*
     }
 }
 
+// k_lu_diag for NB = 64 with the block held in registers: thread t owns row
+// r = t / 8 and the eight columns g, g + 8, ..., g + 56 (g = t % 8), so the
+// eight owners of a row are eight consecutive lanes of one warp.  Step c of
+// the elimination publishes row c of U (final) in shared memory, one
+// barrier, then the owners of column c turn it into L(:, c) and pass it to
+// the rest of their row by a warp shuffle, and every row below c updates its
+// columns right of c.  The two triangular inverses then run together, inv(L)
+// by rows ascending and inv(U) by rows descending, again one barrier per
+// step.  The block is padded with the identity, so all 64 steps run for any
+// kb <= 64 and the padding stays the identity.  Same outputs as k_lu_diag.
+constexpr int kDiag64Threads = 512;
+
+__global__ void __launch_bounds__(kDiag64Threads)
+k_lu_diag64(float2* __restrict__ A, int64_t n, int64_t stride, int64_t k0, float2* __restrict__ Dinv,
+            int64_t dstride, int* __restrict__ bad)
+{
+    constexpr int NB = 64;
+    __shared__ float2 ur[2][NB];           // row c of U, step c
+    __shared__ float2 bl[2][NB], bu[2][NB];  // rows of inv(L) and inv(U)
+    const int64_t b = blockIdx.x;
+    float2* M = A + b * stride;
+    const int kb = (int)min((int64_t)NB, n - k0);
+    const int t = threadIdx.x, r = t >> 3, g = t & 7, lane = t & 31;
+    const int row_lane0 = lane & ~7;
+    float2 a[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int c = g + 8 * m;
+        a[m] = (r < kb && c < kb) ? M[(k0 + c) * n + k0 + r] : make_float2(r == c ? 1.f : 0.f, 0.f);
+    }
+    // elimination
+#pragma unroll
+    for (int mc = 0; mc < 8; ++mc) {
+#pragma unroll
+        for (int cl = 0; cl < 8; ++cl) {
+            const int c = 8 * mc + cl, buf = c & 1;
+            if (r == c) {
+#pragma unroll
+                for (int m = 0; m < 8; ++m) ur[buf][g + 8 * m] = a[m];
+            }
+            __syncthreads();
+            const float2 piv = ur[buf][c];
+            if (r == c && g == cl && c < kb) {
+                const float mag = piv.x * piv.x + piv.y * piv.y;
+                if (!(mag > 1e-30f && mag < 3e38f)) atomicExch(bad + b, 1);
+            }
+            if (g == cl && r > c) a[mc] = cdivf(a[mc], piv);
+            const float2 l = make_float2(__shfl_sync(0xffffffffu, a[mc].x, row_lane0 | cl),
+                                         __shfl_sync(0xffffffffu, a[mc].y, row_lane0 | cl));
+            if (r > c) {
+#pragma unroll
+                for (int m = 0; m < 8; ++m)
+                    if (g + 8 * m > c) a[m] = cfms(a[m], l, ur[buf][g + 8 * m]);
+            }
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int c = g + 8 * m;
+        if (r < kb && c < kb) M[(k0 + c) * n + k0 + r] = a[m];
+    }
+    // inverses: WL = inv(L) (unit lower), WU = inv(U)
+    float2 WL[8], WU[8];
+    float2 diag = a[0];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int c = g + 8 * m;
+        WL[m] = WU[m] = make_float2(r == c ? 1.f : 0.f, 0.f);
+        if (c == r) diag = a[m];
+    }
+    const float2 ud = make_float2(__shfl_sync(0xffffffffu, diag.x, row_lane0 | (r & 7)),
+                                  __shfl_sync(0xffffffffu, diag.y, row_lane0 | (r & 7)));
+    const float2 ird = cdivf(make_float2(1.f, 0.f), ud);
+#pragma unroll
+    for (int s = 0; s < NB; ++s) {
+        const int tl = s, tu = NB - 1 - s, buf = s & 1;
+        if (r == tl) {
+#pragma unroll
+            for (int m = 0; m < 8; ++m) bl[buf][g + 8 * m] = WL[m];
+        }
+        if (r == tu) {
+#pragma unroll
+            for (int m = 0; m < 8; ++m) {
+                WU[m] = cmulf(WU[m], ird);
+                bu[buf][g + 8 * m] = WU[m];
+            }
+        }
+        __syncthreads();
+        const float2 lt = make_float2(__shfl_sync(0xffffffffu, a[tl >> 3].x, row_lane0 | (tl & 7)),
+                                      __shfl_sync(0xffffffffu, a[tl >> 3].y, row_lane0 | (tl & 7)));
+        const float2 ut = make_float2(__shfl_sync(0xffffffffu, a[tu >> 3].x, row_lane0 | (tu & 7)),
+                                      __shfl_sync(0xffffffffu, a[tu >> 3].y, row_lane0 | (tu & 7)));
+        if (r > tl) {
+#pragma unroll
+            for (int m = 0; m < 8; ++m) WL[m] = cfms(WL[m], lt, bl[buf][g + 8 * m]);
+        }
+        if (r < tu) {
+#pragma unroll
+            for (int m = 0; m < 8; ++m) WU[m] = cfms(WU[m], ut, bu[buf][g + 8 * m]);
+        }
+    }
+    float2* out = Dinv + b * dstride + (k0 / NB) * 2 * NB * NB;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int c = g + 8 * m;
+        out[c * NB + r] = WL[m];
+        out[NB * NB + c * NB + r] = WU[m];
+    }
+}
+
 // blockIdx.y == 0: rows of L21 = A21 U11^-1; blockIdx.y == 1: columns of
 // U12 = L11^-1 A12.  blockIdx.z = matrix.
 template <int NB>

@@ -1,30 +1,33 @@
 // Batched pivot-free complex LU with the trailing update on the 5th-generation
 // tensor cores (tcgen05), and block-parallel triangular solves.
 //
-// Block size NB = 64 complex.  Per step k0:
-//   k_lu_diag<64>      factor the 64 x 64 diagonal block (shared memory),
-//                      store inv(L11), inv(U11);
+// Panels of NB = 64 complex columns, trailing updates every two panels (one
+// 128-wide tile).  Per panel k0:
+//   k_lu_diag64        factor the 64 x 64 diagonal block (registers, one
+//                      barrier per elimination step), store inv(L11), inv(U11);
 //   k_lu_trsm_tc       L21 = A21 inv(U11) and U12^T = A12^T inv(L11)^T as
 //                      tcgen05 GEMMs (M=128, N=128, K=128); writes the FP32
 //                      factors into the matrix and the FP16 operand panels of
-//                      the update, pre-packed as their shared-memory images;
-//   k_lu_update_tc     A22 -= L21 U12: the two packed panels arrive by
-//                      cp.async.bulk (no register staging), eight MMAs.
+//                      the update, pre-packed as their shared-memory images
+//                      at absolute 128-row (column) tile slots;
+//   k_lu_update_tc     A22 -= sum_p L21_p U12_p over one or two panel pairs:
+//                      the packed panels arrive by cp.async.bulk (no register
+//                      staging), eight MMAs per pair accumulate in TMEM.
 //
 // The trailing update is one real GEMM per 128 x 128 complex tile of A22:
 // with A = [Re L21 | Im L21] (128 x 128) and
 //   B = [ Re U12^T  -Im U12^T ]   (rows 0..127: real part of the product)
 //       [ Im U12^T   Re U12^T ]   (rows 128..255: imaginary part)
 // D = A B^T (128 x 256) holds Re(L21 U12) in columns 0..127 and Im in
-// 128..255.  Operands are rounded to FP16 and staged by the threads in shared
-// memory in the UMMA K-major no-swizzle layout (8-row x 16-byte core
-// matrices; SBO = 128 B between 8-row groups, LBO = one K chunk of 8
-// elements); one thread issues eight tcgen05.mma.kind::f16 (M=128, N=256,
-// K=16) into a 256-column FP32 accumulator in tensor memory and commits
-// them to an mbarrier; the four warps read their 32 TMEM lanes back with
-// tcgen05.ld and subtract from A22 in FP32.  Every wait is bounded: a
-// timeout marks the matrix bad (the host then re-solves it with the FP64
-// pivoted LU) instead of spinning.
+// 128..255.  Operands are rounded to FP16 and staged in shared memory in the
+// UMMA K-major no-swizzle layout (8-row x 16-byte core matrices; SBO = 128 B
+// between 8-row groups, LBO = one K chunk of 8 elements); one thread issues
+// eight tcgen05.mma.kind::f16 (M=128, N=256, K=16) per panel pair into a
+// 256-column FP32 accumulator in tensor memory and commits them to an
+// mbarrier; the four warps read their 32 TMEM lanes back with tcgen05.ld and
+// subtract from A22 in FP32.  Every wait is bounded: a timeout marks the
+// matrix bad (the host then re-solves it with the FP64 pivoted LU) instead
+// of spinning.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -131,15 +134,16 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-// Eight K=16 MMAs over a K=128 (real) operand pair, then commit to `bar`.
+// Eight K=16 MMAs over a K=128 (real) operand pair, then commit to `bar`;
+// the first one overwrites the accumulator unless `accumulate`.
 __device__ __forceinline__ void mma_k128(uint32_t tmem, uint32_t a0, uint32_t lbo_a, uint32_t b0,
-                                        uint32_t lbo_b, uint32_t idesc, uint32_t bar)
+                                        uint32_t lbo_b, uint32_t idesc, uint32_t bar, bool accumulate = false)
 {
 #pragma unroll
     for (int s = 0; s < TC_KR / 16; ++s) {
         const uint64_t da = umma_desc(a0 + 2 * s * lbo_a, lbo_a, kSbo);
         const uint64_t db = umma_desc(b0 + 2 * s * lbo_b, lbo_b, kSbo);
-        const uint32_t acc = s > 0 ? 1u : 0u;
+        const uint32_t acc = (s > 0 || accumulate) ? 1u : 0u;
         asm volatile(
             "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
             "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
@@ -160,9 +164,13 @@ __device__ __forceinline__ uint4 pack8(const float2* v, bool imag, float sign)
 
 // Panel TRSMs of step k0 on the tensor cores.  blockIdx.x < ntile: a 128-row
 // tile of L21 = A21 inv(U11); otherwise a 128-column tile of U12 = inv(L11)
-// A12, computed as U12^T = A12^T inv(L11)^T.  blockIdx.y = matrix.  Writes the
-// FP32 factors back and the packed FP16 panels Lp (A image of the update) and
-// Up (B image: rows j = [Re U12(:, j) | -Im], rows 128 + j = [Im | Re]).
+// A12, computed as U12^T = A12^T inv(L11)^T.  blockIdx.y = matrix.  Tiles are
+// absolute (tile T holds rows, or columns, 128 T .. 128 T + 127), starting
+// at the tile of row k0 + 64; the rows (columns) of that tile above k0 + 64
+// are zero in the images and are not written back.  Writes the FP32 factors
+// back and the packed FP16 panels Lp (A image of the update) and Up (B
+// image: rows j = [Re U12(:, j) | -Im], rows 128 + j = [Im | Re]), each at
+// its absolute tile slot.
 __global__ void __launch_bounds__(128, 2)
 k_lu_trsm_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
              const float2* __restrict__ Dinv, int64_t dstride, unsigned char* __restrict__ Lp,
@@ -179,10 +187,10 @@ k_lu_trsm_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
     const float2* Li = Dinv + (int64_t)b * dstride + blk * 2 * TC_NB * TC_NB;  // column-major
     const float2* Ui = Li + TC_NB * TC_NB;
     const bool lower = (int)blockIdx.x < ntile;
-    const int tile = lower ? blockIdx.x : blockIdx.x - ntile;
-    const int64_t base = k0 + TC_NB;
-    const int64_t g = base + (int64_t)tile * TC_TM + threadIdx.x;  // row of L21 or column of U12
-    const bool ok = g < n;
+    const int64_t lo = k0 + TC_NB;  // first row of L21 / column of U12
+    const int tile = (int)(lo / TC_TM) + (lower ? (int)blockIdx.x : (int)blockIdx.x - ntile);
+    const int64_t g = (int64_t)tile * TC_TM + threadIdx.x;  // row of L21 or column of U12
+    const bool ok = g >= lo && g < n;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (warp == 0) tmem_alloc(&tmem_slot, 128);
     if (tid == 0) mbar_init(&mbar);
@@ -229,8 +237,8 @@ k_lu_trsm_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (done) {
         const int row = warp * 32 + lane;  // TMEM lane = A row = tid of the loader above
-        const int64_t gg = base + (int64_t)tile * TC_TM + row;
-        const bool okr = gg < n;
+        const int64_t gg = (int64_t)tile * TC_TM + row;
+        const bool okr = gg >= lo && gg < n;
         const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
         unsigned char* panel = lower ? Lp + (int64_t)b * pstride + (int64_t)tile * kPanelL
                                      : Up + (int64_t)b * pstride + (int64_t)tile * kPanelU;
@@ -277,12 +285,19 @@ k_lu_trsm_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
     if (warp == 0) tmem_dealloc(tmem, 128);
 }
 
-// A22 -= L21 U12 for one 128 x 128 complex tile; operands are the packed
-// panels of k_lu_trsm_tc, fetched by cp.async.bulk into shared memory.
+// A22 -= sum_p L21_p U12_p for one 128 x 128 complex tile (absolute tiles
+// ti, tj); the operands are the packed panels of k_lu_trsm_tc (npair = 1 or
+// 2 panel pairs, K = 64 complex each), fetched by cp.async.bulk into shared
+// memory one pair at a time and accumulated in tensor memory.  Only rows and
+// columns >= lo are written.
+// mode 0: tiles t0 + (bx, by) (grid ntile x ntile); mode 1: tile row t0 and
+// tile column t0 (grid 2 ntile - 1, the part the next panel depends on);
+// mode 2: tiles t0 + 1 + (bx, by) (grid (ntile - 1)^2).
 __global__ void __launch_bounds__(128, 2)
-k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
-               const unsigned char* __restrict__ Lp, const unsigned char* __restrict__ Up,
-               int64_t pstride, int* __restrict__ bad, int mode, int ntile)
+k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int t0, int ntile, int mode,
+               const unsigned char* __restrict__ Lp0, const unsigned char* __restrict__ Up0,
+               const unsigned char* __restrict__ Lp1, const unsigned char* __restrict__ Up1, int npair,
+               int64_t pstride, int64_t lo, int* __restrict__ bad)
 {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
     __shared__ uint64_t mbar[2];
@@ -291,50 +306,62 @@ k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
     unsigned char* sB = tc_smem + kSmemA;
     const int b = blockIdx.z;
     float2* M = Ab + (int64_t)b * stride;
-    const int64_t base = k0 + TC_NB;
-    // mode 0: every tile (grid ntile x ntile); 1: tile row 0 and tile column 0
-    // (grid 2 ntile - 1, the part the next panel depends on); 2: the rest
-    // (grid (ntile - 1)^2)
-    int ti = blockIdx.x, tj = blockIdx.y;
+    int ti = t0 + (int)blockIdx.x, tj = t0 + (int)blockIdx.y;
     if (mode == 1) {
-        ti = (int)blockIdx.x < ntile ? (int)blockIdx.x : 0;
-        tj = (int)blockIdx.x < ntile ? 0 : (int)blockIdx.x - ntile + 1;
+        ti = (int)blockIdx.x < ntile ? t0 + (int)blockIdx.x : t0;
+        tj = (int)blockIdx.x < ntile ? t0 : t0 + (int)blockIdx.x - ntile + 1;
     } else if (mode == 2) {
-        ti = blockIdx.x + 1;
-        tj = blockIdx.y + 1;
+        ti = t0 + 1 + (int)blockIdx.x;
+        tj = t0 + 1 + (int)blockIdx.y;
     }
-    const int64_t r0 = base + (int64_t)ti * TC_TM;
-    const int64_t c0 = base + (int64_t)tj * TC_TN;
+    const int64_t r0 = (int64_t)ti * TC_TM;
+    const int64_t c0 = (int64_t)tj * TC_TN;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (warp == 0) tmem_alloc(&tmem_slot, kTmemCols);
     const uint32_t bar_ld = smem_u32(&mbar[0]), bar_mma = smem_u32(&mbar[1]);
     if (tid == 0) {
         mbar_init(&mbar[0]);
         mbar_init(&mbar[1]);
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
-                     :: "r"(bar_ld), "r"(kPanelL + kPanelU) : "memory");
-        const unsigned char* srcA = Lp + (int64_t)b * pstride + (int64_t)ti * kPanelL;
-        const unsigned char* srcB = Up + (int64_t)b * pstride + (int64_t)tj * kPanelU;
-        constexpr uint32_t kChunk = 16384;
-#pragma unroll 1
-        for (uint32_t off = 0; off < kPanelL; off += kChunk)
-            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                         :: "r"(smem_u32(sA + off)), "l"(srcA + off), "r"(kChunk), "r"(bar_ld) : "memory");
-#pragma unroll 1
-        for (uint32_t off = 0; off < kPanelU; off += kChunk)
-            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                         :: "r"(smem_u32(sB + off)), "l"(srcB + off), "r"(kChunk), "r"(bar_ld) : "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_slot;
-    bool ok = __syncthreads_and(mbar_wait(bar_ld, 0)) != 0;
-    if (ok && tid == 0) mma_k128(tmem, smem_u32(sA), kLboA, smem_u32(sB), kLboB, kIdesc, bar_mma);
-    const bool done = ok && __syncthreads_and(mbar_wait(bar_mma, 0)) != 0;
+    bool ok = true;     // every wait so far completed
+    int pend_ld = -1;   // pair whose copies were issued and not seen complete
+    int pend_mma = -1;  // pair whose MMAs were issued and not seen complete
+#pragma unroll 1
+    for (int p = 0; p < npair && ok; ++p) {
+        if (tid == 0) {
+            const unsigned char* srcA = (p == 0 ? Lp0 : Lp1) + (int64_t)b * pstride + (int64_t)ti * kPanelL;
+            const unsigned char* srcB = (p == 0 ? Up0 : Up1) + (int64_t)b * pstride + (int64_t)tj * kPanelU;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                         :: "r"(bar_ld), "r"(kPanelL + kPanelU) : "memory");
+            constexpr uint32_t kChunk = 16384;
+#pragma unroll 1
+            for (uint32_t off = 0; off < kPanelL; off += kChunk)
+                asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                             :: "r"(smem_u32(sA + off)), "l"(srcA + off), "r"(kChunk), "r"(bar_ld) : "memory");
+#pragma unroll 1
+            for (uint32_t off = 0; off < kPanelU; off += kChunk)
+                asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                             :: "r"(smem_u32(sB + off)), "l"(srcB + off), "r"(kChunk), "r"(bar_ld) : "memory");
+        }
+        pend_ld = p;
+        ok = __syncthreads_and(mbar_wait(bar_ld, (uint32_t)(p & 1))) != 0;
+        if (!ok) break;
+        pend_ld = -1;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (tid == 0) mma_k128(tmem, smem_u32(sA), kLboA, smem_u32(sB), kLboB, kIdesc, bar_mma, p > 0);
+        // the next pair's copies overwrite the operands: wait for these MMAs
+        pend_mma = p;
+        ok = __syncthreads_and(mbar_wait(bar_mma, (uint32_t)(p & 1))) != 0;
+        if (ok) pend_mma = -1;
+    }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (done) {
+    if (ok) {
         const int64_t gi = r0 + warp * 32 + lane;
+        const bool row_ok = gi >= lo && gi < n;
         const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
 #pragma unroll 1
         for (int cc = 0; cc < TC_TN / 32; ++cc) {
@@ -342,17 +369,17 @@ k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
             tmem_ld32(lane_base + (uint32_t)(cc * 32), re);
             tmem_ld32(lane_base + (uint32_t)(TC_TN + cc * 32), im);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (gi < n) {
+            if (row_ok) {
                 float2 v[32];
 #pragma unroll
                 for (int q = 0; q < 32; ++q) {
                     const int64_t gj = c0 + cc * 32 + q;
-                    v[q] = gj < n ? M[gj * n + gi] : make_float2(0.f, 0.f);
+                    v[q] = (gj >= lo && gj < n) ? M[gj * n + gi] : make_float2(0.f, 0.f);
                 }
 #pragma unroll
                 for (int q = 0; q < 32; ++q) {
                     const int64_t gj = c0 + cc * 32 + q;
-                    if (gj < n)
+                    if (gj >= lo && gj < n)
                         M[gj * n + gi] = make_float2(v[q].x - __uint_as_float(re[q]),
                                                      v[q].y - __uint_as_float(im[q]));
                 }
@@ -360,8 +387,9 @@ k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
         }
     } else {
         if (lane == 0) atomicExch(bad + b, 2);
-        if (!ok) mbar_wait(bar_ld, 0);   // bounded: copies still in flight
-        mbar_wait(bar_mma, 0);
+        // bounded: copies or MMAs of the failed pair may still be in flight
+        if (pend_ld >= 0) mbar_wait(bar_ld, (uint32_t)(pend_ld & 1));
+        if (pend_mma >= 0) mbar_wait(bar_mma, (uint32_t)(pend_mma & 1));
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -778,26 +806,27 @@ unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
 
 int64_t lu_dinv_stride_tc(int64_t n) { return ((n + TC_NB - 1) / TC_NB) * 2 * TC_NB * TC_NB; }
 
-// Two panel buffers per matrix: the next step's panels are written while the
-// current step's interior update still reads its own.
-int64_t lu_panel_bytes_tc(int64_t n) { return 2 * ((n + TC_TM - 1) / TC_TM) * (int64_t)(kPanelL + kPanelU); }
+// Four panel buffers per matrix: both panel pairs of an outer step stay live
+// while its interior update runs, and the next outer step writes the other two.
+int64_t lu_panel_bytes_tc(int64_t n) { return 4 * ((n + TC_TM - 1) / TC_TM) * (int64_t)(kPanelL + kPanelU); }
 
-// Blocked LU with look-ahead: per step k the main (high-priority) stream runs
-// the diagonal block, the panel TRSM and the update of the tiles the next
-// panel needs (tile row 0 and column 0), then the next diagonal block; the
-// interior tiles of step k run concurrently on the side (low-priority)
-// stream.  Step k+1's edge update waits for step k's interior; the panel
-// buffers alternate between steps so a TRSM never overwrites panels an
-// interior update still reads.
+// Blocked LU in outer steps of 128 columns (two 64-column panels), with
+// look-ahead.  Outer step K0 (tile T0 = K0 / 128), on the main
+// (high-priority) stream: TRSM of panel K0, update of tile row and column
+// T0 with that panel (rows, columns >= K0 + 64), diagonal block K0 + 64,
+// TRSM of panel K0 + 64; then the trailing tiles (>= T0 + 1) are updated
+// with both panel pairs at once (K = 128 complex): tile row and column
+// T0 + 1 on the main stream, the interior concurrently on the side
+// (low-priority) stream, then the next diagonal block.  The trailing matrix
+// is read and written once per 128 columns.  An outer step's trailing update
+// waits for the previous interior; everything before it only touches tile
+// row and column T0, which that interior does not.
 cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int nbatch, float2* Dinv,
                          unsigned char* panels, int* bad)
 {
     cudaError_t e;
-    constexpr int kDiagThreads = 512;
-    if ((e = cudaFuncSetAttribute(k_lu_diag<TC_NB, kDiagThreads>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)lu_diag_smem_bytes<TC_NB>())) != cudaSuccess)
-        return e;
+    static_assert(TC_NB == 64, "the diagonal blocks are factored by k_lu_diag64");
+    static_assert(TC_TM == 2 * TC_NB && TC_TN == TC_TM, "an outer step spans one 128-wide tile");
     if ((e = cudaFuncSetAttribute(k_lu_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kTcSmemBytes)) != cudaSuccess)
         return e;
@@ -805,43 +834,58 @@ cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int 
                                   (int)(kSmemA + kSmemA))) != cudaSuccess)
         return e;
     const int64_t dstride = lu_dinv_stride_tc(n);
-    const int64_t pstride = lu_panel_bytes_tc(n) / 2;  // one buffer, per matrix
-    const int64_t ntiles = (n + TC_TM - 1) / TC_TM;
+    const int64_t pstride = lu_panel_bytes_tc(n) / 4;  // one buffer, per matrix
+    const int ntiles = (int)((n + TC_TM - 1) / TC_TM);
+    const unsigned nbz = (unsigned)nbatch;
     cudaStream_t main_s = ctx->stream, side_s = ctx->side;
     if ((e = cudaEventRecord(ctx->ev_side, side_s)) != cudaSuccess) return e;
-    k_lu_diag<TC_NB, kDiagThreads><<<nbatch, kDiagThreads, lu_diag_smem_bytes<TC_NB>(), main_s>>>(
-        A, n, stride, 0, Dinv, dstride, bad);
+    k_lu_diag64<<<nbatch, kDiag64Threads, 0, main_s>>>(A, n, stride, 0, Dinv, dstride, bad);
     ctx->launches += 1;
-    int step = 0;
-    for (int64_t k0 = 0; k0 < n; k0 += TC_NB, ++step) {
-        const int64_t rest = n - k0 - TC_NB;
-        if (rest <= 0) break;
-        unsigned char* buf = panels + (int64_t)(step & 1) * pstride * nbatch;
-        unsigned char* Lp = buf;
-        unsigned char* Up = buf + ntiles * kPanelL;
-        const unsigned nt = cdiv(rest, TC_TM);
-        k_lu_trsm_tc<<<dim3(2 * nt, (unsigned)nbatch), 128, kSmemA + kSmemA, main_s>>>(
-            A, n, stride, k0, Dinv, dstride, Lp, Up, pstride, (int)nt, bad);
-        // the previous interior update is done before this step's edge update
+    int outer = 0;
+    for (int64_t K0 = 0; K0 < n; K0 += 2 * TC_NB, ++outer) {
+        const int T0 = (int)(K0 / TC_TM);
+        unsigned char* Lp[2];
+        unsigned char* Up[2];
+        for (int s = 0; s < 2; ++s) {
+            Lp[s] = panels + (int64_t)(2 * (outer & 1) + s) * pstride * nbatch;
+            Up[s] = Lp[s] + (int64_t)ntiles * kPanelL;
+        }
+        // panel K0 and the rest of tile row / column T0
+        if (n - K0 - TC_NB <= 0) break;
+        const int nt0 = ntiles - T0;
+        k_lu_trsm_tc<<<dim3(2 * nt0, nbz), 128, kSmemA + kSmemA, main_s>>>(
+            A, n, stride, K0, Dinv, dstride, Lp[0], Up[0], pstride, nt0, bad);
+        k_lu_update_tc<<<dim3(2 * nt0 - 1, 1, nbz), 128, kTcSmemBytes, main_s>>>(
+            A, n, stride, T0, nt0, 1, Lp[0], Up[0], Lp[0], Up[0], 1, pstride, K0 + TC_NB, bad);
+        k_lu_diag64<<<nbatch, kDiag64Threads, 0, main_s>>>(A, n, stride, K0 + TC_NB, Dinv, dstride, bad);
+        ctx->launches += 3;
+        // panel K0 + 64, then the trailing tiles with both panels
+        if (n - K0 - 2 * TC_NB <= 0) break;
+        const int nt1 = ntiles - (T0 + 1);
+        k_lu_trsm_tc<<<dim3(2 * nt1, nbz), 128, kSmemA + kSmemA, main_s>>>(
+            A, n, stride, K0 + TC_NB, Dinv, dstride, Lp[1], Up[1], pstride, nt1, bad);
+        ctx->launches += 1;
+        // the previous interior update is done before this trailing update
         if ((e = cudaStreamWaitEvent(main_s, ctx->ev_side, 0)) != cudaSuccess) return e;
         if ((e = cudaEventRecord(ctx->ev_panel, main_s)) != cudaSuccess) return e;
         if ((e = cudaStreamWaitEvent(side_s, ctx->ev_panel, 0)) != cudaSuccess) return e;
-        if (nt > 1) {
-            k_lu_update_tc<<<dim3(nt - 1, nt - 1, (unsigned)nbatch), 128, kTcSmemBytes, side_s>>>(
-                A, n, stride, k0, Lp, Up, pstride, bad, 2, (int)nt);
+        if (nt1 > 1) {
+            k_lu_update_tc<<<dim3(nt1 - 1, nt1 - 1, nbz), 128, kTcSmemBytes, side_s>>>(
+                A, n, stride, T0 + 1, nt1, 2, Lp[0], Up[0], Lp[1], Up[1], 2, pstride, K0 + 2 * TC_NB, bad);
             ctx->launches += 1;
         }
         if ((e = cudaEventRecord(ctx->ev_side, side_s)) != cudaSuccess) return e;
-        k_lu_update_tc<<<dim3(2 * nt - 1, 1, (unsigned)nbatch), 128, kTcSmemBytes, main_s>>>(
-            A, n, stride, k0, Lp, Up, pstride, bad, 1, (int)nt);
-        ctx->launches += 2;
-        if (k0 + TC_NB < n) {
-            k_lu_diag<TC_NB, kDiagThreads><<<nbatch, kDiagThreads, lu_diag_smem_bytes<TC_NB>(), main_s>>>(
-                A, n, stride, k0 + TC_NB, Dinv, dstride, bad);
+        k_lu_update_tc<<<dim3(2 * nt1 - 1, 1, nbz), 128, kTcSmemBytes, main_s>>>(
+            A, n, stride, T0 + 1, nt1, 1, Lp[0], Up[0], Lp[1], Up[1], 2, pstride, K0 + 2 * TC_NB, bad);
+        ctx->launches += 1;
+        if (K0 + 2 * TC_NB < n) {
+            k_lu_diag64<<<nbatch, kDiag64Threads, 0, main_s>>>(A, n, stride, K0 + 2 * TC_NB, Dinv, dstride,
+                                                                 bad);
             ctx->launches += 1;
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
     // join: everything of the side stream is done before the caller continues
     if ((e = cudaStreamWaitEvent(main_s, ctx->ev_side, 0)) != cudaSuccess) return e;
     return cudaSuccess;

@@ -45,6 +45,20 @@ def test_lowp_lu_reconstructs(mh, gpu, backend, tol, n):
         assert err <= tol, (backend, n, b, err)
 
 
+@pytest.mark.parametrize("n", [40, 64])
+def test_tcgen05_single_block_is_fp32(mh, gpu, n):
+    """One diagonal block (n <= 64, padded with the identity when smaller):
+    no trailing update, so the tensor-core backend's factors are the FP32
+    elimination of the diagonal-block kernel."""
+    rng = np.random.default_rng(n + 1)
+    A = _bem_like(rng, 3, n)
+    LU, bad = gpu.lu_factor_lowp(A, "tcgen05")
+    assert not bad.any()
+    for b in range(A.shape[0]):
+        R = _reconstruct(LU[b].astype(np.complex128))
+        assert np.max(np.abs(R - A[b])) / np.max(np.abs(A[b])) <= 2e-6
+
+
 def test_tcgen05_factors_track_fp32(mh, gpu):
     rng = np.random.default_rng(5)
     A = _bem_like(rng, 2, 300)
