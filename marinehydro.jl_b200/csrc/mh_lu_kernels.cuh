@@ -111,15 +111,19 @@ k_lu_diag(float2* __restrict__ A, int64_t n, int64_t stride, int64_t k0, float2*
 }
 
 // k_lu_diag for NB = 64 with the block held in registers: thread t owns row
-// r = t / 8 and the eight columns g, g + 8, ..., g + 56 (g = t % 8), so the
+// r = t / 8 and the eight columns g + 8 m (g = t % 8, m = 0..7), so the
 // eight owners of a row are eight consecutive lanes of one warp.  Step c of
 // the elimination publishes row c of U (final) in shared memory, one
-// barrier, then the owners of column c turn it into L(:, c) and pass it to
-// the rest of their row by a warp shuffle, and every row below c updates its
-// columns right of c.  The two triangular inverses then run together, inv(L)
-// by rows ascending and inv(U) by rows descending, again one barrier per
-// step.  The block is padded with the identity, so all 64 steps run for any
-// kb <= 64 and the padding stays the identity.  Same outputs as k_lu_diag.
+// barrier, then the owner of column c in each row turns it into L(r, c) and
+// passes it to the rest of the row by a warp shuffle, and every row below c
+// updates its columns right of c.  The column group of step c is kept in
+// register b[0] by rotating b after every eight steps, so the step loop
+// needs no dynamic register index and only eight steps are unrolled.  The
+// two triangular inverses then run together from the factored block in
+// shared memory, inv(L) by rows ascending and inv(U) by rows descending, one
+// barrier per step.  The block is padded with the identity, so all 64 steps
+// run for any kb <= 64 and the padding stays the identity.  Same outputs as
+// k_lu_diag.
 constexpr int kDiag64Threads = 512;
 
 __global__ void __launch_bounds__(kDiag64Threads)
@@ -127,28 +131,28 @@ k_lu_diag64(float2* __restrict__ A, int64_t n, int64_t stride, int64_t k0, float
             int64_t dstride, int* __restrict__ bad)
 {
     constexpr int NB = 64;
-    __shared__ float2 ur[2][NB];           // row c of U, step c
+    __shared__ float2 f[NB][NB + 1];         // factored block
+    __shared__ float2 ur[2][NB];             // row c of U, step c
     __shared__ float2 bl[2][NB], bu[2][NB];  // rows of inv(L) and inv(U)
     const int64_t b = blockIdx.x;
     float2* M = A + b * stride;
     const int kb = (int)min((int64_t)NB, n - k0);
     const int t = threadIdx.x, r = t >> 3, g = t & 7, lane = t & 31;
     const int row_lane0 = lane & ~7;
-    float2 a[8];
+    float2 a[8];  // a[j]: column g + 8 ((j + mc) mod 8) during column group mc
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
         const int c = g + 8 * m;
         a[m] = (r < kb && c < kb) ? M[(k0 + c) * n + k0 + r] : make_float2(r == c ? 1.f : 0.f, 0.f);
     }
-    // elimination
-#pragma unroll
+#pragma unroll 1
     for (int mc = 0; mc < 8; ++mc) {
 #pragma unroll
         for (int cl = 0; cl < 8; ++cl) {
-            const int c = 8 * mc + cl, buf = c & 1;
+            const int c = 8 * mc + cl, buf = cl & 1;
             if (r == c) {
 #pragma unroll
-                for (int m = 0; m < 8; ++m) ur[buf][g + 8 * m] = a[m];
+                for (int j = 0; j < 8; ++j) ur[buf][g + 8 * ((j + mc) & 7)] = a[j];
             }
             __syncthreads();
             const float2 piv = ur[buf][c];
@@ -156,34 +160,34 @@ k_lu_diag64(float2* __restrict__ A, int64_t n, int64_t stride, int64_t k0, float
                 const float mag = piv.x * piv.x + piv.y * piv.y;
                 if (!(mag > 1e-30f && mag < 3e38f)) atomicExch(bad + b, 1);
             }
-            if (g == cl && r > c) a[mc] = cdivf(a[mc], piv);
-            const float2 l = make_float2(__shfl_sync(0xffffffffu, a[mc].x, row_lane0 | cl),
-                                         __shfl_sync(0xffffffffu, a[mc].y, row_lane0 | cl));
+            if (g == cl && r > c) a[0] = cdivf(a[0], piv);
+            const float2 l = make_float2(__shfl_sync(0xffffffffu, a[0].x, row_lane0 | cl),
+                                         __shfl_sync(0xffffffffu, a[0].y, row_lane0 | cl));
             if (r > c) {
+                if (g > cl) a[0] = cfms(a[0], l, ur[buf][g + 8 * mc]);
 #pragma unroll
-                for (int m = 0; m < 8; ++m)
-                    if (g + 8 * m > c) a[m] = cfms(a[m], l, ur[buf][g + 8 * m]);
+                for (int j = 1; j < 8; ++j)
+                    if (j < 8 - mc) a[j] = cfms(a[j], l, ur[buf][g + 8 * (j + mc)]);
             }
         }
+        const float2 a0 = a[0];
+#pragma unroll
+        for (int j = 0; j < 7; ++j) a[j] = a[j + 1];
+        a[7] = a0;
     }
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
         const int c = g + 8 * m;
+        f[r][c] = a[m];
         if (r < kb && c < kb) M[(k0 + c) * n + k0 + r] = a[m];
     }
+    __syncthreads();
     // inverses: WL = inv(L) (unit lower), WU = inv(U)
     float2 WL[8], WU[8];
-    float2 diag = a[0];
 #pragma unroll
-    for (int m = 0; m < 8; ++m) {
-        const int c = g + 8 * m;
-        WL[m] = WU[m] = make_float2(r == c ? 1.f : 0.f, 0.f);
-        if (c == r) diag = a[m];
-    }
-    const float2 ud = make_float2(__shfl_sync(0xffffffffu, diag.x, row_lane0 | (r & 7)),
-                                  __shfl_sync(0xffffffffu, diag.y, row_lane0 | (r & 7)));
-    const float2 ird = cdivf(make_float2(1.f, 0.f), ud);
-#pragma unroll
+    for (int m = 0; m < 8; ++m) WL[m] = WU[m] = make_float2(r == g + 8 * m ? 1.f : 0.f, 0.f);
+    const float2 ird = cdivf(make_float2(1.f, 0.f), f[r][r]);
+#pragma unroll 1
     for (int s = 0; s < NB; ++s) {
         const int tl = s, tu = NB - 1 - s, buf = s & 1;
         if (r == tl) {
@@ -198,15 +202,13 @@ k_lu_diag64(float2* __restrict__ A, int64_t n, int64_t stride, int64_t k0, float
             }
         }
         __syncthreads();
-        const float2 lt = make_float2(__shfl_sync(0xffffffffu, a[tl >> 3].x, row_lane0 | (tl & 7)),
-                                      __shfl_sync(0xffffffffu, a[tl >> 3].y, row_lane0 | (tl & 7)));
-        const float2 ut = make_float2(__shfl_sync(0xffffffffu, a[tu >> 3].x, row_lane0 | (tu & 7)),
-                                      __shfl_sync(0xffffffffu, a[tu >> 3].y, row_lane0 | (tu & 7)));
         if (r > tl) {
+            const float2 lt = f[r][tl];
 #pragma unroll
             for (int m = 0; m < 8; ++m) WL[m] = cfms(WL[m], lt, bl[buf][g + 8 * m]);
         }
         if (r < tu) {
+            const float2 ut = f[r][tu];
 #pragma unroll
             for (int m = 0; m < 8; ++m) WU[m] = cfms(WU[m], ut, bu[buf][g + 8 * m]);
         }
