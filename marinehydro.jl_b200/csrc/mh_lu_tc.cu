@@ -195,32 +195,56 @@ k_lu_trsm_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
     if (warp == 0) tmem_alloc(&tmem_slot, 128);
     if (tid == 0) mbar_init(&mbar);
     // A operand: row tid = A21(g, :) or A12(:, g)^T, 64 complex -> Re chunks 0..7, Im 8..15
-#pragma unroll 1
-    for (int c = 0; c < 8; ++c) {
-        float2 v[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const int64_t t = k0 + 8 * c + q;
-            v[q] = !ok ? make_float2(0.f, 0.f) : (lower ? M[t * n + g] : M[g * n + t]);
-        }
-        *reinterpret_cast<uint4*>(sA + core_off(tid, c, TC_TM)) = pack8(v, false, 1.f);
-        *reinterpret_cast<uint4*>(sA + core_off(tid, 8 + c, TC_TM)) = pack8(v, true, 1.f);
-    }
-    // B operand (N = 128): rows r < 64 give the real part of the product,
-    // rows 64 + r the imaginary part.  Complex row r of B is column r of
-    // inv(U11) (L21) or row r of inv(L11) (U12).
-    {
-        const int r = tid & 63;
-        const bool im_row = tid >= 64;
-#pragma unroll 1
+    if (lower) {  // A21 is column-major: consecutive rows g are consecutive lanes
+#pragma unroll 2
         for (int c = 0; c < 8; ++c) {
             float2 v[8];
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
-                const int t = 8 * c + q;
-                v[q] = lower ? Ui[r * TC_NB + t] : Li[t * TC_NB + r];
+                const int64_t t = k0 + 8 * c + q;
+                v[q] = ok ? M[t * n + g] : make_float2(0.f, 0.f);
             }
-            // rows r: [Re | -Im], rows 64 + r: [Im | Re]
+            *reinterpret_cast<uint4*>(sA + core_off(tid, c, TC_TM)) = pack8(v, false, 1.f);
+            *reinterpret_cast<uint4*>(sA + core_off(tid, 8 + c, TC_TM)) = pack8(v, true, 1.f);
+        }
+    } else {  // a column of A12 is contiguous: one warp reads it, lane l holds t = 2l, 2l + 1
+        const int cpos = (2 * lane) & 7, cc = (2 * lane) >> 3;
+#pragma unroll 4
+        for (int i = 0; i < 32; ++i) {
+            const int row = warp * 32 + i;
+            const int64_t gc = (int64_t)tile * TC_TM + row;
+            float2 v0 = make_float2(0.f, 0.f), v1 = v0;
+            if (gc >= lo && gc < n) {
+                v0 = M[gc * n + k0 + 2 * lane];
+                v1 = M[gc * n + k0 + 2 * lane + 1];
+            }
+            *reinterpret_cast<uint32_t*>(sA + core_off(row, cc, TC_TM) + 2 * cpos) = pack_h2(v0.x, v1.x);
+            *reinterpret_cast<uint32_t*>(sA + core_off(row, 8 + cc, TC_TM) + 2 * cpos) = pack_h2(v0.y, v1.y);
+        }
+    }
+    // B operand (N = 128): rows r < 64 give the real part of the product,
+    // rows 64 + r the imaginary part: rows r = [Re | -Im], rows 64 + r =
+    // [Im | Re] of complex row r, which is column r of inv(U11) (L21) or row
+    // r of inv(L11) (U12).
+    if (lower) {  // column r of inv(U11) is contiguous: one warp per r, lane l holds t = 2l, 2l + 1
+        const int cpos = (2 * lane) & 7, cc = (2 * lane) >> 3;
+#pragma unroll 4
+        for (int i = 0; i < 16; ++i) {
+            const int r = warp * 16 + i;
+            const float2 v0 = Ui[r * TC_NB + 2 * lane], v1 = Ui[r * TC_NB + 2 * lane + 1];
+            *reinterpret_cast<uint32_t*>(sB + core_off(r, cc, 128) + 2 * cpos) = pack_h2(v0.x, v1.x);
+            *reinterpret_cast<uint32_t*>(sB + core_off(r, 8 + cc, 128) + 2 * cpos) = pack_h2(-v0.y, -v1.y);
+            *reinterpret_cast<uint32_t*>(sB + core_off(64 + r, cc, 128) + 2 * cpos) = pack_h2(v0.y, v1.y);
+            *reinterpret_cast<uint32_t*>(sB + core_off(64 + r, 8 + cc, 128) + 2 * cpos) = pack_h2(v0.x, v1.x);
+        }
+    } else {  // row r of inv(L11): consecutive r are consecutive lanes
+        const int r = tid & 63;
+        const bool im_row = tid >= 64;
+#pragma unroll 2
+        for (int c = 0; c < 8; ++c) {
+            float2 v[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) v[q] = Li[(8 * c + q) * TC_NB + r];
             *reinterpret_cast<uint4*>(sB + core_off(tid, c, 128)) = pack8(v, im_row, 1.f);
             *reinterpret_cast<uint4*>(sB + core_off(tid, 8 + c, 128)) =
                 im_row ? pack8(v, false, 1.f) : pack8(v, true, -1.f);
@@ -253,13 +277,24 @@ k_lu_trsm_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
             for (int q = 0; q < 32; ++q)
                 v[q] = okr ? make_float2(__uint_as_float(re[q]), __uint_as_float(im[q]))
                            : make_float2(0.f, 0.f);
-            if (okr) {
+            if (lower) {  // rows gg of L21: consecutive lanes, coalesced per column t
+                if (okr) {
 #pragma unroll 8
-                for (int q = 0; q < 32; ++q) {
-                    const int64_t t = k0 + half * 32 + q;
-                    if (lower) M[t * n + gg] = v[q];
-                    else M[gg * n + t] = v[q];
+                    for (int q = 0; q < 32; ++q) M[(k0 + half * 32 + q) * n + gg] = v[q];
                 }
+            } else {  // columns gg of U12: transposed through shared memory (the operands are
+                      // consumed), then one warp writes 32 contiguous entries of a column
+                auto st = reinterpret_cast<float2 (*)[33]>(tc_smem);
+#pragma unroll
+                for (int q = 0; q < 32; ++q) st[row][q] = v[q];
+                __syncthreads();
+#pragma unroll 4
+                for (int i = 0; i < 32; ++i) {
+                    const int rr = warp * 32 + i;
+                    const int64_t gc = (int64_t)tile * TC_TM + rr;
+                    if (gc >= lo && gc < n) M[gc * n + k0 + half * 32 + lane] = st[rr][lane];
+                }
+                __syncthreads();
             }
 #pragma unroll
             for (int c4 = 0; c4 < 4; ++c4) {
