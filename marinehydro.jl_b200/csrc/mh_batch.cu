@@ -415,8 +415,8 @@ __global__ void k_add_f32(double2* __restrict__ x, const float2* __restrict__ d,
 // residuals, S b, S^H lambda), bandwidth-bound reads of the n x n matrices
 // (column-major, nb of them, n*n apart), nrhs <= kMaxRhs:
 // k_resid_n: R = beta B + alpha A X, one thread per row i, coalesced down the
-// columns; k_resid_c: R = beta B + alpha A^H X, one warp per output j reading
-// column j.  B may be R (read before written) or null when beta = 0.
+// columns; k_resid_c: R = beta B + alpha A^H X, one warp per JW outputs j
+// reading columns j (each x entry loaded once for the JW columns).  B may be R (read before written) or null when beta = 0.
 // Q >= nrhs: accumulators per thread (4, 8 or 16, picked by the launcher).
 template <int Q>
 __global__ void __launch_bounds__(256)
@@ -451,44 +451,56 @@ k_resid_n(const double2* __restrict__ A, const double2* __restrict__ X, const do
         }
 }
 
-template <int Q>
-__global__ void __launch_bounds__(256)
+template <int Q, int JW>
+__global__ void __launch_bounds__(256, 2)
 k_resid_c(const double2* __restrict__ A, const double2* __restrict__ X, const double2* B, double2* R, int64_t n,
           int nrhs, double alpha, double beta)
 {
     const int lane = threadIdx.x & 31;
-    const int64_t j = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int64_t j0 = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * JW;
     const int64_t b = blockIdx.y;
-    if (j >= n) return;  // whole warps leave together
-    const double2* col = A + b * n * n + j * n;
+    if (j0 >= n) return;  // whole warps leave together
+    const double2* M = A + b * n * n;
     const double2* x = X + b * n * nrhs;
-    double ar[Q], ai[Q];
+    int64_t jc[JW];  // columns of this warp (the last one repeated past n, not stored)
 #pragma unroll
-    for (int q = 0; q < Q; ++q) ar[q] = ai[q] = 0.0;
-#pragma unroll 4
+    for (int u = 0; u < JW; ++u) jc[u] = min(j0 + u, n - 1);
+    double ar[JW][Q], ai[JW][Q];
+#pragma unroll
+    for (int u = 0; u < JW; ++u)
+#pragma unroll
+        for (int q = 0; q < Q; ++q) ar[u][q] = ai[u][q] = 0.0;
+#pragma unroll 2
     for (int64_t i = lane; i < n; i += 32) {
-        const double2 m = col[i];  // conj(m) * x
+        double2 m[JW];
+#pragma unroll
+        for (int u = 0; u < JW; ++u) m[u] = M[jc[u] * n + i];
 #pragma unroll
         for (int q = 0; q < Q; ++q)
-            if (q < nrhs) {
+            if (q < nrhs) {  // conj(m) * x, each x entry read once for JW columns
                 const double2 v = __ldg(x + (int64_t)q * n + i);
-                ar[q] = fma(m.x, v.x, fma(m.y, v.y, ar[q]));
-                ai[q] = fma(m.x, v.y, fma(-m.y, v.x, ai[q]));
+#pragma unroll
+                for (int u = 0; u < JW; ++u) {
+                    ar[u][q] = fma(m[u].x, v.x, fma(m[u].y, v.y, ar[u][q]));
+                    ai[u][q] = fma(m[u].x, v.y, fma(-m[u].y, v.x, ai[u][q]));
+                }
             }
     }
 #pragma unroll
-    for (int q = 0; q < Q; ++q)
-        if (q < nrhs) {
-            for (int off = 16; off > 0; off >>= 1) {
-                ar[q] += __shfl_down_sync(0xffffffffu, ar[q], off);
-                ai[q] += __shfl_down_sync(0xffffffffu, ai[q], off);
+    for (int u = 0; u < JW; ++u)
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+            if (q < nrhs) {
+                for (int off = 16; off > 0; off >>= 1) {
+                    ar[u][q] += __shfl_down_sync(0xffffffffu, ar[u][q], off);
+                    ai[u][q] += __shfl_down_sync(0xffffffffu, ai[u][q], off);
+                }
+                if (lane == 0 && j0 + u < n) {
+                    const int64_t o = b * n * nrhs + (int64_t)q * n + j0 + u;
+                    const double2 bo = B ? B[o] : make_double2(0.0, 0.0);
+                    R[o] = make_double2(beta * bo.x + alpha * ar[u][q], beta * bo.y + alpha * ai[u][q]);
+                }
             }
-            if (lane == 0) {
-                const int64_t o = b * n * nrhs + (int64_t)q * n + j;
-                const double2 bo = B ? B[o] : make_double2(0.0, 0.0);
-                R[o] = make_double2(beta * bo.x + alpha * ar[q], beta * bo.y + alpha * ai[q]);
-            }
-        }
 }
 
 // Per (frequency z = blockIdx.x): max over right-hand sides of
@@ -890,11 +902,19 @@ cudaError_t launch_gemv(mh_ctx* ctx, bool conj_trans, const double2* A, int64_t 
 {
     if (nrhs < 1 || nrhs > kMaxRhs) return cudaErrorInvalidValue;
     if (beta == 0.0) B = nullptr;
-    const dim3 gc(blocks(n, 8), (unsigned)nb), gn(blocks(n, 256), (unsigned)nb);
-    if (conj_trans) {
-        if (nrhs <= 4) k_resid_c<4><<<gc, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta);
-        else if (nrhs <= 8) k_resid_c<8><<<gc, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta);
-        else k_resid_c<kMaxRhs><<<gc, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta);
+    const dim3 gn(blocks(n, 256), (unsigned)nb);
+    if (conj_trans) {  // 8 warps per CTA, JW columns per warp
+        const dim3 g4(blocks(n, 32), (unsigned)nb);
+        if (nrhs == 1) k_resid_c<1, 4><<<g4, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta);
+        else if (nrhs == 2) k_resid_c<2, 4><<<g4, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta);
+        else if (nrhs == 3) k_resid_c<3, 4><<<g4, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta);
+        else if (nrhs == 4) k_resid_c<4, 4><<<g4, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta);
+        else if (nrhs <= 8)
+            k_resid_c<8, 2><<<dim3(blocks(n, 16), (unsigned)nb), 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha,
+                                                                                      beta);
+        else
+            k_resid_c<kMaxRhs, 1><<<dim3(blocks(n, 8), (unsigned)nb), 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs,
+                                                                                           alpha, beta);
     } else {
         if (nrhs <= 4) k_resid_n<4><<<gn, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta);
         else if (nrhs <= 8) k_resid_n<8><<<gn, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta);
