@@ -126,6 +126,16 @@ int mh_ctx_set_lu_backend(mh_ctx* ctx, int backend);
 int mh_lu_factor_lowp(mh_ctx* ctx, int backend, int64_t n, int64_t nbatch, const double* A_host,
                       float* LU_host, int* bad_host);
 
+/* Factors like mh_lu_factor_lowp, then solves op(L U) X = B with those
+ * low-precision factors as one step of the mixed refinement does (op = the
+ * identity, or the conjugate transpose when conj_trans != 0).  B_host and
+ * X_host are nbatch x nrhs x n complex128 (right-hand sides contiguous, 1 <=
+ * nrhs <= 16); the solve runs in FP32, X is returned widened to FP64.  Test
+ * and diagnostic hook of the substitution that replaces LAPACK's getrs
+ * (src/matrix_assembly.jl:105-133). */
+int mh_lu_solve_lowp(mh_ctx* ctx, int backend, int64_t n, int64_t nbatch, const double* A_host, int64_t nrhs,
+                     int conj_trans, const double* B_host, double* X_host);
+
 /* Dimensionless wave term at n points (r[i], z[i]), z < 0, on the device:
  * out[6*i .. 6*i+5] = (G, dG/dr, dG/dz) as (re, im) pairs.  `which` is
  * MH_GF_WU (wu.jl:19-30) or MH_GF_DELHOMMEAU (exact_Guevel_Delhommeau.jl:15-59

@@ -75,6 +75,8 @@ SIGNATURES = {
     "mh_lu_factor_lowp": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int64, ctypes.c_int64, _D,
                                          ctypes.POINTER(ctypes.c_float),
                                          ctypes.POINTER(ctypes.c_int)]),
+    "mh_lu_solve_lowp": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int64, ctypes.c_int64, _D, ctypes.c_int64,
+                                        ctypes.c_int, _D, _D]),
     "mh_ctx_set_profiling": (ctypes.c_int, [_P, ctypes.c_int]),
     "mh_ctx_phase_times": (ctypes.c_int, [_P, ctypes.c_int, _D, _I64]),
     "mh_wave_term": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_int64, _D, _D, _D]),
@@ -218,6 +220,23 @@ class Context:
                                       LU.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
                                       bad.ctypes.data_as(ctypes.POINTER(ctypes.c_int))), self._h)
         return np.transpose(LU, (0, 2, 1)), bad
+
+    def lu_solve_lowp(self, A, B, backend: str = "tcgen05", conj_trans: bool = False):
+        """Low-precision LU of A (nbatch, n, n), then op(L U) X = B with those
+        factors (B: (nbatch, n, nrhs)); returns X as complex128."""
+        A = np.asarray(A, dtype=np.complex128)
+        B = np.asarray(B, dtype=np.complex128)
+        if A.ndim == 2:
+            A, B = A[None], B[None]
+        nb, n, _ = A.shape
+        nrhs = B.shape[2]
+        Af = np.ascontiguousarray(np.transpose(A, (0, 2, 1)))
+        Bf = np.ascontiguousarray(np.transpose(B, (0, 2, 1)))  # right-hand sides contiguous
+        X = np.empty_like(Bf)
+        code = {"simt": MH_LU_SIMT_F32, "tcgen05": MH_LU_TCGEN05_F16}[backend]
+        check(lib().mh_lu_solve_lowp(self._h, code, n, nb, dptr(Af), nrhs, int(conj_trans), dptr(Bf), dptr(X)),
+              self._h)
+        return np.transpose(X, (0, 2, 1))
 
     def stream(self) -> int:
         """The ctx's cudaStream_t as an integer handle."""

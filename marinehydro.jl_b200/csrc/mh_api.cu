@@ -421,6 +421,47 @@ int mh_lu_factor_lowp(mh_ctx* ctx, int backend, int64_t n, int64_t nbatch, const
     return sync_status(ctx, "low-precision LU");
 }
 
+int mh_lu_solve_lowp(mh_ctx* ctx, int backend, int64_t n, int64_t nbatch, const double* A_host, int64_t nrhs,
+                     int conj_trans, const double* B_host, double* X_host)
+{
+    int rc;
+    if ((rc = check_ctx(ctx))) return rc;
+    if (backend != MH_LU_SIMT_F32 && backend != MH_LU_TCGEN05_F16)
+        return set_err(ctx, MH_ERR_ARG, "unknown LU backend %d", backend);
+    if (n < 1 || nbatch < 1 || nrhs < 1 || nrhs > kMaxRhs || !A_host || !B_host || !X_host)
+        return set_err(ctx, MH_ERR_ARG, "bad arguments to mh_lu_solve_lowp");
+    const size_t nn = (size_t)n * (size_t)n, cnt = nn * (size_t)nbatch;
+    const size_t nv = (size_t)n * (size_t)nrhs, vcnt = nv * (size_t)nbatch;
+    auto* d64 = (double2*)ws_get(ctx, WS_D, sizeof(double2) * cnt);
+    auto* lo = (float2*)ws_get(ctx, WS_LO, sizeof(float2) * cnt);
+    const int64_t dst = backend == MH_LU_TCGEN05_F16 ? mh::lu_dinv_stride_tc(n) : mh::lu_dinv_stride(n);
+    auto* dinv = (float2*)ws_get(ctx, WS_DINV, sizeof(float2) * (size_t)dst * (size_t)nbatch);
+    auto* bad = (int*)ws_get(ctx, WS_MISC, sizeof(int) * (size_t)nbatch);
+    auto* v64 = (double2*)ws_get(ctx, WS_RHS, sizeof(double2) * vcnt);
+    auto* v32 = (float2*)ws_get(ctx, WS_TMP32, sizeof(float2) * vcnt);
+    if (!d64 || !lo || !dinv || !bad || !v64 || !v32) return MH_ERR_OOM;
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(d64, A_host, sizeof(double2) * cnt, cudaMemcpyHostToDevice,
+                                     ctx->stream));
+    MH_CUDA_TRY(ctx, mh::launch_to_f32(ctx, d64, lo, (int64_t)cnt));
+    MH_CUDA_TRY(ctx, cudaMemsetAsync(bad, 0, sizeof(int) * (size_t)nbatch, ctx->stream));
+    if (backend == MH_LU_TCGEN05_F16) {
+        auto* panels = (unsigned char*)ws_get(ctx, WS_PANEL,
+                                              (size_t)mh::lu_panel_bytes_tc(n) * (size_t)nbatch);
+        if (!panels) return MH_ERR_OOM;
+        MH_CUDA_TRY(ctx, mh::launch_lu_tc(ctx, lo, n, (int64_t)nn, (int)nbatch, dinv, panels, bad));
+    }
+    else
+        MH_CUDA_TRY(ctx, mh::launch_lu_f32(ctx, lo, n, (int64_t)nn, (int)nbatch, dinv, bad));
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(v64, B_host, sizeof(double2) * vcnt, cudaMemcpyHostToDevice, ctx->stream));
+    MH_CUDA_TRY(ctx, mh::launch_to_f32(ctx, v64, v32, (int64_t)vcnt));
+    MH_CUDA_TRY(ctx, mh::launch_lu_solve_persist(ctx, backend, conj_trans != 0, lo, n, (int64_t)nn, (int)nbatch,
+                                                 dinv, v32, (int64_t)nv, (int)nrhs));
+    MH_CUDA_TRY(ctx, cudaMemsetAsync(v64, 0, sizeof(double2) * vcnt, ctx->stream));
+    MH_CUDA_TRY(ctx, mh::launch_add_f32(ctx, v64, v32, (int64_t)vcnt));
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(X_host, v64, sizeof(double2) * vcnt, cudaMemcpyDeviceToHost, ctx->stream));
+    return sync_status(ctx, "low-precision solve");
+}
+
 int mh_wave_term(mh_ctx* ctx, uint32_t which, int64_t n, const double* r, const double* z,
                  double* out)
 {

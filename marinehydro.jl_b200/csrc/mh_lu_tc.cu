@@ -837,6 +837,249 @@ k_lu_solve_persist(const float2* __restrict__ A, int64_t n, int64_t stride, cons
 
 unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
 
+// ---------------------------------------------------------------------------
+// triangular solves with the block-64 factors: flag-synchronised substitution
+// ---------------------------------------------------------------------------
+//
+// One cluster of kFsCluster CTAs per matrix; row block i belongs to CTA
+// i mod kFsCluster, which applies to x_i every off-diagonal tile product
+// T_ik y_k, in the triangle's order of k, and solves y_i = inv(T_ii) x_i.
+// Instead of a barrier after every block, each solved block is published:
+// its owner writes y_i over x_i in global memory and then releases a flag
+// (per matrix, triangle and block; zeroed before the launch), and the other
+// CTAs acquire the flag before reading y_i (from L2, bypassing L1).  The
+// owner of the next block in the triangle's order applies the new y_k to
+// its block first, solves and publishes it, and only then applies y_k to
+// its other blocks, so the sequential chain per block is one 64 x 64 tile
+// product, one 64 x 64 inverse product and one flag hand-off, while the
+// bulk of the tile products of every CTA overlaps with it.  The blocks of
+// one matrix only wait on blocks of the same matrix (same cluster, whose
+// CTAs are co-scheduled), and every wait is bounded: a wait that runs out
+// records the matrix in `bad`, and the CTA stops waiting (its result is
+// then garbage, which the FP64 residual of the refinement rejects).
+//
+// Tile products: thread (r = tid / 4, tq = tid % 4) holds the 16 entries
+// (r, t = 4 j + tq) of a tile in registers, and the four threads of a row
+// reduce by shuffles.  kCT selects the
+// conjugate-transposed factors: triangle 0 is U^H (tile (i, k) =
+// conj(U_ki)^T), triangle 1 is L^H.
+constexpr int kFsThreads = 256;
+constexpr int kFsCluster = 4;
+constexpr int kFsLanes = 4;              // threads per tile row
+constexpr int kFsPer = 64 / kFsLanes;    // tile entries per thread
+constexpr int kFsPolls = 1 << 15;        // bounded wait for a published block ...
+constexpr unsigned kFsSleepNs = 256;     // ... sleeping between polls (~10 ms in all)
+
+__device__ __forceinline__ int fs_ld_acquire(const int* p)
+{
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void fs_st_release(int* p, int v)
+{
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" :: "l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ float2 fs_conj(float2 a) { return make_float2(a.x, -a.y); }
+
+// Entries (r, kFsLanes j + tq), j < kFsPer, of tile (i, k) of the triangle (zero outside the matrix).
+template <bool kCT>
+__device__ __forceinline__ void fs_load(const float2* __restrict__ M, int64_t n, int i, int k,
+                                        float2 (&m)[kFsPer])
+{
+    constexpr int NB = 64;
+    const int r = threadIdx.x / kFsLanes, tq = threadIdx.x % kFsLanes;
+    const int64_t i0 = (int64_t)i * NB, k0 = (int64_t)k * NB;
+    const bool rok = i0 + r < n;
+#pragma unroll
+    for (int j = 0; j < kFsPer; ++j) {
+        const int t = kFsLanes * j + tq;
+        m[j] = make_float2(0.f, 0.f);
+        if (rok && k0 + t < n) m[j] = kCT ? fs_conj(M[(i0 + r) * n + k0 + t]) : M[(k0 + t) * n + i0 + r];
+    }
+}
+
+// The same entries of the inverse diagonal block (column-major; conjugate-transposed for kCT).
+template <bool kCT>
+__device__ __forceinline__ void fs_load_inv(const float2* __restrict__ Inv, float2 (&iv)[kFsPer])
+{
+    constexpr int NB = 64;
+    const int r = threadIdx.x / kFsLanes, tq = threadIdx.x % kFsLanes;
+#pragma unroll
+    for (int j = 0; j < kFsPer; ++j) {
+        const int t = kFsLanes * j + tq;
+        iv[j] = kCT ? fs_conj(Inv[r * NB + t]) : Inv[t * NB + r];
+    }
+}
+
+// Row r of (tile m) (src columns q0 .. q0 + nq), summed over the row's lanes
+// (every lane of the row ends with the sum).
+__device__ __forceinline__ void fs_rowdot(const float2 (&m)[kFsPer], const float2 (*src)[64], int q0, int nq,
+                                          float (&ax)[4], float (&ay)[4])
+{
+    const int tq = threadIdx.x % kFsLanes;
+#pragma unroll
+    for (int qq = 0; qq < 4; ++qq) ax[qq] = ay[qq] = 0.f;
+#pragma unroll
+    for (int j = 0; j < kFsPer; ++j) {
+#pragma unroll
+        for (int qq = 0; qq < 4; ++qq) {
+            if (qq < nq) {
+                const float2 v = src[q0 + qq][kFsLanes * j + tq];
+                ax[qq] += m[j].x * v.x - m[j].y * v.y;
+                ay[qq] += m[j].x * v.y + m[j].y * v.x;
+            }
+        }
+    }
+#pragma unroll
+    for (int qq = 0; qq < 4; ++qq) {
+#pragma unroll
+        for (int o = 1; o < kFsLanes; o <<= 1) {
+            ax[qq] += __shfl_xor_sync(0xffffffffu, ax[qq], o);
+            ay[qq] += __shfl_xor_sync(0xffffffffu, ay[qq], o);
+        }
+    }
+}
+
+// x_i -= T_ik y for the tile held in m (rows of block i).
+__device__ __forceinline__ void fs_apply(const float2 (&m)[kFsPer], int64_t n, int i, float2* x,
+                                         const float2 (*y)[64], int nrhs)
+{
+    const int r = threadIdx.x / kFsLanes, tq = threadIdx.x % kFsLanes;
+    const int64_t row = (int64_t)i * 64 + r;
+    for (int q0 = 0; q0 < nrhs; q0 += 4) {
+        const int nq = min(4, nrhs - q0);
+        float ax[4], ay[4];
+        fs_rowdot(m, y, q0, nq, ax, ay);
+        if (tq == 0 && row < n)
+            for (int qq = 0; qq < nq; ++qq) {
+                float2* p = x + (int64_t)(q0 + qq) * n + row;
+                const float2 v = *p;
+                *p = make_float2(v.x - ax[qq], v.y - ay[qq]);
+            }
+    }
+}
+
+// y_i = inv(T_ii) v (v complete in vs, inverse entries in iv), into ynext and
+// over x_i; then publish.
+__device__ __forceinline__ void fs_solve_publish(const float2 (&iv)[kFsPer], int64_t n, int i, float2* x,
+                                                 const float2 (*vs)[64], float2 (*ynext)[64], int nrhs, int* flag)
+{
+    const int r = threadIdx.x / kFsLanes, tq = threadIdx.x % kFsLanes;
+    const int64_t i0 = (int64_t)i * 64;
+    const bool rok = i0 + r < n;
+    for (int q0 = 0; q0 < nrhs; q0 += 4) {
+        const int nq = min(4, nrhs - q0);
+        float ax[4], ay[4];
+        fs_rowdot(iv, vs, q0, nq, ax, ay);
+        if (tq == 0)
+            for (int qq = 0; qq < nq; ++qq) {
+                const float2 v = rok ? make_float2(ax[qq], ay[qq]) : make_float2(0.f, 0.f);
+                ynext[q0 + qq][r] = v;
+                if (rok) x[(int64_t)(q0 + qq) * n + i0 + r] = v;
+            }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        fs_st_release(flag, 1);
+    }
+}
+
+template <bool kCT>
+__global__ void __cluster_dims__(kFsCluster, 1, 1) __launch_bounds__(kFsThreads, 2)
+k_lu_solve_flags(const float2* __restrict__ A, int64_t n, int64_t stride, const float2* __restrict__ Dinv,
+                 int64_t dstride, float2* X, int64_t xstride, int nrhs, int* flags, int* bad)
+{
+    constexpr int NB = 64;
+    __shared__ float2 ys[2][kMaxRhs][NB];  // y of the block being applied and of the next one
+    __shared__ float2 vs[kMaxRhs][NB];     // x of the block being solved
+    __shared__ int s_fail;
+    const int64_t b = blockIdx.x / kFsCluster;
+    const int rank = (int)cluster_rank();
+    const float2* M = A + b * stride;
+    const float2* Dv = Dinv + b * dstride;
+    float2* x = X + b * xstride;
+    const int nblk = (int)((n + NB - 1) / NB);
+    int* fl = flags + b * 2 * nblk;
+    const int tid = threadIdx.x;
+    if (tid == 0) s_fail = 0;
+    __syncthreads();
+    for (int tri = 0; tri < 2; ++tri) {
+        const bool fwd = tri == 0;
+        // inverse diagonal blocks: inv(L11) at offset 0, inv(U11) at NB * NB
+        const int inv_off = (fwd != kCT) ? 0 : NB * NB;
+        int* tfl = fl + tri * nblk;
+        const int k_first = fwd ? 0 : nblk - 1;
+        if (k_first % kFsCluster == rank) {  // the first block: x is complete
+            float2 iv[kFsPer];
+            fs_load_inv<kCT>(Dv + (int64_t)k_first * 2 * NB * NB + inv_off, iv);
+            const int64_t f0 = (int64_t)k_first * NB;
+            for (int e = tid; e < nrhs * NB; e += blockDim.x) {
+                const int q = e / NB, rr = e % NB;
+                vs[q][rr] = f0 + rr < n ? x[(int64_t)q * n + f0 + rr] : make_float2(0.f, 0.f);
+            }
+            __syncthreads();
+            fs_solve_publish(iv, n, k_first, x, vs, ys[0], nrhs, tfl + k_first);
+        }
+        for (int p = 0; p < nblk; ++p) {
+            const int k = fwd ? p : nblk - 1 - p;
+            const int kn = fwd ? k + 1 : k - 1;
+            const bool next_mine = p + 1 < nblk && kn % kFsCluster == rank;
+            float2 (*y)[NB] = ys[p & 1];
+            if (k % kFsCluster != rank) {
+                if (tid == 0 && !s_fail) {
+                    int it = 0;
+                    while (fs_ld_acquire(tfl + k) == 0 && ++it < kFsPolls) __nanosleep(kFsSleepNs);
+                    if (it >= kFsPolls) {
+                        s_fail = 1;
+                        atomicExch(bad + b, 3);
+                    }
+                }
+                __syncthreads();
+                const int64_t k0 = (int64_t)k * NB;
+                for (int e = tid; e < nrhs * NB; e += blockDim.x) {
+                    const int q = e / NB, rr = e % NB;
+                    y[q][rr] = k0 + rr < n ? __ldcg(x + (int64_t)q * n + k0 + rr) : make_float2(0.f, 0.f);
+                }
+            }
+            __syncthreads();
+            if (next_mine) {  // the next block first: apply y_k to it, solve, publish
+                float2 m[kFsPer];
+                fs_load<kCT>(M, n, kn, k, m);
+                fs_apply(m, n, kn, x, y, nrhs);
+                float2 iv[kFsPer];
+                fs_load_inv<kCT>(Dv + (int64_t)kn * 2 * NB * NB + inv_off, iv);
+                __syncthreads();
+                const int64_t f0 = (int64_t)kn * NB;
+                for (int e = tid; e < nrhs * NB; e += blockDim.x) {
+                    const int q = e / NB, rr = e % NB;
+                    vs[q][rr] = f0 + rr < n ? x[(int64_t)q * n + f0 + rr] : make_float2(0.f, 0.f);
+                }
+                __syncthreads();
+                fs_solve_publish(iv, n, kn, x, vs, ys[(p + 1) & 1], nrhs, tfl + kn);
+            }
+            // the rest of this CTA's blocks after kn in the triangle's order, two tiles in flight
+            int q = p + 2;
+            while (q < nblk && (fwd ? q : nblk - 1 - q) % kFsCluster != rank) ++q;
+            for (; q < nblk; q += 2 * kFsCluster) {
+                const int i1 = fwd ? q : nblk - 1 - q;
+                const int q2 = q + kFsCluster;
+                float2 m1[kFsPer], m2[kFsPer];
+                fs_load<kCT>(M, n, i1, k, m1);
+                if (q2 < nblk) fs_load<kCT>(M, n, fwd ? q2 : nblk - 1 - q2, k, m2);
+                fs_apply(m1, n, i1, x, y, nrhs);
+                if (q2 < nblk) fs_apply(m2, n, fwd ? q2 : nblk - 1 - q2, x, y, nrhs);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+
+
 }  // namespace
 
 int64_t lu_dinv_stride_tc(int64_t n) { return ((n + TC_NB - 1) / TC_NB) * 2 * TC_NB * TC_NB; }
@@ -981,20 +1224,19 @@ cudaError_t launch_lu_solve_persist(mh_ctx* ctx, int backend, bool conj_trans, c
     cudaError_t e;
     if (backend == MH_LU_TCGEN05_F16) {
         const int64_t ds = lu_dinv_stride_tc(n);
-        const size_t sm = persist_smem_bytes<TC_NB>();
-        if (conj_trans) {
-            if ((e = cudaFuncSetAttribute(k_lu_solve_persist<TC_NB, true>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) != cudaSuccess)
-                return e;
-            k_lu_solve_persist<TC_NB, true><<<g, kSolveThreads, sm, ctx->stream>>>(A, n, stride, Dinv, ds, X,
-                                                                                    xstride, nrhs);
-        } else {
-            if ((e = cudaFuncSetAttribute(k_lu_solve_persist<TC_NB, false>,
-                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) != cudaSuccess)
-                return e;
-            k_lu_solve_persist<TC_NB, false><<<g, kSolveThreads, sm, ctx->stream>>>(A, n, stride, Dinv, ds, X,
-                                                                                     xstride, nrhs);
-        }
+        const int64_t nblk = (n + TC_NB - 1) / TC_NB;
+        const size_t fbytes = sizeof(int) * (size_t)(2 * nblk * nbatch + nbatch);
+        auto* flags = (int*)ws_get(ctx, WS_FLAGS, fbytes);
+        if (!flags) return cudaErrorMemoryAllocation;
+        int* fbad = flags + 2 * nblk * nbatch;
+        if ((e = cudaMemsetAsync(flags, 0, fbytes, ctx->stream)) != cudaSuccess) return e;
+        const dim3 gf((unsigned)nbatch * kFsCluster);
+        if (conj_trans)
+            k_lu_solve_flags<true><<<gf, kFsThreads, 0, ctx->stream>>>(A, n, stride, Dinv, ds, X, xstride, nrhs,
+                                                                      flags, fbad);
+        else
+            k_lu_solve_flags<false><<<gf, kFsThreads, 0, ctx->stream>>>(A, n, stride, Dinv, ds, X, xstride, nrhs,
+                                                                       flags, fbad);
     } else {
         const int64_t ds = lu_dinv_stride(n);
         const size_t sm = persist_smem_bytes<32>();

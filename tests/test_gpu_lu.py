@@ -106,3 +106,25 @@ def test_batch_with_fp32_lu(mh, oracle, gpu):
     Ao, Bo, _, _ = oracle.hydro_coefficients(mesh, [0.7, 1.9], dofs)
     assert np.max(np.abs(A - Ao)) / np.max(np.abs(Ao)) < 1e-9
     assert info.refine_iterations <= 4
+
+
+@pytest.mark.parametrize("backend", ["tcgen05", "simt"])
+@pytest.mark.parametrize("conj", [False, True])
+@pytest.mark.parametrize("n,nrhs", [(40, 2), (64, 1), (200, 3), (320, 5), (517, 16)])
+def test_lowp_solve_matches_its_factors(mh, gpu, backend, conj, n, nrhs):
+    """The FP32 block substitution of a refinement step (L U X = B, or
+    (L U)^H X = B for the adjoint) against the same factors solved in FP64:
+    sizes with a partial last block, one block, several right-hand sides."""
+    rng = np.random.default_rng(10 * n + nrhs)
+    A = _bem_like(rng, 2, n)
+    B = rng.normal(size=(2, n, nrhs)) + 1j * rng.normal(size=(2, n, nrhs))
+    LU, bad = gpu.lu_factor_lowp(A, backend)
+    assert not bad.any()
+    X = gpu.lu_solve_lowp(A, B, backend, conj)
+    for b in range(A.shape[0]):
+        M = _reconstruct(LU[b].astype(np.complex128))
+        if conj:
+            M = M.conj().T
+        ref = np.linalg.solve(M, B[b])
+        err = np.max(np.abs(X[b] - ref)) / np.max(np.abs(ref))
+        assert err <= 1e-5, (backend, conj, n, nrhs, b, err)
