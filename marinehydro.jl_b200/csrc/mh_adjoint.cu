@@ -560,38 +560,32 @@ k_adj_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const do
 // Rankine terms
 // ---------------------------------------------------------------------------
 
-// One dual-number pass of the near-field reverse (rankine.jl:36-61, 65-123):
-// pass 0 gives dL/d(centre, normal) and the forward gradient, pass 1 dL/d
-// (vertex 0, vertex 1), pass 2 dL/d(vertex 2, vertex 3), L = ibar I + gb . grad.
-__device__ __noinline__ void rankine_near_pass(const double* y, const Panel& p, double ibar, const double* gb,
-                                               int pass, double* out, double* gr)
+// One tangent direction of the near-field reverse (rankine.jl:36-61,
+// 65-123) with single dual numbers: direction dir 0..2 the centre, 3..5 the
+// normal, 6 + 3 v + c vertex v coordinate c; returns dL/d(direction),
+// L = ibar I + gb . grad, and (direction 0) the forward gradient.  One
+// direction per thread keeps the dual panel in registers.
+__device__ __noinline__ double rankine_near_dir(const double* y, const Panel& p, double ibar, const double* gb,
+                                                int dir, double* gr)
 {
-    PanelT<d6> q;
+    using d1 = dualn<1>;
+    PanelT<d1> q;
     for (int a = 0; a < 3; ++a) {
-        q.c[a] = dconst<6>(p.c[a]);
-        q.n[a] = dconst<6>(p.n[a]);
+        q.c[a] = dconst<1>(p.c[a]);
+        q.n[a] = dconst<1>(p.n[a]);
     }
-    for (int t = 0; t < 12; ++t) q.v[t] = dconst<6>(p.v[t]);
-    q.area = dconst<6>(p.area);
-    q.radius = dconst<6>(p.radius);
-    if (pass == 0) {
-        for (int a = 0; a < 3; ++a) {
-            q.c[a].d[a] = 1.0;
-            q.n[a].d[3 + a] = 1.0;
-        }
-    } else {
-        const int v0 = 2 * (pass - 1);
-        for (int c = 0; c < 3; ++c) {
-            q.v[3 * v0 + c].d[c] = 1.0;
-            q.v[3 * (v0 + 1) + c].d[3 + c] = 1.0;
-        }
-    }
-    const d6 yd[3] = {dconst<6>(y[0]), dconst<6>(y[1]), dconst<6>(y[2])};
-    d6 I, g[3];
+    for (int t = 0; t < 12; ++t) q.v[t] = dconst<1>(p.v[t]);
+    q.area = dconst<1>(p.area);
+    q.radius = dconst<1>(p.radius);
+    if (dir < 3) q.c[dir].d[0] = 1.0;
+    else if (dir < 6) q.n[dir - 3].d[0] = 1.0;
+    else q.v[dir - 6].d[0] = 1.0;
+    const d1 yd[3] = {dconst<1>(y[0]), dconst<1>(y[1]), dconst<1>(y[2])};
+    d1 I, g[3];
     rankine_pair(yd, q, I, g);
-    for (int k = 0; k < 6; ++k) out[k] = ibar * I.d[k] + gb[0] * g[0].d[k] + gb[1] * g[1].d[k] + gb[2] * g[2].d[k];
-    if (pass == 0)
+    if (dir == 0)
         for (int a = 0; a < 3; ++a) gr[a] = g[a].v;
+    return ibar * I.d[0] + gb[0] * g[0].d[0] + gb[1] * g[1].d[0] + gb[2] * g[2].d[0];
 }
 
 // Far field reverse (rankine.jl:33-34): I = A/r, grad = A rb / r^3,
@@ -611,14 +605,15 @@ __device__ __forceinline__ void rankine_far_vjp(const double rb[3], double r, do
 // Rankine-term contraction against the frequency sums WS = sum_w S-bar(w),
 // WD = sum_w D-bar(w) (real parts used), 128 rows x 16 columns per CTA.
 // Far-field terms are reversed in place; near-field (row, column, term)
-// entries are listed per CTA in row-major order and their three dual passes
-// spread over all threads, 128 entries at a time; rows and columns then sum
-// their entries in list order.  Partials as k_adj_wave with GB_NF column
+// entries are listed per CTA in row-major order and their 18 tangent
+// directions (centre, normal, four vertices) spread over all threads, 128
+// entries at a time; rows and columns then sum their entries in list order.  Partials as k_adj_wave with GB_NF column
 // fields.
 constexpr int kNearChunk = 128;
-constexpr int kNearF = 21;  // per entry: pass outputs 18, normal cotangent 3
+constexpr int kNearDirs = 18;
+constexpr int kNearF = 21;  // per entry: direction outputs 18, normal cotangent 3
 
-__global__ void __launch_bounds__(kAR)
+__global__ void __launch_bounds__(kAR, 3)
 k_adj_rankine(const double* __restrict__ geom, int64_t n, uint32_t mask, int direct,
               const double2* __restrict__ WS, const double2* __restrict__ WD, double* __restrict__ rowpart,
               double* __restrict__ colpart)
@@ -714,8 +709,8 @@ k_adj_rankine(const double* __restrict__ geom, int64_t n, uint32_t mask, int dir
     for (int f = 0; f < GB_NF; ++f) cl[f] = 0.0;
     for (int c0 = 0; c0 < total; c0 += kNearChunk) {
         const int m = min(kNearChunk, total - c0);
-        for (int w = tid; w < 3 * m; w += blockDim.x) {
-            const int e = w % m, pass = w / m;
+        for (int w = tid; w < kNearDirs * m; w += blockDim.x) {
+            const int e = w % m, dir = w / m;
             const int code = list[c0 + e];
             const int r = code >> 5, bit = code & 31, jj = bit >> 1, term = bit & 1;
             const int64_t ie = i0 + r, j = j0 + jj;
@@ -734,8 +729,8 @@ k_adj_rankine(const double* __restrict__ geom, int64_t n, uint32_t mask, int dir
             const double gb[3] = {-kI4P * wd * nD[0] * f[0], -kI4P * wd * nD[1] * f[1], -kI4P * wd * nD[2] * f[2]};
             const double y[3] = {xe[0], xe[1], term ? -xe[2] : xe[2]};
             double gr[3];
-            rankine_near_pass(y, p, (term ? sgn : 1.0) * (-kI4P * ws), gb, pass, &res[e][6 * pass], gr);
-            if (pass == 0)
+            res[e][dir] = rankine_near_dir(y, p, (term ? sgn : 1.0) * (-kI4P * ws), gb, dir, gr);
+            if (dir == 0)
                 for (int a = 0; a < 3; ++a) res[e][18 + a] = -kI4P * wd * f[a] * gr[a];
         }
         __syncthreads();

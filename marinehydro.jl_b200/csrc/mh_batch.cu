@@ -131,6 +131,8 @@ k_wave_batch(const double* __restrict__ geom, int64_t n, int direct, const doubl
 // w_q[i] = sum_j c_q[i][j] T_j(v(alpha)) (shared memory), and each frequency
 // then evaluates four 1-D Chebyshev series in R (Clenshaw) with no
 // transcendental calls; the log term splits as log(k) + log((d + |zeta|)/2).
+// The series in R use the table's monomial-in-u copy (Horner's rule, four
+// frequencies per pass).
 // Frequencies at which the pair leaves the polar patch use the full table.
 // Same arithmetic as wave_pair<true> up to reassociation (~1e-16).
 constexpr int kWT = 128;  // threads (rows) per CTA of k_wave_delh_allw
@@ -153,7 +155,7 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
     __shared__ Panel sp[kCols];
     const int64_t j0 = (int64_t)blockIdx.y * kCols;
     stage_panels(sp, geom, n, j0);
-    for (int t = threadIdx.x; t < 4 * kTabPolarFn; t += blockDim.x) coef[t] = tab[t];
+    for (int t = threadIdx.x; t < 4 * kTabPolarFn; t += blockDim.x) coef[t] = tab[kTabMonoOff + t];
     for (int t = threadIdx.x; t < nb; t += blockDim.x) {
         logk[t] = log(kvec[t]);
         invk[t] = 1.0 / kvec[t];
@@ -205,48 +207,42 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
                 }
             }
         }
-        // two frequencies per Clenshaw pass: each series coefficient read from
-        // shared memory feeds both recurrences
-        for (int z0 = 0; z0 < nb; z0 += 2) {
-            const int nz = (z0 + 1 < nb) ? 2 : 1;
-            double kz[2], uz[2];
-            bool pz[2];
+        // four frequencies per Horner pass: each coefficient read from shared
+        // memory feeds four recurrences
+        constexpr int kZP = 4;
+        for (int z0 = 0; z0 < nb; z0 += kZP) {
+            const int nz = min(kZP, nb - z0);
+            double kz[kZP], uz[kZP];
+            bool pz[kZP];
+            bool anyp = false;
 #pragma unroll
-            for (int t = 0; t < 2; ++t) {
+            for (int t = 0; t < kZP; ++t) {
                 kz[t] = kvec[z0 + (t < nz ? t : 0)];
                 const double R = kz[t] * d;
                 pz[t] = t < nz && polar_ok && R < kTabRPolar;
+                anyp |= pz[t];
                 uz[t] = 2.0 * R / kTabRPolar - 1.0;
             }
-            double val[2][4];
-            if (pz[0] || pz[1]) {
-                double b1[2][4], b2[2][4];
+            double val[kZP][4];
+            if (anyp) {
 #pragma unroll
-                for (int t = 0; t < 2; ++t)
+                for (int q = 0; q < 4; ++q) {
+                    const double c = w[(q * kTabNU + kTabNU - 1) * kWT + tid];
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) b1[t][q] = b2[t][q] = 0.0;
+                    for (int t = 0; t < kZP; ++t) val[t][q] = c;
+                }
 #pragma unroll
-                for (int row = kTabNU - 1; row >= 1; --row) {
+                for (int row = kTabNU - 2; row >= 0; --row) {
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         const double c = w[(q * kTabNU + row) * kWT + tid];
 #pragma unroll
-                        for (int t = 0; t < 2; ++t) {
-                            const double nt = fma(2.0 * uz[t], b1[t][q], c - b2[t][q]);
-                            b2[t][q] = b1[t][q];
-                            b1[t][q] = nt;
-                        }
+                        for (int t = 0; t < kZP; ++t) val[t][q] = fma(val[t][q], uz[t], c);
                     }
-                }
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const double c0 = w[q * kTabNU * kWT + tid];
-#pragma unroll
-                    for (int t = 0; t < 2; ++t) val[t][q] = fma(uz[t], b1[t][q], c0 - b2[t][q]);
                 }
             }
 #pragma unroll
-            for (int t = 0; t < 2; ++t) {
+            for (int t = 0; t < kZP; ++t) {
                 if (t >= nz) break;
                 const int z = z0 + t;
                 const double k = kz[t], ik = invk[z];

@@ -140,15 +140,29 @@ int ensure_delh_table(mh_ctx* ctx)
         return set_err(ctx, MH_ERR_CUDA, "Delhommeau table nodes: %s", cudaGetErrorString(e));
     }
     // polar block: B, C, E0, E1, fitted on kTabNP x kTabNP nodes; the first
-    // kTabNU rows (degrees in R) are kept
+    // kTabNU rows (degrees in R) are kept, and again with the rows in the
+    // monomial basis of u: T_i(u) = sum_m P[i][m] u^m
     {
         std::vector<double> full((size_t)kTabNP * kTabNP);
+        std::vector<double> P((size_t)kTabNU * kTabNU, 0.0);  // P[i][m]
+        P[0] = 1.0;
+        if (kTabNU > 1) P[1 * kTabNU + 1] = 1.0;
+        for (int i = 2; i < kTabNU; ++i)  // T_i = 2 u T_{i-1} - T_{i-2}
+            for (int m = 0; m < kTabNU; ++m)
+                P[(size_t)i * kTabNU + m] = (m > 0 ? 2.0 * P[(size_t)(i - 1) * kTabNU + m - 1] : 0.0) -
+                                            P[(size_t)(i - 2) * kTabNU + m];
         const double* src[4] = {hB.data(), hC.data(), hE0.data(), hE1.data()};
         for (int q = 0; q < 4; ++q) {
             cheb_coeffs(kTabNP, src[q], full.data());
             for (int i = 0; i < kTabNU; ++i)
                 for (int j = 0; j < kTabNV; ++j)
                     tab[(size_t)q * kTabPolarFn + i * kTabNV + j] = full[(size_t)i * kTabNP + j];
+            for (int m = 0; m < kTabNU; ++m)
+                for (int j = 0; j < kTabNV; ++j) {
+                    double a = 0.0;
+                    for (int i = m; i < kTabNU; ++i) a += P[(size_t)i * kTabNU + m] * full[(size_t)i * kTabNP + j];
+                    tab[kTabMonoOff + (size_t)q * kTabPolarFn + m * kTabNV + j] = a;
+                }
         }
     }
     // cells

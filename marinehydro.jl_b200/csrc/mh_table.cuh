@@ -45,7 +45,15 @@ constexpr double kTabExtent = kTabH * kTabNCell;
 constexpr int kTabPolarFn = kTabNU * kTabNV;                   // one polar function
 constexpr int kTabPolarWords = 4 * kTabPolarFn;                 // B, C, E0, E1
 constexpr int kTabCellWords = 2 * kTabNC * kTabNC;             // B then C
-constexpr int kTabWords = kTabPolarWords + kTabNCell * kTabNCell * kTabCellWords;
+// The polar functions once more with the R direction in the monomial basis:
+// row m holds the coefficient of u^m (u = 2 R / kTabRPolar - 1), columns
+// still Chebyshev in alpha.  After the alpha contraction each function is a
+// degree-13 polynomial in u whose monomial coefficients sum to less than 5
+// in absolute value (the Chebyshev coefficients decay faster than the basis
+// change grows them), so Horner's rule in u is as accurate as Clenshaw's
+// recurrence and takes one FMA per term instead of two operations.
+constexpr int kTabMonoOff = kTabPolarWords + kTabNCell * kTabNCell * kTabCellWords;
+constexpr int kTabWords = kTabMonoOff + kTabPolarWords;
 
 // sum_i sum_j c[i*NV + j] T_i(u) T_j(v), i < NU, j < NV, by nested Clenshaw
 // recurrences (rows in v, then the row sums in u); a few registers instead
