@@ -137,9 +137,9 @@ k_wave_batch(const double* __restrict__ geom, int64_t n, int direct, const doubl
 // Same arithmetic as wave_pair<true> up to reassociation (~1e-16).
 constexpr int kWT = 128;  // threads (rows) per CTA of k_wave_delh_allw
 constexpr int kAllwMaxFreqs = 128;  // frequencies per launch of k_wave_delh_allw
-// polar tables, the contracted series of every row, log k and 1/k per frequency
-constexpr size_t kWaveAllwSmem =
-    sizeof(double) * (4 * kTabPolarFn + 4 * kTabNU * kWT + 2 * kAllwMaxFreqs);
+// the contracted series of every row, log k and 1/k per frequency (the polar
+// table itself is read through L1: every lane reads the same coefficient)
+constexpr size_t kWaveAllwSmem = sizeof(double) * (4 * kTabNU * kWT + 2 * kAllwMaxFreqs);
 
 __global__ void __launch_bounds__(kWT, 3)
 k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const double* __restrict__ tab,
@@ -148,14 +148,13 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
                  float2* __restrict__ Dlo, double2* __restrict__ tape)
 {
     extern __shared__ double wsm[];
-    double* coef = wsm;                           // 4 polar tables, NP x NP each
-    double* w = wsm + 4 * kTabPolarFn;         // [4 * NU][kWT]
+    const double* coef = tab + kTabMonoOff;        // 4 polar tables, monomial in u
+    double* w = wsm;                               // [4 * NU][kWT]
     double* logk = w + 4 * kTabNU * kWT;           // [nb]
     double* invk = logk + kAllwMaxFreqs;           // [nb], nb <= kAllwMaxFreqs
     __shared__ Panel sp[kCols];
     const int64_t j0 = (int64_t)blockIdx.y * kCols;
     stage_panels(sp, geom, n, j0);
-    for (int t = threadIdx.x; t < 4 * kTabPolarFn; t += blockDim.x) coef[t] = tab[kTabMonoOff + t];
     for (int t = threadIdx.x; t < nb; t += blockDim.x) {
         logk[t] = log(kvec[t]);
         invk[t] = 1.0 / kvec[t];
@@ -199,11 +198,11 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
                     double b1 = 0.0, b2 = 0.0;
 #pragma unroll
                     for (int col = kTabNV - 1; col >= 1; --col) {
-                        const double t = fma(2.0 * v, b1, cr[col] - b2);
+                        const double t = fma(2.0 * v, b1, __ldg(cr + col) - b2);
                         b2 = b1;
                         b1 = t;
                     }
-                    w[(q * kTabNU + row) * kWT + tid] = fma(v, b1, cr[0] - b2);
+                    w[(q * kTabNU + row) * kWT + tid] = fma(v, b1, __ldg(cr) - b2);
                 }
             }
         }

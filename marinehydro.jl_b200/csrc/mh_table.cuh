@@ -16,16 +16,15 @@
 // = e^z J0(r) of the log-moments of e^zeta E1(zeta)).  B and C are smooth
 // in polar coordinates (R, alpha = atan2(r, |z|)) near the origin and in
 // (r, |z|) away from it, so they are tabulated as 2-D Chebyshev series:
-//   - one polar patch, R in [0, 1.5), alpha in [0, pi/2], fitted at 20 x 20
+//   - one polar patch, R in [0, 2), alpha in [0, pi/2], fitted at 24 x 24
 //     nodes, holding B, C and also E0 = e^z J0(r), E1 = e^z J1(r) (smooth;
 //     used by the frequency-batched evaluation, which contracts the alpha
 //     direction once per panel pair and then needs only 1-D series in R per
-//     frequency).  The R direction keeps degree 13: the fitted coefficients
-//     of degrees 14..19 in R are at the rounding level (|c| < 1e-14 for all
-//     four functions), so they are dropped and every series in R is 6 terms
-//     shorter;
-//   - Cartesian cells of 0.5 x 0.5 over r, |z| in [0, 16), degree 12 x 12
-//     (every cell touching R < 1 lies inside the polar patch).
+//     frequency).  Degree 14 in R and 21 in alpha are kept: the fitted
+//     coefficients beyond them are at the rounding level (|c| < 5e-15 for
+//     all four functions);
+//   - Cartesian cells of 0.5 x 0.5 over r, |z| in [0, 16), degree 12 x 12,
+//     for R >= 2 (every cell touching R < 1 lies inside the polar patch).
 // Points outside the table fall back to the adaptive quadrature.  The node
 // values are computed on the device with the FP64 quadrature; the table's
 // error against it is ~1e-12 absolute.
@@ -34,11 +33,11 @@
 
 namespace mh {
 
-constexpr int kTabNP = 20;          // polar patch nodes per direction (fit)
-constexpr int kTabNU = 14;          // polar coefficients kept in R (rows)
-constexpr int kTabNV = kTabNP;      // polar coefficients kept in alpha (columns)
+constexpr int kTabNP = 24;          // polar patch nodes per direction (fit)
+constexpr int kTabNU = 15;          // polar coefficients kept in R (rows)
+constexpr int kTabNV = 22;          // polar coefficients kept in alpha (columns)
 constexpr int kTabNC = 12;          // Cartesian cell degree
-constexpr double kTabRPolar = 1.5;  // polar patch radius
+constexpr double kTabRPolar = 2.0;  // polar patch radius
 constexpr double kTabH = 0.5;       // Cartesian cell size
 constexpr int kTabNCell = 32;       // cells per direction -> extent 16
 constexpr double kTabExtent = kTabH * kTabNCell;
@@ -48,7 +47,7 @@ constexpr int kTabCellWords = 2 * kTabNC * kTabNC;             // B then C
 // The polar functions once more with the R direction in the monomial basis:
 // row m holds the coefficient of u^m (u = 2 R / kTabRPolar - 1), columns
 // still Chebyshev in alpha.  After the alpha contraction each function is a
-// degree-13 polynomial in u whose monomial coefficients sum to less than 5
+// degree-14 polynomial in u whose monomial coefficients sum to less than 6
 // in absolute value (the Chebyshev coefficients decay faster than the basis
 // change grows them), so Horner's rule in u is as accurate as Clenshaw's
 // recurrence and takes one FMA per term instead of two operations.
