@@ -512,7 +512,7 @@ def _peaks():
 # ncu capture (hemisphere 1024 panels, 16 frequencies: dram__bytes_read.sum +
 # dram__bytes_write.sum / (n^2 * 16)); traffic grows with the pairs and
 # frequencies a launch processes, so it is scaled by them.
-WAVE_DRAM_BYTES_PER_PAIR_FREQ = 37.6
+WAVE_DRAM_BYTES_PER_PAIR_FREQ = 38.6
 
 
 def roofline(per_phase, n, args):
@@ -537,12 +537,13 @@ def roofline(per_phase, n, args):
     out = {"kernel": "k_wave_delh_allw", "bound": "hbm", "achieved": achieved, "peak": hbm,
            "unit": "GB/s", "frac": achieved / hbm, "peak_source": src, "traffic": traffic,
            "ms_per_launch": ms, "algorithmic_bytes_per_launch": alg,
-           "note": ("FP64-issue bound (table Clenshaw, log, complex arithmetic per pair and "
-                    "frequency); the HBM fraction shows the writes are not the limit")}
+           "note": ("FP64-issue bound (alpha contraction of the polar table per pair, Horner series "
+                    "in R and complex arithmetic per pair and frequency; ncu: FP64 pipe 34% active "
+                    "at 17% warps active); the HBM fraction shows the writes are not the limit")}
     if "lu" in per_phase:
         fl = 8.0 / 3.0 * float(n) ** 3 * args.n_omega
         ach = fl / (per_phase["lu"] / 1e3) / 1e12
-        out["lu"] = {"kernels": "k_lu_diag + k_lu_trsm_tc + k_lu_update_tc", "bound": "tensor",
+        out["lu"] = {"kernels": "k_lu_diag64 + k_lu_trsm_tc + k_lu_update_tc", "bound": "tensor",
                      "achieved": ach, "peak": tensor, "unit": "TFLOP/s", "frac": ach / tensor,
                      "ms_per_step": per_phase["lu"], "algorithmic_flops_per_step": fl}
     return out
