@@ -565,7 +565,7 @@ k_adj_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const do
 // normal, 6 + 3 v + c vertex v coordinate c; returns dL/d(direction),
 // L = ibar I + gb . grad, and (direction 0) the forward gradient.  One
 // direction per thread keeps the dual panel in registers.
-__device__ __noinline__ double rankine_near_dir(const double* y, const Panel& p, double ibar, const double* gb,
+__device__ __forceinline__ double rankine_near_dir(const double* y, const Panel& p, double ibar, const double* gb,
                                                 int dir, double* gr)
 {
     using d1 = dualn<1>;
@@ -603,30 +603,31 @@ __device__ __forceinline__ void rankine_far_vjp(const double rb[3], double r, do
 }
 
 // Rankine-term contraction against the frequency sums WS = sum_w S-bar(w),
-// WD = sum_w D-bar(w) (real parts used), 128 rows x 16 columns per CTA.
-// Far-field terms are reversed in place; near-field (row, column, term)
-// entries are listed per CTA in row-major order and their 18 tangent
-// directions (centre, normal, four vertices) spread over all threads, 128
-// entries at a time; rows and columns then sum their entries in list order.  Partials as k_adj_wave with GB_NF column
-// fields.
+// WD = sum_w D-bar(w) (real parts used), 128 rows x 16 columns per CTA, in
+// three kernels: k_adj_rankine reverses the far-field terms in place and
+// lists the near-field (row, column, term) entries of its CTA in row-major
+// order (global list, kNearCap codes per CTA); k_adj_near reverses every
+// listed entry along its 18 tangent directions (centre, normal, four
+// vertices), one (entry, direction) per thread over the whole matrix, so
+// the uneven near-field counts of the CTAs do not matter; k_adj_near_accum
+// then adds each CTA's entries to its row and column partials in list order
+// (fixed order: bitwise reproducible).  Partials as k_adj_wave with GB_NF
+// column fields.
 constexpr int kNearChunk = 128;
 constexpr int kNearDirs = 18;
 constexpr int kNearF = 21;  // per entry: direction outputs 18, normal cotangent 3
+constexpr int kNearCap = kAR * kAC * 2;  // entries a CTA can list
 
-__global__ void __launch_bounds__(kAR, 3)
+__global__ void __launch_bounds__(kAR)
 k_adj_rankine(const double* __restrict__ geom, int64_t n, uint32_t mask, int direct,
               const double2* __restrict__ WS, const double2* __restrict__ WD, double* __restrict__ rowpart,
-              double* __restrict__ colpart)
+              double* __restrict__ colpart, unsigned short* __restrict__ ncode, int* __restrict__ ncount)
 {
     __shared__ Panel sp[kAC];
     __shared__ double csm[kAR / 32][kAC][GB_NF];
-    __shared__ double cnear[kAC][GB_NF];
-    __shared__ double res[kNearChunk][kNearF];
-    __shared__ unsigned short list[kAR * kAC * 2];
     __shared__ int offs[kAR + 1];
     const int64_t j0 = (int64_t)blockIdx.y * kAC;
     stage(sp, geom, n, j0);
-    for (int t = threadIdx.x; t < kAC * GB_NF; t += blockDim.x) (&cnear[0][0])[t] = 0.0;
     __syncthreads();
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int64_t i0 = (int64_t)blockIdx.x * kAR;
@@ -696,46 +697,140 @@ k_adj_rankine(const double* __restrict__ geom, int64_t n, uint32_t mask, int dir
     if (tid == 0)
         for (int t = 1; t <= kAR; ++t) offs[t] += offs[t - 1];
     __syncthreads();
+    const int64_t cta = (int64_t)blockIdx.y * gridDim.x + blockIdx.x;
     {
+        unsigned short* list = ncode + cta * kNearCap;
         int o = offs[tid];
         for (uint32_t m = near; m; m &= m - 1) {
             const int bit = __ffs(m) - 1;
             list[o++] = (unsigned short)((tid << 5) | bit);
         }
     }
-    const int total = offs[kAR];
+    if (tid == 0) ncount[cta] = offs[kAR];
+    for (int t = threadIdx.x; t < jend * GB_NF; t += blockDim.x) {
+        const int jj = t / GB_NF, f = t % GB_NF;
+        double s = 0.0;
+        if (f < 7)
+            for (int w = 0; w < kAR / 32; ++w) s += csm[w][jj][f];
+        colpart[((int64_t)blockIdx.x * GB_NF + f) * n + j0 + jj] = s;
+    }
+    if (live) {
+        for (int c = 0; c < 3; ++c) {
+            rowpart[((int64_t)blockIdx.y * kRowF + c) * n + i] = xb[c];
+            rowpart[((int64_t)blockIdx.y * kRowF + 3 + c) * n + i] = nbi[c];
+        }
+    }
+}
+
+// Exclusive prefix sum of the per-CTA near-field counts (one CTA of 1024
+// threads); noff[ncta] = total.
+__global__ void __launch_bounds__(1024) k_near_scan(const int* __restrict__ ncount, int64_t ncta,
+                                                     int64_t* __restrict__ noff)
+{
+    __shared__ int64_t part[1024];
+    const int t = threadIdx.x;
+    const int64_t per = (ncta + 1023) / 1024, b0 = t * per, b1 = min(ncta, b0 + per);
+    int64_t s = 0;
+    for (int64_t c = b0; c < b1; ++c) s += ncount[c];
+    part[t] = s;
     __syncthreads();
+    if (t == 0) {
+        int64_t acc = 0;
+        for (int u = 0; u < 1024; ++u) {
+            const int64_t v = part[u];
+            part[u] = acc;
+            acc += v;
+        }
+        noff[ncta] = acc;
+    }
+    __syncthreads();
+    int64_t acc = part[t];
+    for (int64_t c = b0; c < b1; ++c) {
+        noff[c] = acc;
+        acc += ncount[c];
+    }
+}
+
+__device__ __forceinline__ void load_panel(const double* __restrict__ geom, int64_t n, int64_t j, Panel& p)
+{
+    for (int a = 0; a < 3; ++a) {
+        p.c[a] = geom[(G_CX + a) * n + j];
+        p.n[a] = geom[(G_NX + a) * n + j];
+    }
+    for (int t = 0; t < 12; ++t) p.v[t] = geom[(G_V + t) * n + j];
+    p.area = geom[G_AREA * n + j];
+    p.radius = geom[G_RADIUS * n + j];
+}
+
+// Reverse of every listed near-field entry along one tangent direction per
+// thread: item w = (entry e, direction w mod 18), entries numbered CTA by
+// CTA in list order (noff); res[e][0..17] direction outputs, res[e][18..20]
+// the normal cotangent.
+__global__ void __launch_bounds__(128, 2)
+k_adj_near(const double* __restrict__ geom, int64_t n, uint32_t mask, int direct, const double2* __restrict__ WS,
+           const double2* __restrict__ WD, const unsigned short* __restrict__ ncode,
+           const int64_t* __restrict__ noff, int64_t ncta, int rb, double* __restrict__ res)
+{
+    const int64_t total = noff[ncta];
+    const bool wrt_first = !direct;
+    const double sg = wrt_first ? -1.0 : 1.0, sz = wrt_first ? -1.0 : 1.0;
+    const uint32_t refl = mask & (MH_GF_RANKINE_REFLECTED | MH_GF_RANKINE_REFLECTED_NEGATIVE);
+    const double sgn = (refl == MH_GF_RANKINE_REFLECTED) ? 1.0 : -1.0;
+    const double mref[3] = {sgn * sg, sgn * sg, sgn * sg * sz};
+    for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < total * kNearDirs;
+         w += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e = w / kNearDirs;
+        const int dir = (int)(w % kNearDirs);
+        int64_t lo = 0, hi = ncta - 1;  // the last CTA whose first entry is <= e
+        while (lo < hi) {
+            const int64_t mid = (lo + hi + 1) >> 1;
+            if (noff[mid] <= e) lo = mid;
+            else hi = mid - 1;
+        }
+        const int code = ncode[lo * kNearCap + (e - noff[lo])];
+        const int r = code >> 5, bit = code & 31, jj = bit >> 1, term = bit & 1;
+        const int64_t ie = (lo % rb) * kAR + r, j = (lo / rb) * kAC + jj;
+        Panel p;
+        load_panel(geom, n, j, p);
+        const double xe[3] = {geom[G_CX * n + ie], geom[G_CY * n + ie], geom[G_CZ * n + ie]};
+        double nD[3];
+        for (int a = 0; a < 3; ++a) nD[a] = direct ? p.n[a] : geom[(G_NX + a) * n + ie];
+        const double ws = WS[j * n + ie].x, wd = WD[j * n + ie].x;
+        const double f[3] = {term ? mref[0] : sg, term ? mref[1] : sg, term ? mref[2] : sg};
+        const double gb[3] = {-kI4P * wd * nD[0] * f[0], -kI4P * wd * nD[1] * f[1], -kI4P * wd * nD[2] * f[2]};
+        const double y[3] = {xe[0], xe[1], term ? -xe[2] : xe[2]};
+        double gr[3];
+        res[e * kNearF + dir] = rankine_near_dir(y, p, (term ? sgn : 1.0) * (-kI4P * ws), gb, dir, gr);
+        if (dir == 0)
+            for (int a = 0; a < 3; ++a) res[e * kNearF + 18 + a] = -kI4P * wd * f[a] * gr[a];
+    }
+}
+
+// Each CTA (grid as k_adj_rankine) adds its near-field entries, in list
+// order, to its row and column partials.
+__global__ void __launch_bounds__(kAR)
+k_adj_near_accum(int64_t n, int direct, const unsigned short* __restrict__ ncode, const int64_t* __restrict__ noff,
+                 const double* __restrict__ resg, double* __restrict__ rowpart, double* __restrict__ colpart)
+{
+    __shared__ double res[kNearChunk][kNearF];
+    __shared__ unsigned short codes[kNearChunk];
+    const int tid = threadIdx.x;
+    const int64_t cta = (int64_t)blockIdx.y * gridDim.x + blockIdx.x;
+    const int64_t base = noff[cta];
+    const int total = (int)(noff[cta + 1] - base);
+    if (total == 0) return;
+    const int64_t i = (int64_t)blockIdx.x * kAR + tid;
+    const int64_t j0 = (int64_t)blockIdx.y * kAC;
+    double xb[3] = {0.0, 0.0, 0.0}, nbi[3] = {0.0, 0.0, 0.0};
     double cl[GB_NF];  // this thread's column (tid < kAC) near sums
     for (int f = 0; f < GB_NF; ++f) cl[f] = 0.0;
     for (int c0 = 0; c0 < total; c0 += kNearChunk) {
         const int m = min(kNearChunk, total - c0);
-        for (int w = tid; w < kNearDirs * m; w += blockDim.x) {
-            const int e = w % m, dir = w / m;
-            const int code = list[c0 + e];
-            const int r = code >> 5, bit = code & 31, jj = bit >> 1, term = bit & 1;
-            const int64_t ie = i0 + r, j = j0 + jj;
-            const Panel& p = sp[jj];
-            const double xe[3] = {geom[G_CX * n + ie], geom[G_CY * n + ie], geom[G_CZ * n + ie]};
-            const double* nD = p.n;
-            double nie[3];
-            if (!direct) {
-                nie[0] = geom[G_NX * n + ie];
-                nie[1] = geom[G_NY * n + ie];
-                nie[2] = geom[G_NZ * n + ie];
-                nD = nie;
-            }
-            const double ws = WS[j * n + ie].x, wd = WD[j * n + ie].x;
-            const double f[3] = {term ? mref[0] : sg, term ? mref[1] : sg, term ? mref[2] : sg};
-            const double gb[3] = {-kI4P * wd * nD[0] * f[0], -kI4P * wd * nD[1] * f[1], -kI4P * wd * nD[2] * f[2]};
-            const double y[3] = {xe[0], xe[1], term ? -xe[2] : xe[2]};
-            double gr[3];
-            res[e][dir] = rankine_near_dir(y, p, (term ? sgn : 1.0) * (-kI4P * ws), gb, dir, gr);
-            if (dir == 0)
-                for (int a = 0; a < 3; ++a) res[e][18 + a] = -kI4P * wd * f[a] * gr[a];
-        }
+        for (int t = tid; t < m * kNearF; t += blockDim.x) (&res[0][0])[t] = resg[(base + c0) * kNearF + t];
+        for (int t = tid; t < m; t += blockDim.x) codes[t] = ncode[cta * kNearCap + c0 + t];
         __syncthreads();
         for (int e = 0; e < m; ++e) {
-            const int code = list[c0 + e];
+            const int code = codes[e];
             const int r = code >> 5, bit = code & 31, jj = bit >> 1, term = bit & 1;
             const double* q = res[e];
             if (r == tid) {  // row: y-bar = -(c-bar + sum of vertex bars), mirrored back for the image
@@ -757,20 +852,12 @@ k_adj_rankine(const double* __restrict__ geom, int64_t n, uint32_t mask, int dir
         }
         __syncthreads();
     }
-    if (tid < kAC)
-        for (int f = 0; f < GB_NF; ++f) cnear[tid][f] = cl[f];
-    __syncthreads();
-    for (int t = threadIdx.x; t < jend * GB_NF; t += blockDim.x) {
-        const int jj = t / GB_NF, f = t % GB_NF;
-        double s = cnear[jj][f];
-        if (f < 7)
-            for (int w = 0; w < kAR / 32; ++w) s += csm[w][jj][f];
-        colpart[((int64_t)blockIdx.x * GB_NF + f) * n + j0 + jj] = s;
-    }
-    if (live) {
+    if (tid < kAC && j0 + tid < n)
+        for (int f = 0; f < GB_NF; ++f) colpart[((int64_t)blockIdx.x * GB_NF + f) * n + j0 + tid] += cl[f];
+    if (i < n) {
         for (int c = 0; c < 3; ++c) {
-            rowpart[((int64_t)blockIdx.y * kRowF + c) * n + i] = xb[c];
-            rowpart[((int64_t)blockIdx.y * kRowF + 3 + c) * n + i] = nbi[c];
+            rowpart[((int64_t)blockIdx.y * kRowF + c) * n + i] += xb[c];
+            rowpart[((int64_t)blockIdx.y * kRowF + 3 + c) * n + i] += nbi[c];
         }
     }
 }
@@ -1135,10 +1222,9 @@ int adjoint_mixed_chunk(const Batch& bt, Vjp& vj, const double* d_omegas, const 
                         double tol, int max_iter, FallbackStore& fb, mh_batch_info* info)
 {
     mh_ctx* ctx = bt.ctx;
-    const int64_t n = bt.n, nn = n * n;
+    const int64_t n = bt.n;
     const int nrhs = bt.nrhs;
     const int64_t nv = n * nrhs, cnt = nv * nb;
-    const bool tc = ctx->lu_backend == MH_LU_TCGEN05_F16;
     auto* S64 = (double2*)ctx->ws[WS_S];
     auto* D64 = (double2*)ctx->ws[WS_D];
     auto* Dlo = (float2*)ctx->ws[WS_LO];
@@ -1364,11 +1450,35 @@ int hydro_batch_vjp(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double*
         const unsigned rb = nblk(n, kAR), cb = nblk(n, kAC);
         double* rowpart = vj.part;
         double* colpart = rowpart + (size_t)cb * kRowF * n;
+        const int64_t ncta = (int64_t)rb * cb;
+        auto* nbuf = (char*)ws_get(ctx, WS_NEAR, sizeof(int64_t) * (ncta + 1) + sizeof(int) * ncta +
+                                                     sizeof(unsigned short) * kNearCap * ncta);
+        if (!nbuf) return MH_ERR_OOM;
+        auto* noff = (int64_t*)nbuf;
+        auto* ncount = (int*)(noff + ncta + 1);
+        auto* ncode = (unsigned short*)(ncount + ncta);
         k_adj_rankine<<<dim3(rb, cb), kAR, 0, ctx->stream>>>(m->geom, n, mask, direct, vj.WS, vj.WD, rowpart,
-                                                             colpart);
+                                                             colpart, ncode, ncount);
+        k_near_scan<<<1, 1024, 0, ctx->stream>>>(ncount, ncta, noff);
+        ctx->launches += 2;
+        int64_t total = 0;
+        MH_CUDA_TRY(ctx, cudaMemcpyAsync(&total, noff + ncta, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                                         ctx->stream));
+        MH_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        if (total > 0) {
+            auto* nres = (double*)ws_get(ctx, WS_NEARRES, sizeof(double) * kNearF * (size_t)total);
+            if (!nres) return MH_ERR_OOM;
+            const int64_t items = total * kNearDirs;
+            const unsigned gn = (unsigned)std::min<int64_t>((items + 127) / 128, 148 * 64);
+            k_adj_near<<<gn, 128, 0, ctx->stream>>>(m->geom, n, mask, direct, vj.WS, vj.WD, ncode, noff, ncta,
+                                                    (int)rb, nres);
+            k_adj_near_accum<<<dim3(rb, cb), kAR, 0, ctx->stream>>>(n, direct, ncode, noff, nres, rowpart,
+                                                                    colpart);
+            ctx->launches += 2;
+        }
         k_adj_reduce<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, rowpart, (int)cb, colpart, (int)rb, GB_NF,
                                                             vj.gbar);
-        ctx->launches += 2;
+        ctx->launches += 1;
         phase_end(ctx, PH_ADJ_RANKINE);
         MH_CUDA_TRY(ctx, cudaGetLastError());
     }
