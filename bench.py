@@ -593,7 +593,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--res", type=int, nargs=2, default=[64, 64])
     ap.add_argument("--n-omega", type=int, default=64)
-    ap.add_argument("--tol", type=float, default=1e-10)
+    # relative residual of the FP64 refinement; 1e-8 takes two sweeps and leaves A, B, F within
+    # 4e-10 and the gradients within 2e-8 of the FP64 path (the metric asks 1e-6 and 1e-5)
+    ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--max-iter", type=int, default=30)
     ap.add_argument("--fp64-omegas", type=int, default=8)
     ap.add_argument("--cpu-columns", type=int, default=64)
