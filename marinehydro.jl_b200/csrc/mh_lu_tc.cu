@@ -116,6 +116,17 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
         : "r"(taddr));
 }
 
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+
 __device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols)
 {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -362,6 +373,20 @@ k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int t0, int n
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_slot;
+    // this thread's row of C does not depend on the products: its first 32
+    // columns are loaded while the panel copies and the MMAs run
+    const int64_t gi = r0 + warp * 32 + lane;
+    const bool row_ok = gi >= lo && gi < n;
+    constexpr int kEc = 16;  // columns per epilogue chunk
+    float2 cv[kEc];
+    {
+        const float2* pc = M + c0 * n + gi;
+#pragma unroll
+        for (int q = 0; q < kEc; ++q, pc += n) {
+            const int64_t gj = c0 + q;
+            cv[q] = (row_ok && gj >= lo && gj < n) ? *pc : make_float2(0.f, 0.f);
+        }
+    }
     bool ok = true;     // every wait so far completed
     int pend_ld = -1;   // pair whose copies were issued and not seen complete
     int pend_mma = -1;  // pair whose MMAs were issued and not seen complete
@@ -395,29 +420,35 @@ k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int t0, int n
     }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (ok) {
-        const int64_t gi = r0 + warp * 32 + lane;
-        const bool row_ok = gi >= lo && gi < n;
         const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-#pragma unroll 1
-        for (int cc = 0; cc < TC_TN / 32; ++cc) {
-            uint32_t re[32], im[32];
-            tmem_ld32(lane_base + (uint32_t)(cc * 32), re);
-            tmem_ld32(lane_base + (uint32_t)(TC_TN + cc * 32), im);
+        // chunk cc + 1 of C is loaded before chunk cc is stored
+#pragma unroll
+        for (int cc = 0; cc < TC_TN / kEc; ++cc) {
+            uint32_t re[kEc], im[kEc];
+            tmem_ld16(lane_base + (uint32_t)(cc * kEc), re);
+            tmem_ld16(lane_base + (uint32_t)(TC_TN + cc * kEc), im);
+            float2 nv[kEc];
+            if (cc + 1 < TC_TN / kEc) {
+                const float2* pc = M + (c0 + (cc + 1) * kEc) * n + gi;
+#pragma unroll
+                for (int q = 0; q < kEc; ++q, pc += n) {
+                    const int64_t gj = c0 + (cc + 1) * kEc + q;
+                    nv[q] = (row_ok && gj >= lo && gj < n) ? *pc : make_float2(0.f, 0.f);
+                }
+            }
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (row_ok) {
-                float2 v[32];
+                float2* pc = M + (c0 + cc * kEc) * n + gi;
 #pragma unroll
-                for (int q = 0; q < 32; ++q) {
-                    const int64_t gj = c0 + cc * 32 + q;
-                    v[q] = (gj >= lo && gj < n) ? M[gj * n + gi] : make_float2(0.f, 0.f);
-                }
-#pragma unroll
-                for (int q = 0; q < 32; ++q) {
-                    const int64_t gj = c0 + cc * 32 + q;
+                for (int q = 0; q < kEc; ++q, pc += n) {
+                    const int64_t gj = c0 + cc * kEc + q;
                     if (gj >= lo && gj < n)
-                        M[gj * n + gi] = make_float2(v[q].x - __uint_as_float(re[q]),
-                                                     v[q].y - __uint_as_float(im[q]));
+                        *pc = make_float2(cv[q].x - __uint_as_float(re[q]), cv[q].y - __uint_as_float(im[q]));
                 }
+            }
+            if (cc + 1 < TC_TN / kEc) {
+#pragma unroll
+                for (int q = 0; q < kEc; ++q) cv[q] = nv[q];
             }
         }
     } else {
