@@ -331,19 +331,24 @@ k_lu_trsm_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
     if (warp == 0) tmem_dealloc(tmem, 128);
 }
 
+// Packed panel pairs of one update (one per 64-column panel).
+constexpr int kMaxPairs = 4;
+struct PanelPairs {
+    const unsigned char* L[kMaxPairs];
+    const unsigned char* U[kMaxPairs];
+};
+
 // A22 -= sum_p L21_p U12_p for one 128 x 128 complex tile (absolute tiles
-// ti, tj); the operands are the packed panels of k_lu_trsm_tc (npair = 1 or
-// 2 panel pairs, K = 64 complex each), fetched by cp.async.bulk into shared
+// ti, tj); the operands are the packed panels of k_lu_trsm_tc (npair <= 4
+// panel pairs, K = 64 complex each), fetched by cp.async.bulk into shared
 // memory one pair at a time and accumulated in tensor memory.  Only rows and
-// columns >= lo are written.
-// mode 0: tiles t0 + (bx, by) (grid ntile x ntile); mode 1: tile row t0 and
-// tile column t0 (grid 2 ntile - 1, the part the next panel depends on);
-// mode 2: tiles t0 + 1 + (bx, by) (grid (ntile - 1)^2).
+// columns >= lo are written.  Tiles, relative to t0 (ntile of them per side):
+// mode 1: the first w tile rows and tile columns (an L of width w; grid
+// w (2 ntile - w), the part the next panels depend on); mode 2: the tiles
+// past them (grid (ntile - w)^2).
 __global__ void __launch_bounds__(128, 2)
-k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int t0, int ntile, int mode,
-               const unsigned char* __restrict__ Lp0, const unsigned char* __restrict__ Up0,
-               const unsigned char* __restrict__ Lp1, const unsigned char* __restrict__ Up1, int npair,
-               int64_t pstride, int64_t lo, int* __restrict__ bad)
+k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int t0, int ntile, int mode, int w,
+               PanelPairs pp, int npair, int64_t pstride, int64_t lo, int* __restrict__ bad)
 {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
     __shared__ uint64_t mbar[2];
@@ -352,13 +357,20 @@ k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int t0, int n
     unsigned char* sB = tc_smem + kSmemA;
     const int b = blockIdx.z;
     float2* M = Ab + (int64_t)b * stride;
-    int ti = t0 + (int)blockIdx.x, tj = t0 + (int)blockIdx.y;
+    int ti, tj;
     if (mode == 1) {
-        ti = (int)blockIdx.x < ntile ? t0 + (int)blockIdx.x : t0;
-        tj = (int)blockIdx.x < ntile ? t0 : t0 + (int)blockIdx.x - ntile + 1;
-    } else if (mode == 2) {
-        ti = t0 + 1 + (int)blockIdx.x;
-        tj = t0 + 1 + (int)blockIdx.y;
+        const int x = (int)blockIdx.x;
+        if (x < w * ntile) {
+            ti = t0 + x / ntile;
+            tj = t0 + x % ntile;
+        } else {
+            const int y = x - w * ntile, rest = ntile - w;
+            tj = t0 + y / rest;
+            ti = t0 + w + y % rest;
+        }
+    } else {
+        ti = t0 + w + (int)blockIdx.x;
+        tj = t0 + w + (int)blockIdx.y;
     }
     const int64_t r0 = (int64_t)ti * TC_TM;
     const int64_t c0 = (int64_t)tj * TC_TN;
@@ -393,8 +405,8 @@ k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int t0, int n
 #pragma unroll 1
     for (int p = 0; p < npair && ok; ++p) {
         if (tid == 0) {
-            const unsigned char* srcA = (p == 0 ? Lp0 : Lp1) + (int64_t)b * pstride + (int64_t)ti * kPanelL;
-            const unsigned char* srcB = (p == 0 ? Up0 : Up1) + (int64_t)b * pstride + (int64_t)tj * kPanelU;
+            const unsigned char* srcA = pp.L[p] + (int64_t)b * pstride + (int64_t)ti * kPanelL;
+            const unsigned char* srcB = pp.U[p] + (int64_t)b * pstride + (int64_t)tj * kPanelU;
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
                          :: "r"(bar_ld), "r"(kPanelL + kPanelU) : "memory");
             constexpr uint32_t kChunk = 16384;
@@ -1115,27 +1127,35 @@ k_lu_solve_flags(const float2* __restrict__ A, int64_t n, int64_t stride, const 
 
 int64_t lu_dinv_stride_tc(int64_t n) { return ((n + TC_NB - 1) / TC_NB) * 2 * TC_NB * TC_NB; }
 
-// Four panel buffers per matrix: both panel pairs of an outer step stay live
-// while its interior update runs, and the next outer step writes the other two.
-int64_t lu_panel_bytes_tc(int64_t n) { return 4 * ((n + TC_TM - 1) / TC_TM) * (int64_t)(kPanelL + kPanelU); }
+// Eight panel buffers per matrix: the four panel pairs of an outer step stay
+// live while its interior update runs, and the next outer step writes the
+// other four.
+constexpr int kOuterPanels = 4;  // 64-column panels per outer step (256 columns)
+int64_t lu_panel_bytes_tc(int64_t n)
+{
+    return 2 * kOuterPanels * ((n + TC_TM - 1) / TC_TM) * (int64_t)(kPanelL + kPanelU);
+}
 
-// Blocked LU in outer steps of 128 columns (two 64-column panels), with
+// Blocked LU in outer steps of 256 columns (four 64-column panels), with
 // look-ahead.  Outer step K0 (tile T0 = K0 / 128), on the main
-// (high-priority) stream: TRSM of panel K0, update of tile row and column
-// T0 with that panel (rows, columns >= K0 + 64), diagonal block K0 + 64,
-// TRSM of panel K0 + 64; then the trailing tiles (>= T0 + 1) are updated
-// with both panel pairs at once (K = 128 complex): tile row and column
-// T0 + 1 on the main stream, the interior concurrently on the side
+// (high-priority) stream: for each panel k = K0 + 64 s, its TRSM, then (but
+// for the last) the update of the rest of the outer block's tile rows and
+// columns (an L of width T0 + 2 - tile(k + 64) tiles, rows and columns
+// >= k + 64) with that panel alone, and the next diagonal block; then the
+// trailing tiles (>= T0 + 2) are updated once with all four panel pairs
+// accumulated in TMEM (K = 256 complex): their first two tile rows and
+// columns on the main stream, the interior concurrently on the side
 // (low-priority) stream, then the next diagonal block.  The trailing matrix
-// is read and written once per 128 columns.  An outer step's trailing update
-// waits for the previous interior; everything before it only touches tile
-// row and column T0, which that interior does not.
+// is read and written once per 256 columns.  An outer step's trailing
+// update waits for the previous interior; everything before it only touches
+// tile rows and columns T0, T0 + 1, which that interior does not.
 cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int nbatch, float2* Dinv,
                          unsigned char* panels, int* bad)
 {
     cudaError_t e;
     static_assert(TC_NB == 64, "the diagonal blocks are factored by k_lu_diag64");
-    static_assert(TC_TM == 2 * TC_NB && TC_TN == TC_TM, "an outer step spans one 128-wide tile");
+    static_assert(TC_TM == 2 * TC_NB && TC_TN == TC_TM, "two panels per 128-wide tile");
+    static_assert(kOuterPanels <= kMaxPairs && kOuterPanels == 4, "an outer step spans two tiles");
     if ((e = cudaFuncSetAttribute(k_lu_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kTcSmemBytes)) != cudaSuccess)
         return e;
@@ -1143,53 +1163,65 @@ cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int 
                                   (int)(kSmemA + kSmemA))) != cudaSuccess)
         return e;
     const int64_t dstride = lu_dinv_stride_tc(n);
-    const int64_t pstride = lu_panel_bytes_tc(n) / 4;  // one buffer, per matrix
+    const int64_t pstride = lu_panel_bytes_tc(n) / (2 * kOuterPanels);  // one buffer, per matrix
     const int ntiles = (int)((n + TC_TM - 1) / TC_TM);
     const unsigned nbz = (unsigned)nbatch;
+    constexpr int kW = kOuterPanels / 2;  // tiles per outer step
     cudaStream_t main_s = ctx->stream, side_s = ctx->side;
     if ((e = cudaEventRecord(ctx->ev_side, side_s)) != cudaSuccess) return e;
     k_lu_diag64<<<nbatch, kDiag64Threads, 0, main_s>>>(A, n, stride, 0, Dinv, dstride, bad);
     ctx->launches += 1;
     int outer = 0;
-    for (int64_t K0 = 0; K0 < n; K0 += 2 * TC_NB, ++outer) {
+    for (int64_t K0 = 0; K0 < n; K0 += kOuterPanels * TC_NB, ++outer) {
         const int T0 = (int)(K0 / TC_TM);
-        unsigned char* Lp[2];
-        unsigned char* Up[2];
-        for (int s = 0; s < 2; ++s) {
-            Lp[s] = panels + (int64_t)(2 * (outer & 1) + s) * pstride * nbatch;
-            Up[s] = Lp[s] + (int64_t)ntiles * kPanelL;
+        PanelPairs pp;
+        for (int s = 0; s < kOuterPanels; ++s) {
+            pp.L[s] = panels + (int64_t)(kOuterPanels * (outer & 1) + s) * pstride * nbatch;
+            pp.U[s] = pp.L[s] + (int64_t)ntiles * kPanelL;
         }
-        // panel K0 and the rest of tile row / column T0
-        if (n - K0 - TC_NB <= 0) break;
-        const int nt0 = ntiles - T0;
-        k_lu_trsm_tc<<<dim3(2 * nt0, nbz), 128, kSmemA + kSmemA, main_s>>>(
-            A, n, stride, K0, Dinv, dstride, Lp[0], Up[0], pstride, nt0, bad);
-        k_lu_update_tc<<<dim3(2 * nt0 - 1, 1, nbz), 128, kTcSmemBytes, main_s>>>(
-            A, n, stride, T0, nt0, 1, Lp[0], Up[0], Lp[0], Up[0], 1, pstride, K0 + TC_NB, bad);
-        k_lu_diag64<<<nbatch, kDiag64Threads, 0, main_s>>>(A, n, stride, K0 + TC_NB, Dinv, dstride, bad);
-        ctx->launches += 3;
-        // panel K0 + 64, then the trailing tiles with both panels
-        if (n - K0 - 2 * TC_NB <= 0) break;
-        const int nt1 = ntiles - (T0 + 1);
-        k_lu_trsm_tc<<<dim3(2 * nt1, nbz), 128, kSmemA + kSmemA, main_s>>>(
-            A, n, stride, K0 + TC_NB, Dinv, dstride, Lp[1], Up[1], pstride, nt1, bad);
-        ctx->launches += 1;
+        bool done = false;
+        for (int s = 0; s < kOuterPanels; ++s) {
+            const int64_t k = K0 + (int64_t)s * TC_NB;
+            if (n - k - TC_NB <= 0) {
+                done = true;
+                break;
+            }
+            const int t0 = (int)((k + TC_NB) / TC_TM), nt = ntiles - t0;
+            k_lu_trsm_tc<<<dim3(2 * nt, nbz), 128, kSmemA + kSmemA, main_s>>>(
+                A, n, stride, k, Dinv, dstride, (unsigned char*)pp.L[s], (unsigned char*)pp.U[s], pstride, nt, bad);
+            ctx->launches += 1;
+            if (s + 1 < kOuterPanels) {  // the rest of the outer block with this panel, then its next diagonal block
+                PanelPairs one;
+                one.L[0] = pp.L[s];
+                one.U[0] = pp.U[s];
+                const int w = std::min(T0 + kW - t0, nt);
+                k_lu_update_tc<<<dim3(w * (2 * nt - w), 1, nbz), 128, kTcSmemBytes, main_s>>>(
+                    A, n, stride, t0, nt, 1, w, one, 1, pstride, k + TC_NB, bad);
+                k_lu_diag64<<<nbatch, kDiag64Threads, 0, main_s>>>(A, n, stride, k + TC_NB, Dinv, dstride, bad);
+                ctx->launches += 2;
+            }
+        }
+        if (done) break;
+        // trailing tiles >= T0 + kW with all four panel pairs
+        const int64_t lo = K0 + (int64_t)kOuterPanels * TC_NB;
+        const int t0 = T0 + kW, nt = ntiles - t0;
+        if (nt <= 0) break;
         // the previous interior update is done before this trailing update
         if ((e = cudaStreamWaitEvent(main_s, ctx->ev_side, 0)) != cudaSuccess) return e;
         if ((e = cudaEventRecord(ctx->ev_panel, main_s)) != cudaSuccess) return e;
         if ((e = cudaStreamWaitEvent(side_s, ctx->ev_panel, 0)) != cudaSuccess) return e;
-        if (nt1 > 1) {
-            k_lu_update_tc<<<dim3(nt1 - 1, nt1 - 1, nbz), 128, kTcSmemBytes, side_s>>>(
-                A, n, stride, T0 + 1, nt1, 2, Lp[0], Up[0], Lp[1], Up[1], 2, pstride, K0 + 2 * TC_NB, bad);
+        const int w = std::min(kW, nt);
+        if (nt > w) {
+            k_lu_update_tc<<<dim3(nt - w, nt - w, nbz), 128, kTcSmemBytes, side_s>>>(
+                A, n, stride, t0, nt, 2, w, pp, kOuterPanels, pstride, lo, bad);
             ctx->launches += 1;
         }
         if ((e = cudaEventRecord(ctx->ev_side, side_s)) != cudaSuccess) return e;
-        k_lu_update_tc<<<dim3(2 * nt1 - 1, 1, nbz), 128, kTcSmemBytes, main_s>>>(
-            A, n, stride, T0 + 1, nt1, 1, Lp[0], Up[0], Lp[1], Up[1], 2, pstride, K0 + 2 * TC_NB, bad);
+        k_lu_update_tc<<<dim3(w * (2 * nt - w), 1, nbz), 128, kTcSmemBytes, main_s>>>(
+            A, n, stride, t0, nt, 1, w, pp, kOuterPanels, pstride, lo, bad);
         ctx->launches += 1;
-        if (K0 + 2 * TC_NB < n) {
-            k_lu_diag64<<<nbatch, kDiag64Threads, 0, main_s>>>(A, n, stride, K0 + 2 * TC_NB, Dinv, dstride,
-                                                                 bad);
+        if (lo < n) {
+            k_lu_diag64<<<nbatch, kDiag64Threads, 0, main_s>>>(A, n, stride, lo, Dinv, dstride, bad);
             ctx->launches += 1;
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
