@@ -117,23 +117,32 @@ k_lu_diag(float2* __restrict__ A, int64_t n, int64_t stride, int64_t k0, float2*
 // barrier, then the owner of column c in each row turns it into L(r, c) and
 // passes it to the rest of the row by a warp shuffle, and every row below c
 // updates its columns right of c.  The column group of step c is kept in
-// register b[0] by rotating b after every eight steps, so the step loop
+// register a[0] by rotating a after every eight steps, so the step loop
 // needs no dynamic register index and only eight steps are unrolled.  The
-// two triangular inverses then run together from the factored block in
-// shared memory, inv(L) by rows ascending and inv(U) by rows descending, one
-// barrier per step.  The block is padded with the identity, so all 64 steps
-// run for any kb <= 64 and the padding stays the identity.  Same outputs as
-// k_lu_diag.
+// two triangular inverses are then built by recursive doubling from the
+// factored block in shared memory: with the inverses of the diagonal blocks
+// A and C of size s known, [A 0; B C]^-1 has the off-diagonal block
+// -inv(C) B inv(A) (and [A B; 0 C]^-1 has -inv(A) B inv(C)), two small
+// products per level, s = 1, 2, ..., 32: twelve barriers instead of one per
+// row.  The block is padded with the identity, so all 64 steps run for any
+// kb <= 64 and the padding stays the identity.  Same outputs as k_lu_diag.
 constexpr int kDiag64Threads = 512;
+// dynamic shared memory: the factored block, the inverses (inv(L) strictly
+// below the diagonal, inv(U) on and above), two product buffers
+constexpr int kDiagLd = 65;
+constexpr size_t kDiag64Smem = sizeof(float2) * (2 * 64 * kDiagLd + 2 * 32 * 32 * 2);
 
 __global__ void __launch_bounds__(kDiag64Threads)
 k_lu_diag64(float2* __restrict__ A, int64_t n, int64_t stride, int64_t k0, float2* __restrict__ Dinv,
             int64_t dstride, int* __restrict__ bad)
 {
     constexpr int NB = 64;
-    __shared__ float2 f[NB][NB + 1];         // factored block
-    __shared__ float2 ur[2][NB];             // row c of U, step c
-    __shared__ float2 bl[2][NB], bu[2][NB];  // rows of inv(L) and inv(U)
+    extern __shared__ float2 diag_smem[];
+    auto f = reinterpret_cast<float2 (*)[kDiagLd]>(diag_smem);                 // factored block
+    auto x = reinterpret_cast<float2 (*)[kDiagLd]>(diag_smem + NB * kDiagLd);  // the two inverses
+    float2* tl_buf = diag_smem + 2 * NB * kDiagLd;                               // products
+    float2* tu_buf = tl_buf + 2 * 32 * 32;
+    __shared__ float2 ur[2][NB];  // row c of U, step c
     const int64_t b = blockIdx.x;
     float2* M = A + b * stride;
     const int kb = (int)min((int64_t)NB, n - k0);
@@ -182,43 +191,67 @@ k_lu_diag64(float2* __restrict__ A, int64_t n, int64_t stride, int64_t k0, float
         if (r < kb && c < kb) M[(k0 + c) * n + k0 + r] = a[m];
     }
     __syncthreads();
-    // inverses: WL = inv(L) (unit lower), WU = inv(U)
-    float2 WL[8], WU[8];
-#pragma unroll
-    for (int m = 0; m < 8; ++m) WL[m] = WU[m] = make_float2(r == g + 8 * m ? 1.f : 0.f, 0.f);
-    const float2 ird = cdivf(make_float2(1.f, 0.f), f[r][r]);
+    // inverses by recursive doubling; x starts as the inverse diagonal of U
+    for (int e = t; e < NB * NB; e += blockDim.x) {
+        const int i = e / NB, j = e % NB;
+        x[i][j] = i == j ? cdivf(make_float2(1.f, 0.f), f[i][i]) : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
 #pragma unroll 1
-    for (int s = 0; s < NB; ++s) {
-        const int tl = s, tu = NB - 1 - s, buf = s & 1;
-        if (r == tl) {
-#pragma unroll
-            for (int m = 0; m < 8; ++m) bl[buf][g + 8 * m] = WL[m];
-        }
-        if (r == tu) {
-#pragma unroll
-            for (int m = 0; m < 8; ++m) {
-                WU[m] = cmulf(WU[m], ird);
-                bu[buf][g + 8 * m] = WU[m];
+    for (int sz = 1; sz < NB; sz *= 2) {
+        const int items = (NB / (2 * sz)) * sz * sz;  // outputs per triangle and phase
+        // phase 1: -L[C,A] inv(L)[A,A] and -U[A,C] inv(U)[C,C]
+        for (int e = t; e < 2 * items; e += blockDim.x) {
+            const bool up = e >= items;
+            const int ee = up ? e - items : e;
+            const int pr = ee / (sz * sz), i = (ee / sz) % sz, j = ee % sz;
+            const int a0 = 2 * sz * pr, c0 = a0 + sz;
+            float2 acc = make_float2(0.f, 0.f);
+            if (!up) {  // row c0 + i, column a0 + j; inv(L) is 1 on the diagonal
+                for (int u = j; u < sz; ++u) {
+                    const float2 xl = u == j ? make_float2(1.f, 0.f) : x[a0 + u][a0 + j];
+                    acc = cfms(acc, f[c0 + i][a0 + u], xl);
+                }
+                tl_buf[ee] = acc;
+            } else {  // row a0 + i, column c0 + j; inv(U)[u][j] for u <= j
+                for (int u = 0; u <= j; ++u) acc = cfms(acc, f[a0 + i][c0 + u], x[c0 + u][c0 + j]);
+                tu_buf[ee] = acc;
             }
         }
         __syncthreads();
-        if (r > tl) {
-            const float2 lt = f[r][tl];
-#pragma unroll
-            for (int m = 0; m < 8; ++m) WL[m] = cfms(WL[m], lt, bl[buf][g + 8 * m]);
+        // phase 2: inv(L)[C,A] = inv(L)[C,C] (phase 1), inv(U)[A,C] = inv(U)[A,A] (phase 1)
+        for (int e = t; e < 2 * items; e += blockDim.x) {
+            const bool up = e >= items;
+            const int ee = up ? e - items : e;
+            const int pr = ee / (sz * sz), i = (ee / sz) % sz, j = ee % sz;
+            const int a0 = 2 * sz * pr, c0 = a0 + sz;
+            const float2* T = (up ? tu_buf : tl_buf) + pr * sz * sz;
+            float2 acc = make_float2(0.f, 0.f);
+            if (!up) {  // inv(L)[c0+i][c0+u] for u <= i (1 on the diagonal)
+                for (int u = 0; u <= i; ++u) {
+                    const float2 xl = u == i ? make_float2(1.f, 0.f) : x[c0 + i][c0 + u];
+                    const float2 tv = T[u * sz + j];
+                    acc.x += xl.x * tv.x - xl.y * tv.y;
+                    acc.y += xl.x * tv.y + xl.y * tv.x;
+                }
+                x[c0 + i][a0 + j] = acc;
+            } else {  // inv(U)[a0+i][a0+u] for u >= i
+                for (int u = i; u < sz; ++u) {
+                    const float2 xu = x[a0 + i][a0 + u];
+                    const float2 tv = T[u * sz + j];
+                    acc.x += xu.x * tv.x - xu.y * tv.y;
+                    acc.y += xu.x * tv.y + xu.y * tv.x;
+                }
+                x[a0 + i][c0 + j] = acc;
+            }
         }
-        if (r < tu) {
-            const float2 ut = f[r][tu];
-#pragma unroll
-            for (int m = 0; m < 8; ++m) WU[m] = cfms(WU[m], ut, bu[buf][g + 8 * m]);
-        }
+        __syncthreads();
     }
     float2* out = Dinv + b * dstride + (k0 / NB) * 2 * NB * NB;
-#pragma unroll
-    for (int m = 0; m < 8; ++m) {
-        const int c = g + 8 * m;
-        out[c * NB + r] = WL[m];
-        out[NB * NB + c * NB + r] = WU[m];
+    for (int e = t; e < NB * NB; e += blockDim.x) {
+        const int c = e / NB, rr = e % NB;
+        out[e] = rr == c ? make_float2(1.f, 0.f) : (rr > c ? x[rr][c] : make_float2(0.f, 0.f));
+        out[NB * NB + e] = rr <= c ? x[rr][c] : make_float2(0.f, 0.f);
     }
 }
 

@@ -1162,6 +1162,9 @@ cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int 
     if ((e = cudaFuncSetAttribute(k_lu_trsm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(kSmemA + kSmemA))) != cudaSuccess)
         return e;
+    if ((e = cudaFuncSetAttribute(k_lu_diag64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kDiag64Smem)) != cudaSuccess)
+        return e;
     const int64_t dstride = lu_dinv_stride_tc(n);
     const int64_t pstride = lu_panel_bytes_tc(n) / (2 * kOuterPanels);  // one buffer, per matrix
     const int ntiles = (int)((n + TC_TM - 1) / TC_TM);
@@ -1169,7 +1172,7 @@ cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int 
     constexpr int kW = kOuterPanels / 2;  // tiles per outer step
     cudaStream_t main_s = ctx->stream, side_s = ctx->side;
     if ((e = cudaEventRecord(ctx->ev_side, side_s)) != cudaSuccess) return e;
-    k_lu_diag64<<<nbatch, kDiag64Threads, 0, main_s>>>(A, n, stride, 0, Dinv, dstride, bad);
+    k_lu_diag64<<<nbatch, kDiag64Threads, kDiag64Smem, main_s>>>(A, n, stride, 0, Dinv, dstride, bad);
     ctx->launches += 1;
     int outer = 0;
     for (int64_t K0 = 0; K0 < n; K0 += kOuterPanels * TC_NB, ++outer) {
@@ -1197,7 +1200,7 @@ cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int 
                 const int w = std::min(T0 + kW - t0, nt);
                 k_lu_update_tc<<<dim3(w * (2 * nt - w), 1, nbz), 128, kTcSmemBytes, main_s>>>(
                     A, n, stride, t0, nt, 1, w, one, 1, pstride, k + TC_NB, bad);
-                k_lu_diag64<<<nbatch, kDiag64Threads, 0, main_s>>>(A, n, stride, k + TC_NB, Dinv, dstride, bad);
+                k_lu_diag64<<<nbatch, kDiag64Threads, kDiag64Smem, main_s>>>(A, n, stride, k + TC_NB, Dinv, dstride, bad);
                 ctx->launches += 2;
             }
         }
@@ -1221,7 +1224,7 @@ cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int 
             A, n, stride, t0, nt, 1, w, pp, kOuterPanels, pstride, lo, bad);
         ctx->launches += 1;
         if (lo < n) {
-            k_lu_diag64<<<nbatch, kDiag64Threads, 0, main_s>>>(A, n, stride, lo, Dinv, dstride, bad);
+            k_lu_diag64<<<nbatch, kDiag64Threads, kDiag64Smem, main_s>>>(A, n, stride, lo, Dinv, dstride, bad);
             ctx->launches += 1;
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
