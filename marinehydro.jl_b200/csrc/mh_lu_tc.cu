@@ -986,8 +986,9 @@ __device__ __forceinline__ void fs_rowdot(const float2 (&m)[kFsPer], const float
     }
 }
 
-// x_i -= T_ik y for the tile held in m (rows of block i).
-__device__ __forceinline__ void fs_apply(const float2 (&m)[kFsPer], int64_t n, int i, float2* x,
+// x_i -= T_ik y for the tile held in m; entry (q, r) of block i at
+// xb[q * xq + r] (global memory or the CTA's shared copy).
+__device__ __forceinline__ void fs_apply(const float2 (&m)[kFsPer], int64_t n, int i, float2* xb, int64_t xq,
                                          const float2 (*y)[64], int nrhs)
 {
     const int r = threadIdx.x / kFsLanes, tq = threadIdx.x % kFsLanes;
@@ -998,7 +999,7 @@ __device__ __forceinline__ void fs_apply(const float2 (&m)[kFsPer], int64_t n, i
         fs_rowdot(m, y, q0, nq, ax, ay);
         if (tq == 0 && row < n)
             for (int qq = 0; qq < nq; ++qq) {
-                float2* p = x + (int64_t)(q0 + qq) * n + row;
+                float2* p = xb + (q0 + qq) * xq + r;
                 const float2 v = *p;
                 *p = make_float2(v.x - ax[qq], v.y - ay[qq]);
             }
@@ -1006,7 +1007,7 @@ __device__ __forceinline__ void fs_apply(const float2 (&m)[kFsPer], int64_t n, i
 }
 
 // y_i = inv(T_ii) v (v complete in vs, inverse entries in iv), into ynext and
-// over x_i; then publish.
+// over x_i; then publish.  vs may be the CTA's shared copy of block i.
 __device__ __forceinline__ void fs_solve_publish(const float2 (&iv)[kFsPer], int64_t n, int i, float2* x,
                                                  const float2 (*vs)[64], float2 (*ynext)[64], int nrhs, int* flag)
 {
@@ -1031,15 +1032,20 @@ __device__ __forceinline__ void fs_solve_publish(const float2 (&iv)[kFsPer], int
     }
 }
 
-template <bool kCT>
+// kXS: the x entries of the CTA's own blocks live in shared memory (dynamic,
+// ceil(nblk / kFsCluster) * nrhs * 64 entries) from the start to the end of
+// the kernel, so the tile products update them without global round trips;
+// each solved block is still written to global memory when published.
+template <bool kCT, bool kXS>
 __global__ void __cluster_dims__(kFsCluster, 1, 1) __launch_bounds__(kFsThreads, 2)
 k_lu_solve_flags(const float2* __restrict__ A, int64_t n, int64_t stride, const float2* __restrict__ Dinv,
                  int64_t dstride, float2* X, int64_t xstride, int nrhs, int* flags, int* bad)
 {
     constexpr int NB = 64;
     __shared__ float2 ys[2][kMaxRhs][NB];  // y of the block being applied and of the next one
-    __shared__ float2 vs[kMaxRhs][NB];     // x of the block being solved
+    __shared__ float2 vs[kMaxRhs][NB];     // x of the block being solved (global x)
     __shared__ int s_fail;
+    extern __shared__ float2 xs_smem[];    // kXS: [own block][nrhs][NB]
     const int64_t b = blockIdx.x / kFsCluster;
     const int rank = (int)cluster_rank();
     const float2* M = A + b * stride;
@@ -1048,7 +1054,22 @@ k_lu_solve_flags(const float2* __restrict__ A, int64_t n, int64_t stride, const 
     const int nblk = (int)((n + NB - 1) / NB);
     int* fl = flags + b * 2 * nblk;
     const int tid = threadIdx.x;
+    // block i's entries (q, r) at xblk(i)[q * xq + r]
+    const int64_t xq = kXS ? NB : n;
+    auto xblk = [&](int i) -> float2* {
+        return kXS ? xs_smem + (int64_t)(i / kFsCluster) * nrhs * NB : x + (int64_t)i * NB;
+    };
     if (tid == 0) s_fail = 0;
+    if (kXS) {
+        for (int i = rank; i < nblk; i += kFsCluster) {
+            float2* xb = xblk(i);
+            const int64_t i0 = (int64_t)i * NB;
+            for (int e = tid; e < nrhs * NB; e += blockDim.x) {
+                const int q = e / NB, rr = e % NB;
+                xb[q * NB + rr] = i0 + rr < n ? x[(int64_t)q * n + i0 + rr] : make_float2(0.f, 0.f);
+            }
+        }
+    }
     __syncthreads();
     for (int tri = 0; tri < 2; ++tri) {
         const bool fwd = tri == 0;
@@ -1056,17 +1077,28 @@ k_lu_solve_flags(const float2* __restrict__ A, int64_t n, int64_t stride, const 
         const int inv_off = (fwd != kCT) ? 0 : NB * NB;
         int* tfl = fl + tri * nblk;
         const int k_first = fwd ? 0 : nblk - 1;
-        if (k_first % kFsCluster == rank) {  // the first block: x is complete
+        // solve block i from its complete x (shared copy or staged), publish, keep y in ynext
+        auto solve_own = [&](int i, float2 (*ynext)[NB]) {
             float2 iv[kFsPer];
-            fs_load_inv<kCT>(Dv + (int64_t)k_first * 2 * NB * NB + inv_off, iv);
-            const int64_t f0 = (int64_t)k_first * NB;
-            for (int e = tid; e < nrhs * NB; e += blockDim.x) {
-                const int q = e / NB, rr = e % NB;
-                vs[q][rr] = f0 + rr < n ? x[(int64_t)q * n + f0 + rr] : make_float2(0.f, 0.f);
+            fs_load_inv<kCT>(Dv + (int64_t)i * 2 * NB * NB + inv_off, iv);
+            const float2 (*src)[NB] = vs;
+            if (kXS) {
+                src = reinterpret_cast<const float2 (*)[NB]>(xblk(i));
+            } else {
+                const int64_t f0 = (int64_t)i * NB;
+                for (int e = tid; e < nrhs * NB; e += blockDim.x) {
+                    const int q = e / NB, rr = e % NB;
+                    vs[q][rr] = f0 + rr < n ? x[(int64_t)q * n + f0 + rr] : make_float2(0.f, 0.f);
+                }
             }
             __syncthreads();
-            fs_solve_publish(iv, n, k_first, x, vs, ys[0], nrhs, tfl + k_first);
-        }
+            fs_solve_publish(iv, n, i, x, src, ynext, nrhs, tfl + i);
+            if (kXS) {  // the solved block becomes the next triangle's right-hand side
+                float2* xb = xblk(i);
+                for (int e = tid; e < nrhs * NB; e += blockDim.x) xb[e] = ynext[e / NB][e % NB];
+            }
+        };
+        if (k_first % kFsCluster == rank) solve_own(k_first, ys[0]);
         for (int p = 0; p < nblk; ++p) {
             const int k = fwd ? p : nblk - 1 - p;
             const int kn = fwd ? k + 1 : k - 1;
@@ -1092,17 +1124,8 @@ k_lu_solve_flags(const float2* __restrict__ A, int64_t n, int64_t stride, const 
             if (next_mine) {  // the next block first: apply y_k to it, solve, publish
                 float2 m[kFsPer];
                 fs_load<kCT>(M, n, kn, k, m);
-                fs_apply(m, n, kn, x, y, nrhs);
-                float2 iv[kFsPer];
-                fs_load_inv<kCT>(Dv + (int64_t)kn * 2 * NB * NB + inv_off, iv);
-                __syncthreads();
-                const int64_t f0 = (int64_t)kn * NB;
-                for (int e = tid; e < nrhs * NB; e += blockDim.x) {
-                    const int q = e / NB, rr = e % NB;
-                    vs[q][rr] = f0 + rr < n ? x[(int64_t)q * n + f0 + rr] : make_float2(0.f, 0.f);
-                }
-                __syncthreads();
-                fs_solve_publish(iv, n, kn, x, vs, ys[(p + 1) & 1], nrhs, tfl + kn);
+                fs_apply(m, n, kn, xblk(kn), xq, y, nrhs);
+                solve_own(kn, ys[(p + 1) & 1]);
             }
             // the rest of this CTA's blocks after kn in the triangle's order, two tiles in flight
             int q = p + 2;
@@ -1110,11 +1133,12 @@ k_lu_solve_flags(const float2* __restrict__ A, int64_t n, int64_t stride, const 
             for (; q < nblk; q += 2 * kFsCluster) {
                 const int i1 = fwd ? q : nblk - 1 - q;
                 const int q2 = q + kFsCluster;
+                const int i2 = fwd ? q2 : nblk - 1 - q2;
                 float2 m1[kFsPer], m2[kFsPer];
                 fs_load<kCT>(M, n, i1, k, m1);
-                if (q2 < nblk) fs_load<kCT>(M, n, fwd ? q2 : nblk - 1 - q2, k, m2);
-                fs_apply(m1, n, i1, x, y, nrhs);
-                if (q2 < nblk) fs_apply(m2, n, fwd ? q2 : nblk - 1 - q2, x, y, nrhs);
+                if (q2 < nblk) fs_load<kCT>(M, n, i2, k, m2);
+                fs_apply(m1, n, i1, xblk(i1), xq, y, nrhs);
+                if (q2 < nblk) fs_apply(m2, n, i2, xblk(i2), xq, y, nrhs);
             }
         }
         __syncthreads();
@@ -1297,12 +1321,19 @@ cudaError_t launch_lu_solve_persist(mh_ctx* ctx, int backend, bool conj_trans, c
         int* fbad = flags + 2 * nblk * nbatch;
         if ((e = cudaMemsetAsync(flags, 0, fbytes, ctx->stream)) != cudaSuccess) return e;
         const dim3 gf((unsigned)nbatch * kFsCluster);
-        if (conj_trans)
-            k_lu_solve_flags<true><<<gf, kFsThreads, 0, ctx->stream>>>(A, n, stride, Dinv, ds, X, xstride, nrhs,
-                                                                      flags, fbad);
-        else
-            k_lu_solve_flags<false><<<gf, kFsThreads, 0, ctx->stream>>>(A, n, stride, Dinv, ds, X, xstride, nrhs,
-                                                                       flags, fbad);
+        const size_t xsb = sizeof(float2) * (size_t)((nblk + kFsCluster - 1) / kFsCluster) * nrhs * TC_NB;
+        const bool shared_x = xsb <= 96 * 1024;
+        auto go = [&](auto kern, size_t smem) -> cudaError_t {
+            cudaError_t e2;
+            if (smem && (e2 = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
+                            cudaSuccess)
+                return e2;
+            kern<<<gf, kFsThreads, smem, ctx->stream>>>(A, n, stride, Dinv, ds, X, xstride, nrhs, flags, fbad);
+            return cudaSuccess;
+        };
+        if (conj_trans) e = shared_x ? go(k_lu_solve_flags<true, true>, xsb) : go(k_lu_solve_flags<true, false>, 0);
+        else e = shared_x ? go(k_lu_solve_flags<false, true>, xsb) : go(k_lu_solve_flags<false, false>, 0);
+        if (e != cudaSuccess) return e;
     } else {
         const int64_t ds = lu_dinv_stride(n);
         const size_t sm = persist_smem_bytes<32>();
