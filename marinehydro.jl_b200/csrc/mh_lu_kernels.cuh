@@ -6,6 +6,7 @@
 // Dinv holds, per matrix and diagonal block, inv(L11) then inv(U11), each
 // NB x NB column-major.
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -110,6 +111,43 @@ k_lu_diag(float2* __restrict__ A, int64_t n, int64_t stride, int64_t k0, float2*
     }
 }
 
+// The B operands of the tensor-core panel TRSMs of a diagonal block, packed
+// once here instead of by every TRSM CTA: 128 x 128 FP16 K-major no-swizzle
+// images (8-row x 16-byte core matrices), rows R < 64 = [Re v | -Im v],
+// rows 64 + R = [Im v | Re v] of the complex row v = column R of inv(U11)
+// (image 0, for L21 = A21 inv(U11)) or row R of inv(L11) (image 1, for
+// U12^T = A12^T inv(L11)^T).  x holds inv(L) strictly below the diagonal
+// (unit diagonal implicit) and inv(U) on and above it.
+constexpr int kTrsmBImage = 128 * 128 * 2;  // bytes per image
+
+template <int LD>
+__device__ __forceinline__ void pack_trsm_b(const float2 (*x)[LD], unsigned char* img)
+{
+    for (int e = threadIdx.x; e < 2 * 128 * 16; e += blockDim.x) {
+        const int im = e / (128 * 16), R = (e / 16) % 128, cc = e % 16;
+        const int r = R & 63, t0 = (cc & 7) * 8;
+        float v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int t = t0 + q;
+            float2 z;
+            if (im == 0) z = t <= r ? x[t][r] : make_float2(0.f, 0.f);  // inv(U)[t][r]
+            else z = t == r ? make_float2(1.f, 0.f) : (r > t ? x[r][t] : make_float2(0.f, 0.f));  // inv(L)[r][t]
+            const bool im_row = R >= 64, second = cc >= 8;
+            v[q] = im_row ? (second ? z.x : z.y) : (second ? -z.y : z.x);
+        }
+        uint4 w;
+        __half2 h0 = __floats2half2_rn(v[0], v[1]), h1 = __floats2half2_rn(v[2], v[3]);
+        __half2 h2 = __floats2half2_rn(v[4], v[5]), h3 = __floats2half2_rn(v[6], v[7]);
+        w.x = *reinterpret_cast<uint32_t*>(&h0);
+        w.y = *reinterpret_cast<uint32_t*>(&h1);
+        w.z = *reinterpret_cast<uint32_t*>(&h2);
+        w.w = *reinterpret_cast<uint32_t*>(&h3);
+        const uint32_t off = (uint32_t)((cc * 16 + R / 8) * 128 + (R % 8) * 16);
+        *reinterpret_cast<uint4*>(img + (size_t)im * kTrsmBImage + off) = w;
+    }
+}
+
 // k_lu_diag for NB = 64 with the block held in registers: thread t owns row
 // r = t / 8 and the eight columns g + 8 m (g = t % 8, m = 0..7), so the
 // eight owners of a row are eight consecutive lanes of one warp.  Step c of
@@ -134,7 +172,7 @@ constexpr size_t kDiag64Smem = sizeof(float2) * (2 * 64 * kDiagLd + 2 * 32 * 32 
 
 __global__ void __launch_bounds__(kDiag64Threads)
 k_lu_diag64(float2* __restrict__ A, int64_t n, int64_t stride, int64_t k0, float2* __restrict__ Dinv,
-            int64_t dstride, int* __restrict__ bad)
+            int64_t dstride, int* __restrict__ bad, unsigned char* __restrict__ bimg, int64_t bstride)
 {
     constexpr int NB = 64;
     extern __shared__ float2 diag_smem[];
@@ -253,6 +291,7 @@ k_lu_diag64(float2* __restrict__ A, int64_t n, int64_t stride, int64_t k0, float
         out[e] = rr == c ? make_float2(1.f, 0.f) : (rr > c ? x[rr][c] : make_float2(0.f, 0.f));
         out[NB * NB + e] = rr <= c ? x[rr][c] : make_float2(0.f, 0.f);
     }
+    if (bimg) pack_trsm_b<kDiagLd>(x, bimg + b * bstride + (k0 / NB) * 2 * kTrsmBImage);
 }
 
 // blockIdx.y == 0: rows of L21 = A21 U11^-1; blockIdx.y == 1: columns of

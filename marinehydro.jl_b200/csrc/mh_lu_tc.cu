@@ -184,19 +184,17 @@ __device__ __forceinline__ uint4 pack8(const float2* v, bool imag, float sign)
 // its absolute tile slot.
 __global__ void __launch_bounds__(128, 2)
 k_lu_trsm_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
-             const float2* __restrict__ Dinv, int64_t dstride, unsigned char* __restrict__ Lp,
+             const unsigned char* __restrict__ bimg, int64_t bstride, unsigned char* __restrict__ Lp,
              unsigned char* __restrict__ Up, int64_t pstride, int ntile, int* __restrict__ bad)
 {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
-    __shared__ uint64_t mbar;
+    __shared__ uint64_t mbar, mbar_ld;
     __shared__ uint32_t tmem_slot;
     unsigned char* sA = tc_smem;             // 128 x 128 FP16 (32 KiB)
     unsigned char* sB = tc_smem + kSmemA;    // 128 x 128 FP16 (32 KiB)
     const int b = blockIdx.y;
     float2* M = Ab + (int64_t)b * stride;
     const int64_t blk = k0 / TC_NB;
-    const float2* Li = Dinv + (int64_t)b * dstride + blk * 2 * TC_NB * TC_NB;  // column-major
-    const float2* Ui = Li + TC_NB * TC_NB;
     const bool lower = (int)blockIdx.x < ntile;
     const int64_t lo = k0 + TC_NB;  // first row of L21 / column of U12
     const int tile = (int)(lo / TC_TM) + (lower ? (int)blockIdx.x : (int)blockIdx.x - ntile);
@@ -204,7 +202,21 @@ k_lu_trsm_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
     const bool ok = g >= lo && g < n;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (warp == 0) tmem_alloc(&tmem_slot, 128);
-    if (tid == 0) mbar_init(&mbar);
+    const uint32_t bar_ld = smem_u32(&mbar_ld);
+    if (tid == 0) {
+        mbar_init(&mbar);
+        mbar_init(&mbar_ld);
+        // B operand: the image the diagonal kernel packed (inv(U11) columns for
+        // L21, inv(L11) rows for U12), by bulk copy while the threads stage A
+        const unsigned char* src = bimg + (int64_t)b * bstride + (blk * 2 + (lower ? 0 : 1)) * kTrsmBImage;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                     :: "r"(bar_ld), "r"((uint32_t)kTrsmBImage) : "memory");
+        constexpr uint32_t kChunk = 16384;
+#pragma unroll 1
+        for (uint32_t off = 0; off < (uint32_t)kTrsmBImage; off += kChunk)
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                         :: "r"(smem_u32(sB + off)), "l"(src + off), "r"(kChunk), "r"(bar_ld) : "memory");
+    }
     // A operand: row tid = A21(g, :) or A12(:, g)^T, 64 complex -> Re chunks 0..7, Im 8..15
     if (lower) {  // A21 is column-major: consecutive rows g are consecutive lanes
 #pragma unroll 2
@@ -233,42 +245,15 @@ k_lu_trsm_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
             *reinterpret_cast<uint32_t*>(sA + core_off(row, 8 + cc, TC_TM) + 2 * cpos) = pack_h2(v0.y, v1.y);
         }
     }
-    // B operand (N = 128): rows r < 64 give the real part of the product,
-    // rows 64 + r the imaginary part: rows r = [Re | -Im], rows 64 + r =
-    // [Im | Re] of complex row r, which is column r of inv(U11) (L21) or row
-    // r of inv(L11) (U12).
-    if (lower) {  // column r of inv(U11) is contiguous: one warp per r, lane l holds t = 2l, 2l + 1
-        const int cpos = (2 * lane) & 7, cc = (2 * lane) >> 3;
-#pragma unroll 4
-        for (int i = 0; i < 16; ++i) {
-            const int r = warp * 16 + i;
-            const float2 v0 = Ui[r * TC_NB + 2 * lane], v1 = Ui[r * TC_NB + 2 * lane + 1];
-            *reinterpret_cast<uint32_t*>(sB + core_off(r, cc, 128) + 2 * cpos) = pack_h2(v0.x, v1.x);
-            *reinterpret_cast<uint32_t*>(sB + core_off(r, 8 + cc, 128) + 2 * cpos) = pack_h2(-v0.y, -v1.y);
-            *reinterpret_cast<uint32_t*>(sB + core_off(64 + r, cc, 128) + 2 * cpos) = pack_h2(v0.y, v1.y);
-            *reinterpret_cast<uint32_t*>(sB + core_off(64 + r, 8 + cc, 128) + 2 * cpos) = pack_h2(v0.x, v1.x);
-        }
-    } else {  // row r of inv(L11): consecutive r are consecutive lanes
-        const int r = tid & 63;
-        const bool im_row = tid >= 64;
-#pragma unroll 2
-        for (int c = 0; c < 8; ++c) {
-            float2 v[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) v[q] = Li[(8 * c + q) * TC_NB + r];
-            *reinterpret_cast<uint4*>(sB + core_off(tid, c, 128)) = pack8(v, im_row, 1.f);
-            *reinterpret_cast<uint4*>(sB + core_off(tid, 8 + c, 128)) =
-                im_row ? pack8(v, false, 1.f) : pack8(v, true, -1.f);
-        }
-    }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_slot;
     const uint32_t bar = smem_u32(&mbar);
-    if (tid == 0) mma_k128(tmem, smem_u32(sA), kLboA, smem_u32(sB), kLboB128, kIdescN128, bar);
-    const bool done = __syncthreads_and(mbar_wait(bar, 0)) != 0;
+    const bool loaded = __syncthreads_and(mbar_wait(bar_ld, 0)) != 0;
+    if (loaded && tid == 0) mma_k128(tmem, smem_u32(sA), kLboA, smem_u32(sB), kLboB128, kIdescN128, bar);
+    const bool done = loaded && __syncthreads_and(mbar_wait(bar, 0)) != 0;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (done) {
         const int row = warp * 32 + lane;  // TMEM lane = A row = tid of the loader above
@@ -324,7 +309,9 @@ k_lu_trsm_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
         }
     } else {
         if (lane == 0) atomicExch(bad + b, 2);
-        mbar_wait(bar, 0);
+        // bounded: the image copy or the MMAs may still be in flight
+        if (!loaded) mbar_wait(bar_ld, 0);
+        else mbar_wait(bar, 0);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -1155,9 +1142,11 @@ int64_t lu_dinv_stride_tc(int64_t n) { return ((n + TC_NB - 1) / TC_NB) * 2 * TC
 // live while its interior update runs, and the next outer step writes the
 // other four.
 constexpr int kOuterPanels = 4;  // 64-column panels per outer step (256 columns)
+// After them, the packed TRSM B operands of every diagonal block (two images each).
 int64_t lu_panel_bytes_tc(int64_t n)
 {
-    return 2 * kOuterPanels * ((n + TC_TM - 1) / TC_TM) * (int64_t)(kPanelL + kPanelU);
+    return 2 * kOuterPanels * ((n + TC_TM - 1) / TC_TM) * (int64_t)(kPanelL + kPanelU) +
+           ((n + TC_NB - 1) / TC_NB) * 2 * (int64_t)kTrsmBImage;
 }
 
 // Blocked LU in outer steps of 256 columns (four 64-column panels), with
@@ -1190,13 +1179,16 @@ cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int 
                                   (int)kDiag64Smem)) != cudaSuccess)
         return e;
     const int64_t dstride = lu_dinv_stride_tc(n);
-    const int64_t pstride = lu_panel_bytes_tc(n) / (2 * kOuterPanels);  // one buffer, per matrix
+    const int64_t pstride = (int64_t)((n + TC_TM - 1) / TC_TM) * (kPanelL + kPanelU);  // one buffer, per matrix
+    const int64_t bstride = ((n + TC_NB - 1) / TC_NB) * 2 * (int64_t)kTrsmBImage;       // B images, per matrix
+    unsigned char* bimg = panels + 2 * kOuterPanels * pstride * nbatch;
     const int ntiles = (int)((n + TC_TM - 1) / TC_TM);
     const unsigned nbz = (unsigned)nbatch;
     constexpr int kW = kOuterPanels / 2;  // tiles per outer step
     cudaStream_t main_s = ctx->stream, side_s = ctx->side;
     if ((e = cudaEventRecord(ctx->ev_side, side_s)) != cudaSuccess) return e;
-    k_lu_diag64<<<nbatch, kDiag64Threads, kDiag64Smem, main_s>>>(A, n, stride, 0, Dinv, dstride, bad);
+    k_lu_diag64<<<nbatch, kDiag64Threads, kDiag64Smem, main_s>>>(A, n, stride, 0, Dinv, dstride, bad, bimg,
+                                                                   bstride);
     ctx->launches += 1;
     int outer = 0;
     for (int64_t K0 = 0; K0 < n; K0 += kOuterPanels * TC_NB, ++outer) {
@@ -1215,7 +1207,7 @@ cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int 
             }
             const int t0 = (int)((k + TC_NB) / TC_TM), nt = ntiles - t0;
             k_lu_trsm_tc<<<dim3(2 * nt, nbz), 128, kSmemA + kSmemA, main_s>>>(
-                A, n, stride, k, Dinv, dstride, (unsigned char*)pp.L[s], (unsigned char*)pp.U[s], pstride, nt, bad);
+                A, n, stride, k, bimg, bstride, (unsigned char*)pp.L[s], (unsigned char*)pp.U[s], pstride, nt, bad);
             ctx->launches += 1;
             if (s + 1 < kOuterPanels) {  // the rest of the outer block with this panel, then its next diagonal block
                 PanelPairs one;
@@ -1224,7 +1216,8 @@ cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int 
                 const int w = std::min(T0 + kW - t0, nt);
                 k_lu_update_tc<<<dim3(w * (2 * nt - w), 1, nbz), 128, kTcSmemBytes, main_s>>>(
                     A, n, stride, t0, nt, 1, w, one, 1, pstride, k + TC_NB, bad);
-                k_lu_diag64<<<nbatch, kDiag64Threads, kDiag64Smem, main_s>>>(A, n, stride, k + TC_NB, Dinv, dstride, bad);
+                k_lu_diag64<<<nbatch, kDiag64Threads, kDiag64Smem, main_s>>>(A, n, stride, k + TC_NB, Dinv, dstride,
+                                                                           bad, bimg, bstride);
                 ctx->launches += 2;
             }
         }
@@ -1248,7 +1241,8 @@ cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int 
             A, n, stride, t0, nt, 1, w, pp, kOuterPanels, pstride, lo, bad);
         ctx->launches += 1;
         if (lo < n) {
-            k_lu_diag64<<<nbatch, kDiag64Threads, kDiag64Smem, main_s>>>(A, n, stride, lo, Dinv, dstride, bad);
+            k_lu_diag64<<<nbatch, kDiag64Threads, kDiag64Smem, main_s>>>(A, n, stride, lo, Dinv, dstride, bad,
+                                                                         bimg, bstride);
             ctx->launches += 1;
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
