@@ -237,21 +237,24 @@ k_adj_delh_tape(const double* __restrict__ geom, int64_t n, int direct, const do
     const int jend = (int)min((int64_t)kAC, n - j0);
     const int64_t nv = n * nrhs, nn = n * n;
     double xb[3] = {0.0, 0.0, 0.0}, nbi[3] = {0.0, 0.0, 0.0};
+    const double sg = direct ? -1.0 : 1.0;  // +1 for the gradient with respect to the first variable
     for (int jb = 0; jb < jend; jb += kTJ) {
         WaveGeom wg[kTJ];
-        double irho[kTJ];
-        double cacc[kTJ][kWaveF];
+        double irho[kTJ], s01[kTJ];
+        // frequency moments of the chain: sums over z of k^p re(c G') (see below)
+        double Sa2[kTJ], Sb3r[kTJ], Sc3[kTJ], Sc3r[kTJ], Sd2r[kTJ], Se2[kTJ], Sf3[kTJ], Sg1[kTJ], Sh2[kTJ];
 #pragma unroll
         for (int u = 0; u < kTJ; ++u) {
             const int jj = min(jb + u, jend - 1);  // a short last sweep repeats its last pair, masked below
             wg[u] = wave_geom(x, sp[jj]);
             irho[u] = 1.0 / hypot(wg[u].dis, wg[u].zs);
-#pragma unroll
-            for (int f = 0; f < kWaveF; ++f) cacc[u][f] = 0.0;
+            const double* nD = direct ? sp[jj].n : ni;
+            s01[u] = sg * (nD[0] * wg[u].u0 + nD[1] * wg[u].u1);
+            Sa2[u] = Sb3r[u] = Sc3[u] = Sc3r[u] = Sd2r[u] = Se2[u] = Sf3[u] = Sg1[u] = Sh2[u] = 0.0;
         }
         for (int z = 0; z < nb; ++z) {
             const int64_t base = (int64_t)z * nv;
-            const double k = ksh[z], ik = iksh[z];
+            const double k = ksh[z], ik = iksh[z], k2 = k * k, k3 = k2 * k;
             double bk = 0.0;
             double sr[kTJ], si[kTJ], dr[kTJ], di[kTJ];
 #pragma unroll
@@ -272,51 +275,95 @@ k_adj_delh_tape(const double* __restrict__ geom, int64_t n, int direct, const do
             for (int u = 0; u < kTJ; ++u) {
                 const int jj = jb + u;
                 if (jj >= jend) break;
+                if (!live) continue;
                 const Panel& p = sp[jj];
-                const int64_t j = j0 + jj;
+                const double* nD = direct ? p.n : ni;
+                const int64_t m = (int64_t)z * nn + (j0 + jj) * n + ii;
                 // cs = conj(-S-bar / 4pi), cw = conj(-D-bar / 4pi)
-                const cplx cs = mk(-kI4P * sr[u], kI4P * si[u]), cw = mk(-kI4P * dr[u], kI4P * di[u]);
-                if (live) {
-                    const double* nD = direct ? p.n : ni;
-                    WaveBar wb;
-                    const int64_t m = (int64_t)z * nn + j * n + ii;
-                    const double iR = ik * irho[u];  // 1 / R, R = k rho
-                    const double2 g0 = tape[2 * m], g1 = tape[2 * m + 1];
-                    cplx G[3];
-                    G[0] = mk(g0.x, g0.y);
-                    G[1] = mk(g1.x, g1.y);
-                    G[2] = mk(g0.x + 2.0 * iR, g0.y);
-                    GDer o;
-                    gder_identities_inv(G, k * wg[u].dis, k * wg[u].zs, iR, ik * wg[u].invd, o);
-                    wave_chain(o, wg[u], k, p.area, !direct, cs, cw, nD, wb);
-                    xb[0] += wb.dx;
-                    xb[1] += wb.dy;
-                    xb[2] += wb.zs;
-                    cacc[u][0] -= wb.dx;
-                    cacc[u][1] -= wb.dy;
-                    cacc[u][2] += wb.zs;
-                    if (direct) {
-                        cacc[u][3] += wb.n[0];
-                        cacc[u][4] += wb.n[1];
-                        cacc[u][5] += wb.n[2];
-                    } else {
-                        nbi[0] += wb.n[0];
-                        nbi[1] += wb.n[1];
-                        nbi[2] += wb.n[2];
-                    }
-                    cacc[u][6] += wb.area;
-                    bk += wb.k;
+                const double csr = -kI4P * sr[u], csi = kI4P * si[u];
+                const double cwr = -kI4P * dr[u], cwi = kI4P * di[u];
+                // dimensionless G, G_r from the tape; G_z = G + 2/R, second
+                // derivatives from the identities (as gder_identities)
+                const double iR = ik * irho[u], iR3 = iR * iR * iR;  // 1 / R, R = k rho
+                const double r = k * wg[u].dis, zz = k * wg[u].zs;
+                const double2 g0 = tape[2 * m], g1 = tape[2 * m + 1];
+                const double G2r = g0.x + 2.0 * iR, G2i = g0.y;
+                const double Gzzr = G2r - 2.0 * zz * iR3, Gzzi = G2i;
+                const double Grzr = g1.x - 2.0 * r * iR3, Grzi = g1.y;
+                double Grrr, Grri;
+                if (r > 1e-3) {
+                    const double ir = ik * wg[u].invd;
+                    Grrr = -g1.x * ir - Gzzr;
+                    Grri = -g1.y * ir - Gzzi;
+                } else {
+                    Grrr = -0.5 * Gzzr;
+                    Grri = -0.5 * Gzzi;
                 }
+                const double va = csr * g1.x - csi * g1.y;  // re(cs G_r)
+                const double vb = cwr * Grrr - cwi * Grri;  // re(cw G_rr)
+                const double vc = cwr * Grzr - cwi * Grzi;  // re(cw G_rz)
+                const double vd = cwr * g1.x - cwi * g1.y;  // re(cw G_r)
+                const double ve = csr * G2r - csi * G2i;    // re(cs G_z)
+                const double vf = cwr * Gzzr - cwi * Gzzi;  // re(cw G_zz)
+                const double vg = csr * g0.x - csi * g0.y;  // re(cs G)
+                const double vh = cwr * G2r - cwi * G2i;    // re(cw G_z)
+                const bool rad = fabs(r) > 1e-6;
+                Sa2[u] += k2 * va;
+                Sc3[u] += k3 * vc;
+                Se2[u] += k2 * ve;
+                Sf3[u] += k3 * vf;
+                Sg1[u] += k * vg;
+                Sh2[u] += k2 * vh;
+                if (rad) {
+                    Sb3r[u] += k3 * vb;
+                    Sc3r[u] += k3 * vc;
+                    Sd2r[u] += k2 * vd;
+                }
+                // dL/dk of this pair and frequency (wave_chain's k term)
+                const double A = p.area, rs = rad ? s01[u] : 0.0;
+                const double Lr = A * (k * va + rs * k2 * vb + nD[2] * k2 * vc);
+                const double Lz = A * (k * ve + rs * k2 * vc + nD[2] * k2 * vf);
+                bk += Lr * wg[u].dis + Lz * wg[u].zs + A * vg + 2.0 * k * A * (rs * vd + nD[2] * vh);
             }
             bk = warp_sum(bk);
             if (lane == 0) ksm[warp * nb + z] += bk;
         }
+        // the chain of wave_chain summed over the frequencies: per pair
+        // dx, dy, z, area and the normal, from the moments
 #pragma unroll
         for (int u = 0; u < kTJ; ++u) {
             if (jb + u >= jend) break;
+            double col[kWaveF] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            if (live) {
+                const Panel& p = sp[jb + u];
+                const double* nD = direct ? p.n : ni;
+                const double A = p.area, u0 = wg[u].u0, u1 = wg[u].u1, invd = wg[u].invd;
+                const double lin = Sa2[u] + s01[u] * Sb3r[u] + nD[2] * Sc3[u];
+                const double dx = A * u0 * lin + sg * A * invd * (nD[0] * (1.0 - u0 * u0) - nD[1] * u0 * u1) * Sd2r[u];
+                const double dy = A * u1 * lin + sg * A * invd * (nD[1] * (1.0 - u1 * u1) - nD[0] * u0 * u1) * Sd2r[u];
+                const double zs = A * (Se2[u] + s01[u] * Sc3r[u] + nD[2] * Sf3[u]);
+                const double area = Sg1[u] + s01[u] * Sd2r[u] + nD[2] * Sh2[u];
+                const double nb0 = sg * A * u0 * Sd2r[u], nb1 = sg * A * u1 * Sd2r[u], nb2 = A * Sh2[u];
+                xb[0] += dx;
+                xb[1] += dy;
+                xb[2] += zs;
+                col[0] = -dx;
+                col[1] = -dy;
+                col[2] = zs;
+                if (direct) {
+                    col[3] = nb0;
+                    col[4] = nb1;
+                    col[5] = nb2;
+                } else {
+                    nbi[0] += nb0;
+                    nbi[1] += nb1;
+                    nbi[2] += nb2;
+                }
+                col[6] = area;
+            }
 #pragma unroll
             for (int f = 0; f < kWaveF; ++f) {
-                const double v = warp_sum(cacc[u][f]);
+                const double v = warp_sum(col[f]);
                 if (lane == 0) csm[warp][jb + u][f] = v;
             }
         }
