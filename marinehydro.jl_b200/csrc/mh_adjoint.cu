@@ -203,23 +203,60 @@ k_adj_wave(int kind, const double* __restrict__ geom, int64_t n, int direct, con
 // S-bar_ij(z) = sum_q VA_iq conj(VB_jq), D-bar_ij(z) = -sum_q VC_iq conj(VD_jq)
 // (vectors [z][q][n]).  Each sweep over the frequencies takes kTJ columns
 // at once, so the row vectors VA, VC are read once per kTJ pairs and the
-// k partial sums are reduced across the warp once per kTJ pairs.  The
-// kernel waits on its loads more than it computes, so it runs at five CTAs
-// per SM (96 registers, a few spills): 15% faster than four at N=2048.
+// k partial sums are reduced across the warp once per kTJ pairs.
+// The kernel is bound by load latency, so every load of an iteration
+// (sweep, z) is issued one iteration ahead by cp.async into a two-slot ring
+// in shared memory, in flight without holding registers:
+//   - per thread: its 2 kTJ tape entries (G, G_r of each pair) and, when the
+//     right-hand-side count NQ is a compile-time constant (1 to 3), its row
+//     vectors VA, VC of every right-hand side;
+//   - per warp: the column vectors VB, VD of the iteration (the same for
+//     every lane), one entry per lane.
+// Each thread waits on its own copies, then a __syncwarp publishes the
+// warp's VB/VD slot and retires the slot that the next copies overwrite;
+// there is no CTA barrier in the loop.  NQ = 0 takes any count up to
+// kMaxRhs and loads VA, VC directly.
 // rowpart[colblock][kRowF][n], colpart[rowblock][kWaveF][n],
 // kpart[z][block]: deterministic partial sums.
 constexpr int kTJ = 2;
+constexpr int kTapeStages = 2;
 static_assert(kAC % kTJ == 0, "column blocks split into sweeps of kTJ pairs");
 
-__global__ void __launch_bounds__(kAR, 5)
+template <int NQ>
+struct TapeRing {
+    static constexpr int kThread = 2 * kTJ + 2 * NQ;                // double2 per thread and slot
+    static constexpr int kWarp = 2 * kTJ * (NQ > 0 ? NQ : kMaxRhs);  // double2 per warp and slot
+    static constexpr size_t kBytes = sizeof(double2) * kTapeStages * (kThread * kAR + kWarp * (kAR / 32));
+};
+
+template <int NQ>
+size_t tape_smem(int nb)
+{
+    return TapeRing<NQ>::kBytes + sizeof(double) * (kAR / 32 + 2) * nb;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+template <int NQ>
+__global__ void __launch_bounds__(kAR, 4)
 k_adj_delh_tape(const double* __restrict__ geom, int64_t n, int direct, const double2* __restrict__ tape,
                 const double* __restrict__ kvec, int nb, int nrhs, const double2* __restrict__ VA,
                 const double2* __restrict__ VB, const double2* __restrict__ VC, const double2* __restrict__ VD,
                 double* __restrict__ rowpart, double* __restrict__ colpart, double* __restrict__ kpart)
 {
-    extern __shared__ double ksm[];  // [4 warps][nb], then k and 1/k [nb] each
-    double* ksh = ksm + (kAR / 32) * nb;
-    double* iksh = ksh + nb;
+    using Ring = TapeRing<NQ>;
+    extern __shared__ __align__(16) unsigned char tsm[];
+    double2* ring = (double2*)tsm;                                                // [slot][Ring::kThread][kAR]
+    double2* wring = ring + kTapeStages * Ring::kThread * kAR;                    // [slot][warp][Ring::kWarp]
+    double* ksm = (double*)(wring + kTapeStages * Ring::kWarp * (kAR / 32));      // [4 warps][nb]
+    double* ksh = ksm + (kAR / 32) * nb;                                          // k [nb]
+    double* iksh = ksh + nb;                                                      // 1/k [nb]
     __shared__ Panel sp[kAC];
     __shared__ double csm[kAR / 32][kAC][kWaveF];
     const int64_t j0 = (int64_t)blockIdx.y * kAC;
@@ -240,6 +277,46 @@ k_adj_delh_tape(const double* __restrict__ geom, int64_t n, int direct, const do
     const int64_t nv = n * nrhs, nn = n * n;
     double xb[3] = {0.0, 0.0, 0.0}, nbi[3] = {0.0, 0.0, 0.0};
     const double sg = direct ? -1.0 : 1.0;  // +1 for the gradient with respect to the first variable
+    // ring fill: iterations (sweep, z) in loop order, slot = iteration & 1.
+    // Out-of-range rows copy row 0 and a short last sweep its last pair (in
+    // bounds, unused), so every lane copies the same pattern.
+    const int went = 2 * kTJ * (NQ > 0 ? NQ : nrhs);  // VB/VD entries per iteration: (q * kTJ + u) * 2 + {B, D}
+    const int nsweep = (jend + kTJ - 1) / kTJ;
+    int pf_s = 0, pf_z = 0, pf_slot = 0;
+    auto ring_issue = [&]() {
+        if (pf_s < nsweep) {
+            double2* mine = ring + (size_t)pf_slot * Ring::kThread * kAR + threadIdx.x;
+            const int64_t zo = (int64_t)pf_z * nv;
+#pragma unroll
+            for (int u = 0; u < kTJ; ++u) {
+                const int64_t j = j0 + min(pf_s * kTJ + u, jend - 1);
+                const double2* src = tape + 2 * ((int64_t)pf_z * nn + j * n + ii);
+                cp_async16(mine + (2 * u) * kAR, src);
+                cp_async16(mine + (2 * u + 1) * kAR, src + 1);
+            }
+            if constexpr (NQ > 0) {
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) {
+                    cp_async16(mine + (2 * kTJ + 2 * q) * kAR, VA + zo + (int64_t)q * n + ii);
+                    cp_async16(mine + (2 * kTJ + 2 * q + 1) * kAR, VC + zo + (int64_t)q * n + ii);
+                }
+            }
+            double2* wslot = wring + ((size_t)pf_slot * (kAR / 32) + warp) * Ring::kWarp;
+            for (int e = lane; e < went; e += 32) {
+                const int q = e / (2 * kTJ), u = (e >> 1) % kTJ;
+                const int64_t j = j0 + min(pf_s * kTJ + u, jend - 1);
+                cp_async16(wslot + e, ((e & 1) ? VD : VB) + zo + (int64_t)q * n + j);
+            }
+            if (++pf_z == nb) {
+                pf_z = 0;
+                ++pf_s;
+            }
+        }
+        cp_async_commit();
+        pf_slot ^= 1;
+    };
+    ring_issue();
+    int rd_slot = 0;
     for (int jb = 0; jb < jend; jb += kTJ) {
         WaveGeom wg[kTJ];
         double irho[kTJ], s01[kTJ];
@@ -255,23 +332,34 @@ k_adj_delh_tape(const double* __restrict__ geom, int64_t n, int direct, const do
             Sa2[u] = Sb3r[u] = Sc3[u] = Sc3r[u] = Sd2r[u] = Se2[u] = Sf3[u] = Sg1[u] = Sh2[u] = 0.0;
         }
         for (int z = 0; z < nb; ++z) {
-            const int64_t base = (int64_t)z * nv;
             const double k = ksh[z], ik = iksh[z], k2 = k * k, k3 = k2 * k;
+            cp_async_wait_all();  // this thread's copies of iteration (jb, z)
+            __syncwarp();         // the warp's VB/VD copies; every lane is done with the other slot
+            ring_issue();         // iteration (jb, z) + 1 into the other slot
+            const double2* mine = ring + (size_t)rd_slot * Ring::kThread * kAR + threadIdx.x;
+            const double2* vcol = wring + ((size_t)rd_slot * (kAR / 32) + warp) * Ring::kWarp;
+            rd_slot ^= 1;
             double bk = 0.0;
             double sr[kTJ], si[kTJ], dr[kTJ], di[kTJ];
 #pragma unroll
             for (int u = 0; u < kTJ; ++u) sr[u] = si[u] = dr[u] = di[u] = 0.0;
-            for (int q = 0; q < nrhs; ++q) {
-                const double2 a = VA[base + q * n + ii], c = VC[base + q * n + ii];
+            auto rhs_term = [&](int q, double2 a, double2 c) {
 #pragma unroll
                 for (int u = 0; u < kTJ; ++u) {
-                    const int64_t j = j0 + min(jb + u, jend - 1);
-                    const double2 b = VB[base + q * n + j], d = VD[base + q * n + j];
+                    const double2 b = vcol[(q * kTJ + u) * 2], d = vcol[(q * kTJ + u) * 2 + 1];
                     sr[u] += a.x * b.x + a.y * b.y;
                     si[u] += a.y * b.x - a.x * b.y;
                     dr[u] -= c.x * d.x + c.y * d.y;
                     di[u] -= c.y * d.x - c.x * d.y;
                 }
+            };
+            if constexpr (NQ > 0) {
+#pragma unroll
+                for (int q = 0; q < NQ; ++q)
+                    rhs_term(q, mine[(2 * kTJ + 2 * q) * kAR], mine[(2 * kTJ + 2 * q + 1) * kAR]);
+            } else {
+                const int64_t base = (int64_t)z * nv;
+                for (int q = 0; q < nrhs; ++q) rhs_term(q, VA[base + q * n + ii], VC[base + q * n + ii]);
             }
 #pragma unroll
             for (int u = 0; u < kTJ; ++u) {
@@ -280,7 +368,6 @@ k_adj_delh_tape(const double* __restrict__ geom, int64_t n, int direct, const do
                 if (!live) continue;
                 const Panel& p = sp[jj];
                 const double* nD = direct ? p.n : ni;
-                const int64_t m = (int64_t)z * nn + (j0 + jj) * n + ii;
                 // cs = conj(-S-bar / 4pi), cw = conj(-D-bar / 4pi)
                 const double csr = -kI4P * sr[u], csi = kI4P * si[u];
                 const double cwr = -kI4P * dr[u], cwi = kI4P * di[u];
@@ -288,7 +375,7 @@ k_adj_delh_tape(const double* __restrict__ geom, int64_t n, int direct, const do
                 // derivatives from the identities (as gder_identities)
                 const double iR = ik * irho[u], iR3 = iR * iR * iR;  // 1 / R, R = k rho
                 const double r = k * wg[u].dis, zz = k * wg[u].zs;
-                const double2 g0 = tape[2 * m], g1 = tape[2 * m + 1];
+                const double2 g0 = mine[(2 * u) * kAR], g1 = mine[(2 * u + 1) * kAR];
                 const double G2r = g0.x + 2.0 * iR, G2i = g0.y;
                 const double Gzzr = G2r - 2.0 * zz * iR3, Gzzi = G2i;
                 const double Grzr = g1.x - 2.0 * r * iR3, Grzi = g1.y;
@@ -370,6 +457,7 @@ k_adj_delh_tape(const double* __restrict__ geom, int64_t n, int direct, const do
             }
         }
     }
+    cp_async_wait_all();  // only an empty group remains
     __syncthreads();
     for (int t = threadIdx.x; t < jend * kWaveF; t += blockDim.x) {
         const int jj = t / kWaveF, f = t % kWaveF;
@@ -1185,10 +1273,18 @@ int contract_pairs_wave(const Batch& bt, Vjp& vj, const double* d_k, int nb, int
         double* colpart = rowpart + (size_t)ncb * kRowF * n;
         double* kpart = colpart + (size_t)nrb * kWaveF * n;
         if (use_tape) {
-            const size_t smem = sizeof(double) * (kAR / 32 + 2) * nb;
-            k_adj_delh_tape<<<dim3(nrb, cb), kAR, smem, ctx->stream>>>(bt.m->geom, n, bt.direct, vj.tape, d_k, nb,
-                                                                       bt.nrhs, VA, VB, VC, VD, rowpart, colpart,
-                                                                       kpart);
+            if (bt.nrhs < 1 || bt.nrhs > kMaxRhs) return MH_ERR_ARG;  // the VB/VD ring holds kMaxRhs at most
+            auto* kern = bt.nrhs == 1   ? k_adj_delh_tape<1>
+                         : bt.nrhs == 2 ? k_adj_delh_tape<2>
+                         : bt.nrhs == 3 ? k_adj_delh_tape<3>
+                                        : k_adj_delh_tape<0>;
+            const size_t smem = bt.nrhs == 1   ? tape_smem<1>(nb)
+                                : bt.nrhs == 2 ? tape_smem<2>(nb)
+                                : bt.nrhs == 3 ? tape_smem<3>(nb)
+                                               : tape_smem<0>(nb);
+            MH_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            kern<<<dim3(nrb, cb), kAR, smem, ctx->stream>>>(bt.m->geom, n, bt.direct, vj.tape, d_k, nb, bt.nrhs, VA,
+                                                            VB, VC, VD, rowpart, colpart, kpart);
         } else if (allw) {
             const size_t smem = adj_allw_smem(nb);
             MH_CUDA_TRY(ctx, cudaFuncSetAttribute(k_adj_delh_allw, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -248,3 +248,28 @@ def test_vjp_frequency_batched_many_slices(mh, gpu):
     for f in ("vertices", "centers", "normals", "areas"):
         x, y = getattr(a.mesh, f), getattr(b.mesh, f)
         assert np.max(np.abs(x - y)) <= 1e-8 * np.max(np.abs(y)), f
+
+
+@pytest.mark.parametrize("names,betas", [
+    (["Heave"], []),
+    (["Heave"], [0.2]),
+    (["Surge", "Heave", "Pitch"], [0.2]),
+    (["Surge", "Sway", "Heave", "Roll", "Pitch", "Yaw"], [0.2]),
+])
+def test_vjp_tape_right_hand_side_counts(mh, gpu, names, betas):
+    """The tape adjoint loads the row vectors of all right-hand sides of a
+    frequency together for 1 to 4 of them and one at a time beyond (here 7,
+    six rigid modes and a wave); the column vectors pass through shared
+    memory in chunks whose length depends on the count.  Mixed (tape) against
+    FP64 (no tape) on the same frequencies."""
+    mesh = mh.mesh_hemisphere(1.1, (0, 0, 0), (10, 14))
+    body = mh.FloatingBody.rigid(mesh, names, rotation_center=(0.0, 0.0, -0.2))
+    dofs = list(body.dofs.values())
+    om = np.linspace(0.3, 4.0, 9)
+    w = _weights(len(dofs), len(om), len(betas), seed=11)
+    a = _vjp(mh, gpu, mesh, om, dofs, betas, w, DELH, True, "mixed")
+    b = _vjp(mh, gpu, mesh, om, dofs, betas, w, DELH, True, "fp64")
+    assert np.max(np.abs(a.omegas - b.omegas)) <= 1e-8 * np.max(np.abs(b.omegas))
+    for f in ("vertices", "centers", "normals", "areas"):
+        x, y = getattr(a.mesh, f), getattr(b.mesh, f)
+        assert np.max(np.abs(x - y)) <= 1e-8 * np.max(np.abs(y)), f
