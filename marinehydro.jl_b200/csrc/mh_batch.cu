@@ -135,6 +135,43 @@ k_wave_batch(const double* __restrict__ geom, int64_t n, int direct, const doubl
 // frequencies per pass).
 // Frequencies at which the pair leaves the polar patch use the full table.
 // Same arithmetic as wave_pair<true> up to reassociation (~1e-16).
+// One pair of the frequency-batched pass and its output: S, D (FP64 and the
+// FP32 copy of D) and the tape of frequency z from the dimensionless
+// (G, G_r, G_z) in o3.
+struct AllwPair {
+    double dx, dy, rho, inv_rho, area, sr, dr;
+    const double* nn3;  // the normal of D (source panel when direct)
+    int64_t o;          // pair offset j * n + i
+    bool wrt_first;
+};
+
+__device__ __forceinline__ void allw_emit(const AllwPair& q, int z, double k, const cplx o3[3], int64_t nn,
+                                          double2* __restrict__ S64, double2* __restrict__ D64,
+                                          float2* __restrict__ Dlo, double2* __restrict__ tape)
+{
+    const double r = k * q.rho;
+    double d1 = 0.0, d2 = 0.0;
+    if (fabs(r) > 1e-6) {
+        const double f = k * q.inv_rho;  // k^2 / r
+        d1 = q.wrt_first ? f * q.dx : -f * q.dx;
+        d2 = q.wrt_first ? f * q.dy : -f * q.dy;
+    }
+    const double ka = k * q.area;
+    const cplx s = ka * o3[0];
+    const cplx g0 = (ka * d1) * o3[1], g1 = (ka * d2) * o3[1], g2 = (ka * k) * o3[2];
+    const double Sr = q.sr - kInv4Pi * s.re, Si = -kInv4Pi * s.im;
+    const double Dr = q.dr - kInv4Pi * (q.nn3[0] * g0.re + q.nn3[1] * g1.re + q.nn3[2] * g2.re);
+    const double Di = -kInv4Pi * (q.nn3[0] * g0.im + q.nn3[1] * g1.im + q.nn3[2] * g2.im);
+    const int64_t m = (int64_t)z * nn + q.o;
+    S64[m] = make_double2(Sr, Si);
+    D64[m] = make_double2(Dr, Di);
+    Dlo[m] = make_float2((float)Dr, (float)Di);
+    if (tape) {  // (G, G_r) for the adjoint of the same call
+        tape[2 * m] = make_double2(o3[0].re, o3[0].im);
+        tape[2 * m + 1] = make_double2(o3[1].re, o3[1].im);
+    }
+}
+
 constexpr int kWT = 128;  // threads (rows) per CTA of k_wave_delh_allw
 constexpr int kAllwMaxFreqs = 128;  // frequencies per launch of k_wave_delh_allw
 // the contracted series of every row, log k and 1/k per frequency (the polar
@@ -145,7 +182,7 @@ __global__ void __launch_bounds__(kWT, 3)
 k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const double* __restrict__ tab,
                  const double* __restrict__ kvec, int nb, const double* __restrict__ SR,
                  const double* __restrict__ DR, double2* __restrict__ S64, double2* __restrict__ D64,
-                 float2* __restrict__ Dlo, double2* __restrict__ tape)
+                 float2* __restrict__ Dlo, double2* __restrict__ tape, int* __restrict__ fall)
 {
     extern __shared__ double wsm[];
     const double* coef = tab + kTabMonoOff;        // 4 polar tables, monomial in u
@@ -187,28 +224,37 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
         const double gp = rho / (d * (d + az));
         const double inv_d = 1.0 / d, inv_rho = rho > 0.0 ? 1.0 / rho : 0.0;
         const double sr = SR[o], dr = DR[o];
-        // contract alpha: w_q[row] = sum_j c_q[row][j] T_j(v)
+        // contract alpha: w_q[row] = sum_j c_q[row][j] T_j(v), the four
+        // functions' Clenshaw recurrences interleaved (four independent
+        // dependency chains per row)
         if (polar_ok) {
+            const double v2 = 2.0 * v;
 #pragma unroll 1
-            for (int q = 0; q < 4; ++q) {
-                const double* c = coef + q * kTabPolarFn;
-#pragma unroll 1
-                for (int row = 0; row < kTabNU; ++row) {
-                    const double* cr = c + row * kTabNV;
-                    double b1 = 0.0, b2 = 0.0;
+            for (int row = 0; row < kTabNU; ++row) {
+                const double* cr = coef + row * kTabNV;
+                double b1[4] = {0.0, 0.0, 0.0, 0.0}, b2[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-                    for (int col = kTabNV - 1; col >= 1; --col) {
-                        const double t = fma(2.0 * v, b1, __ldg(cr + col) - b2);
-                        b2 = b1;
-                        b1 = t;
+                for (int col = kTabNV - 1; col >= 1; --col) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const double t = fma(v2, b1[q], __ldg(cr + q * kTabPolarFn + col) - b2[q]);
+                        b2[q] = b1[q];
+                        b1[q] = t;
                     }
-                    w[(q * kTabNU + row) * kWT + tid] = fma(v, b1, __ldg(cr) - b2);
                 }
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    w[(q * kTabNU + row) * kWT + tid] = fma(v, b1[q], __ldg(cr + q * kTabPolarFn) - b2[q]);
             }
         }
+        const AllwPair q{dx, dy, rho, inv_rho, p.area, sr, dr, nn3, o, wrt_first};
         // four frequencies per Horner pass: each coefficient read from shared
-        // memory feeds four recurrences
+        // memory feeds four recurrences.  Frequencies off the polar patch are
+        // only counted here: k_wave_delh_allw_rest evaluates them with the
+        // full table, so this kernel makes no out-of-line call (whose calling
+        // convention would cost spills on the hot path)
         constexpr int kZP = 4;
+        int nfall = 0;
         for (int z0 = 0; z0 < nb; z0 += kZP) {
             const int nz = min(kZP, nb - z0);
             double kz[kZP], uz[kZP];
@@ -243,41 +289,67 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
 #pragma unroll
             for (int t = 0; t < kZP; ++t) {
                 if (t >= nz) break;
+                if (!pz[t]) {
+                    ++nfall;
+                    continue;
+                }
                 const int z = z0 + t;
-                const double k = kz[t], ik = invk[z];
-                const double r = k * rho, zz = k * zeta;
+                const double ik = invk[z];
+                const double B = val[t][0], C = val[t][1], E0 = val[t][2], E1 = val[t][3];
+                const double L = logk[z] + lp;
+                const double G_re = -2.0 * E0 * L + B, G_im = 2.0 * kPi * E0;
                 cplx o3[3];
-                if (pz[t]) {
-                    const double B = val[t][0], C = val[t][1], E0 = val[t][2], E1 = val[t][3];
-                    const double L = logk[z] + lp;
-                    const double G_re = -2.0 * E0 * L + B, G_im = 2.0 * kPi * E0;
-                    o3[0] = mk(G_re, G_im);
-                    o3[1] = mk(2.0 * E1 * L - 2.0 * E0 * gp * ik + C, -2.0 * kPi * E1);
-                    o3[2] = mk(G_re + 2.0 * inv_d * ik, G_im);  // 2 / R, R = k d
-                } else {
-                    delh_dimless_table(tab, r, zz, o3);
-                }
-                double d1 = 0.0, d2 = 0.0;
-                if (fabs(r) > 1e-6) {
-                    const double f = k * inv_rho;  // k^2 / r
-                    d1 = wrt_first ? f * dx : -f * dx;
-                    d2 = wrt_first ? f * dy : -f * dy;
-                }
-                const double ka = k * p.area;
-                const cplx s = ka * o3[0];
-                const cplx g0 = (ka * d1) * o3[1], g1 = (ka * d2) * o3[1], g2 = (ka * k) * o3[2];
-                const double Sr = sr - kInv4Pi * s.re, Si = -kInv4Pi * s.im;
-                const double Dr = dr - kInv4Pi * (nn3[0] * g0.re + nn3[1] * g1.re + nn3[2] * g2.re);
-                const double Di = -kInv4Pi * (nn3[0] * g0.im + nn3[1] * g1.im + nn3[2] * g2.im);
-                const int64_t m = (int64_t)z * nn + o;
-                S64[m] = make_double2(Sr, Si);
-                D64[m] = make_double2(Dr, Di);
-                Dlo[m] = make_float2((float)Dr, (float)Di);
-                if (tape) {  // (G, G_r) for the adjoint of the same call
-                    tape[2 * m] = make_double2(o3[0].re, o3[0].im);
-                    tape[2 * m + 1] = make_double2(o3[1].re, o3[1].im);
-                }
+                o3[0] = mk(G_re, G_im);
+                o3[1] = mk(2.0 * E1 * L - 2.0 * E0 * gp * ik + C, -2.0 * kPi * E1);
+                o3[2] = mk(G_re + 2.0 * inv_d * ik, G_im);  // 2 / R, R = k d
+                allw_emit(q, z, kz[t], o3, nn, S64, D64, Dlo, tape);
             }
+        }
+        if (nfall) *fall = 1;
+    }
+}
+
+// The frequencies k_wave_delh_allw left to the full table (pairs above the
+// free surface or at R = k d >= 2); exits at once when it flagged none.  The
+// test takes a margin of 1e-12 in R so that a pair on the patch edge is
+// written by one kernel at least, whatever the rounding of d in each (a pair
+// written by both gets this kernel's value, which runs second).
+__global__ void __launch_bounds__(kWT)
+k_wave_delh_allw_rest(const int* __restrict__ fall, const double* __restrict__ geom, int64_t n, int direct,
+                      const double* __restrict__ tab, const double* __restrict__ kvec, int nb,
+                      const double* __restrict__ SR, const double* __restrict__ DR, double2* __restrict__ S64,
+                      double2* __restrict__ D64, float2* __restrict__ Dlo, double2* __restrict__ tape)
+{
+    if (*fall == 0) return;
+    __shared__ Panel sp[kCols];
+    const int64_t j0 = (int64_t)blockIdx.y * kCols;
+    stage_panels(sp, geom, n, j0);
+    __syncthreads();
+    const int64_t i = (int64_t)blockIdx.x * kWT + threadIdx.x;
+    if (i >= n) return;
+    const int64_t nn = n * n;
+    const double x[3] = {geom[G_CX * n + i], geom[G_CY * n + i], geom[G_CZ * n + i]};
+    const double ni[3] = {geom[G_NX * n + i], geom[G_NY * n + i], geom[G_NZ * n + i]};
+    const int jend = (int)min((int64_t)kCols, n - j0);
+    for (int jj = 0; jj < jend; ++jj) {
+        const Panel& p = sp[jj];
+        const int64_t o = (j0 + jj) * n + i;
+        const double dx = x[0] - p.c[0], dy = x[1] - p.c[1];
+        const double dis2 = dx * dx + dy * dy;
+        const double purt = 1e-18;
+        const double rho = (dis2 == 0.0) ? sqrt(dis2 + purt * purt) - purt : sqrt(dis2);
+        const double zeta = x[2] + p.c[2];
+        const double d = hypot(rho, zeta);
+        const bool polar_ok = -zeta >= 0.0;
+        const AllwPair q{dx, dy, rho, rho > 0.0 ? 1.0 / rho : 0.0, p.area, SR[o], DR[o], direct ? p.n : ni, o,
+                         !direct};
+#pragma unroll 1
+        for (int z = 0; z < nb; ++z) {
+            const double k = kvec[z];
+            if (polar_ok && k * d < kTabRPolar * (1.0 - 1e-12)) continue;
+            cplx o3[3];
+            delh_dimless_table(tab, k * rho, k * zeta, o3);
+            allw_emit(q, z, k, o3, nn, S64, D64, Dlo, tape);
         }
     }
 }
@@ -670,6 +742,7 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
     double2* RHS = R + nv * nb;  // right-hand side of the D (or K) system
     auto* d_res = (double*)misc;
     auto* d_bad = (int*)(misc + sizeof(double) * nb);
+    auto* d_fall = d_bad + nb;  // set when the frequency-batched pass left pairs to the full table
     int rc;
     const double* tab = delh_table_for(ctx, bt.mask, &rc);
     if (rc) return rc;
@@ -687,10 +760,15 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
         for (int z = 0; z < nb; z += kAllwMaxFreqs) {
             const int m = std::min(kAllwMaxFreqs, nb - z);
             const int64_t off = (int64_t)z * nn;
-            k_wave_delh_allw<<<dim3(blocks(n, kWT), blocks(n, kCols)), kWT, kWaveAllwSmem, ctx->stream>>>(
-                bt.m->geom, n, bt.direct, tab, d_k + z, m, SR, DR, S64 + off, D64 + off, Dlo + off,
-                bt.tape ? bt.tape + 2 * off : nullptr);
-            ctx->launches += (z > 0);
+            double2* tp = bt.tape ? bt.tape + 2 * off : nullptr;
+            const dim3 g2(blocks(n, kWT), blocks(n, kCols));
+            MH_CUDA_TRY(ctx, cudaMemsetAsync(d_fall, 0, sizeof(int), ctx->stream));
+            k_wave_delh_allw<<<g2, kWT, kWaveAllwSmem, ctx->stream>>>(bt.m->geom, n, bt.direct, tab, d_k + z, m, SR,
+                                                                      DR, S64 + off, D64 + off, Dlo + off, tp,
+                                                                      d_fall);
+            k_wave_delh_allw_rest<<<g2, kWT, 0, ctx->stream>>>(d_fall, bt.m->geom, n, bt.direct, tab, d_k + z, m,
+                                                              SR, DR, S64 + off, D64 + off, Dlo + off, tp);
+            ctx->launches += 1 + (z > 0);
         }
     } else if (wave == MH_GF_DELHOMMEAU)
         k_wave_batch<true><<<grid, kRows, 0, ctx->stream>>>(bt.m->geom, n, bt.direct, tab, d_k, SR, DR,
