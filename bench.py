@@ -509,10 +509,11 @@ def _peaks():
 
 
 # DRAM bytes (read + write) per pair-frequency of k_wave_delh_allw from an
-# ncu capture (hemisphere 1024 panels, 16 frequencies: dram__bytes_read.sum +
-# dram__bytes_write.sum / (n^2 * 16)); traffic grows with the pairs and
-# frequencies a launch processes, so it is scaled by them.
-WAVE_DRAM_BYTES_PER_PAIR_FREQ = 38.6
+# ncu capture (hemisphere 1024 panels, 64 frequencies, the solve step's
+# launch without tape: (dram__bytes_read.sum + dram__bytes_write.sum) /
+# (n^2 * 64)); traffic grows with the pairs and frequencies a launch
+# processes, so it is scaled by them.
+WAVE_DRAM_BYTES_PER_PAIR_FREQ = 39.4
 
 
 def roofline(per_phase, n, args):
@@ -538,8 +539,9 @@ def roofline(per_phase, n, args):
            "unit": "GB/s", "frac": achieved / hbm, "peak_source": src, "traffic": traffic,
            "ms_per_launch": ms, "algorithmic_bytes_per_launch": alg,
            "note": ("FP64-issue bound (alpha contraction of the polar table per pair, Horner series "
-                    "in R and complex arithmetic per pair and frequency; ncu: FP64 pipe 34% active "
-                    "at 17% warps active); the HBM fraction shows the writes are not the limit")}
+                    "in R and complex arithmetic per pair and frequency; ncu at 1024 panels x 64 "
+                    "frequencies: FP64 pipe 50% active at 15% warps active, no spills); the HBM "
+                    "fraction shows the writes are not the limit")}
     if "lu" in per_phase:
         fl = 8.0 / 3.0 * float(n) ** 3 * args.n_omega
         ach = fl / (per_phase["lu"] / 1e3) / 1e12
