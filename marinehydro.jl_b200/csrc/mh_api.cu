@@ -285,6 +285,19 @@ int mh_ctx_create(int device, mh_ctx** out)
         delete ctx;
         return set_err(nullptr, MH_ERR_CUDA, "stream/event creation: %s", cudaGetErrorString(e));
     }
+    for (int g = 0; g < kLuGroups - 1 && e == cudaSuccess; ++g) {
+        if ((e = cudaStreamCreateWithPriority(&ctx->grp_main[g], cudaStreamNonBlocking, greatest)) != cudaSuccess ||
+            (e = cudaStreamCreateWithPriority(&ctx->grp_side[g], cudaStreamNonBlocking, least)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&ctx->grp_ev_panel[g], cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&ctx->grp_ev_side[g], cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&ctx->grp_ev_join[g], cudaEventDisableTiming)) != cudaSuccess)
+            break;
+    }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        mh_ctx_destroy(ctx);
+        return set_err(nullptr, MH_ERR_CUDA, "stream/event creation: %s", cudaGetErrorString(e));
+    }
     if (cublasCreate(&ctx->cublas) != CUBLAS_STATUS_SUCCESS ||
         cusolverDnCreate(&ctx->cusolver) != CUSOLVER_STATUS_SUCCESS) {
         mh_ctx_destroy(ctx);
@@ -302,6 +315,10 @@ int mh_ctx_destroy(mh_ctx* ctx)
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->side) cudaStreamSynchronize(ctx->side);
+    for (int g = 0; g < kLuGroups - 1; ++g) {
+        if (ctx->grp_main[g]) cudaStreamSynchronize(ctx->grp_main[g]);
+        if (ctx->grp_side[g]) cudaStreamSynchronize(ctx->grp_side[g]);
+    }
     for (int s = 0; s < WS_NSLOTS; ++s)
         if (ctx->ws[s]) cudaFree(ctx->ws[s]);
     if (ctx->delh_table) cudaFree(ctx->delh_table);
@@ -311,6 +328,14 @@ int mh_ctx_destroy(mh_ctx* ctx)
     if (ctx->cublas) cublasDestroy(ctx->cublas);
     if (ctx->ev_panel) cudaEventDestroy(ctx->ev_panel);
     if (ctx->ev_side) cudaEventDestroy(ctx->ev_side);
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    for (int g = 0; g < kLuGroups - 1; ++g) {
+        if (ctx->grp_ev_panel[g]) cudaEventDestroy(ctx->grp_ev_panel[g]);
+        if (ctx->grp_ev_side[g]) cudaEventDestroy(ctx->grp_ev_side[g]);
+        if (ctx->grp_ev_join[g]) cudaEventDestroy(ctx->grp_ev_join[g]);
+        if (ctx->grp_side[g]) cudaStreamDestroy(ctx->grp_side[g]);
+        if (ctx->grp_main[g]) cudaStreamDestroy(ctx->grp_main[g]);
+    }
     if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;

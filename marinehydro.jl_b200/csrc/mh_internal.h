@@ -44,11 +44,22 @@ enum Phase : int {
     PH_ADJ_SOLVE, PH_ADJ_WAVE, PH_ADJ_RANKINE, PH_ADJ_LINEAR, PH_N
 };
 
+// Groups of matrices whose blocked LUs run concurrently on their own
+// streams, so one group's latency-bound panel work (diagonal blocks, panel
+// solves) overlaps another's trailing updates.
+constexpr int kLuGroups = 2;
+
 struct mh_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;  // every call's work (highest priority)
     cudaStream_t side = nullptr;    // concurrent work inside a call (lowest priority)
     cudaEvent_t ev_panel = nullptr, ev_side = nullptr;
+    // further (main, side) stream pairs: the batched LU runs its matrices in
+    // kLuGroups groups, group 0 on (stream, side), group g on these; forked
+    // from and joined back to stream inside each call
+    cudaStream_t grp_main[kLuGroups - 1] = {}, grp_side[kLuGroups - 1] = {};
+    cudaEvent_t grp_ev_panel[kLuGroups - 1] = {}, grp_ev_side[kLuGroups - 1] = {}, grp_ev_join[kLuGroups - 1] = {};
+    cudaEvent_t ev_fork = nullptr;
     cublasHandle_t cublas = nullptr;
     cusolverDnHandle_t cusolver = nullptr;
     std::string err;

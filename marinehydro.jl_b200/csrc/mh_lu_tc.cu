@@ -1162,22 +1162,14 @@ int64_t lu_panel_bytes_tc(int64_t n)
 // is read and written once per 256 columns.  An outer step's trailing
 // update waits for the previous interior; everything before it only touches
 // tile rows and columns T0, T0 + 1, which that interior does not.
-cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int nbatch, float2* Dinv,
-                         unsigned char* panels, int* bad)
+namespace {
+// The schedule above for nbatch matrices on one (main, side) stream pair;
+// panels: lu_panel_bytes_tc(n) * nbatch bytes for these matrices.
+cudaError_t lu_tc_group(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int nbatch, float2* Dinv,
+                        unsigned char* panels, int* bad, cudaStream_t main_s, cudaStream_t side_s,
+                        cudaEvent_t ev_side, cudaEvent_t ev_panel)
 {
     cudaError_t e;
-    static_assert(TC_NB == 64, "the diagonal blocks are factored by k_lu_diag64");
-    static_assert(TC_TM == 2 * TC_NB && TC_TN == TC_TM, "two panels per 128-wide tile");
-    static_assert(kOuterPanels <= kMaxPairs && kOuterPanels == 4, "an outer step spans two tiles");
-    if ((e = cudaFuncSetAttribute(k_lu_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)kTcSmemBytes)) != cudaSuccess)
-        return e;
-    if ((e = cudaFuncSetAttribute(k_lu_trsm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(kSmemA + kSmemA))) != cudaSuccess)
-        return e;
-    if ((e = cudaFuncSetAttribute(k_lu_diag64, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)kDiag64Smem)) != cudaSuccess)
-        return e;
     const int64_t dstride = lu_dinv_stride_tc(n);
     const int64_t pstride = (int64_t)((n + TC_TM - 1) / TC_TM) * (kPanelL + kPanelU);  // one buffer, per matrix
     const int64_t bstride = ((n + TC_NB - 1) / TC_NB) * 2 * (int64_t)kTrsmBImage;       // B images, per matrix
@@ -1185,8 +1177,7 @@ cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int 
     const int ntiles = (int)((n + TC_TM - 1) / TC_TM);
     const unsigned nbz = (unsigned)nbatch;
     constexpr int kW = kOuterPanels / 2;  // tiles per outer step
-    cudaStream_t main_s = ctx->stream, side_s = ctx->side;
-    if ((e = cudaEventRecord(ctx->ev_side, side_s)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(ev_side, side_s)) != cudaSuccess) return e;
     k_lu_diag64<<<nbatch, kDiag64Threads, kDiag64Smem, main_s>>>(A, n, stride, 0, Dinv, dstride, bad, bimg,
                                                                    bstride);
     ctx->launches += 1;
@@ -1227,16 +1218,16 @@ cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int 
         const int t0 = T0 + kW, nt = ntiles - t0;
         if (nt <= 0) break;
         // the previous interior update is done before this trailing update
-        if ((e = cudaStreamWaitEvent(main_s, ctx->ev_side, 0)) != cudaSuccess) return e;
-        if ((e = cudaEventRecord(ctx->ev_panel, main_s)) != cudaSuccess) return e;
-        if ((e = cudaStreamWaitEvent(side_s, ctx->ev_panel, 0)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(main_s, ev_side, 0)) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(ev_panel, main_s)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(side_s, ev_panel, 0)) != cudaSuccess) return e;
         const int w = std::min(kW, nt);
         if (nt > w) {
             k_lu_update_tc<<<dim3(nt - w, nt - w, nbz), 128, kTcSmemBytes, side_s>>>(
                 A, n, stride, t0, nt, 2, w, pp, kOuterPanels, pstride, lo, bad);
             ctx->launches += 1;
         }
-        if ((e = cudaEventRecord(ctx->ev_side, side_s)) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(ev_side, side_s)) != cudaSuccess) return e;
         k_lu_update_tc<<<dim3(w * (2 * nt - w), 1, nbz), 128, kTcSmemBytes, main_s>>>(
             A, n, stride, t0, nt, 1, w, pp, kOuterPanels, pstride, lo, bad);
         ctx->launches += 1;
@@ -1248,8 +1239,55 @@ cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int 
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    // join: everything of the side stream is done before the caller continues
-    if ((e = cudaStreamWaitEvent(main_s, ctx->ev_side, 0)) != cudaSuccess) return e;
+    // join: everything of the side stream is done before the main stream goes on
+    if ((e = cudaStreamWaitEvent(main_s, ev_side, 0)) != cudaSuccess) return e;
+    return cudaSuccess;
+}
+}  // namespace
+
+// The matrices in kLuGroups groups (contiguous, sizes differing by one at
+// most), each on its own (main, side) stream pair: group 0 on the context's
+// streams, the others forked from its stream and joined back, so the
+// diagonal-block factorisations and panel solves of one group (one CTA per
+// matrix, latency bound) run beside the trailing updates of another.
+cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int nbatch, float2* Dinv,
+                         unsigned char* panels, int* bad)
+{
+    cudaError_t e;
+    static_assert(TC_NB == 64, "the diagonal blocks are factored by k_lu_diag64");
+    static_assert(TC_TM == 2 * TC_NB && TC_TN == TC_TM, "two panels per 128-wide tile");
+    static_assert(kOuterPanels <= kMaxPairs && kOuterPanels == 4, "an outer step spans two tiles");
+    if ((e = cudaFuncSetAttribute(k_lu_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kTcSmemBytes)) != cudaSuccess)
+        return e;
+    if ((e = cudaFuncSetAttribute(k_lu_trsm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(kSmemA + kSmemA))) != cudaSuccess)
+        return e;
+    if ((e = cudaFuncSetAttribute(k_lu_diag64, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kDiag64Smem)) != cudaSuccess)
+        return e;
+    const int groups = std::min(kLuGroups, nbatch);
+    const int64_t dstride = lu_dinv_stride_tc(n);
+    const int64_t pbytes = lu_panel_bytes_tc(n);
+    if (groups > 1) {
+        if ((e = cudaEventRecord(ctx->ev_fork, ctx->stream)) != cudaSuccess) return e;
+        for (int g = 1; g < groups; ++g)
+            if ((e = cudaStreamWaitEvent(ctx->grp_main[g - 1], ctx->ev_fork, 0)) != cudaSuccess) return e;
+    }
+    int b0 = 0;
+    for (int g = 0; g < groups; ++g) {
+        const int nbg = nbatch / groups + (g < nbatch % groups ? 1 : 0);
+        cudaStream_t ms = g ? ctx->grp_main[g - 1] : ctx->stream, ss = g ? ctx->grp_side[g - 1] : ctx->side;
+        cudaEvent_t es = g ? ctx->grp_ev_side[g - 1] : ctx->ev_side, ep = g ? ctx->grp_ev_panel[g - 1] : ctx->ev_panel;
+        if ((e = lu_tc_group(ctx, A + (int64_t)b0 * stride, n, stride, nbg, Dinv + (int64_t)b0 * dstride,
+                             panels + (int64_t)b0 * pbytes, bad + b0, ms, ss, es, ep)) != cudaSuccess)
+            return e;
+        b0 += nbg;
+    }
+    for (int g = 1; g < groups; ++g) {
+        if ((e = cudaEventRecord(ctx->grp_ev_join[g - 1], ctx->grp_main[g - 1])) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(ctx->stream, ctx->grp_ev_join[g - 1], 0)) != cudaSuccess) return e;
+    }
     return cudaSuccess;
 }
 
