@@ -7,7 +7,8 @@ The compute runs in ``lib/libmarinehydro_b200.so`` (hand-written CUDA for
 sm_100a behind the C ABI in ``include/marinehydro_b200.h``).  This package is
 the host-side mirror of the reference's public API for that path.
 """
-from .meshes import Mesh, combine_meshes, mesh_hemisphere, mesh_two_hemispheres, panel_geometry
+from .meshes import (Mesh, combine_meshes, mesh_hemisphere, mesh_two_hemispheres, panel_geometry,
+                     wavebot_profile, axisymmetric_mesh, polygon_geometry, wavebot_mesh)
 from .api import (SETTINGS, set_g, set_rho, GreensFunction, Rankine, RankineReflected,
                   RankineReflectedNegative, GFWu, ExactGuevelDelhommeau, gf_mask,
                   DEFAULT_GREEN_FUNCTIONS, DeviceMesh, device_mesh, assemble_matrices,
@@ -19,7 +20,8 @@ from .bodies import (FloatingBody, combine_floatingbodies, make_body_name_list_u
                      compute_hydrodynamic_coefficients)
 from .gradients import (MeshTangent, VjpResult, JvpResult, hydro_batch_vjp, hydro_batch_jvp,
                         hydro_batch_rrule,
-                        hemisphere_tangents, two_hemispheres_tangents)
+                        hemisphere_tangents, two_hemispheres_tangents, polygon_geometry_jvp,
+                        wavebot_tangents)
 from .power import two_body_power
 from .design import SplitMix64, Design, designs, design_batch
 from ._native import (Context, MarineHydroError, ArgumentError, NotConvergedError,

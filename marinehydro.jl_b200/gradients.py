@@ -254,3 +254,65 @@ def two_hemispheres_tangents(radius: float = 1.0, separation: float = 5.0,
 
     zero = MeshTangent.zeros_like(mesh_hemisphere(radius, (0.0, 0.0, 0.0), resolution))
     return {"radius": cat(t1["radius"], t2["radius"]), "separation": cat(zero, t2["cx"])}
+
+
+def polygon_geometry_jvp(vertices: np.ndarray, faces: np.ndarray, dvertices: np.ndarray) -> MeshTangent:
+    """Tangent of every field of a mesh built by ``polygon_geometry`` (the
+    reference's polygon-mesh conventions, src/meshes.jl:353-423) along a
+    vertex tangent: the exact derivatives of the area-weighted centroid, the
+    unit normal of (b - a) x (c - a), the area and the radius |a - centre|."""
+    v, dv = vertices[faces], dvertices[faces]
+    a, b, c, d = v[:, 0], v[:, 1], v[:, 2], v[:, 3]
+    da, db, dc, dd = dv[:, 0], dv[:, 1], dv[:, 2], dv[:, 3]
+    cr1, cr2 = np.cross(b - a, c - a), np.cross(c - a, d - a)
+    dcr1 = np.cross(db - da, c - a) + np.cross(b - a, dc - da)
+    dcr2 = np.cross(dc - da, d - a) + np.cross(c - a, dd - da)
+    n1, n2 = np.linalg.norm(cr1, axis=1), np.linalg.norm(cr2, axis=1)
+    area1, area2 = 0.5 * n1, 0.5 * n2
+    # a degenerate second triangle (triangle panels) has no area and no tangent
+    dn1 = np.einsum("ij,ij->i", cr1, dcr1) / n1
+    dn2 = np.where(n2 > 0.0, np.einsum("ij,ij->i", cr2, dcr2) / np.where(n2 > 0.0, n2, 1.0), 0.0)
+    darea1, darea2 = 0.5 * dn1, 0.5 * dn2
+    areas, dareas = area1 + area2, darea1 + darea2
+    c1, c2 = (a + b + c) / 3.0, (a + c + d) / 3.0
+    dc1, dc2 = (da + db + dc) / 3.0, (da + dc + dd) / 3.0
+    centers = (c1 * area1[:, None] + c2 * area2[:, None]) / areas[:, None]
+    dcenters = (dc1 * area1[:, None] + c1 * darea1[:, None] + dc2 * area2[:, None] + c2 * darea2[:, None]
+                - centers * dareas[:, None]) / areas[:, None]
+    nrm = cr1 / n1[:, None]
+    dnormals = dcr1 / n1[:, None] - nrm * (dn1 / n1)[:, None]
+    ra = a - centers
+    rr = np.linalg.norm(ra, axis=1)
+    dradii = np.einsum("ij,ij->i", ra, da - dcenters) / rr
+    return MeshTangent(np.asarray(dvertices, dtype=np.float64).copy(), dcenters, dnormals, dareas, dradii)
+
+
+def wavebot_tangents(r1: float, r2: float, d1: float, d2: float, n_points=(5, 10, 5),
+                     n_theta: int = 72) -> dict:
+    """Exact derivatives of ``wavebot_mesh(r1, r2, d1, d2, n_points,
+    n_theta)`` with respect to {"r1", "r2", "d1", "d2"} -> MeshTangent (the
+    reference obtains them by automatic differentiation through
+    src/meshes.jl:247-479).  The profile is linear in the four parameters,
+    so its derivative along one of them is the profile with that parameter 1
+    and the others 0; each ring's vertices (r cos theta, r sin theta, z)
+    follow, and the face fields by ``polygon_geometry_jvp``.  Valid for
+    r1, r2 > 0 (the ring structure does not change under the derivative)."""
+    from .meshes import axisymmetric_mesh, wavebot_profile
+
+    prof = wavebot_profile(d1, d2, r1, r2, n_points)
+    verts, faces = axisymmetric_mesh(prof, n_theta)
+    th = 2.0 * np.pi * np.arange(int(n_theta)) / int(n_theta)
+    ct, st = np.cos(th), np.sin(th)
+    unit = {"r1": (0.0, 0.0, 1.0, 0.0), "r2": (0.0, 0.0, 0.0, 1.0),
+            "d1": (1.0, 0.0, 0.0, 0.0), "d2": (0.0, 1.0, 0.0, 0.0)}
+    out = {}
+    for name, (h1, h2, rt, rb) in unit.items():
+        dprof = wavebot_profile(h1, h2, rt, rb, n_points)
+        dv = []
+        for (r, _), (dr, dz) in zip(prof, dprof):
+            if r == 0.0:
+                dv.append((0.0, 0.0, dz))
+            else:
+                dv.extend(zip(dr * ct, dr * st, np.full(th.shape, dz)))
+        out[name] = polygon_geometry_jvp(verts, faces, np.asarray(dv, dtype=np.float64))
+    return out

@@ -1,5 +1,5 @@
-"""Panel meshes: the ``Mesh`` container, multi-body concatenation and a
-hemisphere generator.
+"""Panel meshes: the ``Mesh`` container, multi-body concatenation, a
+hemisphere generator and the reference's axisymmetric / WaveBot generators.
 
 ``Mesh`` mirrors the reference's struct (src/meshes.jl:12-37): vertices
 (V x 3), faces (N x 4, 0-based vertex indices; triangles repeat a vertex),
@@ -163,3 +163,112 @@ def mesh_two_hemispheres(radius: float = 1.0, separation: float = 5.0,
     m1 = mesh_hemisphere(radius, (0.0, 0.0, 0.0), resolution)
     m2 = mesh_hemisphere(radius, (separation, 0.0, 0.0), resolution)
     return m1 + m2
+
+
+# --------------------------------------------------------------------------
+# Axisymmetric meshes and the WaveBot (src/meshes.jl:247-479)
+# --------------------------------------------------------------------------
+
+def wavebot_profile(cylinder_height: float = 0.16, frustum_height: float = 0.37,
+                    top_radius: float = 0.88, bottom_radius: float = 0.35,
+                    n_points=(5, 10, 5)) -> np.ndarray:
+    """(r, z) points of the WaveBot profile, from the waterline down
+    (src/meshes.jl:316-350): a cylinder of ``top_radius`` from z = 0 to
+    -cylinder_height (n_cylinder points), a frustum narrowing to
+    ``bottom_radius`` over ``frustum_height`` (n_frustum - 1 more) and the
+    flat bottom to the axis (n_bottom - 1 more, the last at r = 0).
+    ``n_points = (n_bottom, n_frustum, n_cylinder)`` as in the reference;
+    lengths in metres."""
+    n_bottom, n_frustum, n_cylinder = (int(x) for x in n_points)
+    if min(n_bottom, n_frustum, n_cylinder) < 2:
+        raise ValueError("each part of the profile needs at least 2 points")
+    pts = []
+    for j in range(n_cylinder):
+        t = j / (n_cylinder - 1)
+        pts.append((top_radius, -cylinder_height * t))
+    for j in range(1, n_frustum):
+        t = j / (n_frustum - 1)
+        pts.append((top_radius + (bottom_radius - top_radius) * t, -cylinder_height - frustum_height * t))
+    z_bottom = -cylinder_height - frustum_height
+    for j in range(1, n_bottom):
+        t = j / (n_bottom - 1)
+        pts.append((bottom_radius * (1.0 - t), z_bottom))
+    return np.asarray(pts, dtype=np.float64)
+
+
+def axisymmetric_mesh(profile, n_theta: int = 72):
+    """Vertices (V x 3) and 0-based faces (N x 4) of the surface swept by a
+    profile of (r, z) points revolved about the z axis
+    (src/meshes.jl:247-314).  Each profile point becomes a ring of n_theta
+    vertices at theta = 2 pi i / n_theta, or one vertex on the axis when
+    r = 0; consecutive rings are joined by quads (i1, i3, i4, i2) (upper ring
+    i, lower ring i, lower ring i + 1, upper ring i + 1), and a ring next to
+    an axis point by triangles, stored with their last vertex repeated
+    (src/meshes.jl:366-368)."""
+    prof = np.asarray(profile, dtype=np.float64)
+    n_theta = int(n_theta)
+    if n_theta < 3:
+        raise ValueError("n_theta must be at least 3")
+    if prof.ndim != 2 or prof.shape[1] != 2 or prof.shape[0] < 2:
+        raise ValueError("profile must contain at least two (r, z) points")
+    if np.any(prof[:, 0] < 0.0):
+        raise ValueError("profile radii must be nonnegative")
+    th = 2.0 * math.pi * np.arange(n_theta) / n_theta
+    ct, st = np.cos(th), np.sin(th)
+    verts, starts, sizes = [], [], []
+    for r, z in prof:
+        starts.append(len(verts))
+        if r == 0.0:
+            sizes.append(1)
+            verts.append((0.0, 0.0, z))
+        else:
+            sizes.append(n_theta)
+            verts.extend(zip(r * ct, r * st, np.full(n_theta, z)))
+    faces = []
+    for layer in range(len(prof) - 1):
+        s1, s2 = starts[layer], starts[layer + 1]
+        n1, n2 = sizes[layer], sizes[layer + 1]
+        if n1 == 1 and n2 == 1:
+            raise ValueError("adjacent points cannot both have radius 0")
+        for i in range(n_theta):
+            i2n = (i + 1) % n_theta
+            if n1 == 1:
+                faces.append((s1, s2 + i, s2 + i2n, s2 + i2n))
+            elif n2 == 1:
+                faces.append((s1 + i, s2, s1 + i2n, s1 + i2n))
+            else:
+                faces.append((s1 + i, s2 + i, s2 + i2n, s1 + i2n))
+    return np.asarray(verts, dtype=np.float64), np.asarray(faces, dtype=np.int64)
+
+
+def polygon_geometry(vertices: np.ndarray, faces: np.ndarray):
+    """Centres, normals, areas and radii with the conventions of the
+    reference's conversion of a polygon mesh (src/meshes.jl:353-423): the
+    area-weighted centroid of triangles (a, b, c) and (a, c, d) (a triangle
+    repeats c as d, so its second triangle has no area), the unit normal of
+    (b - a) x (c - a), the area of the polygon (the two triangles) and the
+    radius |a - centre| (distance to the first vertex; ``panel_geometry``
+    takes the largest vertex distance instead)."""
+    v = vertices[faces]
+    a, b, c, d = v[:, 0], v[:, 1], v[:, 2], v[:, 3]
+    cr1 = np.cross(b - a, c - a)
+    cr2 = np.cross(c - a, d - a)
+    area1 = 0.5 * np.linalg.norm(cr1, axis=1)
+    area2 = 0.5 * np.linalg.norm(cr2, axis=1)
+    areas = area1 + area2
+    centers = ((a + b + c) / 3.0 * area1[:, None] + (a + c + d) / 3.0 * area2[:, None]) / areas[:, None]
+    normals = cr1 / np.linalg.norm(cr1, axis=1)[:, None]
+    radii = np.linalg.norm(a - centers, axis=1)
+    return centers, normals, areas, radii
+
+
+def wavebot_mesh(r1: float, r2: float, d1: float, d2: float, n_points=(5, 10, 5),
+                 n_theta: int = 72) -> Mesh:
+    """The WaveBot buoy (src/meshes.jl:458-479): top radius r1, bottom radius
+    r2, cylinder height d1, frustum height d2 (metres), revolved with n_theta
+    sectors.  The default (5, 10, 5) profile and 72 sectors give 17 x 72 =
+    1224 panels, the last ring of them triangles at the bottom centre."""
+    prof = wavebot_profile(d1, d2, r1, r2, n_points)
+    verts, faces = axisymmetric_mesh(prof, n_theta)
+    centers, normals, areas, radii = polygon_geometry(verts, faces)
+    return Mesh(verts, faces, centers, normals, areas, radii)
