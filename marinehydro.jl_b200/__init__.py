@@ -22,7 +22,7 @@ from .gradients import (MeshTangent, VjpResult, JvpResult, hydro_batch_vjp, hydr
                         hydro_batch_rrule,
                         hemisphere_tangents, two_hemispheres_tangents, polygon_geometry_jvp,
                         wavebot_tangents)
-from .power import two_body_power
+from .power import two_body_power, optimize_two_body_power
 from .design import SplitMix64, Design, designs, design_batch
 from ._native import (Context, MarineHydroError, ArgumentError, NotConvergedError,
                       SingularMatrixError, device_count, default_context)

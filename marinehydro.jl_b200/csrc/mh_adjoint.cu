@@ -1282,13 +1282,12 @@ int contract_pairs_wave(const Batch& bt, Vjp& vj, const double* d_k, int nb, int
                                 : bt.nrhs == 2 ? tape_smem<2>(nb)
                                 : bt.nrhs == 3 ? tape_smem<3>(nb)
                                                : tape_smem<0>(nb);
-            MH_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            MH_CUDA_TRY(ctx, raise_smem_cap((const void*)kern, smem));
             kern<<<dim3(nrb, cb), kAR, smem, ctx->stream>>>(bt.m->geom, n, bt.direct, vj.tape, d_k, nb, bt.nrhs, VA,
                                                             VB, VC, VD, rowpart, colpart, kpart);
         } else if (allw) {
             const size_t smem = adj_allw_smem(nb);
-            MH_CUDA_TRY(ctx, cudaFuncSetAttribute(k_adj_delh_allw, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                  (int)smem));
+            MH_CUDA_TRY(ctx, raise_smem_cap((const void*)k_adj_delh_allw, smem));
             k_adj_delh_allw<<<dim3(nrb, ncb), kAW, smem, ctx->stream>>>(bt.m->geom, n, bt.direct, tab, d_k, nb,
                                                                         bt.nrhs, VA, VB, VC, VD, rowpart, colpart,
                                                                         kpart);

@@ -7,8 +7,11 @@
 #include <stdio.h>
 
 #include <cmath>
+#include <map>
+#include <mutex>
 #include <new>
 #include <string>
+#include <utility>
 
 #include "mh_internal.h"
 
@@ -35,6 +38,22 @@ int set_err(mh_ctx* ctx, int code, const char* fmt, ...)
     if (ctx) ctx->err = buf;
     else g_create_err = buf;
     return code;
+}
+
+cudaError_t raise_smem_cap(const void* kernel, size_t bytes)
+{
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, size_t> caps;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t& cur = caps[{kernel, dev}];
+    if (bytes <= cur) return cudaSuccess;
+    if ((e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes)) != cudaSuccess)
+        return e;
+    cur = bytes;
+    return cudaSuccess;
 }
 
 void* ws_get(mh_ctx* ctx, int slot, size_t bytes)

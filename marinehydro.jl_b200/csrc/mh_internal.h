@@ -87,6 +87,12 @@ void phase_collect(mh_ctx* ctx);
 // Returns a device buffer of at least `bytes` for `slot` (nullptr + error set on failure).
 void* ws_get(mh_ctx* ctx, int slot, size_t bytes);
 
+// Opt a kernel in to `bytes` of dynamic shared memory on the current device.
+// The limit is per kernel and process-wide, so concurrent contexts that set
+// different sizes would race (one lowering it under another's launch): the
+// limit is only ever raised, under a process-wide lock.
+cudaError_t raise_smem_cap(const void* kernel, size_t bytes);
+
 // ---- kernels (mh_kernels.cu) ----
 // S, D: n x n complex128 column-major device buffers (either may be null);
 // tab: Delhommeau table or null (adaptive quadrature).

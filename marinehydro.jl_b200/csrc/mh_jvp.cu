@@ -458,8 +458,7 @@ int tangent_matrices(const Batch& bt, const Jvp& jv, const double* d_k, const do
     const int64_t n = bt.n;
     if (jv.wave_kind == 2 && tab && nb >= kJvpAllwMinFreqs) {
         const size_t smem = tan_allw_smem(nb);
-        MH_CUDA_TRY(ctx, cudaFuncSetAttribute(k_wave_tangent_allw, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)smem));
+        MH_CUDA_TRY(ctx, raise_smem_cap((const void*)k_wave_tangent_allw, smem));
         k_wave_tangent_allw<<<dim3(nblk(n, kTW), nblk(n, kGradCols)), kTW, smem, ctx->stream>>>(
             bt.m->geom, jv.tgeom, n, bt.direct, tab, d_k, d_dk, nb, jv.dSR, jv.dDR, dS, dD);
     } else {

@@ -1357,9 +1357,7 @@ cudaError_t launch_lu_solve_persist(mh_ctx* ctx, int backend, bool conj_trans, c
         const bool shared_x = xsb <= 96 * 1024;
         auto go = [&](auto kern, size_t smem) -> cudaError_t {
             cudaError_t e2;
-            if (smem && (e2 = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) !=
-                            cudaSuccess)
-                return e2;
+            if (smem && (e2 = raise_smem_cap((const void*)kern, smem)) != cudaSuccess) return e2;
             kern<<<gf, kFsThreads, smem, ctx->stream>>>(A, n, stride, Dinv, ds, X, xstride, nrhs, flags, fbad);
             return cudaSuccess;
         };

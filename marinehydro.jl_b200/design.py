@@ -71,17 +71,73 @@ class DesignResult:
     d_damping_dR: np.ndarray
 
 
-def design_batch(population, omegas, *, green_functions=None, precision="mixed", tol=1e-10, ctx=None) -> list:
-    """Heave A, B and dA/dR, dB/dR of every design at every frequency."""
+def _one_design(d: Design, om, gfs, precision, tol, ctx) -> DesignResult:
+    mesh = mesh_hemisphere(d.radius, (0.0, 0.0, 0.0), d.resolution)
+    body = FloatingBody.rigid(mesh, ["Heave"])
+    tan = hemisphere_tangents(d.radius, (0.0, 0.0, 0.0), d.resolution)["radius"]
+    r = hydro_batch_jvp(mesh, om, list(body.dofs.values()), (), tan, green_functions=gfs,
+                        precision=precision, tol=tol, ctx=ctx)
+    return DesignResult(d, mesh.nfaces, r.added_mass[0, 0].copy(), r.damping[0, 0].copy(),
+                        r.d_added_mass[0, 0].copy(), r.d_damping[0, 0].copy())
+
+
+def design_batch(population, omegas, *, green_functions=None, precision="mixed", tol=1e-10, ctx=None,
+                 workers: int = 1, device: int = 0, contexts=None) -> list:
+    """Heave A, B and dA/dR, dB/dR of every design at every frequency, in
+    the population's order.
+
+    ``workers > 1`` runs that many host threads, each with its own library
+    context (its own CUDA streams and workspace) on ``device``, taking the
+    designs largest first from a shared queue: small meshes leave most of the
+    GPU idle one at a time, and distinct contexts run concurrently (the
+    library calls release the GIL).  Every design's result is the same as
+    in a serial run (each call is deterministic and independent).
+    ``contexts`` (a list of ``Context``) gives the workers instead: one
+    thread per context, reused across calls, so their workspaces and
+    Delhommeau tables are built once rather than per call."""
     gfs = green_functions or (Rankine(), RankineReflected(), ExactGuevelDelhommeau())
     om = np.asarray(omegas, dtype=np.float64)
-    res = []
-    for d in population:
-        mesh = mesh_hemisphere(d.radius, (0.0, 0.0, 0.0), d.resolution)
-        body = FloatingBody.rigid(mesh, ["Heave"])
-        tan = hemisphere_tangents(d.radius, (0.0, 0.0, 0.0), d.resolution)["radius"]
-        r = hydro_batch_jvp(mesh, om, list(body.dofs.values()), (), tan, green_functions=gfs,
-                            precision=precision, tol=tol, ctx=ctx)
-        res.append(DesignResult(d, mesh.nfaces, r.added_mass[0, 0].copy(), r.damping[0, 0].copy(),
-                                r.d_added_mass[0, 0].copy(), r.d_damping[0, 0].copy()))
+    pop = list(population)
+    if contexts is not None:
+        contexts = list(contexts)
+        workers = len(contexts)
+    if workers <= 1 or len(pop) <= 1:
+        c = contexts[0] if contexts else ctx
+        return [_one_design(d, om, gfs, precision, tol, c) for d in pop]
+    import threading
+
+    from ._native import Context
+
+    # largest first (panels ~ n_theta^2), so the last designs taken are short
+    order = sorted(range(len(pop)), key=lambda q: -pop[q].resolution[0] * pop[q].resolution[1])
+    res = [None] * len(pop)
+    errors = []
+    lock = threading.Lock()
+    nxt = [0]
+
+    def run(given):
+        c = given if given is not None else Context(device)
+        try:
+            while True:
+                with lock:
+                    if nxt[0] >= len(order) or errors:
+                        return
+                    q = order[nxt[0]]
+                    nxt[0] += 1
+                res[q] = _one_design(pop[q], om, gfs, precision, tol, c)
+        except BaseException as e:  # noqa: BLE001 - re-raised in the caller's thread
+            with lock:
+                errors.append(e)
+        finally:
+            if given is None:
+                c.close()
+
+    nt = min(int(workers), len(pop))
+    threads = [threading.Thread(target=run, args=(contexts[t] if contexts else None,)) for t in range(nt)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    if errors:
+        raise errors[0]
     return res

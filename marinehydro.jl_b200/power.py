@@ -110,3 +110,46 @@ def two_body_power(r1: float = 1.0, dx1: float = 4.0, omega: float = 1.03, *, re
     tan_dx = cat(zero, t2["cx"])
     grads = {"r1": g[13] + r.mesh.dot(tan_r), "dx1": r.mesh.dot(tan_dx), "omega": g[12] + float(r.omegas[0])}
     return float(J.detach()), grads
+
+
+def optimize_two_body_power(r0: float = 2.0, dx0: float = 3.0, lower=(1.0, 1.0), upper=(4.0, 4.0), *,
+                            omega: float = 1.03, iterations: int = 100, g_tol: float = 1e-3, callback=None,
+                            **kw) -> dict:
+    """Maximise the two-body power over (r1, dx1) in a box
+    (paper/optimization.jl: J = power(r, dx), start (2, 3), bounds [1, 4]^2,
+    100 iterations, gradient tolerance 1e-3).  Each evaluation is one
+    ``two_body_power(..., grad=True)``: the forward batch and its adjoint on
+    the device.  The reference runs Optim's Fminbox(LBFGS()) (a barrier for
+    the box around L-BFGS); this uses scipy's L-BFGS-B, whose box handling is
+    a projection, so the two take different paths to the same bounded
+    optimum.  ``kw`` goes to ``two_body_power`` (resolution, precision,
+    green functions, ctx).  ``callback(x, J)`` sees every accepted iterate.
+    Returns {"x": (r1, dx1), "power", "iterations", "evaluations",
+    "history": [(r1, dx1, power) per iterate], "converged", "message"}."""
+    from scipy.optimize import minimize
+
+    history = []
+    evals = [0]
+    cache = {}
+
+    def f(x):
+        key = (float(x[0]), float(x[1]))
+        if key not in cache:
+            J, g = two_body_power(key[0], key[1], omega, grad=True, **kw)
+            evals[0] += 1
+            cache[key] = (-J, np.array([-g["r1"], -g["dx1"]]))
+        return cache[key]
+
+    def on_iterate(xk):
+        J = -f(xk)[0]
+        history.append((float(xk[0]), float(xk[1]), J))
+        if callback is not None:
+            callback(np.array(xk, dtype=np.float64), J)
+
+    x0 = np.array([r0, dx0], dtype=np.float64)
+    history.append((r0, dx0, -f(x0)[0]))
+    res = minimize(f, x0, jac=True, method="L-BFGS-B", bounds=list(zip(lower, upper)),
+                   callback=on_iterate, options=dict(maxiter=int(iterations), gtol=float(g_tol)))
+    return {"x": (float(res.x[0]), float(res.x[1])), "power": float(-res.fun), "iterations": int(res.nit),
+            "evaluations": evals[0], "history": history, "converged": bool(res.success),
+            "message": str(res.message)}

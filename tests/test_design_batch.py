@@ -34,3 +34,26 @@ def test_design_batch_radius_derivatives(mh, gpu):
         for got, a, b in ((r.d_added_mass_dR, p.added_mass, m.added_mass), (r.d_damping_dR, p.damping, m.damping)):
             fd = (a - b) / (2 * h)
             assert np.max(np.abs(got - fd)) <= 1e-6 * np.max(np.abs(fd))
+
+
+@pytest.mark.gpu
+def test_design_batch_concurrent_contexts_match_serial(mh, gpu):
+    """Four worker threads with a context each give, design by design, the
+    serial results (bit for bit: every call is deterministic).  Meshes of 64
+    to 1640 panels in flight together also exercise kernels whose dynamic
+    shared memory depends on the size (one process-wide limit per kernel)."""
+    pop = mh.designs(seed=3, count=24, ntheta=(8, 40))
+    om = np.linspace(0.3, 3.0, 8)
+    serial = mh.design_batch(pop, om, precision="mixed", tol=1e-12, ctx=gpu)
+    conc = mh.design_batch(pop, om, precision="mixed", tol=1e-12, workers=4)
+    ctxs = [mh.Context(0) for _ in range(3)]
+    try:
+        given = mh.design_batch(pop, om, precision="mixed", tol=1e-12, contexts=ctxs)
+    finally:
+        for c in ctxs:
+            c.close()
+    for a, b, c in zip(serial, conc, given):
+        assert a.design == b.design == c.design and a.nfaces == b.nfaces == c.nfaces
+        for f in ("added_mass", "damping", "d_added_mass_dR", "d_damping_dR"):
+            assert np.array_equal(getattr(a, f), getattr(b, f)), f
+            assert np.array_equal(getattr(a, f), getattr(c, f)), f
