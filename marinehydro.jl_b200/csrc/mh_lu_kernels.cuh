@@ -236,13 +236,14 @@ k_lu_diag64(float2* __restrict__ A, int64_t n, int64_t stride, int64_t k0, float
     }
     __syncthreads();
 #pragma unroll 1
-    for (int sz = 1; sz < NB; sz *= 2) {
+    for (int lsz = 0; (1 << lsz) < NB; ++lsz) {  // block size sz = 2^lsz: index arithmetic by shifts
+        const int sz = 1 << lsz;
         const int items = (NB / (2 * sz)) * sz * sz;  // outputs per triangle and phase
         // phase 1: -L[C,A] inv(L)[A,A] and -U[A,C] inv(U)[C,C]
         for (int e = t; e < 2 * items; e += blockDim.x) {
             const bool up = e >= items;
             const int ee = up ? e - items : e;
-            const int pr = ee / (sz * sz), i = (ee / sz) % sz, j = ee % sz;
+            const int pr = ee >> (2 * lsz), i = (ee >> lsz) & (sz - 1), j = ee & (sz - 1);
             const int a0 = 2 * sz * pr, c0 = a0 + sz;
             float2 acc = make_float2(0.f, 0.f);
             if (!up) {  // row c0 + i, column a0 + j; inv(L) is 1 on the diagonal
@@ -261,7 +262,7 @@ k_lu_diag64(float2* __restrict__ A, int64_t n, int64_t stride, int64_t k0, float
         for (int e = t; e < 2 * items; e += blockDim.x) {
             const bool up = e >= items;
             const int ee = up ? e - items : e;
-            const int pr = ee / (sz * sz), i = (ee / sz) % sz, j = ee % sz;
+            const int pr = ee >> (2 * lsz), i = (ee >> lsz) & (sz - 1), j = ee & (sz - 1);
             const int a0 = 2 * sz * pr, c0 = a0 + sz;
             const float2* T = (up ? tu_buf : tl_buf) + pr * sz * sz;
             float2 acc = make_float2(0.f, 0.f);
