@@ -1038,6 +1038,44 @@ __global__ void __launch_bounds__(256) k_sum_parts(const double* __restrict__ pa
 // O(n) terms: forces, Froude-Krylov, boundary conditions
 // ---------------------------------------------------------------------------
 
+// The frequency loops of k_adj_forces and k_adj_bc run in chunks of zper
+// frequencies (blockIdx.y), so a launch has nblk(n) x chunks CTAs instead of
+// nblk(n).  Each chunk stores its per-panel sums as lin_fields(ndof) rows
+// of cpart[chunk][field][n] (field: centre 0-2, normal 3-5, area 6, then
+// dof d component c at 7 + 3 d + c); k_adj_lin_reduce adds the chunks in
+// order into gbar and dofbar.
+__host__ __device__ inline int lin_fields(int ndof) { return 7 + 3 * ndof; }
+
+__device__ __forceinline__ void lin_chunk_store(double* __restrict__ cpart, int64_t n, int64_t i, int ndof,
+                                                const double* gc, const double* gn, double ga,
+                                                const double (*zb)[3])
+{
+    double* p = cpart + (int64_t)blockIdx.y * lin_fields(ndof) * n + i;
+    for (int c = 0; c < 3; ++c) {
+        p[c * n] = gc[c];
+        p[(3 + c) * n] = gn[c];
+    }
+    p[6 * n] = ga;
+    for (int d = 0; d < ndof; ++d)
+        for (int c = 0; c < 3; ++c) p[(7 + 3 * d + c) * n] = zb[d][c];
+}
+
+__global__ void __launch_bounds__(256)
+k_adj_lin_reduce(const double* __restrict__ cpart, int nchunk, int ndof, int64_t n, double* __restrict__ gbar,
+                 double* __restrict__ dofbar)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int F = lin_fields(ndof);
+    for (int f = 0; f < F; ++f) {
+        double s = 0.0;
+        for (int c = 0; c < nchunk; ++c) s += cpart[((int64_t)c * F + f) * n + i];
+        double* dst = f < 3 ? gbar + (GB_C + f) * n : f < 6 ? gbar + (GB_N + f - 3) * n
+                    : f == 6 ? gbar + GB_A * n : dofbar + (int64_t)(f - 7) * n;
+        dst[i] += s;
+    }
+}
+
 // Reverse of the force sums (src/waves.jl:72-85, 157-163) for the nb
 // frequencies of a chunk; thread = panel.  CF[z][q][d]: complex cotangent of
 // F_dq; CK[z][b][d]: of the Froude-Krylov force.  Writes phi-bar
@@ -1047,8 +1085,8 @@ __global__ void __launch_bounds__(256)
 k_adj_forces(const double* __restrict__ geom, int64_t n, const double* __restrict__ dofs, int ndof,
              const double* __restrict__ betas, int nbeta, const double* __restrict__ omegas, int nb,
              double rho, double gacc, const double2* __restrict__ PHI, const double2* __restrict__ CF,
-             const double2* __restrict__ CK, double2* __restrict__ PB, double* __restrict__ gbar,
-             double* __restrict__ dofbar, double* __restrict__ kpart)
+             const double2* __restrict__ CK, double2* __restrict__ PB, int zper, double* __restrict__ cpart,
+             double* __restrict__ kpart)
 {
     __shared__ double red[8];
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1067,7 +1105,8 @@ k_adj_forces(const double* __restrict__ geom, int64_t n, const double* __restric
         nzd[d] = nx * dd[ii] + ny * dd[n + ii] + nz * dd[2 * n + ii];
         md[d] = -nzd[d] * a;
     }
-    for (int z = 0; z < nb; ++z) {
+    const int zlo = (int)blockIdx.y * zper, zhi = min(nb, zlo + zper);
+    for (int z = zlo; z < zhi; ++z) {
         const double w = omegas[z], k = w * w / gacc;
         const double2* cf = CF + (int64_t)z * nrhs * ndof;
         double mb[kMaxRhs];
@@ -1123,13 +1162,7 @@ k_adj_forces(const double* __restrict__ geom, int64_t n, const double* __restric
         if (threadIdx.x == 0) kpart[(int64_t)z * gridDim.x + blockIdx.x] = s;
     }
     if (!live) return;
-    for (int c = 0; c < 3; ++c) {
-        gbar[(GB_C + c) * n + i] += gc[c];
-        gbar[(GB_N + c) * n + i] += gn[c];
-    }
-    gbar[GB_A * n + i] += ga;
-    for (int d = 0; d < ndof; ++d)
-        for (int c = 0; c < 3; ++c) dofbar[((int64_t)d * 3 + c) * n + i] += zb[d][c];
+    lin_chunk_store(cpart, n, i, ndof, gc, gn, ga, zb);
 }
 
 // Reverse of the boundary conditions (src/waves.jl:89-101, 121-142) for
@@ -1139,8 +1172,8 @@ k_adj_forces(const double* __restrict__ geom, int64_t n, const double* __restric
 __global__ void __launch_bounds__(256)
 k_adj_bc(const double* __restrict__ geom, int64_t n, const double* __restrict__ dofs, int ndof,
          const double* __restrict__ betas, int nbeta, const double* __restrict__ omegas, int nb, double gacc,
-         const double2* __restrict__ BB, double* __restrict__ gbar, double* __restrict__ dofbar,
-         double* __restrict__ kpart, double* __restrict__ wpart)
+         const double2* __restrict__ BB, int zper, double* __restrict__ cpart, double* __restrict__ kpart,
+         double* __restrict__ wpart)
 {
     __shared__ double red[8];
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1150,7 +1183,10 @@ k_adj_bc(const double* __restrict__ geom, int64_t n, const double* __restrict__ 
     const double x = geom[G_CX * n + ii], y = geom[G_CY * n + ii], zc = geom[G_CZ * n + ii];
     const double nv[3] = {geom[G_NX * n + ii], geom[G_NY * n + ii], geom[G_NZ * n + ii]};
     double gc[3] = {0.0, 0.0, 0.0}, gn[3] = {0.0, 0.0, 0.0};
-    for (int z = 0; z < nb; ++z) {
+    double zb[kMaxRhs][3];
+    for (int q = 0; q < ndof; ++q) zb[q][0] = zb[q][1] = zb[q][2] = 0.0;
+    const int zlo = (int)blockIdx.y * zper, zhi = min(nb, zlo + zper);
+    for (int z = zlo; z < zhi; ++z) {
         const double w = omegas[z], k = w * w / gacc;
         double kb = 0.0, wb = 0.0;
         for (int q = 0; q < ndof; ++q) {
@@ -1159,7 +1195,7 @@ k_adj_bc(const double* __restrict__ geom, int64_t n, const double* __restrict__ 
             const double s = -BB[((int64_t)z * nrhs + q) * n + ii].y;  // Re(conj(b-bar) (-i))
             for (int c = 0; c < 3; ++c) {
                 gn[c] += w * s * zeta[c];
-                if (live) dofbar[((int64_t)q * 3 + c) * n + i] += w * s * nv[c];
+                zb[q][c] += w * s * nv[c];
             }
             wb += s * (nv[0] * zeta[0] + nv[1] * zeta[1] + nv[2] * zeta[2]);
         }
@@ -1191,10 +1227,7 @@ k_adj_bc(const double* __restrict__ geom, int64_t n, const double* __restrict__ 
         if (threadIdx.x == 0) wpart[(int64_t)z * gridDim.x + blockIdx.x] = s;
     }
     if (!live) return;
-    for (int c = 0; c < 3; ++c) {
-        gbar[(GB_C + c) * n + i] += gc[c];
-        gbar[(GB_N + c) * n + i] += gn[c];
-    }
+    lin_chunk_store(cpart, n, i, ndof, gc, gn, 0.0, zb);
 }
 
 // ---------------------------------------------------------------------------
@@ -1247,11 +1280,13 @@ struct Vjp {
     int nwave;
 };
 
+constexpr int kLinChunks = 16;  // frequency chunks of k_adj_forces / k_adj_bc
+
 size_t part_words_needed(int64_t n, int nb)
 {
     const int64_t rb = nblk(n, std::min(kAR, kAW)), cb = nblk(n, kAC);
     const size_t pairs = (size_t)cb * kRowF * n + (size_t)rb * GB_NF * n + (size_t)nb * rb * cb;
-    const size_t lin = (size_t)2 * nb * nblk(n, 256);
+    const size_t lin = (size_t)2 * nb * nblk(n, 256) + (size_t)kLinChunks * lin_fields(kMaxRhs) * n;
     return std::max(pairs, lin);
 }
 
@@ -1328,11 +1363,14 @@ int adjoint_tail(const Batch& bt, Vjp& vj, const double* d_omegas, const double*
     const unsigned lb = nblk(n, 256);
     double* kpart = vj.part;
     double* wpart = kpart + (size_t)nb * lb;
-    k_adj_bc<<<lb, 256, 0, ctx->stream>>>(bt.m->geom, n, bt.d_dofs, bt.ndof, bt.d_betas, bt.nbeta, d_omegas,
-                                          nb, bt.g, BB, vj.gbar, vj.dofbar, kpart, wpart);
+    double* cpart = wpart + (size_t)nb * lb;
+    const int zper = (nb + kLinChunks - 1) / kLinChunks, nch = (nb + zper - 1) / zper;
+    k_adj_bc<<<dim3(lb, nch), 256, 0, ctx->stream>>>(bt.m->geom, n, bt.d_dofs, bt.ndof, bt.d_betas, bt.nbeta,
+                                                     d_omegas, nb, bt.g, BB, zper, cpart, kpart, wpart);
+    k_adj_lin_reduce<<<lb, 256, 0, ctx->stream>>>(cpart, nch, bt.ndof, n, vj.gbar, vj.dofbar);
     k_sum_parts<<<nb, 256, 0, ctx->stream>>>(kpart, lb, vj.kbar + z0);
     k_sum_parts<<<nb, 256, 0, ctx->stream>>>(wpart, lb, vj.wbar + z0);
-    ctx->launches += 3;
+    ctx->launches += 4;
     phase_end(ctx, PH_ADJ_LINEAR);
     MH_CUDA_TRY(ctx, cudaGetLastError());
     return MH_OK;
@@ -1345,14 +1383,17 @@ int seed_forces(const Batch& bt, Vjp& vj, const double* d_omegas, int nb, int z0
     const int64_t n = bt.n;
     const unsigned lb = nblk(n, 256);
     double* kpart = vj.part;
+    double* cpart = kpart + (size_t)2 * nb * lb;
+    const int zper = (nb + kLinChunks - 1) / kLinChunks, nch = (nb + zper - 1) / zper;
     phase_begin(ctx, PH_ADJ_LINEAR);
-    k_adj_forces<<<lb, 256, 0, ctx->stream>>>(bt.m->geom, n, bt.d_dofs, bt.ndof, bt.d_betas, bt.nbeta,
-                                              d_omegas, nb, bt.rho, bt.g, PHI,
-                                              vj.CF + (int64_t)z0 * bt.nrhs * bt.ndof,
-                                              vj.CK + (int64_t)z0 * bt.nbeta * bt.ndof, PB, vj.gbar,
-                                              vj.dofbar, kpart);
+    k_adj_forces<<<dim3(lb, nch), 256, 0, ctx->stream>>>(bt.m->geom, n, bt.d_dofs, bt.ndof, bt.d_betas,
+                                                         bt.nbeta, d_omegas, nb, bt.rho, bt.g, PHI,
+                                                         vj.CF + (int64_t)z0 * bt.nrhs * bt.ndof,
+                                                         vj.CK + (int64_t)z0 * bt.nbeta * bt.ndof, PB, zper,
+                                                         cpart, kpart);
+    k_adj_lin_reduce<<<lb, 256, 0, ctx->stream>>>(cpart, nch, bt.ndof, n, vj.gbar, vj.dofbar);
     k_sum_parts<<<nb, 256, 0, ctx->stream>>>(kpart, lb, vj.kbar + z0);
-    ctx->launches += 2;
+    ctx->launches += 3;
     phase_end(ctx, PH_ADJ_LINEAR);
     MH_CUDA_TRY(ctx, cudaGetLastError());
     return MH_OK;
