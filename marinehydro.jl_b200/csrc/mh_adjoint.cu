@@ -999,19 +999,22 @@ k_adj_near_accum(int64_t n, int direct, const unsigned short* __restrict__ ncode
     }
 }
 
-// gbar[f][i] += sum over row partials (fields 0..kRowF) and column partials
-// (fields 0..colF), in a fixed order.
+// gbar[f][i] += sum over row partials (fields 0..kRowF), then += sum over
+// column partials (fields 0..colF), each in a fixed order; field f =
+// blockIdx.y (launch max(kRowF, colF) of them), so every (panel, field) sum
+// has its own thread.
 __global__ void k_adj_reduce(int64_t n, const double* __restrict__ rowpart, int nrow, const double* __restrict__ colpart,
                              int ncol, int colF, double* __restrict__ gbar)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int f = (int)blockIdx.y;
     if (i >= n) return;
-    for (int f = 0; f < kRowF; ++f) {
+    if (f < kRowF) {
         double s = 0.0;
         for (int p = 0; p < nrow; ++p) s += rowpart[((int64_t)p * kRowF + f) * n + i];
         gbar[(int64_t)f * n + i] += s;
     }
-    for (int f = 0; f < colF; ++f) {
+    if (f < colF) {
         double s = 0.0;
         for (int p = 0; p < ncol; ++p) s += colpart[((int64_t)p * colF + f) * n + i];
         gbar[(int64_t)f * n + i] += s;
@@ -1332,8 +1335,8 @@ int contract_pairs_wave(const Batch& bt, Vjp& vj, const double* d_k, int nb, int
                                                                  kind == 2 ? tab : nullptr, d_k, nb, bt.nrhs,
                                                                  VA, VB, VC, VD, rowpart, colpart, kpart);
         }
-        k_adj_reduce<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, rowpart, (int)ncb, colpart, (int)nrb, kWaveF,
-                                                            vj.gbar);
+        const dim3 gr(nblk(n, 256), std::max(kRowF, kWaveF));
+        k_adj_reduce<<<gr, 256, 0, ctx->stream>>>(n, rowpart, (int)ncb, colpart, (int)nrb, kWaveF, vj.gbar);
         k_sum_parts<<<nb, 256, 0, ctx->stream>>>(kpart, (int64_t)nrb * ncb, vj.kbar + z0);
         ctx->launches += 3;
         MH_CUDA_TRY(ctx, cudaGetLastError());
@@ -1661,8 +1664,8 @@ int hydro_batch_vjp(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double*
                                                                     colpart);
             ctx->launches += 2;
         }
-        k_adj_reduce<<<nblk(n, 256), 256, 0, ctx->stream>>>(n, rowpart, (int)cb, colpart, (int)rb, GB_NF,
-                                                            vj.gbar);
+        const dim3 gr(nblk(n, 256), std::max(kRowF, (int)GB_NF));
+        k_adj_reduce<<<gr, 256, 0, ctx->stream>>>(n, rowpart, (int)cb, colpart, (int)rb, GB_NF, vj.gbar);
         ctx->launches += 1;
         phase_end(ctx, PH_ADJ_RANKINE);
         MH_CUDA_TRY(ctx, cudaGetLastError());
