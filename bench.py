@@ -88,50 +88,96 @@ def config_dict(mesh, omegas, args):
 # --------------------------------------------------------------------------
 
 class ClockSampler:
+    """SM clock and clock-event reasons of the bench's GPU while the timed
+    region runs.  Read-only NVML queries from a background thread every
+    5 ms (the library calls release the GIL), so a timed region of tens of
+    milliseconds still gets a few dozen samples; without NVML, nvidia-smi
+    polls every 50 ms into a temporary file.  Nothing is changed on the GPU."""
+
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index: str):
-        self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+    def __init__(self, gpu_index: str, device: int = 0):
+        import threading
+
+        self.sm, self.mx, self.reasons = [], None, set()
+        self.proc = self.thread = None
+        self.stop_flag = threading.Event()
         try:
-            self.path.parent.mkdir(exist_ok=True)
-            self.fh = open(self.path, "w")
+            import pynvml as nv
+            import torch
+
+            nv.nvmlInit()
+            prop = torch.cuda.get_device_properties(device)
+            bus = f"{prop.pci_domain_id:08x}:{prop.pci_bus_id:02x}:{prop.pci_device_id:02x}.0"
+            try:
+                h = nv.nvmlDeviceGetHandleByPciBusId(bus.encode())
+            except nv.NVMLError:
+                h = nv.nvmlDeviceGetHandleByIndex(int(gpu_index))
+            self.mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            bits = [(name, getattr(nv, attr)) for name, attr in self.REASONS]
+
+            def run():
+                while not self.stop_flag.is_set():
+                    try:
+                        self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.reasons.update(name for name, bit in bits if r & bit)
+                    except nv.NVMLError:
+                        return
+                    self.stop_flag.wait(0.005)
+
+            self.thread = threading.Thread(target=run, daemon=True)
+            self.thread.start()
+            return
+        except Exception:  # noqa: BLE001 - no NVML: fall back to nvidia-smi
+            self.thread = None
+        try:
+            import tempfile
+
+            self.fh = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", gpu_index], stdout=self.fh, stderr=subprocess.DEVNULL)
+                 "-lms", "50", "-i", gpu_index], stdout=self.fh, stderr=subprocess.DEVNULL)
         except (OSError, FileNotFoundError):
             self.proc = None
 
     def stop(self):
-        if self.proc is None:
-            return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        self.fh.close()
-        rows = [r.split(",") for r in self.path.read_text().splitlines() if r.strip()]
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in rows:
-            r = [x.strip() for x in r]
-            if len(r) < 9:
-                continue
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+        elif self.proc is not None:
+            self.proc.terminate()
             try:
-                sm.append(float(r[1]))
-                mx = float(r[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, r[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        if not sm:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.fh.flush()
+            self.fh.seek(0)
+            names = [nm for nm, _ in self.REASONS]
+            for r in (x.split(",") for x in self.fh.read().splitlines() if x.strip()):
+                r = [x.strip() for x in r]
+                if len(r) < 9:
+                    continue
+                try:
+                    self.sm.append(float(r[1]))
+                    self.mx = float(r[2])
+                except ValueError:
+                    continue
+                self.reasons.update(nm for nm, v in zip(names, r[5:9]) if v.lower().startswith("active"))
+            self.fh.close()
+            os.unlink(self.fh.name)
+        else:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if not self.sm:
+            return None
+        return {"sm_mhz": statistics.median(self.sm), "sm_max_mhz": self.mx, "reasons": sorted(self.reasons),
+                "samples": len(self.sm), "source": "nvml" if self.thread is not None else "nvidia-smi"}
 
 
 # --------------------------------------------------------------------------
@@ -413,7 +459,7 @@ def run_ours(args):
     # ---- timed region (resident inputs) ----
     vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
     gpu_index = vis.split(",")[local] if vis and vis.split(",")[local].strip().isdigit() else str(local)
-    sampler = ClockSampler(gpu_index)
+    sampler = ClockSampler(gpu_index, local)
     ctx.set_profiling(True)
     launches0 = ctx.kernel_launches()
     ev0 = torch.cuda.Event(enable_timing=True)
