@@ -174,9 +174,10 @@ __device__ __forceinline__ void allw_emit(const AllwPair& q, int z, double k, co
 
 constexpr int kWT = 128;  // threads (rows) per CTA of k_wave_delh_allw
 constexpr int kAllwMaxFreqs = 128;  // frequencies per launch of k_wave_delh_allw
-// the contracted series of every row, log k and 1/k per frequency (the polar
-// table itself is read through L1: every lane reads the same coefficient)
-constexpr size_t kWaveAllwSmem = sizeof(double) * (4 * kTabNU * kWT + 2 * kAllwMaxFreqs);
+// the contracted series of every row, k, log k and 1/k per frequency (the
+// polar table itself is read through L1: every lane reads the same
+// coefficient)
+constexpr size_t kWaveAllwSmem = sizeof(double) * (4 * kTabNU * kWT + 3 * kAllwMaxFreqs);
 
 __global__ void __launch_bounds__(kWT, 3)
 k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const double* __restrict__ tab,
@@ -189,10 +190,12 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
     double* w = wsm;                               // [4 * NU][kWT]
     double* logk = w + 4 * kTabNU * kWT;           // [nb]
     double* invk = logk + kAllwMaxFreqs;           // [nb], nb <= kAllwMaxFreqs
+    double* ksm = invk + kAllwMaxFreqs;            // [nb]
     __shared__ Panel sp[kCols];
     const int64_t j0 = (int64_t)blockIdx.y * kCols;
     stage_panels(sp, geom, n, j0);
     for (int t = threadIdx.x; t < nb; t += blockDim.x) {
+        ksm[t] = kvec[t];
         logk[t] = log(kvec[t]);
         invk[t] = 1.0 / kvec[t];
     }
@@ -262,7 +265,7 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
             bool anyp = false;
 #pragma unroll
             for (int t = 0; t < kZP; ++t) {
-                kz[t] = kvec[z0 + (t < nz ? t : 0)];
+                kz[t] = ksm[z0 + (t < nz ? t : 0)];
                 const double R = kz[t] * d;
                 pz[t] = t < nz && polar_ok && R < kTabRPolar;
                 anyp |= pz[t];
