@@ -172,11 +172,17 @@ __device__ __forceinline__ void allw_emit(const AllwPair& q, int z, double k, co
     }
 }
 
+// The four polar functions' monomial-in-u coefficients in constant memory:
+// every lane of the alpha contraction reads the same coefficient, which the
+// constant cache broadcasts.  Copied from the context's table before each
+// launch; every context builds the same table, so concurrent copies write
+// identical bytes.
+__constant__ double c_polar_mono[4 * kTabPolarFn];
+
 constexpr int kWT = 128;  // threads (rows) per CTA of k_wave_delh_allw
 constexpr int kAllwMaxFreqs = 128;  // frequencies per launch of k_wave_delh_allw
 // the contracted series of every row, k, log k and 1/k per frequency (the
-// polar table itself is read through L1: every lane reads the same
-// coefficient)
+// polar coefficients are read from constant memory)
 constexpr size_t kWaveAllwSmem = sizeof(double) * (4 * kTabNU * kWT + 3 * kAllwMaxFreqs);
 
 __global__ void __launch_bounds__(kWT, 3)
@@ -186,7 +192,6 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
                  float2* __restrict__ Dlo, double2* __restrict__ tape, int* __restrict__ fall)
 {
     extern __shared__ double wsm[];
-    const double* coef = tab + kTabMonoOff;        // 4 polar tables, monomial in u
     double* w = wsm;                               // [4 * NU][kWT]
     double* logk = w + 4 * kTabNU * kWT;           // [nb]
     double* invk = logk + kAllwMaxFreqs;           // [nb], nb <= kAllwMaxFreqs
@@ -234,20 +239,20 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
             const double v2 = 2.0 * v;
 #pragma unroll 1
             for (int row = 0; row < kTabNU; ++row) {
-                const double* cr = coef + row * kTabNV;
+                const double* cr = c_polar_mono + row * kTabNV;
                 double b1[4] = {0.0, 0.0, 0.0, 0.0}, b2[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
                 for (int col = kTabNV - 1; col >= 1; --col) {
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        const double t = fma(v2, b1[q], __ldg(cr + q * kTabPolarFn + col) - b2[q]);
+                        const double t = fma(v2, b1[q], cr[q * kTabPolarFn + col] - b2[q]);
                         b2[q] = b1[q];
                         b1[q] = t;
                     }
                 }
 #pragma unroll
                 for (int q = 0; q < 4; ++q)
-                    w[(q * kTabNU + row) * kWT + tid] = fma(v, b1[q], __ldg(cr + q * kTabPolarFn) - b2[q]);
+                    w[(q * kTabNU + row) * kWT + tid] = fma(v, b1[q], cr[q * kTabPolarFn] - b2[q]);
             }
         }
         const AllwPair q{dx, dy, rho, inv_rho, p.area, sr, dr, nn3, o, wrt_first};
@@ -760,6 +765,8 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
         MH_CUDA_TRY(ctx, cudaFuncSetAttribute(k_wave_delh_allw,
                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)kWaveAllwSmem));
+        MH_CUDA_TRY(ctx, cudaMemcpyToSymbolAsync(c_polar_mono, tab + kTabMonoOff, sizeof(c_polar_mono), 0,
+                                                 cudaMemcpyDeviceToDevice, ctx->stream));
         for (int z = 0; z < nb; z += kAllwMaxFreqs) {
             const int m = std::min(kAllwMaxFreqs, nb - z);
             const int64_t off = (int64_t)z * nn;
