@@ -79,33 +79,51 @@ void* ws_get(mh_ctx* ctx, int slot, size_t bytes)
     return p;
 }
 
+namespace {
+cudaEvent_t pooled_event(mh_ctx* ctx)
+{
+    if (!ctx->ev_pool.empty()) {
+        cudaEvent_t e = ctx->ev_pool.back();
+        ctx->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    return e;
+}
+}  // namespace
+
 void phase_begin(mh_ctx* ctx, int ph)
 {
     if (!ctx->profile) return;
-    if (ctx->ev_pending[ph]) phase_collect(ctx);
-    cudaEventRecord(ctx->ev[2 * ph], ctx->stream);
+    if (ctx->ev_open[ph]) ctx->ev_pool.push_back(ctx->ev_open[ph]);
+    ctx->ev_open[ph] = pooled_event(ctx);
+    if (ctx->ev_open[ph]) cudaEventRecord(ctx->ev_open[ph], ctx->stream);
 }
 
 void phase_end(mh_ctx* ctx, int ph)
 {
-    if (!ctx->profile) return;
-    cudaEventRecord(ctx->ev[2 * ph + 1], ctx->stream);
-    ctx->ev_pending[ph] = true;
+    if (!ctx->profile || !ctx->ev_open[ph]) return;
+    cudaEvent_t e = pooled_event(ctx);
+    if (!e) return;
+    cudaEventRecord(e, ctx->stream);
+    ctx->ev_recs.push_back({ph, ctx->ev_open[ph], e});
+    ctx->ev_open[ph] = nullptr;
+    if (ctx->ev_recs.size() >= 512) phase_collect(ctx);
 }
 
 void phase_collect(mh_ctx* ctx)
 {
-    if (!ctx->profile) return;
-    cudaStreamSynchronize(ctx->stream);
-    for (int ph = 0; ph < PH_N; ++ph) {
-        if (!ctx->ev_pending[ph]) continue;
+    for (auto& r : ctx->ev_recs) {
         float ms = 0.f;
-        if (cudaEventElapsedTime(&ms, ctx->ev[2 * ph], ctx->ev[2 * ph + 1]) == cudaSuccess) {
-            ctx->phase_ms[ph] += ms;
-            ctx->phase_calls[ph] += 1;
+        if (cudaEventSynchronize(r.e) == cudaSuccess && cudaEventElapsedTime(&ms, r.b, r.e) == cudaSuccess) {
+            ctx->phase_ms[r.ph] += ms;
+            ctx->phase_calls[r.ph] += 1;
         }
-        ctx->ev_pending[ph] = false;
+        ctx->ev_pool.push_back(r.b);
+        ctx->ev_pool.push_back(r.e);
     }
+    ctx->ev_recs.clear();
     cudaGetLastError();
 }
 
@@ -341,8 +359,10 @@ int mh_ctx_destroy(mh_ctx* ctx)
     for (int s = 0; s < WS_NSLOTS; ++s)
         if (ctx->ws[s]) cudaFree(ctx->ws[s]);
     if (ctx->delh_table) cudaFree(ctx->delh_table);
-    for (int q = 0; q < 2 * PH_N; ++q)
-        if (ctx->ev[q]) cudaEventDestroy(ctx->ev[q]);
+    mh::phase_collect(ctx);
+    for (int q = 0; q < PH_N; ++q)
+        if (ctx->ev_open[q]) cudaEventDestroy(ctx->ev_open[q]);
+    for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
     if (ctx->cusolver) cusolverDnDestroy(ctx->cusolver);
     if (ctx->cublas) cublasDestroy(ctx->cublas);
     if (ctx->ev_panel) cudaEventDestroy(ctx->ev_panel);
@@ -384,17 +404,13 @@ int mh_ctx_set_profiling(mh_ctx* ctx, int enable)
 {
     int rc;
     if ((rc = check_ctx(ctx))) return rc;
-    if (enable && !ctx->ev[0]) {
-        for (int q = 0; q < 2 * PH_N; ++q)
-            if (cudaEventCreate(&ctx->ev[q]) != cudaSuccess)
-                return set_err(ctx, MH_ERR_CUDA, "cudaEventCreate failed");
-    }
     mh::phase_collect(ctx);
     ctx->profile = enable != 0;
     for (int q = 0; q < PH_N; ++q) {
         ctx->phase_ms[q] = 0.0;
         ctx->phase_calls[q] = 0;
-        ctx->ev_pending[q] = false;
+        if (ctx->ev_open[q]) ctx->ev_pool.push_back(ctx->ev_open[q]);
+        ctx->ev_open[q] = nullptr;
     }
     return MH_OK;
 }

@@ -68,8 +68,14 @@ struct mh_ctx {
     int lu_backend = MH_LU_TCGEN05_F16;
     double* delh_table = nullptr;  // device, kTabWords doubles (built on first use)
     bool profile = false;
-    cudaEvent_t ev[2 * PH_N] = {};
-    bool ev_pending[PH_N] = {};
+    // phase timing: events recorded on whichever stream issues the phase
+    struct PhaseRec {
+        int ph;
+        cudaEvent_t b, e;
+    };
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<PhaseRec> ev_recs;
+    cudaEvent_t ev_open[PH_N] = {};
     double phase_ms[PH_N] = {};
     int64_t phase_calls[PH_N] = {};
     void* ws[WS_NSLOTS] = {};
@@ -80,7 +86,8 @@ namespace mh {
 
 int set_err(mh_ctx* ctx, int code, const char* fmt, ...);
 // Phase timing (no-ops unless ctx->profile): begin/end record events on the
-// ctx stream; collect() adds the elapsed times of completed phases.
+// ctx stream current at the call; collect() waits for the recorded phases and
+// adds their elapsed times (a phase issued several times adds every span).
 void phase_begin(mh_ctx* ctx, int ph);
 void phase_end(mh_ctx* ctx, int ph);
 void phase_collect(mh_ctx* ctx);
