@@ -209,22 +209,37 @@ k_wave_tangent(int kind, const double* __restrict__ geom, const double* __restri
 constexpr int kTW = 64;  // rows (threads) per CTA
 constexpr int kTS = 4;   // series: B, C, E0, E1
 
-size_t tan_allw_smem(int nb) { return sizeof(double) * ((size_t)kTS * kTabNU * kTW + nb); }
+// contracted series of every row, then k, 1/k, log k and dk/d(direction) per frequency
+size_t tan_allw_smem(int nb) { return sizeof(double) * ((size_t)kTS * kTabNU * kTW + 4 * (size_t)nb); }
+
+// The four polar functions' Chebyshev coefficients in constant memory (every
+// lane of the alpha contraction reads the same one); copied from the
+// context's table before each launch (every context builds the same table).
+__constant__ double c_polar_cheb[kTS * kTabPolarFn];
 
 __global__ void __launch_bounds__(kTW, 5)
 k_wave_tangent_allw(const double* __restrict__ geom, const double* __restrict__ tgeom, int64_t n, int direct,
                     const double* __restrict__ tab, const double* __restrict__ kvec,
                     const double* __restrict__ dkvec, int nb, const double2* __restrict__ dSR,
-                    const double2* __restrict__ dDR, double2* __restrict__ dS, double2* __restrict__ dD)
+                    const double2* __restrict__ dDR, double2* __restrict__ dS, double2* __restrict__ dD,
+                    int* __restrict__ fall)
 {
     extern __shared__ double dsm[];
-    double* w = dsm;                    // [kTS * kTabNU][kTW]
-    double* logk = w + kTS * kTabNU * kTW;  // [nb]
+    double* w = dsm;                        // [kTS * kTabNU][kTW]
+    double* ksh = w + kTS * kTabNU * kTW;   // [nb] k
+    double* iksh = ksh + nb;                // [nb] 1/k
+    double* logk = iksh + nb;               // [nb] log k
+    double* dksh = logk + nb;               // [nb] dk
     __shared__ Panel sp[kGradCols], tp[kGradCols];
     const int64_t j0 = (int64_t)blockIdx.y * kGradCols;
     stage(sp, geom, n, j0);
     stage_t(tp, tgeom, n, j0);
-    for (int t = threadIdx.x; t < nb; t += blockDim.x) logk[t] = log(kvec[t]);
+    for (int t = threadIdx.x; t < nb; t += blockDim.x) {
+        ksh[t] = kvec[t];
+        iksh[t] = 1.0 / kvec[t];
+        logk[t] = log(kvec[t]);
+        dksh[t] = dkvec[t];
+    }
     __syncthreads();
     const int tid = threadIdx.x;
     const int64_t i = (int64_t)blockIdx.x * kTW + tid;
@@ -250,31 +265,36 @@ k_wave_tangent_allw(const double* __restrict__ geom, const double* __restrict__ 
         const double lp = log(0.5 * (rho + az1));
         const double gp = wg.dis / (rho * (rho + az1));
         const double2 sR = dSR[o], dR_ = dDR[o];
-        if (polar_ok) {
-            const double v = 4.0 * atan2(wg.dis, az1) / kPi - 1.0;
+        if (polar_ok) {  // the four functions' recurrences interleaved
+            const double v = 4.0 * atan2(wg.dis, az1) / kPi - 1.0, v2 = 2.0 * v;
 #pragma unroll 1
-            for (int q = 0; q < kTS; ++q) {
-                const double* c = tab + q * kTabPolarFn;
-#pragma unroll 1
-                for (int row = 0; row < kTabNU; ++row) {
-                    const double* cr = c + row * kTabNV;
-                    double b1 = 0.0, b2 = 0.0;
+            for (int row = 0; row < kTabNU; ++row) {
+                const double* cr = c_polar_cheb + row * kTabNV;
+                double b1[kTS] = {0.0, 0.0, 0.0, 0.0}, b2[kTS] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
-                    for (int col = kTabNV - 1; col >= 1; --col) {
-                        const double t = fma(2.0 * v, b1, __ldg(cr + col) - b2);
-                        b2 = b1;
-                        b1 = t;
+                for (int col = kTabNV - 1; col >= 1; --col) {
+#pragma unroll
+                    for (int q = 0; q < kTS; ++q) {
+                        const double t = fma(v2, b1[q], cr[q * kTabPolarFn + col] - b2[q]);
+                        b2[q] = b1[q];
+                        b1[q] = t;
                     }
-                    wt[(q * kTabNU + row) * kTW] = fma(v, b1, __ldg(cr) - b2);
                 }
+#pragma unroll
+                for (int q = 0; q < kTS; ++q) wt[(q * kTabNU + row) * kTW] = fma(v, b1[q], cr[q * kTabPolarFn] - b2[q]);
             }
         }
+        bool nfall = false;
         for (int z = 0; z < nb; ++z) {
-            const double k = kvec[z];
-            const WaveTan t = pair_tan(tx, tni, tp[jj], direct, dkvec[z]);
+            const double k = ksh[z];
             const double R = k * rho;
+            if (!(polar_ok && R < kTabRPolar)) {  // left to k_wave_tangent_allw_rest
+                nfall = true;
+                continue;
+            }
+            const WaveTan t = pair_tan(tx, tni, tp[jj], direct, dksh[z]);
             GDer o3;
-            if (polar_ok && R < kTabRPolar) {
+            {
                 const double u = 2.0 * R / kTabRPolar - 1.0, u2 = 2.0 * u;
                 double b1[kTS], b2[kTS];
 #pragma unroll
@@ -294,12 +314,62 @@ k_wave_tangent_allw(const double* __restrict__ geom, const double* __restrict__ 
                 cplx G[3];
                 const double G_re = -2.0 * sv[2] * L + sv[0], G_im = 2.0 * kPi * sv[2];
                 G[0] = mk(G_re, G_im);
-                G[1] = mk(2.0 * sv[3] * L - 2.0 * sv[2] * gp / k + sv[1], -2.0 * kPi * sv[3]);
+                G[1] = mk(2.0 * sv[3] * L - 2.0 * sv[2] * gp * iksh[z] + sv[1], -2.0 * kPi * sv[3]);
                 G[2] = mk(G_re + 2.0 / R, G_im);
                 gder_identities(G, k * wg.dis, k * wg.zs, R, o3);
-            } else {
-                delh_point_grad(tab, k * wg.dis, k * wg.zs, &o3);
             }
+            cplx ds, dDn;
+            wave_tangent(o3, wg, k, p.area, !direct, nD, t, ds, dDn);
+            dS[(int64_t)z * nn + o] = make_double2(sR.x - kI4P * ds.re, sR.y - kI4P * ds.im);
+            dD[(int64_t)z * nn + o] = make_double2(dR_.x - kI4P * dDn.re, dR_.y - kI4P * dDn.im);
+        }
+        if (nfall) *fall = 1;
+    }
+}
+
+// The (pair, frequency) tangents k_wave_tangent_allw left to the full table
+// (pairs above the free surface or at R = k d >= 2); exits at once when it
+// flagged none.  The test takes a margin of 1e-12 in R, so a pair on the
+// patch edge is written by one kernel at least (by this one last when both).
+__global__ void __launch_bounds__(kTW)
+k_wave_tangent_allw_rest(const int* __restrict__ fall, const double* __restrict__ geom,
+                         const double* __restrict__ tgeom, int64_t n, int direct, const double* __restrict__ tab,
+                         const double* __restrict__ kvec, const double* __restrict__ dkvec, int nb,
+                         const double2* __restrict__ dSR, const double2* __restrict__ dDR, double2* __restrict__ dS,
+                         double2* __restrict__ dD)
+{
+    if (*fall == 0) return;
+    __shared__ Panel sp[kGradCols], tp[kGradCols];
+    const int64_t j0 = (int64_t)blockIdx.y * kGradCols;
+    stage(sp, geom, n, j0);
+    stage_t(tp, tgeom, n, j0);
+    __syncthreads();
+    const int64_t i = (int64_t)blockIdx.x * kTW + threadIdx.x;
+    if (i >= n) return;
+    double x[3], ni[3], tx[3], tni[3];
+    for (int c = 0; c < 3; ++c) {
+        x[c] = geom[(G_CX + c) * n + i];
+        ni[c] = geom[(G_NX + c) * n + i];
+        tx[c] = tgeom[(G_CX + c) * n + i];
+        tni[c] = tgeom[(G_NX + c) * n + i];
+    }
+    const int jend = (int)min((int64_t)kGradCols, n - j0);
+    const int64_t nn = n * n;
+    for (int jj = 0; jj < jend; ++jj) {
+        const Panel& p = sp[jj];
+        const int64_t o = (j0 + jj) * n + i;
+        const double* nD = direct ? p.n : ni;
+        const WaveGeom wg = wave_geom(x, p);
+        const double rho = hypot(wg.dis, wg.zs);
+        const bool polar_ok = -wg.zs >= 0.0 && rho > 0.0;
+        const double2 sR = dSR[o], dR_ = dDR[o];
+#pragma unroll 1
+        for (int z = 0; z < nb; ++z) {
+            const double k = kvec[z];
+            if (polar_ok && k * rho < kTabRPolar * (1.0 - 1e-12)) continue;
+            const WaveTan t = pair_tan(tx, tni, tp[jj], direct, dkvec[z]);
+            GDer o3;
+            delh_point_grad(tab, k * wg.dis, k * wg.zs, &o3);
             cplx ds, dDn;
             wave_tangent(o3, wg, k, p.area, !direct, nD, t, ds, dDn);
             dS[(int64_t)z * nn + o] = make_double2(sR.x - kI4P * ds.re, sR.y - kI4P * ds.im);
@@ -458,9 +528,18 @@ int tangent_matrices(const Batch& bt, const Jvp& jv, const double* d_k, const do
     const int64_t n = bt.n;
     if (jv.wave_kind == 2 && tab && nb >= kJvpAllwMinFreqs) {
         const size_t smem = tan_allw_smem(nb);
+        auto* fall = (int*)ws_get(ctx, WS_FALL, sizeof(int));
+        if (!fall) return MH_ERR_OOM;
         MH_CUDA_TRY(ctx, raise_smem_cap((const void*)k_wave_tangent_allw, smem));
-        k_wave_tangent_allw<<<dim3(nblk(n, kTW), nblk(n, kGradCols)), kTW, smem, ctx->stream>>>(
-            bt.m->geom, jv.tgeom, n, bt.direct, tab, d_k, d_dk, nb, jv.dSR, jv.dDR, dS, dD);
+        MH_CUDA_TRY(ctx, cudaMemcpyToSymbolAsync(c_polar_cheb, tab, sizeof(c_polar_cheb), 0, cudaMemcpyDeviceToDevice,
+                                                 ctx->stream));
+        MH_CUDA_TRY(ctx, cudaMemsetAsync(fall, 0, sizeof(int), ctx->stream));
+        const dim3 g2(nblk(n, kTW), nblk(n, kGradCols));
+        k_wave_tangent_allw<<<g2, kTW, smem, ctx->stream>>>(bt.m->geom, jv.tgeom, n, bt.direct, tab, d_k, d_dk, nb,
+                                                            jv.dSR, jv.dDR, dS, dD, fall);
+        k_wave_tangent_allw_rest<<<g2, kTW, 0, ctx->stream>>>(fall, bt.m->geom, jv.tgeom, n, bt.direct, tab, d_k,
+                                                             d_dk, nb, jv.dSR, jv.dDR, dS, dD);
+        ctx->launches += 1;
     } else {
         k_wave_tangent<<<dim3(nblk(n, kJR), nblk(n, kGradCols), (unsigned)nb), kJR, 0, ctx->stream>>>(
             jv.wave_kind, bt.m->geom, jv.tgeom, n, bt.direct, jv.wave_kind == 2 ? tab : nullptr, d_k, d_dk, jv.dSR,
