@@ -586,7 +586,7 @@ def roofline(per_phase, n, args):
            "ms_per_launch": ms, "algorithmic_bytes_per_launch": alg,
            "note": ("FP64-issue bound (alpha contraction of the polar table per pair, Horner series "
                     "in R and complex arithmetic per pair and frequency; ncu at 1024 panels x 64 "
-                    "frequencies: FP64 pipe 50% active at 15% warps active, no spills); the HBM "
+                    "frequencies: FP64 pipe 64% active at 15% warps active, no spills); the HBM "
                     "fraction shows the writes are not the limit")}
     if "lu" in per_phase:
         fl = 8.0 / 3.0 * float(n) ** 3 * args.n_omega
