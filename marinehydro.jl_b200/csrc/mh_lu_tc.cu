@@ -325,6 +325,82 @@ struct PanelPairs {
     const unsigned char* U[kMaxPairs];
 };
 
+// Epilogue of a full interior tile through shared memory: C -= P (P the
+// product in TMEM) in kCChunks chunks of 32 complex columns (32 KB, one
+// column = 128 rows = 1 KB contiguous), kCBufs chunk buffers in the freed
+// operand space.  Chunks 0..kCBufs-1 are fetched at once by cp.async.bulk;
+// each chunk is updated in place by the thread of its row, made visible to
+// the async proxy, stored by cp.async.bulk and, once that store has read
+// its buffer, the buffer takes chunk + kCBufs.  Every wait is bounded:
+// false when one ran out (after waiting, bounded, for what is in flight).
+constexpr int kCCols = 32;                      // complex columns per chunk
+constexpr int kCChunks = TC_TN / kCCols;        // 4
+constexpr int kCBufs = 3;                       // chunk buffers
+constexpr uint32_t kCBytes = kCCols * TC_TM * sizeof(float2);  // 32 KB
+static_assert(kCBufs * kCBytes <= kSmemA + kSmemB, "the chunk buffers fit in the operand space");
+
+__device__ __forceinline__ void bulk_load_chunk(const float2* M, int64_t n, int64_t r0, int64_t col0,
+                                                unsigned char* buf, uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(bar), "r"(kCBytes) : "memory");
+    for (int q = 0; q < kCCols; ++q)
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                     :: "r"(smem_u32(buf + q * TC_TM * sizeof(float2))), "l"(M + (col0 + q) * n + r0),
+                        "r"((uint32_t)(TC_TM * sizeof(float2))), "r"(bar) : "memory");
+}
+
+__device__ __forceinline__ bool epilogue_bulk(float2* M, int64_t n, int64_t r0, int64_t c0, unsigned char* smem,
+                                              uint64_t* cbar, uint32_t tmem, int warp, int lane, int tid)
+{
+    const int row = warp * 32 + lane;
+    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+    if (tid == 0)
+        for (int k = 0; k < kCBufs; ++k)
+            bulk_load_chunk(M, n, r0, c0 + k * kCCols, smem + k * kCBytes, smem_u32(&cbar[k]));
+    // thread 0 issues chunk k + kCBufs at the end of iteration k, so before
+    // iteration k the loads of chunks 0 .. min(kCChunks, kCBufs + k) - 1 are issued
+    bool ok = true;
+    int k = 0;
+    for (; k < kCChunks; ++k) {
+        const int bi = k % kCBufs;
+        ok = __syncthreads_and(mbar_wait(smem_u32(&cbar[bi]), (uint32_t)((k / kCBufs) & 1))) != 0;
+        if (!ok) break;
+        float2* cs = reinterpret_cast<float2*>(smem + bi * kCBytes);
+#pragma unroll
+        for (int cc = 0; cc < kCCols / 16; ++cc) {
+            uint32_t re[16], im[16];
+            tmem_ld16(lane_base + (uint32_t)(k * kCCols + cc * 16), re);
+            tmem_ld16(lane_base + (uint32_t)(TC_TN + k * kCCols + cc * 16), im);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                float2& v = cs[(cc * 16 + q) * TC_TM + row];
+                v = make_float2(v.x - __uint_as_float(re[q]), v.y - __uint_as_float(im[q]));
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            for (int q = 0; q < kCCols; ++q)
+                asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
+                             :: "l"(M + (c0 + k * kCCols + q) * n + r0),
+                                "r"(smem_u32(cs + q * TC_TM)), "r"((uint32_t)(TC_TM * sizeof(float2)))
+                             : "memory");
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+            if (k + kCBufs < kCChunks) {  // this buffer takes chunk k + kCBufs once the store has read it
+                asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+                bulk_load_chunk(M, n, r0, c0 + (k + kCBufs) * kCCols, smem + bi * kCBytes, smem_u32(&cbar[bi]));
+            }
+        }
+    }
+    if (!ok) {  // loads of chunks k .. issued - 1 may still land: wait for them (bounded)
+        const int issued = min(kCChunks, kCBufs + k);
+        for (int j = k; j < issued; ++j) mbar_wait(smem_u32(&cbar[j % kCBufs]), (uint32_t)((j / kCBufs) & 1));
+    }
+    if (tid == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    return ok;
+}
+
 // A22 -= sum_p L21_p U12_p for one 128 x 128 complex tile (absolute tiles
 // ti, tj); the operands are the packed panels of k_lu_trsm_tc (npair <= 4
 // panel pairs, K = 64 complex each), fetched by cp.async.bulk into shared
@@ -338,7 +414,7 @@ k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int t0, int n
                PanelPairs pp, int npair, int64_t pstride, int64_t lo, int* __restrict__ bad)
 {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
-    __shared__ uint64_t mbar[2];
+    __shared__ uint64_t mbar[2 + kCBufs];
     __shared__ uint32_t tmem_slot;
     unsigned char* sA = tc_smem;
     unsigned char* sB = tc_smem + kSmemA;
@@ -364,21 +440,23 @@ k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int t0, int n
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     if (warp == 0) tmem_alloc(&tmem_slot, kTmemCols);
     const uint32_t bar_ld = smem_u32(&mbar[0]), bar_mma = smem_u32(&mbar[1]);
-    if (tid == 0) {
-        mbar_init(&mbar[0]);
-        mbar_init(&mbar[1]);
-    }
+    if (tid == 0)
+        for (int q = 0; q < 2 + kCBufs; ++q) mbar_init(&mbar[q]);
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_slot;
-    // this thread's row of C does not depend on the products: its first 32
+    // a tile wholly inside the trailing matrix (and n even, so every column
+    // of it starts on a 16-byte boundary) goes through shared memory by bulk
+    // copies after the MMAs; other tiles use per-thread loads and stores
+    const bool full = r0 >= lo && c0 >= lo && r0 + TC_TM <= n && c0 + TC_TN <= n && (n & 1) == 0;
+    // this thread's row of C does not depend on the products: its first 16
     // columns are loaded while the panel copies and the MMAs run
     const int64_t gi = r0 + warp * 32 + lane;
     const bool row_ok = gi >= lo && gi < n;
     constexpr int kEc = 16;  // columns per epilogue chunk
     float2 cv[kEc];
-    {
+    if (!full) {
         const float2* pc = M + c0 * n + gi;
 #pragma unroll
         for (int q = 0; q < kEc; ++q, pc += n) {
@@ -418,7 +496,10 @@ k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int t0, int n
         if (ok) pend_mma = -1;
     }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (ok) {
+    if (ok && full) {
+        ok = epilogue_bulk(M, n, r0, c0, tc_smem, mbar + 2, tmem, warp, lane, tid);
+        if (!ok && lane == 0) atomicExch(bad + b, 2);
+    } else if (ok) {
         const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
         // chunk cc + 1 of C is loaded before chunk cc is stored
 #pragma unroll
