@@ -4,8 +4,10 @@ Backends: FP32 on the CUDA cores (block 32) and the block-64 LU whose
 trailing update runs on tcgen05 with FP16 operands and FP32 accumulation.
 Checked by reconstruction, ||L U - A||_max / ||A||_max: <= 2e-6 for FP32,
 <= 4e-3 for the FP16 tensor-core update (operands rounded to 11 significant
-bits), on sizes that are not multiples of the tiles; and end to end through
-the batch driver, whose FP64 refinement must still reach the FP64 result.
+bits), on sizes that are not multiples of the tiles (640: several 256-column
+outer steps whose interior tiles take the bulk-copy epilogue; 641: odd, so
+every tile takes the per-thread one); and end to end through the batch
+driver, whose FP64 refinement must still reach the FP64 result.
 """
 from __future__ import annotations
 
@@ -33,7 +35,7 @@ def _reconstruct(LU):
 
 
 @pytest.mark.parametrize("backend,tol", [("simt", 2e-6), ("tcgen05", 4e-3)])
-@pytest.mark.parametrize("n", [64, 200, 320])
+@pytest.mark.parametrize("n", [64, 200, 320, 640, 641])
 def test_lowp_lu_reconstructs(mh, gpu, backend, tol, n):
     rng = np.random.default_rng(n)
     A = _bem_like(rng, 3, n)
