@@ -148,15 +148,13 @@ __device__ __forceinline__ void pack_trsm_b(const float2 (*x)[LD], unsigned char
     }
 }
 
-// k_lu_diag for NB = 64 with the block held in registers: thread t owns row
-// r = t / 8 and the eight columns g + 8 m (g = t % 8, m = 0..7), so the
-// eight owners of a row are eight consecutive lanes of one warp.  Step c of
-// the elimination publishes row c of U (final) in shared memory, one
-// barrier, then the owner of column c in each row turns it into L(r, c) and
-// passes it to the rest of the row by a warp shuffle, and every row below c
-// updates its columns right of c.  The column group of step c is kept in
-// register a[0] by rotating a after every eight steps, so the step loop
-// needs no dynamic register index and only eight steps are unrolled.  The
+// k_lu_diag for NB = 64, blocked by eight columns in shared memory: for each
+// panel P of columns 8P .. 8P+7, (1) one warp factors the panel (rows 8P ..
+// 63, two rows per lane, the pivot row passed by warp shuffles: no CTA
+// barrier inside the panel), (2) the panel's block row of U right of it is
+// solved with the panel's unit-lower 8 x 8 L, one column per thread, (3)
+// every thread applies the rank-8 update to its part of the trailing block:
+// three barriers per panel, 24 in all instead of one per column.  The
 // two triangular inverses are then built by recursive doubling from the
 // factored block in shared memory: with the inverses of the diagonal blocks
 // A and C of size s known, [A 0; B C]^-1 has the off-diagonal block
@@ -180,53 +178,102 @@ k_lu_diag64(float2* __restrict__ A, int64_t n, int64_t stride, int64_t k0, float
     auto x = reinterpret_cast<float2 (*)[kDiagLd]>(diag_smem + NB * kDiagLd);  // the two inverses
     float2* tl_buf = diag_smem + 2 * NB * kDiagLd;                               // products
     float2* tu_buf = tl_buf + 2 * 32 * 32;
-    __shared__ float2 ur[2][NB];  // row c of U, step c
     const int64_t b = blockIdx.x;
     float2* M = A + b * stride;
     const int kb = (int)min((int64_t)NB, n - k0);
-    const int t = threadIdx.x, r = t >> 3, g = t & 7, lane = t & 31;
-    const int row_lane0 = lane & ~7;
-    float2 a[8];  // a[j]: column g + 8 ((j + mc) mod 8) during column group mc
-#pragma unroll
-    for (int m = 0; m < 8; ++m) {
-        const int c = g + 8 * m;
-        a[m] = (r < kb && c < kb) ? M[(k0 + c) * n + k0 + r] : make_float2(r == c ? 1.f : 0.f, 0.f);
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+    // the block, padded with the identity past kb, column by column (coalesced)
+    for (int e = t; e < NB * NB; e += blockDim.x) {
+        const int c = e / NB, r = e % NB;
+        f[r][c] = (r < kb && c < kb) ? M[(k0 + c) * n + k0 + r] : make_float2(r == c ? 1.f : 0.f, 0.f);
     }
+    __syncthreads();
 #pragma unroll 1
-    for (int mc = 0; mc < 8; ++mc) {
+    for (int P = 0; P < NB / 8; ++P) {
+        const int p0 = 8 * P;
+        // (1) panel: lane l holds rows p0 + l and p0 + l + 32 (when < 64)
+        if (warp == 0) {
+            const int ra = p0 + lane, rb = ra + 32;
+            const bool has_a = ra < NB, has_b = rb < NB;
+            float2 va[8], vb[8];
 #pragma unroll
-        for (int cl = 0; cl < 8; ++cl) {
-            const int c = 8 * mc + cl, buf = cl & 1;
-            if (r == c) {
-#pragma unroll
-                for (int j = 0; j < 8; ++j) ur[buf][g + 8 * ((j + mc) & 7)] = a[j];
+            for (int j = 0; j < 8; ++j) {
+                va[j] = has_a ? f[ra][p0 + j] : make_float2(0.f, 0.f);
+                vb[j] = has_b ? f[rb][p0 + j] : make_float2(0.f, 0.f);
             }
-            __syncthreads();
-            const float2 piv = ur[buf][c];
-            if (r == c && g == cl && c < kb) {
-                const float mag = piv.x * piv.x + piv.y * piv.y;
-                if (!(mag > 1e-30f && mag < 3e38f)) atomicExch(bad + b, 1);
-            }
-            if (g == cl && r > c) a[0] = cdivf(a[0], piv);
-            const float2 l = make_float2(__shfl_sync(0xffffffffu, a[0].x, row_lane0 | cl),
-                                         __shfl_sync(0xffffffffu, a[0].y, row_lane0 | cl));
-            if (r > c) {
-                if (g > cl) a[0] = cfms(a[0], l, ur[buf][g + 8 * mc]);
 #pragma unroll
-                for (int j = 1; j < 8; ++j)
-                    if (j < 8 - mc) a[j] = cfms(a[j], l, ur[buf][g + 8 * (j + mc)]);
+            for (int c = 0; c < 8; ++c) {
+                // pivot row p0 + c is lane c's first row
+                float2 pr[8];
+#pragma unroll
+                for (int j = c; j < 8; ++j)
+                    pr[j] = make_float2(__shfl_sync(0xffffffffu, va[j].x, c), __shfl_sync(0xffffffffu, va[j].y, c));
+                const float2 piv = pr[c];
+                if (lane == c && p0 + c < kb) {
+                    const float mag = piv.x * piv.x + piv.y * piv.y;
+                    if (!(mag > 1e-30f && mag < 3e38f)) atomicExch(bad + b, 1);
+                }
+                // 1 / piv once per step (one division), then products
+                const float im2 = 1.f / (piv.x * piv.x + piv.y * piv.y);
+                const float2 ip = make_float2(piv.x * im2, -piv.y * im2);
+                if (has_a && ra > p0 + c) {
+                    const float2 l = make_float2(va[c].x * ip.x - va[c].y * ip.y, va[c].x * ip.y + va[c].y * ip.x);
+                    va[c] = l;
+#pragma unroll
+                    for (int j = c + 1; j < 8; ++j) va[j] = cfms(va[j], l, pr[j]);
+                }
+                if (has_b) {  // rb >= 32 > p0 + c for every panel with rows past 32
+                    const float2 l = make_float2(vb[c].x * ip.x - vb[c].y * ip.y, vb[c].x * ip.y + vb[c].y * ip.x);
+                    vb[c] = l;
+#pragma unroll
+                    for (int j = c + 1; j < 8; ++j) vb[j] = cfms(vb[j], l, pr[j]);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                if (has_a) f[ra][p0 + j] = va[j];
+                if (has_b) f[rb][p0 + j] = vb[j];
             }
         }
-        const float2 a0 = a[0];
+        __syncthreads();
+        const int q0 = p0 + 8;  // first column (and row) past the panel
+        if (q0 >= NB) break;
+        // (2) U block row: rows p0 .. p0+7, columns q0 .. 63, by the panel's unit-lower L
+        if (t < NB - q0) {
+            const int cq = q0 + t;
+            float2 u[8];
 #pragma unroll
-        for (int j = 0; j < 7; ++j) a[j] = a[j + 1];
-        a[7] = a0;
+            for (int i = 0; i < 8; ++i) u[i] = f[p0 + i][cq];
+#pragma unroll
+            for (int i = 1; i < 8; ++i)
+#pragma unroll
+                for (int k2 = 0; k2 < i; ++k2) u[i] = cfms(u[i], f[p0 + i][p0 + k2], u[k2]);
+#pragma unroll
+            for (int i = 1; i < 8; ++i) f[p0 + i][cq] = u[i];
+        }
+        __syncthreads();
+        // (3) rank-8 update of rows and columns q0 .. 63: thread t takes row
+        // q0 + t / 8 and the columns q0 + t % 8 + 8 j
+        {
+            const int r = q0 + (t >> 3), g = t & 7;
+            if (r < NB) {
+                float2 lr[8];
+#pragma unroll
+                for (int k2 = 0; k2 < 8; ++k2) lr[k2] = f[r][p0 + k2];
+                for (int cq = q0 + g; cq < NB; cq += 8) {
+                    float2 acc = f[r][cq];
+#pragma unroll
+                    for (int k2 = 0; k2 < 8; ++k2) acc = cfms(acc, lr[k2], f[p0 + k2][cq]);
+                    f[r][cq] = acc;
+                }
+            }
+        }
+        __syncthreads();
     }
-#pragma unroll
-    for (int m = 0; m < 8; ++m) {
-        const int c = g + 8 * m;
-        f[r][c] = a[m];
-        if (r < kb && c < kb) M[(k0 + c) * n + k0 + r] = a[m];
+    // the factors back over the block (coalesced)
+    for (int e = t; e < NB * NB; e += blockDim.x) {
+        const int c = e / NB, r = e % NB;
+        if (r < kb && c < kb) M[(k0 + c) * n + k0 + r] = f[r][c];
     }
     __syncthreads();
     // inverses by recursive doubling; x starts as the inverse diagonal of U
