@@ -219,7 +219,7 @@ __constant__ double c_polar_cheb[kTS * kTabPolarFn];
 
 __global__ void __launch_bounds__(kTW, 5)
 k_wave_tangent_allw(const double* __restrict__ geom, const double* __restrict__ tgeom, int64_t n, int direct,
-                    const double* __restrict__ tab, const double* __restrict__ kvec,
+                    const double* __restrict__ kvec,
                     const double* __restrict__ dkvec, int nb, const double2* __restrict__ dSR,
                     const double2* __restrict__ dDR, double2* __restrict__ dS, double2* __restrict__ dD,
                     int* __restrict__ fall)
@@ -535,7 +535,7 @@ int tangent_matrices(const Batch& bt, const Jvp& jv, const double* d_k, const do
                                                  ctx->stream));
         MH_CUDA_TRY(ctx, cudaMemsetAsync(fall, 0, sizeof(int), ctx->stream));
         const dim3 g2(nblk(n, kTW), nblk(n, kGradCols));
-        k_wave_tangent_allw<<<g2, kTW, smem, ctx->stream>>>(bt.m->geom, jv.tgeom, n, bt.direct, tab, d_k, d_dk, nb,
+        k_wave_tangent_allw<<<g2, kTW, smem, ctx->stream>>>(bt.m->geom, jv.tgeom, n, bt.direct, d_k, d_dk, nb,
                                                             jv.dSR, jv.dDR, dS, dD, fall);
         k_wave_tangent_allw_rest<<<g2, kTW, 0, ctx->stream>>>(fall, bt.m->geom, jv.tgeom, n, bt.direct, tab, d_k,
                                                              d_dk, nb, jv.dSR, jv.dDR, dS, dD);
