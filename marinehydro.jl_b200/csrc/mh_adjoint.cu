@@ -697,34 +697,6 @@ k_adj_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const do
 // Rankine terms
 // ---------------------------------------------------------------------------
 
-// One tangent direction of the near-field reverse (rankine.jl:36-61,
-// 65-123) with single dual numbers: direction dir 0..2 the centre, 3..5 the
-// normal, 6 + 3 v + c vertex v coordinate c; returns dL/d(direction),
-// L = ibar I + gb . grad, and (direction 0) the forward gradient.  One
-// direction per thread keeps the dual panel in registers.
-__device__ __forceinline__ double rankine_near_dir(const double* y, const Panel& p, double ibar, const double* gb,
-                                                int dir, double* gr)
-{
-    using d1 = dualn<1>;
-    PanelT<d1> q;
-    for (int a = 0; a < 3; ++a) {
-        q.c[a] = dconst<1>(p.c[a]);
-        q.n[a] = dconst<1>(p.n[a]);
-    }
-    for (int t = 0; t < 12; ++t) q.v[t] = dconst<1>(p.v[t]);
-    q.area = dconst<1>(p.area);
-    q.radius = dconst<1>(p.radius);
-    if (dir < 3) q.c[dir].d[0] = 1.0;
-    else if (dir < 6) q.n[dir - 3].d[0] = 1.0;
-    else q.v[dir - 6].d[0] = 1.0;
-    const d1 yd[3] = {dconst<1>(y[0]), dconst<1>(y[1]), dconst<1>(y[2])};
-    d1 I, g[3];
-    rankine_pair(yd, q, I, g);
-    if (dir == 0)
-        for (int a = 0; a < 3; ++a) gr[a] = g[a].v;
-    return ibar * I.d[0] + gb[0] * g[0].d[0] + gb[1] * g[1].d[0] + gb[2] * g[2].d[0];
-}
-
 // Far field reverse (rankine.jl:33-34): I = A/r, grad = A rb / r^3,
 // L = ibar I + gb . grad; returns dL/dy (= -dL/dc) and adds dL/dA.
 __device__ __forceinline__ void rankine_far_vjp(const double rb[3], double r, double A, double ibar,
@@ -739,20 +711,191 @@ __device__ __forceinline__ void rankine_far_vjp(const double rb[3], double r, do
     ab += ibar * ir + gdr * ir3;
 }
 
+// Reverse of rankine_pair for L = ibar I + gb . grad in one pass: out[0..2]
+// dL/dc, out[3..5] dL/dn, out[6 + 3 a + k] dL/dv_a,k, and gr the forward
+// gradient.  The forward sweep is rankine_pair's (rankine.jl:36-61, 65-123:
+// same branches and guards); the reverse walks each edge's terms back to
+// the edge vector, the normal, the point-to-vertex vectors and the vertex
+// distances, then GZ = (y - c) . n.  |GZ| is differentiated as the dual
+// numbers do (slope +1 at 0), sign(GZ) and the guards are constants.  One
+// thread per entry replaces eighteen forward passes (one per direction).
+__device__ __forceinline__ void rankine_pair_vjp(const double y[3], const Panel& p, double ibar, const double gb[3],
+                                                 double out[18], double gr[3])
+{
+#pragma unroll
+    for (int k = 0; k < 18; ++k) out[k] = 0.0;
+    const double rb[3] = {y[0] - p.c[0], y[1] - p.c[1], y[2] - p.c[2]};
+    const double r = sqrt(rb[0] * rb[0] + rb[1] * rb[1] + rb[2] * rb[2]);
+    if (r > 7.0 * p.radius) {  // far field: only the centre moves it (the area is not a direction here)
+        double yb[3], ab = 0.0;
+        rankine_far_vjp(rb, r, p.area, ibar, gb, yb, ab, gr);
+        for (int a = 0; a < 3; ++a) out[a] = -yb[a];
+        return;
+    }
+    const double GZ = rb[0] * p.n[0] + rb[1] * p.n[1] + rb[2] * p.n[2];
+    const double aGZ = fabs(GZ);
+    const double sg = signd(GZ);
+    const bool use_at = aGZ >= 1e-4 * p.radius;
+    double RR[4], DRX[4][3];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const double d0 = y[0] - p.v[3 * a], d1 = y[1] - p.v[3 * a + 1], d2 = y[2] - p.v[3 * a + 2];
+        RR[a] = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+        DRX[a][0] = d0 / RR[a];
+        DRX[a][1] = d1 / RR[a];
+        DRX[a][2] = d2 / RR[a];
+    }
+    double RRb[4] = {0.0, 0.0, 0.0, 0.0}, DRXb[4][3] = {};
+    double aGZb = 0.0, nb[3] = {0.0, 0.0, 0.0};
+    double* vb = out + 6;
+    double g[3] = {0.0, 0.0, 0.0};
+    const double w[3] = {-gb[0], -gb[1], -gb[2]};  // dL/dgg: grad = -sum over edges of gg
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int b = (a + 1) & 3;
+        const double e[3] = {p.v[3 * b] - p.v[3 * a], p.v[3 * b + 1] - p.v[3 * a + 1], p.v[3 * b + 2] - p.v[3 * a + 2]};
+        const double L = sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+        if (!(L >= 1e-3 * p.radius)) continue;
+        // ---- forward ----
+        const double u[3] = {e[0] / L, e[1] / L, e[2] / L};
+        const double GYX[3] = {p.n[1] * u[2] - p.n[2] * u[1], p.n[2] * u[0] - p.n[0] * u[2],
+                               p.n[0] * u[1] - p.n[1] * u[0]};
+        const double pa[3] = {y[0] - p.v[3 * a], y[1] - p.v[3 * a + 1], y[2] - p.v[3 * a + 2]};
+        const double GY = pa[0] * GYX[0] + pa[1] * GYX[1] + pa[2] * GYX[2];
+        const double sE = RR[b] + RR[a];
+        const double ANT = 2.0 * GY * L;
+        const double DNT = sE * sE - L * L + 2.0 * aGZ * sE;
+        const double ANL = sE + L, DNL = sE - L;
+        const double ALDEN = log(ANL / DNL);
+        const double AT = use_at ? atan2(ANT, DNT) : 0.0;
+        const double q = GY * (DNL - ANL) / (ANL * DNL);
+        const double den = ANT * ANT + DNT * DNT;
+        double ANLX[3], ANTX[3], DNTX[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            ANLX[c] = DRX[b][c] + DRX[a][c];
+            ANTX[c] = 2.0 * L * GYX[c];
+            DNTX[c] = 2.0 * (sE + aGZ) * ANLX[c] + (2.0 * sg) * sE * p.n[c];
+            g[c] -= ALDEN * GYX[c] - (2.0 * sg) * AT * p.n[c] + q * ANLX[c]
+                    - 2.0 * aGZ * (ANTX[c] * DNT - DNTX[c] * ANT) / den;
+        }
+        // ---- reverse of gg[c] (weights w[c]) ----
+        const double K = -2.0 * aGZ / den;
+        double ALDENb = 0.0, ATb = 0.0, qb = 0.0, denb = 0.0, DNTb = 0.0, ANTb = 0.0, sb = 0.0, Lb = 0.0;
+        double GYXb[3], ANLXb[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double term = ANTX[c] * DNT - DNTX[c] * ANT;
+            ALDENb += w[c] * GYX[c];
+            GYXb[c] = w[c] * ALDEN;
+            ATb += w[c] * (-2.0 * sg * p.n[c]);
+            nb[c] += w[c] * (-2.0 * sg * AT);
+            qb += w[c] * ANLX[c];
+            ANLXb[c] = w[c] * q;
+            aGZb += w[c] * (-2.0 * term / den);
+            denb += w[c] * (2.0 * aGZ * term / (den * den));
+            const double ANTXb = w[c] * K * DNT;
+            DNTb += w[c] * K * ANTX[c];
+            const double DNTXb = -w[c] * K * ANT;
+            ANTb += -w[c] * K * DNTX[c];
+            // DNTX = 2 (s + aGZ) ANLX + 2 sg s n
+            sb += DNTXb * (2.0 * ANLX[c] + 2.0 * sg * p.n[c]);
+            aGZb += DNTXb * 2.0 * ANLX[c];
+            ANLXb[c] += DNTXb * 2.0 * (sE + aGZ);
+            nb[c] += DNTXb * 2.0 * sg * sE;
+            // ANTX = 2 L GYX
+            Lb += ANTXb * 2.0 * GYX[c];
+            GYXb[c] += ANTXb * 2.0 * L;
+            // ANLX = DRX_b + DRX_a
+            DRXb[b][c] += ANLXb[c];
+            DRXb[a][c] += ANLXb[c];
+        }
+        // den = ANT^2 + DNT^2
+        ANTb += denb * 2.0 * ANT;
+        DNTb += denb * 2.0 * DNT;
+        // q = GY (1/ANL - 1/DNL)
+        double GYb = qb * (1.0 / ANL - 1.0 / DNL);
+        double ANLb = -qb * GY / (ANL * ANL), DNLb = qb * GY / (DNL * DNL);
+        // integral: -2 aGZ AT (use_at) + GY ALDEN (|GY| > 1e-5)
+        if (use_at) {
+            aGZb += ibar * (-2.0 * AT);
+            ATb += ibar * (-2.0 * aGZ);
+        }
+        if (fabs(GY) > 1e-5) {
+            GYb += ibar * ALDEN;
+            ALDENb += ibar * GY;
+        }
+        if (use_at) {  // AT = atan2(ANT, DNT)
+            ANTb += ATb * DNT / den;
+            DNTb += -ATb * ANT / den;
+        }
+        // ALDEN = log(ANL) - log(DNL)
+        ANLb += ALDENb / ANL;
+        DNLb -= ALDENb / DNL;
+        // ANL = s + L, DNL = s - L
+        sb += ANLb + DNLb;
+        Lb += ANLb - DNLb;
+        // DNT = s^2 - L^2 + 2 aGZ s
+        sb += DNTb * (2.0 * sE + 2.0 * aGZ);
+        Lb += DNTb * (-2.0 * L);
+        aGZb += DNTb * 2.0 * sE;
+        // ANT = 2 GY L
+        GYb += ANTb * 2.0 * L;
+        Lb += ANTb * 2.0 * GY;
+        // s = RR_b + RR_a
+        RRb[b] += sb;
+        RRb[a] += sb;
+        // GY = pa . GYX, pa = y - v_a
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            GYXb[c] += GYb * pa[c];
+            vb[3 * a + c] -= GYb * GYX[c];
+        }
+        // GYX = n x u: n-bar += u x GYX-bar, u-bar = GYX-bar x n
+        nb[0] += u[1] * GYXb[2] - u[2] * GYXb[1];
+        nb[1] += u[2] * GYXb[0] - u[0] * GYXb[2];
+        nb[2] += u[0] * GYXb[1] - u[1] * GYXb[0];
+        const double ub[3] = {GYXb[1] * p.n[2] - GYXb[2] * p.n[1], GYXb[2] * p.n[0] - GYXb[0] * p.n[2],
+                              GYXb[0] * p.n[1] - GYXb[1] * p.n[0]};
+        // u = e / L, L = |e|
+        const double udot = ub[0] * u[0] + ub[1] * u[1] + ub[2] * u[2];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double eb = (ub[c] - udot * u[c]) / L + Lb * u[c];
+            vb[3 * b + c] += eb;
+            vb[3 * a + c] -= eb;
+        }
+    }
+    // RR_a = |y - v_a|, DRX_a = (y - v_a) / RR_a
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const double dd = DRXb[a][0] * DRX[a][0] + DRXb[a][1] * DRX[a][1] + DRXb[a][2] * DRX[a][2];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) vb[3 * a + c] -= (DRXb[a][c] - dd * DRX[a][c]) / RR[a] + RRb[a] * DRX[a][c];
+    }
+    // aGZ = |GZ| (slope +1 at 0, as the dual numbers), GZ = (y - c) . n
+    const double GZb = aGZb * (GZ < 0.0 ? -1.0 : 1.0);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        out[c] = -GZb * p.n[c];
+        out[3 + c] = nb[c] + GZb * rb[c];
+        gr[c] = g[c];
+    }
+}
+
 // Rankine-term contraction against the frequency sums WS = sum_w S-bar(w),
 // WD = sum_w D-bar(w) (real parts used), 128 rows x 16 columns per CTA, in
 // three kernels: k_adj_rankine reverses the far-field terms in place and
 // lists the near-field (row, column, term) entries of its CTA in row-major
 // order (global list, kNearCap codes per CTA); k_adj_near reverses every
-// listed entry along its 18 tangent directions (centre, normal, four
-// vertices), one (entry, direction) per thread over the whole matrix, so
+// listed entry by rankine_pair_vjp (cotangents of the centre, normal and
+// four vertices in one pass), one entry per thread over the whole matrix, so
 // the uneven near-field counts of the CTAs do not matter; k_adj_near_accum
 // then adds each CTA's entries to its row and column partials in list order
 // (fixed order: bitwise reproducible).  Partials as k_adj_wave with GB_NF
 // column fields.
 constexpr int kNearChunk = 128;
-constexpr int kNearDirs = 18;
-constexpr int kNearF = 21;  // per entry: direction outputs 18, normal cotangent 3
+constexpr int kNearF = 21;  // per entry: centre, normal, vertex cotangents (18), D-term normal cotangent (3)
 constexpr int kNearCap = kAR * kAC * 2;  // entries a CTA can list
 
 __global__ void __launch_bounds__(kAR)
@@ -899,10 +1042,10 @@ __device__ __forceinline__ void load_panel(const double* __restrict__ geom, int6
     p.radius = geom[G_RADIUS * n + j];
 }
 
-// Reverse of every listed near-field entry along one tangent direction per
-// thread: item w = (entry e, direction w mod 18), entries numbered CTA by
-// CTA in list order (noff); res[e][0..17] direction outputs, res[e][18..20]
-// the normal cotangent.
+// Reverse of every listed near-field entry, one entry per thread (entries
+// numbered CTA by CTA in list order, noff): res[e][0..17] the cotangents of
+// the panel's centre, normal and four vertices, res[e][18..20] the normal
+// cotangent of the D term.
 __global__ void __launch_bounds__(128, 2)
 k_adj_near(const double* __restrict__ geom, int64_t n, uint32_t mask, int direct, const double2* __restrict__ WS,
            const double2* __restrict__ WD, const unsigned short* __restrict__ ncode,
@@ -914,10 +1057,8 @@ k_adj_near(const double* __restrict__ geom, int64_t n, uint32_t mask, int direct
     const uint32_t refl = mask & (MH_GF_RANKINE_REFLECTED | MH_GF_RANKINE_REFLECTED_NEGATIVE);
     const double sgn = (refl == MH_GF_RANKINE_REFLECTED) ? 1.0 : -1.0;
     const double mref[3] = {sgn * sg, sgn * sg, sgn * sg * sz};
-    for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < total * kNearDirs;
-         w += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t e = w / kNearDirs;
-        const int dir = (int)(w % kNearDirs);
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (int64_t)gridDim.x * blockDim.x) {
         int64_t lo = 0, hi = ncta - 1;  // the last CTA whose first entry is <= e
         while (lo < hi) {
             const int64_t mid = (lo + hi + 1) >> 1;
@@ -936,10 +1077,10 @@ k_adj_near(const double* __restrict__ geom, int64_t n, uint32_t mask, int direct
         const double f[3] = {term ? mref[0] : sg, term ? mref[1] : sg, term ? mref[2] : sg};
         const double gb[3] = {-kI4P * wd * nD[0] * f[0], -kI4P * wd * nD[1] * f[1], -kI4P * wd * nD[2] * f[2]};
         const double y[3] = {xe[0], xe[1], term ? -xe[2] : xe[2]};
-        double gr[3];
-        res[e * kNearF + dir] = rankine_near_dir(y, p, (term ? sgn : 1.0) * (-kI4P * ws), gb, dir, gr);
-        if (dir == 0)
-            for (int a = 0; a < 3; ++a) res[e * kNearF + 18 + a] = -kI4P * wd * f[a] * gr[a];
+        double out[18], gr[3];
+        rankine_pair_vjp(y, p, (term ? sgn : 1.0) * (-kI4P * ws), gb, out, gr);
+        for (int k = 0; k < 18; ++k) res[e * kNearF + k] = out[k];
+        for (int a = 0; a < 3; ++a) res[e * kNearF + 18 + a] = -kI4P * wd * f[a] * gr[a];
     }
 }
 
@@ -1656,8 +1797,7 @@ int hydro_batch_vjp(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double*
         if (total > 0) {
             auto* nres = (double*)ws_get(ctx, WS_NEARRES, sizeof(double) * kNearF * (size_t)total);
             if (!nres) return MH_ERR_OOM;
-            const int64_t items = total * kNearDirs;
-            const unsigned gn = (unsigned)std::min<int64_t>((items + 127) / 128, 148 * 64);
+            const unsigned gn = (unsigned)std::min<int64_t>((total + 127) / 128, 148 * 64);
             k_adj_near<<<gn, 128, 0, ctx->stream>>>(m->geom, n, mask, direct, vj.WS, vj.WD, ncode, noff, ncta,
                                                     (int)rb, nres);
             k_adj_near_accum<<<dim3(rb, cb), kAR, 0, ctx->stream>>>(n, direct, ncode, noff, nres, rowpart,
