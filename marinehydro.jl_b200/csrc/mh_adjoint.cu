@@ -894,16 +894,18 @@ __device__ __forceinline__ void rankine_pair_vjp(const double y[3], const Panel&
 // then adds each CTA's entries to its row and column partials in list order
 // (fixed order: bitwise reproducible).  Partials as k_adj_wave with GB_NF
 // column fields.
-constexpr int kNearChunk = 128;
 constexpr int kNearF = 21;  // per entry: centre, normal, vertex cotangents (18), D-term normal cotangent (3)
 constexpr int kNearCap = kAR * kAC * 2;  // entries a CTA can list
 
 __global__ void __launch_bounds__(kAR)
 k_adj_rankine(const double* __restrict__ geom, int64_t n, uint32_t mask, int direct,
               const double2* __restrict__ WS, const double2* __restrict__ WD, double* __restrict__ rowpart,
-              double* __restrict__ colpart, unsigned short* __restrict__ ncode, int* __restrict__ ncount)
+              double* __restrict__ colpart, unsigned short* __restrict__ ncode, int* __restrict__ ncount,
+              int* __restrict__ nrow, int* __restrict__ ncol, unsigned short* __restrict__ ccode)
 {
     __shared__ Panel sp[kAC];
+    __shared__ int cpre[kAC][kAR + 1];  // per column: entries of the rows before each row
+    __shared__ int cbase[kAC + 1];
     __shared__ double csm[kAR / 32][kAC][GB_NF];
     __shared__ int offs[kAR + 1];
     const int64_t j0 = (int64_t)blockIdx.y * kAC;
@@ -978,15 +980,36 @@ k_adj_rankine(const double* __restrict__ geom, int64_t n, uint32_t mask, int dir
         for (int t = 1; t <= kAR; ++t) offs[t] += offs[t - 1];
     __syncthreads();
     const int64_t cta = (int64_t)blockIdx.y * gridDim.x + blockIdx.x;
+    // the same entries in column order (column, then row, then term): per
+    // column an exclusive count over the rows, then the column bases
+    for (int jj = 0; jj < kAC; ++jj) cpre[jj][tid + 1] = __popc((near >> (2 * jj)) & 3u);
+    if (tid < kAC) cpre[tid][0] = 0;
+    __syncthreads();
+    if (tid < kAC)
+        for (int t = 1; t <= kAR; ++t) cpre[tid][t] += cpre[tid][t - 1];
+    __syncthreads();
+    if (tid == 0) {
+        cbase[0] = 0;
+        for (int jj = 0; jj < kAC; ++jj) cbase[jj + 1] = cbase[jj] + cpre[jj][kAR];
+    }
+    __syncthreads();
     {
         unsigned short* list = ncode + cta * kNearCap;
+        unsigned short* clist = ccode + cta * kNearCap;
         int o = offs[tid];
         for (uint32_t m = near; m; m &= m - 1) {
-            const int bit = __ffs(m) - 1;
+            const int bit = __ffs(m) - 1, jj = bit >> 1;
+            const int sub = (bit & 1) && (near & (1u << (2 * jj))) ? 1 : 0;  // term 1 after term 0
+            clist[cbase[jj] + cpre[jj][tid] + sub] = (unsigned short)o;
             list[o++] = (unsigned short)((tid << 5) | bit);
         }
     }
-    if (tid == 0) ncount[cta] = offs[kAR];
+    nrow[cta * (kAR + 1) + tid] = offs[tid];
+    if (tid == 0) {
+        nrow[cta * (kAR + 1) + kAR] = offs[kAR];
+        ncount[cta] = offs[kAR];
+    }
+    if (tid < kAC) ncol[cta * kAC + tid] = cpre[tid][kAR];
     for (int t = threadIdx.x; t < jend * GB_NF; t += blockDim.x) {
         const int jj = t / GB_NF, f = t % GB_NF;
         double s = 0.0;
@@ -1084,59 +1107,64 @@ k_adj_near(const double* __restrict__ geom, int64_t n, uint32_t mask, int direct
     }
 }
 
-// Each CTA (grid as k_adj_rankine) adds its near-field entries, in list
-// order, to its row and column partials.
+// Each CTA (grid as k_adj_rankine) adds its near-field entries to its row
+// and column partials in list order: every row sums its own contiguous
+// segment of the row-major list (nrow), and every (column, field) sum has a
+// thread that walks the column's entries through the column-order index
+// (ccode: column, row, term), so no thread scans the whole list.  Each sum
+// runs in the same order as a walk of the row-major list would.
+constexpr int kNearColF = 18;  // column fields: centre 3, normal 3, vertices 12
 __global__ void __launch_bounds__(kAR)
-k_adj_near_accum(int64_t n, int direct, const unsigned short* __restrict__ ncode, const int64_t* __restrict__ noff,
-                 const double* __restrict__ resg, double* __restrict__ rowpart, double* __restrict__ colpart)
+k_adj_near_accum(int64_t n, int direct, const unsigned short* __restrict__ ncode,
+                 const unsigned short* __restrict__ ccode, const int* __restrict__ nrow,
+                 const int* __restrict__ ncol, const int64_t* __restrict__ noff, const double* __restrict__ resg,
+                 double* __restrict__ rowpart, double* __restrict__ colpart)
 {
-    __shared__ double res[kNearChunk][kNearF];
-    __shared__ unsigned short codes[kNearChunk];
+    __shared__ int cstart[kAC + 1];
     const int tid = threadIdx.x;
     const int64_t cta = (int64_t)blockIdx.y * gridDim.x + blockIdx.x;
     const int64_t base = noff[cta];
-    const int total = (int)(noff[cta + 1] - base);
-    if (total == 0) return;
+    if (noff[cta + 1] == base) return;
     const int64_t i = (int64_t)blockIdx.x * kAR + tid;
     const int64_t j0 = (int64_t)blockIdx.y * kAC;
-    double xb[3] = {0.0, 0.0, 0.0}, nbi[3] = {0.0, 0.0, 0.0};
-    double cl[GB_NF];  // this thread's column (tid < kAC) near sums
-    for (int f = 0; f < GB_NF; ++f) cl[f] = 0.0;
-    for (int c0 = 0; c0 < total; c0 += kNearChunk) {
-        const int m = min(kNearChunk, total - c0);
-        for (int t = tid; t < m * kNearF; t += blockDim.x) (&res[0][0])[t] = resg[(base + c0) * kNearF + t];
-        for (int t = tid; t < m; t += blockDim.x) codes[t] = ncode[cta * kNearCap + c0 + t];
-        __syncthreads();
-        for (int e = 0; e < m; ++e) {
-            const int code = codes[e];
-            const int r = code >> 5, bit = code & 31, jj = bit >> 1, term = bit & 1;
-            const double* q = res[e];
-            if (r == tid) {  // row: y-bar = -(c-bar + sum of vertex bars), mirrored back for the image
-                double yb[3];
-                for (int a = 0; a < 3; ++a) yb[a] = -(q[a] + q[6 + a] + q[9 + a] + q[12 + a] + q[15 + a]);
-                xb[0] += yb[0];
-                xb[1] += yb[1];
-                xb[2] += term ? -yb[2] : yb[2];
-                if (!direct)
-                    for (int a = 0; a < 3; ++a) nbi[a] += q[18 + a];
-            }
-            if (jj == tid) {  // column: centre, normal, vertices (+ normal cotangent when direct)
-                for (int a = 0; a < 3; ++a) {
-                    cl[GB_C + a] += q[a];
-                    cl[GB_N + a] += q[3 + a] + (direct ? q[18 + a] : 0.0);
-                }
-                for (int t = 0; t < 12; ++t) cl[GB_V + t] += q[6 + t];
-            }
-        }
-        __syncthreads();
+    if (tid == 0) {
+        cstart[0] = 0;
+        for (int jj = 0; jj < kAC; ++jj) cstart[jj + 1] = cstart[jj] + ncol[cta * kAC + jj];
     }
-    if (tid < kAC && j0 + tid < n)
-        for (int f = 0; f < GB_NF; ++f) colpart[((int64_t)blockIdx.x * GB_NF + f) * n + j0 + tid] += cl[f];
-    if (i < n) {
-        for (int c = 0; c < 3; ++c) {
-            rowpart[((int64_t)blockIdx.y * kRowF + c) * n + i] += xb[c];
-            rowpart[((int64_t)blockIdx.y * kRowF + 3 + c) * n + i] += nbi[c];
+    // rows: y-bar = -(c-bar + sum of vertex bars), mirrored back for the image
+    {
+        double xb[3] = {0.0, 0.0, 0.0}, nbi[3] = {0.0, 0.0, 0.0};
+        const int e1 = nrow[cta * (kAR + 1) + tid + 1];
+        for (int e = nrow[cta * (kAR + 1) + tid]; e < e1; ++e) {
+            const int term = ncode[cta * kNearCap + e] & 1;
+            const double* q = resg + (base + e) * kNearF;
+            double yb[3];
+            for (int a = 0; a < 3; ++a) yb[a] = -(q[a] + q[6 + a] + q[9 + a] + q[12 + a] + q[15 + a]);
+            xb[0] += yb[0];
+            xb[1] += yb[1];
+            xb[2] += term ? -yb[2] : yb[2];
+            if (!direct)
+                for (int a = 0; a < 3; ++a) nbi[a] += q[18 + a];
         }
+        if (i < n) {
+            for (int c = 0; c < 3; ++c) {
+                rowpart[((int64_t)blockIdx.y * kRowF + c) * n + i] += xb[c];
+                rowpart[((int64_t)blockIdx.y * kRowF + 3 + c) * n + i] += nbi[c];
+            }
+        }
+    }
+    __syncthreads();
+    // columns: centre, normal (+ the D term's normal cotangent when direct), vertices
+    for (int task = tid; task < kAC * kNearColF; task += blockDim.x) {
+        const int jj = task / kNearColF, f = task % kNearColF;
+        if (j0 + jj >= n) continue;
+        double sum = 0.0;
+        for (int k = cstart[jj]; k < cstart[jj + 1]; ++k) {
+            const double* q = resg + (base + ccode[cta * kNearCap + k]) * kNearF;
+            sum += (f >= 3 && f < 6) ? q[f] + (direct ? q[15 + f] : 0.0) : q[f];
+        }
+        const int gf = f < 3 ? GB_C + f : f < 6 ? GB_N + (f - 3) : GB_V + (f - 6);
+        colpart[((int64_t)blockIdx.x * GB_NF + gf) * n + j0 + jj] += sum;
     }
 }
 
@@ -1780,14 +1808,18 @@ int hydro_batch_vjp(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double*
         double* rowpart = vj.part;
         double* colpart = rowpart + (size_t)cb * kRowF * n;
         const int64_t ncta = (int64_t)rb * cb;
-        auto* nbuf = (char*)ws_get(ctx, WS_NEAR, sizeof(int64_t) * (ncta + 1) + sizeof(int) * ncta +
-                                                     sizeof(unsigned short) * kNearCap * ncta);
+        auto* nbuf = (char*)ws_get(ctx, WS_NEAR, sizeof(int64_t) * (ncta + 1) +
+                                                     sizeof(int) * ncta * (1 + (kAR + 1) + kAC) +
+                                                     2 * sizeof(unsigned short) * kNearCap * ncta);
         if (!nbuf) return MH_ERR_OOM;
         auto* noff = (int64_t*)nbuf;
         auto* ncount = (int*)(noff + ncta + 1);
-        auto* ncode = (unsigned short*)(ncount + ncta);
+        auto* nrow = ncount + ncta;                           // [cta][kAR + 1] row offsets
+        auto* ncol = nrow + ncta * (kAR + 1);                 // [cta][kAC] entries per column
+        auto* ncode = (unsigned short*)(ncol + ncta * kAC);   // [cta][kNearCap] row-major list
+        auto* ccode = ncode + ncta * kNearCap;                // [cta][kNearCap] column-order index
         k_adj_rankine<<<dim3(rb, cb), kAR, 0, ctx->stream>>>(m->geom, n, mask, direct, vj.WS, vj.WD, rowpart,
-                                                             colpart, ncode, ncount);
+                                                             colpart, ncode, ncount, nrow, ncol, ccode);
         k_near_scan<<<1, 1024, 0, ctx->stream>>>(ncount, ncta, noff);
         ctx->launches += 2;
         int64_t total = 0;
@@ -1800,8 +1832,8 @@ int hydro_batch_vjp(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double*
             const unsigned gn = (unsigned)std::min<int64_t>((total + 127) / 128, 148 * 64);
             k_adj_near<<<gn, 128, 0, ctx->stream>>>(m->geom, n, mask, direct, vj.WS, vj.WD, ncode, noff, ncta,
                                                     (int)rb, nres);
-            k_adj_near_accum<<<dim3(rb, cb), kAR, 0, ctx->stream>>>(n, direct, ncode, noff, nres, rowpart,
-                                                                    colpart);
+            k_adj_near_accum<<<dim3(rb, cb), kAR, 0, ctx->stream>>>(n, direct, ncode, ccode, nrow, ncol, noff,
+                                                                    nres, rowpart, colpart);
             ctx->launches += 2;
         }
         const dim3 gr(nblk(n, 256), std::max(kRowF, (int)GB_NF));
