@@ -545,7 +545,7 @@ k_resid_c(const double2* __restrict__ A, const double2* __restrict__ X, const do
     for (int u = 0; u < JW; ++u)
 #pragma unroll
         for (int q = 0; q < Q; ++q) ar[u][q] = ai[u][q] = 0.0;
-#pragma unroll 2
+#pragma unroll 4
     for (int64_t i = lane; i < n; i += 32) {
         double2 m[JW];
 #pragma unroll
