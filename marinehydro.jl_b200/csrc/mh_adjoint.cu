@@ -883,8 +883,8 @@ __device__ __forceinline__ void rankine_pair_vjp(const double y[3], const Panel&
     }
 }
 
-// Rankine-term contraction against the frequency sums WS = sum_w S-bar(w),
-// WD = sum_w D-bar(w) (real parts used), 128 rows x 16 columns per CTA, in
+// Rankine-term contraction against the frequency sums WS = Re sum_w S-bar(w),
+// WD = Re sum_w D-bar(w) (only the real parts enter), 128 rows x 16 columns per CTA, in
 // three kernels: k_adj_rankine reverses the far-field terms in place and
 // lists the near-field (row, column, term) entries of its CTA in row-major
 // order (global list, kNearCap codes per CTA); k_adj_near reverses every
@@ -899,7 +899,7 @@ constexpr int kNearCap = kAR * kAC * 2;  // entries a CTA can list
 
 __global__ void __launch_bounds__(kAR)
 k_adj_rankine(const double* __restrict__ geom, int64_t n, uint32_t mask, int direct,
-              const double2* __restrict__ WS, const double2* __restrict__ WD, double* __restrict__ rowpart,
+              const double* __restrict__ WS, const double* __restrict__ WD, double* __restrict__ rowpart,
               double* __restrict__ colpart, unsigned short* __restrict__ ncode, int* __restrict__ ncount,
               int* __restrict__ nrow, int* __restrict__ ncol, unsigned short* __restrict__ ccode)
 {
@@ -935,7 +935,7 @@ k_adj_rankine(const double* __restrict__ geom, int64_t n, uint32_t mask, int dir
         const double* nD = direct ? p.n : ni;
         double pb[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // centre, normal, area
         if (live) {
-            const double ws = WS[j * n + i].x, wd = WD[j * n + i].x;
+            const double ws = WS[j * n + i], wd = WD[j * n + i];
             const double ibar = -kI4P * ws;
             const double gbar[3] = {-kI4P * wd * nD[0], -kI4P * wd * nD[1], -kI4P * wd * nD[2]};
             double gt[3] = {0.0, 0.0, 0.0};
@@ -1070,8 +1070,8 @@ __device__ __forceinline__ void load_panel(const double* __restrict__ geom, int6
 // the panel's centre, normal and four vertices, res[e][18..20] the normal
 // cotangent of the D term.
 __global__ void __launch_bounds__(128, 2)
-k_adj_near(const double* __restrict__ geom, int64_t n, uint32_t mask, int direct, const double2* __restrict__ WS,
-           const double2* __restrict__ WD, const unsigned short* __restrict__ ncode,
+k_adj_near(const double* __restrict__ geom, int64_t n, uint32_t mask, int direct, const double* __restrict__ WS,
+           const double* __restrict__ WD, const unsigned short* __restrict__ ncode,
            const int64_t* __restrict__ noff, int64_t ncta, int rb, double* __restrict__ res)
 {
     const int64_t total = noff[ncta];
@@ -1096,7 +1096,7 @@ k_adj_near(const double* __restrict__ geom, int64_t n, uint32_t mask, int direct
         const double xe[3] = {geom[G_CX * n + ie], geom[G_CY * n + ie], geom[G_CZ * n + ie]};
         double nD[3];
         for (int a = 0; a < 3; ++a) nD[a] = direct ? p.n[a] : geom[(G_NX + a) * n + ie];
-        const double ws = WS[j * n + ie].x, wd = WD[j * n + ie].x;
+        const double ws = WS[j * n + ie], wd = WD[j * n + ie];
         const double f[3] = {term ? mref[0] : sg, term ? mref[1] : sg, term ? mref[2] : sg};
         const double gb[3] = {-kI4P * wd * nD[0] * f[0], -kI4P * wd * nD[1] * f[1], -kI4P * wd * nD[2] * f[2]};
         const double y[3] = {xe[0], xe[1], term ? -xe[2] : xe[2]};
@@ -1421,16 +1421,36 @@ int zgemm_ct_strided(mh_ctx* ctx, int64_t n, int nrhs, const double2* A, const d
     return MH_OK;
 }
 
-// W += alpha U V^H, U and V n x K.
-int zgemm_outer(mh_ctx* ctx, int64_t n, int64_t K, const double2* U, const double2* V, double2* W, double alpha_re)
+// out[k][i] = in[k][i].x, out[K + k][i] = in[k][i].y: K complex columns of
+// length n as 2K real ones.
+__global__ void k_split_re_im(const double2* __restrict__ in, int64_t n, int64_t K, double* __restrict__ out)
 {
-    const cuDoubleComplex alpha = make_cuDoubleComplex(alpha_re, 0.0);
-    const cuDoubleComplex beta = make_cuDoubleComplex(1.0, 0.0);
-    cublasStatus_t st = cublasZgemm(ctx->cublas, CUBLAS_OP_N, CUBLAS_OP_C, (int)n, (int)n, (int)K, &alpha,
-                                    (const cuDoubleComplex*)U, (int)n, (const cuDoubleComplex*)V, (int)n,
-                                    &beta, (cuDoubleComplex*)W, (int)n);
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n * K) return;
+    const double2 v = in[t];
+    out[t] = v.x;
+    out[n * K + t] = v.y;
+}
+
+// W += alpha Re(U V^H) = alpha (Re U Re V^T + Im U Im V^T), U and V n x K
+// complex, W n x n real: one real product over the stacked 2K columns (half
+// the flops and half the output of the complex product, whose imaginary
+// part the contraction does not use).
+int dgemm_outer_re(mh_ctx* ctx, int64_t n, int64_t K, const double2* U, const double2* V, double* W,
+                   double alpha)
+{
+    auto* U2 = (double*)ws_get(ctx, WS_REPACK, sizeof(double) * 4 * (size_t)n * K);
+    if (!U2) return MH_ERR_OOM;
+    double* V2 = U2 + 2 * n * K;
+    const unsigned g = (unsigned)((n * K + 255) / 256);
+    k_split_re_im<<<g, 256, 0, ctx->stream>>>(U, n, K, U2);
+    k_split_re_im<<<g, 256, 0, ctx->stream>>>(V, n, K, V2);
+    ctx->launches += 2;
+    const double beta = 1.0;
+    cublasStatus_t st = cublasDgemm(ctx->cublas, CUBLAS_OP_N, CUBLAS_OP_T, (int)n, (int)n, (int)(2 * K), &alpha,
+                                    U2, (int)n, V2, (int)n, &beta, W, (int)n);
     if (st != CUBLAS_STATUS_SUCCESS)
-        return set_err(ctx, MH_ERR_CUDA, "cublasZgemm (outer product) failed (%d)", (int)st);
+        return set_err(ctx, MH_ERR_CUDA, "cublasDgemm (outer product) failed (%d)", (int)st);
     return MH_OK;
 }
 
@@ -1440,8 +1460,8 @@ struct Vjp {
     double* dofbar;  // [ndof][3][n]
     double* kbar;    // [nomega]
     double* wbar;    // [nomega] explicit omega cotangent
-    double2* WS;     // n x n, sum over frequencies of S-bar (Rankine contraction)
-    double2* WD;
+    double* WS;      // n x n, real part of the sum over frequencies of S-bar (Rankine contraction)
+    double* WD;
     double2* CF;     // [nomega][nrhs][ndof]
     double2* CK;     // [nomega][nbeta][ndof]
     double* part;    // partial sums
@@ -1526,8 +1546,8 @@ int adjoint_tail(const Batch& bt, Vjp& vj, const double* d_omegas, const double*
     if (vj.rankine) {
         phase_begin(ctx, PH_ADJ_RANKINE);
         const int64_t K = (int64_t)nb * bt.nrhs;
-        if ((rc = zgemm_outer(ctx, n, K, VA, VB, vj.WS, 1.0))) return rc;
-        if ((rc = zgemm_outer(ctx, n, K, VC, VD, vj.WD, -1.0))) return rc;
+        if ((rc = dgemm_outer_re(ctx, n, K, VA, VB, vj.WS, 1.0))) return rc;
+        if ((rc = dgemm_outer_re(ctx, n, K, VC, VD, vj.WD, -1.0))) return rc;
         phase_end(ctx, PH_ADJ_RANKINE);
     }
     if ((rc = contract_pairs_wave(bt, vj, d_k, nb, z0, tab, VA, VB, VC, VD))) return rc;
@@ -1753,10 +1773,10 @@ int hydro_batch_vjp(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double*
     if (mask & MH_GF_DELHOMMEAU) vj.wave_kinds[vj.nwave++] = 2;
     const size_t nn = (size_t)n * (size_t)n;
     if (vj.rankine) {
-        vj.WS = (double2*)ws_get(ctx, WS_WSD, sizeof(double2) * nn * 2);
+        vj.WS = (double*)ws_get(ctx, WS_WSD, sizeof(double) * nn * 2);
         if (!vj.WS) return MH_ERR_OOM;
         vj.WD = vj.WS + nn;
-        MH_CUDA_TRY(ctx, cudaMemsetAsync(vj.WS, 0, sizeof(double2) * nn * 2, ctx->stream));
+        MH_CUDA_TRY(ctx, cudaMemsetAsync(vj.WS, 0, sizeof(double) * nn * 2, ctx->stream));
     }
     Batch bt{ctx, m, n, (int)ndof, (int)nbeta, nrhs, d_dofs, d_betas, rho, g, mask, direct};
     int rc = MH_OK;

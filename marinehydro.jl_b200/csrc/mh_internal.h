@@ -32,7 +32,7 @@ struct mh_mesh {
 enum WsSlot : int {
     WS_S = 0, WS_D, WS_RHS, WS_PHI, WS_TMP, WS_PIV, WS_INFO, WS_LWORK,
     WS_DOF, WS_OUT, WS_LO, WS_DINV, WS_TMP32, WS_MISC, WS_SR, WS_TMP32B, WS_PANEL, WS_FB,
-    WS_ADJ, WS_WSD, WS_PART, WS_GBAR, WS_TAPE, WS_FLAGS, WS_NEAR, WS_NEARRES, WS_FALL, WS_NSLOTS
+    WS_ADJ, WS_WSD, WS_PART, WS_GBAR, WS_TAPE, WS_FLAGS, WS_NEAR, WS_NEARRES, WS_FALL, WS_REPACK, WS_NSLOTS
 };
 
 // Largest number of right-hand sides (radiating dofs + headings) per frequency.
