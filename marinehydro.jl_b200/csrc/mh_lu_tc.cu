@@ -995,7 +995,12 @@ __device__ __forceinline__ void fs_st_release(int* p, int v)
 
 __device__ __forceinline__ float2 fs_conj(float2 a) { return make_float2(a.x, -a.y); }
 
-// Entries (r, kFsLanes j + tq), j < kFsPer, of tile (i, k) of the triangle (zero outside the matrix).
+// Column t of a tile held by entry j of the thread with lane tq of its row:
+// each thread holds the adjacent pairs (t, t + 1), t = 8 (j / 2) + 2 tq, so
+// one 16-byte shared load brings the two y entries a pair multiplies.
+__device__ __forceinline__ int fs_t(int j, int tq) { return 8 * (j >> 1) + 2 * tq + (j & 1); }
+
+// Entries (r, fs_t(j, tq)), j < kFsPer, of tile (i, k) of the triangle (zero outside the matrix).
 template <bool kCT>
 __device__ __forceinline__ void fs_load(const float2* __restrict__ M, int64_t n, int i, int k,
                                         float2 (&m)[kFsPer])
@@ -1003,10 +1008,22 @@ __device__ __forceinline__ void fs_load(const float2* __restrict__ M, int64_t n,
     constexpr int NB = 64;
     const int r = threadIdx.x / kFsLanes, tq = threadIdx.x % kFsLanes;
     const int64_t i0 = (int64_t)i * NB, k0 = (int64_t)k * NB;
+    if (i0 + NB <= n && k0 + NB <= n) {  // the whole tile inside: no checks, one row or column pointer
+        if (kCT) {
+            const float2* p = M + (i0 + r) * n + k0 + 2 * tq;
+#pragma unroll
+            for (int j = 0; j < kFsPer; ++j) m[j] = fs_conj(p[8 * (j >> 1) + (j & 1)]);
+        } else {
+            const float2* p = M + (k0 + 2 * tq) * n + i0 + r;
+#pragma unroll
+            for (int j = 0; j < kFsPer; ++j) m[j] = p[(int64_t)(8 * (j >> 1) + (j & 1)) * n];
+        }
+        return;
+    }
     const bool rok = i0 + r < n;
 #pragma unroll
     for (int j = 0; j < kFsPer; ++j) {
-        const int t = kFsLanes * j + tq;
+        const int t = fs_t(j, tq);
         m[j] = make_float2(0.f, 0.f);
         if (rok && k0 + t < n) m[j] = kCT ? fs_conj(M[(i0 + r) * n + k0 + t]) : M[(k0 + t) * n + i0 + r];
     }
@@ -1020,13 +1037,62 @@ __device__ __forceinline__ void fs_load_inv(const float2* __restrict__ Inv, floa
     const int r = threadIdx.x / kFsLanes, tq = threadIdx.x % kFsLanes;
 #pragma unroll
     for (int j = 0; j < kFsPer; ++j) {
-        const int t = kFsLanes * j + tq;
+        const int t = fs_t(j, tq);
         iv[j] = kCT ? fs_conj(Inv[r * NB + t]) : Inv[t * NB + r];
     }
 }
 
+// A staged 64 x 64 block: column-major, columns padded to kFsLd entries (an
+// unpadded column would put the four lanes of a row on one bank).
+constexpr int kFsLd = 68;
+constexpr size_t kFsStageBytes = sizeof(float2) * 64 * kFsLd;
+
+// Rows row0 .. row0 + 63, columns col0 .. col0 + 63 of the column-major
+// matrix src (leading dimension ld, both extents lim) into dst by 8-byte
+// cp.async (8 bytes keep any ld aligned); entries outside are zero-filled
+// (source size 0, with the in-range address src).
+__device__ __forceinline__ void fs_stage(float2* dst, const float2* __restrict__ src, int64_t ld, int64_t row0,
+                                         int64_t col0, int64_t lim)
+{
+    for (int e = threadIdx.x; e < 64 * 64; e += kFsThreads) {
+        const int c = e / 64, rr = e % 64;
+        const bool ok = row0 + rr < lim && col0 + c < lim;
+        const float2* g = ok ? src + (col0 + c) * ld + row0 + rr : src;
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;"
+                     :: "r"(smem_u32(dst + c * kFsLd + rr)), "l"(g), "r"(ok ? 8 : 0) : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+__device__ __forceinline__ void fs_stage_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// The entries fs_load / fs_load_inv give, from a block staged by fs_stage
+// (at (i0, k0) of the factors, or (k0, i0) for kCT; the inverse at (0, 0)).
+template <bool kCT>
+__device__ __forceinline__ void fs_from_stage(const float2* s, float2 (&m)[kFsPer])
+{
+    const int r = threadIdx.x / kFsLanes, tq = threadIdx.x % kFsLanes;
+#pragma unroll
+    for (int j = 0; j < kFsPer; ++j) {
+        const int t = fs_t(j, tq);
+        m[j] = kCT ? fs_conj(s[r * kFsLd + t]) : s[t * kFsLd + r];
+    }
+}
+
+// Two adjacent y entries (16 bytes of shared memory).  Volatile, so that it
+// stays inside the tile loop: held in registers across tiles, a thread's 16
+// entries of up to four right-hand sides would not fit beside the tiles.
+__device__ __forceinline__ float4 fs_lds4(const float2* p)
+{
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(smem_u32(p)) : "memory");
+    return v;
+}
+
 // Row r of (tile m) (src columns q0 .. q0 + nq), summed over the row's lanes
-// (every lane of the row ends with the sum).
+// (every lane of the row ends with the sum).  src: shared memory, rows
+// 16-byte aligned.
 __device__ __forceinline__ void fs_rowdot(const float2 (&m)[kFsPer], const float2 (*src)[64], int q0, int nq,
                                           float (&ax)[4], float (&ay)[4])
 {
@@ -1034,13 +1100,16 @@ __device__ __forceinline__ void fs_rowdot(const float2 (&m)[kFsPer], const float
 #pragma unroll
     for (int qq = 0; qq < 4; ++qq) ax[qq] = ay[qq] = 0.f;
 #pragma unroll
-    for (int j = 0; j < kFsPer; ++j) {
+    for (int j = 0; j < kFsPer; j += 2) {
 #pragma unroll
         for (int qq = 0; qq < 4; ++qq) {
             if (qq < nq) {
-                const float2 v = src[q0 + qq][kFsLanes * j + tq];
-                ax[qq] += m[j].x * v.x - m[j].y * v.y;
-                ay[qq] += m[j].x * v.y + m[j].y * v.x;
+                const float4 v = fs_lds4(&src[q0 + qq][fs_t(j, tq)]);
+                const float2 a = m[j], b = m[j + 1];
+                ax[qq] += a.x * v.x - a.y * v.y;
+                ay[qq] += a.x * v.y + a.y * v.x;
+                ax[qq] += b.x * v.z - b.y * v.w;
+                ay[qq] += b.x * v.w + b.y * v.z;
             }
         }
     }
@@ -1055,42 +1124,53 @@ __device__ __forceinline__ void fs_rowdot(const float2 (&m)[kFsPer], const float
 }
 
 // x_i -= T_ik y for the tile held in m; entry (q, r) of block i at
-// xb[q * xq + r] (global memory or the CTA's shared copy).
+// xb[q * xq + r] (global memory or the CTA's shared copy).  NQ > 0: exactly
+// NQ (<= 4) right-hand sides, known at compile time; 0: nrhs of them.
+template <int NQ>
 __device__ __forceinline__ void fs_apply(const float2 (&m)[kFsPer], int64_t n, int i, float2* xb, int64_t xq,
                                          const float2 (*y)[64], int nrhs)
 {
     const int r = threadIdx.x / kFsLanes, tq = threadIdx.x % kFsLanes;
     const int64_t row = (int64_t)i * 64 + r;
-    for (int q0 = 0; q0 < nrhs; q0 += 4) {
-        const int nq = min(4, nrhs - q0);
+    const int nr = NQ ? NQ : nrhs;
+    for (int q0 = 0; q0 < nr; q0 += 4) {
+        const int nq = NQ ? NQ : min(4, nrhs - q0);
         float ax[4], ay[4];
         fs_rowdot(m, y, q0, nq, ax, ay);
         if (tq == 0 && row < n)
-            for (int qq = 0; qq < nq; ++qq) {
-                float2* p = xb + (q0 + qq) * xq + r;
-                const float2 v = *p;
-                *p = make_float2(v.x - ax[qq], v.y - ay[qq]);
+#pragma unroll
+            for (int qq = 0; qq < 4; ++qq) {
+                if (qq < nq) {
+                    float2* p = xb + (q0 + qq) * xq + r;
+                    const float2 v = *p;
+                    *p = make_float2(v.x - ax[qq], v.y - ay[qq]);
+                }
             }
     }
 }
 
 // y_i = inv(T_ii) v (v complete in vs, inverse entries in iv), into ynext and
 // over x_i; then publish.  vs may be the CTA's shared copy of block i.
+template <int NQ>
 __device__ __forceinline__ void fs_solve_publish(const float2 (&iv)[kFsPer], int64_t n, int i, float2* x,
                                                  const float2 (*vs)[64], float2 (*ynext)[64], int nrhs, int* flag)
 {
     const int r = threadIdx.x / kFsLanes, tq = threadIdx.x % kFsLanes;
     const int64_t i0 = (int64_t)i * 64;
     const bool rok = i0 + r < n;
-    for (int q0 = 0; q0 < nrhs; q0 += 4) {
-        const int nq = min(4, nrhs - q0);
+    const int nr = NQ ? NQ : nrhs;
+    for (int q0 = 0; q0 < nr; q0 += 4) {
+        const int nq = NQ ? NQ : min(4, nrhs - q0);
         float ax[4], ay[4];
         fs_rowdot(iv, vs, q0, nq, ax, ay);
         if (tq == 0)
-            for (int qq = 0; qq < nq; ++qq) {
-                const float2 v = rok ? make_float2(ax[qq], ay[qq]) : make_float2(0.f, 0.f);
-                ynext[q0 + qq][r] = v;
-                if (rok) x[(int64_t)(q0 + qq) * n + i0 + r] = v;
+#pragma unroll
+            for (int qq = 0; qq < 4; ++qq) {
+                if (qq < nq) {
+                    const float2 v = rok ? make_float2(ax[qq], ay[qq]) : make_float2(0.f, 0.f);
+                    ynext[q0 + qq][r] = v;
+                    if (rok) x[(int64_t)(q0 + qq) * n + i0 + r] = v;
+                }
             }
     }
     __syncthreads();
@@ -1104,16 +1184,17 @@ __device__ __forceinline__ void fs_solve_publish(const float2 (&iv)[kFsPer], int
 // ceil(nblk / kFsCluster) * nrhs * 64 entries) from the start to the end of
 // the kernel, so the tile products update them without global round trips;
 // each solved block is still written to global memory when published.
-template <bool kCT, bool kXS>
+// NQ > 0: exactly NQ right-hand sides (<= 4), known at compile time; 0: nrhs.
+template <bool kCT, bool kXS, int NQ>
 __global__ void __cluster_dims__(kFsCluster, 1, 1) __launch_bounds__(kFsThreads, 2)
 k_lu_solve_flags(const float2* __restrict__ A, int64_t n, int64_t stride, const float2* __restrict__ Dinv,
-                 int64_t dstride, float2* X, int64_t xstride, int nrhs, int* flags, int* bad)
+                 int64_t dstride, float2* X, int64_t xstride, int nrhs, int* flags, int* bad, int stage)
 {
     constexpr int NB = 64;
-    __shared__ float2 ys[2][kMaxRhs][NB];  // y of the block being applied and of the next one
-    __shared__ float2 vs[kMaxRhs][NB];     // x of the block being solved (global x)
+    __shared__ __align__(16) float2 ys[2][kMaxRhs][NB];  // y of the block being applied and of the next one
+    __shared__ __align__(16) float2 vs[kMaxRhs][NB];     // x of the block being solved (global x)
     __shared__ int s_fail;
-    extern __shared__ float2 xs_smem[];    // kXS: [own block][nrhs][NB]
+    extern __shared__ __align__(16) float2 xs_smem[];  // kXS: [own block][nrhs][NB]; then, if stage, two staged blocks
     const int64_t b = blockIdx.x / kFsCluster;
     const int rank = (int)cluster_rank();
     const float2* M = A + b * stride;
@@ -1122,11 +1203,15 @@ k_lu_solve_flags(const float2* __restrict__ A, int64_t n, int64_t stride, const 
     const int nblk = (int)((n + NB - 1) / NB);
     int* fl = flags + b * 2 * nblk;
     const int tid = threadIdx.x;
+    if (NQ) nrhs = NQ;
     // block i's entries (q, r) at xblk(i)[q * xq + r]
     const int64_t xq = kXS ? NB : n;
     auto xblk = [&](int i) -> float2* {
         return kXS ? xs_smem + (int64_t)(i / kFsCluster) * nrhs * NB : x + (int64_t)i * NB;
     };
+    // the next block's tile and inverse diagonal block, staged during the wait for y_k
+    float2* st_tile = xs_smem + (kXS ? (int64_t)((nblk + kFsCluster - 1) / kFsCluster) * nrhs * NB : 0);
+    float2* st_inv = st_tile + NB * kFsLd;
     if (tid == 0) s_fail = 0;
     if (kXS) {
         for (int i = rank; i < nblk; i += kFsCluster) {
@@ -1145,10 +1230,9 @@ k_lu_solve_flags(const float2* __restrict__ A, int64_t n, int64_t stride, const 
         const int inv_off = (fwd != kCT) ? 0 : NB * NB;
         int* tfl = fl + tri * nblk;
         const int k_first = fwd ? 0 : nblk - 1;
-        // solve block i from its complete x (shared copy or staged), publish, keep y in ynext
-        auto solve_own = [&](int i, float2 (*ynext)[NB]) {
-            float2 iv[kFsPer];
-            fs_load_inv<kCT>(Dv + (int64_t)i * 2 * NB * NB + inv_off, iv);
+        // solve block i from its complete x (shared copy or staged) with its
+        // inverse diagonal block iv, publish, keep y in ynext
+        auto solve_own = [&](int i, float2 (*ynext)[NB], const float2 (&iv)[kFsPer]) {
             const float2 (*src)[NB] = vs;
             if (kXS) {
                 src = reinterpret_cast<const float2 (*)[NB]>(xblk(i));
@@ -1160,18 +1244,31 @@ k_lu_solve_flags(const float2* __restrict__ A, int64_t n, int64_t stride, const 
                 }
             }
             __syncthreads();
-            fs_solve_publish(iv, n, i, x, src, ynext, nrhs, tfl + i);
+            fs_solve_publish<NQ>(iv, n, i, x, src, ynext, nrhs, tfl + i);
             if (kXS) {  // the solved block becomes the next triangle's right-hand side
                 float2* xb = xblk(i);
                 for (int e = tid; e < nrhs * NB; e += blockDim.x) xb[e] = ynext[e / NB][e % NB];
             }
         };
-        if (k_first % kFsCluster == rank) solve_own(k_first, ys[0]);
+        if (k_first % kFsCluster == rank) {
+            float2 iv[kFsPer];
+            fs_load_inv<kCT>(Dv + (int64_t)k_first * 2 * NB * NB + inv_off, iv);
+            solve_own(k_first, ys[0], iv);
+        }
         for (int p = 0; p < nblk; ++p) {
             const int k = fwd ? p : nblk - 1 - p;
             const int kn = fwd ? k + 1 : k - 1;
             const bool next_mine = p + 1 < nblk && kn % kFsCluster == rank;
             float2 (*y)[NB] = ys[p & 1];
+            // the next block's tile (kn, k) and inverse diagonal block do not
+            // depend on y_k: with stage, they are copied into shared memory
+            // during the wait for it, so the hand-off chain holds no
+            // global-memory round trip but y_k's
+            if (next_mine && stage) {
+                const int64_t a0 = (int64_t)(kCT ? k : kn) * NB, b0 = (int64_t)(kCT ? kn : k) * NB;
+                fs_stage(st_tile, M, n, a0, b0, n);
+                fs_stage(st_inv, Dv + (int64_t)kn * 2 * NB * NB + inv_off, NB, 0, 0, NB);
+            }
             if (k % kFsCluster != rank) {
                 if (tid == 0 && !s_fail) {
                     int it = 0;
@@ -1188,12 +1285,17 @@ k_lu_solve_flags(const float2* __restrict__ A, int64_t n, int64_t stride, const 
                     y[q][rr] = k0 + rr < n ? __ldcg(x + (int64_t)q * n + k0 + rr) : make_float2(0.f, 0.f);
                 }
             }
+            if (next_mine && stage) fs_stage_wait();
             __syncthreads();
             if (next_mine) {  // the next block first: apply y_k to it, solve, publish
                 float2 m[kFsPer];
-                fs_load<kCT>(M, n, kn, k, m);
-                fs_apply(m, n, kn, xblk(kn), xq, y, nrhs);
-                solve_own(kn, ys[(p + 1) & 1]);
+                if (stage) fs_from_stage<kCT>(st_tile, m);
+                else fs_load<kCT>(M, n, kn, k, m);
+                fs_apply<NQ>(m, n, kn, xblk(kn), xq, y, nrhs);
+                float2 iv[kFsPer];
+                if (stage) fs_from_stage<kCT>(st_inv, iv);
+                else fs_load_inv<kCT>(Dv + (int64_t)kn * 2 * NB * NB + inv_off, iv);
+                solve_own(kn, ys[(p + 1) & 1], iv);
             }
             // the rest of this CTA's blocks after kn in the triangle's order, two tiles in flight
             int q = p + 2;
@@ -1205,8 +1307,8 @@ k_lu_solve_flags(const float2* __restrict__ A, int64_t n, int64_t stride, const 
                 float2 m1[kFsPer], m2[kFsPer];
                 fs_load<kCT>(M, n, i1, k, m1);
                 if (q2 < nblk) fs_load<kCT>(M, n, i2, k, m2);
-                fs_apply(m1, n, i1, xblk(i1), xq, y, nrhs);
-                if (q2 < nblk) fs_apply(m2, n, i2, xblk(i2), xq, y, nrhs);
+                fs_apply<NQ>(m1, n, i1, xblk(i1), xq, y, nrhs);
+                if (q2 < nblk) fs_apply<NQ>(m2, n, i2, xblk(i2), xq, y, nrhs);
             }
         }
         __syncthreads();
@@ -1436,14 +1538,45 @@ cudaError_t launch_lu_solve_persist(mh_ctx* ctx, int backend, bool conj_trans, c
         const dim3 gf((unsigned)nbatch * kFsCluster);
         const size_t xsb = sizeof(float2) * (size_t)((nblk + kFsCluster - 1) / kFsCluster) * nrhs * TC_NB;
         const bool shared_x = xsb <= 96 * 1024;
-        auto go = [&](auto kern, size_t smem) -> cudaError_t {
+        // staging of the next block (two more 34 KB blocks) only while two
+        // CTAs still fit on an SM
+        int dev = 0, sm_bytes = 0, reserved = 0;
+        if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev)) != cudaSuccess)
+            return e;
+        if ((e = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev)) != cudaSuccess)
+            return e;
+        auto go = [&](auto kern, size_t xs) -> cudaError_t {
             cudaError_t e2;
+            cudaFuncAttributes fa;
+            if ((e2 = cudaFuncGetAttributes(&fa, (const void*)kern)) != cudaSuccess) return e2;
+            const bool stage = 2 * (fa.sharedSizeBytes + xs + 2 * kFsStageBytes + (size_t)reserved) <= (size_t)sm_bytes;
+            const size_t smem = xs + (stage ? 2 * kFsStageBytes : 0);
             if (smem && (e2 = raise_smem_cap((const void*)kern, smem)) != cudaSuccess) return e2;
-            kern<<<gf, kFsThreads, smem, ctx->stream>>>(A, n, stride, Dinv, ds, X, xstride, nrhs, flags, fbad);
+            kern<<<gf, kFsThreads, smem, ctx->stream>>>(A, n, stride, Dinv, ds, X, xstride, nrhs, flags, fbad,
+                                                        stage ? 1 : 0);
             return cudaSuccess;
         };
-        if (conj_trans) e = shared_x ? go(k_lu_solve_flags<true, true>, xsb) : go(k_lu_solve_flags<true, false>, 0);
-        else e = shared_x ? go(k_lu_solve_flags<false, true>, xsb) : go(k_lu_solve_flags<false, false>, 0);
+        // right-hand-side counts 1 to 4 (radiation dofs and headings of one
+        // body) by their own compile-time variants
+        const int nq = shared_x && nrhs <= 4 ? nrhs : 0;
+        if (conj_trans) {
+            switch (nq) {
+            case 1: e = go(k_lu_solve_flags<true, true, 1>, xsb); break;
+            case 2: e = go(k_lu_solve_flags<true, true, 2>, xsb); break;
+            case 3: e = go(k_lu_solve_flags<true, true, 3>, xsb); break;
+            case 4: e = go(k_lu_solve_flags<true, true, 4>, xsb); break;
+            default: e = shared_x ? go(k_lu_solve_flags<true, true, 0>, xsb) : go(k_lu_solve_flags<true, false, 0>, 0);
+            }
+        } else {
+            switch (nq) {
+            case 1: e = go(k_lu_solve_flags<false, true, 1>, xsb); break;
+            case 2: e = go(k_lu_solve_flags<false, true, 2>, xsb); break;
+            case 3: e = go(k_lu_solve_flags<false, true, 3>, xsb); break;
+            case 4: e = go(k_lu_solve_flags<false, true, 4>, xsb); break;
+            default: e = shared_x ? go(k_lu_solve_flags<false, true, 0>, xsb) : go(k_lu_solve_flags<false, false, 0>, 0);
+            }
+        }
         if (e != cudaSuccess) return e;
     } else {
         const int64_t ds = lu_dinv_stride(n);
