@@ -116,16 +116,23 @@ def test_host_helpers_match_oracle(mh, oracle):
                       oracle.froude_krylov_force(m, w, [0, 0, 1.0]), rtol=1e-14)
 
 
-def test_mesh_is_hashable_and_digest_tracks_changes(mh):
+def test_mesh_is_hashable_and_snapshot_tracks_changes(mh):
+    """The device-mesh cache is keyed by the mesh object and re-uploads when
+    an array was changed in place or replaced by one of another shape."""
     import weakref
 
     m = mh.mesh_hemisphere(1.0, (0, 0, 0), (4, 6))
     d = weakref.WeakKeyDictionary()
     d[m] = 1
     assert d[m] == 1
-    dig = mh.api._mesh_digest(m)
+    snap = mh.api._mesh_snapshot(m)
+    assert mh.api._mesh_unchanged(snap, m)
     m.centers[0, 0] += 1e-3
-    assert mh.api._mesh_digest(m) != dig
+    assert not mh.api._mesh_unchanged(snap, m)
+    m.centers[0, 0] -= 1e-3
+    assert mh.api._mesh_unchanged(mh.api._mesh_snapshot(m), m)
+    m.areas = np.append(m.areas, 1.0)
+    assert not mh.api._mesh_unchanged(snap, m)
 
 
 def test_rigid_dofs_follow_reference(mh):
