@@ -116,13 +116,29 @@ int mh_ctx_set_delhommeau_method(mh_ctx* ctx, int method);
  * reference counterpart (the reference factors in FP64 with LAPACK). */
 int mh_ctx_set_lu_backend(mh_ctx* ctx, int backend);
 
+/* Failure injection for tests (no reference counterpart): while enabled, the
+ * flag waits of the tensor-core backend's triangular solves on this ctx wait
+ * on a flag that nothing publishes, with a limit of 64 polls, so each wait
+ * expires the way a lost hand-off would.  The solve marks its matrices:
+ * mh_lu_solve_lowp returns MH_ERR_TIMEOUT, the batched mixed paths solve the
+ * marked matrices with the FP64 LU instead (mh_batch_info.n_fallback).  The
+ * kernels still end normally and the ctx stays usable. */
+int mh_ctx_set_wait_injection(mh_ctx* ctx, int enable);
+
 /* Pivot-free low-precision LU of nbatch n x n complex matrices as the mixed
  * path computes it: A_host is nbatch x n x n complex128 column-major, LU_host
  * receives the factors (unit-lower L below the diagonal, U on and above) as
- * complex64 (interleaved float32), bad_host[b] != 0 flags a matrix with a bad
- * pivot or a timed-out tensor-core wait.  Test and diagnostic hook of the
- * factorisation that replaces LAPACK's getrf in `solve`
- * (src/matrix_assembly.jl:105-133). */
+ * complex64 (interleaved float32), bad_host[b] flags a matrix: 1 a zero or
+ * non-finite pivot, 2 a timed-out tensor-core wait.  Test and diagnostic hook
+ * of the factorisation that replaces LAPACK's getrf in `solve`
+ * (src/matrix_assembly.jl:105-133).
+ * Limits: no pivoting, so it is meant for the diagonally dominant
+ * second-kind matrices D and K of this path (partial pivoting moves no row on
+ * them); the MH_LU_TCGEN05_F16 backend rounds the trailing-update operands to
+ * FP16 without scaling, so entries of the Schur complements must stay within
+ * FP16's range (|x| < 65504, and well above 6e-5 to keep precision).  Inside
+ * the batched mixed path, a matrix outside these limits is caught by the bad
+ * marks or by the FP64 residual and solved by the pivoted FP64 LU instead. */
 int mh_lu_factor_lowp(mh_ctx* ctx, int backend, int64_t n, int64_t nbatch, const double* A_host,
                       float* LU_host, int* bad_host);
 
@@ -130,7 +146,10 @@ int mh_lu_factor_lowp(mh_ctx* ctx, int backend, int64_t n, int64_t nbatch, const
  * low-precision factors as one step of the mixed refinement does (op = the
  * identity, or the conjugate transpose when conj_trans != 0).  B_host and
  * X_host are nbatch x nrhs x n complex128 (right-hand sides contiguous, 1 <=
- * nrhs <= 16); the solve runs in FP32, X is returned widened to FP64.  Test
+ * nrhs <= 16); the solve runs in FP32, X is returned widened to FP64.
+ * Returns MH_ERR_SINGULAR when a factorisation met a zero or non-finite
+ * pivot and MH_ERR_TIMEOUT when a bounded device wait of the factorisation or
+ * of the solve ran out (X_host is then written but not meaningful).  Test
  * and diagnostic hook of the substitution that replaces LAPACK's getrs
  * (src/matrix_assembly.jl:105-133). */
 int mh_lu_solve_lowp(mh_ctx* ctx, int backend, int64_t n, int64_t nbatch, const double* A_host, int64_t nrhs,
@@ -318,7 +337,11 @@ int mh_hydro_batch_jvp(mh_ctx* ctx, const mh_mesh* mesh,
  * after the work is done.  All calls on a device share the array: calls that
  * overlap on the GPU race, so serialise them.  The first call on a device
  * looks up the array's address (cudaGetSymbolAddress) and should come before
- * any stream capture.  A bad FP32 pivot or no convergence within max_iter
+ * any stream capture; the address is kept for the life of the process, so
+ * after cudaDeviceReset of a device this entry point must not be called on
+ * it again.  A, B and X must be memory of the current device (or managed
+ * memory); a pointer to another GPU's memory or to host memory gives
+ * MH_ERR_ARG and nothing is launched.  A bad FP32 pivot or no convergence within max_iter
  * gives MH_ERR_NOT_CONVERGED (X then holds the last iterate).
  * iterations / rel_residual (host, may be NULL) report the sweeps used and
  * the final residual ratio; errors go to mh_last_error(NULL). */

@@ -53,6 +53,10 @@ class NotConvergedError(MarineHydroError):
     pass
 
 
+class DeviceTimeoutError(MarineHydroError):
+    """A bounded device-side wait ran out (MH_ERR_TIMEOUT)."""
+
+
 class SingularMatrixError(MarineHydroError):
     pass
 
@@ -72,6 +76,7 @@ SIGNATURES = {
     "mh_ctx_set_delhommeau_method": (ctypes.c_int, [_P, ctypes.c_int]),
     "mh_ctx_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
     "mh_ctx_set_lu_backend": (ctypes.c_int, [_P, ctypes.c_int]),
+    "mh_ctx_set_wait_injection": (ctypes.c_int, [_P, ctypes.c_int]),
     "mh_lu_factor_lowp": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int64, ctypes.c_int64, _D,
                                          ctypes.POINTER(ctypes.c_float),
                                          ctypes.POINTER(ctypes.c_int)]),
@@ -160,6 +165,8 @@ def check(rc: int, ctx=None):
         raise NotConvergedError(rc, msg)
     if rc == MH_ERR_SINGULAR:
         raise SingularMatrixError(rc, msg)
+    if rc == MH_ERR_TIMEOUT:
+        raise DeviceTimeoutError(rc, msg)
     raise MarineHydroError(rc, msg)
 
 
@@ -203,6 +210,11 @@ class Context:
         """'simt' (FP32 CUDA cores) or 'tcgen05' (FP16 tensor-core trailing update)."""
         code = {"simt": MH_LU_SIMT_F32, "tcgen05": MH_LU_TCGEN05_F16}[backend]
         check(lib().mh_ctx_set_lu_backend(self._h, code), self._h)
+
+    def set_wait_injection(self, enable: bool):
+        """Failure injection (tests): the triangular solves' flag waits wait
+        on a flag nothing publishes, so they expire (``mh_ctx_set_wait_injection``)."""
+        check(lib().mh_ctx_set_wait_injection(self._h, int(bool(enable))), self._h)
 
     def lu_factor_lowp(self, A, backend: str = "tcgen05"):
         """Pivot-free low-precision LU of a batch (nbatch, n, n) of complex

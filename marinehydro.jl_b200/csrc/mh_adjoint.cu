@@ -1611,7 +1611,7 @@ int adjoint_mixed_chunk(const Batch& bt, Vjp& vj, const double* d_omegas, const 
     auto* PHIi = (double2*)ctx->ws[WS_TMP];  // phi = S sigma (indirect)
     auto* adj = (double2*)ws_get(ctx, WS_ADJ, sizeof(double2) * cnt * 5);
     auto* R32 = (float2*)ws_get(ctx, WS_TMP32, sizeof(float2) * cnt);
-    auto* misc = (double*)ws_get(ctx, WS_MISC, (sizeof(double) + sizeof(int)) * nb + 64);
+    auto* misc = ws_get(ctx, WS_MISC, refine_ctl_bytes(nb) + 64);
     if (!adj || !R32 || !misc) return MH_ERR_OOM;
     double2* PB = adj;
     double2* LAM = adj + cnt;

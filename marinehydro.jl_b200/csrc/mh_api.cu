@@ -515,11 +515,33 @@ int mh_lu_solve_lowp(mh_ctx* ctx, int backend, int64_t n, int64_t nbatch, const 
     MH_CUDA_TRY(ctx, cudaMemcpyAsync(v64, B_host, sizeof(double2) * vcnt, cudaMemcpyHostToDevice, ctx->stream));
     MH_CUDA_TRY(ctx, mh::launch_to_f32(ctx, v64, v32, (int64_t)vcnt));
     MH_CUDA_TRY(ctx, mh::launch_lu_solve_persist(ctx, backend, conj_trans != 0, lo, n, (int64_t)nn, (int)nbatch,
-                                                 dinv, v32, (int64_t)nv, (int)nrhs));
+                                                 dinv, v32, (int64_t)nv, (int)nrhs, bad));
     MH_CUDA_TRY(ctx, cudaMemsetAsync(v64, 0, sizeof(double2) * vcnt, ctx->stream));
     MH_CUDA_TRY(ctx, mh::launch_add_f32(ctx, v64, v32, (int64_t)vcnt));
     MH_CUDA_TRY(ctx, cudaMemcpyAsync(X_host, v64, sizeof(double2) * vcnt, cudaMemcpyDeviceToHost, ctx->stream));
-    return sync_status(ctx, "low-precision solve");
+    std::vector<int> h_bad((size_t)nbatch);
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(h_bad.data(), bad, sizeof(int) * (size_t)nbatch, cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+    if ((rc = sync_status(ctx, "low-precision solve"))) return rc;
+    // marks of the factorisation (1: zero or non-finite pivot; 2: a tensor-core
+    // wait ran out) and of the solve (3: a flag wait ran out)
+    for (int64_t b = 0; b < nbatch; ++b) {
+        if (h_bad[(size_t)b] == 1)
+            return set_err(ctx, MH_ERR_SINGULAR, "matrix %lld: zero or non-finite pivot in the low-precision LU",
+                           (long long)b);
+        if (h_bad[(size_t)b] == 2 || h_bad[(size_t)b] == 3)
+            return set_err(ctx, MH_ERR_TIMEOUT, "matrix %lld: a bounded device wait of the %s ran out",
+                           (long long)b, h_bad[(size_t)b] == 2 ? "factorisation" : "triangular solve");
+    }
+    return MH_OK;
+}
+
+int mh_ctx_set_wait_injection(mh_ctx* ctx, int enable)
+{
+    int rc;
+    if ((rc = check_ctx(ctx))) return rc;
+    ctx->inject_wait_timeout = enable != 0;
+    return MH_OK;
 }
 
 int mh_wave_term(mh_ctx* ctx, uint32_t which, int64_t n, const double* r, const double* z,

@@ -496,11 +496,12 @@ __global__ void k_add_f32(double2* __restrict__ x, const float2* __restrict__ d,
 template <int Q>
 __global__ void __launch_bounds__(256)
 k_resid_n(const double2* __restrict__ A, const double2* __restrict__ X, const double2* B, double2* R, int64_t n,
-          int nrhs, double alpha, double beta)
+          int nrhs, double alpha, double beta, const int* done, const int* bad)
 {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int64_t b = blockIdx.y;
     if (i >= n) return;
+    if (done && (done[b] || bad[b])) return;  // refinement: converged or marked matrices
     const double2* M = A + b * n * n;
     const double2* x = X + b * n * nrhs;
     double ar[Q], ai[Q];
@@ -529,12 +530,13 @@ k_resid_n(const double2* __restrict__ A, const double2* __restrict__ X, const do
 template <int Q, int JW>
 __global__ void __launch_bounds__(256, 2)
 k_resid_c(const double2* __restrict__ A, const double2* __restrict__ X, const double2* B, double2* R, int64_t n,
-          int nrhs, double alpha, double beta)
+          int nrhs, double alpha, double beta, const int* done, const int* bad)
 {
     const int lane = threadIdx.x & 31;
     const int64_t j0 = ((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * JW;
     const int64_t b = blockIdx.y;
     if (j0 >= n) return;  // whole warps leave together
+    if (done && (done[b] || bad[b])) return;  // refinement: converged or marked matrices
     const double2* M = A + b * n * n;
     const double2* x = X + b * n * nrhs;
     int64_t jc[JW];  // columns of this warp (the last one repeated past n, not stored)
@@ -582,9 +584,12 @@ k_resid_c(const double2* __restrict__ A, const double2* __restrict__ X, const do
 // max_i |r_iq| / max_i |b_iq|.
 __global__ void __launch_bounds__(256)
 k_rel_residual(const double2* __restrict__ r, const double2* __restrict__ b, int64_t n, int nrhs,
-               double* __restrict__ out)
+               double* __restrict__ out, double tol, int* done, const int* bad, int* sweeps, int sweep)
 {
     __shared__ double sr[256], sb[256];
+    // refinement control (done != null): skip converged or marked matrices,
+    // mark the ones that reach tol and count the sweeps of each
+    if (done && (done[blockIdx.x] || bad[blockIdx.x])) return;
     double worst = 0.0;
     for (int q = 0; q < nrhs; ++q) {
         const int64_t off = ((int64_t)blockIdx.x * nrhs + q) * n;
@@ -607,7 +612,36 @@ k_rel_residual(const double2* __restrict__ r, const double2* __restrict__ b, int
         else if (sr[0] > 0.0 || sr[0] != sr[0]) worst = INFINITY;
         __syncthreads();
     }
-    if (threadIdx.x == 0) out[blockIdx.x] = (worst == worst) ? worst : INFINITY;
+    if (threadIdx.x == 0) {
+        worst = (worst == worst) ? worst : INFINITY;
+        out[blockIdx.x] = worst;
+        if (done) {
+            sweeps[blockIdx.x] = sweep;
+            if (worst <= tol) done[blockIdx.x] = 1;
+        }
+    }
+}
+
+// X += d and R32 = fp32(R) of the refinement, skipping converged or marked
+// matrices (per = entries per matrix).
+__global__ void k_refine_add(double2* __restrict__ x, const float2* __restrict__ d, int64_t per, int64_t count,
+                             const int* __restrict__ done, const int* __restrict__ bad)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const int64_t z = t / per;
+    if (done[z] || bad[z]) return;
+    x[t] = make_double2(x[t].x + (double)d[t].x, x[t].y + (double)d[t].y);
+}
+
+__global__ void k_refine_to_f32(const double2* __restrict__ a, float2* __restrict__ b, int64_t per, int64_t count,
+                                const int* __restrict__ done, const int* __restrict__ bad)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const int64_t z = t / per;
+    if (done[z] || bad[z]) return;
+    b[t] = make_float2((float)a[t].x, (float)a[t].y);
 }
 
 // ---------------------------------------------------------------------------
@@ -745,12 +779,12 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
     auto* X = (double2*)ws_get(ctx, WS_PHI, sizeof(double2) * nv * nb);
     auto* R = (double2*)ws_get(ctx, WS_TMP, sizeof(double2) * nv * nb * 2);
     auto* R32 = (float2*)ws_get(ctx, WS_TMP32, sizeof(float2) * nv * nb);
-    auto* misc = (char*)ws_get(ctx, WS_MISC, (sizeof(double) + sizeof(int)) * nb + 64);
+    auto* misc = (char*)ws_get(ctx, WS_MISC, refine_ctl_bytes(nb) + 64);
     if (!S64 || !D64 || !Dlo || !Dinv || !T32 || !BC || !X || !R || !R32 || !misc) return MH_ERR_OOM;
     double2* RHS = R + nv * nb;  // right-hand side of the D (or K) system
-    auto* d_res = (double*)misc;
-    auto* d_bad = (int*)(misc + sizeof(double) * nb);
-    auto* d_fall = d_bad + nb;  // set when the frequency-batched pass left pairs to the full table
+    const RefineCtl ctl = refine_ctl(misc, nb);
+    int* d_bad = ctl.bad;
+    auto* d_fall = (int*)(misc + refine_ctl_bytes(nb));  // set when the frequency-batched pass left pairs to the full table
     int rc;
     const double* tab = delh_table_for(ctx, bt.mask, &rc);
     if (rc) return rc;
@@ -812,42 +846,15 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
     else MH_CUDA_TRY(ctx, launch_lu_f32(ctx, Dlo, n, nn, nb, Dinv, d_bad));
     phase_end(ctx, PH_LU);
     phase_begin(ctx, PH_REFINE);
-    // refinement: x = 0, r = rhs
-    MH_CUDA_TRY(ctx, cudaMemsetAsync(X, 0, sizeof(double2) * nv * nb, ctx->stream));
-    MH_CUDA_TRY(ctx, cudaMemcpyAsync(R, RHS, sizeof(double2) * nv * nb, cudaMemcpyDeviceToDevice,
-                                     ctx->stream));
-    std::vector<double> h_res(nb);
-    std::vector<int> h_bad(nb);
-    const int64_t cnt = nv * nb;
-    int it = 0;
-    double worst = INFINITY;
-    for (it = 1; it <= max_iter; ++it) {
-        k_to_f32<<<blocks(cnt, 256), 256, 0, ctx->stream>>>(R, R32, cnt);
-        ctx->launches += 1;
-        MH_CUDA_TRY(ctx, launch_lu_solve_persist(ctx, ctx->lu_backend, false, Dlo, n, nn, nb, Dinv, R32, nv,
-                                                 nrhs));
-        k_add_f32<<<blocks(cnt, 256), 256, 0, ctx->stream>>>(X, R32, cnt);
-        ctx->launches += 1;
-        // R = RHS - D X
-        MH_CUDA_TRY(ctx, launch_residual(ctx, false, D64, n, nb, X, RHS, R, nrhs));
-        k_rel_residual<<<nb, 256, 0, ctx->stream>>>(R, RHS, n, nrhs, d_res);
-        ctx->launches += 1;
-        MH_CUDA_TRY(ctx, cudaMemcpyAsync(h_res.data(), d_res, sizeof(double) * nb,
-                                         cudaMemcpyDeviceToHost, ctx->stream));
-        MH_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-        worst = 0.0;
-        for (int z = 0; z < nb; ++z) worst = std::max(worst, std::isfinite(h_res[z]) ? h_res[z] : INFINITY);
-        if (worst <= tol) break;
-    }
+    RefineState h;
+    if ((rc = refine_sweeps(ctx, false, n, nb, nrhs, D64, Dlo, Dinv, RHS, X, R, R32, ctl, tol, max_iter, h)))
+        return rc;
     phase_end(ctx, PH_REFINE);
-    MH_CUDA_TRY(ctx, cudaMemcpyAsync(h_bad.data(), d_bad, sizeof(int) * nb, cudaMemcpyDeviceToHost,
-                                     ctx->stream));
-    MH_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-    info->refine_iterations = std::max(info->refine_iterations, std::min(it, max_iter));
-    // FP64 fallback for bad or unconverged problems
+    info->refine_iterations = std::max(info->refine_iterations, h.most_sweeps());
+    // FP64 fallback for bad (pivot, wait timeout) or unconverged problems
     for (int z = 0; z < nb; ++z) {
-        if (!(h_bad[z] || !(h_res[z] <= tol))) {
-            info->max_rel_residual = std::max(info->max_rel_residual, h_res[z]);
+        if (h.ok(z)) {
+            info->max_rel_residual = std::max(info->max_rel_residual, h.res[z]);
             continue;
         }
         info->n_fallback += 1;
@@ -877,34 +884,98 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
     return MH_OK;
 }
 
-int mixed_refine_solve(mh_ctx* ctx, int64_t n, int nb, int nrhs, const double2* D64, const float2* Dlo,
-                       const float2* Dinv, const double2* RHS, double2* X, double2* R, float2* R32, double* d_res,
-                       bool conj_trans, double tol, int max_iter, FallbackStore& fb, mh_batch_info* info)
+size_t refine_ctl_bytes(int nb) { return (sizeof(double) + 3 * sizeof(int)) * (size_t)nb + 16; }
+
+RefineCtl refine_ctl(void* block, int nb)
+{
+    RefineCtl c;
+    c.res = (double*)block;
+    c.bad = (int*)(c.res + nb);
+    c.done = c.bad + nb;
+    c.sweeps = c.done + nb;
+    return c;
+}
+
+int RefineState::most_sweeps() const
+{
+    int m = 0;
+    for (size_t z = 0; z < sweeps.size(); ++z)
+        if (!bad[z]) m = std::max(m, sweeps[z]);
+    return m;
+}
+
+int refine_sweeps(mh_ctx* ctx, bool conj_trans, int64_t n, int nb, int nrhs, const double2* D64,
+                  const float2* Dlo, const float2* Dinv, const double2* RHS, double2* X, double2* R, float2* R32,
+                  const RefineCtl& c, double tol, int max_iter, RefineState& h)
 {
     const int64_t nn = n * n, nv = n * nrhs, cnt = nv * nb;
-    int rc;
     MH_CUDA_TRY(ctx, cudaMemsetAsync(X, 0, sizeof(double2) * cnt, ctx->stream));
     MH_CUDA_TRY(ctx, cudaMemcpyAsync(R, RHS, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, ctx->stream));
-    std::vector<double> h_res(nb, INFINITY);
-    for (int it = 1; it <= max_iter; ++it) {
-        MH_CUDA_TRY(ctx, launch_to_f32(ctx, R, R32, cnt));
-        MH_CUDA_TRY(ctx, launch_lu_solve_persist(ctx, ctx->lu_backend, conj_trans, Dlo, n, nn, nb, Dinv, R32, nv,
-                                                 nrhs));
-        MH_CUDA_TRY(ctx, launch_add_f32(ctx, X, R32, cnt));
-        MH_CUDA_TRY(ctx, launch_residual(ctx, conj_trans, D64, n, nb, X, RHS, R, nrhs));
-        MH_CUDA_TRY(ctx, launch_rel_residual(ctx, R, RHS, n, nrhs, nb, d_res));
-        MH_CUDA_TRY(ctx, cudaMemcpyAsync(h_res.data(), d_res, sizeof(double) * nb, cudaMemcpyDeviceToHost,
-                                         ctx->stream));
+    MH_CUDA_TRY(ctx, cudaMemsetAsync(c.done, 0, sizeof(int) * 2 * (size_t)nb, ctx->stream));  // done, sweeps
+    const size_t bytes = (sizeof(double) + 3 * sizeof(int)) * (size_t)nb;
+    std::vector<unsigned char> host(bytes);
+    h.res.assign(nb, INFINITY);
+    h.bad.assign(nb, 0);
+    h.done.assign(nb, 0);
+    h.sweeps.assign(nb, 0);
+    const int dir = conj_trans ? 1 : 0;
+    const int ahead = std::max(1, std::min(ctx->refine_ahead[dir], max_iter));
+    int it = 0;
+    while (it < max_iter) {
+        // the sweeps the last call needed, then one at a time; a sweep costs
+        // next to nothing on matrices that converged or are marked
+        for (int s = 0, k = it == 0 ? ahead : 1; s < k && it < max_iter; ++s) {
+            ++it;
+            k_refine_to_f32<<<blocks(cnt, 256), 256, 0, ctx->stream>>>(R, R32, nv, cnt, c.done, c.bad);
+            MH_CUDA_TRY(ctx, launch_lu_solve_persist(ctx, ctx->lu_backend, conj_trans, Dlo, n, nn, nb, Dinv, R32,
+                                                     nv, nrhs, c.bad, c.done));
+            k_refine_add<<<blocks(cnt, 256), 256, 0, ctx->stream>>>(X, R32, nv, cnt, c.done, c.bad);
+            // R = RHS - op(D) X, then the residual ratio and the marks
+            MH_CUDA_TRY(ctx, launch_gemv(ctx, conj_trans, D64, n, nb, X, RHS, R, nrhs, -1.0, 1.0, c.done, c.bad));
+            k_rel_residual<<<nb, 256, 0, ctx->stream>>>(R, RHS, n, nrhs, c.res, tol, c.done, c.bad, c.sweeps, it);
+            ctx->launches += 3;
+            MH_CUDA_TRY(ctx, cudaGetLastError());
+        }
+        MH_CUDA_TRY(ctx, cudaMemcpyAsync(host.data(), c.res, bytes, cudaMemcpyDeviceToHost, ctx->stream));
         MH_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-        double worst = 0.0;
-        for (int z = 0; z < nb; ++z)
-            if (!fb.used[z]) worst = std::max(worst, std::isfinite(h_res[z]) ? h_res[z] : INFINITY);
-        info->refine_iterations = std::max(info->refine_iterations, it);
-        if (worst <= tol) break;
+        const auto* hr = (const double*)host.data();
+        const auto* hi = (const int*)(hr + nb);
+        bool active = false;
+        for (int z = 0; z < nb; ++z) {
+            h.bad[z] = hi[z];
+            h.done[z] = hi[nb + z];
+            h.sweeps[z] = hi[2 * nb + z];
+            h.res[z] = h.sweeps[z] ? hr[z] : INFINITY;
+            active = active || (!h.bad[z] && !h.done[z]);
+        }
+        if (!active) break;
     }
+    int most = 0;
+    for (int z = 0; z < nb; ++z)
+        if (h.ok(z)) most = std::max(most, h.sweeps[z]);
+    if (most > 0) ctx->refine_ahead[dir] = std::min(most, 8);
+    return MH_OK;
+}
+
+int mixed_refine_solve(mh_ctx* ctx, int64_t n, int nb, int nrhs, const double2* D64, const float2* Dlo,
+                       const float2* Dinv, const double2* RHS, double2* X, double2* R, float2* R32, void* ctl_block,
+                       bool conj_trans, double tol, int max_iter, FallbackStore& fb, mh_batch_info* info)
+{
+    const int64_t nn = n * n, nv = n * nrhs;
+    int rc;
+    const RefineCtl c = refine_ctl(ctl_block, nb);
+    // problems whose forward solve fell back to FP64 are not refined
+    std::vector<int> used(nb, 0);
+    for (int z = 0; z < nb; ++z) used[z] = fb.used[z] ? 1 : 0;
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(c.bad, used.data(), sizeof(int) * (size_t)nb, cudaMemcpyHostToDevice,
+                                     ctx->stream));
+    RefineState h;
+    if ((rc = refine_sweeps(ctx, conj_trans, n, nb, nrhs, D64, Dlo, Dinv, RHS, X, R, R32, c, tol, max_iter, h)))
+        return rc;
+    info->refine_iterations = std::max(info->refine_iterations, h.most_sweeps());
     for (int z = 0; z < nb; ++z) {
-        if (!fb.used[z] && h_res[z] <= tol) {
-            info->max_rel_residual = std::max(info->max_rel_residual, h_res[z]);
+        if (!fb.used[z] && h.ok(z)) {
+            info->max_rel_residual = std::max(info->max_rel_residual, h.res[z]);
             continue;
         }
         if (!fb.used[z]) {
@@ -981,27 +1052,28 @@ cudaError_t launch_add_f32(mh_ctx* ctx, double2* x, const float2* d, int64_t cou
 }
 
 cudaError_t launch_gemv(mh_ctx* ctx, bool conj_trans, const double2* A, int64_t n, int nb, const double2* X,
-                        const double2* B, double2* R, int nrhs, double alpha, double beta)
+                        const double2* B, double2* R, int nrhs, double alpha, double beta, const int* done,
+                        const int* bad)
 {
     if (nrhs < 1 || nrhs > kMaxRhs) return cudaErrorInvalidValue;
     if (beta == 0.0) B = nullptr;
     const dim3 gn(blocks(n, 256), (unsigned)nb);
     if (conj_trans) {  // 8 warps per CTA, JW columns per warp
         const dim3 g4(blocks(n, 32), (unsigned)nb);
-        if (nrhs == 1) k_resid_c<1, 4><<<g4, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta);
-        else if (nrhs == 2) k_resid_c<2, 4><<<g4, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta);
-        else if (nrhs == 3) k_resid_c<3, 4><<<g4, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta);
-        else if (nrhs == 4) k_resid_c<4, 4><<<g4, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta);
+        if (nrhs == 1) k_resid_c<1, 4><<<g4, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta, done, bad);
+        else if (nrhs == 2) k_resid_c<2, 4><<<g4, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta, done, bad);
+        else if (nrhs == 3) k_resid_c<3, 4><<<g4, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta, done, bad);
+        else if (nrhs == 4) k_resid_c<4, 4><<<g4, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta, done, bad);
         else if (nrhs <= 8)
             k_resid_c<8, 2><<<dim3(blocks(n, 16), (unsigned)nb), 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha,
-                                                                                      beta);
+                                                                                      beta, done, bad);
         else
             k_resid_c<kMaxRhs, 1><<<dim3(blocks(n, 8), (unsigned)nb), 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs,
-                                                                                           alpha, beta);
+                                                                                           alpha, beta, done, bad);
     } else {
-        if (nrhs <= 4) k_resid_n<4><<<gn, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta);
-        else if (nrhs <= 8) k_resid_n<8><<<gn, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta);
-        else k_resid_n<kMaxRhs><<<gn, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta);
+        if (nrhs <= 4) k_resid_n<4><<<gn, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta, done, bad);
+        else if (nrhs <= 8) k_resid_n<8><<<gn, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta, done, bad);
+        else k_resid_n<kMaxRhs><<<gn, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta, done, bad);
     }
     ctx->launches += 1;
     return cudaGetLastError();
@@ -1016,7 +1088,7 @@ cudaError_t launch_residual(mh_ctx* ctx, bool conj_trans, const double2* A, int6
 cudaError_t launch_rel_residual(mh_ctx* ctx, const double2* r, const double2* b, int64_t n, int nrhs,
                                 int nb, double* out)
 {
-    k_rel_residual<<<nb, 256, 0, ctx->stream>>>(r, b, n, nrhs, out);
+    k_rel_residual<<<nb, 256, 0, ctx->stream>>>(r, b, n, nrhs, out, 0.0, nullptr, nullptr, nullptr, 0);
     ctx->launches += 1;
     return cudaGetLastError();
 }

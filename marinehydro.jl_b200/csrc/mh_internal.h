@@ -66,6 +66,12 @@ struct mh_ctx {
     int64_t launches = 0;
     int delh_method = MH_DELHOMMEAU_TABLE;
     int lu_backend = MH_LU_TCGEN05_F16;
+    // failure injection (tests): the triangular solves' flag waits wait on a
+    // flag that nothing publishes, so they expire
+    bool inject_wait_timeout = false;
+    // refinement sweeps launched before the first host check, per direction
+    // (0: D x = b, 1: D^H x = b): the most any matrix needed in the last call
+    int refine_ahead[2] = {2, 2};
     double* delh_table = nullptr;  // device, kTabWords doubles (built on first use)
     bool profile = false;
     // phase timing: events recorded on whichever stream issues the phase
@@ -142,9 +148,12 @@ cudaError_t launch_lu_solve_blocks32(mh_ctx* ctx, const float2* A, int64_t n, in
 
 // Persistent (one CTA per matrix, one launch) solve with the factors of
 // launch_lu_tc / launch_lu_f32: X <- (LU)^-1 X, or (LU)^-H X when conj_trans.
+// bad (device, per matrix, may be null): a flag wait of the tensor-core
+// backend that runs out writes 3 there.  done (device, per matrix, may be
+// null; needs bad): matrices with done[b] or bad[b] nonzero are skipped.
 cudaError_t launch_lu_solve_persist(mh_ctx* ctx, int backend, bool conj_trans, const float2* A, int64_t n,
                                     int64_t stride, int nbatch, const float2* Dinv, float2* X, int64_t xstride,
-                                    int nrhs);
+                                    int nrhs, int* bad = nullptr, const int* done = nullptr);
 // Conjugate-transposed solve D^H X = X with the factors of launch_lu_tc
 // (backend MH_LU_TCGEN05_F16) or launch_lu_f32 (MH_LU_SIMT_F32).
 cudaError_t launch_lu_solve_ct(mh_ctx* ctx, int backend, const float2* A, int64_t n, int64_t stride,
@@ -177,8 +186,10 @@ cudaError_t launch_to_f32(mh_ctx* ctx, const double2* a, float2* b, int64_t coun
 cudaError_t launch_add_f32(mh_ctx* ctx, double2* x, const float2* d, int64_t count);
 // R = beta B + alpha op(A) X for nb n x n complex matrices (op = identity or
 // ^H), X and B n x nrhs per matrix; B may be R, or null when beta = 0.
+// done, bad (device, per matrix, both or neither): skip matrices with either set.
 cudaError_t launch_gemv(mh_ctx* ctx, bool conj_trans, const double2* A, int64_t n, int nb, const double2* X,
-                        const double2* B, double2* R, int nrhs, double alpha, double beta);
+                        const double2* B, double2* R, int nrhs, double alpha, double beta,
+                        const int* done = nullptr, const int* bad = nullptr);
 // R = B - op(A) X for nb n x n complex matrices (op = identity or ^H).
 cudaError_t launch_residual(mh_ctx* ctx, bool conj_trans, const double2* A, int64_t n, int nb, const double2* X,
                             const double2* B, double2* R, int nrhs);
@@ -196,12 +207,40 @@ int fp64_getrs(mh_ctx* ctx, bool conj_trans, int64_t n, const double2* LU, const
                int nrhs);
 int fp64_lu_solve(mh_ctx* ctx, int64_t n, double2* A, double2* B, int nrhs);
 int fallback_factor(mh_ctx* ctx, FallbackStore* fb, int64_t n, int nb, int z, const double2* D);
-// X = op(D)^-1 RHS for nb problems (op = identity or ^H) with the low-precision
-// factors (Dlo, Dinv) and FP64 refinement against D64 to tol; problems whose
-// forward solve fell back (fb.used) or that do not converge use FP64 factors.
-// R (FP64) and R32 (FP32) are scratch of the size of RHS, d_res nb doubles.
+// Per-matrix control of a refinement run, in device memory (one block of
+// refine_ctl_bytes(nb)): residual ratios, then marks of bad matrices (low-
+// precision LU pivot or wait timeout), of converged ones, and sweep counts.
+struct RefineCtl {
+    double* res;
+    int* bad;
+    int* done;
+    int* sweeps;
+};
+size_t refine_ctl_bytes(int nb);
+RefineCtl refine_ctl(void* block, int nb);
+// Host copy of a RefineCtl after a run.
+struct RefineState {
+    std::vector<double> res;
+    std::vector<int> bad, done, sweeps;
+    bool ok(int z) const { return !bad[z] && done[z]; }
+    int most_sweeps() const;
+};
+// Mixed-precision refinement of op(D) X = RHS (op = identity or ^H) for nb
+// matrices with the low-precision factors (Dlo, Dinv) and FP64 residuals
+// against D64, controlled on the device: each sweep skips the matrices that
+// converged (residual ratio <= tol) or are marked bad, and the host checks
+// only after the number of sweeps the last call needed (then one sweep at a
+// time), at most max_iter sweeps.  c.bad must hold the marks on entry;
+// timeouts of the solve add to them.  R (FP64), R32 (FP32): scratch of the
+// size of RHS.  Leaves the control block's host copy in h.
+int refine_sweeps(mh_ctx* ctx, bool conj_trans, int64_t n, int nb, int nrhs, const double2* D64,
+                  const float2* Dlo, const float2* Dinv, const double2* RHS, double2* X, double2* R, float2* R32,
+                  const RefineCtl& c, double tol, int max_iter, RefineState& h);
+// X = op(D)^-1 RHS for nb problems by refine_sweeps; problems whose forward
+// solve fell back (fb.used), are marked bad or do not converge use FP64
+// factors.  ctl: a device block of refine_ctl_bytes(nb).
 int mixed_refine_solve(mh_ctx* ctx, int64_t n, int nb, int nrhs, const double2* D64, const float2* Dlo,
-                       const float2* Dinv, const double2* RHS, double2* X, double2* R, float2* R32, double* d_res,
+                       const float2* Dinv, const double2* RHS, double2* X, double2* R, float2* R32, void* ctl,
                        bool conj_trans, double tol, int max_iter, FallbackStore& fb, mh_batch_info* info);
 // Frequency-independent Rankine parts SR, DR (n x n real) of the mixed path.
 int rankine_real(const Batch& bt, double* SR, double* DR);

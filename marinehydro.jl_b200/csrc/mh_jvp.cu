@@ -739,7 +739,7 @@ int hydro_batch_jvp(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double*
             auto* dmat = (double2*)ws_get(ctx, WS_PART, sizeof(double2) * nn * nb * 2);
             auto* vec = (double2*)ws_get(ctx, WS_ADJ, sizeof(double2) * cnt * 6);
             auto* R32 = (float2*)ws_get(ctx, WS_TMP32, sizeof(float2) * cnt);
-            auto* misc = (double*)ws_get(ctx, WS_MISC, (sizeof(double) + sizeof(int)) * nb + 64);
+            auto* misc = ws_get(ctx, WS_MISC, refine_ctl_bytes(nb) + 64);
             if (!dmat || !vec || !R32 || !misc) return MH_ERR_OOM;
             auto* S64 = (double2*)ctx->ws[WS_S];
             auto* D64 = (double2*)ctx->ws[WS_D];

@@ -900,13 +900,15 @@ __device__ __forceinline__ unsigned cluster_rank()
 template <int NB, bool kCT>
 __global__ void __cluster_dims__(kSolveCluster, 1, 1) __launch_bounds__(kSolveThreads, 2)
 k_lu_solve_persist(const float2* __restrict__ A, int64_t n, int64_t stride, const float2* __restrict__ Dinv,
-                   int64_t dstride, float2* __restrict__ X, int64_t xstride, int nrhs)
+                   int64_t dstride, float2* __restrict__ X, int64_t xstride, int nrhs, const int* done,
+                   const int* bad)
 {
     extern __shared__ float2 psm[];
     float2* ys[2] = {psm, psm + kMaxRhs * NB};
     float2* xs = psm + 2 * kMaxRhs * NB;
     float2* ts = psm + 3 * kMaxRhs * NB;  // NB x (NB + 1)
     const int64_t b = blockIdx.x / kSolveCluster;
+    if (done && (done[b] || bad[b])) return;  // the whole cluster, before any cluster barrier
     const int rank = (int)cluster_rank();
     const float2* M = A + b * stride;
     const float2* Dv = Dinv + b * dstride;
@@ -980,6 +982,7 @@ constexpr int kFsLanes = 4;              // threads per tile row
 constexpr int kFsPer = 64 / kFsLanes;    // tile entries per thread
 constexpr int kFsPolls = 1 << 15;        // bounded wait for a published block ...
 constexpr unsigned kFsSleepNs = 256;     // ... sleeping between polls (~10 ms in all)
+constexpr int kFsInjectPolls = 64;       // limit of an injected wait on a flag nothing sets
 
 __device__ __forceinline__ int fs_ld_acquire(const int* p)
 {
@@ -1188,7 +1191,8 @@ __device__ __forceinline__ void fs_solve_publish(const float2 (&iv)[kFsPer], int
 template <bool kCT, bool kXS, int NQ>
 __global__ void __cluster_dims__(kFsCluster, 1, 1) __launch_bounds__(kFsThreads, 2)
 k_lu_solve_flags(const float2* __restrict__ A, int64_t n, int64_t stride, const float2* __restrict__ Dinv,
-                 int64_t dstride, float2* X, int64_t xstride, int nrhs, int* flags, int* bad, int stage)
+                 int64_t dstride, float2* X, int64_t xstride, int nrhs, int* flags, int* bad, int stage,
+                 const int* done, const int* unset_flag)
 {
     constexpr int NB = 64;
     __shared__ __align__(16) float2 ys[2][kMaxRhs][NB];  // y of the block being applied and of the next one
@@ -1196,6 +1200,9 @@ k_lu_solve_flags(const float2* __restrict__ A, int64_t n, int64_t stride, const 
     __shared__ int s_fail;
     extern __shared__ __align__(16) float2 xs_smem[];  // kXS: [own block][nrhs][NB]; then, if stage, two staged blocks
     const int64_t b = blockIdx.x / kFsCluster;
+    // a matrix whose refinement converged, or that is marked bad, is left
+    // alone (every CTA of its cluster returns here, before any barrier)
+    if (done && (done[b] || bad[b])) return;
     const int rank = (int)cluster_rank();
     const float2* M = A + b * stride;
     const float2* Dv = Dinv + b * dstride;
@@ -1271,9 +1278,13 @@ k_lu_solve_flags(const float2* __restrict__ A, int64_t n, int64_t stride, const 
             }
             if (k % kFsCluster != rank) {
                 if (tid == 0 && !s_fail) {
+                    // failure injection: wait on a flag that nothing publishes,
+                    // with a short limit, so the wait expires
+                    const int* wf = unset_flag ? unset_flag : tfl + k;
+                    const int limit = unset_flag ? kFsInjectPolls : kFsPolls;
                     int it = 0;
-                    while (fs_ld_acquire(tfl + k) == 0 && ++it < kFsPolls) __nanosleep(kFsSleepNs);
-                    if (it >= kFsPolls) {
+                    while (fs_ld_acquire(wf) == 0 && ++it < limit) __nanosleep(kFsSleepNs);
+                    if (it >= limit) {
                         s_fail = 1;
                         atomicExch(bad + b, 3);
                     }
@@ -1522,18 +1533,22 @@ cudaError_t solve_blocks_ct(mh_ctx* ctx, const float2* A, int64_t n, int64_t str
 
 cudaError_t launch_lu_solve_persist(mh_ctx* ctx, int backend, bool conj_trans, const float2* A, int64_t n,
                                     int64_t stride, int nbatch, const float2* Dinv, float2* X, int64_t xstride,
-                                    int nrhs)
+                                    int nrhs, int* bad, const int* done)
 {
     if (nrhs < 1 || nrhs > kMaxRhs) return cudaErrorInvalidValue;
+    if (done && !bad) return cudaErrorInvalidValue;
     const dim3 g((unsigned)nbatch * kSolveCluster);
     cudaError_t e;
     if (backend == MH_LU_TCGEN05_F16) {
         const int64_t ds = lu_dinv_stride_tc(n);
         const int64_t nblk = (n + TC_NB - 1) / TC_NB;
-        const size_t fbytes = sizeof(int) * (size_t)(2 * nblk * nbatch + nbatch);
+        // flags of every block and triangle, then (when the caller gives no
+        // per-matrix array) the timeout marks, then one flag nothing publishes
+        const size_t fbytes = sizeof(int) * (size_t)(2 * nblk * nbatch + nbatch + 1);
         auto* flags = (int*)ws_get(ctx, WS_FLAGS, fbytes);
         if (!flags) return cudaErrorMemoryAllocation;
-        int* fbad = flags + 2 * nblk * nbatch;
+        int* fbad = bad ? bad : flags + 2 * nblk * nbatch;
+        const int* unset = ctx->inject_wait_timeout ? flags + 2 * nblk * nbatch + nbatch : nullptr;
         if ((e = cudaMemsetAsync(flags, 0, fbytes, ctx->stream)) != cudaSuccess) return e;
         const dim3 gf((unsigned)nbatch * kFsCluster);
         const size_t xsb = sizeof(float2) * (size_t)((nblk + kFsCluster - 1) / kFsCluster) * nrhs * TC_NB;
@@ -1554,7 +1569,7 @@ cudaError_t launch_lu_solve_persist(mh_ctx* ctx, int backend, bool conj_trans, c
             const size_t smem = xs + (stage ? 2 * kFsStageBytes : 0);
             if (smem && (e2 = raise_smem_cap((const void*)kern, smem)) != cudaSuccess) return e2;
             kern<<<gf, kFsThreads, smem, ctx->stream>>>(A, n, stride, Dinv, ds, X, xstride, nrhs, flags, fbad,
-                                                        stage ? 1 : 0);
+                                                        stage ? 1 : 0, done, unset);
             return cudaSuccess;
         };
         // right-hand-side counts 1 to 4 (radiation dofs and headings of one
@@ -1583,10 +1598,10 @@ cudaError_t launch_lu_solve_persist(mh_ctx* ctx, int backend, bool conj_trans, c
         const size_t sm = persist_smem_bytes<32>();
         if (conj_trans)
             k_lu_solve_persist<32, true><<<g, kSolveThreads, sm, ctx->stream>>>(A, n, stride, Dinv, ds, X,
-                                                                                 xstride, nrhs);
+                                                                                 xstride, nrhs, done, bad);
         else
             k_lu_solve_persist<32, false><<<g, kSolveThreads, sm, ctx->stream>>>(A, n, stride, Dinv, ds, X,
-                                                                                  xstride, nrhs);
+                                                                                  xstride, nrhs, done, bad);
     }
     ctx->launches += 1;
     return cudaGetLastError();

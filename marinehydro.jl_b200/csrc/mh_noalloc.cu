@@ -23,7 +23,13 @@
 //    streams, at once) race on the array: serialise them;
 //  - the first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (this also loads the module on that device); make
-//    that first call before any stream capture.
+//    that first call before any stream capture.  The address is kept for the
+//    life of the process: after cudaDeviceReset (or anything else that
+//    destroys the device's primary context) the kept address is stale, so do
+//    not call this entry point on that device again in the same process;
+//  - A, B and X must be device memory of the current device (or managed
+//    memory); a pointer into another GPU's memory is rejected with
+//    MH_ERR_ARG before anything is launched.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -157,14 +163,19 @@ k_na_norm(const double2* __restrict__ R, const double2* __restrict__ B, int64_t 
     if (threadIdx.x == 0) st->ratio = (worst == worst) ? worst : INFINITY;
 }
 
-bool is_device_pointer(const void* p)
+// Memory that kernels launched on `device` may read and write: device memory
+// of that device, or managed memory.  Device memory of another GPU is
+// rejected: without peer access a kernel touching it faults, which would
+// poison the context; the check launches nothing on the pointer.
+bool is_local_device_pointer(const void* p, int device)
 {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    if (a.type == cudaMemoryTypeManaged) return true;
+    return a.type == cudaMemoryTypeDevice && a.device == device;
 }
 
 unsigned nblk(int64_t count) { return (unsigned)((count + 255) / 256); }
@@ -186,13 +197,16 @@ extern "C" int mh_solve_mixed_noalloc(int64_t n, const void* A, const void* B, i
         return set_err(nullptr, MH_ERR_ARG, "mh_solve_mixed_noalloc: need tol > 0, 1 <= max_iter <= 100");
     if (!A || !B || !X || X == B || X == A)
         return set_err(nullptr, MH_ERR_ARG, "mh_solve_mixed_noalloc: A, B, X must be distinct non-NULL");
-    if (!is_device_pointer(A) || !is_device_pointer(B) || !is_device_pointer(X))
-        return set_err(nullptr, MH_ERR_ARG, "mh_solve_mixed_noalloc: A, B and X must be device memory");
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess) {
         cudaGetLastError();
         return set_err(nullptr, MH_ERR_NO_DEVICE, "no current CUDA device");
     }
+    if (!is_local_device_pointer(A, device) || !is_local_device_pointer(B, device) ||
+        !is_local_device_pointer(X, device))
+        return set_err(nullptr, MH_ERR_ARG,
+                       "mh_solve_mixed_noalloc: A, B and X must be device memory of the current device "
+                       "(%d) or managed memory", device);
     void* base = nullptr;
     int rc = scratch_address(device, &base);
     if (rc) return rc;

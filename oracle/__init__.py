@@ -299,26 +299,42 @@ def hydro_coefficients(mesh, omegas, dofs, betas=(), rho=1000.0, g=9.81,
     Fd = np.zeros((nd, nw, nb), dtype=np.complex128)
     Fk = np.zeros((nd, nw, nb), dtype=np.complex128)
     for w_i, w in enumerate(omegas):
-        k = w * w / g
-        S, D = assemble(mesh, k, gf_mask, direct, nthreads)
-        import scipy.linalg as sla
-        lu = sla.lu_factor(D, check_finite=False)
-        for j, dj in enumerate(dofs):
-            bc = radiation_bc(mesh.normals, dj, w)
-            phi = sla.lu_solve(lu, S @ bc) if direct else S @ sla.lu_solve(lu, bc)
-            p = 1j * rho * w * phi
-            for i, di in enumerate(dofs):
-                F = integrate_pressure(mesh.normals, mesh.areas, p, di)
-                A[i, j, w_i] = F.real / w ** 2
-                B[i, j, w_i] = F.imag / w
-        for b_i, beta in enumerate(betas):
-            bc = airy_bc(mesh.centers, mesh.normals, w, beta, g)
-            phi = sla.lu_solve(lu, S @ bc) if direct else S @ sla.lu_solve(lu, bc)
-            p = 1j * rho * phi * w
-            pk = airy_waves_pressure(mesh.centers, w, beta, rho, g)
-            for i, di in enumerate(dofs):
-                Fd[i, w_i, b_i] = integrate_pressure(mesh.normals, mesh.areas, p, di)
-                Fk[i, w_i, b_i] = integrate_pressure(mesh.normals, mesh.areas, pk, di)
+        S, D = assemble(mesh, w * w / g, gf_mask, direct, nthreads)
+        A[:, :, w_i], B[:, :, w_i], Fd[:, w_i, :], Fk[:, w_i, :] = coefficients_from_matrices(
+            mesh, S, D, w, dofs, betas, rho, g, direct)
+    return A, B, Fd, Fk
+
+
+def coefficients_from_matrices(mesh, S, D, omega, dofs, betas=(), rho=1000.0, g=9.81, direct=True):
+    """The per-frequency part of ``hydro_coefficients`` on given S and D (or
+    K): one LU, every radiation and diffraction problem at this frequency.
+    Returns added_mass[i, j], damping[i, j], diffraction[i, b],
+    froude_krylov[i, b] (src/problems_and_results.jl:105-181)."""
+    import scipy.linalg as sla
+
+    w = float(omega)
+    nd, nb = len(dofs), len(betas)
+    A = np.zeros((nd, nd))
+    B = np.zeros((nd, nd))
+    Fd = np.zeros((nd, nb), dtype=np.complex128)
+    Fk = np.zeros((nd, nb), dtype=np.complex128)
+    lu = sla.lu_factor(D, check_finite=False)
+    for j, dj in enumerate(dofs):
+        bc = radiation_bc(mesh.normals, dj, w)
+        phi = sla.lu_solve(lu, S @ bc) if direct else S @ sla.lu_solve(lu, bc)
+        p = 1j * rho * w * phi
+        for i, di in enumerate(dofs):
+            F = integrate_pressure(mesh.normals, mesh.areas, p, di)
+            A[i, j] = F.real / w ** 2
+            B[i, j] = F.imag / w
+    for b_i, beta in enumerate(betas):
+        bc = airy_bc(mesh.centers, mesh.normals, w, beta, g)
+        phi = sla.lu_solve(lu, S @ bc) if direct else S @ sla.lu_solve(lu, bc)
+        p = 1j * rho * phi * w
+        pk = airy_waves_pressure(mesh.centers, w, beta, rho, g)
+        for i, di in enumerate(dofs):
+            Fd[i, b_i] = integrate_pressure(mesh.normals, mesh.areas, p, di)
+            Fk[i, b_i] = integrate_pressure(mesh.normals, mesh.areas, pk, di)
     return A, B, Fd, Fk
 
 

@@ -133,3 +133,56 @@ def test_lowp_solve_matches_its_factors(mh, gpu, backend, conj, n, nrhs):
         ref = np.linalg.solve(M, B[b])
         err = np.max(np.abs(X[b] - ref)) / np.max(np.abs(ref))
         assert err <= 1e-5, (backend, conj, n, nrhs, b, err)
+
+
+def test_solve_wait_timeout_is_reported(mh, gpu):
+    """Failure injection: the flag waits of the tensor-core backend's
+    triangular solve wait on a flag that nothing publishes (64 polls), so they
+    expire; the solve marks the matrices, the call returns MH_ERR_TIMEOUT,
+    the kernel ends and the context stays usable."""
+    rng = np.random.default_rng(21)
+    A = _bem_like(rng, 2, 256)
+    B = rng.normal(size=(2, 256, 2)) + 1j * rng.normal(size=(2, 256, 2))
+    gpu.set_wait_injection(True)
+    try:
+        with pytest.raises(mh.native.DeviceTimeoutError):
+            gpu.lu_solve_lowp(A, B, "tcgen05")
+    finally:
+        gpu.set_wait_injection(False)
+    X = gpu.lu_solve_lowp(A, B, "tcgen05")
+    for b in range(2):
+        ref = np.linalg.solve(A[b], B[b])
+        assert np.max(np.abs(X[b] - ref)) / np.max(np.abs(ref)) <= 1e-2
+
+
+def test_batch_falls_back_when_the_solve_times_out(mh, oracle, gpu):
+    """A timed-out wait in the mixed refinement marks its frequency; the batch
+    solves it with the pivoted FP64 LU instead, so the outputs stay exact."""
+    mesh = mh.mesh_hemisphere(1.0, (0, 0, 0), (12, 16))
+    dofs = [mh.translational_dofs(mesh, "Heave")]
+    gpu.set_lu_backend("tcgen05")
+    gpu.set_wait_injection(True)
+    try:
+        A, B, _, _, info = mh.hydro_batch(mesh, [0.7, 1.9], dofs, precision="mixed", tol=1e-12, ctx=gpu)
+    finally:
+        gpu.set_wait_injection(False)
+    assert info.n_fallback == 2
+    Ao, Bo, _, _ = oracle.hydro_coefficients(mesh, [0.7, 1.9], dofs)
+    assert np.max(np.abs(A - Ao)) / np.max(np.abs(Ao)) < 1e-10
+    assert np.max(np.abs(B - Bo)) / np.max(np.abs(Bo)) < 1e-10
+    A2, _, _, _, info2 = mh.hydro_batch(mesh, [0.7, 1.9], dofs, precision="mixed", tol=1e-12, ctx=gpu)
+    assert info2.n_fallback == 0 and np.max(np.abs(A2 - Ao)) / np.max(np.abs(Ao)) < 1e-9
+
+
+def test_refinement_skips_converged_frequencies(mh, oracle, gpu):
+    """Per-frequency convergence: the frequencies are refined independently,
+    each to tol, and the sweep count reported is the largest any needed."""
+    mesh = mh.mesh_hemisphere(1.0, (0, 0, 0), (12, 16))
+    dofs = [mh.translational_dofs(mesh, "Heave")]
+    om = [0.3, 1.0, 2.0, 3.0]
+    for tol in (1e-6, 1e-12):
+        A, B, _, _, info = mh.hydro_batch(mesh, om, dofs, precision="mixed", tol=tol, ctx=gpu)
+        assert info.n_fallback == 0 and info.max_rel_residual <= tol
+        assert 1 <= info.refine_iterations <= 6
+    Ao, _, _, _ = oracle.hydro_coefficients(mesh, om, dofs)
+    assert np.max(np.abs(A - Ao)) / np.max(np.abs(Ao)) < 1e-9

@@ -173,3 +173,64 @@ def test_gk15_rule_exactness(oracle):
     j = math.exp(z) * (e1 / math.pi + 1j)
     assert abs(G.real - 2 * math.pi * j.real) < 1e-13
     assert abs(G.imag - 2 * math.pi * math.exp(z)) < 1e-13
+
+
+def _pair_coefficients(mh, oracle, radius, dx, omega, resolution=(6, 6)):
+    """A, B (2 x 2) of two heaving hemispheres, body 2 centred at
+    x = radius + dx; column j = radiation of body j (paper/ArraySensitivities.jl:16-50)."""
+    m1 = mh.mesh_hemisphere(radius, (0.0, 0.0, 0.0), resolution)
+    m2 = mh.mesh_hemisphere(radius, (radius + dx, 0.0, 0.0), resolution)
+    mesh = m1 + m2
+    h1 = np.zeros((mesh.nfaces, 3))
+    h1[:m1.nfaces, 2] = 1.0
+    h2 = np.zeros((mesh.nfaces, 3))
+    h2[m1.nfaces:, 2] = 1.0
+    A, B, _, _ = oracle.hydro_coefficients(mesh, [omega], [h1, h2], [], 1000.0, 9.81,
+                                           oracle.GF_RANKINE | oracle.GF_RANKINE_REFLECTED | oracle.GF_WU,
+                                           True, 1)
+    return A[:, :, 0], B[:, :, 0]
+
+
+def _pair_fd(mh, oracle, radius, dx, omega, which, h=1e-6):
+    if which == "dx":
+        p, m = (radius, dx + h), (radius, dx - h)
+    else:
+        p, m = (radius + h, dx), (radius - h, dx)
+    Ap, Bp = _pair_coefficients(mh, oracle, *p, omega)
+    Am, Bm = _pair_coefficients(mh, oracle, *m, omega)
+    return (Ap - Am) / (2 * h), (Bp - Bm) / (2 * h)
+
+
+@pytest.mark.parametrize("table,which", [("pair_sensitivity_dx", "dx"), ("pair_sensitivity_dr", "r")])
+def test_oracle_reproduces_reference_pair_gradients(mh, oracle, table, which):
+    """The reference's own Zygote gradients of two 6 x 6 hemispheres
+    (paper/Plots/11_heuristics_d{x,r}_DELhommeau.csv, written by
+    paper/ArraySensitivities.jl:52-68 through the finite-difference mesh
+    rrules of paper/meshGradients_pair.jl) against central differences
+    (h = 1e-6) of the oracle on this package's hemisphere mesh.  Agreement to
+    1e-6 of each column's scale pins the oracle, the mesh generator (the
+    stand-in for Capytaine's sphere) and the solve at once."""
+    p = PINS[table]
+    dA_ref, dB_ref = np.array(p["dA11"]), np.array(p["dB11"])
+    got = [_pair_fd(mh, oracle, p["radius"], dx, p["omega"], which) for dx in p["dx"]]
+    dA = np.array([g[0][0, 0] for g in got])
+    dB = np.array([g[1][0, 0] for g in got])
+    assert np.max(np.abs(dA - dA_ref)) <= 1e-6 * np.max(np.abs(dA_ref))
+    assert np.max(np.abs(dB - dB_ref)) <= 1e-6 * np.max(np.abs(dB_ref))
+
+
+def test_oracle_reproduces_reference_dimensionless_gradients(mh, oracle):
+    """dA21/dr and dB21/dr on the reference's (dx/r, kr) grid
+    (paper/Plots/added_mass_data_dimensionless.csv and
+    damping_data_dimensionless.csv; omega = sqrt(kr 9.8 / r), k = omega^2 / 9.81
+    as in paper/ArraySensitivities.jl:71-97): every row."""
+    p = PINS["pair_sensitivity_dimensionless"]
+    r = p["radius"]
+    dA, dB = [], []
+    for dxr, kr in zip(p["dx_r_ratio"], p["kr"]):
+        gA, gB = _pair_fd(mh, oracle, r, dxr * r, math.sqrt(kr * 9.8 / r), "r")
+        dA.append(gA[1, 0])
+        dB.append(gB[1, 0])
+    dA_ref, dB_ref = np.array(p["dA21_dr"]), np.array(p["dB21_dr"])
+    assert np.max(np.abs(np.array(dA) - dA_ref)) <= 1e-6 * np.max(np.abs(dA_ref))
+    assert np.max(np.abs(np.array(dB) - dB_ref)) <= 1e-6 * np.max(np.abs(dB_ref))

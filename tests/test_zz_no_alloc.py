@@ -71,3 +71,65 @@ def test_noalloc_rejects_sizes_beyond_its_maximum(mh, gpu):
                                   1, ctypes.c_void_p(dX.data_ptr()), 1e-10, 10, None, None, None)
     assert rc == mh.native.MH_ERR_ARG
     assert b"1024" in L.mh_last_error(None)
+
+
+def test_noalloc_at_its_maximum_allocates_nothing(mh, gpu):
+    """n = 1024 and nrhs = 16 (every scratch region full), against mh_solve;
+    the device's free memory is the same before and after a second call (the
+    first call loads the module and looks up the scratch address)."""
+    torch = pytest.importorskip("torch")
+    mesh = mh.mesh_hemisphere(1.0, (0, 0, 0), (32, 64))
+    assert mesh.nfaces == 1024
+    _, D = mh.assemble_matrices(mh.DEFAULT_GREEN_FUNCTIONS, mesh, 0.9, ctx=gpu)
+    rng = np.random.default_rng(5)
+    B = rng.standard_normal((1024, 16)) + 1j * rng.standard_normal((1024, 16))
+    ref = mh.solve(D, np.eye(1024, dtype=np.complex128), B, ctx=gpu)
+    dA, dB = _device(D, torch), _device(B, torch)
+    dX = torch.empty((16, 1024), dtype=torch.complex128, device="cuda")
+    L = mh.native.lib()
+    stream = torch.cuda.current_stream().cuda_stream
+    iters = ctypes.c_int32(0)
+    res = ctypes.c_double(0.0)
+
+    def call():
+        return L.mh_solve_mixed_noalloc(1024, ctypes.c_void_p(dA.data_ptr()), ctypes.c_void_p(dB.data_ptr()), 16,
+                                        ctypes.c_void_p(dX.data_ptr()), 1e-12, 30, ctypes.c_void_p(stream),
+                                        ctypes.byref(iters), ctypes.byref(res))
+
+    assert call() == 0, L.mh_last_error(None)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    assert call() == 0, L.mh_last_error(None)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    X = dX.cpu().numpy().T
+    assert np.max(np.abs(X - ref)) / np.max(np.abs(ref)) < 1e-9
+    assert res.value <= 1e-12
+
+
+def test_noalloc_reports_no_convergence(mh, gpu):
+    """One sweep cannot reach tol = 1e-30: MH_ERR_NOT_CONVERGED after exactly
+    one sweep, with the residual of that sweep reported."""
+    torch = pytest.importorskip("torch")
+    mesh = mh.mesh_hemisphere(1.0, (0, 0, 0), (12, 16))
+    _, D = mh.assemble_matrices(mh.DEFAULT_GREEN_FUNCTIONS, mesh, 0.9, ctx=gpu)
+    B = np.ones((mesh.nfaces, 1), dtype=np.complex128)
+    rc, _, iters, res = _noalloc(mh, torch, D, B, tol=1e-30, max_iter=1)
+    assert rc == mh.native.MH_ERR_NOT_CONVERGED
+    assert iters == 1
+    assert 0.0 < res < 1e-3
+
+
+def test_noalloc_rejects_host_memory(mh, gpu):
+    """Host buffers are refused before anything is launched on them."""
+    torch = pytest.importorskip("torch")
+    n = 8
+    A = np.eye(n, dtype=np.complex128)
+    B = np.ones((n, 1), dtype=np.complex128)
+    X = np.zeros((n, 1), dtype=np.complex128)
+    L = mh.native.lib()
+    rc = L.mh_solve_mixed_noalloc(n, ctypes.c_void_p(A.ctypes.data), ctypes.c_void_p(B.ctypes.data), 1,
+                                  ctypes.c_void_p(X.ctypes.data), 1e-10, 10, None, None, None)
+    assert rc == mh.native.MH_ERR_ARG
+    assert b"current device" in L.mh_last_error(None)
