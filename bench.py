@@ -1,13 +1,14 @@
 #!/usr/bin/env python
-"""Benchmark: batched BEM solves/s at N=2048 panels on B200.
+"""Benchmark: batched BEM solves/s and adjoint grads/s at N=2048 panels on B200.
 
 Workload (one "step" = one pass of the hot path over one batch): a
-hemisphere of radius 1 m meshed with 32 x 64 panels (2048), 64 frequencies
-omega = linspace(0.3, 3.0), heave and surge radiating/influenced, one
-incident heading (beta = 0), Rankine + reflected Rankine + tabulated
-Guevel-Delhommeau wave term, direct formulation; mixed precision (FP32 LU,
-FP64 refinement to max|r|/max|b| <= 1e-10).  A solve is one (mesh,
-frequency) problem with all its right-hand sides and outputs (A, B, F, FK).
+hemisphere of radius 1 m meshed at resolution 64 x 64 (2048 panels), 64
+frequencies omega = linspace(0.3, 3.0), heave and surge radiating and
+influenced, one incident heading (beta = 0), Rankine + reflected Rankine +
+tabulated Guevel-Delhommeau wave term, direct formulation; mixed precision
+(FP16 tensor-core LU updates with FP32 panels, FP64 refinement to
+max|r|/max|b| <= 1e-8, two sweeps).  A solve is one (mesh, frequency) problem
+with all its right-hand sides and outputs (A, B, F, FK).
 
   value  solves/s with the mesh already resident on the device
   e2e    the same through the C ABI from pinned host buffers: mesh upload,
@@ -16,13 +17,18 @@ frequency) problem with all its right-hand sides and outputs (A, B, F, FK).
          forward, its adjoint solve and the tangent contraction, giving the
          cotangents of every mesh field and of omega for a scalar objective
          J = sum(wA A) + sum(wB B) + Re sum(conj(wF) F) (seeded weights), and
-         from them dJ/dR through the exact mesh tangent; mixed path, with
-         the FP64 GPU path and the gradient agreement beside it
+         from them dJ/dR through the exact mesh tangent
+  grads_two_body
+         the two-body power objective (two 1024-panel hemispheres 5 m apart,
+         Wu, indirect, omega = 1.03) and dJ/d(r1, dx1, omega), end to end
+         through two_body_power(grad=True)
 
-Also reported: the plain FP64 GPU path (cuSOLVER zgetrf) on a frequency
-subsample, the relative error of the mixed outputs against it, per-phase
-times measured with CUDA events on the library's stream, clocks sampled
-during the timed region, and the CPU oracle baseline.
+Also reported: the FP64 GPU path batched the same way (the denominator of
+the mixed path's speed-up) and one frequency at a time; the error of the
+mixed outputs against the FP64 oracle's exact-quadrature fixture at all 64
+frequencies; per-phase times measured with CUDA events on the library's
+stream; the roofline of the LU phase and of the wave pass; clocks sampled
+during the timed region; and the CPU oracle baseline.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 """
@@ -184,22 +190,48 @@ class ClockSampler:
 # CPU baseline (the FP64 CPU oracle; test infrastructure, timed as the baseline)
 # --------------------------------------------------------------------------
 
-def cpu_baseline(mh, mesh, dofs, omegas, betas, columns: int):
+def cpu_threads() -> int:
+    """Host threads this process may use: the affinity mask, capped by the
+    cgroup CPU quota when one is set (a container may see more cores than
+    its quota lets it run)."""
+    n = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    try:
+        quota, period = open("/sys/fs/cgroup/cpu.max").read().split()[:2]
+        if quota != "max":
+            n = max(1, min(n, int(int(quota) // int(period))))
+    except (OSError, ValueError):
+        pass
+    return n
+
+
+def cpu_baseline(mh, mesh, dofs, omegas, betas, columns: int, offset: int = 0):
+    """One (mesh, frequency) solve of the FP64 CPU oracle at the middle
+    frequency: exact-quadrature Delhommeau assembly of the `columns` source
+    columns from `offset` (wrapping), scaled to all n columns, plus LAPACK
+    zgetrf/zgetrs, the right-hand sides and the forces on a full matrix."""
     sys.path.insert(0, str(ROOT))
     import oracle
     import scipy.linalg as sla
 
     oracle.lib()
+    threads = cpu_threads()
     n = mesh.nfaces
     w = float(omegas[len(omegas) // 2])
     k = w * w / 9.81
     mask = oracle.GF_RANKINE | oracle.GF_RANKINE_REFLECTED | oracle.GF_DELHOMMEAU
+    j0 = offset % n
+    spans = [(j0, min(n, j0 + columns))]
+    if j0 + columns > n:
+        spans.append((0, j0 + columns - n))
     t0 = time.perf_counter()
-    S, D = oracle.assemble(mesh, k, mask, True, columns=(0, columns))
+    for a, b in spans:
+        oracle.assemble(mesh, k, mask, True, threads, columns=(a, b))
     t_asm = (time.perf_counter() - t0) * n / columns
-    # LU and solves on a full FP64 matrix of the same size (Wu assembly is cheap)
+    # LU and solves on a full FP64 matrix of the same size: LAPACK does the
+    # same work on any dense complex n x n matrix, and the exact-quadrature
+    # Delhommeau D would need all n columns; the Wu D is cheap to assemble
     S, D = oracle.assemble(mesh, k, oracle.GF_RANKINE | oracle.GF_RANKINE_REFLECTED | oracle.GF_WU,
-                           True)
+                           True, threads)
     t0 = time.perf_counter()
     lu = sla.lu_factor(D, check_finite=False)
     bcs = [oracle.radiation_bc(mesh.normals, d, w) for d in dofs]
@@ -210,11 +242,22 @@ def cpu_baseline(mh, mesh, dofs, omegas, betas, columns: int):
             oracle.integrate_pressure(mesh.normals, mesh.areas, 1j * 1000.0 * w * phi[:, q], d)
     t_lu = time.perf_counter() - t0
     per_solve = t_asm + t_lu
-    return {"value": 1.0 / per_solve, "unit": "solves/s", "cores": oracle.max_threads(),
-            "kind": "port",
-            "sample": (f"1 frequency (omega={w:.3f}): exact-quadrature Delhommeau assembly of "
-                       f"{columns} of {n} columns scaled x{n / columns:g} ({t_asm:.2f} s), plus "
-                       f"LAPACK zgetrf/zgetrs + 3 right-hand sides + forces ({t_lu:.3f} s)")}
+    return {"value": 1.0 / per_solve, "unit": "solves/s", "cores": threads, "kind": "port",
+            "extrapolated": True, "columns": [j0, columns], "assembly_scale": n / columns,
+            "sample": (f"1 frequency (omega={w:.3f}): FP64 exact-quadrature Delhommeau assembly of "
+                       f"source columns {j0}..{(j0 + columns - 1) % n} ({columns} of {n}) scaled "
+                       f"x{n / columns:g} ({t_asm:.2f} s), plus LAPACK zgetrf/zgetrs on the Wu-assembled "
+                       f"D of the same mesh + 3 right-hand sides + forces ({t_lu:.3f} s)")}
+
+
+def reference_config(mesh, omegas, args):
+    c = config_dict(mesh, omegas, args)
+    c.update(green_functions="Rankine+RankineReflected+ExactGuevelDelhommeau (adaptive quadrature per pair)",
+             precision="FP64 (CPU oracle, the C restatement of the reference's path) + LAPACK",
+             lu_backend="LAPACK zgetrf (scipy)", tol=None,
+             solve="one (mesh, omega) problem, 3 right-hand sides; assembly timed on a window of "
+                   "source columns per step and scaled to all columns")
+    return c
 
 
 # --------------------------------------------------------------------------
@@ -230,17 +273,26 @@ def run_reference(args):
     times = []
     base = None
     for step in range(args.warmup + args.steps):
-        base = cpu_baseline(mh, mesh, dofs, omegas, betas, args.cpu_columns)
+        # each step assembles the next window of columns, so the timed steps
+        # cover distinct columns rather than one block repeatedly
+        base = cpu_baseline(mh, mesh, dofs, omegas, betas, args.cpu_columns, step * args.cpu_columns)
         if step >= args.warmup:
             times.append(1.0 / base["value"])
     per = float(np.mean(times))
     v = 1.0 / per
+    n = mesh.nfaces
+    timed_cols = min(n, args.steps * args.cpu_columns)
     line = {"metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": config_dict(mesh, omegas, args), "impl": "reference",
+            "data": "synthetic", "config": reference_config(mesh, omegas, args), "impl": "reference",
+            "extrapolated": True, "sampled_columns": timed_cols,
+            "note": (f"each step times the exact-quadrature assembly of {args.cpu_columns} source columns "
+                     f"(the window advances every step; the {args.steps} timed steps cover {timed_cols} "
+                     f"distinct columns of {n}) and scales it to all {n}; ms_per_step is that "
+                     "extrapolated time of one full solve, not the wall time of a step"),
             "cpu_baseline": {"value": v, "unit": "solves/s", "cores": base["cores"],
-                             "kind": "port", "sample": base["sample"]},
+                             "kind": "port", "sample": base["sample"], "extrapolated": True},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -399,6 +451,7 @@ def run_grads(mh, ctx, mesh, dofs, omegas, betas, gfs, args, stream, barrier, di
     a = times[2] - 2 * b
     per = (a + nw * b) / nw
     out["fp64_gpu"] = {"value": 1e3 / per, "unit": "grads/s", "ms_per_grad_at_n_omega": per,
+                       "mode": "FP64 forward + adjoint one frequency at a time (no batched FP64 adjoint)",
                        "fit_ms": {"per_call": a, "per_omega": b}, "omegas_timed": [2, int(len(sub))]}
     out["speedup_vs_fp64_gpu"] = out["value"] / out["fp64_gpu"]["value"]
     acc = {}
@@ -530,11 +583,16 @@ def run_ours(args):
     if not args.no_grads:
         line["grads"] = run_grads(mh, ctx, mesh, dofs, omegas, betas, gfs, args, stream, barrier, dist,
                                   world, torch)
+    acc = oracle_accuracy(omegas, (A, B, Fd, Fk), args)
+    if acc is not None:
+        line["accuracy"] = acc
     if rank == 0 and not args.no_fp64:
-        line["fp64_gpu"], line["accuracy"] = fp64_baseline(mh, ctx, mesh, dofs, omegas, betas, gfs,
-                                                           (A, B, Fd), args)
-        if line["fp64_gpu"]["table"]["value"] > 0:
-            line["speedup_vs_fp64_gpu"] = value / line["fp64_gpu"]["table"]["value"]
+        line["fp64_gpu"], line["accuracy_vs_fp64_gpu"] = fp64_baseline(mh, ctx, mesh, dofs, omegas, betas, gfs,
+                                                                       (A, B, Fd, Fk), args)
+        line["speedup_vs_fp64_gpu"] = value / line["fp64_gpu"]["batched"]["value"]
+        line["speedup_vs_fp64_gpu_per_frequency"] = value / line["fp64_gpu"]["table"]["value"]
+    if rank == 0 and not args.no_grads and not args.no_two_body:
+        line["grads_two_body"] = run_two_body(mh, ctx, args, torch)
     if rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(mh, mesh, dofs, omegas, betas, args.cpu_columns)
     if rank == 0:
@@ -560,77 +618,171 @@ def _peaks():
 # (n^2 * 64)); traffic grows with the pairs and frequencies a launch
 # processes, so it is scaled by them.
 WAVE_DRAM_BYTES_PER_PAIR_FREQ = 39.4
+# FP64 operations of k_wave_delh_allw counted from its source (an FMA is 2,
+# any other arithmetic operation or library call 1): per pair, the geometry
+# (20) and the alpha contraction of the four polar functions (15 rows x 21
+# Clenshaw steps x 4 functions x (FMA + subtraction) = 3780, plus the 15 x 4
+# closing steps, 180); per pair and frequency, R and u (3), the four degree-14
+# Horner series (14 x 4 FMAs = 112), G, G_r, G_z from them (16) and the
+# scaling into S and D (32).
+WAVE_FLOPS_PER_PAIR = 3980.0
+WAVE_FLOPS_PER_PAIR_FREQ = 163.0
+# Nominal FP64 peak of a B200 (148 SMs x 64 FP64 FMA per clock x 2 x 1.965 GHz);
+# no FP64 figure is measured on this pool.
+FP64_PEAK_TFLOPS = 37.2
+# DRAM bytes of the LU phase per matrix of 2048, from ncu captures of the
+# three LU kernels (the FP32 Schur complement re-read and re-written once per
+# 256-column outer step, the in-block updates, panels and diagonal blocks):
+# 16.7 GB per 64 matrices.
+LU_DRAM_BYTES_PER_MATRIX_2048 = 16.7e9 / 64
 
 
 def roofline(per_phase, n, args):
-    """Dominant kernel of the solve step: the frequency-batched wave pass
-    k_wave_delh_allw (one launch per step, timed alone by its phase events).
-    Algorithmic bytes per launch: the FP64 Rankine parts of S and D read once
-    per pair (16 B), S and D written in FP64 complex and the FP32 LU copy of D
-    per pair and frequency (40 B).  The LU phase is given beside it against
-    the dense tensor peak, (8/3) n^3 real flops per matrix."""
+    """Dominant phase of the solve step: the low-precision LU (k_lu_diag64 +
+    k_lu_trsm_tc + k_lu_update_tc), tensor bound, (8/3) n^3 real flops per
+    matrix, timed by its phase events on the library's streams; against the
+    measured dense bf16 tensor peak (the burst figure, the sustained one
+    beside it).  The wave pass k_wave_delh_allw beside it, against the FP64
+    issue rate with its flops counted from the source, and its HBM bytes."""
     peaks, src = _peaks()
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     tensor = float(peaks.get("bf16_tflops", 1590.0))
-    if "wave" not in per_phase:
+    tensor_sus = float(peaks.get("bf16_tflops_sustained", 1400.0))
+    if "lu" not in per_phase:
         return None
-    ms = per_phase["wave"]
     nn = float(n) * n
-    alg = nn * (16.0 + 40.0 * args.n_omega)
-    achieved = alg / (ms / 1e3) / 1e9
-    traffic = None
-    if WAVE_DRAM_BYTES_PER_PAIR_FREQ is not None:
-        traffic = WAVE_DRAM_BYTES_PER_PAIR_FREQ * nn * args.n_omega
-    out = {"kernel": "k_wave_delh_allw", "bound": "hbm", "achieved": achieved, "peak": hbm,
-           "unit": "GB/s", "frac": achieved / hbm, "peak_source": src, "traffic": traffic,
-           "ms_per_launch": ms, "algorithmic_bytes_per_launch": alg,
-           "note": ("FP64-issue bound (alpha contraction of the polar table per pair, Horner series "
-                    "in R and complex arithmetic per pair and frequency; ncu at 1024 panels x 64 "
-                    "frequencies: FP64 pipe 64% active at 15% warps active, no spills); the HBM "
-                    "fraction shows the writes are not the limit")}
-    if "lu" in per_phase:
-        fl = 8.0 / 3.0 * float(n) ** 3 * args.n_omega
-        ach = fl / (per_phase["lu"] / 1e3) / 1e12
-        out["lu"] = {"kernels": "k_lu_diag64 + k_lu_trsm_tc + k_lu_update_tc", "bound": "tensor",
-                     "achieved": ach, "peak": tensor, "unit": "TFLOP/s", "frac": ach / tensor,
-                     "ms_per_step": per_phase["lu"], "algorithmic_flops_per_step": fl}
+    fl = 8.0 / 3.0 * float(n) ** 3 * args.n_omega
+    ach = fl / (per_phase["lu"] / 1e3) / 1e12
+    out = {"kernel": "LU phase: k_lu_update_tc (tcgen05) + k_lu_diag64 + k_lu_trsm_tc", "bound": "tensor",
+           "achieved": ach, "peak": tensor, "unit": "TFLOP/s", "frac": ach / tensor,
+           "frac_of_sustained_peak": ach / tensor_sus, "peak_source": src,
+           "traffic": (LU_DRAM_BYTES_PER_MATRIX_2048 * args.n_omega * (n / 2048.0) ** 2
+                       if LU_DRAM_BYTES_PER_MATRIX_2048 else None),
+           "ms_per_step": per_phase["lu"], "algorithmic_flops_per_step": fl,
+           "note": ("achieved = (8/3) n^3 real flops x matrices / LU phase time; traffic from ncu "
+                    "(scaled by n^2 from 2048); the algorithmic bytes (each FP32 matrix read and "
+                    "written once) are 8 n^2 x 2 per matrix")}
+    if "wave" in per_phase:
+        ms = per_phase["wave"]
+        alg = nn * (16.0 + 40.0 * args.n_omega)
+        flops = nn * (WAVE_FLOPS_PER_PAIR + WAVE_FLOPS_PER_PAIR_FREQ * args.n_omega)
+        out["wave"] = {"kernel": "k_wave_delh_allw", "bound": "fp64",
+                       "achieved": flops / (ms / 1e3) / 1e12, "peak": FP64_PEAK_TFLOPS,
+                       "unit": "TFLOP/s", "frac": flops / (ms / 1e3) / 1e12 / FP64_PEAK_TFLOPS,
+                       "peak_source": "nominal (148 SMs x 128 FP64 flop/clock x 1.965 GHz)",
+                       "flops_per_launch": flops, "flops_per_pair": WAVE_FLOPS_PER_PAIR,
+                       "flops_per_pair_freq": WAVE_FLOPS_PER_PAIR_FREQ, "ms_per_launch": ms,
+                       "hbm": {"achieved": alg / (ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+                               "frac": alg / (ms / 1e3) / 1e9 / hbm, "algorithmic_bytes_per_launch": alg,
+                               "traffic": WAVE_DRAM_BYTES_PER_PAIR_FREQ * nn * args.n_omega}}
     return out
 
 
 def fp64_baseline(mh, ctx, mesh, dofs, omegas, betas, gfs, mixed, args):
-    """Plain FP64 GPU path on a frequency subsample: FP64 assembly (table and
-    exact quadrature), cuSOLVER zgetrf/zgetrs, one frequency at a time; timed
-    with CUDA events on the library's stream."""
+    """The FP64 GPU path, timed with CUDA events on the library's stream:
+    batched (MH_PRECISION_FP64_BATCHED: Rankine part once, the
+    frequency-batched FP64 wave pass, cuSOLVER zgetrf/zgetrs per frequency)
+    over all frequencies, the denominator of the mixed path's speed-up; and
+    one frequency at a time (FP64 assembly with the table and with exact
+    quadrature) on a subsample."""
     import torch
 
     stream = torch.cuda.ExternalStream(ctx.stream())
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    sub = np.arange(0, len(omegas), max(1, len(omegas) // args.fp64_omegas))[:args.fp64_omegas]
     res = {}
-    out64 = None
+
+    def timed(om, prec):
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        o = mh.hydro_batch(mesh, om, dofs, betas, green_functions=gfs, precision=prec, ctx=ctx)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        return o, ev0.elapsed_time(ev1) / 1e3
+
+    mh.hydro_batch(mesh, omegas[:kAllw_warm], dofs, betas, green_functions=gfs, precision="fp64_batched",
+                   ctx=ctx)
+    o_b, dt = timed(omegas, "fp64_batched")
+    res["batched"] = {"value": len(omegas) / dt, "unit": "solves/s", "omegas": int(len(omegas)),
+                      "ms_per_solve": dt / len(omegas) * 1e3}
+    sub = np.arange(0, len(omegas), max(1, len(omegas) // args.fp64_omegas))[:args.fp64_omegas]
     for method in ("table", "exact"):
         ctx.set_delhommeau_method(method)
         om = omegas[sub] if method == "table" else omegas[sub[:2]]
         mh.hydro_batch(mesh, om[:1], dofs, betas, green_functions=gfs, precision="fp64", ctx=ctx)
-        torch.cuda.synchronize()
-        ev0.record(stream)
-        o = mh.hydro_batch(mesh, om, dofs, betas, green_functions=gfs, precision="fp64", ctx=ctx)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-        dt = ev0.elapsed_time(ev1) / 1e3
+        _, dt = timed(om, "fp64")
         res[method] = {"value": len(om) / dt, "unit": "solves/s", "omegas": int(len(om)),
-                       "ms_per_solve": dt / len(om) * 1e3}
-        if method == "table":
-            out64 = o
+                       "ms_per_solve": dt / len(om) * 1e3, "mode": "one frequency at a time"}
     ctx.set_delhommeau_method("table")
-    A, B, Fd = mixed
+    A, B, Fd, Fk = mixed
     acc = {}
-    for name, a, b in (("A", A[:, :, sub], out64[0]), ("B", B[:, :, sub], out64[1]),
-                       ("F", Fd[:, sub], out64[2])):
+    for name, a, b in (("A", A, o_b[0]), ("B", B, o_b[1]), ("F", Fd, o_b[2]), ("FK", Fk, o_b[3])):
         acc[name] = float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
-    acc["note"] = "max abs difference / max abs value, mixed vs FP64 GPU path, same frequencies"
+    acc["note"] = "max abs difference / max abs value, mixed vs batched FP64 GPU path, all frequencies"
     return res, acc
+
+
+kAllw_warm = 8  # frequencies of the warm-up call (the frequency-batched wave pass needs >= 6)
+
+
+def oracle_accuracy(omegas, mixed, args):
+    """The mixed outputs against the FP64 oracle's fixture of this workload
+    (tests/golden/hemisphere_2048p_delhommeau.npz: exact-quadrature assembly,
+    LAPACK; written by tests/golden/make_fixtures.py), every frequency."""
+    path = ROOT / "tests" / "golden" / "hemisphere_2048p_delhommeau.npz"
+    if not path.exists() or tuple(args.res) != (64, 64):
+        return None
+    fx = np.load(path)
+    if fx["omegas"].shape != omegas.shape or not np.allclose(fx["omegas"], omegas, rtol=0, atol=1e-14):
+        return None
+    A, B, Fd, Fk = mixed
+    out = {}
+    for name, a, key in (("A", A, "added_mass"), ("B", B, "damping"), ("F", Fd, "diffraction"),
+                         ("FK", Fk, "froude_krylov")):
+        ref = fx[key]
+        out[name] = float(np.max(np.abs(a - ref)) / np.max(np.abs(ref)))
+    out["note"] = ("max abs difference / max abs value over all 64 frequencies, mixed path vs the FP64 "
+                   "oracle (exact-quadrature Delhommeau, LAPACK)")
+    return out
+
+
+def run_two_body(mh, ctx, args, torch):
+    """Grads of the two-body power objective (paper/Power.jl:13-83): two
+    1024-panel hemispheres 5 m apart, Wu, indirect, omega = 1.03; one grad =
+    J and dJ/d(r1, dx1, omega) through two_body_power(grad=True) (mesh
+    generation and tangents on the host, forward + adjoint batch on the
+    device), timed end to end; against the oracle's central differences."""
+    kw = dict(resolution=(32, 64), direct=False, tol=args.tol, max_iter=args.max_iter, ctx=ctx)
+
+    def call(prec):
+        return mh.two_body_power(1.0, 4.0, 1.03, precision=prec, grad=True, **kw)
+
+    call("mixed")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        J, g = call("mixed")
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / args.steps
+    call("fp64")
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    J64, g64 = call("fp64")
+    torch.cuda.synchronize()
+    dt64 = time.perf_counter() - t0
+    out = {"value": 1.0 / dt, "unit": "grads/s", "ms_per_grad": dt * 1e3,
+           "workload": "two_hemispheres_2x1024p_wu_indirect_power_grad", "panels": 2048,
+           "timing": "host wall clock around the public call (mesh generation, upload, forward, adjoint)",
+           "J": J, "grad": g, "fp64_gpu": {"value": 1.0 / dt64, "unit": "grads/s", "ms_per_grad": dt64 * 1e3}}
+    path = ROOT / "tests" / "golden" / "two_hemispheres_2048p_wu.npz"
+    if path.exists():
+        fx = np.load(path)
+        out["accuracy_vs_oracle_fd"] = {k: abs(g[k] - float(fx[f"fd_{k}"])) / abs(float(fx[f"fd_{k}"]))
+                                        for k in ("r1", "dx1", "omega")}
+        out["accuracy_vs_oracle_fd"]["J"] = abs(J - float(fx["power"])) / abs(float(fx["power"]))
+        out["accuracy_vs_oracle_fd"]["note"] = ("relative difference to central differences (h = 1e-6) of "
+                                                "the FP64 oracle")
+    return out
 
 
 def main():
@@ -651,6 +803,7 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-grads", action="store_true")
+    ap.add_argument("--no-two-body", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

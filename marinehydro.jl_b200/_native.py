@@ -32,6 +32,7 @@ MH_LU_TCGEN05_F16 = 1
 
 MH_PRECISION_FP64 = 0
 MH_PRECISION_MIXED = 1
+MH_PRECISION_FP64_BATCHED = 2
 
 _NAMES = {MH_ERR_ARG: "MH_ERR_ARG", MH_ERR_CUDA: "MH_ERR_CUDA",
           MH_ERR_NOT_CONVERGED: "MH_ERR_NOT_CONVERGED", MH_ERR_TIMEOUT: "MH_ERR_TIMEOUT",

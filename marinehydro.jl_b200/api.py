@@ -176,6 +176,8 @@ def _precision_code(precision) -> int:
         return N.MH_PRECISION_FP64
     if precision in ("mixed", N.MH_PRECISION_MIXED):
         return N.MH_PRECISION_MIXED
+    if precision in ("fp64_batched", N.MH_PRECISION_FP64_BATCHED):
+        return N.MH_PRECISION_FP64_BATCHED
     raise ValueError(f"unknown precision {precision!r}")
 
 

@@ -884,6 +884,108 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
     return MH_OK;
 }
 
+// FP64 path with the mixed path's batch structure, for one chunk of nb
+// frequencies: the frequency-batched wave pass writes the FP64 S and D (the
+// Rankine part SR, DR computed once per call), then cuSOLVER zgetrf/zgetrs
+// factor and solve each frequency's FP64 D (or K) with partial pivoting, the
+// pivot checks of all frequencies read back once at the end.
+int run_fp64_chunk(const Batch& bt, const double* d_omegas, const double* d_k, int nb, const double* SR,
+                   const double* DR, double2* d_F, double2* d_FK)
+{
+    mh_ctx* ctx = bt.ctx;
+    const int64_t n = bt.n, nn = n * n;
+    const int nrhs = bt.nrhs;
+    const int64_t nv = n * nrhs;
+    auto* S64 = (double2*)ws_get(ctx, WS_S, sizeof(double2) * nn * nb);
+    auto* D64 = (double2*)ws_get(ctx, WS_D, sizeof(double2) * nn * nb);
+    auto* Dlo = (float2*)ws_get(ctx, WS_LO, sizeof(float2) * nn * nb);
+    auto* BC = (double2*)ws_get(ctx, WS_RHS, sizeof(double2) * nv * nb);
+    auto* X = (double2*)ws_get(ctx, WS_PHI, sizeof(double2) * nv * nb);
+    auto* P = (double2*)ws_get(ctx, WS_TMP, sizeof(double2) * nv * nb);
+    auto* piv = (int*)ws_get(ctx, WS_PIV, sizeof(int) * (size_t)(n * nb + 2 * nb + 2));
+    auto* d_fall = (int*)ws_get(ctx, WS_MISC, 64);
+    if (!S64 || !D64 || !Dlo || !BC || !X || !P || !piv || !d_fall) return MH_ERR_OOM;
+    int* infos = piv + n * nb;
+    int rc;
+    const double* tab = delh_table_for(ctx, bt.mask, &rc);
+    if (rc) return rc;
+    const uint32_t wave = bt.mask & (MH_GF_WU | MH_GF_DELHOMMEAU);
+    phase_begin(ctx, PH_WAVE);
+    if (wave == MH_GF_WU) {
+        dim3 grid(blocks(n, kRows), blocks(n, kCols), (unsigned)nb);
+        k_wave_batch<false><<<grid, kRows, 0, ctx->stream>>>(bt.m->geom, n, bt.direct, nullptr, d_k, SR, DR, S64,
+                                                            D64, Dlo, nullptr);
+        ctx->launches += 1;
+    } else if (wave == MH_GF_DELHOMMEAU && tab && nb >= kAllwMinFreqs) {
+        MH_CUDA_TRY(ctx, cudaFuncSetAttribute(k_wave_delh_allw, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)kWaveAllwSmem));
+        MH_CUDA_TRY(ctx, cudaMemcpyToSymbolAsync(c_polar_mono, tab + kTabMonoOff, sizeof(c_polar_mono), 0,
+                                                 cudaMemcpyDeviceToDevice, ctx->stream));
+        for (int z = 0; z < nb; z += kAllwMaxFreqs) {
+            const int m = std::min(kAllwMaxFreqs, nb - z);
+            const int64_t off = (int64_t)z * nn;
+            const dim3 g2(blocks(n, kWT), blocks(n, kCols));
+            MH_CUDA_TRY(ctx, cudaMemsetAsync(d_fall, 0, sizeof(int), ctx->stream));
+            k_wave_delh_allw<<<g2, kWT, kWaveAllwSmem, ctx->stream>>>(bt.m->geom, n, bt.direct, tab, d_k + z, m, SR,
+                                                                      DR, S64 + off, D64 + off, Dlo + off, nullptr,
+                                                                      d_fall);
+            k_wave_delh_allw_rest<<<g2, kWT, 0, ctx->stream>>>(d_fall, bt.m->geom, n, bt.direct, tab, d_k + z, m,
+                                                              SR, DR, S64 + off, D64 + off, Dlo + off, nullptr);
+            ctx->launches += 2;
+        }
+    } else if (wave == MH_GF_DELHOMMEAU) {
+        dim3 grid(blocks(n, kRows), blocks(n, kCols), (unsigned)nb);
+        k_wave_batch<true><<<grid, kRows, 0, ctx->stream>>>(bt.m->geom, n, bt.direct, tab, d_k, SR, DR, S64, D64,
+                                                           Dlo, nullptr);
+        ctx->launches += 1;
+    } else if (wave == 0) {
+        k_no_wave_batch<<<dim3(blocks(nn, 256), nb), 256, 0, ctx->stream>>>(nn, SR, DR, S64, D64, Dlo);
+        ctx->launches += 1;
+    } else {
+        return set_err(ctx, MH_ERR_ARG, "the batched FP64 path takes one wave term (GFWu or Delhommeau)");
+    }
+    phase_end(ctx, PH_WAVE);
+    MH_CUDA_TRY(ctx, cudaGetLastError());
+    phase_begin(ctx, PH_RHS);
+    MH_CUDA_TRY(ctx, launch_bc_batch(bt, d_omegas, nb, BC));
+    if (bt.direct) MH_CUDA_TRY(ctx, launch_gemv(ctx, false, S64, n, nb, BC, nullptr, X, nrhs, 1.0, 0.0));
+    else MH_CUDA_TRY(ctx, cudaMemcpyAsync(X, BC, sizeof(double2) * nv * nb, cudaMemcpyDeviceToDevice, ctx->stream));
+    phase_end(ctx, PH_RHS);
+    phase_begin(ctx, PH_FP64_LU);
+    int lwork = 0;
+    cusolverStatus_t st = cusolverDnZgetrf_bufferSize(ctx->cusolver, (int)n, (int)n, (cuDoubleComplex*)D64,
+                                                      (int)n, &lwork);
+    if (st != CUSOLVER_STATUS_SUCCESS)
+        return set_err(ctx, MH_ERR_CUDA, "cusolverDnZgetrf_bufferSize failed (%d)", (int)st);
+    auto* work = (cuDoubleComplex*)ws_get(ctx, WS_LWORK, sizeof(cuDoubleComplex) * (size_t)lwork);
+    if (!work) return MH_ERR_OOM;
+    for (int z = 0; z < nb; ++z) {
+        auto* Dz = (cuDoubleComplex*)(D64 + (int64_t)z * nn);
+        st = cusolverDnZgetrf(ctx->cusolver, (int)n, (int)n, Dz, (int)n, work, piv + z * n, infos + z);
+        if (st != CUSOLVER_STATUS_SUCCESS)
+            return set_err(ctx, MH_ERR_CUDA, "cusolverDnZgetrf failed (%d)", (int)st);
+        st = cusolverDnZgetrs(ctx->cusolver, CUBLAS_OP_N, (int)n, nrhs, Dz, (int)n, piv + z * n,
+                              (cuDoubleComplex*)(X + (int64_t)z * nv), (int)n, infos + nb + z);
+        if (st != CUSOLVER_STATUS_SUCCESS)
+            return set_err(ctx, MH_ERR_CUDA, "cusolverDnZgetrs failed (%d)", (int)st);
+    }
+    phase_end(ctx, PH_FP64_LU);
+    double2* PHI = X;
+    if (!bt.direct) {
+        MH_CUDA_TRY(ctx, launch_gemv(ctx, false, S64, n, nb, X, nullptr, P, nrhs, 1.0, 0.0));
+        PHI = P;
+    }
+    phase_begin(ctx, PH_FORCES);
+    MH_CUDA_TRY(ctx, launch_forces_batch(bt, d_omegas, nb, PHI, d_F, d_FK));
+    phase_end(ctx, PH_FORCES);
+    std::vector<int> h(nb);
+    MH_CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), infos, sizeof(int) * (size_t)nb, cudaMemcpyDeviceToHost, ctx->stream));
+    MH_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int z = 0; z < nb; ++z)
+        if (h[z] > 0) return set_err(ctx, MH_ERR_SINGULAR, "frequency %d: zero pivot at column %d", z, h[z]);
+    return MH_OK;
+}
+
 size_t refine_ctl_bytes(int nb) { return (sizeof(double) + 3 * sizeof(int)) * (size_t)nb + 16; }
 
 RefineCtl refine_ctl(void* block, int nb)
@@ -1172,8 +1274,12 @@ int hydro_batch(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double* ome
         const int chunk = (int)std::max<int64_t>(1, std::min<int64_t>(nomega, kBatchBytes / per));
         for (int64_t z0 = 0; z0 < nomega && rc == MH_OK; z0 += chunk) {
             const int nb = (int)std::min<int64_t>(chunk, nomega - z0);
-            rc = run_mixed_chunk(bt, d_omegas + z0, d_k + z0, nb, SR, DR, tol, max_iter,
-                                 d_F + z0 * nrhs * ndof, d_FK + z0 * nbeta * ndof, &local, nullptr);
+            if (precision == MH_PRECISION_FP64_BATCHED)
+                rc = run_fp64_chunk(bt, d_omegas + z0, d_k + z0, nb, SR, DR, d_F + z0 * nrhs * ndof,
+                                    d_FK + z0 * nbeta * ndof);
+            else
+                rc = run_mixed_chunk(bt, d_omegas + z0, d_k + z0, nb, SR, DR, tol, max_iter,
+                                     d_F + z0 * nrhs * ndof, d_FK + z0 * nbeta * ndof, &local, nullptr);
         }
     }
     if (rc) return rc;

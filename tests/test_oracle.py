@@ -234,3 +234,28 @@ def test_oracle_reproduces_reference_dimensionless_gradients(mh, oracle):
     dA_ref, dB_ref = np.array(p["dA21_dr"]), np.array(p["dB21_dr"])
     assert np.max(np.abs(np.array(dA) - dA_ref)) <= 1e-6 * np.max(np.abs(dA_ref))
     assert np.max(np.abs(np.array(dB) - dB_ref)) <= 1e-6 * np.max(np.abs(dB_ref))
+
+
+@pytest.mark.parametrize("name", ["grad_fd_wu_direct", "grad_fd_delh_indirect"])
+def test_gradient_fixture_reproduces(mh, oracle, name):
+    """The committed gradient anchors are the oracle's own numbers: the
+    objective value at the base point is recomputed here."""
+    fx = np.load(pathlib.Path(__file__).parent / "golden" / f"{name}.npz")
+    mesh = mh.mesh_hemisphere(1.0, (0.0, 0.0, 0.0), tuple(int(x) for x in fx["resolution"]))
+    dofs = [np.tile([0.0, 0.0, 1.0], (mesh.nfaces, 1)), np.tile([1.0, 0.0, 0.0], (mesh.nfaces, 1))]
+    A, B, Fd, Fk = oracle.hydro_coefficients(mesh, fx["omegas"], dofs, [0.0], 1000.0, 9.81, int(fx["gf_mask"]),
+                                             bool(fx["direct"]))
+    J = (np.sum(fx["wA"] * A) + np.sum(fx["wB"] * B) + np.real(np.sum(np.conj(fx["wF"]) * Fd))
+         + np.real(np.sum(np.conj(fx["wK"]) * Fk)))
+    assert abs(J - float(fx["J"])) <= 1e-12 * abs(float(fx["J"]))
+
+
+def test_size_fixture_reproduces(mh, oracle):
+    """The 1024-panel exact-Delhommeau fixture: A, B and two sampled S, D
+    entries recomputed from the oracle."""
+    fx = np.load(pathlib.Path(__file__).parent / "golden" / "hemisphere_1024p_delhommeau.npz")
+    mesh = mh.mesh_hemisphere(1.0, (0.0, 0.0, 0.0), (32, 64))
+    heave = np.tile([0.0, 0.0, 1.0], (mesh.nfaces, 1))
+    A, B, _, _ = oracle.hydro_coefficients(mesh, fx["omegas"], [heave], [], 1000.0, 9.81, int(fx["gf_mask"]), True)
+    assert abs(A[0, 0, 0] - fx["added_mass"][0, 0, 0]) <= 1e-12 * abs(fx["added_mass"][0, 0, 0])
+    assert abs(B[0, 0, 0] - fx["damping"][0, 0, 0]) <= 1e-12 * abs(fx["damping"][0, 0, 0])
