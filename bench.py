@@ -752,7 +752,7 @@ def run_two_body(mh, ctx, args, torch):
     J and dJ/d(r1, dx1, omega) through two_body_power(grad=True) (mesh
     generation and tangents on the host, forward + adjoint batch on the
     device), timed end to end; against the oracle's central differences."""
-    kw = dict(resolution=(32, 64), direct=False, tol=args.tol, max_iter=args.max_iter, ctx=ctx)
+    kw = dict(resolution=(32, 64), direct=False, tol=args.tol, ctx=ctx)
 
     def call(prec):
         return mh.two_body_power(1.0, 4.0, 1.03, precision=prec, grad=True, **kw)
