@@ -536,6 +536,97 @@ int mh_lu_solve_lowp(mh_ctx* ctx, int backend, int64_t n, int64_t nbatch, const 
     return MH_OK;
 }
 
+int mh_ctx_set_lu_schedule(mh_ctx* ctx, int64_t n, int groups, int outer_panels)
+{
+    int rc;
+    if ((rc = check_ctx(ctx))) return rc;
+    if (n < 0 || groups < 1 || groups > kLuGroups || outer_panels < 2 || outer_panels > 8 || (outer_panels & 1))
+        return set_err(ctx, MH_ERR_ARG, "LU schedule: need n >= 0, 1 <= groups <= %d, outer_panels in {2, 4, 6, 8}",
+                       kLuGroups);
+    LuSchedule s;
+    s.groups = groups;
+    s.outer = outer_panels;
+    if (n == 0) {
+        ctx->lu_default = s;
+        return MH_OK;
+    }
+    for (auto& e : ctx->lu_table)
+        if (e.first == n) {
+            e.second = s;
+            return MH_OK;
+        }
+    ctx->lu_table.emplace_back(n, s);
+    return MH_OK;
+}
+
+int mh_ctx_get_lu_schedule(mh_ctx* ctx, int64_t n, int* groups, int* outer_panels)
+{
+    int rc;
+    if ((rc = check_ctx(ctx))) return rc;
+    if (n < 0 || !groups || !outer_panels) return set_err(ctx, MH_ERR_ARG, "bad arguments to mh_ctx_get_lu_schedule");
+    const LuSchedule s = n == 0 ? ctx->lu_default : ctx->lu_schedule(n);
+    *groups = s.groups;
+    *outer_panels = s.outer;
+    return MH_OK;
+}
+
+int mh_lu_autotune(mh_ctx* ctx, int64_t n, int64_t nbatch, int ncand, const int* groups, const int* outer_panels,
+                   double* ms, int* best)
+{
+    int rc;
+    if ((rc = check_ctx(ctx))) return rc;
+    if (n < 1 || nbatch < 1 || ncand < 1 || !groups || !outer_panels || !ms)
+        return set_err(ctx, MH_ERR_ARG, "bad arguments to mh_lu_autotune");
+    for (int c = 0; c < ncand; ++c)
+        if (groups[c] < 1 || groups[c] > kLuGroups || outer_panels[c] < 2 || outer_panels[c] > 8 ||
+            (outer_panels[c] & 1))
+            return set_err(ctx, MH_ERR_ARG, "candidate %d: need 1 <= groups <= %d, outer_panels in {2, 4, 6, 8}", c,
+                           kLuGroups);
+    const size_t nn = (size_t)n * (size_t)n;
+    auto* lo = (float2*)ws_get(ctx, WS_LO, sizeof(float2) * nn * (size_t)nbatch);
+    auto* dinv = (float2*)ws_get(ctx, WS_DINV, sizeof(float2) * (size_t)mh::lu_dinv_stride_tc(n) * (size_t)nbatch);
+    auto* panels = (unsigned char*)ws_get(ctx, WS_PANEL, (size_t)mh::lu_panel_bytes_tc(n) * (size_t)nbatch);
+    auto* bad = (int*)ws_get(ctx, WS_MISC, sizeof(int) * (size_t)nbatch);
+    if (!lo || !dinv || !panels || !bad) return MH_ERR_OOM;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    MH_CUDA_TRY(ctx, cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return set_err(ctx, MH_ERR_CUDA, "event creation failed");
+    }
+    const auto table = ctx->lu_table;
+    const LuSchedule dflt = ctx->lu_default;
+    ctx->lu_table.clear();
+    cudaError_t e = cudaSuccess;
+    int fastest = 0;
+    for (int c = 0; c < ncand && e == cudaSuccess; ++c) {
+        ctx->lu_default.groups = groups[c];
+        ctx->lu_default.outer = outer_panels[c];
+        ms[c] = INFINITY;
+        // one warm-up factorisation, then one timed; fresh matrices each time
+        for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep) {
+            if ((e = mh::launch_fill_lu_test(ctx, lo, n, (int)nbatch)) != cudaSuccess) break;
+            if ((e = cudaMemsetAsync(bad, 0, sizeof(int) * (size_t)nbatch, ctx->stream)) != cudaSuccess) break;
+            if ((e = cudaEventRecord(e0, ctx->stream)) != cudaSuccess) break;
+            if ((e = mh::launch_lu_tc(ctx, lo, n, (int64_t)nn, (int)nbatch, dinv, panels, bad)) != cudaSuccess) break;
+            if ((e = cudaEventRecord(e1, ctx->stream)) != cudaSuccess) break;
+            if ((e = cudaEventSynchronize(e1)) != cudaSuccess) break;
+            float t = 0.f;
+            if ((e = cudaEventElapsedTime(&t, e0, e1)) != cudaSuccess) break;
+            ms[c] = t;
+        }
+        if (e == cudaSuccess && ms[c] < ms[fastest]) fastest = c;
+    }
+    ctx->lu_table = table;
+    ctx->lu_default = dflt;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return set_err(ctx, MH_ERR_CUDA, "LU autotune: %s", cudaGetErrorString(e));
+    if ((rc = mh_ctx_set_lu_schedule(ctx, n, groups[fastest], outer_panels[fastest]))) return rc;
+    if (best) *best = fastest;
+    return MH_OK;
+}
+
 int mh_ctx_set_wait_injection(mh_ctx* ctx, int enable)
 {
     int rc;

@@ -5,7 +5,9 @@
 #include <cusolverDn.h>
 #include <stdint.h>
 
+#include <cmath>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "marinehydro_b200.h"
@@ -46,8 +48,15 @@ enum Phase : int {
 
 // Groups of matrices whose blocked LUs run concurrently on their own
 // streams, so one group's latency-bound panel work (diagonal blocks, panel
-// solves) overlaps another's trailing updates.
-constexpr int kLuGroups = 2;
+// solves) overlaps another's trailing updates: at most this many.
+constexpr int kLuGroups = 4;
+
+// Schedule of the tensor-core LU: groups of matrices on their own stream
+// pairs (1 .. kLuGroups) and 64-column panels per outer step (even, 2 .. 8).
+struct LuSchedule {
+    int groups = 2;
+    int outer = 4;
+};
 
 struct mh_ctx {
     int device = 0;
@@ -69,6 +78,23 @@ struct mh_ctx {
     // failure injection (tests): the triangular solves' flag waits wait on a
     // flag that nothing publishes, so they expire
     bool inject_wait_timeout = false;
+    // LU schedules by matrix size (set by hand or by the autotuner); sizes
+    // with no entry use the nearest entry in log n, else lu_default
+    std::vector<std::pair<int64_t, LuSchedule>> lu_table;
+    LuSchedule lu_default;
+    LuSchedule lu_schedule(int64_t n) const
+    {
+        const LuSchedule* best = &lu_default;
+        double gap = 1e300;
+        for (const auto& e : lu_table) {
+            const double d = std::fabs(std::log((double)e.first / (double)n));
+            if (d < gap) {
+                gap = d;
+                best = &e.second;
+            }
+        }
+        return *best;
+    }
     // refinement sweeps launched before the first host check, per direction
     // (0: D x = b, 1: D^H x = b): the most any matrix needed in the last call
     int refine_ahead[2] = {2, 2};
@@ -136,6 +162,8 @@ cudaError_t launch_lu_solve_f32(mh_ctx* ctx, const float2* A, int64_t n, int64_t
 int64_t lu_dinv_stride_tc(int64_t n);
 // Bytes of packed FP16 operand panels per matrix (scratch of launch_lu_tc).
 int64_t lu_panel_bytes_tc(int64_t n);
+// Diagonally dominant FP32 complex test matrices (the LU autotuner's input).
+cudaError_t launch_fill_lu_test(mh_ctx* ctx, float2* A, int64_t n, int nbatch);
 cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int nbatch, float2* Dinv,
                          unsigned char* panels, int* bad);
 // Block-parallel (LU)^-1 X in place; T: scratch of the same size as X.

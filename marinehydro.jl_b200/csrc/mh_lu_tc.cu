@@ -319,7 +319,7 @@ k_lu_trsm_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
 }
 
 // Packed panel pairs of one update (one per 64-column panel).
-constexpr int kMaxPairs = 4;
+constexpr int kMaxPairs = 8;
 struct PanelPairs {
     const unsigned char* L[kMaxPairs];
     const unsigned char* U[kMaxPairs];
@@ -1332,59 +1332,89 @@ k_lu_solve_flags(const float2* __restrict__ A, int64_t n, int64_t stride, const 
 
 int64_t lu_dinv_stride_tc(int64_t n) { return ((n + TC_NB - 1) / TC_NB) * 2 * TC_NB * TC_NB; }
 
-// Eight panel buffers per matrix: the four panel pairs of an outer step stay
-// live while its interior update runs, and the next outer step writes the
-// other four.
-constexpr int kOuterPanels = 4;  // 64-column panels per outer step (256 columns)
+namespace {
+// Test matrices of the LU autotuner: 1/2 on the diagonal plus off-diagonal
+// entries of modulus <= 0.3 / n from a hash of (matrix, row, column), so
+// every matrix is strictly diagonally dominant (no pivoting needed).
+__global__ void k_fill_lu_test(float2* __restrict__ A, int64_t n, int64_t count)
+{
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const int64_t e = t % (n * n);
+    const int64_t i = e % n, j = e / n;
+    uint64_t h = (uint64_t)t * 0x9E3779B97F4A7C15ull + 0x632BE59BD9B4E019ull;
+    h ^= h >> 31;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 29;
+    const float u = (float)(h & 0xFFFFFF) / 16777216.f - 0.5f;
+    const float v = (float)((h >> 24) & 0xFFFFFF) / 16777216.f - 0.5f;
+    const float s = 0.4f / (float)n;
+    A[t] = i == j ? make_float2(0.5f, 0.f) : make_float2(s * u, s * v);
+}
+}  // namespace
+
+cudaError_t launch_fill_lu_test(mh_ctx* ctx, float2* A, int64_t n, int nbatch)
+{
+    const int64_t count = n * n * nbatch;
+    k_fill_lu_test<<<(unsigned)((count + 255) / 256), 256, 0, ctx->stream>>>(A, n, count);
+    ctx->launches += 1;
+    return cudaGetLastError();
+}
+
+// Panel buffers per matrix: the panel pairs of an outer step stay live while
+// its interior update runs, and the next outer step writes the other set
+// (2 x the outer step's panels, sized for the widest schedule).
+constexpr int kOuterMax = kMaxPairs;  // 64-column panels per outer step, at most (512 columns)
 // After them, the packed TRSM B operands of every diagonal block (two images each).
 int64_t lu_panel_bytes_tc(int64_t n)
 {
-    return 2 * kOuterPanels * ((n + TC_TM - 1) / TC_TM) * (int64_t)(kPanelL + kPanelU) +
+    return 2 * kOuterMax * ((n + TC_TM - 1) / TC_TM) * (int64_t)(kPanelL + kPanelU) +
            ((n + TC_NB - 1) / TC_NB) * 2 * (int64_t)kTrsmBImage;
 }
 
-// Blocked LU in outer steps of 256 columns (four 64-column panels), with
-// look-ahead.  Outer step K0 (tile T0 = K0 / 128), on the main
+// Blocked LU in outer steps of op 64-column panels (op even: 2 to 8, i.e.
+// 128 to 512 columns; op = 4 by default), with look-ahead.  Outer step K0
+// (tile T0 = K0 / 128), on the main
 // (high-priority) stream: for each panel k = K0 + 64 s, its TRSM, then (but
 // for the last) the update of the rest of the outer block's tile rows and
-// columns (an L of width T0 + 2 - tile(k + 64) tiles, rows and columns
+// columns (an L of width T0 + op/2 - tile(k + 64) tiles, rows and columns
 // >= k + 64) with that panel alone, and the next diagonal block; then the
-// trailing tiles (>= T0 + 2) are updated once with all four panel pairs
-// accumulated in TMEM (K = 256 complex): their first two tile rows and
+// trailing tiles (>= T0 + op/2) are updated once with all op panel pairs
+// accumulated in TMEM (K = 64 op complex): their first op/2 tile rows and
 // columns on the main stream, the interior concurrently on the side
 // (low-priority) stream, then the next diagonal block.  The trailing matrix
-// is read and written once per 256 columns.  An outer step's trailing
+// is read and written once per outer step.  An outer step's trailing
 // update waits for the previous interior; everything before it only touches
-// tile rows and columns T0, T0 + 1, which that interior does not.
+// tile rows and columns T0 .. T0 + op/2 - 1, which that interior does not.
 namespace {
 // The schedule above for nbatch matrices on one (main, side) stream pair;
 // panels: lu_panel_bytes_tc(n) * nbatch bytes for these matrices.
 cudaError_t lu_tc_group(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int nbatch, float2* Dinv,
                         unsigned char* panels, int* bad, cudaStream_t main_s, cudaStream_t side_s,
-                        cudaEvent_t ev_side, cudaEvent_t ev_panel)
+                        cudaEvent_t ev_side, cudaEvent_t ev_panel, const int op)
 {
     cudaError_t e;
     const int64_t dstride = lu_dinv_stride_tc(n);
     const int64_t pstride = (int64_t)((n + TC_TM - 1) / TC_TM) * (kPanelL + kPanelU);  // one buffer, per matrix
     const int64_t bstride = ((n + TC_NB - 1) / TC_NB) * 2 * (int64_t)kTrsmBImage;       // B images, per matrix
-    unsigned char* bimg = panels + 2 * kOuterPanels * pstride * nbatch;
+    unsigned char* bimg = panels + 2 * kOuterMax * pstride * nbatch;
     const int ntiles = (int)((n + TC_TM - 1) / TC_TM);
     const unsigned nbz = (unsigned)nbatch;
-    constexpr int kW = kOuterPanels / 2;  // tiles per outer step
+    const int kW = op / 2;  // tiles per outer step
     if ((e = cudaEventRecord(ev_side, side_s)) != cudaSuccess) return e;
     k_lu_diag64<<<nbatch, kDiag64Threads, kDiag64Smem, main_s>>>(A, n, stride, 0, Dinv, dstride, bad, bimg,
                                                                    bstride);
     ctx->launches += 1;
     int outer = 0;
-    for (int64_t K0 = 0; K0 < n; K0 += kOuterPanels * TC_NB, ++outer) {
+    for (int64_t K0 = 0; K0 < n; K0 += op * TC_NB, ++outer) {
         const int T0 = (int)(K0 / TC_TM);
         PanelPairs pp;
-        for (int s = 0; s < kOuterPanels; ++s) {
-            pp.L[s] = panels + (int64_t)(kOuterPanels * (outer & 1) + s) * pstride * nbatch;
+        for (int s = 0; s < op; ++s) {
+            pp.L[s] = panels + (int64_t)(op * (outer & 1) + s) * pstride * nbatch;
             pp.U[s] = pp.L[s] + (int64_t)ntiles * kPanelL;
         }
         bool done = false;
-        for (int s = 0; s < kOuterPanels; ++s) {
+        for (int s = 0; s < op; ++s) {
             const int64_t k = K0 + (int64_t)s * TC_NB;
             if (n - k - TC_NB <= 0) {
                 done = true;
@@ -1394,7 +1424,7 @@ cudaError_t lu_tc_group(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int n
             k_lu_trsm_tc<<<dim3(2 * nt, nbz), 128, kSmemA + kSmemA, main_s>>>(
                 A, n, stride, k, bimg, bstride, (unsigned char*)pp.L[s], (unsigned char*)pp.U[s], pstride, nt, bad);
             ctx->launches += 1;
-            if (s + 1 < kOuterPanels) {  // the rest of the outer block with this panel, then its next diagonal block
+            if (s + 1 < op) {  // the rest of the outer block with this panel, then its next diagonal block
                 PanelPairs one;
                 one.L[0] = pp.L[s];
                 one.U[0] = pp.U[s];
@@ -1408,7 +1438,7 @@ cudaError_t lu_tc_group(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int n
         }
         if (done) break;
         // trailing tiles >= T0 + kW with all four panel pairs
-        const int64_t lo = K0 + (int64_t)kOuterPanels * TC_NB;
+        const int64_t lo = K0 + (int64_t)op * TC_NB;
         const int t0 = T0 + kW, nt = ntiles - t0;
         if (nt <= 0) break;
         // the previous interior update is done before this trailing update
@@ -1418,12 +1448,12 @@ cudaError_t lu_tc_group(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int n
         const int w = std::min(kW, nt);
         if (nt > w) {
             k_lu_update_tc<<<dim3(nt - w, nt - w, nbz), 128, kTcSmemBytes, side_s>>>(
-                A, n, stride, t0, nt, 2, w, pp, kOuterPanels, pstride, lo, bad);
+                A, n, stride, t0, nt, 2, w, pp, op, pstride, lo, bad);
             ctx->launches += 1;
         }
         if ((e = cudaEventRecord(ev_side, side_s)) != cudaSuccess) return e;
         k_lu_update_tc<<<dim3(w * (2 * nt - w), 1, nbz), 128, kTcSmemBytes, main_s>>>(
-            A, n, stride, t0, nt, 1, w, pp, kOuterPanels, pstride, lo, bad);
+            A, n, stride, t0, nt, 1, w, pp, op, pstride, lo, bad);
         ctx->launches += 1;
         if (lo < n) {
             k_lu_diag64<<<nbatch, kDiag64Threads, kDiag64Smem, main_s>>>(A, n, stride, lo, Dinv, dstride, bad,
@@ -1439,8 +1469,8 @@ cudaError_t lu_tc_group(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int n
 }
 }  // namespace
 
-// The matrices in kLuGroups groups (contiguous, sizes differing by one at
-// most), each on its own (main, side) stream pair: group 0 on the context's
+// The matrices in groups (the ctx's schedule for n: 1 to kLuGroups groups,
+// contiguous, sizes differing by one at most), each on its own (main, side) stream pair: group 0 on the context's
 // streams, the others forked from its stream and joined back, so the
 // diagonal-block factorisations and panel solves of one group (one CTA per
 // matrix, latency bound) run beside the trailing updates of another.
@@ -1450,7 +1480,10 @@ cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int 
     cudaError_t e;
     static_assert(TC_NB == 64, "the diagonal blocks are factored by k_lu_diag64");
     static_assert(TC_TM == 2 * TC_NB && TC_TN == TC_TM, "two panels per 128-wide tile");
-    static_assert(kOuterPanels <= kMaxPairs && kOuterPanels == 4, "an outer step spans two tiles");
+    const LuSchedule sched = ctx->lu_schedule(n);
+    if (sched.groups < 1 || sched.groups > kLuGroups || sched.outer < 2 || sched.outer > kOuterMax ||
+        (sched.outer & 1))
+        return cudaErrorInvalidValue;
     if ((e = cudaFuncSetAttribute(k_lu_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kTcSmemBytes)) != cudaSuccess)
         return e;
@@ -1460,7 +1493,7 @@ cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int 
     if ((e = cudaFuncSetAttribute(k_lu_diag64, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kDiag64Smem)) != cudaSuccess)
         return e;
-    const int groups = std::min(kLuGroups, nbatch);
+    const int groups = std::min(sched.groups, nbatch);
     const int64_t dstride = lu_dinv_stride_tc(n);
     const int64_t pbytes = lu_panel_bytes_tc(n);
     if (groups > 1) {
@@ -1474,7 +1507,7 @@ cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int 
         cudaStream_t ms = g ? ctx->grp_main[g - 1] : ctx->stream, ss = g ? ctx->grp_side[g - 1] : ctx->side;
         cudaEvent_t es = g ? ctx->grp_ev_side[g - 1] : ctx->ev_side, ep = g ? ctx->grp_ev_panel[g - 1] : ctx->ev_panel;
         if ((e = lu_tc_group(ctx, A + (int64_t)b0 * stride, n, stride, nbg, Dinv + (int64_t)b0 * dstride,
-                             panels + (int64_t)b0 * pbytes, bad + b0, ms, ss, es, ep)) != cudaSuccess)
+                             panels + (int64_t)b0 * pbytes, bad + b0, ms, ss, es, ep, sched.outer)) != cudaSuccess)
             return e;
         b0 += nbg;
     }

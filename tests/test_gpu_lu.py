@@ -186,3 +186,33 @@ def test_refinement_skips_converged_frequencies(mh, oracle, gpu):
         assert 1 <= info.refine_iterations <= 6
     Ao, _, _, _ = oracle.hydro_coefficients(mesh, om, dofs)
     assert np.max(np.abs(A - Ao)) / np.max(np.abs(Ao)) < 1e-9
+
+
+@pytest.mark.parametrize("groups,outer", [(1, 2), (1, 4), (2, 6), (3, 8), (4, 4), (4, 8)])
+@pytest.mark.parametrize("n", [640, 641, 1100])
+def test_tcgen05_lu_schedules_reconstruct(mh, gpu, groups, outer, n):
+    """Every schedule the autotuner may pick (stream groups, 64-column panels
+    per outer step) factors the same matrices to the same accuracy; 1100 has
+    several outer steps of every width and a ragged last tile."""
+    rng = np.random.default_rng(n + 7 * outer + groups)
+    A = _bem_like(rng, 5, n)
+    gpu.set_lu_schedule(0, groups, outer)
+    try:
+        LU, bad = gpu.lu_factor_lowp(A, "tcgen05")
+    finally:
+        gpu.set_lu_schedule(0, 2, 4)
+    assert not bad.any()
+    for b in range(A.shape[0]):
+        R = _reconstruct(LU[b].astype(np.complex128))
+        assert np.max(np.abs(R - A[b])) / np.max(np.abs(A[b])) <= 4e-3, (groups, outer, n, b)
+
+
+def test_lu_autotune_sets_the_fastest(mh, gpu):
+    cand = [(1, 4), (2, 4), (2, 8)]
+    out = gpu.autotune_lu(512, 6, cand)
+    assert set(out["ms"]) == set(cand) and all(0.0 < t < 1e4 for t in out["ms"].values())
+    assert out["best"] == min(out["ms"], key=out["ms"].get)
+    assert gpu.lu_schedule(512) == out["best"]
+    assert gpu.lu_schedule(500) == out["best"]  # nearest entry
+    assert gpu.lu_schedule(0) == (2, 4)  # the default is untouched
+    gpu.set_lu_schedule(512, 2, 4)
