@@ -126,22 +126,25 @@ int mh_ctx_set_lu_backend(mh_ctx* ctx, int backend);
  * its own pair of streams, so that one group's latency-bound diagonal blocks
  * and panel solves overlap another's trailing updates; `outer_panels` (2, 4,
  * 6 or 8) 64-column panels per outer step, the trailing matrix being updated
- * once per outer step with all of them accumulated in tensor memory.  n = 0
- * sets the default for sizes with no entry of their own (2 groups, 4 panels);
- * otherwise a size uses the entry nearest to it (in log n).  No reference
- * counterpart (the reference factors with LAPACK). */
-int mh_ctx_set_lu_schedule(mh_ctx* ctx, int64_t n, int groups, int outer_panels);
-int mh_ctx_get_lu_schedule(mh_ctx* ctx, int64_t n, int* groups, int* outer_panels);
+ * once per outer step with all of them accumulated in tensor memory;
+ * `update_kernel` 0 (the trailing tile C read and written through shared
+ * memory by bulk copies after the MMAs) or 1 (C staged in tensor memory
+ * before the MMAs, which accumulate onto it).  n = 0 sets the default for
+ * sizes with no entry of their own (2 groups, 4 panels, kernel 0); otherwise
+ * a size uses the entry nearest to it (in log n).  No reference counterpart
+ * (the reference factors with LAPACK). */
+int mh_ctx_set_lu_schedule(mh_ctx* ctx, int64_t n, int groups, int outer_panels, int update_kernel);
+int mh_ctx_get_lu_schedule(mh_ctx* ctx, int64_t n, int* groups, int* outer_panels, int* update_kernel);
 
 /* Autotuner of that schedule: factors nbatch synthetic n x n diagonally
  * dominant matrices (generated on the device) with each of the ncand
- * candidate schedules (groups[c], outer_panels[c]), one warm-up and one
+ * candidate schedules (groups[c], outer_panels[c], update_kernel[c]), one warm-up and one
  * timed factorisation each (CUDA events on the ctx stream), writes the times
  * to ms[c] (host, milliseconds), sets the fastest as the ctx's schedule for
  * n and returns its index in *best (may be NULL).  Uses the ctx's workspace
  * (n^2 nbatch complex64 plus the LU scratch).  No reference counterpart. */
 int mh_lu_autotune(mh_ctx* ctx, int64_t n, int64_t nbatch, int ncand, const int* groups,
-                   const int* outer_panels, double* ms, int* best);
+                   const int* outer_panels, const int* update_kernel, double* ms, int* best);
 
 /* Failure injection for tests (no reference counterpart): while enabled, the
  * flag waits of the tensor-core backend's triangular solves on this ctx wait

@@ -78,12 +78,12 @@ SIGNATURES = {
     "mh_ctx_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
     "mh_ctx_set_lu_backend": (ctypes.c_int, [_P, ctypes.c_int]),
     "mh_ctx_set_wait_injection": (ctypes.c_int, [_P, ctypes.c_int]),
-    "mh_ctx_set_lu_schedule": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_int, ctypes.c_int]),
+    "mh_ctx_set_lu_schedule": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "mh_ctx_get_lu_schedule": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.POINTER(ctypes.c_int),
-                                              ctypes.POINTER(ctypes.c_int)]),
+                                              ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "mh_lu_autotune": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
-                                      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), _D,
-                                      ctypes.POINTER(ctypes.c_int)]),
+                                      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                      ctypes.POINTER(ctypes.c_int), _D, ctypes.POINTER(ctypes.c_int)]),
     "mh_lu_factor_lowp": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int64, ctypes.c_int64, _D,
                                          ctypes.POINTER(ctypes.c_float),
                                          ctypes.POINTER(ctypes.c_int)]),
@@ -218,34 +218,40 @@ class Context:
         code = {"simt": MH_LU_SIMT_F32, "tcgen05": MH_LU_TCGEN05_F16}[backend]
         check(lib().mh_ctx_set_lu_backend(self._h, code), self._h)
 
-    # candidates of the LU autotuner: (groups, 64-column panels per outer step)
-    LU_CANDIDATES = ((1, 4), (2, 2), (2, 4), (2, 6), (2, 8), (3, 4), (4, 4), (4, 8))
+    # candidates of the LU autotuner: (groups, 64-column panels per outer
+    # step, update kernel 0 = C through shared memory after the MMAs,
+    # 1 = C staged in tensor memory before them)
+    LU_CANDIDATES = ((1, 4, 0), (2, 2, 0), (2, 4, 0), (2, 6, 0), (3, 4, 0), (4, 4, 0),
+                     (1, 4, 1), (2, 2, 1), (2, 4, 1), (2, 6, 1), (3, 4, 1), (4, 4, 1))
 
-    def set_lu_schedule(self, n: int, groups: int, outer_panels: int):
+    def set_lu_schedule(self, n: int, groups: int, outer_panels: int, update_kernel: int = 0):
         """Tensor-core LU schedule for matrices of n panels (n = 0: the default)."""
-        check(lib().mh_ctx_set_lu_schedule(self._h, int(n), int(groups), int(outer_panels)), self._h)
+        check(lib().mh_ctx_set_lu_schedule(self._h, int(n), int(groups), int(outer_panels), int(update_kernel)),
+              self._h)
 
     def lu_schedule(self, n: int = 0) -> tuple:
-        g, o = ctypes.c_int(0), ctypes.c_int(0)
-        check(lib().mh_ctx_get_lu_schedule(self._h, int(n), ctypes.byref(g), ctypes.byref(o)), self._h)
-        return int(g.value), int(o.value)
+        g, o, u = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+        check(lib().mh_ctx_get_lu_schedule(self._h, int(n), ctypes.byref(g), ctypes.byref(o), ctypes.byref(u)),
+              self._h)
+        return int(g.value), int(o.value), int(u.value)
 
     def autotune_lu(self, n: int, nbatch: int, candidates=None) -> dict:
-        """Time each candidate schedule on nbatch synthetic n x n matrices and
-        keep the fastest for n (``mh_lu_autotune``).  Returns
-        {"n", "nbatch", "best": (groups, outer_panels), "ms": {(g, o): ms}}."""
-        cand = list(candidates or self.LU_CANDIDATES)
+        """Time each candidate schedule (groups, outer_panels, update_kernel)
+        on nbatch synthetic n x n matrices and keep the fastest for n
+        (``mh_lu_autotune``).  Returns {"n", "nbatch", "best", "ms": {candidate: ms}}."""
+        cand = [tuple(c) if len(c) == 3 else (c[0], c[1], 0) for c in (candidates or self.LU_CANDIDATES)]
         g = (ctypes.c_int * len(cand))(*[c[0] for c in cand])
         o = (ctypes.c_int * len(cand))(*[c[1] for c in cand])
+        u = (ctypes.c_int * len(cand))(*[c[2] for c in cand])
         ms = np.zeros(len(cand))
         best = ctypes.c_int(-1)
-        check(lib().mh_lu_autotune(self._h, int(n), int(nbatch), len(cand), g, o, dptr(ms), ctypes.byref(best)),
+        check(lib().mh_lu_autotune(self._h, int(n), int(nbatch), len(cand), g, o, u, dptr(ms), ctypes.byref(best)),
               self._h)
-        return {"n": int(n), "nbatch": int(nbatch), "best": tuple(cand[best.value]),
-                "ms": {tuple(c): float(t) for c, t in zip(cand, ms)}}
+        return {"n": int(n), "nbatch": int(nbatch), "best": cand[best.value],
+                "ms": {c: float(t) for c, t in zip(cand, ms)}}
 
     def save_lu_table(self, path, entries):
-        """Write autotuner results ({n: (groups, outer_panels)}) as JSON."""
+        """Write autotuner results ({n: (groups, outer_panels, update_kernel)}) as JSON."""
         import json
 
         pathlib.Path(path).write_text(json.dumps({str(int(k)): list(v) for k, v in entries.items()}, indent=1))
@@ -255,8 +261,8 @@ class Context:
         import json
 
         table = {int(k): tuple(v) for k, v in json.loads(pathlib.Path(path).read_text()).items()}
-        for n, (g_, o_) in table.items():
-            self.set_lu_schedule(n, g_, o_)
+        for n, sched in table.items():
+            self.set_lu_schedule(n, *sched)
         return table
 
     def set_wait_injection(self, enable: bool):

@@ -536,16 +536,19 @@ int mh_lu_solve_lowp(mh_ctx* ctx, int backend, int64_t n, int64_t nbatch, const 
     return MH_OK;
 }
 
-int mh_ctx_set_lu_schedule(mh_ctx* ctx, int64_t n, int groups, int outer_panels)
+int mh_ctx_set_lu_schedule(mh_ctx* ctx, int64_t n, int groups, int outer_panels, int update_kernel)
 {
     int rc;
     if ((rc = check_ctx(ctx))) return rc;
-    if (n < 0 || groups < 1 || groups > kLuGroups || outer_panels < 2 || outer_panels > 8 || (outer_panels & 1))
-        return set_err(ctx, MH_ERR_ARG, "LU schedule: need n >= 0, 1 <= groups <= %d, outer_panels in {2, 4, 6, 8}",
+    if (n < 0 || groups < 1 || groups > kLuGroups || outer_panels < 2 || outer_panels > 8 || (outer_panels & 1) ||
+        update_kernel < 0 || update_kernel > 1)
+        return set_err(ctx, MH_ERR_ARG,
+                       "LU schedule: need n >= 0, 1 <= groups <= %d, outer_panels in {2, 4, 6, 8}, update_kernel 0 or 1",
                        kLuGroups);
     LuSchedule s;
     s.groups = groups;
     s.outer = outer_panels;
+    s.update = update_kernel;
     if (n == 0) {
         ctx->lu_default = s;
         return MH_OK;
@@ -559,29 +562,32 @@ int mh_ctx_set_lu_schedule(mh_ctx* ctx, int64_t n, int groups, int outer_panels)
     return MH_OK;
 }
 
-int mh_ctx_get_lu_schedule(mh_ctx* ctx, int64_t n, int* groups, int* outer_panels)
+int mh_ctx_get_lu_schedule(mh_ctx* ctx, int64_t n, int* groups, int* outer_panels, int* update_kernel)
 {
     int rc;
     if ((rc = check_ctx(ctx))) return rc;
-    if (n < 0 || !groups || !outer_panels) return set_err(ctx, MH_ERR_ARG, "bad arguments to mh_ctx_get_lu_schedule");
+    if (n < 0 || !groups || !outer_panels || !update_kernel)
+        return set_err(ctx, MH_ERR_ARG, "bad arguments to mh_ctx_get_lu_schedule");
     const LuSchedule s = n == 0 ? ctx->lu_default : ctx->lu_schedule(n);
     *groups = s.groups;
     *outer_panels = s.outer;
+    *update_kernel = s.update;
     return MH_OK;
 }
 
 int mh_lu_autotune(mh_ctx* ctx, int64_t n, int64_t nbatch, int ncand, const int* groups, const int* outer_panels,
-                   double* ms, int* best)
+                   const int* update_kernel, double* ms, int* best)
 {
     int rc;
     if ((rc = check_ctx(ctx))) return rc;
-    if (n < 1 || nbatch < 1 || ncand < 1 || !groups || !outer_panels || !ms)
+    if (n < 1 || nbatch < 1 || ncand < 1 || !groups || !outer_panels || !update_kernel || !ms)
         return set_err(ctx, MH_ERR_ARG, "bad arguments to mh_lu_autotune");
     for (int c = 0; c < ncand; ++c)
         if (groups[c] < 1 || groups[c] > kLuGroups || outer_panels[c] < 2 || outer_panels[c] > 8 ||
-            (outer_panels[c] & 1))
-            return set_err(ctx, MH_ERR_ARG, "candidate %d: need 1 <= groups <= %d, outer_panels in {2, 4, 6, 8}", c,
-                           kLuGroups);
+            (outer_panels[c] & 1) || update_kernel[c] < 0 || update_kernel[c] > 1)
+            return set_err(ctx, MH_ERR_ARG,
+                           "candidate %d: need 1 <= groups <= %d, outer_panels in {2, 4, 6, 8}, update_kernel 0 or 1",
+                           c, kLuGroups);
     const size_t nn = (size_t)n * (size_t)n;
     auto* lo = (float2*)ws_get(ctx, WS_LO, sizeof(float2) * nn * (size_t)nbatch);
     auto* dinv = (float2*)ws_get(ctx, WS_DINV, sizeof(float2) * (size_t)mh::lu_dinv_stride_tc(n) * (size_t)nbatch);
@@ -602,6 +608,7 @@ int mh_lu_autotune(mh_ctx* ctx, int64_t n, int64_t nbatch, int ncand, const int*
     for (int c = 0; c < ncand && e == cudaSuccess; ++c) {
         ctx->lu_default.groups = groups[c];
         ctx->lu_default.outer = outer_panels[c];
+        ctx->lu_default.update = update_kernel[c];
         ms[c] = INFINITY;
         // one warm-up factorisation, then one timed; fresh matrices each time
         for (int rep = 0; rep < 2 && e == cudaSuccess; ++rep) {
@@ -622,7 +629,8 @@ int mh_lu_autotune(mh_ctx* ctx, int64_t n, int64_t nbatch, int ncand, const int*
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (e != cudaSuccess) return set_err(ctx, MH_ERR_CUDA, "LU autotune: %s", cudaGetErrorString(e));
-    if ((rc = mh_ctx_set_lu_schedule(ctx, n, groups[fastest], outer_panels[fastest]))) return rc;
+    if ((rc = mh_ctx_set_lu_schedule(ctx, n, groups[fastest], outer_panels[fastest], update_kernel[fastest])))
+        return rc;
     if (best) *best = fastest;
     return MH_OK;
 }

@@ -52,10 +52,13 @@ enum Phase : int {
 constexpr int kLuGroups = 4;
 
 // Schedule of the tensor-core LU: groups of matrices on their own stream
-// pairs (1 .. kLuGroups) and 64-column panels per outer step (even, 2 .. 8).
+// pairs (1 .. kLuGroups), 64-column panels per outer step (even, 2 .. 8) and
+// the trailing-update kernel (0: C through shared memory after the MMAs,
+// 1: C staged in tensor memory before them).
 struct LuSchedule {
     int groups = 2;
     int outer = 4;
+    int update = 0;
 };
 
 struct mh_ctx {

@@ -127,6 +127,16 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
         : "r"(taddr));
 }
 
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16])
+{
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
+        "{%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16};"
+        :: "r"(taddr), "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+           "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+        : "memory");
+}
+
 __device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols)
 {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
@@ -529,6 +539,136 @@ k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int t0, int n
             if (cc + 1 < TC_TN / kEc) {
 #pragma unroll
                 for (int q = 0; q < kEc; ++q) cv[q] = nv[q];
+            }
+        }
+    } else {
+        if (lane == 0) atomicExch(bad + b, 2);
+        // bounded: copies or MMAs of the failed pair may still be in flight
+        if (pend_ld >= 0) mbar_wait(bar_ld, (uint32_t)(pend_ld & 1));
+        if (pend_mma >= 0) mbar_wait(bar_mma, (uint32_t)(pend_mma & 1));
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, kTmemCols);
+}
+
+// The same update with C staged in tensor memory first: every thread loads
+// its row of the C tile (negated) into the accumulator's TMEM columns while
+// the first panel pair is copied, the MMAs accumulate L21 U12 onto it, and
+// the epilogue only reads the accumulator back and stores C - L21 U12 (the
+// negation undone).  The C read thus overlaps the operand copies instead of
+// following the MMAs.  Grid, tiles and operands as k_lu_update_tc.
+__global__ void __launch_bounds__(128, 2)
+k_lu_update_tc_acc(float2* __restrict__ Ab, int64_t n, int64_t stride, int t0, int ntile, int mode, int w,
+                   PanelPairs pp, int npair, int64_t pstride, int64_t lo, int* __restrict__ bad)
+{
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    __shared__ uint64_t mbar[2];
+    __shared__ uint32_t tmem_slot;
+    unsigned char* sA = tc_smem;
+    unsigned char* sB = tc_smem + kSmemA;
+    const int b = blockIdx.z;
+    float2* M = Ab + (int64_t)b * stride;
+    int ti, tj;
+    if (mode == 1) {
+        const int x = (int)blockIdx.x;
+        if (x < w * ntile) {
+            ti = t0 + x / ntile;
+            tj = t0 + x % ntile;
+        } else {
+            const int y = x - w * ntile, rest = ntile - w;
+            tj = t0 + y / rest;
+            ti = t0 + w + y % rest;
+        }
+    } else {
+        ti = t0 + w + (int)blockIdx.x;
+        tj = t0 + w + (int)blockIdx.y;
+    }
+    const int64_t r0 = (int64_t)ti * TC_TM;
+    const int64_t c0 = (int64_t)tj * TC_TN;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (warp == 0) tmem_alloc(&tmem_slot, kTmemCols);
+    const uint32_t bar_ld = smem_u32(&mbar[0]), bar_mma = smem_u32(&mbar[1]);
+    if (tid == 0) {
+        mbar_init(&mbar[0]);
+        mbar_init(&mbar[1]);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+    auto copy_pair = [&](int p) {
+        const unsigned char* srcA = pp.L[p] + (int64_t)b * pstride + (int64_t)ti * kPanelL;
+        const unsigned char* srcB = pp.U[p] + (int64_t)b * pstride + (int64_t)tj * kPanelU;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                     :: "r"(bar_ld), "r"(kPanelL + kPanelU) : "memory");
+        constexpr uint32_t kChunk = 16384;
+#pragma unroll 1
+        for (uint32_t off = 0; off < kPanelL; off += kChunk)
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                         :: "r"(smem_u32(sA + off)), "l"(srcA + off), "r"(kChunk), "r"(bar_ld) : "memory");
+#pragma unroll 1
+        for (uint32_t off = 0; off < kPanelU; off += kChunk)
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                         :: "r"(smem_u32(sB + off)), "l"(srcB + off), "r"(kChunk), "r"(bar_ld) : "memory");
+    };
+    if (tid == 0) copy_pair(0);
+    // -C into the accumulator, 16 columns at a time (rows or columns outside
+    // [lo, n) as zeros; they are not stored back)
+    const int64_t gi = r0 + warp * 32 + lane;
+    const bool row_ok = gi >= lo && gi < n;
+    constexpr int kEc = 16;
+#pragma unroll 2
+    for (int cc = 0; cc < TC_TN / kEc; ++cc) {
+        uint32_t re[kEc], im[kEc];
+        const float2* pc = M + (c0 + cc * kEc) * n + gi;
+#pragma unroll
+        for (int q = 0; q < kEc; ++q) {
+            const int64_t gj = c0 + cc * kEc + q;
+            const float2 v = (row_ok && gj >= lo && gj < n) ? pc[(int64_t)q * n] : make_float2(0.f, 0.f);
+            re[q] = __float_as_uint(-v.x);
+            im[q] = __float_as_uint(-v.y);
+        }
+        tmem_st16(lane_base + (uint32_t)(cc * kEc), re);
+        tmem_st16(lane_base + (uint32_t)(TC_TN + cc * kEc), im);
+    }
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    bool ok = true;     // every wait so far completed
+    int pend_ld = -1;   // pair whose copies were issued and not seen complete
+    int pend_mma = -1;  // pair whose MMAs were issued and not seen complete
+#pragma unroll 1
+    for (int p = 0; p < npair && ok; ++p) {
+        if (tid == 0 && p > 0) copy_pair(p);
+        pend_ld = p;
+        // also orders every thread's TMEM stores of C before the first MMAs
+        ok = __syncthreads_and(mbar_wait(bar_ld, (uint32_t)(p & 1))) != 0;
+        if (!ok) break;
+        pend_ld = -1;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (tid == 0) mma_k128(tmem, smem_u32(sA), kLboA, smem_u32(sB), kLboB, kIdesc, bar_mma, true);
+        // the next pair's copies overwrite the operands: wait for these MMAs
+        pend_mma = p;
+        ok = __syncthreads_and(mbar_wait(bar_mma, (uint32_t)(p & 1))) != 0;
+        if (ok) pend_mma = -1;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (ok) {
+#pragma unroll 2
+        for (int cc = 0; cc < TC_TN / kEc; ++cc) {
+            uint32_t re[kEc], im[kEc];
+            tmem_ld16(lane_base + (uint32_t)(cc * kEc), re);
+            tmem_ld16(lane_base + (uint32_t)(TC_TN + cc * kEc), im);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row_ok) {
+                float2* pc = M + (c0 + cc * kEc) * n + gi;
+#pragma unroll
+                for (int q = 0; q < kEc; ++q) {
+                    const int64_t gj = c0 + cc * kEc + q;
+                    if (gj >= lo && gj < n)
+                        pc[(int64_t)q * n] = make_float2(-__uint_as_float(re[q]), -__uint_as_float(im[q]));
+                }
             }
         }
     } else {
@@ -1391,8 +1531,9 @@ namespace {
 // panels: lu_panel_bytes_tc(n) * nbatch bytes for these matrices.
 cudaError_t lu_tc_group(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int nbatch, float2* Dinv,
                         unsigned char* panels, int* bad, cudaStream_t main_s, cudaStream_t side_s,
-                        cudaEvent_t ev_side, cudaEvent_t ev_panel, const int op)
+                        cudaEvent_t ev_side, cudaEvent_t ev_panel, const int op, const int update)
 {
+    auto* upd = update ? k_lu_update_tc_acc : k_lu_update_tc;
     cudaError_t e;
     const int64_t dstride = lu_dinv_stride_tc(n);
     const int64_t pstride = (int64_t)((n + TC_TM - 1) / TC_TM) * (kPanelL + kPanelU);  // one buffer, per matrix
@@ -1429,7 +1570,7 @@ cudaError_t lu_tc_group(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int n
                 one.L[0] = pp.L[s];
                 one.U[0] = pp.U[s];
                 const int w = std::min(T0 + kW - t0, nt);
-                k_lu_update_tc<<<dim3(w * (2 * nt - w), 1, nbz), 128, kTcSmemBytes, main_s>>>(
+                upd<<<dim3(w * (2 * nt - w), 1, nbz), 128, kTcSmemBytes, main_s>>>(
                     A, n, stride, t0, nt, 1, w, one, 1, pstride, k + TC_NB, bad);
                 k_lu_diag64<<<nbatch, kDiag64Threads, kDiag64Smem, main_s>>>(A, n, stride, k + TC_NB, Dinv, dstride,
                                                                            bad, bimg, bstride);
@@ -1447,12 +1588,12 @@ cudaError_t lu_tc_group(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int n
         if ((e = cudaStreamWaitEvent(side_s, ev_panel, 0)) != cudaSuccess) return e;
         const int w = std::min(kW, nt);
         if (nt > w) {
-            k_lu_update_tc<<<dim3(nt - w, nt - w, nbz), 128, kTcSmemBytes, side_s>>>(
+            upd<<<dim3(nt - w, nt - w, nbz), 128, kTcSmemBytes, side_s>>>(
                 A, n, stride, t0, nt, 2, w, pp, op, pstride, lo, bad);
             ctx->launches += 1;
         }
         if ((e = cudaEventRecord(ev_side, side_s)) != cudaSuccess) return e;
-        k_lu_update_tc<<<dim3(w * (2 * nt - w), 1, nbz), 128, kTcSmemBytes, main_s>>>(
+        upd<<<dim3(w * (2 * nt - w), 1, nbz), 128, kTcSmemBytes, main_s>>>(
             A, n, stride, t0, nt, 1, w, pp, op, pstride, lo, bad);
         ctx->launches += 1;
         if (lo < n) {
@@ -1482,10 +1623,13 @@ cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int 
     static_assert(TC_TM == 2 * TC_NB && TC_TN == TC_TM, "two panels per 128-wide tile");
     const LuSchedule sched = ctx->lu_schedule(n);
     if (sched.groups < 1 || sched.groups > kLuGroups || sched.outer < 2 || sched.outer > kOuterMax ||
-        (sched.outer & 1))
+        (sched.outer & 1) || sched.update < 0 || sched.update > 1)
         return cudaErrorInvalidValue;
     if ((e = cudaFuncSetAttribute(k_lu_update_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kTcSmemBytes)) != cudaSuccess)
+        return e;
+    if ((e = cudaFuncSetAttribute(k_lu_update_tc_acc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(kSmemA + kSmemB))) != cudaSuccess)
         return e;
     if ((e = cudaFuncSetAttribute(k_lu_trsm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(kSmemA + kSmemA))) != cudaSuccess)
@@ -1507,7 +1651,8 @@ cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int 
         cudaStream_t ms = g ? ctx->grp_main[g - 1] : ctx->stream, ss = g ? ctx->grp_side[g - 1] : ctx->side;
         cudaEvent_t es = g ? ctx->grp_ev_side[g - 1] : ctx->ev_side, ep = g ? ctx->grp_ev_panel[g - 1] : ctx->ev_panel;
         if ((e = lu_tc_group(ctx, A + (int64_t)b0 * stride, n, stride, nbg, Dinv + (int64_t)b0 * dstride,
-                             panels + (int64_t)b0 * pbytes, bad + b0, ms, ss, es, ep, sched.outer)) != cudaSuccess)
+                             panels + (int64_t)b0 * pbytes, bad + b0, ms, ss, es, ep, sched.outer,
+                             sched.update)) != cudaSuccess)
             return e;
         b0 += nbg;
     }

@@ -188,15 +188,17 @@ def test_refinement_skips_converged_frequencies(mh, oracle, gpu):
     assert np.max(np.abs(A - Ao)) / np.max(np.abs(Ao)) < 1e-9
 
 
-@pytest.mark.parametrize("groups,outer", [(1, 2), (1, 4), (2, 6), (3, 8), (4, 4), (4, 8)])
+@pytest.mark.parametrize("groups,outer,update", [(1, 2, 0), (1, 4, 1), (2, 6, 0), (2, 4, 1), (3, 8, 1), (4, 4, 0),
+                                                 (4, 8, 1)])
 @pytest.mark.parametrize("n", [640, 641, 1100])
-def test_tcgen05_lu_schedules_reconstruct(mh, gpu, groups, outer, n):
+def test_tcgen05_lu_schedules_reconstruct(mh, gpu, groups, outer, update, n):
     """Every schedule the autotuner may pick (stream groups, 64-column panels
-    per outer step) factors the same matrices to the same accuracy; 1100 has
-    several outer steps of every width and a ragged last tile."""
+    per outer step, update kernel) factors the same matrices to the same
+    accuracy; 1100 has several outer steps of every width and a ragged last
+    tile."""
     rng = np.random.default_rng(n + 7 * outer + groups)
     A = _bem_like(rng, 5, n)
-    gpu.set_lu_schedule(0, groups, outer)
+    gpu.set_lu_schedule(0, groups, outer, update)
     try:
         LU, bad = gpu.lu_factor_lowp(A, "tcgen05")
     finally:
@@ -208,11 +210,11 @@ def test_tcgen05_lu_schedules_reconstruct(mh, gpu, groups, outer, n):
 
 
 def test_lu_autotune_sets_the_fastest(mh, gpu):
-    cand = [(1, 4), (2, 4), (2, 8)]
+    cand = [(1, 4, 0), (2, 4, 0), (2, 8, 1)]
     out = gpu.autotune_lu(512, 6, cand)
     assert set(out["ms"]) == set(cand) and all(0.0 < t < 1e4 for t in out["ms"].values())
     assert out["best"] == min(out["ms"], key=out["ms"].get)
     assert gpu.lu_schedule(512) == out["best"]
     assert gpu.lu_schedule(500) == out["best"]  # nearest entry
-    assert gpu.lu_schedule(0) == (2, 4)  # the default is untouched
+    assert gpu.lu_schedule(0) == (2, 4, 0)  # the default is untouched
     gpu.set_lu_schedule(512, 2, 4)
