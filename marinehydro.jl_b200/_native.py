@@ -78,6 +78,7 @@ SIGNATURES = {
     "mh_ctx_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
     "mh_ctx_set_lu_backend": (ctypes.c_int, [_P, ctypes.c_int]),
     "mh_ctx_set_wait_injection": (ctypes.c_int, [_P, ctypes.c_int]),
+    "mh_ctx_set_wave_series_fp32": (ctypes.c_int, [_P, ctypes.c_int]),
     "mh_ctx_set_lu_schedule": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "mh_ctx_get_lu_schedule": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.POINTER(ctypes.c_int),
                                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
@@ -264,6 +265,11 @@ class Context:
         for n, sched in table.items():
             self.set_lu_schedule(n, *sched)
         return table
+
+    def set_wave_series_fp32(self, enable: bool):
+        """Mixed path: the per-frequency Horner series of the tabulated
+        Delhommeau term in FP32 (``mh_ctx_set_wave_series_fp32``; off by default)."""
+        check(lib().mh_ctx_set_wave_series_fp32(self._h, int(bool(enable))), self._h)
 
     def set_wait_injection(self, enable: bool):
         """Failure injection (tests): the triangular solves' flag waits wait

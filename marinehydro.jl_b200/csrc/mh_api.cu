@@ -364,6 +364,8 @@ int mh_ctx_destroy(mh_ctx* ctx)
         if (ctx->ev_open[q]) cudaEventDestroy(ctx->ev_open[q]);
     for (cudaEvent_t e : ctx->ev_pool) cudaEventDestroy(e);
     if (ctx->cusolver) cusolverDnDestroy(ctx->cusolver);
+    for (int g = 0; g < kLuGroups - 1; ++g)
+        if (ctx->cusolver_grp[g]) cusolverDnDestroy(ctx->cusolver_grp[g]);
     if (ctx->cublas) cublasDestroy(ctx->cublas);
     if (ctx->ev_panel) cudaEventDestroy(ctx->ev_panel);
     if (ctx->ev_side) cudaEventDestroy(ctx->ev_side);
@@ -632,6 +634,14 @@ int mh_lu_autotune(mh_ctx* ctx, int64_t n, int64_t nbatch, int ncand, const int*
     if ((rc = mh_ctx_set_lu_schedule(ctx, n, groups[fastest], outer_panels[fastest], update_kernel[fastest])))
         return rc;
     if (best) *best = fastest;
+    return MH_OK;
+}
+
+int mh_ctx_set_wave_series_fp32(mh_ctx* ctx, int enable)
+{
+    int rc;
+    if ((rc = check_ctx(ctx))) return rc;
+    ctx->wave_series_fp32 = enable != 0;
     return MH_OK;
 }
 

@@ -181,10 +181,24 @@ __constant__ double c_polar_mono[4 * kTabPolarFn];
 
 constexpr int kWT = 128;  // threads (rows) per CTA of k_wave_delh_allw
 constexpr int kAllwMaxFreqs = 128;  // frequencies per launch of k_wave_delh_allw
-// the contracted series of every row, k, log k and 1/k per frequency (the
-// polar coefficients are read from constant memory)
-constexpr size_t kWaveAllwSmem = sizeof(double) * (4 * kTabNU * kWT + 3 * kAllwMaxFreqs);
+// k, log k and 1/k per frequency, then the contracted series of every row
+// in the type HT of the per-frequency Horner pass (the polar coefficients
+// are read from constant memory)
+template <typename HT>
+constexpr size_t wave_allw_smem()
+{
+    return sizeof(double) * 3 * kAllwMaxFreqs + sizeof(HT) * 4 * kTabNU * kWT;
+}
+constexpr size_t kWaveAllwSmem = wave_allw_smem<double>();
 
+__device__ __forceinline__ double hfma(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float hfma(float a, float b, float c) { return fmaf(a, b, c); }
+
+// HT: the type of the per-frequency Horner series in R (double; float is the
+// reduced-precision option of the mixed path, mh_ctx_set_wave_series_fp32).
+// The alpha contraction, the log terms and everything after the series stay
+// in FP64.
+template <typename HT>
 __global__ void __launch_bounds__(kWT, 3)
 k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const double* __restrict__ tab,
                  const double* __restrict__ kvec, int nb, const double* __restrict__ SR,
@@ -192,10 +206,10 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
                  float2* __restrict__ Dlo, double2* __restrict__ tape, int* __restrict__ fall)
 {
     extern __shared__ double wsm[];
-    double* w = wsm;                               // [4 * NU][kWT]
-    double* logk = w + 4 * kTabNU * kWT;           // [nb]
+    double* logk = wsm;                            // [nb]
     double* invk = logk + kAllwMaxFreqs;           // [nb], nb <= kAllwMaxFreqs
     double* ksm = invk + kAllwMaxFreqs;            // [nb]
+    HT* w = reinterpret_cast<HT*>(ksm + kAllwMaxFreqs);  // [4 * NU][kWT]
     __shared__ Panel sp[kCols];
     const int64_t j0 = (int64_t)blockIdx.y * kCols;
     stage_panels(sp, geom, n, j0);
@@ -252,7 +266,7 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
                 }
 #pragma unroll
                 for (int q = 0; q < 4; ++q)
-                    w[(q * kTabNU + row) * kWT + tid] = fma(v, b1[q], cr[q * kTabPolarFn] - b2[q]);
+                    w[(q * kTabNU + row) * kWT + tid] = (HT)fma(v, b1[q], cr[q * kTabPolarFn] - b2[q]);
             }
         }
         const AllwPair q{dx, dy, rho, inv_rho, p.area, sr, dr, nn3, o, wrt_first};
@@ -265,7 +279,8 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
         int nfall = 0;
         for (int z0 = 0; z0 < nb; z0 += kZP) {
             const int nz = min(kZP, nb - z0);
-            double kz[kZP], uz[kZP];
+            double kz[kZP];
+            HT uz[kZP];
             bool pz[kZP];
             bool anyp = false;
 #pragma unroll
@@ -274,13 +289,13 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
                 const double R = kz[t] * d;
                 pz[t] = t < nz && polar_ok && R < kTabRPolar;
                 anyp |= pz[t];
-                uz[t] = 2.0 * R / kTabRPolar - 1.0;
+                uz[t] = (HT)(2.0 * R / kTabRPolar - 1.0);
             }
-            double val[kZP][4];
+            HT val[kZP][4];
             if (anyp) {
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    const double c = w[(q * kTabNU + kTabNU - 1) * kWT + tid];
+                    const HT c = w[(q * kTabNU + kTabNU - 1) * kWT + tid];
 #pragma unroll
                     for (int t = 0; t < kZP; ++t) val[t][q] = c;
                 }
@@ -288,9 +303,9 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
                 for (int row = kTabNU - 2; row >= 0; --row) {
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        const double c = w[(q * kTabNU + row) * kWT + tid];
+                        const HT c = w[(q * kTabNU + row) * kWT + tid];
 #pragma unroll
-                        for (int t = 0; t < kZP; ++t) val[t][q] = fma(val[t][q], uz[t], c);
+                        for (int t = 0; t < kZP; ++t) val[t][q] = hfma(val[t][q], uz[t], c);
                     }
                 }
             }
@@ -303,7 +318,8 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
                 }
                 const int z = z0 + t;
                 const double ik = invk[z];
-                const double B = val[t][0], C = val[t][1], E0 = val[t][2], E1 = val[t][3];
+                const double B = (double)val[t][0], C = (double)val[t][1], E0 = (double)val[t][2],
+                             E1 = (double)val[t][3];
                 const double L = logk[z] + lp;
                 const double G_re = -2.0 * E0 * L + B, G_im = 2.0 * kPi * E0;
                 cplx o3[3];
@@ -796,9 +812,10 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
         k_wave_batch<false><<<grid, kRows, 0, ctx->stream>>>(bt.m->geom, n, bt.direct, nullptr, d_k, SR,
                                                             DR, S64, D64, Dlo, nullptr);
     else if (wave == MH_GF_DELHOMMEAU && tab && nb >= kAllwMinFreqs) {
-        MH_CUDA_TRY(ctx, cudaFuncSetAttribute(k_wave_delh_allw,
-                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)kWaveAllwSmem));
+        const bool f32 = ctx->wave_series_fp32;
+        auto* wk = f32 ? k_wave_delh_allw<float> : k_wave_delh_allw<double>;
+        const size_t wsm = f32 ? wave_allw_smem<float>() : wave_allw_smem<double>();
+        MH_CUDA_TRY(ctx, cudaFuncSetAttribute(wk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
         MH_CUDA_TRY(ctx, cudaMemcpyToSymbolAsync(c_polar_mono, tab + kTabMonoOff, sizeof(c_polar_mono), 0,
                                                  cudaMemcpyDeviceToDevice, ctx->stream));
         for (int z = 0; z < nb; z += kAllwMaxFreqs) {
@@ -807,9 +824,8 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
             double2* tp = bt.tape ? bt.tape + 2 * off : nullptr;
             const dim3 g2(blocks(n, kWT), blocks(n, kCols));
             MH_CUDA_TRY(ctx, cudaMemsetAsync(d_fall, 0, sizeof(int), ctx->stream));
-            k_wave_delh_allw<<<g2, kWT, kWaveAllwSmem, ctx->stream>>>(bt.m->geom, n, bt.direct, tab, d_k + z, m, SR,
-                                                                      DR, S64 + off, D64 + off, Dlo + off, tp,
-                                                                      d_fall);
+            wk<<<g2, kWT, wsm, ctx->stream>>>(bt.m->geom, n, bt.direct, tab, d_k + z, m, SR, DR, S64 + off,
+                                              D64 + off, Dlo + off, tp, d_fall);
             k_wave_delh_allw_rest<<<g2, kWT, 0, ctx->stream>>>(d_fall, bt.m->geom, n, bt.direct, tab, d_k + z, m,
                                                               SR, DR, S64 + off, D64 + off, Dlo + off, tp);
             ctx->launches += 1 + (z > 0);
@@ -887,8 +903,9 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
 // FP64 path with the mixed path's batch structure, for one chunk of nb
 // frequencies: the frequency-batched wave pass writes the FP64 S and D (the
 // Rankine part SR, DR computed once per call), then cuSOLVER zgetrf/zgetrs
-// factor and solve each frequency's FP64 D (or K) with partial pivoting, the
-// pivot checks of all frequencies read back once at the end.
+// factor and solve each frequency's FP64 D (or K) with partial pivoting,
+// frequencies spread over several streams, the pivot checks of all
+// frequencies read back once at the end.
 int run_fp64_chunk(const Batch& bt, const double* d_omegas, const double* d_k, int nb, const double* SR,
                    const double* DR, double2* d_F, double2* d_FK)
 {
@@ -917,7 +934,7 @@ int run_fp64_chunk(const Batch& bt, const double* d_omegas, const double* d_k, i
                                                             D64, Dlo, nullptr);
         ctx->launches += 1;
     } else if (wave == MH_GF_DELHOMMEAU && tab && nb >= kAllwMinFreqs) {
-        MH_CUDA_TRY(ctx, cudaFuncSetAttribute(k_wave_delh_allw, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        MH_CUDA_TRY(ctx, cudaFuncSetAttribute(k_wave_delh_allw<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)kWaveAllwSmem));
         MH_CUDA_TRY(ctx, cudaMemcpyToSymbolAsync(c_polar_mono, tab + kTabMonoOff, sizeof(c_polar_mono), 0,
                                                  cudaMemcpyDeviceToDevice, ctx->stream));
@@ -926,7 +943,7 @@ int run_fp64_chunk(const Batch& bt, const double* d_omegas, const double* d_k, i
             const int64_t off = (int64_t)z * nn;
             const dim3 g2(blocks(n, kWT), blocks(n, kCols));
             MH_CUDA_TRY(ctx, cudaMemsetAsync(d_fall, 0, sizeof(int), ctx->stream));
-            k_wave_delh_allw<<<g2, kWT, kWaveAllwSmem, ctx->stream>>>(bt.m->geom, n, bt.direct, tab, d_k + z, m, SR,
+            k_wave_delh_allw<double><<<g2, kWT, kWaveAllwSmem, ctx->stream>>>(bt.m->geom, n, bt.direct, tab, d_k + z, m, SR,
                                                                       DR, S64 + off, D64 + off, Dlo + off, nullptr,
                                                                       d_fall);
             k_wave_delh_allw_rest<<<g2, kWT, 0, ctx->stream>>>(d_fall, bt.m->geom, n, bt.direct, tab, d_k + z, m,
@@ -952,22 +969,44 @@ int run_fp64_chunk(const Batch& bt, const double* d_omegas, const double* d_k, i
     else MH_CUDA_TRY(ctx, cudaMemcpyAsync(X, BC, sizeof(double2) * nv * nb, cudaMemcpyDeviceToDevice, ctx->stream));
     phase_end(ctx, PH_RHS);
     phase_begin(ctx, PH_FP64_LU);
+    // one frequency per stream, kLuGroups streams (the LU groups' main
+    // streams), each with its own cuSOLVER handle and workspace, so the
+    // latency-bound panel factorisations of different frequencies overlap
+    const int ns = std::min(kLuGroups, nb);
+    for (int g = 0; g + 1 < ns; ++g)
+        if (!ctx->cusolver_grp[g]) {
+            if (cusolverDnCreate(&ctx->cusolver_grp[g]) != CUSOLVER_STATUS_SUCCESS) {
+                ctx->cusolver_grp[g] = nullptr;
+                return set_err(ctx, MH_ERR_CUDA, "cuSOLVER handle creation failed");
+            }
+            cusolverDnSetStream(ctx->cusolver_grp[g], ctx->grp_main[g]);
+        }
     int lwork = 0;
     cusolverStatus_t st = cusolverDnZgetrf_bufferSize(ctx->cusolver, (int)n, (int)n, (cuDoubleComplex*)D64,
                                                       (int)n, &lwork);
     if (st != CUSOLVER_STATUS_SUCCESS)
         return set_err(ctx, MH_ERR_CUDA, "cusolverDnZgetrf_bufferSize failed (%d)", (int)st);
-    auto* work = (cuDoubleComplex*)ws_get(ctx, WS_LWORK, sizeof(cuDoubleComplex) * (size_t)lwork);
+    auto* work = (cuDoubleComplex*)ws_get(ctx, WS_LWORK, sizeof(cuDoubleComplex) * (size_t)lwork * ns);
     if (!work) return MH_ERR_OOM;
+    if (ns > 1) {
+        MH_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream));
+        for (int g = 0; g + 1 < ns; ++g) MH_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->grp_main[g], ctx->ev_fork, 0));
+    }
     for (int z = 0; z < nb; ++z) {
+        const int q = z % ns;
+        cusolverDnHandle_t h = q ? ctx->cusolver_grp[q - 1] : ctx->cusolver;
         auto* Dz = (cuDoubleComplex*)(D64 + (int64_t)z * nn);
-        st = cusolverDnZgetrf(ctx->cusolver, (int)n, (int)n, Dz, (int)n, work, piv + z * n, infos + z);
+        st = cusolverDnZgetrf(h, (int)n, (int)n, Dz, (int)n, work + (size_t)lwork * q, piv + z * n, infos + z);
         if (st != CUSOLVER_STATUS_SUCCESS)
             return set_err(ctx, MH_ERR_CUDA, "cusolverDnZgetrf failed (%d)", (int)st);
-        st = cusolverDnZgetrs(ctx->cusolver, CUBLAS_OP_N, (int)n, nrhs, Dz, (int)n, piv + z * n,
+        st = cusolverDnZgetrs(h, CUBLAS_OP_N, (int)n, nrhs, Dz, (int)n, piv + z * n,
                               (cuDoubleComplex*)(X + (int64_t)z * nv), (int)n, infos + nb + z);
         if (st != CUSOLVER_STATUS_SUCCESS)
             return set_err(ctx, MH_ERR_CUDA, "cusolverDnZgetrs failed (%d)", (int)st);
+    }
+    for (int g = 0; g + 1 < ns; ++g) {
+        MH_CUDA_TRY(ctx, cudaEventRecord(ctx->grp_ev_join[g], ctx->grp_main[g]));
+        MH_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, ctx->grp_ev_join[g], 0));
     }
     phase_end(ctx, PH_FP64_LU);
     double2* PHI = X;

@@ -74,6 +74,9 @@ struct mh_ctx {
     cudaEvent_t ev_fork = nullptr;
     cublasHandle_t cublas = nullptr;
     cusolverDnHandle_t cusolver = nullptr;
+    // cuSOLVER handles on grp_main[g] (created on first use by the batched
+    // FP64 path, which factors one frequency per stream concurrently)
+    cusolverDnHandle_t cusolver_grp[kLuGroups - 1] = {};
     std::string err;
     int64_t launches = 0;
     int delh_method = MH_DELHOMMEAU_TABLE;
@@ -81,6 +84,9 @@ struct mh_ctx {
     // failure injection (tests): the triangular solves' flag waits wait on a
     // flag that nothing publishes, so they expire
     bool inject_wait_timeout = false;
+    // per-frequency Horner series of the tabulated Delhommeau term in FP32
+    // (mixed path only; off by default)
+    bool wave_series_fp32 = false;
     // LU schedules by matrix size (set by hand or by the autotuner); sizes
     // with no entry use the nearest entry in log n, else lu_default
     std::vector<std::pair<int64_t, LuSchedule>> lu_table;

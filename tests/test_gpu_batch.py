@@ -147,3 +147,36 @@ def test_frequency_batched_delhommeau_many_slices(mh, oracle, gpu):
     sel = [0, 127, 128, 149]
     Ao, Bo, _, _ = oracle.hydro_coefficients(mesh, om[sel], dofs, [0.0], gf_mask=DELH)
     assert _rel(A[..., sel], Ao) < 1e-9 and _rel(B[..., sel], Bo) < 1e-9
+
+
+@pytest.mark.parametrize("mask", [WU, DELH])
+@pytest.mark.parametrize("direct", [True, False])
+@pytest.mark.parametrize("nw", [3, 8])
+def test_batched_fp64_matches_oracle(mh, oracle, gpu, body, mask, direct, nw):
+    """MH_PRECISION_FP64_BATCHED (the Rankine part once, the frequency-batched
+    wave pass, cuSOLVER per frequency on several streams): the FP64 bound.
+    Eight frequencies take the frequency-batched Delhommeau pass, three the
+    per-frequency one."""
+    omegas = list(np.linspace(0.4, 2.2, nw))
+    betas = [0.0, 0.6]
+    dofs = list(body.dofs.values())
+    A, B, Fd, Fk, _ = mh.hydro_batch(body.mesh, omegas, dofs, betas, green_functions=_gfs(mh, mask),
+                                     direct=direct, precision="fp64_batched", ctx=gpu)
+    Ao, Bo, Fdo, Fko = oracle.hydro_coefficients(body.mesh, omegas, dofs, betas, gf_mask=mask, direct=direct)
+    assert _rel(A, Ao) < 1e-10 and _rel(B, Bo) < 1e-10 and _rel(Fd, Fdo) < 1e-10 and _rel(Fk, Fko) < 1e-12
+
+
+def test_wave_series_fp32_option(mh, oracle, gpu, body):
+    """The reduced-precision option of the mixed path: the Horner series in
+    FP32 (alpha contraction, logs, S and D in FP64); bounded against the
+    oracle at 1e-6, and off again afterwards."""
+    omegas = list(np.linspace(0.4, 2.2, 8))
+    dofs = list(body.dofs.values())
+    gpu.set_wave_series_fp32(True)
+    try:
+        A, B, _, _, _ = mh.hydro_batch(body.mesh, omegas, dofs, green_functions=_gfs(mh, DELH),
+                                       precision="mixed", tol=1e-12, ctx=gpu)
+    finally:
+        gpu.set_wave_series_fp32(False)
+    Ao, Bo, _, _ = oracle.hydro_coefficients(body.mesh, omegas, dofs, gf_mask=DELH)
+    assert _rel(A, Ao) < 1e-6 and _rel(B, Bo) < 1e-6
