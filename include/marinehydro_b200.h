@@ -146,12 +146,13 @@ int mh_ctx_get_lu_schedule(mh_ctx* ctx, int64_t n, int* groups, int* outer_panel
 int mh_lu_autotune(mh_ctx* ctx, int64_t n, int64_t nbatch, int ncand, const int* groups,
                    const int* outer_panels, const int* update_kernel, double* ms, int* best);
 
-/* Reduced-precision option of the mixed path (off by default): the
- * per-frequency Horner series in R of the tabulated Delhommeau term (the
- * frequency-batched wave pass) in FP32 instead of FP64; the alpha
- * contraction, the log terms, S and D stay FP64.  The FP64 paths never use
- * it.  No reference counterpart (the reference integrates in FP64). */
-int mh_ctx_set_wave_series_fp32(mh_ctx* ctx, int enable);
+/* Reduced-precision levels of the mixed path's frequency-batched
+ * tabulated-Delhommeau pass: 0 all FP64; 1 the per-frequency Horner series
+ * in R in FP32; 2 also the per-pair alpha contraction of the polar table in
+ * FP32.  The pair geometry, the log terms, the assembly of S and D and their
+ * Rankine parts stay FP64, and the FP64 paths never use these levels.  No
+ * reference counterpart (the reference integrates in FP64). */
+int mh_ctx_set_wave_series_fp32(mh_ctx* ctx, int level);
 
 /* Failure injection for tests (no reference counterpart): while enabled, the
  * flag waits of the tensor-core backend's triangular solves on this ctx wait

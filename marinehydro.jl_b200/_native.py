@@ -266,10 +266,16 @@ class Context:
             self.set_lu_schedule(n, *sched)
         return table
 
-    def set_wave_series_fp32(self, enable: bool):
-        """Mixed path: the per-frequency Horner series of the tabulated
-        Delhommeau term in FP32 (``mh_ctx_set_wave_series_fp32``; off by default)."""
-        check(lib().mh_ctx_set_wave_series_fp32(self._h, int(bool(enable))), self._h)
+    def wave_series_level(self) -> int:
+        """The level last set with set_wave_series_fp32 on this Context (0 unless set)."""
+        return getattr(self, "_wave_level", 0)
+
+    def set_wave_series_fp32(self, level: int):
+        """Reduced-precision level of the mixed path's frequency-batched
+        Delhommeau pass (``mh_ctx_set_wave_series_fp32``): 0 all FP64, 1 the
+        per-frequency Horner series in FP32, 2 also the alpha contraction."""
+        check(lib().mh_ctx_set_wave_series_fp32(self._h, int(level)), self._h)
+        self._wave_level = int(level)
 
     def set_wait_injection(self, enable: bool):
         """Failure injection (tests): the triangular solves' flag waits wait

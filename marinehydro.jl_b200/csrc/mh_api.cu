@@ -637,11 +637,12 @@ int mh_lu_autotune(mh_ctx* ctx, int64_t n, int64_t nbatch, int ncand, const int*
     return MH_OK;
 }
 
-int mh_ctx_set_wave_series_fp32(mh_ctx* ctx, int enable)
+int mh_ctx_set_wave_series_fp32(mh_ctx* ctx, int level)
 {
     int rc;
     if ((rc = check_ctx(ctx))) return rc;
-    ctx->wave_series_fp32 = enable != 0;
+    if (level < 0 || level > 2) return set_err(ctx, MH_ERR_ARG, "wave series precision level must be 0, 1 or 2");
+    ctx->wave_series_fp32 = level;
     return MH_OK;
 }
 

@@ -178,6 +178,15 @@ __device__ __forceinline__ void allw_emit(const AllwPair& q, int z, double k, co
 // launch; every context builds the same table, so concurrent copies write
 // identical bytes.
 __constant__ double c_polar_mono[4 * kTabPolarFn];
+// The same coefficients rounded to FP32 (the FP32 alpha contraction).
+__constant__ float c_polar_mono_f[4 * kTabPolarFn];
+
+template <typename CT>
+__device__ __forceinline__ CT polar_coef(int i);
+template <>
+__device__ __forceinline__ double polar_coef<double>(int i) { return c_polar_mono[i]; }
+template <>
+__device__ __forceinline__ float polar_coef<float>(int i) { return c_polar_mono_f[i]; }
 
 constexpr int kWT = 128;  // threads (rows) per CTA of k_wave_delh_allw
 constexpr int kAllwMaxFreqs = 128;  // frequencies per launch of k_wave_delh_allw
@@ -191,14 +200,20 @@ constexpr size_t wave_allw_smem()
 }
 constexpr size_t kWaveAllwSmem = wave_allw_smem<double>();
 
+__global__ void k_coef_to_f32(const double* __restrict__ a, float* __restrict__ b, int count)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < count) b[t] = (float)a[t];
+}
+
 __device__ __forceinline__ double hfma(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ float hfma(float a, float b, float c) { return fmaf(a, b, c); }
 
-// HT: the type of the per-frequency Horner series in R (double; float is the
-// reduced-precision option of the mixed path, mh_ctx_set_wave_series_fp32).
-// The alpha contraction, the log terms and everything after the series stay
-// in FP64.
-template <typename HT>
+// HT: the type of the per-frequency Horner series in R; CT: the type of the
+// alpha contraction (double, or float in the reduced-precision levels of the
+// mixed path, mh_ctx_set_wave_series_fp32).  The pair geometry, the log
+// terms and everything after the series stay in FP64.
+template <typename HT, typename CT>
 __global__ void __launch_bounds__(kWT, 3)
 k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const double* __restrict__ tab,
                  const double* __restrict__ kvec, int nb, const double* __restrict__ SR,
@@ -250,23 +265,23 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
         // functions' Clenshaw recurrences interleaved (four independent
         // dependency chains per row)
         if (polar_ok) {
-            const double v2 = 2.0 * v;
+            const CT vc = (CT)v, v2 = (CT)(2.0 * v);
 #pragma unroll 1
             for (int row = 0; row < kTabNU; ++row) {
-                const double* cr = c_polar_mono + row * kTabNV;
-                double b1[4] = {0.0, 0.0, 0.0, 0.0}, b2[4] = {0.0, 0.0, 0.0, 0.0};
+                const int cr = row * kTabNV;
+                CT b1[4] = {0, 0, 0, 0}, b2[4] = {0, 0, 0, 0};
 #pragma unroll
                 for (int col = kTabNV - 1; col >= 1; --col) {
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                        const double t = fma(v2, b1[q], cr[q * kTabPolarFn + col] - b2[q]);
+                        const CT t = hfma(v2, b1[q], polar_coef<CT>(cr + q * kTabPolarFn + col) - b2[q]);
                         b2[q] = b1[q];
                         b1[q] = t;
                     }
                 }
 #pragma unroll
                 for (int q = 0; q < 4; ++q)
-                    w[(q * kTabNU + row) * kWT + tid] = (HT)fma(v, b1[q], cr[q * kTabPolarFn] - b2[q]);
+                    w[(q * kTabNU + row) * kWT + tid] = (HT)hfma(vc, b1[q], polar_coef<CT>(cr + q * kTabPolarFn) - b2[q]);
             }
         }
         const AllwPair q{dx, dy, rho, inv_rho, p.area, sr, dr, nn3, o, wrt_first};
@@ -812,10 +827,20 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
         k_wave_batch<false><<<grid, kRows, 0, ctx->stream>>>(bt.m->geom, n, bt.direct, nullptr, d_k, SR,
                                                             DR, S64, D64, Dlo, nullptr);
     else if (wave == MH_GF_DELHOMMEAU && tab && nb >= kAllwMinFreqs) {
-        const bool f32 = ctx->wave_series_fp32;
-        auto* wk = f32 ? k_wave_delh_allw<float> : k_wave_delh_allw<double>;
-        const size_t wsm = f32 ? wave_allw_smem<float>() : wave_allw_smem<double>();
+        const int lvl = ctx->wave_series_fp32;
+        auto* wk = lvl == 2 ? k_wave_delh_allw<float, float>
+                 : lvl == 1 ? k_wave_delh_allw<float, double> : k_wave_delh_allw<double, double>;
+        const size_t wsm = lvl ? wave_allw_smem<float>() : wave_allw_smem<double>();
         MH_CUDA_TRY(ctx, cudaFuncSetAttribute(wk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
+        if (lvl == 2) {  // FP32 copy of the polar coefficients for the FP32 contraction
+            auto* cf = (float*)ws_get(ctx, WS_COEF32, sizeof(float) * 4 * kTabPolarFn);
+            if (!cf) return MH_ERR_OOM;
+            k_coef_to_f32<<<blocks(4 * kTabPolarFn, 256), 256, 0, ctx->stream>>>(tab + kTabMonoOff, cf,
+                                                                                 4 * kTabPolarFn);
+            ctx->launches += 1;
+            MH_CUDA_TRY(ctx, cudaMemcpyToSymbolAsync(c_polar_mono_f, cf, sizeof(float) * 4 * kTabPolarFn, 0,
+                                                     cudaMemcpyDeviceToDevice, ctx->stream));
+        }
         MH_CUDA_TRY(ctx, cudaMemcpyToSymbolAsync(c_polar_mono, tab + kTabMonoOff, sizeof(c_polar_mono), 0,
                                                  cudaMemcpyDeviceToDevice, ctx->stream));
         for (int z = 0; z < nb; z += kAllwMaxFreqs) {
@@ -934,7 +959,7 @@ int run_fp64_chunk(const Batch& bt, const double* d_omegas, const double* d_k, i
                                                             D64, Dlo, nullptr);
         ctx->launches += 1;
     } else if (wave == MH_GF_DELHOMMEAU && tab && nb >= kAllwMinFreqs) {
-        MH_CUDA_TRY(ctx, cudaFuncSetAttribute(k_wave_delh_allw<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        MH_CUDA_TRY(ctx, cudaFuncSetAttribute(k_wave_delh_allw<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)kWaveAllwSmem));
         MH_CUDA_TRY(ctx, cudaMemcpyToSymbolAsync(c_polar_mono, tab + kTabMonoOff, sizeof(c_polar_mono), 0,
                                                  cudaMemcpyDeviceToDevice, ctx->stream));
@@ -943,7 +968,7 @@ int run_fp64_chunk(const Batch& bt, const double* d_omegas, const double* d_k, i
             const int64_t off = (int64_t)z * nn;
             const dim3 g2(blocks(n, kWT), blocks(n, kCols));
             MH_CUDA_TRY(ctx, cudaMemsetAsync(d_fall, 0, sizeof(int), ctx->stream));
-            k_wave_delh_allw<double><<<g2, kWT, kWaveAllwSmem, ctx->stream>>>(bt.m->geom, n, bt.direct, tab, d_k + z, m, SR,
+            k_wave_delh_allw<double, double><<<g2, kWT, kWaveAllwSmem, ctx->stream>>>(bt.m->geom, n, bt.direct, tab, d_k + z, m, SR,
                                                                       DR, S64 + off, D64 + off, Dlo + off, nullptr,
                                                                       d_fall);
             k_wave_delh_allw_rest<<<g2, kWT, 0, ctx->stream>>>(d_fall, bt.m->geom, n, bt.direct, tab, d_k + z, m,

@@ -33,7 +33,7 @@ struct mh_mesh {
 // Workspace slots of a context; each is a grow-only device buffer.
 enum WsSlot : int {
     WS_S = 0, WS_D, WS_RHS, WS_PHI, WS_TMP, WS_PIV, WS_INFO, WS_LWORK,
-    WS_DOF, WS_OUT, WS_LO, WS_DINV, WS_TMP32, WS_MISC, WS_SR, WS_TMP32B, WS_PANEL, WS_FB,
+    WS_DOF, WS_OUT, WS_LO, WS_DINV, WS_TMP32, WS_MISC, WS_SR, WS_TMP32B, WS_PANEL, WS_FB, WS_COEF32,
     WS_ADJ, WS_WSD, WS_PART, WS_GBAR, WS_TAPE, WS_FLAGS, WS_NEAR, WS_NEARRES, WS_FALL, WS_REPACK, WS_NSLOTS
 };
 
@@ -84,9 +84,10 @@ struct mh_ctx {
     // failure injection (tests): the triangular solves' flag waits wait on a
     // flag that nothing publishes, so they expire
     bool inject_wait_timeout = false;
-    // per-frequency Horner series of the tabulated Delhommeau term in FP32
-    // (mixed path only; off by default)
-    bool wave_series_fp32 = false;
+    // reduced-precision levels of the frequency-batched Delhommeau pass
+    // (mixed path only): 0 all FP64, 1 the per-frequency Horner series in
+    // FP32, 2 also the alpha contraction in FP32
+    int wave_series_fp32 = 0;
     // LU schedules by matrix size (set by hand or by the autotuner); sizes
     // with no entry use the nearest entry in log n, else lu_default
     std::vector<std::pair<int64_t, LuSchedule>> lu_table;

@@ -166,17 +166,19 @@ def test_batched_fp64_matches_oracle(mh, oracle, gpu, body, mask, direct, nw):
     assert _rel(A, Ao) < 1e-10 and _rel(B, Bo) < 1e-10 and _rel(Fd, Fdo) < 1e-10 and _rel(Fk, Fko) < 1e-12
 
 
-def test_wave_series_fp32_option(mh, oracle, gpu, body):
-    """The reduced-precision option of the mixed path: the Horner series in
-    FP32 (alpha contraction, logs, S and D in FP64); bounded against the
-    oracle at 1e-6, and off again afterwards."""
+@pytest.mark.parametrize("level", [1, 2])
+def test_wave_series_fp32_levels(mh, oracle, gpu, body, level):
+    """The reduced-precision levels of the mixed path's wave pass (1: the
+    Horner series in FP32; 2: also the alpha contraction; logs, S and D in
+    FP64), bounded against the oracle at 1e-6, the metric's bound."""
     omegas = list(np.linspace(0.4, 2.2, 8))
     dofs = list(body.dofs.values())
-    gpu.set_wave_series_fp32(True)
+    old = gpu.wave_series_level()
+    gpu.set_wave_series_fp32(level)
     try:
         A, B, _, _, _ = mh.hydro_batch(body.mesh, omegas, dofs, green_functions=_gfs(mh, DELH),
                                        precision="mixed", tol=1e-12, ctx=gpu)
     finally:
-        gpu.set_wave_series_fp32(False)
+        gpu.set_wave_series_fp32(old)
     Ao, Bo, _, _ = oracle.hydro_coefficients(body.mesh, omegas, dofs, gf_mask=DELH)
     assert _rel(A, Ao) < 1e-6 and _rel(B, Bo) < 1e-6
