@@ -147,9 +147,11 @@ int mh_lu_autotune(mh_ctx* ctx, int64_t n, int64_t nbatch, int ncand, const int*
                    const int* outer_panels, const int* update_kernel, double* ms, int* best);
 
 /* Reduced-precision levels of the mixed path's frequency-batched
- * tabulated-Delhommeau pass: 0 all FP64; 1 the per-frequency Horner series
- * in R in FP32; 2 also the per-pair alpha contraction of the polar table in
- * FP32.  The pair geometry, the log terms, the assembly of S and D and their
+ * tabulated-Delhommeau pass: 0 all FP64; 1 (the default) the per-frequency
+ * Horner series in R in FP32; 2 also the per-pair alpha contraction of the
+ * polar table in FP32.  Measured at 2048 panels and 64 frequencies against
+ * the FP64 oracle's exact quadrature: A, B, F within 6e-10 (level 0), 2e-9
+ * (1), 7.5e-8 (2).  The pair geometry, the log terms, the assembly of S and D and their
  * Rankine parts stay FP64, and the FP64 paths never use these levels.  No
  * reference counterpart (the reference integrates in FP64). */
 int mh_ctx_set_wave_series_fp32(mh_ctx* ctx, int level);

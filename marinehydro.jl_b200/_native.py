@@ -267,13 +267,15 @@ class Context:
         return table
 
     def wave_series_level(self) -> int:
-        """The level last set with set_wave_series_fp32 on this Context (0 unless set)."""
-        return getattr(self, "_wave_level", 0)
+        """The level last set with set_wave_series_fp32 on this Context (the
+        library's default, 1, unless set)."""
+        return getattr(self, "_wave_level", 1)
 
     def set_wave_series_fp32(self, level: int):
         """Reduced-precision level of the mixed path's frequency-batched
-        Delhommeau pass (``mh_ctx_set_wave_series_fp32``): 0 all FP64, 1 the
-        per-frequency Horner series in FP32, 2 also the alpha contraction."""
+        Delhommeau pass (``mh_ctx_set_wave_series_fp32``): 0 all FP64, 1 (the
+        default) the per-frequency Horner series in FP32, 2 also the alpha
+        contraction."""
         check(lib().mh_ctx_set_wave_series_fp32(self._h, int(level)), self._h)
         self._wave_level = int(level)
 
