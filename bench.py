@@ -83,7 +83,9 @@ def config_dict(mesh, omegas, args):
             "green_functions": "Rankine+RankineReflected+ExactGuevelDelhommeau(table)",
             "formulation": "direct",
             "precision": ("mixed: FP16 tcgen05 trailing update / FP32 LU, FP64 refinement"
-                          if args.lu == "tcgen05" else "mixed: FP32 LU, FP64 refinement"),
+                          if args.lu == "tcgen05" else "mixed: FP32 LU, FP64 refinement")
+            + {0: "; wave series FP64", 1: "; wave-pass Horner series FP32, the rest of the assembly FP64",
+               2: "; wave-pass series and alpha contraction FP32, the rest of the assembly FP64"}[args.wave_level],
             "lu_backend": args.lu,
             "tol": args.tol, "solve": "one (mesh, omega) problem, 3 right-hand sides",
             "l2": "working set ~11 GB per step, larger than the 126 MB L2 (no flush needed)"}
@@ -492,6 +494,7 @@ def run_ours(args):
     mh = load_package()
     ctx = mh.Context(local)
     ctx.set_lu_backend(args.lu)
+    ctx.set_wave_series_fp32(args.wave_level)
     stream = torch.cuda.ExternalStream(ctx.stream())
     mesh, dofs, omegas, betas, gfs = workload(mh, args.res, args.n_omega)
     mask = mh.gf_mask(gfs)
@@ -629,9 +632,13 @@ WAVE_DRAM_BYTES_PER_PAIR_FREQ = 39.4
 # scaling into S and D (32).
 WAVE_FLOPS_PER_PAIR = 3980.0
 WAVE_FLOPS_PER_PAIR_FREQ = 163.0
-# Nominal FP64 peak of a B200 (148 SMs x 64 FP64 FMA per clock x 2 x 1.965 GHz);
-# no FP64 figure is measured on this pool.
+# Nominal FP64 and FP32 (CUDA-core) peaks of a B200: 148 SMs x 64 FP64 or
+# 128 FP32 FMA per clock x 2 x 1.965 GHz; neither is measured on this pool.
 FP64_PEAK_TFLOPS = 37.2
+FP32_PEAK_TFLOPS = 74.5
+# Of the per pair-frequency operations, the Horner series (112) runs in FP32
+# at the mixed path's default series level (1), the rest (51) in FP64.
+WAVE_FP32_FLOPS_PER_PAIR_FREQ = 112.0
 # DRAM bytes of the LU phase per matrix of 2048, from ncu captures of the
 # three LU kernels (the FP32 Schur complement re-read and re-written once per
 # 256-column outer step, the in-block updates, panels and diagonal blocks):
@@ -668,12 +675,18 @@ def roofline(per_phase, n, args):
         ms = per_phase["wave"]
         alg = nn * (16.0 + 40.0 * args.n_omega)
         flops = nn * (WAVE_FLOPS_PER_PAIR + WAVE_FLOPS_PER_PAIR_FREQ * args.n_omega)
-        out["wave"] = {"kernel": "k_wave_delh_allw", "bound": "fp64",
-                       "achieved": flops / (ms / 1e3) / 1e12, "peak": FP64_PEAK_TFLOPS,
-                       "unit": "TFLOP/s", "frac": flops / (ms / 1e3) / 1e12 / FP64_PEAK_TFLOPS,
-                       "peak_source": "nominal (148 SMs x 128 FP64 flop/clock x 1.965 GHz)",
-                       "flops_per_launch": flops, "flops_per_pair": WAVE_FLOPS_PER_PAIR,
+        f32 = nn * WAVE_FP32_FLOPS_PER_PAIR_FREQ * args.n_omega if args.wave_level >= 1 else 0.0
+        f64 = flops - f32
+        # issue-bound roofline: the time the FP64 and FP32 work take at their peaks
+        ideal_ms = (f64 / FP64_PEAK_TFLOPS + f32 / FP32_PEAK_TFLOPS) / 1e9
+        out["wave"] = {"kernel": "k_wave_delh_allw", "bound": "fp64+fp32 issue",
+                       "achieved": flops / (ms / 1e3) / 1e12, "unit": "TFLOP/s",
+                       "frac": ideal_ms / ms, "ideal_ms": ideal_ms,
+                       "peak": {"fp64": FP64_PEAK_TFLOPS, "fp32": FP32_PEAK_TFLOPS},
+                       "peak_source": "nominal (148 SMs x 64 FP64 / 128 FP32 FMA per clock x 2 x 1.965 GHz)",
+                       "flops_per_launch": {"fp64": f64, "fp32": f32}, "flops_per_pair": WAVE_FLOPS_PER_PAIR,
                        "flops_per_pair_freq": WAVE_FLOPS_PER_PAIR_FREQ, "ms_per_launch": ms,
+                       "series_level": args.wave_level,
                        "hbm": {"achieved": alg / (ms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
                                "frac": alg / (ms / 1e3) / 1e9 / hbm, "algorithmic_bytes_per_launch": alg,
                                "traffic": WAVE_DRAM_BYTES_PER_PAIR_FREQ * nn * args.n_omega}}
@@ -846,6 +859,9 @@ def main():
     ap.add_argument("--no-grads", action="store_true")
     ap.add_argument("--no-two-body", action="store_true")
     ap.add_argument("--no-design", action="store_true")
+    # precision level of the wave pass's series (0 FP64, 1 the default FP32 Horner series, 2 also the
+    # FP32 alpha contraction)
+    ap.add_argument("--wave-level", type=int, default=1, choices=[0, 1, 2])
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -62,3 +62,14 @@ def rel_err(a, b):
     a = np.asarray(a)
     b = np.asarray(b)
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+@pytest.fixture
+def series_fp64(gpu):
+    """The mixed path's wave pass with its Horner series in FP64 (level 0)
+    for the duration of a test: the tests that check the frequency-batched
+    kernels against the one-frequency FP64 path to 1e-8 or tighter run the
+    kernels' FP64 form; the default FP32 series (level 1) has its own bounds."""
+    gpu.set_wave_series_fp32(0)
+    yield gpu
+    gpu.set_wave_series_fp32(1)

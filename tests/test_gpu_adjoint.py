@@ -209,7 +209,7 @@ def test_rrule_pullback(mh, gpu, setup):
 
 
 @pytest.mark.parametrize("direct", [True, False])
-def test_vjp_frequency_batched_delhommeau(mh, gpu, direct):
+def test_vjp_frequency_batched_delhommeau(mh, gpu, direct, series_fp64):
     """Chunks of >= 4 frequencies take the frequency-batched Delhommeau
     adjoint (alpha contraction once per pair); over [0.3, 4.0] rad/s pairs
     leave the polar patch, so the per-point path runs too.  Checked against
@@ -234,7 +234,7 @@ def test_vjp_frequency_batched_delhommeau(mh, gpu, direct):
         assert np.max(np.abs(x - y)) <= 1e-8 * np.max(np.abs(y)), f
 
 
-def test_vjp_frequency_batched_many_slices(mh, gpu):
+def test_vjp_frequency_batched_many_slices(mh, gpu, series_fp64):
     """A chunk of 150 frequencies: the forward writes the (G, G_r) tape in
     slices of 128 frequencies, which the adjoint reads back at the same
     offsets; mixed against FP64."""
@@ -256,7 +256,7 @@ def test_vjp_frequency_batched_many_slices(mh, gpu):
     (["Surge", "Heave", "Pitch"], [0.2]),
     (["Surge", "Sway", "Heave", "Roll", "Pitch", "Yaw"], [0.2]),
 ])
-def test_vjp_tape_right_hand_side_counts(mh, gpu, names, betas):
+def test_vjp_tape_right_hand_side_counts(mh, gpu, names, betas, series_fp64):
     """The tape adjoint loads the row vectors of all right-hand sides of a
     frequency together for 1 to 4 of them and one at a time beyond (here 7,
     six rigid modes and a wave); the column vectors pass through shared

@@ -113,7 +113,7 @@ def test_batch_argument_errors(mh, gpu, body):
 
 
 @pytest.mark.parametrize("direct", [True, False])
-def test_frequency_batched_delhommeau(mh, oracle, gpu, direct):
+def test_frequency_batched_delhommeau(mh, oracle, gpu, direct, series_fp64):
     """Chunks of >= 6 frequencies take the frequency-batched Delhommeau pass
     (alpha contraction once per pair); across [0.3, 4.0] rad/s pairs move from
     the polar patch into the Cartesian cells, so both branches run."""
@@ -131,7 +131,7 @@ def test_frequency_batched_delhommeau(mh, oracle, gpu, direct):
     assert _rel(A, A64) < 1e-10 and _rel(B, B64) < 1e-10
 
 
-def test_frequency_batched_delhommeau_many_slices(mh, oracle, gpu):
+def test_frequency_batched_delhommeau_many_slices(mh, oracle, gpu, series_fp64):
     """More frequencies in one chunk than one launch of the batched pass
     takes (128): the chunk runs in frequency slices whose outputs and tape
     land at their own offsets."""

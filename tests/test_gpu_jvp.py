@@ -97,7 +97,7 @@ def test_jvp_matches_finite_differences(mh, gpu, setup, mask, direct):
 
 
 @pytest.mark.parametrize("direct", [True, False])
-def test_jvp_mixed_and_batched(mh, gpu, direct):
+def test_jvp_mixed_and_batched(mh, gpu, direct, series_fp64):
     """Mixed (frequency-batched Delhommeau tangent for >= 4 frequencies) vs
     FP64 one frequency per call."""
     mesh = mh.mesh_hemisphere(1.3, (0, 0, 0), (10, 14))

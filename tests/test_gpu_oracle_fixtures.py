@@ -19,8 +19,9 @@ where the metric is quoted, not only point-wise.
 
 Tolerances, relative to the largest entry of each output: FP64 path 1e-9;
 mixed path 1e-6 at refinement tolerance 1e-8 (the benchmark's setting and
-the metric's bound) and 1e-9 at 1e-12; matrix entries 1e-9 of the largest
-sampled entry; gradients 1e-5.
+the metric's bound), 1e-8 at 1e-12 with the default FP32 Horner series of
+the wave pass and 1e-9 with its FP64 form; matrix entries 1e-9 of the
+largest sampled entry; gradients 1e-5.
 """
 from __future__ import annotations
 
@@ -78,10 +79,21 @@ CASES = {
 
 
 @pytest.mark.parametrize("name", list(CASES))
-@pytest.mark.parametrize("precision,tol,bound", [("fp64", 1e-12, 1e-9), ("mixed", 1e-8, 1e-6),
-                                                 ("mixed", 1e-12, 1e-9)])
-def test_coefficients_match_oracle_at_size(mh, gpu, name, precision, tol, bound):
+@pytest.mark.parametrize("precision,tol,bound,level", [("fp64", 1e-12, 1e-9, 1), ("mixed", 1e-8, 1e-6, 1),
+                                                       ("mixed", 1e-12, 1e-8, 1), ("mixed", 1e-12, 1e-9, 0),
+                                                       ("mixed", 1e-8, 1e-6, 2)])
+def test_coefficients_match_oracle_at_size(mh, gpu, name, precision, tol, bound, level):
+    """level: the precision level of the mixed path's wave series (0 FP64,
+    1 the default FP32 Horner series, 2 also the FP32 alpha contraction)."""
     fx = _load(name)
+    gpu.set_wave_series_fp32(level)
+    try:
+        _check_at_size(mh, gpu, name, fx, precision, tol, bound)
+    finally:
+        gpu.set_wave_series_fp32(1)
+
+
+def _check_at_size(mh, gpu, name, fx, precision, tol, bound):
     mesh, dofs = CASES[name](mh)
     assert np.allclose(_fingerprint(mesh), fx["fingerprint"], rtol=1e-13, atol=1e-10)
     mask = int(fx["gf_mask"])
