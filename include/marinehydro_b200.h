@@ -54,9 +54,11 @@ extern "C" {
 #define MH_PRECISION_FP64   0  /* FP64 assembly + FP64 LU (cuSOLVER zgetrf/zgetrs) */
 #define MH_PRECISION_MIXED  1  /* FP64-accurate matrices, low-precision LU, FP64 iterative refinement */
 /* FP64 everywhere with the batch structure of the mixed path (mh_hydro_batch
- * only): the frequency-independent Rankine part once, the frequency-batched
- * wave pass, then cuSOLVER zgetrf/zgetrs per frequency on the FP64 matrices.
- * The plain-FP64 denominator of the mixed path's speed-up. */
+ * and mh_hydro_batch_vjp): the frequency-independent Rankine part once, the
+ * frequency-batched wave pass, then cuSOLVER zgetrf/zgetrs per frequency on
+ * the FP64 matrices, frequencies spread over four streams (the adjoint solves
+ * with the same pivoted factors, conjugate transposed).  The plain-FP64
+ * denominator of the mixed path's speed-up. */
 #define MH_PRECISION_FP64_BATCHED 2
 
 /* evaluation of the ExactGuevelDelhommeau wave term */
@@ -280,8 +282,8 @@ int mh_diffraction_force(mh_ctx* ctx, const mh_mesh* mesh, double omega,
  *   added_mass, damping      n_dof x n_dof x n_omega  ([influenced, radiating, omega])
  *   diffraction, froude_krylov  complex n_dof x n_omega x n_beta ([dof, omega, beta])
  *   (any output may be NULL)
- *   precision     MH_PRECISION_FP64, MH_PRECISION_MIXED or (mh_hydro_batch
- *                 only) MH_PRECISION_FP64_BATCHED
+ *   precision     MH_PRECISION_FP64, MH_PRECISION_MIXED or (mh_hydro_batch,
+ *                 mh_hydro_batch_vjp) MH_PRECISION_FP64_BATCHED
  *   tol, max_iter mixed only: refinement stops when max|b - A x|/max|b| <= tol
  *                 for every right-hand side; problems that do not get there in
  *                 max_iter sweeps are re-solved in FP64 (info->n_fallback).

@@ -1638,6 +1638,43 @@ int adjoint_mixed_chunk(const Batch& bt, Vjp& vj, const double* d_omegas, const 
     return adjoint_tail(bt, vj, d_omegas, d_k, nb, z0, tab, PB, X, LAM, X, LAM);
 }
 
+// Adjoint of one chunk of the batched FP64 path: the forward state of
+// run_fp64_chunk is in the workspace; D^H lam = rhs with its pivoted FP64
+// factors (cuSOLVER zgetrs, conjugate transpose), then the same tail as the
+// mixed adjoint.
+int adjoint_fp64_batched_chunk(const Batch& bt, Vjp& vj, const double* d_omegas, const double* d_k, int nb,
+                               int z0)
+{
+    mh_ctx* ctx = bt.ctx;
+    const int64_t n = bt.n;
+    const int nrhs = bt.nrhs;
+    const int64_t nv = n * nrhs, cnt = nv * nb;
+    auto* S64 = (double2*)ctx->ws[WS_S];
+    auto* BC = (double2*)ctx->ws[WS_RHS];
+    auto* X = (double2*)ctx->ws[WS_PHI];
+    auto* PHIi = (double2*)ctx->ws[WS_TMP];  // phi = S sigma (indirect)
+    auto* adj = (double2*)ws_get(ctx, WS_ADJ, sizeof(double2) * cnt * 5);
+    if (!adj) return MH_ERR_OOM;
+    double2* PB = adj;
+    double2* LAM = adj + cnt;
+    double2* BB = adj + 2 * cnt;
+    int rc;
+    const double* tab = delh_table_for(ctx, bt.mask, &rc);
+    if (rc) return rc;
+    if ((rc = seed_forces(bt, vj, d_omegas, nb, z0, bt.direct ? X : PHIi, PB))) return rc;
+    phase_begin(ctx, PH_ADJ_SOLVE);
+    if (bt.direct) {
+        MH_CUDA_TRY(ctx, cudaMemcpyAsync(LAM, PB, sizeof(double2) * cnt, cudaMemcpyDeviceToDevice, ctx->stream));
+    } else {
+        MH_CUDA_TRY(ctx, launch_gemv(ctx, true, S64, n, nb, PB, nullptr, LAM, nrhs, 1.0, 0.0));
+    }
+    if ((rc = fp64_batched_getrs(ctx, true, n, nb, nrhs, LAM))) return rc;
+    if (bt.direct) MH_CUDA_TRY(ctx, launch_gemv(ctx, true, S64, n, nb, LAM, nullptr, BB, nrhs, 1.0, 0.0));
+    phase_end(ctx, PH_ADJ_SOLVE);
+    if (bt.direct) return adjoint_tail(bt, vj, d_omegas, d_k, nb, z0, tab, LAM, BC, LAM, X, BB);
+    return adjoint_tail(bt, vj, d_omegas, d_k, nb, z0, tab, PB, X, LAM, X, LAM);
+}
+
 // FP64 forward + adjoint of one frequency (pivoted cuSOLVER LU, kept for
 // the conjugate-transposed solve).
 int fp64_vjp_one(const Batch& bt, Vjp& vj, const double* d_omega, const double* d_k, double k, int z,
@@ -1815,6 +1852,12 @@ int hydro_batch_vjp(mh_ctx* ctx, const mh_mesh* m, int64_t nomega, const double*
             fb.lu = nullptr;
             fb.piv = nullptr;
             fb.used.assign(nb, 0);
+            if (precision == MH_PRECISION_FP64_BATCHED) {
+                rc = run_fp64_chunk(bt, d_om + z0, d_k + z0, nb, SR, DR, d_F + z0 * nrhs * ndof,
+                                    d_FK + z0 * nbeta * ndof);
+                if (rc == MH_OK) rc = adjoint_fp64_batched_chunk(bt, vj, d_om + z0, d_k + z0, nb, (int)z0);
+                continue;
+            }
             rc = run_mixed_chunk(bt, d_om + z0, d_k + z0, nb, SR, DR, tol, max_iter, d_F + z0 * nrhs * ndof,
                                  d_FK + z0 * nbeta * ndof, &local, &fb);
             if (rc == MH_OK)

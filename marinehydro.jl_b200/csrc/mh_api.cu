@@ -912,9 +912,12 @@ int mh_hydro_batch_vjp(mh_ctx* ctx, const mh_mesh* mesh, int64_t n_omega, const 
                        double* d_dofs, mh_batch_info* info)
 {
     int rc;
+    const bool batched64 = precision == MH_PRECISION_FP64_BATCHED;
     if ((rc = check_batch(ctx, mesh, n_omega, omegas, n_dof, dofs, n_beta, betas, rho, g, gf_mask,
-                          precision, tol, max_iter)))
+                          batched64 ? MH_PRECISION_FP64 : precision, tol, max_iter)))
         return rc;
+    if (batched64 && (gf_mask & MH_GF_WU) && (gf_mask & MH_GF_DELHOMMEAU))
+        return set_err(ctx, MH_ERR_ARG, "the batched FP64 path takes one wave term (GFWu or Delhommeau)");
     const int64_t nrad = n_dof * n_dof * n_omega, ndif = 2 * n_dof * n_omega * n_beta;
     if ((bar_added_mass && !finite_array(bar_added_mass, nrad)) ||
         (bar_damping && !finite_array(bar_damping, nrad)) ||

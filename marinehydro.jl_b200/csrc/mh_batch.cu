@@ -968,17 +968,17 @@ int run_fp64_chunk(const Batch& bt, const double* d_omegas, const double* d_k, i
             const int64_t off = (int64_t)z * nn;
             const dim3 g2(blocks(n, kWT), blocks(n, kCols));
             MH_CUDA_TRY(ctx, cudaMemsetAsync(d_fall, 0, sizeof(int), ctx->stream));
-            k_wave_delh_allw<double, double><<<g2, kWT, kWaveAllwSmem, ctx->stream>>>(bt.m->geom, n, bt.direct, tab, d_k + z, m, SR,
-                                                                      DR, S64 + off, D64 + off, Dlo + off, nullptr,
-                                                                      d_fall);
+            double2* tp = bt.tape ? bt.tape + 2 * off : nullptr;
+            k_wave_delh_allw<double, double><<<g2, kWT, kWaveAllwSmem, ctx->stream>>>(
+                bt.m->geom, n, bt.direct, tab, d_k + z, m, SR, DR, S64 + off, D64 + off, Dlo + off, tp, d_fall);
             k_wave_delh_allw_rest<<<g2, kWT, 0, ctx->stream>>>(d_fall, bt.m->geom, n, bt.direct, tab, d_k + z, m,
-                                                              SR, DR, S64 + off, D64 + off, Dlo + off, nullptr);
+                                                              SR, DR, S64 + off, D64 + off, Dlo + off, tp);
             ctx->launches += 2;
         }
     } else if (wave == MH_GF_DELHOMMEAU) {
         dim3 grid(blocks(n, kRows), blocks(n, kCols), (unsigned)nb);
         k_wave_batch<true><<<grid, kRows, 0, ctx->stream>>>(bt.m->geom, n, bt.direct, tab, d_k, SR, DR, S64, D64,
-                                                           Dlo, nullptr);
+                                                           Dlo, bt.tape);
         ctx->launches += 1;
     } else if (wave == 0) {
         k_no_wave_batch<<<dim3(blocks(nn, 256), nb), 256, 0, ctx->stream>>>(nn, SR, DR, S64, D64, Dlo);
@@ -1047,6 +1047,37 @@ int run_fp64_chunk(const Batch& bt, const double* d_omegas, const double* d_k, i
     MH_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     for (int z = 0; z < nb; ++z)
         if (h[z] > 0) return set_err(ctx, MH_ERR_SINGULAR, "frequency %d: zero pivot at column %d", z, h[z]);
+    return MH_OK;
+}
+
+// op(D_z)^-1 X_z for nb frequencies with the pivoted FP64 factors that
+// run_fp64_chunk left in place (D64 in WS_D, pivots in WS_PIV), one frequency
+// per stream as in the forward solve.
+int fp64_batched_getrs(mh_ctx* ctx, bool conj_trans, int64_t n, int nb, int nrhs, double2* X)
+{
+    const int64_t nn = n * n, nv = n * nrhs;
+    auto* D64 = (double2*)ctx->ws[WS_D];
+    auto* piv = (int*)ctx->ws[WS_PIV];
+    if (!D64 || !piv) return set_err(ctx, MH_ERR_ARG, "no batched FP64 factors to solve with");
+    int* infos = piv + n * nb;
+    const int ns = std::min(kLuGroups, nb);
+    if (ns > 1) {
+        MH_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_fork, ctx->stream));
+        for (int g = 0; g + 1 < ns; ++g) MH_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->grp_main[g], ctx->ev_fork, 0));
+    }
+    for (int z = 0; z < nb; ++z) {
+        const int q = z % ns;
+        cusolverDnHandle_t h = q ? ctx->cusolver_grp[q - 1] : ctx->cusolver;
+        const cusolverStatus_t st = cusolverDnZgetrs(h, conj_trans ? CUBLAS_OP_C : CUBLAS_OP_N, (int)n, nrhs,
+                                                     (const cuDoubleComplex*)(D64 + (int64_t)z * nn), (int)n,
+                                                     piv + z * n, (cuDoubleComplex*)(X + (int64_t)z * nv), (int)n,
+                                                     infos + nb + z);
+        if (st != CUSOLVER_STATUS_SUCCESS) return set_err(ctx, MH_ERR_CUDA, "cusolverDnZgetrs failed (%d)", (int)st);
+    }
+    for (int g = 0; g + 1 < ns; ++g) {
+        MH_CUDA_TRY(ctx, cudaEventRecord(ctx->grp_ev_join[g], ctx->grp_main[g]));
+        MH_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, ctx->grp_ev_join[g], 0));
+    }
     return MH_OK;
 }
 

@@ -289,6 +289,14 @@ int rankine_real(const Batch& bt, double* SR, double* DR);
 int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, int nb,
                     const double* SR, const double* DR, double tol, int max_iter, double2* d_F,
                     double2* d_FK, mh_batch_info* info, FallbackStore* fb);
+// One chunk of the batched FP64 path (MH_PRECISION_FP64_BATCHED): leaves S
+// (WS_S), the pivoted FP64 factors of D (WS_D, pivots in WS_PIV), the
+// boundary conditions (WS_RHS), the solution (WS_PHI; phi = S sigma in WS_TMP
+// when indirect) in place; writes the wave tape when bt.tape is set.
+int run_fp64_chunk(const Batch& bt, const double* d_omegas, const double* d_k, int nb, const double* SR,
+                   const double* DR, double2* d_F, double2* d_FK);
+// X_z = op(D_z)^-1 X_z with the factors run_fp64_chunk left (op = identity or ^H).
+int fp64_batched_getrs(mh_ctx* ctx, bool conj_trans, int64_t n, int nb, int nrhs, double2* X);
 cudaError_t launch_bc_batch(const Batch& bt, const double* d_omegas, int nb, double2* BC);
 cudaError_t launch_forces_batch(const Batch& bt, const double* d_omegas, int nb, const double2* PHI,
                                 double2* d_F, double2* d_FK);
