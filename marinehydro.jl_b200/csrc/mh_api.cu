@@ -330,6 +330,12 @@ int mh_ctx_create(int device, mh_ctx** out)
             (e = cudaEventCreateWithFlags(&ctx->grp_ev_join[g], cudaEventDisableTiming)) != cudaSuccess)
             break;
     }
+    for (int g = 0; g < kLuGroups && e == cudaSuccess; ++g) {
+        if ((e = cudaStreamCreateWithPriority(&ctx->lu_strip[g], cudaStreamNonBlocking, greatest)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&ctx->lu_ev_strip_go[g], cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&ctx->lu_ev_strip_done[g], cudaEventDisableTiming)) != cudaSuccess)
+            break;
+    }
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         mh_ctx_destroy(ctx);
@@ -356,6 +362,8 @@ int mh_ctx_destroy(mh_ctx* ctx)
         if (ctx->grp_main[g]) cudaStreamSynchronize(ctx->grp_main[g]);
         if (ctx->grp_side[g]) cudaStreamSynchronize(ctx->grp_side[g]);
     }
+    for (int g = 0; g < kLuGroups; ++g)
+        if (ctx->lu_strip[g]) cudaStreamSynchronize(ctx->lu_strip[g]);
     for (int s = 0; s < WS_NSLOTS; ++s)
         if (ctx->ws[s]) cudaFree(ctx->ws[s]);
     if (ctx->delh_table) cudaFree(ctx->delh_table);
@@ -376,6 +384,11 @@ int mh_ctx_destroy(mh_ctx* ctx)
         if (ctx->grp_ev_join[g]) cudaEventDestroy(ctx->grp_ev_join[g]);
         if (ctx->grp_side[g]) cudaStreamDestroy(ctx->grp_side[g]);
         if (ctx->grp_main[g]) cudaStreamDestroy(ctx->grp_main[g]);
+    }
+    for (int g = 0; g < kLuGroups; ++g) {
+        if (ctx->lu_ev_strip_go[g]) cudaEventDestroy(ctx->lu_ev_strip_go[g]);
+        if (ctx->lu_ev_strip_done[g]) cudaEventDestroy(ctx->lu_ev_strip_done[g]);
+        if (ctx->lu_strip[g]) cudaStreamDestroy(ctx->lu_strip[g]);
     }
     if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);

@@ -55,6 +55,12 @@ constexpr int kLuGroups = 4;
 // pairs (1 .. kLuGroups), 64-column panels per outer step (even, 2 .. 8) and
 // the trailing-update kernel (0: C through shared memory after the MMAs,
 // 1: C staged in tensor memory before them).
+// The streams and events one group of the tensor-core LU runs on.
+struct LuStreams {
+    cudaStream_t main, side, strip;
+    cudaEvent_t ev_side, ev_panel, ev_strip_go, ev_strip_done;
+};
+
 struct LuSchedule {
     int groups = 2;
     int outer = 4;
@@ -72,6 +78,10 @@ struct mh_ctx {
     cudaStream_t grp_main[kLuGroups - 1] = {}, grp_side[kLuGroups - 1] = {};
     cudaEvent_t grp_ev_panel[kLuGroups - 1] = {}, grp_ev_side[kLuGroups - 1] = {}, grp_ev_join[kLuGroups - 1] = {};
     cudaEvent_t ev_fork = nullptr;
+    // per LU group: the stream of the in-block strip updates (high priority,
+    // concurrent with the next diagonal-block factorisation) and its events
+    cudaStream_t lu_strip[kLuGroups] = {};
+    cudaEvent_t lu_ev_strip_go[kLuGroups] = {}, lu_ev_strip_done[kLuGroups] = {};
     cublasHandle_t cublas = nullptr;
     cusolverDnHandle_t cusolver = nullptr;
     // cuSOLVER handles on grp_main[g] (created on first use by the batched

@@ -412,16 +412,18 @@ __device__ __forceinline__ bool epilogue_bulk(float2* M, int64_t n, int64_t r0, 
 }
 
 // A22 -= sum_p L21_p U12_p for one 128 x 128 complex tile (absolute tiles
-// ti, tj); the operands are the packed panels of k_lu_trsm_tc (npair <= 4
+// ti, tj); the operands are the packed panels of k_lu_trsm_tc (npair <= 8
 // panel pairs, K = 64 complex each), fetched by cp.async.bulk into shared
 // memory one pair at a time and accumulated in tensor memory.  Only rows and
 // columns >= lo are written.  Tiles, relative to t0 (ntile of them per side):
-// mode 1: the first w tile rows and tile columns (an L of width w; grid
-// w (2 ntile - w), the part the next panels depend on); mode 2: the tiles
-// past them (grid (ntile - w)^2).
+// mode 1: the first w tile rows and tile columns (an L of width w; w (2 ntile
+// - w) tiles, the part the next panels depend on; tile x of the L is
+// blockIdx.x + xoff, tile 0 being the diagonal tile (t0, t0)); mode 2: the
+// tiles past them (grid (ntile - w)^2).
 __global__ void __launch_bounds__(128, 2)
 k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int t0, int ntile, int mode, int w,
-               PanelPairs pp, int npair, int64_t pstride, int64_t lo, int* __restrict__ bad)
+               PanelPairs pp, int npair, int64_t pstride, int64_t lo, int* __restrict__ bad,
+               int xoff)
 {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
     __shared__ uint64_t mbar[2 + kCBufs];
@@ -432,7 +434,7 @@ k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int t0, int n
     float2* M = Ab + (int64_t)b * stride;
     int ti, tj;
     if (mode == 1) {
-        const int x = (int)blockIdx.x;
+        const int x = (int)blockIdx.x + xoff;
         if (x < w * ntile) {
             ti = t0 + x / ntile;
             tj = t0 + x % ntile;
@@ -560,7 +562,8 @@ k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int t0, int n
 // following the MMAs.  Grid, tiles and operands as k_lu_update_tc.
 __global__ void __launch_bounds__(128, 2)
 k_lu_update_tc_acc(float2* __restrict__ Ab, int64_t n, int64_t stride, int t0, int ntile, int mode, int w,
-                   PanelPairs pp, int npair, int64_t pstride, int64_t lo, int* __restrict__ bad)
+                   PanelPairs pp, int npair, int64_t pstride, int64_t lo, int* __restrict__ bad,
+               int xoff)
 {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
     __shared__ uint64_t mbar[2];
@@ -571,7 +574,7 @@ k_lu_update_tc_acc(float2* __restrict__ Ab, int64_t n, int64_t stride, int t0, i
     float2* M = Ab + (int64_t)b * stride;
     int ti, tj;
     if (mode == 1) {
-        const int x = (int)blockIdx.x;
+        const int x = (int)blockIdx.x + xoff;
         if (x < w * ntile) {
             ti = t0 + x / ntile;
             tj = t0 + x % ntile;
@@ -1530,11 +1533,11 @@ namespace {
 // The schedule above for nbatch matrices on one (main, side) stream pair;
 // panels: lu_panel_bytes_tc(n) * nbatch bytes for these matrices.
 cudaError_t lu_tc_group(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int nbatch, float2* Dinv,
-                        unsigned char* panels, int* bad, cudaStream_t main_s, cudaStream_t side_s,
-                        cudaEvent_t ev_side, cudaEvent_t ev_panel, const int op, const int update)
+                        unsigned char* panels, int* bad, const LuStreams& st, const int op, const int update)
 {
     auto* upd = update ? k_lu_update_tc_acc : k_lu_update_tc;
     cudaError_t e;
+    cudaStream_t main_s = st.main, side_s = st.side, strip_s = st.strip;
     const int64_t dstride = lu_dinv_stride_tc(n);
     const int64_t pstride = (int64_t)((n + TC_TM - 1) / TC_TM) * (kPanelL + kPanelU);  // one buffer, per matrix
     const int64_t bstride = ((n + TC_NB - 1) / TC_NB) * 2 * (int64_t)kTrsmBImage;       // B images, per matrix
@@ -1542,7 +1545,29 @@ cudaError_t lu_tc_group(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int n
     const int ntiles = (int)((n + TC_TM - 1) / TC_TM);
     const unsigned nbz = (unsigned)nbatch;
     const int kW = op / 2;  // tiles per outer step
-    if ((e = cudaEventRecord(ev_side, side_s)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(st.ev_side, side_s)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(st.ev_strip_done, strip_s)) != cudaSuccess) return e;
+    // An L of the trailing matrix (mode 1 at tile t0, width w) updated with
+    // the panel pairs q: its diagonal tile (t0, t0), which holds the next
+    // diagonal block, on the main stream; the rest on the strip stream,
+    // concurrently with the next diagonal-block factorisation; the next panel
+    // solve waits for it (strip_join).
+    auto strip = [&](int t0, int nt, int w, const PanelPairs& q, int np, int64_t lo) -> cudaError_t {
+        cudaError_t e2;
+        upd<<<dim3(1, 1, nbz), 128, kTcSmemBytes, main_s>>>(A, n, stride, t0, nt, 1, w, q, np, pstride, lo, bad, 0);
+        ctx->launches += 1;
+        const int rest = w * (2 * nt - w) - 1;
+        if (rest > 0) {
+            if ((e2 = cudaEventRecord(st.ev_strip_go, main_s)) != cudaSuccess) return e2;
+            if ((e2 = cudaStreamWaitEvent(strip_s, st.ev_strip_go, 0)) != cudaSuccess) return e2;
+            upd<<<dim3(rest, 1, nbz), 128, kTcSmemBytes, strip_s>>>(A, n, stride, t0, nt, 1, w, q, np, pstride, lo,
+                                                                    bad, 1);
+            ctx->launches += 1;
+            if ((e2 = cudaEventRecord(st.ev_strip_done, strip_s)) != cudaSuccess) return e2;
+        }
+        return cudaGetLastError();
+    };
+    auto strip_join = [&]() { return cudaStreamWaitEvent(main_s, st.ev_strip_done, 0); };
     k_lu_diag64<<<nbatch, kDiag64Threads, kDiag64Smem, main_s>>>(A, n, stride, 0, Dinv, dstride, bad, bimg,
                                                                    bstride);
     ctx->launches += 1;
@@ -1562,6 +1587,8 @@ cudaError_t lu_tc_group(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int n
                 break;
             }
             const int t0 = (int)((k + TC_NB) / TC_TM), nt = ntiles - t0;
+            // the panel's column and row blocks carry every earlier update
+            if ((e = strip_join()) != cudaSuccess) return e;
             k_lu_trsm_tc<<<dim3(2 * nt, nbz), 128, kSmemA + kSmemA, main_s>>>(
                 A, n, stride, k, bimg, bstride, (unsigned char*)pp.L[s], (unsigned char*)pp.U[s], pstride, nt, bad);
             ctx->launches += 1;
@@ -1570,32 +1597,31 @@ cudaError_t lu_tc_group(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int n
                 one.L[0] = pp.L[s];
                 one.U[0] = pp.U[s];
                 const int w = std::min(T0 + kW - t0, nt);
-                upd<<<dim3(w * (2 * nt - w), 1, nbz), 128, kTcSmemBytes, main_s>>>(
-                    A, n, stride, t0, nt, 1, w, one, 1, pstride, k + TC_NB, bad);
+                if ((e = strip(t0, nt, w, one, 1, k + TC_NB)) != cudaSuccess) return e;
                 k_lu_diag64<<<nbatch, kDiag64Threads, kDiag64Smem, main_s>>>(A, n, stride, k + TC_NB, Dinv, dstride,
                                                                            bad, bimg, bstride);
-                ctx->launches += 2;
+                ctx->launches += 1;
             }
         }
         if (done) break;
-        // trailing tiles >= T0 + kW with all four panel pairs
+        // trailing tiles >= T0 + kW with all the outer step's panel pairs
         const int64_t lo = K0 + (int64_t)op * TC_NB;
         const int t0 = T0 + kW, nt = ntiles - t0;
         if (nt <= 0) break;
-        // the previous interior update is done before this trailing update
-        if ((e = cudaStreamWaitEvent(main_s, ev_side, 0)) != cudaSuccess) return e;
-        if ((e = cudaEventRecord(ev_panel, main_s)) != cudaSuccess) return e;
-        if ((e = cudaStreamWaitEvent(side_s, ev_panel, 0)) != cudaSuccess) return e;
+        // the previous interior update and the in-block strips are done
+        // before this trailing update
+        if ((e = cudaStreamWaitEvent(main_s, st.ev_side, 0)) != cudaSuccess) return e;
+        if ((e = strip_join()) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(st.ev_panel, main_s)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(side_s, st.ev_panel, 0)) != cudaSuccess) return e;
         const int w = std::min(kW, nt);
         if (nt > w) {
             upd<<<dim3(nt - w, nt - w, nbz), 128, kTcSmemBytes, side_s>>>(
-                A, n, stride, t0, nt, 2, w, pp, op, pstride, lo, bad);
+                A, n, stride, t0, nt, 2, w, pp, op, pstride, lo, bad, 0);
             ctx->launches += 1;
         }
-        if ((e = cudaEventRecord(ev_side, side_s)) != cudaSuccess) return e;
-        upd<<<dim3(w * (2 * nt - w), 1, nbz), 128, kTcSmemBytes, main_s>>>(
-            A, n, stride, t0, nt, 1, w, pp, op, pstride, lo, bad);
-        ctx->launches += 1;
+        if ((e = cudaEventRecord(st.ev_side, side_s)) != cudaSuccess) return e;
+        if ((e = strip(t0, nt, w, pp, op, lo)) != cudaSuccess) return e;
         if (lo < n) {
             k_lu_diag64<<<nbatch, kDiag64Threads, kDiag64Smem, main_s>>>(A, n, stride, lo, Dinv, dstride, bad,
                                                                          bimg, bstride);
@@ -1604,8 +1630,9 @@ cudaError_t lu_tc_group(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int n
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    // join: everything of the side stream is done before the main stream goes on
-    if ((e = cudaStreamWaitEvent(main_s, ev_side, 0)) != cudaSuccess) return e;
+    // join: everything of the side and strip streams is done before the main stream goes on
+    if ((e = cudaStreamWaitEvent(main_s, st.ev_side, 0)) != cudaSuccess) return e;
+    if ((e = strip_join()) != cudaSuccess) return e;
     return cudaSuccess;
 }
 }  // namespace
@@ -1648,11 +1675,16 @@ cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int 
     int b0 = 0;
     for (int g = 0; g < groups; ++g) {
         const int nbg = nbatch / groups + (g < nbatch % groups ? 1 : 0);
-        cudaStream_t ms = g ? ctx->grp_main[g - 1] : ctx->stream, ss = g ? ctx->grp_side[g - 1] : ctx->side;
-        cudaEvent_t es = g ? ctx->grp_ev_side[g - 1] : ctx->ev_side, ep = g ? ctx->grp_ev_panel[g - 1] : ctx->ev_panel;
+        LuStreams st;
+        st.main = g ? ctx->grp_main[g - 1] : ctx->stream;
+        st.side = g ? ctx->grp_side[g - 1] : ctx->side;
+        st.strip = ctx->lu_strip[g];
+        st.ev_side = g ? ctx->grp_ev_side[g - 1] : ctx->ev_side;
+        st.ev_panel = g ? ctx->grp_ev_panel[g - 1] : ctx->ev_panel;
+        st.ev_strip_go = ctx->lu_ev_strip_go[g];
+        st.ev_strip_done = ctx->lu_ev_strip_done[g];
         if ((e = lu_tc_group(ctx, A + (int64_t)b0 * stride, n, stride, nbg, Dinv + (int64_t)b0 * dstride,
-                             panels + (int64_t)b0 * pbytes, bad + b0, ms, ss, es, ep, sched.outer,
-                             sched.update)) != cudaSuccess)
+                             panels + (int64_t)b0 * pbytes, bad + b0, st, sched.outer, sched.update)) != cudaSuccess)
             return e;
         b0 += nbg;
     }
