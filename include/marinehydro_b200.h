@@ -133,7 +133,9 @@ int mh_ctx_set_lu_backend(mh_ctx* ctx, int backend);
  * memory by bulk copies after the MMAs) or 1 (C staged in tensor memory
  * before the MMAs, which accumulate onto it).  n = 0 sets the default for
  * sizes with no entry of their own (2 groups, 4 panels, kernel 0); otherwise
- * a size uses the entry nearest to it (in log n).  No reference counterpart
+ * a size uses the entry nearest to it (in log n).  A new ctx holds the
+ * entries the autotuner chose on a B200: 512 -> (1, 4, 1), 1024 -> (2, 2, 0),
+ * 2048 -> (2, 4, 0).  No reference counterpart
  * (the reference factors with LAPACK). */
 int mh_ctx_set_lu_schedule(mh_ctx* ctx, int64_t n, int groups, int outer_panels, int update_kernel);
 int mh_ctx_get_lu_schedule(mh_ctx* ctx, int64_t n, int* groups, int* outer_panels, int* update_kernel);

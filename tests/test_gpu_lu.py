@@ -209,6 +209,20 @@ def test_tcgen05_lu_schedules_reconstruct(mh, gpu, groups, outer, update, n):
         assert np.max(np.abs(R - A[b])) / np.max(np.abs(A[b])) <= 4e-3, (groups, outer, n, b)
 
 
+def test_builtin_lu_schedule_table(mh):
+    """A new context carries the autotuner's choices per size; other sizes
+    take the nearest entry (in log n)."""
+    ctx = mh.Context(0)
+    try:
+        assert ctx.lu_schedule(512) == (1, 4, 1)
+        assert ctx.lu_schedule(1024) == (2, 2, 0)
+        assert ctx.lu_schedule(2048) == (2, 4, 0)
+        assert ctx.lu_schedule(1640) == (2, 4, 0) and ctx.lu_schedule(64) == (1, 4, 1)
+        assert ctx.lu_schedule(0) == (2, 4, 0)
+    finally:
+        ctx.close()
+
+
 def test_lu_autotune_sets_the_fastest(mh, gpu):
     cand = [(1, 4, 0), (2, 4, 0), (2, 8, 1)]
     out = gpu.autotune_lu(512, 6, cand)
@@ -217,4 +231,4 @@ def test_lu_autotune_sets_the_fastest(mh, gpu):
     assert gpu.lu_schedule(512) == out["best"]
     assert gpu.lu_schedule(500) == out["best"]  # nearest entry
     assert gpu.lu_schedule(0) == (2, 4, 0)  # the default is untouched
-    gpu.set_lu_schedule(512, 2, 4)
+    gpu.set_lu_schedule(512, 1, 4, 1)  # back to the built-in entry
