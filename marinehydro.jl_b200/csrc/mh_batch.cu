@@ -1250,27 +1250,28 @@ cudaError_t launch_add_f32(mh_ctx* ctx, double2* x, const float2* d, int64_t cou
 
 cudaError_t launch_gemv(mh_ctx* ctx, bool conj_trans, const double2* A, int64_t n, int nb, const double2* X,
                         const double2* B, double2* R, int nrhs, double alpha, double beta, const int* done,
-                        const int* bad)
+                        const int* bad, cudaStream_t stream)
 {
+    cudaStream_t strm = stream ? stream : ctx->stream;
     if (nrhs < 1 || nrhs > kMaxRhs) return cudaErrorInvalidValue;
     if (beta == 0.0) B = nullptr;
     const dim3 gn(blocks(n, 256), (unsigned)nb);
     if (conj_trans) {  // 8 warps per CTA, JW columns per warp
         const dim3 g4(blocks(n, 32), (unsigned)nb);
-        if (nrhs == 1) k_resid_c<1, 4><<<g4, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta, done, bad);
-        else if (nrhs == 2) k_resid_c<2, 4><<<g4, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta, done, bad);
-        else if (nrhs == 3) k_resid_c<3, 4><<<g4, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta, done, bad);
-        else if (nrhs == 4) k_resid_c<4, 4><<<g4, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta, done, bad);
+        if (nrhs == 1) k_resid_c<1, 4><<<g4, 256, 0, strm>>>(A, X, B, R, n, nrhs, alpha, beta, done, bad);
+        else if (nrhs == 2) k_resid_c<2, 4><<<g4, 256, 0, strm>>>(A, X, B, R, n, nrhs, alpha, beta, done, bad);
+        else if (nrhs == 3) k_resid_c<3, 4><<<g4, 256, 0, strm>>>(A, X, B, R, n, nrhs, alpha, beta, done, bad);
+        else if (nrhs == 4) k_resid_c<4, 4><<<g4, 256, 0, strm>>>(A, X, B, R, n, nrhs, alpha, beta, done, bad);
         else if (nrhs <= 8)
-            k_resid_c<8, 2><<<dim3(blocks(n, 16), (unsigned)nb), 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha,
+            k_resid_c<8, 2><<<dim3(blocks(n, 16), (unsigned)nb), 256, 0, strm>>>(A, X, B, R, n, nrhs, alpha,
                                                                                       beta, done, bad);
         else
-            k_resid_c<kMaxRhs, 1><<<dim3(blocks(n, 8), (unsigned)nb), 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs,
+            k_resid_c<kMaxRhs, 1><<<dim3(blocks(n, 8), (unsigned)nb), 256, 0, strm>>>(A, X, B, R, n, nrhs,
                                                                                            alpha, beta, done, bad);
     } else {
-        if (nrhs <= 4) k_resid_n<4><<<gn, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta, done, bad);
-        else if (nrhs <= 8) k_resid_n<8><<<gn, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta, done, bad);
-        else k_resid_n<kMaxRhs><<<gn, 256, 0, ctx->stream>>>(A, X, B, R, n, nrhs, alpha, beta, done, bad);
+        if (nrhs <= 4) k_resid_n<4><<<gn, 256, 0, strm>>>(A, X, B, R, n, nrhs, alpha, beta, done, bad);
+        else if (nrhs <= 8) k_resid_n<8><<<gn, 256, 0, strm>>>(A, X, B, R, n, nrhs, alpha, beta, done, bad);
+        else k_resid_n<kMaxRhs><<<gn, 256, 0, strm>>>(A, X, B, R, n, nrhs, alpha, beta, done, bad);
     }
     ctx->launches += 1;
     return cudaGetLastError();

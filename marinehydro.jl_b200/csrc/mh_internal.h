@@ -34,7 +34,7 @@ struct mh_mesh {
 enum WsSlot : int {
     WS_S = 0, WS_D, WS_RHS, WS_PHI, WS_TMP, WS_PIV, WS_INFO, WS_LWORK,
     WS_DOF, WS_OUT, WS_LO, WS_DINV, WS_TMP32, WS_MISC, WS_SR, WS_TMP32B, WS_PANEL, WS_FB, WS_COEF32,
-    WS_ADJ, WS_WSD, WS_PART, WS_GBAR, WS_TAPE, WS_FLAGS, WS_NEAR, WS_NEARRES, WS_FALL, WS_REPACK, WS_NSLOTS
+    WS_ADJ, WS_WSD, WS_PART, WS_GBAR, WS_TAPE, WS_FLAGS, WS_FLAGS2, WS_NEAR, WS_NEARRES, WS_FALL, WS_REPACK, WS_NSLOTS
 };
 
 // Largest number of right-hand sides (radiating dofs + headings) per frequency.
@@ -200,9 +200,12 @@ cudaError_t launch_lu_solve_blocks32(mh_ctx* ctx, const float2* A, int64_t n, in
 // bad (device, per matrix, may be null): a flag wait of the tensor-core
 // backend that runs out writes 3 there.  done (device, per matrix, may be
 // null; needs bad): matrices with done[b] or bad[b] nonzero are skipped.
+// stream: where to launch (null: the ctx stream); flags_slot: the workspace
+// slot of the hand-off flags (solves running concurrently need their own).
 cudaError_t launch_lu_solve_persist(mh_ctx* ctx, int backend, bool conj_trans, const float2* A, int64_t n,
                                     int64_t stride, int nbatch, const float2* Dinv, float2* X, int64_t xstride,
-                                    int nrhs, int* bad = nullptr, const int* done = nullptr);
+                                    int nrhs, int* bad = nullptr, const int* done = nullptr,
+                                    cudaStream_t stream = nullptr, int flags_slot = WS_FLAGS);
 // Conjugate-transposed solve D^H X = X with the factors of launch_lu_tc
 // (backend MH_LU_TCGEN05_F16) or launch_lu_f32 (MH_LU_SIMT_F32).
 cudaError_t launch_lu_solve_ct(mh_ctx* ctx, int backend, const float2* A, int64_t n, int64_t stride,
@@ -238,7 +241,7 @@ cudaError_t launch_add_f32(mh_ctx* ctx, double2* x, const float2* d, int64_t cou
 // done, bad (device, per matrix, both or neither): skip matrices with either set.
 cudaError_t launch_gemv(mh_ctx* ctx, bool conj_trans, const double2* A, int64_t n, int nb, const double2* X,
                         const double2* B, double2* R, int nrhs, double alpha, double beta,
-                        const int* done = nullptr, const int* bad = nullptr);
+                        const int* done = nullptr, const int* bad = nullptr, cudaStream_t stream = nullptr);
 // R = B - op(A) X for nb n x n complex matrices (op = identity or ^H).
 cudaError_t launch_residual(mh_ctx* ctx, bool conj_trans, const double2* A, int64_t n, int nb, const double2* X,
                             const double2* B, double2* R, int nrhs);

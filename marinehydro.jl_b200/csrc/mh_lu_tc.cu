@@ -1743,8 +1743,9 @@ cudaError_t solve_blocks_ct(mh_ctx* ctx, const float2* A, int64_t n, int64_t str
 
 cudaError_t launch_lu_solve_persist(mh_ctx* ctx, int backend, bool conj_trans, const float2* A, int64_t n,
                                     int64_t stride, int nbatch, const float2* Dinv, float2* X, int64_t xstride,
-                                    int nrhs, int* bad, const int* done)
+                                    int nrhs, int* bad, const int* done, cudaStream_t stream, int flags_slot)
 {
+    cudaStream_t strm = stream ? stream : ctx->stream;
     if (nrhs < 1 || nrhs > kMaxRhs) return cudaErrorInvalidValue;
     if (done && !bad) return cudaErrorInvalidValue;
     const dim3 g((unsigned)nbatch * kSolveCluster);
@@ -1755,11 +1756,11 @@ cudaError_t launch_lu_solve_persist(mh_ctx* ctx, int backend, bool conj_trans, c
         // flags of every block and triangle, then (when the caller gives no
         // per-matrix array) the timeout marks, then one flag nothing publishes
         const size_t fbytes = sizeof(int) * (size_t)(2 * nblk * nbatch + nbatch + 1);
-        auto* flags = (int*)ws_get(ctx, WS_FLAGS, fbytes);
+        auto* flags = (int*)ws_get(ctx, flags_slot, fbytes);
         if (!flags) return cudaErrorMemoryAllocation;
         int* fbad = bad ? bad : flags + 2 * nblk * nbatch;
         const int* unset = ctx->inject_wait_timeout ? flags + 2 * nblk * nbatch + nbatch : nullptr;
-        if ((e = cudaMemsetAsync(flags, 0, fbytes, ctx->stream)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(flags, 0, fbytes, strm)) != cudaSuccess) return e;
         const dim3 gf((unsigned)nbatch * kFsCluster);
         const size_t xsb = sizeof(float2) * (size_t)((nblk + kFsCluster - 1) / kFsCluster) * nrhs * TC_NB;
         const bool shared_x = xsb <= 96 * 1024;
@@ -1778,7 +1779,7 @@ cudaError_t launch_lu_solve_persist(mh_ctx* ctx, int backend, bool conj_trans, c
             const bool stage = 2 * (fa.sharedSizeBytes + xs + 2 * kFsStageBytes + (size_t)reserved) <= (size_t)sm_bytes;
             const size_t smem = xs + (stage ? 2 * kFsStageBytes : 0);
             if (smem && (e2 = raise_smem_cap((const void*)kern, smem)) != cudaSuccess) return e2;
-            kern<<<gf, kFsThreads, smem, ctx->stream>>>(A, n, stride, Dinv, ds, X, xstride, nrhs, flags, fbad,
+            kern<<<gf, kFsThreads, smem, strm>>>(A, n, stride, Dinv, ds, X, xstride, nrhs, flags, fbad,
                                                         stage ? 1 : 0, done, unset);
             return cudaSuccess;
         };
@@ -1807,10 +1808,10 @@ cudaError_t launch_lu_solve_persist(mh_ctx* ctx, int backend, bool conj_trans, c
         const int64_t ds = lu_dinv_stride(n);
         const size_t sm = persist_smem_bytes<32>();
         if (conj_trans)
-            k_lu_solve_persist<32, true><<<g, kSolveThreads, sm, ctx->stream>>>(A, n, stride, Dinv, ds, X,
+            k_lu_solve_persist<32, true><<<g, kSolveThreads, sm, strm>>>(A, n, stride, Dinv, ds, X,
                                                                                  xstride, nrhs, done, bad);
         else
-            k_lu_solve_persist<32, false><<<g, kSolveThreads, sm, ctx->stream>>>(A, n, stride, Dinv, ds, X,
+            k_lu_solve_persist<32, false><<<g, kSolveThreads, sm, strm>>>(A, n, stride, Dinv, ds, X,
                                                                                   xstride, nrhs, done, bad);
     }
     ctx->launches += 1;
