@@ -160,14 +160,6 @@ int mh_lu_autotune(mh_ctx* ctx, int64_t n, int64_t nbatch, int ncand, const int*
  * reference counterpart (the reference integrates in FP64). */
 int mh_ctx_set_wave_series_fp32(mh_ctx* ctx, int level);
 
-/* Frequency pipeline of the mixed path (on by default): in a batch of at
- * least 12 frequencies with the frequency-batched Delhommeau pass and the
- * tensor-core LU, the second half of the frequencies is assembled on a
- * low-priority stream while the first half is factored, then factored on
- * its own streams.  The results are the same bits either way.  No reference
- * counterpart. */
-int mh_ctx_set_frequency_pipeline(mh_ctx* ctx, int enable);
-
 /* Failure injection for tests (no reference counterpart): while enabled, the
  * flag waits of the tensor-core backend's triangular solves on this ctx wait
  * on a flag that nothing publishes, with a limit of 64 polls, so each wait

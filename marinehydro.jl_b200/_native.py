@@ -79,7 +79,6 @@ SIGNATURES = {
     "mh_ctx_set_lu_backend": (ctypes.c_int, [_P, ctypes.c_int]),
     "mh_ctx_set_wait_injection": (ctypes.c_int, [_P, ctypes.c_int]),
     "mh_ctx_set_wave_series_fp32": (ctypes.c_int, [_P, ctypes.c_int]),
-    "mh_ctx_set_frequency_pipeline": (ctypes.c_int, [_P, ctypes.c_int]),
     "mh_ctx_set_lu_schedule": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     "mh_ctx_get_lu_schedule": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.POINTER(ctypes.c_int),
                                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
@@ -279,11 +278,6 @@ class Context:
         contraction."""
         check(lib().mh_ctx_set_wave_series_fp32(self._h, int(level)), self._h)
         self._wave_level = int(level)
-
-    def set_frequency_pipeline(self, enable: bool):
-        """Mixed path: assemble the second half of a batch's frequencies while
-        the first half is factored (``mh_ctx_set_frequency_pipeline``; on by default)."""
-        check(lib().mh_ctx_set_frequency_pipeline(self._h, int(bool(enable))), self._h)
 
     def set_wait_injection(self, enable: bool):
         """Failure injection (tests): the triangular solves' flag waits wait

@@ -337,10 +337,6 @@ int mh_ctx_create(int device, mh_ctx** out)
             break;
     }
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_panel_join, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&ctx->pipe, cudaStreamNonBlocking, least);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_pipe_go, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_pipe_done, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         mh_ctx_destroy(ctx);
         return set_err(nullptr, MH_ERR_CUDA, "stream/event creation: %s", cudaGetErrorString(e));
@@ -374,7 +370,6 @@ int mh_ctx_destroy(mh_ctx* ctx)
     }
     for (int g = 0; g < kLuGroups; ++g)
         if (ctx->lu_strip[g]) cudaStreamSynchronize(ctx->lu_strip[g]);
-    if (ctx->pipe) cudaStreamSynchronize(ctx->pipe);
     for (int s = 0; s < WS_NSLOTS; ++s)
         if (ctx->ws[s]) cudaFree(ctx->ws[s]);
     if (ctx->delh_table) cudaFree(ctx->delh_table);
@@ -389,10 +384,6 @@ int mh_ctx_destroy(mh_ctx* ctx)
     if (ctx->ev_panel) cudaEventDestroy(ctx->ev_panel);
     if (ctx->ev_side) cudaEventDestroy(ctx->ev_side);
     if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
-    if (ctx->ev_panel_join) cudaEventDestroy(ctx->ev_panel_join);
-    if (ctx->ev_pipe_go) cudaEventDestroy(ctx->ev_pipe_go);
-    if (ctx->ev_pipe_done) cudaEventDestroy(ctx->ev_pipe_done);
-    if (ctx->pipe) cudaStreamDestroy(ctx->pipe);
     for (int g = 0; g < kLuGroups - 1; ++g) {
         if (ctx->grp_ev_panel[g]) cudaEventDestroy(ctx->grp_ev_panel[g]);
         if (ctx->grp_ev_side[g]) cudaEventDestroy(ctx->grp_ev_side[g]);
@@ -671,14 +662,6 @@ int mh_ctx_set_wave_series_fp32(mh_ctx* ctx, int level)
     if ((rc = check_ctx(ctx))) return rc;
     if (level < 0 || level > 2) return set_err(ctx, MH_ERR_ARG, "wave series precision level must be 0, 1 or 2");
     ctx->wave_series_fp32 = level;
-    return MH_OK;
-}
-
-int mh_ctx_set_frequency_pipeline(mh_ctx* ctx, int enable)
-{
-    int rc;
-    if ((rc = check_ctx(ctx))) return rc;
-    ctx->frequency_pipeline = enable != 0;
     return MH_OK;
 }
 

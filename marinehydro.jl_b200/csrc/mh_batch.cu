@@ -813,23 +813,24 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
     auto* misc = (char*)ws_get(ctx, WS_MISC, refine_ctl_bytes(nb) + 64);
     if (!S64 || !D64 || !Dlo || !Dinv || !T32 || !BC || !X || !R || !R32 || !misc) return MH_ERR_OOM;
     double2* RHS = R + nv * nb;  // right-hand side of the D (or K) system
-    // (d_fall below: two flags, one per pipeline half)
     const RefineCtl ctl = refine_ctl(misc, nb);
     int* d_bad = ctl.bad;
     auto* d_fall = (int*)(misc + refine_ctl_bytes(nb));  // set when the frequency-batched pass left pairs to the full table
     int rc;
     const double* tab = delh_table_for(ctx, bt.mask, &rc);
     if (rc) return rc;
-    // matrices, right-hand sides and low-precision factors
+    // matrices
     const uint32_t wave = bt.mask & (MH_GF_WU | MH_GF_DELHOMMEAU);
-    const bool allw = wave == MH_GF_DELHOMMEAU && tab && nb >= kAllwMinFreqs;
-    const int lvl = ctx->wave_series_fp32;
-    auto* wk = lvl == 2 ? k_wave_delh_allw<float, float>
-             : lvl == 1 ? k_wave_delh_allw<float, double> : k_wave_delh_allw<double, double>;
-    const size_t wsm = lvl ? wave_allw_smem<float>() : wave_allw_smem<double>();
-    if (wave != 0 && wave != MH_GF_WU && wave != MH_GF_DELHOMMEAU)
-        return set_err(ctx, MH_ERR_ARG, "the mixed path takes one wave term (GFWu or Delhommeau)");
-    if (allw) {  // the polar coefficients into constant memory, before any wave launch
+    dim3 grid(blocks(n, kRows), blocks(n, kCols), (unsigned)nb);
+    phase_begin(ctx, PH_WAVE);
+    if (wave == MH_GF_WU)
+        k_wave_batch<false><<<grid, kRows, 0, ctx->stream>>>(bt.m->geom, n, bt.direct, nullptr, d_k, SR,
+                                                            DR, S64, D64, Dlo, nullptr);
+    else if (wave == MH_GF_DELHOMMEAU && tab && nb >= kAllwMinFreqs) {
+        const int lvl = ctx->wave_series_fp32;
+        auto* wk = lvl == 2 ? k_wave_delh_allw<float, float>
+                 : lvl == 1 ? k_wave_delh_allw<float, double> : k_wave_delh_allw<double, double>;
+        const size_t wsm = lvl ? wave_allw_smem<float>() : wave_allw_smem<double>();
         MH_CUDA_TRY(ctx, cudaFuncSetAttribute(wk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsm));
         if (lvl == 2) {  // FP32 copy of the polar coefficients for the FP32 contraction
             auto* cf = (float*)ws_get(ctx, WS_COEF32, sizeof(float) * 4 * kTabPolarFn);
@@ -842,92 +843,48 @@ int run_mixed_chunk(const Batch& bt, const double* d_omegas, const double* d_k, 
         }
         MH_CUDA_TRY(ctx, cudaMemcpyToSymbolAsync(c_polar_mono, tab + kTabMonoOff, sizeof(c_polar_mono), 0,
                                                  cudaMemcpyDeviceToDevice, ctx->stream));
-    }
-    MH_CUDA_TRY(ctx, cudaMemsetAsync(d_bad, 0, sizeof(int) * nb, ctx->stream));
-    // the wave pass of frequencies [z0, z0 + nz) on stream s
-    auto wave_pass = [&](int z0, int nz, cudaStream_t s, int* fall) -> int {
-        const int64_t o0 = (int64_t)z0 * nn;
-        double2* tp0 = bt.tape ? bt.tape + 2 * o0 : nullptr;
-        if (wave == MH_GF_WU) {
-            k_wave_batch<false><<<dim3(blocks(n, kRows), blocks(n, kCols), (unsigned)nz), kRows, 0, s>>>(
-                bt.m->geom, n, bt.direct, nullptr, d_k + z0, SR, DR, S64 + o0, D64 + o0, Dlo + o0, nullptr);
-            ctx->launches += 1;
-        } else if (allw) {
-            for (int z = z0; z < z0 + nz; z += kAllwMaxFreqs) {
-                const int m = std::min(kAllwMaxFreqs, z0 + nz - z);
-                const int64_t off = (int64_t)z * nn;
-                double2* tp = bt.tape ? bt.tape + 2 * off : nullptr;
-                const dim3 g2(blocks(n, kWT), blocks(n, kCols));
-                MH_CUDA_TRY(ctx, cudaMemsetAsync(fall, 0, sizeof(int), s));
-                wk<<<g2, kWT, wsm, s>>>(bt.m->geom, n, bt.direct, tab, d_k + z, m, SR, DR, S64 + off, D64 + off,
-                                        Dlo + off, tp, fall);
-                k_wave_delh_allw_rest<<<g2, kWT, 0, s>>>(fall, bt.m->geom, n, bt.direct, tab, d_k + z, m, SR, DR,
-                                                        S64 + off, D64 + off, Dlo + off, tp);
-                ctx->launches += 2;
-            }
-        } else if (wave == MH_GF_DELHOMMEAU) {
-            k_wave_batch<true><<<dim3(blocks(n, kRows), blocks(n, kCols), (unsigned)nz), kRows, 0, s>>>(
-                bt.m->geom, n, bt.direct, tab, d_k + z0, SR, DR, S64 + o0, D64 + o0, Dlo + o0, tp0);
-            ctx->launches += 1;
-        } else {
-            k_no_wave_batch<<<dim3(blocks(nn, 256), nz), 256, 0, s>>>(nn, SR, DR, S64 + o0, D64 + o0, Dlo + o0);
-            ctx->launches += 1;
+        for (int z = 0; z < nb; z += kAllwMaxFreqs) {
+            const int m = std::min(kAllwMaxFreqs, nb - z);
+            const int64_t off = (int64_t)z * nn;
+            double2* tp = bt.tape ? bt.tape + 2 * off : nullptr;
+            const dim3 g2(blocks(n, kWT), blocks(n, kCols));
+            MH_CUDA_TRY(ctx, cudaMemsetAsync(d_fall, 0, sizeof(int), ctx->stream));
+            wk<<<g2, kWT, wsm, ctx->stream>>>(bt.m->geom, n, bt.direct, tab, d_k + z, m, SR, DR, S64 + off,
+                                              D64 + off, Dlo + off, tp, d_fall);
+            k_wave_delh_allw_rest<<<g2, kWT, 0, ctx->stream>>>(d_fall, bt.m->geom, n, bt.direct, tab, d_k + z, m,
+                                                              SR, DR, S64 + off, D64 + off, Dlo + off, tp);
+            ctx->launches += 1 + (z > 0);
         }
-        MH_CUDA_TRY(ctx, cudaGetLastError());
-        return MH_OK;
-    };
-    // boundary conditions, right-hand sides and the factorisation of [z0, z0 + nz)
-    auto rhs_lu = [&](int z0, int nz, cudaStream_t s, int slot0, int nslots, bool timed) -> int {
-        const int64_t v0 = (int64_t)z0 * nv, o0 = (int64_t)z0 * nn;
-        if (timed) phase_begin(ctx, PH_RHS);
-        k_bc_batch<<<dim3(blocks(n, 256), nz), 256, 0, s>>>(bt.m->geom, n, bt.d_dofs, bt.ndof, bt.d_betas,
-                                                            bt.nbeta, d_omegas + z0, bt.g, BC + v0);
-        ctx->launches += 1;
-        MH_CUDA_TRY(ctx, cudaGetLastError());
-        if (bt.direct) {
-            MH_CUDA_TRY(ctx, launch_gemv(ctx, false, S64 + o0, n, nz, BC + v0, nullptr, RHS + v0, nrhs, 1.0, 0.0,
-                                         nullptr, nullptr, s));
-        } else {
-            MH_CUDA_TRY(ctx, cudaMemcpyAsync(RHS + v0, BC + v0, sizeof(double2) * nv * nz, cudaMemcpyDeviceToDevice,
-                                             s));
-        }
-        if (timed) phase_end(ctx, PH_RHS);
-        if (timed) phase_begin(ctx, PH_LU);
-        if (tc) {
-            auto* panels = (unsigned char*)ctx->ws[WS_PANEL];
-            MH_CUDA_TRY(ctx, launch_lu_tc(ctx, Dlo + o0, n, nn, nz, Dinv + (int64_t)z0 * dinv_stride,
-                                          panels + (int64_t)z0 * lu_panel_bytes_tc(n), d_bad + z0, s, slot0,
-                                          nslots));
-        } else {
-            // (only reached without the pipeline: s is the ctx stream)
-            MH_CUDA_TRY(ctx, launch_lu_f32(ctx, Dlo + o0, n, nn, nz, Dinv + (int64_t)z0 * dinv_stride, d_bad + z0));
-        }
-        return MH_OK;
-    };
-    if (tc && !ws_get(ctx, WS_PANEL, (size_t)lu_panel_bytes_tc(n) * nb)) return MH_ERR_OOM;
-    // Frequency pipeline: the first half's matrices are assembled at full
-    // speed, then factored while the second half's wave pass runs beside the
-    // factorisation on a low-priority stream (the LU leaves much of the GPU
-    // idle on its chain of panel steps; the wave pass is compute bound), and
-    // the second half is factored on its own stream slots.
-    const bool pipe = ctx->frequency_pipeline && tc && allw && nb >= 2 * kAllwMinFreqs;
-    phase_begin(ctx, PH_WAVE);
-    if (!pipe) {
-        if ((rc = wave_pass(0, nb, ctx->stream, d_fall))) return rc;
-        phase_end(ctx, PH_WAVE);
-        if ((rc = rhs_lu(0, nb, ctx->stream, 0, kLuGroups, true))) return rc;
+    } else if (wave == MH_GF_DELHOMMEAU)
+        k_wave_batch<true><<<grid, kRows, 0, ctx->stream>>>(bt.m->geom, n, bt.direct, tab, d_k, SR, DR,
+                                                           S64, D64, Dlo, bt.tape);
+    else if (wave == 0)
+        k_no_wave_batch<<<dim3(blocks(nn, 256), nb), 256, 0, ctx->stream>>>(nn, SR, DR, S64, D64, Dlo);
+    else
+        return set_err(ctx, MH_ERR_ARG, "the mixed path takes one wave term (GFWu or Delhommeau)");
+    ctx->launches += 1;
+    phase_end(ctx, PH_WAVE);
+    phase_begin(ctx, PH_RHS);
+    k_bc_batch<<<dim3(blocks(n, 256), nb), 256, 0, ctx->stream>>>(
+        bt.m->geom, n, bt.d_dofs, bt.ndof, bt.d_betas, bt.nbeta, d_omegas, bt.g, BC);
+    ctx->launches += 1;
+    MH_CUDA_TRY(ctx, cudaGetLastError());
+    if (bt.direct) {
+        MH_CUDA_TRY(ctx, launch_gemv(ctx, false, S64, n, nb, BC, nullptr, RHS, nrhs, 1.0, 0.0));
     } else {
-        const int na = nb / 2;
-        if ((rc = wave_pass(0, na, ctx->stream, d_fall))) return rc;
-        phase_end(ctx, PH_WAVE);
-        MH_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_pipe_go, ctx->stream));
-        if ((rc = rhs_lu(0, na, ctx->stream, 0, kLuGroups / 2, true))) return rc;
-        MH_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->pipe, ctx->ev_pipe_go, 0));
-        if ((rc = wave_pass(na, nb - na, ctx->pipe, d_fall + 1))) return rc;
-        if ((rc = rhs_lu(na, nb - na, ctx->pipe, kLuGroups / 2, kLuGroups / 2, false))) return rc;
-        MH_CUDA_TRY(ctx, cudaEventRecord(ctx->ev_pipe_done, ctx->pipe));
-        MH_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, ctx->ev_pipe_done, 0));
+        MH_CUDA_TRY(ctx, cudaMemcpyAsync(RHS, BC, sizeof(double2) * nv * nb, cudaMemcpyDeviceToDevice,
+                                         ctx->stream));
     }
+    phase_end(ctx, PH_RHS);
+    // FP32 LU of every D (or K)
+    MH_CUDA_TRY(ctx, cudaMemsetAsync(d_bad, 0, sizeof(int) * nb, ctx->stream));
+    phase_begin(ctx, PH_LU);
+    if (tc) {
+        auto* panels = (unsigned char*)ws_get(ctx, WS_PANEL, (size_t)lu_panel_bytes_tc(n) * nb);
+        if (!panels) return MH_ERR_OOM;
+        MH_CUDA_TRY(ctx, launch_lu_tc(ctx, Dlo, n, nn, nb, Dinv, panels, d_bad));
+    }
+    else MH_CUDA_TRY(ctx, launch_lu_f32(ctx, Dlo, n, nn, nb, Dinv, d_bad));
     phase_end(ctx, PH_LU);
     phase_begin(ctx, PH_REFINE);
     RefineState h;

@@ -78,7 +78,6 @@ struct mh_ctx {
     cudaStream_t grp_main[kLuGroups - 1] = {}, grp_side[kLuGroups - 1] = {};
     cudaEvent_t grp_ev_panel[kLuGroups - 1] = {}, grp_ev_side[kLuGroups - 1] = {}, grp_ev_join[kLuGroups - 1] = {};
     cudaEvent_t ev_fork = nullptr;
-    cudaEvent_t ev_panel_join = nullptr;  // slot 0 joining a home stream other than `stream`
     // per LU group: the stream of the in-block strip updates (high priority,
     // concurrent with the next diagonal-block factorisation) and its events
     cudaStream_t lu_strip[kLuGroups] = {};
@@ -95,12 +94,6 @@ struct mh_ctx {
     // failure injection (tests): the triangular solves' flag waits wait on a
     // flag that nothing publishes, so they expire
     bool inject_wait_timeout = false;
-    // frequency pipeline of the mixed path (on by default): the second half
-    // of a batch's frequencies is assembled on `pipe` (low priority) while
-    // the first half is factored
-    bool frequency_pipeline = true;
-    cudaStream_t pipe = nullptr;
-    cudaEvent_t ev_pipe_go = nullptr, ev_pipe_done = nullptr;
     // reduced-precision levels of the frequency-batched Delhommeau pass
     // (mixed path only): 0 all FP64, 1 the per-frequency Horner series in
     // FP32 (the default: A, B, F within 2e-9 of the FP64 oracle at 2048
@@ -192,13 +185,8 @@ int64_t lu_dinv_stride_tc(int64_t n);
 int64_t lu_panel_bytes_tc(int64_t n);
 // Diagonally dominant FP32 complex test matrices (the LU autotuner's input).
 cudaError_t launch_fill_lu_test(mh_ctx* ctx, float2* A, int64_t n, int nbatch);
-// home: the stream the factorisation is ordered on (null: the ctx stream);
-// its groups use the stream slots slot0 .. slot0 + nslots - 1 (slot 0 is the
-// ctx's (stream, side) pair, slot g > 0 its group streams g - 1), so two
-// factorisations on disjoint slots can run at once.
 cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int nbatch, float2* Dinv,
-                         unsigned char* panels, int* bad, cudaStream_t home = nullptr, int slot0 = 0,
-                         int nslots = kLuGroups);
+                         unsigned char* panels, int* bad);
 // Block-parallel (LU)^-1 X in place; T: scratch of the same size as X.
 cudaError_t launch_lu_solve_tc(mh_ctx* ctx, const float2* A, int64_t n, int64_t stride, int nbatch,
                                const float2* Dinv, float2* X, float2* T, int64_t xstride, int nrhs);

@@ -1643,13 +1643,11 @@ cudaError_t lu_tc_group(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int n
 // diagonal-block factorisations and panel solves of one group (one CTA per
 // matrix, latency bound) run beside the trailing updates of another.
 cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int nbatch, float2* Dinv,
-                         unsigned char* panels, int* bad, cudaStream_t home, int slot0, int nslots)
+                         unsigned char* panels, int* bad)
 {
     cudaError_t e;
     static_assert(TC_NB == 64, "the diagonal blocks are factored by k_lu_diag64");
     static_assert(TC_TM == 2 * TC_NB && TC_TN == TC_TM, "two panels per 128-wide tile");
-    if (!home) home = ctx->stream;
-    if (slot0 < 0 || nslots < 1 || slot0 + nslots > kLuGroups) return cudaErrorInvalidValue;
     const LuSchedule sched = ctx->lu_schedule(n);
     if (sched.groups < 1 || sched.groups > kLuGroups || sched.outer < 2 || sched.outer > kOuterMax ||
         (sched.outer & 1) || sched.update < 0 || sched.update > 1)
@@ -1666,44 +1664,33 @@ cudaError_t launch_lu_tc(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int 
     if ((e = cudaFuncSetAttribute(k_lu_diag64, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kDiag64Smem)) != cudaSuccess)
         return e;
-    const int groups = std::min(std::min(sched.groups, nbatch), nslots);
+    const int groups = std::min(sched.groups, nbatch);
     const int64_t dstride = lu_dinv_stride_tc(n);
     const int64_t pbytes = lu_panel_bytes_tc(n);
-    auto slot_main = [&](int sl) { return sl ? ctx->grp_main[sl - 1] : ctx->stream; };
-    // every group's main stream starts after what `home` has issued so far
-    bool forked = false;
-    for (int g = 0; g < groups; ++g)
-        if (slot_main(slot0 + g) != home) {
-            if (!forked) {
-                if ((e = cudaEventRecord(ctx->ev_fork, home)) != cudaSuccess) return e;
-                forked = true;
-            }
-            if ((e = cudaStreamWaitEvent(slot_main(slot0 + g), ctx->ev_fork, 0)) != cudaSuccess) return e;
-        }
+    if (groups > 1) {
+        if ((e = cudaEventRecord(ctx->ev_fork, ctx->stream)) != cudaSuccess) return e;
+        for (int g = 1; g < groups; ++g)
+            if ((e = cudaStreamWaitEvent(ctx->grp_main[g - 1], ctx->ev_fork, 0)) != cudaSuccess) return e;
+    }
     int b0 = 0;
     for (int g = 0; g < groups; ++g) {
-        const int sl = slot0 + g;
         const int nbg = nbatch / groups + (g < nbatch % groups ? 1 : 0);
         LuStreams st;
-        st.main = slot_main(sl);
-        st.side = sl ? ctx->grp_side[sl - 1] : ctx->side;
-        st.strip = ctx->lu_strip[sl];
-        st.ev_side = sl ? ctx->grp_ev_side[sl - 1] : ctx->ev_side;
-        st.ev_panel = sl ? ctx->grp_ev_panel[sl - 1] : ctx->ev_panel;
-        st.ev_strip_go = ctx->lu_ev_strip_go[sl];
-        st.ev_strip_done = ctx->lu_ev_strip_done[sl];
+        st.main = g ? ctx->grp_main[g - 1] : ctx->stream;
+        st.side = g ? ctx->grp_side[g - 1] : ctx->side;
+        st.strip = ctx->lu_strip[g];
+        st.ev_side = g ? ctx->grp_ev_side[g - 1] : ctx->ev_side;
+        st.ev_panel = g ? ctx->grp_ev_panel[g - 1] : ctx->ev_panel;
+        st.ev_strip_go = ctx->lu_ev_strip_go[g];
+        st.ev_strip_done = ctx->lu_ev_strip_done[g];
         if ((e = lu_tc_group(ctx, A + (int64_t)b0 * stride, n, stride, nbg, Dinv + (int64_t)b0 * dstride,
                              panels + (int64_t)b0 * pbytes, bad + b0, st, sched.outer, sched.update)) != cudaSuccess)
             return e;
         b0 += nbg;
     }
-    // `home` goes on after every group
-    for (int g = 0; g < groups; ++g) {
-        const int sl = slot0 + g;
-        if (slot_main(sl) == home) continue;
-        cudaEvent_t ej = sl ? ctx->grp_ev_join[sl - 1] : ctx->ev_panel_join;
-        if ((e = cudaEventRecord(ej, slot_main(sl))) != cudaSuccess) return e;
-        if ((e = cudaStreamWaitEvent(home, ej, 0)) != cudaSuccess) return e;
+    for (int g = 1; g < groups; ++g) {
+        if ((e = cudaEventRecord(ctx->grp_ev_join[g - 1], ctx->grp_main[g - 1])) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(ctx->stream, ctx->grp_ev_join[g - 1], 0)) != cudaSuccess) return e;
     }
     return cudaSuccess;
 }

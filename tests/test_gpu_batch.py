@@ -182,25 +182,3 @@ def test_wave_series_fp32_levels(mh, oracle, gpu, body, level):
         gpu.set_wave_series_fp32(old)
     Ao, Bo, _, _ = oracle.hydro_coefficients(body.mesh, omegas, dofs, gf_mask=DELH)
     assert _rel(A, Ao) < 1e-6 and _rel(B, Bo) < 1e-6
-
-
-@pytest.mark.parametrize("direct", [True, False])
-def test_frequency_pipeline_gives_the_same_bits(mh, gpu, direct):
-    """The frequency pipeline (the second half of the frequencies assembled
-    while the first half is factored, each half on its own streams) computes
-    every frequency exactly as the unpipelined batch does."""
-    mesh = mh.mesh_hemisphere(1.0, (0, 0, 0), (16, 24))
-    dofs = [mh.translational_dofs(mesh, "Heave"), mh.translational_dofs(mesh, "Surge")]
-    om = np.linspace(0.3, 3.0, 20)
-    gfs = _gfs(mh, DELH)
-    out = {}
-    for on in (True, False):
-        gpu.set_frequency_pipeline(on)
-        try:
-            out[on] = mh.hydro_batch(mesh, om, dofs, [0.0], green_functions=gfs, direct=direct, precision="mixed",
-                                     tol=1e-12, ctx=gpu)
-        finally:
-            gpu.set_frequency_pipeline(True)
-    for a, b in zip(out[True][:4], out[False][:4]):
-        assert np.array_equal(a, b)
-    assert out[True][4].n_fallback == 0
