@@ -835,12 +835,12 @@ def run_design_batch(mh, args, torch):
     16 frequencies in [0.3, 3.0], heave, Delhommeau, mixed; each design's A, B
     and forward-mode dA/dR, dB/dR at every frequency (one
     hydro_batch_jvp call per design), the designs dealt largest first over
-    four library contexts on their own host threads.  Timed end to end on
+    eight library contexts on their own host threads.  Timed end to end on
     the host clock around the public call; one solve = one (design,
     frequency) problem with its radius tangent."""
     pop = mh.designs(0, 48)
     om = np.linspace(0.3, 3.0, 16)
-    ctxs = [mh.Context(0) for _ in range(4)]
+    ctxs = [mh.Context(0) for _ in range(8)]
     try:
         mh.design_batch(pop, om, precision="mixed", tol=args.tol, contexts=ctxs)
         torch.cuda.synchronize()
@@ -861,10 +861,10 @@ def run_design_batch(mh, args, torch):
     nprob = len(pop) * len(om)
     return {"value": nprob / dt, "unit": "solves/s (each with dA/dR, dB/dR)", "ms_per_batch": dt * 1e3,
             "workload": "design_population_48_hemispheres_64_to_1640p_16omega_heave_delhommeau",
-            "panels_total": int(sum(r.nfaces for r in res)), "contexts": 4,
+            "panels_total": int(sum(r.nfaces for r in res)), "contexts": len(ctxs),
             "timing": "host wall clock around design_batch (mesh generation, uploads, forward + tangent)",
             "fp64_gpu": {"value": nprob / dt64, "unit": "solves/s", "ms_per_batch": dt64 * 1e3,
-                         "mode": "FP64 path one frequency at a time, same four contexts"},
+                         "mode": "FP64 path one frequency at a time, same contexts"},
             "accuracy_dA_dR_vs_fp64": acc}
 
 

@@ -74,7 +74,7 @@ class DesignResult:
 def _one_design(d: Design, om, gfs, precision, tol, ctx) -> DesignResult:
     mesh = mesh_hemisphere(d.radius, (0.0, 0.0, 0.0), d.resolution)
     body = FloatingBody.rigid(mesh, ["Heave"])
-    tan = hemisphere_tangents(d.radius, (0.0, 0.0, 0.0), d.resolution)["radius"]
+    tan = hemisphere_tangents(d.radius, (0.0, 0.0, 0.0), d.resolution, mesh=mesh)["radius"]
     r = hydro_batch_jvp(mesh, om, list(body.dofs.values()), (), tan, green_functions=gfs,
                         precision=precision, tol=tol, ctx=ctx)
     return DesignResult(d, mesh.nfaces, r.added_mass[0, 0].copy(), r.damping[0, 0].copy(),

@@ -220,13 +220,14 @@ def hydro_batch_rrule(mesh: Mesh, omegas, dofs, betas=(), **kw):
     return (A, B, Fd, Fk), pullback
 
 
-def hemisphere_tangents(radius: float = 1.0, center=(0.0, 0.0, 0.0), resolution=(10, 10)) -> dict:
+def hemisphere_tangents(radius: float = 1.0, center=(0.0, 0.0, 0.0), resolution=(10, 10), mesh=None) -> dict:
     """Exact derivatives of ``mesh_hemisphere(radius, center, resolution)``
     with respect to its parameters: {"radius", "cx", "cy", "cz"} ->
     MeshTangent.  Every field is homogeneous in the radius about the centre:
     vertices and centres are centre + R u, normals do not change, areas
-    scale as R^2 and radii as R."""
-    m = mesh_hemisphere(radius, center, resolution)
+    scale as R^2 and radii as R.  ``mesh``: that mesh when the caller has
+    already generated it."""
+    m = mesh if mesh is not None else mesh_hemisphere(radius, center, resolution)
     c = np.asarray(center, dtype=np.float64).reshape(1, 3)
     out = {"radius": MeshTangent((m.vertices - c) / radius, (m.centers - c) / radius,
                                  np.zeros_like(m.normals), 2.0 * m.areas / radius, m.radii / radius)}

@@ -131,28 +131,27 @@ def mesh_hemisphere(radius: float = 1.0, center=(0.0, 0.0, 0.0),
     thetas = 0.5 * math.pi + 0.5 * math.pi * np.arange(nb + 1) / nb
     phis = 2.0 * math.pi * np.arange(nphi) / nphi
     cx, cy, cz = (float(c) for c in center)
-    verts = []
-    for t in thetas[:-1]:
-        st, ct = math.sin(t), math.cos(t)
-        for p in phis:
-            verts.append((cx + radius * st * math.cos(p), cy + radius * st * math.sin(p),
-                          cz + radius * ct))
-    pole = len(verts)
-    verts.append((cx, cy, cz - radius))
-    verts = np.asarray(verts, dtype=np.float64)
-    faces = []
-    for b in range(nb):
-        for s in range(nphi):
-            s2 = (s + 1) % nphi
-            a_ = b * nphi + s
-            d_ = b * nphi + s2
-            if b + 1 < nb:
-                b_ = (b + 1) * nphi + s
-                c_ = (b + 1) * nphi + s2
-                faces.append((a_, b_, c_, d_))
-            else:
-                faces.append((a_, pole, d_, d_))
-    faces = np.asarray(faces, dtype=np.int64)
+    # band b, sector s -> vertex b * nphi + s (the sines and cosines of the
+    # angles by the C library, the products in the same order per vertex)
+    st = np.array([math.sin(t) for t in thetas[:-1]])
+    ct = np.array([math.cos(t) for t in thetas[:-1]])
+    cp = np.array([math.cos(p) for p in phis])
+    sp = np.array([math.sin(p) for p in phis])
+    rs = radius * st
+    verts = np.empty((nb * nphi + 1, 3))
+    verts[:-1, 0] = (cx + rs[:, None] * cp[None, :]).reshape(-1)
+    verts[:-1, 1] = (cy + rs[:, None] * sp[None, :]).reshape(-1)
+    verts[:-1, 2] = np.repeat(cz + radius * ct, nphi)
+    pole = nb * nphi
+    verts[pole] = (cx, cy, cz - radius)
+    b = np.repeat(np.arange(nb), nphi)
+    s = np.tile(np.arange(nphi), nb)
+    s2 = (s + 1) % nphi
+    a_ = b * nphi + s
+    d_ = b * nphi + s2
+    last = b + 1 == nb
+    faces = np.stack([a_, np.where(last, pole, (b + 1) * nphi + s), np.where(last, d_, (b + 1) * nphi + s2), d_],
+                     axis=1).astype(np.int64)
     centers, normals, areas, radii = panel_geometry(verts, faces)
     return Mesh(verts, faces, centers, normals, areas, radii)
 
