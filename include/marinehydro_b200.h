@@ -219,6 +219,9 @@ int mh_mesh_create(mh_ctx* ctx, int64_t nfaces, int64_t nvertices,
                    const double* centers, const double* normals,
                    const double* areas, const double* radii,
                    mh_mesh** out);
+/* Releases a mesh; pass the ctx that created it: its device memory is then
+ * released in stream order on that ctx, after the ctx's work issued so far,
+ * without synchronising the device (with ctx = NULL it is freed at once). */
 int mh_mesh_destroy(mh_ctx* ctx, mh_mesh* mesh);
 int mh_mesh_nfaces(const mh_mesh* mesh, int64_t* nfaces);
 

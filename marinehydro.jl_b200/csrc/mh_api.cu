@@ -60,14 +60,17 @@ void* ws_get(mh_ctx* ctx, int slot, size_t bytes)
 {
     if (bytes == 0) bytes = 16;
     if (ctx->ws_bytes[slot] >= bytes) return ctx->ws[slot];
+    // stream-ordered: the old buffer is released after the work already
+    // issued on the ctx stream (which the ctx's other streams join), and
+    // neither call synchronises the device, so contexts on other host threads
+    // keep running
     if (ctx->ws[slot]) {
-        cudaStreamSynchronize(ctx->stream);
-        cudaFree(ctx->ws[slot]);
+        cudaFreeAsync(ctx->ws[slot], ctx->stream);
         ctx->ws[slot] = nullptr;
         ctx->ws_bytes[slot] = 0;
     }
     void* p = nullptr;
-    cudaError_t e = cudaMalloc(&p, bytes);
+    cudaError_t e = cudaMallocAsync(&p, bytes, ctx->stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
         set_err(ctx, MH_ERR_OOM, "device allocation of %zu bytes failed: %s", bytes,
@@ -310,6 +313,16 @@ int mh_ctx_create(int device, mh_ctx** out)
     auto* ctx = new (std::nothrow) mh_ctx();
     if (!ctx) return set_err(nullptr, MH_ERR_OOM, "host allocation failed");
     ctx->device = device;
+    {  // keep freed stream-ordered memory in the device's pool instead of
+       // returning it to the driver at every synchronisation (a setting of
+       // this process's pool, not of the GPU)
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        cudaGetLastError();
+    }
     int least = 0, greatest = 0;
     cudaDeviceGetStreamPriorityRange(&least, &greatest);
     if ((e = cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, greatest)) != cudaSuccess ||
@@ -745,7 +758,9 @@ int mh_mesh_create(mh_ctx* ctx, int64_t nfaces, int64_t nvertices, const double*
         return set_err(ctx, MH_ERR_OOM, "host allocation failed");
     }
     size_t bytes = sizeof(double) * (size_t)G_NFIELDS * (size_t)n;
-    cudaError_t e = cudaMalloc(&m->geom, bytes);
+    // stream-ordered allocation: no device-wide synchronisation, so meshes
+    // come and go without stalling other contexts
+    cudaError_t e = cudaMallocAsync((void**)&m->geom, bytes, ctx->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(m->geom, h, bytes, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     delete[] h;
@@ -763,10 +778,13 @@ int mh_mesh_destroy(mh_ctx* ctx, mh_mesh* mesh)
 {
     if (!mesh) return MH_OK;
     if (ctx) {
+        // released after the ctx's work issued so far, without waiting for it
+        // or synchronising the device
         cudaSetDevice(ctx->device);
-        cudaStreamSynchronize(ctx->stream);
+        if (mesh->geom) cudaFreeAsync(mesh->geom, ctx->stream);
+    } else if (mesh->geom) {
+        cudaFree(mesh->geom);
     }
-    if (mesh->geom) cudaFree(mesh->geom);
     delete mesh;
     return MH_OK;
 }
