@@ -1213,15 +1213,16 @@ __device__ __forceinline__ void fs_stage(float2* dst, const float2* __restrict__
 __device__ __forceinline__ void fs_stage_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // The entries fs_load / fs_load_inv give, from a block staged by fs_stage
-// (at (i0, k0) of the factors, or (k0, i0) for kCT; the inverse at (0, 0)).
-template <bool kCT>
+// (at (i0, k0) of the factors, or (k0, i0) for kCT; the inverse at (0, 0)),
+// columns LD entries apart.
+template <bool kCT, int LD = kFsLd>
 __device__ __forceinline__ void fs_from_stage(const float2* s, float2 (&m)[kFsPer])
 {
     const int r = threadIdx.x / kFsLanes, tq = threadIdx.x % kFsLanes;
 #pragma unroll
     for (int j = 0; j < kFsPer; ++j) {
         const int t = fs_t(j, tq);
-        m[j] = kCT ? fs_conj(s[r * kFsLd + t]) : s[t * kFsLd + r];
+        m[j] = kCT ? fs_conj(s[r * LD + t]) : s[t * LD + r];
     }
 }
 
@@ -1469,7 +1470,331 @@ k_lu_solve_flags(const float2* __restrict__ A, int64_t n, int64_t stride, const 
     }
 }
 
+// ---------------------------------------------------------------------------
+// streamed triangular solves: left-looking, operands streamed ahead
+// ---------------------------------------------------------------------------
+//
+// The triangles, block ownership (block i to CTA i mod kFsCluster of the
+// matrix's cluster) and published flags of k_lu_solve_flags, with the work
+// of each block gathered on its owner (left-looking): x_i = b_i - sum_j
+// T_ij y_j accumulates in registers over the blocks j before i in the
+// triangle's order, then y_i = inv(T_ii) x_i is written over x_i and
+// published.  Every operand a CTA reads is known in advance (its blocks'
+// tiles in order, each block followed by its inverse diagonal block), so
+// two producer warps stream them through a ring of kSsStages shared-memory
+// stages while eight consumer warps multiply: the tile warp copies each tile
+// (64 columns of up to 512 bytes, one column per warp instruction of 16-byte
+// cp.async) as soon as its stage is free, one lane of the y warp adds the
+// y_j the tile multiplies (cp.async.bulk) once y_j's flag is published
+// (separate warps: a lane spinning on a flag would hold up the tile copies
+// of its warp; 16-byte copies: 64 bulk copies of 512 bytes per tile kept
+// the SM's bulk-copy unit from streaming at the memory's rate).  The tile
+// stream thus runs ahead of the flag chain, whose step is one copy of a
+// published y_j, one tile product and one inverse product.
+// Needs n even (16-byte aligned columns) and one to four right-hand sides;
+// the launcher uses k_lu_solve_flags otherwise.  Stage waits and flag waits
+// are bounded: a flag wait that runs out marks the matrix (3) and the
+// kernel finishes with garbage for it; a stage wait that runs out marks it
+// (2).  Failure injection (unset_flag) as k_lu_solve_flags.
+constexpr int kSsStages = 3;
+constexpr int kSsLd = 66;  // staged column stride in float2: the consumers' reads are bank-conflict-free
+constexpr uint32_t kSsTileBytes = 64 * kSsLd * sizeof(float2);
+constexpr uint32_t kSsYBytes = 4 * 64 * sizeof(float2);  // y_j of up to four right-hand sides
+constexpr uint32_t kSsStageBytes = kSsTileBytes + kSsYBytes;
+constexpr int kSsConsumers = 256;
+constexpr int kSsThreads = kSsConsumers + 64;  // eight consumer warps, the tile warp and the y warp
+constexpr size_t kSsSmemBytes = (size_t)kSsStages * kSsStageBytes + kSsYBytes;  // + x_i of the block being solved
+constexpr int kSsWaitPolls = 1 << 17;     // bounded stage waits (each poll sleeps >= 64 ns: > 8 ms in all) ...
+constexpr int kSsFlagPolls = 1 << 17;     // ... and flag waits, as long as k_lu_solve_flags' flag waits
 
+__device__ __forceinline__ void ss_bar_init(uint64_t* bar, int count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ bool ss_wait(uint64_t* bar, uint32_t phase)
+{
+    const uint32_t a = smem_u32(bar);
+    for (int it = 0; it < kSsWaitPolls; ++it) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(ok)
+            : "r"(a), "r"(phase)
+            : "memory");
+        if (ok) return true;
+        __nanosleep(64);
+    }
+    return false;
+}
+
+__device__ __forceinline__ void ss_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void ss_arrive_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void ss_copy(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void ss_consumer_sync()
+{
+    asm volatile("bar.sync 1, %0;" :: "r"(kSsConsumers) : "memory");
+}
+
+// The blocks of CTA `rank` in the order of triangle `tri` (0: ascending,
+// 1: descending): count and the bi-th one.
+__device__ __forceinline__ int ss_nown(int nblk, int rank)
+{
+    return rank < nblk ? (nblk - 1 - rank) / kFsCluster + 1 : 0;
+}
+
+__device__ __forceinline__ int ss_own(int tri, int nblk, int rank, int bi)
+{
+    return tri == 0 ? rank + kFsCluster * bi : rank + kFsCluster * (ss_nown(nblk, rank) - 1 - bi);
+}
+
+// Tiles of block i (the blocks before it in the triangle's order) and the jj-th of them.
+__device__ __forceinline__ int ss_ntiles(int tri, int nblk, int i) { return tri == 0 ? i : nblk - 1 - i; }
+__device__ __forceinline__ int ss_tile_j(int tri, int nblk, int jj) { return tri == 0 ? jj : nblk - 1 - jj; }
+
+template <bool kCT, int NQ>
+__global__ void __cluster_dims__(kFsCluster, 1, 1) __launch_bounds__(kSsThreads, 2)
+k_lu_solve_stream(const float2* __restrict__ A, int64_t n, int64_t stride, const float2* __restrict__ Dinv,
+                  int64_t dstride, float2* X, int64_t xstride, int* flags, int* bad, const int* done,
+                  const int* unset_flag)
+{
+    constexpr int NB = 64;
+    extern __shared__ __align__(128) unsigned char ss_smem[];
+    __shared__ uint64_t full[kSsStages], empty[kSsStages];
+    const int64_t b = blockIdx.x / kFsCluster;
+    // a matrix whose refinement converged, or that is marked bad, is left
+    // alone (every CTA of its cluster returns here, before any barrier)
+    if (done && (done[b] || bad[b])) return;
+    const int rank = (int)cluster_rank();
+    const float2* M = A + b * stride;
+    const float2* Dv = Dinv + b * dstride;
+    float2* x = X + b * xstride;
+    const int nblk = (int)((n + NB - 1) / NB);
+    int* fl = flags + b * 2 * nblk;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nown = ss_nown(nblk, rank);
+    auto stage = [&](int s) { return reinterpret_cast<float2*>(ss_smem + (size_t)s * kSsStageBytes); };
+    auto ystage = [&](int s) {
+        return reinterpret_cast<float2(*)[NB]>(ss_smem + (size_t)s * kSsStageBytes + kSsTileBytes);
+    };
+    auto xs = reinterpret_cast<float2(*)[NB]>(ss_smem + (size_t)kSsStages * kSsStageBytes);
+    if (tid == 0) {
+        for (int s = 0; s < kSsStages; ++s) {
+            ss_bar_init(&full[s], 33);                      // the tile warp's lanes and the y lane
+            ss_bar_init(&empty[s], kSsConsumers / 32);      // every consumer warp
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (warp >= kSsConsumers / 32) {  // producer warps
+        if (warp == kSsConsumers / 32) {  // tiles
+            int t = 0;
+            for (int tri = 0; tri < 2; ++tri) {
+                const int inv_off = ((tri == 0) != kCT) ? 0 : NB * NB;
+                for (int bi = 0; bi < nown; ++bi) {
+                    const int i = ss_own(tri, nblk, rank, bi);
+                    const int nt = ss_ntiles(tri, nblk, i);
+                    for (int jj = 0; jj <= nt; ++jj, ++t) {
+                        const int s = t % kSsStages;
+                        // lane 0 waits for the stage; the other lanes write into it after
+                        if (t >= kSsStages && lane == 0 && !ss_wait(&empty[s], (uint32_t)((t / kSsStages - 1) & 1)))
+                            atomicExch(bad + b, 2);
+                        __syncwarp();
+                        const float2* src;
+                        int64_t ld;
+                        int ncol, nrow;
+                        if (jj < nt) {  // tile (i, j): rows of block i and columns of block j (kCT: transposed)
+                            const int64_t i0 = (int64_t)i * NB, j0 = (int64_t)ss_tile_j(tri, nblk, jj) * NB;
+                            const int64_t r0 = kCT ? j0 : i0, c0 = kCT ? i0 : j0;
+                            src = M + c0 * n + r0;
+                            ld = n;
+                            ncol = (int)min((int64_t)NB, n - c0);
+                            nrow = (int)min((int64_t)NB, n - r0);
+                        } else {  // inverse diagonal block of i (full 64 x 64, column-major)
+                            src = Dv + (int64_t)i * 2 * NB * NB + inv_off;
+                            ld = NB;
+                            ncol = NB;
+                            nrow = NB;
+                        }
+                        // one 16-byte cp.async per lane and column: a column (512 bytes)
+                        // per warp instruction; each lane's arrival on the stage's
+                        // barrier fires when its copies have landed
+                        if (2 * lane < nrow) {
+                            const float2* sp = src + 2 * lane;
+                            const uint32_t dp = smem_u32(stage(s) + 2 * lane);
+#pragma unroll 8
+                            for (int c = 0; c < ncol; ++c)
+                                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;"
+                                             :: "r"(dp + (uint32_t)(c * kSsLd * sizeof(float2))), "l"(sp + c * ld)
+                                             : "memory");
+                        }
+                        asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];"
+                                     :: "r"(smem_u32(&full[s])) : "memory");
+                    }
+                }
+            }
+        } else if (lane == 0) {  // y
+            int t = 0;
+            bool gave_up = false;
+            // flags already acquired: the blocks of a triangle are needed in its
+            // order (block i takes j = 0 .. i - 1, or nblk - 1 .. i + 1), so the
+            // acquired ones form a prefix (seen_f) or a suffix (seen_b)
+            int seen_f = 0, seen_b = nblk;
+            for (int tri = 0; tri < 2; ++tri) {
+                for (int bi = 0; bi < nown; ++bi) {
+                    const int i = ss_own(tri, nblk, rank, bi);
+                    const int nt = ss_ntiles(tri, nblk, i);
+                    for (int jj = 0; jj <= nt; ++jj, ++t) {
+                        const int s = t % kSsStages;
+                        if (t >= kSsStages && !ss_wait(&empty[s], (uint32_t)((t / kSsStages - 1) & 1)))
+                            atomicExch(bad + b, 2);
+                        if (jj == nt) {  // the inverse item carries no y
+                            ss_arrive(&full[s]);
+                            continue;
+                        }
+                        const int j = ss_tile_j(tri, nblk, jj);
+                        const bool known = tri == 0 ? j < seen_f : j >= seen_b;
+                        if (!known && !gave_up) {
+                            // failure injection: a wait on another CTA's block waits
+                            // on a flag that nothing publishes, with a short limit
+                            const bool inject = unset_flag && j % kFsCluster != rank;
+                            const int* wf = inject ? unset_flag : fl + tri * nblk + j;
+                            const int limit = inject ? kFsInjectPolls : kSsFlagPolls;
+                            int it = 0;
+                            while (fs_ld_acquire(wf) == 0 && ++it < limit) __nanosleep(64);
+                            if (it >= limit) {
+                                gave_up = true;  // later flags are not waited for: the matrix is garbage now
+                                atomicExch(bad + b, 3);
+                            }
+                            if (tri == 0 && j == seen_f) ++seen_f;
+                            if (tri == 1 && j == seen_b - 1) --seen_b;
+                            // the y_j just acquired was written by generic stores:
+                            // order the bulk copies that read it after the acquire
+                            asm volatile("fence.proxy.async.global;" ::: "memory");
+                        }
+                        const int64_t j0 = (int64_t)j * NB;
+                        const int nrow = (int)min((int64_t)NB, n - j0);
+                        ss_arrive_tx(&full[s], (uint32_t)(NQ * nrow * sizeof(float2)));
+#pragma unroll
+                        for (int q = 0; q < NQ; ++q)
+                            ss_copy(ystage(s)[q], x + (int64_t)q * n + j0, (uint32_t)(nrow * sizeof(float2)),
+                                    &full[s]);
+                    }
+                }
+            }
+        }
+        return;
+    }
+    // consumer warps: thread (r, tq) holds entries (r, fs_t(jj, tq)) of each tile
+    const int r = tid / kFsLanes, tq = tid % kFsLanes;
+    int t = 0;
+    bool ok = true;
+    auto take = [&](int s) {
+        if (!ss_wait(&full[s], (uint32_t)((t / kSsStages) & 1)) && ok) {
+            ok = false;
+            if (lane == 0) atomicExch(bad + b, 2);
+        }
+    };
+    auto give = [&](int s) {
+        __syncwarp();
+        if (lane == 0) ss_arrive(&empty[s]);
+        ++t;
+    };
+    for (int tri = 0; tri < 2; ++tri) {
+        for (int bi = 0; bi < nown; ++bi) {
+            const int i = ss_own(tri, nblk, rank, bi);
+            const int nt = ss_ntiles(tri, nblk, i);
+            const int64_t i0 = (int64_t)i * NB;
+            const bool rok = i0 + r < n;
+            float ax[4] = {0.f, 0.f, 0.f, 0.f}, ay[4] = {0.f, 0.f, 0.f, 0.f};
+            for (int jj = 0; jj < nt; ++jj) {
+                const int s = t % kSsStages;
+                const int64_t j0 = (int64_t)ss_tile_j(tri, nblk, jj) * NB;
+                const bool whole = i0 + NB <= n && j0 + NB <= n;
+                take(s);
+                const float2* st = stage(s);
+                float2 m[kFsPer];
+#pragma unroll
+                for (int e = 0; e < kFsPer; ++e) {
+                    const int c = fs_t(e, tq);
+                    m[e] = kCT ? fs_conj(st[r * kSsLd + c]) : st[c * kSsLd + r];
+                    if (!whole && !(rok && j0 + c < n)) m[e] = make_float2(0.f, 0.f);
+                }
+                const float2 (*ys)[NB] = ystage(s);
+#pragma unroll
+                for (int e = 0; e < kFsPer; e += 2) {
+                    const int c = fs_t(e, tq);
+                    const bool cok = whole || j0 + c < n;  // n even: c and c + 1 together
+#pragma unroll
+                    for (int qq = 0; qq < NQ; ++qq) {
+                        float4 v = fs_lds4(&ys[qq][c]);
+                        if (!cok) v = make_float4(0.f, 0.f, 0.f, 0.f);
+                        const float2 a = m[e], a2 = m[e + 1];
+                        ax[qq] += a.x * v.x - a.y * v.y;
+                        ay[qq] += a.x * v.y + a.y * v.x;
+                        ax[qq] += a2.x * v.z - a2.y * v.w;
+                        ay[qq] += a2.x * v.w + a2.y * v.z;
+                    }
+                }
+                give(s);
+            }
+#pragma unroll
+            for (int qq = 0; qq < NQ; ++qq) {
+#pragma unroll
+                for (int o = 1; o < kFsLanes; o <<= 1) {
+                    ax[qq] += __shfl_xor_sync(0xffffffffu, ax[qq], o);
+                    ay[qq] += __shfl_xor_sync(0xffffffffu, ay[qq], o);
+                }
+            }
+            // x_i = b_i - sum_j T_ij y_j, rows outside the matrix zero
+            if (tq == 0) {
+#pragma unroll
+                for (int qq = 0; qq < NQ; ++qq) {
+                    float2 v = make_float2(0.f, 0.f);
+                    if (rok) {
+                        const float2 bv = __ldcg(x + (int64_t)qq * n + i0 + r);
+                        v = make_float2(bv.x - ax[qq], bv.y - ay[qq]);
+                    }
+                    xs[qq][r] = v;
+                }
+            }
+            ss_consumer_sync();
+            // y_i = inv(T_ii) x_i, over x_i; then publish
+            const int s = t % kSsStages;
+            take(s);
+            float2 iv[kFsPer];
+            fs_from_stage<kCT, kSsLd>(stage(s), iv);
+            float bx[4], by[4];
+            fs_rowdot(iv, xs, 0, NQ, bx, by);
+            give(s);
+            if (tq == 0 && rok) {
+#pragma unroll
+                for (int qq = 0; qq < NQ; ++qq) x[(int64_t)qq * n + i0 + r] = make_float2(bx[qq], by[qq]);
+            }
+            ss_consumer_sync();
+            if (tid == 0) {
+                __threadfence();
+                fs_st_release(fl + tri * nblk + i, 1);
+            }
+        }
+    }
+}
 
 }  // namespace
 
@@ -1762,6 +2087,35 @@ cudaError_t launch_lu_solve_persist(mh_ctx* ctx, int backend, bool conj_trans, c
         const int* unset = ctx->inject_wait_timeout ? flags + 2 * nblk * nbatch + nbatch : nullptr;
         if ((e = cudaMemsetAsync(flags, 0, fbytes, strm)) != cudaSuccess) return e;
         const dim3 gf((unsigned)nbatch * kFsCluster);
+        // n even (every column and block of y starts on 16 bytes) and one to
+        // four right-hand sides: the streamed left-looking solve
+        auto a16 = [](const void* p) { return ((uintptr_t)p & 15) == 0; };
+        if (n % 2 == 0 && nrhs <= 4 && stride % 2 == 0 && xstride % 2 == 0 && a16(A) && a16(Dinv) && a16(X)) {
+            auto run = [&](auto kern) -> cudaError_t {
+                cudaError_t e2;
+                if ((e2 = raise_smem_cap((const void*)kern, kSsSmemBytes)) != cudaSuccess) return e2;
+                // two CTAs per SM need the largest shared-memory carveout
+                if ((e2 = cudaFuncSetAttribute((const void*)kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                               100)) != cudaSuccess)
+                    return e2;
+                kern<<<gf, kSsThreads, kSsSmemBytes, strm>>>(A, n, stride, Dinv, ds, X, xstride, flags, fbad, done,
+                                                             unset);
+                return cudaSuccess;
+            };
+            switch (nrhs * 2 + (conj_trans ? 1 : 0)) {
+            case 2: e = run(k_lu_solve_stream<false, 1>); break;
+            case 3: e = run(k_lu_solve_stream<true, 1>); break;
+            case 4: e = run(k_lu_solve_stream<false, 2>); break;
+            case 5: e = run(k_lu_solve_stream<true, 2>); break;
+            case 6: e = run(k_lu_solve_stream<false, 3>); break;
+            case 7: e = run(k_lu_solve_stream<true, 3>); break;
+            case 8: e = run(k_lu_solve_stream<false, 4>); break;
+            default: e = run(k_lu_solve_stream<true, 4>); break;
+            }
+            if (e != cudaSuccess) return e;
+            ctx->launches += 1;
+            return cudaGetLastError();
+        }
         const size_t xsb = sizeof(float2) * (size_t)((nblk + kFsCluster - 1) / kFsCluster) * nrhs * TC_NB;
         const bool shared_x = xsb <= 96 * 1024;
         // staging of the next block (two more 34 KB blocks) only while two

@@ -112,14 +112,18 @@ def test_batch_with_fp32_lu(mh, oracle, gpu):
 
 @pytest.mark.parametrize("backend", ["tcgen05", "simt"])
 @pytest.mark.parametrize("conj", [False, True])
-@pytest.mark.parametrize("n,nrhs", [(40, 2), (64, 1), (200, 3), (256, 4), (320, 5), (517, 16), (1024, 16)])
+@pytest.mark.parametrize("n,nrhs", [(40, 2), (64, 1), (130, 3), (200, 3), (256, 4), (320, 5), (517, 16),
+                                    (1024, 16), (1100, 4), (1101, 3)])
 def test_lowp_solve_matches_its_factors(mh, gpu, backend, conj, n, nrhs):
     """The FP32 block substitution of a refinement step (L U X = B, or
     (L U)^H X = B for the adjoint) against the same factors solved in FP64:
     sizes with a partial last block, one block, whole blocks only; one to
-    four right-hand sides (each count its own compile-time variant) and more;
-    at 1024 x 16 the next block is not staged in shared memory (two CTAs would
-    no longer fit on an SM) and is loaded after the wait instead."""
+    four right-hand sides (each count its own compile-time variant) and more.
+    Even sizes with one to four right-hand sides take the streamed
+    left-looking solve of the tensor-core backend (its partial last block:
+    130 and 1100); odd sizes and more right-hand sides the flag-synchronised
+    right-looking one, where at 1024 x 16 the next block is not staged in
+    shared memory (two CTAs would no longer fit on an SM)."""
     rng = np.random.default_rng(10 * n + nrhs)
     A = _bem_like(rng, 2, n)
     B = rng.normal(size=(2, n, nrhs)) + 1j * rng.normal(size=(2, n, nrhs))
