@@ -1504,8 +1504,9 @@ constexpr uint32_t kSsStageBytes = kSsTileBytes + kSsYBytes;
 constexpr int kSsConsumers = 256;
 constexpr int kSsThreads = kSsConsumers + 64;  // eight consumer warps, the tile warp and the y warp
 constexpr size_t kSsSmemBytes = (size_t)kSsStages * kSsStageBytes + kSsYBytes;  // + x_i of the block being solved
-constexpr int kSsWaitPolls = 1 << 17;     // bounded stage waits (each poll sleeps >= 64 ns: > 8 ms in all) ...
-constexpr int kSsFlagPolls = 1 << 17;     // ... and flag waits, as long as k_lu_solve_flags' flag waits
+constexpr int kSsWaitPolls = 1 << 14;     // bounded stage waits (polls suspending up to kSsWaitHintNs each) ...
+constexpr uint32_t kSsWaitHintNs = 1000;
+constexpr int kSsFlagPolls = 1 << 17;     // ... and flag waits (> 8 ms), as long as k_lu_solve_flags' flag waits
 
 __device__ __forceinline__ void ss_bar_init(uint64_t* bar, int count)
 {
@@ -1519,13 +1520,12 @@ __device__ __forceinline__ bool ss_wait(uint64_t* bar, uint32_t phase)
         uint32_t ok;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
             "selp.b32 %0, 1, 0, p;\n\t}\n"
             : "=r"(ok)
-            : "r"(a), "r"(phase)
+            : "r"(a), "r"(phase), "r"(kSsWaitHintNs)
             : "memory");
         if (ok) return true;
-        __nanosleep(64);
     }
     return false;
 }
@@ -1567,6 +1567,42 @@ __device__ __forceinline__ int ss_own(int tri, int nblk, int rank, int bi)
 // Tiles of block i (the blocks before it in the triangle's order) and the jj-th of them.
 __device__ __forceinline__ int ss_ntiles(int tri, int nblk, int i) { return tri == 0 ? i : nblk - 1 - i; }
 __device__ __forceinline__ int ss_tile_j(int tri, int nblk, int jj) { return tri == 0 ? jj : nblk - 1 - jj; }
+
+// x_i -= T_ij y_j for one staged tile, as partial sums of row r over the
+// thread's 16 columns (reduced over the row's lanes once per block).  kMask:
+// a tile at the matrix's edge, whose rows past the end (!rok) and columns
+// from jlim on are stale shared memory and count as zero (n even: columns c
+// and c + 1 are valid together).
+template <bool kCT, int NQ, bool kMask>
+__device__ inline void ss_tile(const float2* __restrict__ st, const float2 (*__restrict__ ys)[64], int r,
+                                        int tq, bool rok, int jlim, float (&ax)[4], float (&ay)[4])
+{
+    float2 m[kFsPer];
+#pragma unroll
+    for (int e = 0; e < kFsPer; ++e) {
+        const int c = fs_t(e, tq);
+        m[e] = kCT ? fs_conj(st[r * kSsLd + c]) : st[c * kSsLd + r];
+        if (kMask && !(rok && c < jlim)) m[e] = make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int e = 0; e < kFsPer; e += 2) {
+        const int c = fs_t(e, tq);
+#pragma unroll
+        for (int qq = 0; qq < NQ; ++qq) {
+            float4 v = fs_lds4(&ys[qq][c]);  // volatile: the loads stay in the loop, beside their FMAs
+            if (kMask && c >= jlim) v = make_float4(0.f, 0.f, 0.f, 0.f);
+            const float2 a = m[e], a2 = m[e + 1];
+            ax[qq] = fmaf(a.x, v.x, ax[qq]);
+            ax[qq] = fmaf(-a.y, v.y, ax[qq]);
+            ay[qq] = fmaf(a.x, v.y, ay[qq]);
+            ay[qq] = fmaf(a.y, v.x, ay[qq]);
+            ax[qq] = fmaf(a2.x, v.z, ax[qq]);
+            ax[qq] = fmaf(-a2.y, v.w, ax[qq]);
+            ay[qq] = fmaf(a2.x, v.w, ay[qq]);
+            ay[qq] = fmaf(a2.y, v.z, ay[qq]);
+        }
+    }
+}
 
 template <bool kCT, int NQ>
 __global__ void __cluster_dims__(kFsCluster, 1, 1) __launch_bounds__(kSsThreads, 2)
@@ -1726,32 +1762,11 @@ k_lu_solve_stream(const float2* __restrict__ A, int64_t n, int64_t stride, const
             for (int jj = 0; jj < nt; ++jj) {
                 const int s = t % kSsStages;
                 const int64_t j0 = (int64_t)ss_tile_j(tri, nblk, jj) * NB;
-                const bool whole = i0 + NB <= n && j0 + NB <= n;
                 take(s);
-                const float2* st = stage(s);
-                float2 m[kFsPer];
-#pragma unroll
-                for (int e = 0; e < kFsPer; ++e) {
-                    const int c = fs_t(e, tq);
-                    m[e] = kCT ? fs_conj(st[r * kSsLd + c]) : st[c * kSsLd + r];
-                    if (!whole && !(rok && j0 + c < n)) m[e] = make_float2(0.f, 0.f);
-                }
-                const float2 (*ys)[NB] = ystage(s);
-#pragma unroll
-                for (int e = 0; e < kFsPer; e += 2) {
-                    const int c = fs_t(e, tq);
-                    const bool cok = whole || j0 + c < n;  // n even: c and c + 1 together
-#pragma unroll
-                    for (int qq = 0; qq < NQ; ++qq) {
-                        float4 v = fs_lds4(&ys[qq][c]);
-                        if (!cok) v = make_float4(0.f, 0.f, 0.f, 0.f);
-                        const float2 a = m[e], a2 = m[e + 1];
-                        ax[qq] += a.x * v.x - a.y * v.y;
-                        ay[qq] += a.x * v.y + a.y * v.x;
-                        ax[qq] += a2.x * v.z - a2.y * v.w;
-                        ay[qq] += a2.x * v.w + a2.y * v.z;
-                    }
-                }
+                if (i0 + NB <= n && j0 + NB <= n)  // the whole tile inside the matrix: no masks
+                    ss_tile<kCT, NQ, false>(stage(s), ystage(s), r, tq, true, NB, ax, ay);
+                else
+                    ss_tile<kCT, NQ, true>(stage(s), ystage(s), r, tq, rok, (int)min((int64_t)NB, n - j0), ax, ay);
                 give(s);
             }
 #pragma unroll
