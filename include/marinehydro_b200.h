@@ -224,6 +224,54 @@ int mh_mesh_create(mh_ctx* ctx, int64_t nfaces, int64_t nvertices,
  * without synchronising the device (with ctx = NULL it is freed at once). */
 int mh_mesh_destroy(mh_ctx* ctx, mh_mesh* mesh);
 int mh_mesh_nfaces(const mh_mesh* mesh, int64_t* nfaces);
+int mh_mesh_nvertices(const mh_mesh* mesh, int64_t* nvertices);
+
+/* ---- meshes generated on the device, and their derivatives --------------
+ * Vertices, faces and panel fields computed by kernels straight into the
+ * mesh's device geometry (no host arrays in, one copy of the faces back to
+ * the host), with the exact derivative of every field with respect to the
+ * generator's parameters.  Replaces the reference's mesh generators
+ * (src/meshes.jl:247-479; the hemispheres its tests and paper scripts load
+ * from Capytaine's mesh_sphere, src/meshes.jl:122-127) and the
+ * finite-difference rrules that differentiate them
+ * (paper/MeshGradients_singlebody.jl:85-167, paper/meshGradients_pair.jl:100-210).
+ *
+ * Immersed half (z <= cz) of a latitude-longitude sphere of the given radius
+ * and centre: ceil(ntheta / 2) polar bands of nphi sectors, the bottom band
+ * triangles stored as quads with a repeated vertex; panel radius = largest
+ * vertex distance.  Parameters, in order: radius, cx, cy, cz. */
+int mh_mesh_hemisphere(mh_ctx* ctx, double radius, double cx, double cy, double cz, int ntheta, int nphi,
+                       mh_mesh** out);
+/* The WaveBot buoy (src/meshes.jl:458-479): top radius r1, bottom radius r2
+ * (both > 0), cylinder height d1, frustum height d2, profile points
+ * (n_bottom, n_frustum, n_cylinder) revolved with n_theta sectors; panel
+ * radius = distance to the first vertex (src/meshes.jl:353-423).
+ * Parameters, in order: r1, r2, d1, d2. */
+int mh_mesh_wavebot(mh_ctx* ctx, double r1, double r2, double d1, double d2, int n_bottom, int n_frustum,
+                    int n_cylinder, int n_theta, mh_mesh** out);
+/* Concatenation of meshes of this ctx's device (combine_meshes,
+ * src/meshes.jl:53-99, with cumulative vertex offsets); the inputs stay
+ * valid.  The parameters of the result are those of its generated parts in
+ * order (an uploaded mesh has none). */
+int mh_mesh_combine(mh_ctx* ctx, int count, const mh_mesh* const* meshes, mh_mesh** out);
+int mh_mesh_nparams(const mh_mesh* mesh, int* nparams);
+/* The mesh's fields, in the layouts of mh_mesh_create, into host or device
+ * buffers (each may be NULL). */
+int mh_mesh_fields(mh_ctx* ctx, const mh_mesh* mesh, double* vertices, int64_t* faces, double* centers,
+                   double* normals, double* areas, double* radii);
+/* Forward mode: the derivative of every field with respect to parameter
+ * `param` (0 <= param < mh_mesh_nparams), computed on the device, into host
+ * or device buffers in the layouts of mh_mesh_fields (each may be NULL);
+ * these are the t_* arguments of mh_hydro_batch_jvp. */
+int mh_mesh_tangent(mh_ctx* ctx, const mh_mesh* mesh, int param, double* t_vertices, double* t_centers,
+                    double* t_normals, double* t_areas, double* t_radii);
+/* Reverse mode: the cotangents of the parameters (bar_params, host,
+ * mh_mesh_nparams of them) from the cotangents of the fields (host or
+ * device, each may be NULL = zero), e.g. the d_* outputs of
+ * mh_hydro_batch_vjp: bar_params[p] = sum over fields of bar . tangent_p. */
+int mh_mesh_param_vjp(mh_ctx* ctx, const mh_mesh* mesh, const double* bar_vertices, const double* bar_centers,
+                      const double* bar_normals, const double* bar_areas, const double* bar_radii,
+                      double* bar_params);
 
 /* ---- matrix level ------------------------------------------------------ */
 

@@ -97,6 +97,16 @@ SIGNATURES = {
                                       ctypes.POINTER(_P)]),
     "mh_mesh_destroy": (ctypes.c_int, [_P, _P]),
     "mh_mesh_nfaces": (ctypes.c_int, [_P, _I64]),
+    "mh_mesh_nvertices": (ctypes.c_int, [_P, _I64]),
+    "mh_mesh_hemisphere": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_int, ctypes.c_int, ctypes.POINTER(_P)]),
+    "mh_mesh_wavebot": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_P)]),
+    "mh_mesh_combine": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(_P), ctypes.POINTER(_P)]),
+    "mh_mesh_nparams": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
+    "mh_mesh_fields": (ctypes.c_int, [_P, _P, _D, _I64, _D, _D, _D, _D]),
+    "mh_mesh_tangent": (ctypes.c_int, [_P, _P, ctypes.c_int, _D, _D, _D, _D, _D]),
+    "mh_mesh_param_vjp": (ctypes.c_int, [_P, _P, _D, _D, _D, _D, _D, _D]),
     "mh_assemble_matrices": (ctypes.c_int, [_P, _P, ctypes.c_double, ctypes.c_uint32, ctypes.c_int,
                                             _D, _D]),
     "mh_assemble_matrices_device": (ctypes.c_int, [_P, _P, ctypes.c_double, ctypes.c_uint32,

@@ -752,6 +752,10 @@ int mh_mesh_create(mh_ctx* ctx, int64_t nfaces, int64_t nvertices, const double*
     m->device = ctx->device;
     try {
         m->faces.assign(faces, faces + 4 * n);
+        MeshPart part;
+        part.nf = n;
+        part.nv = nvertices;
+        m->parts.push_back(part);
     } catch (...) {
         delete[] h;
         delete m;
@@ -762,10 +766,16 @@ int mh_mesh_create(mh_ctx* ctx, int64_t nfaces, int64_t nvertices, const double*
     // come and go without stalling other contexts
     cudaError_t e = cudaMallocAsync((void**)&m->geom, bytes, ctx->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(m->geom, h, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    // the vertices too, so that the mesh can be combined with generated ones
+    if (e == cudaSuccess) e = cudaMallocAsync((void**)&m->verts, sizeof(double) * 3 * (size_t)nvertices, ctx->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(m->verts, vertices, sizeof(double) * 3 * (size_t)nvertices, cudaMemcpyHostToDevice,
+                            ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     delete[] h;
     if (e != cudaSuccess) {
         if (m->geom) cudaFree(m->geom);
+        if (m->verts) cudaFree(m->verts);
         delete m;
         return set_err(ctx, e == cudaErrorMemoryAllocation ? MH_ERR_OOM : MH_ERR_CUDA,
                        "mesh upload failed: %s", cudaGetErrorString(e));
@@ -782,8 +792,10 @@ int mh_mesh_destroy(mh_ctx* ctx, mh_mesh* mesh)
         // or synchronising the device
         cudaSetDevice(ctx->device);
         if (mesh->geom) cudaFreeAsync(mesh->geom, ctx->stream);
-    } else if (mesh->geom) {
-        cudaFree(mesh->geom);
+        if (mesh->verts) cudaFreeAsync(mesh->verts, ctx->stream);
+    } else {
+        if (mesh->geom) cudaFree(mesh->geom);
+        if (mesh->verts) cudaFree(mesh->verts);
     }
     delete mesh;
     return MH_OK;

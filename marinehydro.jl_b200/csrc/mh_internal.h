@@ -22,12 +22,28 @@ enum GeomField : int {
     G_NFIELDS = 20
 };
 
+// One generated part of a mesh (mh_mesh_hemisphere, mh_mesh_wavebot), kept so
+// that the mesh's fields can be differentiated with respect to the part's
+// parameters on the device; a part of kind MESH_UPLOADED has none.
+enum MeshKind : int { MESH_UPLOADED = 0, MESH_HEMISPHERE = 1, MESH_WAVEBOT = 2 };
+constexpr int kMeshPartParams = 4;
+struct MeshPart {
+    int kind = MESH_UPLOADED;
+    double p[kMeshPartParams] = {};  // hemisphere: radius, cx, cy, cz; wavebot: r1, r2, d1, d2
+    int ip[4] = {};                  // hemisphere: bands, sectors; wavebot: n_bottom, n_frustum, n_cylinder, n_theta
+    int64_t f0 = 0, nf = 0;          // its faces ...
+    int64_t v0 = 0, nv = 0;          // ... and vertices in the mesh
+    int radius_max = 0;              // panel radius: 1 largest vertex distance, 0 distance to the first vertex
+};
+
 struct mh_mesh {
     int64_t n = 0;
     int64_t nv = 0;
     int device = 0;
     double* geom = nullptr;      // device, G_NFIELDS * n doubles
     std::vector<int64_t> faces;  // host copy, 4 x n column-major (vertex cotangent scatter)
+    double* verts = nullptr;     // device, nv x 3 column-major (generated and combined meshes)
+    std::vector<MeshPart> parts; // generated and combined meshes: their parts in order
 };
 
 // Workspace slots of a context; each is a grow-only device buffer.

@@ -48,6 +48,10 @@ def test_null_arguments_rejected_without_device(mh):
     assert L.mh_device_count(None) == mh.native.MH_ERR_ARG
     assert L.mh_ctx_destroy(None) == 0
     assert L.mh_mesh_nfaces(None, None) == mh.native.MH_ERR_ARG
+    assert L.mh_mesh_nvertices(None, None) == mh.native.MH_ERR_ARG
+    assert L.mh_mesh_nparams(None, None) == mh.native.MH_ERR_ARG
+    assert L.mh_mesh_hemisphere(None, 1.0, 0.0, 0.0, 0.0, 10, 10, None) == mh.native.MH_ERR_ARG
+    assert L.mh_mesh_wavebot(None, 0.88, 0.35, 0.16, 0.37, 5, 10, 5, 72, None) == mh.native.MH_ERR_ARG
 
 
 @pytest.mark.parametrize("res,nf", [((10, 10), 50), ((32, 64), 1024), ((64, 64), 2048),
