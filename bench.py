@@ -862,7 +862,7 @@ def run_design_batch(mh, args, torch):
     return {"value": nprob / dt, "unit": "solves/s (each with dA/dR, dB/dR)", "ms_per_batch": dt * 1e3,
             "workload": "design_population_48_hemispheres_64_to_1640p_16omega_heave_delhommeau",
             "panels_total": int(sum(r.nfaces for r in res)), "contexts": len(ctxs),
-            "timing": "host wall clock around design_batch (mesh generation, uploads, forward + tangent)",
+            "timing": "host wall clock around design_batch (meshes and radius tangents generated on the device, forward + tangent)",
             "fp64_gpu": {"value": nprob / dt64, "unit": "solves/s", "ms_per_batch": dt64 * 1e3,
                          "mode": "FP64 path one frequency at a time, same contexts"},
             "accuracy_dA_dR_vs_fp64": acc}

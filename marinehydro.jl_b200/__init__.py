@@ -23,7 +23,7 @@ from .gradients import (MeshTangent, VjpResult, JvpResult, hydro_batch_vjp, hydr
                         hemisphere_tangents, two_hemispheres_tangents, polygon_geometry_jvp,
                         wavebot_tangents)
 from .meshgen import (GeneratedMesh, generate_hemisphere, generate_two_hemispheres, generate_wavebot,
-                      generate_combined, generated_tangents, generated_param_grad)
+                      generate_combined, generated_tangents, generated_tangent, generated_param_grad)
 from .power import two_body_power, optimize_two_body_power
 from .design import SplitMix64, Design, designs, design_batch
 from ._native import (Context, MarineHydroError, ArgumentError, NotConvergedError,

@@ -23,8 +23,9 @@ import numpy as np
 
 from .api import ExactGuevelDelhommeau, Rankine, RankineReflected
 from .bodies import FloatingBody
-from .gradients import hemisphere_tangents, hydro_batch_jvp
-from .meshes import mesh_hemisphere
+from ._native import default_context
+from .gradients import hydro_batch_jvp
+from .meshgen import generate_hemisphere, generated_tangent
 
 _MASK64 = (1 << 64) - 1
 
@@ -72,9 +73,11 @@ class DesignResult:
 
 
 def _one_design(d: Design, om, gfs, precision, tol, ctx) -> DesignResult:
-    mesh = mesh_hemisphere(d.radius, (0.0, 0.0, 0.0), d.resolution)
+    # the mesh and its radius tangent made on the device (no host generation
+    # or upload on the design loop's host threads)
+    mesh = generate_hemisphere(d.radius, (0.0, 0.0, 0.0), d.resolution, ctx=ctx or default_context())
     body = FloatingBody.rigid(mesh, ["Heave"])
-    tan = hemisphere_tangents(d.radius, (0.0, 0.0, 0.0), d.resolution, mesh=mesh)["radius"]
+    tan = generated_tangent(mesh, "radius")
     r = hydro_batch_jvp(mesh, om, list(body.dofs.values()), (), tan, green_functions=gfs,
                         precision=precision, tol=tol, ctx=ctx)
     return DesignResult(d, mesh.nfaces, r.added_mass[0, 0].copy(), r.damping[0, 0].copy(),

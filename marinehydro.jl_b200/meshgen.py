@@ -162,6 +162,14 @@ def generated_tangents(mesh: Mesh) -> dict:
     return {nm: gm.tangent(p) for p, nm in enumerate(gm.param_names)}
 
 
+def generated_tangent(mesh: Mesh, name: str) -> MeshTangent:
+    """The tangent of one generator parameter (see ``generated_tangents``)."""
+    gm = generated_mesh(mesh)
+    if name not in gm.param_names:
+        raise ValueError(f"{name!r} is not a parameter of this mesh: {gm.param_names}")
+    return gm.tangent(gm.param_names.index(name))
+
+
 def generated_param_grad(mesh: Mesh, cotangent: MeshTangent) -> dict:
     """{parameter name: cotangent}: a mesh cotangent (``VjpResult.mesh`` of
     ``hydro_batch_vjp``) pulled back to the generator's parameters on the
