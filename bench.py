@@ -793,9 +793,10 @@ def oracle_accuracy(omegas, mixed, args):
 def run_two_body(mh, ctx, args, torch):
     """Grads of the two-body power objective (paper/Power.jl:13-83): two
     1024-panel hemispheres 5 m apart, Wu, indirect, omega = 1.03; one grad =
-    J and dJ/d(r1, dx1, omega) through two_body_power(grad=True) (mesh
-    generation and tangents on the host, forward + adjoint batch on the
-    device), timed end to end; against the oracle's central differences."""
+    J and dJ/d(r1, dx1, omega) through two_body_power(grad=True) (meshes
+    generated on the device, forward + adjoint batch, the mesh cotangent
+    pulled back to the parameters on the device), timed end to end; against
+    the oracle's central differences."""
     kw = dict(resolution=(32, 64), direct=False, tol=args.tol, ctx=ctx)
 
     def call(prec):
@@ -816,7 +817,7 @@ def run_two_body(mh, ctx, args, torch):
     dt64 = time.perf_counter() - t0
     out = {"value": 1.0 / dt, "unit": "grads/s", "ms_per_grad": dt * 1e3,
            "workload": "two_hemispheres_2x1024p_wu_indirect_power_grad", "panels": 2048,
-           "timing": "host wall clock around the public call (mesh generation, upload, forward, adjoint)",
+           "timing": "host wall clock around the public call (meshes generated on the device, forward, adjoint, parameter pull-back)",
            "J": J, "grad": g, "fp64_gpu": {"value": 1.0 / dt64, "unit": "grads/s", "ms_per_grad": dt64 * 1e3}}
     path = ROOT / "tests" / "golden" / "two_hemispheres_2048p_wu.npz"
     if path.exists():

@@ -15,8 +15,9 @@ rho = 1000 (src/waves.jl:150-153).
 
 `two_body_power(..., grad=True)` returns dJ/d(r1, dx1, omega): the small
 2x2 algebra is differentiated with torch autograd on the host (exact), the
-boundary-element part with one `mh_hydro_batch_vjp` call and the exact mesh
-tangents of the generator.
+boundary-element part with one `mh_hydro_batch_vjp` call, whose mesh
+cotangent is pulled back to the generator parameters on the device
+(`mh_mesh_param_vjp`): the two hemispheres are generated there.
 """
 from __future__ import annotations
 
@@ -24,22 +25,25 @@ import math
 
 import numpy as np
 
+from ._native import default_context
 from .api import GFWu, Rankine, RankineReflected
 from .bodies import FloatingBody, hydro_batch
-from .gradients import MeshTangent, hemisphere_tangents, hydro_batch_vjp
-from .meshes import mesh_hemisphere
+from .gradients import hydro_batch_vjp
+from .meshgen import generate_combined, generate_hemisphere, generated_param_grad
 
 RHO = 1000.0
 RHO_DIFFRACTION = 1023.0
 G = 9.81
 
 
-def _bodies(r1, dx1, resolution):
-    m1 = mesh_hemisphere(r1, (0.0, 0.0, 0.0), resolution)
-    m2 = mesh_hemisphere(r1, (r1 + dx1, 0.0, 0.0), resolution)
+def _bodies(r1, dx1, resolution, ctx):
+    """The two heaving bodies (their dofs) and their mesh, generated on the
+    device (parameters radius0, cx0, cy0, cz0, radius1, cx1, cy1, cz1)."""
+    m1 = generate_hemisphere(r1, (0.0, 0.0, 0.0), resolution, ctx)
+    m2 = generate_hemisphere(r1, (r1 + dx1, 0.0, 0.0), resolution, ctx)
     both = FloatingBody.rigid(m1, ["Heave"], body_name="sphere") + \
         FloatingBody.rigid(m2, ["Heave"], body_name="sphere")
-    return both
+    return both, generate_combined([m1, m2], ctx)
 
 
 def _objective(A11, A12, B11, B12, F1r, F1i, F2r, F2i, K1r, K1i, K2r, K2i, w, r1):
@@ -71,11 +75,12 @@ def two_body_power(r1: float = 1.0, dx1: float = 4.0, omega: float = 1.03, *, re
     import torch
 
     gfs = green_functions or (Rankine(), RankineReflected(), GFWu())
-    body = _bodies(r1, dx1, resolution)
+    ctx = ctx or default_context()
+    body, mesh = _bodies(r1, dx1, resolution, ctx)
     dofs = list(body.dofs.values())
     om = np.array([omega])
     kw = dict(green_functions=gfs, direct=direct, precision=precision, tol=tol, rho=RHO, g=G, ctx=ctx)
-    A, B, Fd, Fk, _ = hydro_batch(body.mesh, om, dofs, [0.0], **kw)
+    A, B, Fd, Fk, _ = hydro_batch(mesh, om, dofs, [0.0], **kw)
     # outputs used by Power.jl: radiation of sphere 1 (A[:, 0]), forces on both
     leaves = [A[0, 0, 0], A[1, 0, 0], B[0, 0, 0], B[1, 0, 0],
               Fd[0, 0, 0].real, Fd[0, 0, 0].imag, Fd[1, 0, 0].real, Fd[1, 0, 0].imag,
@@ -95,20 +100,11 @@ def two_body_power(r1: float = 1.0, dx1: float = 4.0, omega: float = 1.03, *, re
     bF[1, 0, 0] = g[6] + 1j * g[7]
     bK[0, 0, 0] = g[8] + 1j * g[9]
     bK[1, 0, 0] = g[10] + 1j * g[11]
-    r = hydro_batch_vjp(body.mesh, om, dofs, [0.0], bA, bB, bF, bK, **kw)
-    t1 = hemisphere_tangents(r1, (0.0, 0.0, 0.0), resolution)
-    t2 = hemisphere_tangents(r1, (r1 + dx1, 0.0, 0.0), resolution)
-
-    def cat(a: MeshTangent, b: MeshTangent) -> MeshTangent:
-        return MeshTangent(np.concatenate([a.vertices, b.vertices]), np.concatenate([a.centers, b.centers]),
-                           np.concatenate([a.normals, b.normals]), np.concatenate([a.areas, b.areas]),
-                           np.concatenate([a.radii, b.radii]))
-
-    zero = MeshTangent.zeros_like(mesh_hemisphere(r1, (0.0, 0.0, 0.0), resolution))
+    r = hydro_batch_vjp(mesh, om, dofs, [0.0], bA, bB, bF, bK, **kw)
+    p = generated_param_grad(mesh, r.mesh)
     # r1 scales both bodies and moves the second centre (x = r1 + dx1)
-    tan_r = cat(t1["radius"], t2["radius"] + t2["cx"])
-    tan_dx = cat(zero, t2["cx"])
-    grads = {"r1": g[13] + r.mesh.dot(tan_r), "dx1": r.mesh.dot(tan_dx), "omega": g[12] + float(r.omegas[0])}
+    grads = {"r1": g[13] + p["radius0"] + p["radius1"] + p["cx1"], "dx1": p["cx1"],
+             "omega": g[12] + float(r.omegas[0])}
     return float(J.detach()), grads
 
 
