@@ -122,6 +122,40 @@ function hydro_batch_vjp(ctx, mesh, omegas, dofs, betas, Abar, Bbar, Fdbar, Fkba
     mesh_bar = Tangent{Mesh}(vertices=dV, centers=dC, normals=dN, areas=dA, radii=dR)
     (mesh_bar, dW, [reshape(dD[(q-1)*3*mesh.nfaces+1:q*3*mesh.nfaces], :, 3) for q in 1:nd])
 end
+
+# Meshes generated on the device (mh_mesh_hemisphere / mh_mesh_wavebot): the
+# WaveBot of src/meshes.jl:458-479 and the hemispheres the paper scripts load;
+# parameters (radius, cx, cy, cz) and (r1, r2, d1, d2).
+function hemisphere_mesh(ctx, radius, center, ntheta, nphi)
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:mh_mesh_hemisphere, lib), Cint,
+        (Ptr{Cvoid}, Float64, Float64, Float64, Float64, Cint, Cint, Ref{Ptr{Cvoid}}),
+        ctx.h, radius, center[1], center[2], center[3], ntheta, nphi, r), ctx.h)
+    m = DeviceMesh(r[], ctx)
+    finalizer(x -> ccall((:mh_mesh_destroy, lib), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), x.ctx.h, x.h), m)
+end
+function wavebot_mesh(ctx, r1, r2, d1, d2; n_points=(5, 10, 5), n_theta=72)
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:mh_mesh_wavebot, lib), Cint,
+        (Ptr{Cvoid}, Float64, Float64, Float64, Float64, Cint, Cint, Cint, Cint, Ref{Ptr{Cvoid}}),
+        ctx.h, r1, r2, d1, d2, n_points[1], n_points[2], n_points[3], n_theta, r), ctx.h)
+    m = DeviceMesh(r[], ctx)
+    finalizer(x -> ccall((:mh_mesh_destroy, lib), Cint, (Ptr{Cvoid}, Ptr{Cvoid}), x.ctx.h, x.h), m)
+end
+# The generator-parameter cotangents of a mesh cotangent (the mesh_bar of
+# hydro_batch_vjp): the device replacement of the finite-difference rrules of
+# paper/MeshGradients_singlebody.jl:85-167.
+function mesh_param_vjp(ctx, dm::DeviceMesh, mesh_bar)
+    np = Ref{Cint}(0)
+    check(ccall((:mh_mesh_nparams, lib), Cint, (Ptr{Cvoid}, Ref{Cint}), dm.h, np), ctx.h)
+    out = zeros(np[])
+    check(ccall((:mh_mesh_param_vjp, lib), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64},
+         Ptr{Float64}),
+        ctx.h, dm.h, mesh_bar.vertices, mesh_bar.centers, mesh_bar.normals, mesh_bar.areas,
+        mesh_bar.radii, out), ctx.h)
+    out
+end
 end
 
 # One Zygote node per batch call (ChainRulesCore):
