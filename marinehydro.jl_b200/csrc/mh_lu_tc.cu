@@ -1859,9 +1859,11 @@ int64_t lu_panel_bytes_tc(int64_t n)
 // 128 to 512 columns; op = 4 by default), with look-ahead.  Outer step K0
 // (tile T0 = K0 / 128), on the main
 // (high-priority) stream: for each panel k = K0 + 64 s, its TRSM, then (but
-// for the last) the update of the rest of the outer block's tile rows and
-// columns (an L of width T0 + op/2 - tile(k + 64) tiles, rows and columns
-// >= k + 64) with that panel alone, and the next diagonal block; then the
+// for the last) the update of the tile row and column holding the next
+// panel (an L of width 1, rows and columns >= k + 64) -- with this panel
+// when the next one is in the same tile, else with all the outer step's
+// panels so far (the next tile's first update in this outer step) -- and
+// the next diagonal block; then the
 // trailing tiles (>= T0 + op/2) are updated once with all op panel pairs
 // accumulated in TMEM (K = 64 op complex): their first op/2 tile rows and
 // columns on the main stream, the interior concurrently on the side
@@ -1932,12 +1934,20 @@ cudaError_t lu_tc_group(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int n
             k_lu_trsm_tc<<<dim3(2 * nt, nbz), 128, kSmemA + kSmemA, main_s>>>(
                 A, n, stride, k, bimg, bstride, (unsigned char*)pp.L[s], (unsigned char*)pp.U[s], pstride, nt, bad);
             ctx->launches += 1;
-            if (s + 1 < op) {  // the rest of the outer block with this panel, then its next diagonal block
-                PanelPairs one;
-                one.L[0] = pp.L[s];
-                one.U[0] = pp.U[s];
-                const int w = std::min(T0 + kW - t0, nt);
-                if ((e = strip(t0, nt, w, one, 1, k + TC_NB)) != cudaSuccess) return e;
+            if (s + 1 < op) {
+                // only the tile holding the next panel (t0) is brought up to
+                // date, left-looking: after the first panel of a tile (s
+                // even), that tile's L with this panel; after the second (s
+                // odd), the next tile's L, untouched in this outer step so
+                // far, with all its panels 0 .. s at once (one pass over it
+                // instead of one per panel); then the next diagonal block
+                PanelPairs q;
+                int np = 0;
+                for (int r = (s & 1) ? 0 : s; r <= s; ++r, ++np) {
+                    q.L[np] = pp.L[r];
+                    q.U[np] = pp.U[r];
+                }
+                if ((e = strip(t0, nt, 1, q, np, k + TC_NB)) != cudaSuccess) return e;
                 k_lu_diag64<<<nbatch, kDiag64Threads, kDiag64Smem, main_s>>>(A, n, stride, k + TC_NB, Dinv, dstride,
                                                                            bad, bimg, bstride);
                 ctx->launches += 1;
