@@ -361,12 +361,16 @@ int mh_ctx_create(int device, mh_ctx** out)
     }
     cublasSetStream(ctx->cublas, ctx->stream);
     cusolverDnSetStream(ctx->cusolver, ctx->stream);
-    // LU schedules the autotuner chose on a B200 (mh_lu_autotune; times in
-    // ms for 16, 64 and 64 matrices): 512 panels, 1 group x 4 panels with C
-    // staged in tensor memory (0.554 vs 0.644 for the default); 1024, 2 x 2
-    // (1.81 vs 1.82); 2048, 2 x 4 (the default).  Other sizes take the
-    // nearest entry; mh_ctx_set_lu_schedule or the autotuner replace them.
-    ctx->lu_table = {{512, LuSchedule{1, 4, 1}}, {1024, LuSchedule{2, 2, 0}}, {2048, LuSchedule{2, 4, 0}}};
+    // LU schedules the autotuner chose on a B200 (mh_lu_autotune, median of
+    // three sweeps over groups 1-4 x 2-8 panels per outer step x both update
+    // kernels; ms against the default 2 x 4): 512 panels x 16 matrices, 1
+    // group x 4 panels with C staged in tensor memory (0.555 vs 0.651);
+    // 1024 x 64, 1 x 4 (1.730 vs 1.736; 1.232 vs 1.413 at 1024 x 16); 1536
+    // x 16, 1 x 4 (2.00 vs 2.20); 2048 x 64, 2 x 8 (5.67 vs 6.27).  Other
+    // sizes take the nearest entry; mh_ctx_set_lu_schedule or the autotuner
+    // replace them.
+    ctx->lu_table = {{512, LuSchedule{1, 4, 1}}, {1024, LuSchedule{1, 4, 0}}, {1536, LuSchedule{1, 4, 0}},
+                     {2048, LuSchedule{2, 8, 0}}};
     *out = ctx;
     return MH_OK;
 }

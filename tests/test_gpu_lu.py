@@ -202,11 +202,15 @@ def test_tcgen05_lu_schedules_reconstruct(mh, gpu, groups, outer, update, n):
     tile."""
     rng = np.random.default_rng(n + 7 * outer + groups)
     A = _bem_like(rng, 5, n)
-    gpu.set_lu_schedule(0, groups, outer, update)
+    # a context of its own: an entry for this size in its schedule table (a
+    # size takes the nearest entry, so the default alone would not be used)
+    ctx = mh.Context(0)
     try:
-        LU, bad = gpu.lu_factor_lowp(A, "tcgen05")
+        ctx.set_lu_schedule(n, groups, outer, update)
+        assert ctx.lu_schedule(n) == (groups, outer, update)
+        LU, bad = ctx.lu_factor_lowp(A, "tcgen05")
     finally:
-        gpu.set_lu_schedule(0, 2, 4)
+        ctx.close()
     assert not bad.any()
     for b in range(A.shape[0]):
         R = _reconstruct(LU[b].astype(np.complex128))
@@ -219,9 +223,9 @@ def test_builtin_lu_schedule_table(mh):
     ctx = mh.Context(0)
     try:
         assert ctx.lu_schedule(512) == (1, 4, 1)
-        assert ctx.lu_schedule(1024) == (2, 2, 0)
-        assert ctx.lu_schedule(2048) == (2, 4, 0)
-        assert ctx.lu_schedule(1640) == (2, 4, 0) and ctx.lu_schedule(64) == (1, 4, 1)
+        assert ctx.lu_schedule(1024) == (1, 4, 0)
+        assert ctx.lu_schedule(2048) == (2, 8, 0)
+        assert ctx.lu_schedule(1640) == (1, 4, 0) and ctx.lu_schedule(64) == (1, 4, 1)
         assert ctx.lu_schedule(0) == (2, 4, 0)
     finally:
         ctx.close()
