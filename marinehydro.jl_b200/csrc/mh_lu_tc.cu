@@ -329,7 +329,7 @@ k_lu_trsm_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
 }
 
 // Packed panel pairs of one update (one per 64-column panel).
-constexpr int kMaxPairs = 8;
+constexpr int kMaxPairs = 16;  // an outer step's panels (8 at most) and the previous step's deferred ones
 struct PanelPairs {
     const unsigned char* L[kMaxPairs];
     const unsigned char* U[kMaxPairs];
@@ -412,7 +412,7 @@ __device__ __forceinline__ bool epilogue_bulk(float2* M, int64_t n, int64_t r0, 
 }
 
 // A22 -= sum_p L21_p U12_p for one 128 x 128 complex tile (absolute tiles
-// ti, tj); the operands are the packed panels of k_lu_trsm_tc (npair <= 8
+// ti, tj); the operands are the packed panels of k_lu_trsm_tc (npair <= 16
 // panel pairs, K = 64 complex each), fetched by cp.async.bulk into shared
 // memory one pair at a time and accumulated in tensor memory.  Only rows and
 // columns >= lo are written.  Tiles, relative to t0 (ntile of them per side):
@@ -1847,7 +1847,7 @@ cudaError_t launch_fill_lu_test(mh_ctx* ctx, float2* A, int64_t n, int nbatch)
 // Panel buffers per matrix: the panel pairs of an outer step stay live while
 // its interior update runs, and the next outer step writes the other set
 // (2 x the outer step's panels, sized for the widest schedule).
-constexpr int kOuterMax = kMaxPairs;  // 64-column panels per outer step, at most (512 columns)
+constexpr int kOuterMax = 8;  // 64-column panels per outer step, at most (512 columns)
 // After them, the packed TRSM B operands of every diagonal block (two images each).
 int64_t lu_panel_bytes_tc(int64_t n)
 {
@@ -1914,6 +1914,8 @@ cudaError_t lu_tc_group(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int n
                                                                    bstride);
     ctx->launches += 1;
     int outer = 0;
+    PanelPairs prev;  // the previous outer step's panels (their update of this step's tiles past the first is deferred)
+    int nprev = 0;
     for (int64_t K0 = 0; K0 < n; K0 += op * TC_NB, ++outer) {
         const int T0 = (int)(K0 / TC_TM);
         PanelPairs pp;
@@ -1938,11 +1940,18 @@ cudaError_t lu_tc_group(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int n
                 // only the tile holding the next panel (t0) is brought up to
                 // date, left-looking: after the first panel of a tile (s
                 // even), that tile's L with this panel; after the second (s
-                // odd), the next tile's L, untouched in this outer step so
-                // far, with all its panels 0 .. s at once (one pass over it
-                // instead of one per panel); then the next diagonal block
+                // odd), the next tile's L, untouched since the previous outer
+                // step's first tile update, with the previous step's panels
+                // and all of this step's panels 0 .. s at once (one pass over
+                // it instead of one per outer step and panel); then the next
+                // diagonal block
                 PanelPairs q;
                 int np = 0;
+                if (s & 1)
+                    for (int r = 0; r < nprev; ++r, ++np) {
+                        q.L[np] = prev.L[r];
+                        q.U[np] = prev.U[r];
+                    }
                 for (int r = (s & 1) ? 0 : s; r <= s; ++r, ++np) {
                     q.L[np] = pp.L[r];
                     q.U[np] = pp.U[r];
@@ -1964,6 +1973,10 @@ cudaError_t lu_tc_group(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int n
         if ((e = strip_join()) != cudaSuccess) return e;
         if ((e = cudaEventRecord(st.ev_panel, main_s)) != cudaSuccess) return e;
         if ((e = cudaStreamWaitEvent(side_s, st.ev_panel, 0)) != cudaSuccess) return e;
+        // the interior: tiles past the next outer step's tiles, on the side
+        // stream; the next outer step's first tile row and column now (its
+        // first panel needs them), its other tiles' rows and columns with
+        // these panels when that step reaches them (deferred, above)
         const int w = std::min(kW, nt);
         if (nt > w) {
             upd<<<dim3(nt - w, nt - w, nbz), 128, kTcSmemBytes, side_s>>>(
@@ -1971,7 +1984,9 @@ cudaError_t lu_tc_group(mh_ctx* ctx, float2* A, int64_t n, int64_t stride, int n
             ctx->launches += 1;
         }
         if ((e = cudaEventRecord(st.ev_side, side_s)) != cudaSuccess) return e;
-        if ((e = strip(t0, nt, w, pp, op, lo)) != cudaSuccess) return e;
+        if ((e = strip(t0, nt, 1, pp, op, lo)) != cudaSuccess) return e;
+        prev = pp;
+        nprev = op;
         if (lo < n) {
             k_lu_diag64<<<nbatch, kDiag64Threads, kDiag64Smem, main_s>>>(A, n, stride, lo, Dinv, dstride, bad,
                                                                          bimg, bstride);
