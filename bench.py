@@ -668,11 +668,13 @@ FP32_PEAK_TFLOPS = 74.5
 # Of the per pair-frequency operations, the Horner series (112) runs in FP32
 # at the mixed path's default series level (1), the rest (51) in FP64.
 WAVE_FP32_FLOPS_PER_PAIR_FREQ = 112.0
-# DRAM bytes of the LU phase per matrix of 2048, from ncu captures of the
-# three LU kernels (the FP32 Schur complement re-read and re-written once per
-# 256-column outer step, the in-block updates, panels and diagonal blocks):
-# 16.7 GB per 64 matrices.
-LU_DRAM_BYTES_PER_MATRIX_2048 = 16.7e9 / 64
+# DRAM bytes of the LU phase per matrix of 2048, from an ncu capture of the
+# three LU kernels over one factorisation of 16 matrices of 2048 with the
+# default schedule (2 groups x 8 panels per outer step; the FP32 Schur
+# complement re-read once per 512-column outer step, the left-looking tile
+# updates, panels and diagonal blocks): 3.677 GB / 16 = 229.8 MB per matrix
+# (14.7 GB per 64; 16.7 GB with 256-column steps and right-looking strips).
+LU_DRAM_BYTES_PER_MATRIX_2048 = 3.677e9 / 16
 
 
 def roofline(per_phase, n, args):
