@@ -1504,8 +1504,8 @@ constexpr uint32_t kSsStageBytes = kSsTileBytes + kSsYBytes;
 constexpr int kSsConsumers = 256;
 constexpr int kSsThreads = kSsConsumers + 64;  // eight consumer warps, the tile warp and the y warp
 constexpr size_t kSsSmemBytes = (size_t)kSsStages * kSsStageBytes + kSsYBytes;  // + x_i of the block being solved
-constexpr int kSsWaitPolls = 1 << 14;     // bounded stage waits (polls suspending up to kSsWaitHintNs each) ...
-constexpr uint32_t kSsWaitHintNs = 1000;
+constexpr uint64_t kSsWaitNs = 50000000;   // bounded stage waits: 50 ms of the global timer (a poll may
+constexpr uint32_t kSsWaitHintNs = 1000;    // return before its suspend hint, so the bound is in time) ...
 constexpr int kSsFlagPolls = 1 << 17;     // ... and flag waits (> 8 ms), as long as k_lu_solve_flags' flag waits
 
 __device__ __forceinline__ void ss_bar_init(uint64_t* bar, int count)
@@ -1516,7 +1516,9 @@ __device__ __forceinline__ void ss_bar_init(uint64_t* bar, int count)
 __device__ __forceinline__ bool ss_wait(uint64_t* bar, uint32_t phase)
 {
     const uint32_t a = smem_u32(bar);
-    for (int it = 0; it < kSsWaitPolls; ++it) {
+    uint64_t t0;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    for (;;) {
         uint32_t ok;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -1526,8 +1528,10 @@ __device__ __forceinline__ bool ss_wait(uint64_t* bar, uint32_t phase)
             : "r"(a), "r"(phase), "r"(kSsWaitHintNs)
             : "memory");
         if (ok) return true;
+        uint64_t t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        if (t - t0 > kSsWaitNs) return false;
     }
-    return false;
 }
 
 __device__ __forceinline__ void ss_arrive(uint64_t* bar)
