@@ -174,6 +174,16 @@ __device__ __forceinline__ void mma_k128(uint32_t tmem, uint32_t a0, uint32_t lb
                  :: "r"(bar) : "memory");
 }
 
+// Eight consecutive FP32 words of a TMEM read-back (x[o .. o + 7], o a
+// compile-time offset after unrolling) as FP16, times sign.
+__device__ __forceinline__ uint4 pack8u(const uint32_t (&x)[32], int o, float sign)
+{
+    return make_uint4(pack_h2(sign * __uint_as_float(x[o]), sign * __uint_as_float(x[o + 1])),
+                      pack_h2(sign * __uint_as_float(x[o + 2]), sign * __uint_as_float(x[o + 3])),
+                      pack_h2(sign * __uint_as_float(x[o + 4]), sign * __uint_as_float(x[o + 5])),
+                      pack_h2(sign * __uint_as_float(x[o + 6]), sign * __uint_as_float(x[o + 7])));
+}
+
 __device__ __forceinline__ uint4 pack8(const float2* v, bool imag, float sign)
 {
     if (imag)
@@ -278,21 +288,21 @@ k_lu_trsm_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
             tmem_ld32(lane_base + (uint32_t)(half * 32), re);
             tmem_ld32(lane_base + (uint32_t)(64 + half * 32), im);
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            float2 v[32];
+            if (!okr) {
 #pragma unroll
-            for (int q = 0; q < 32; ++q)
-                v[q] = okr ? make_float2(__uint_as_float(re[q]), __uint_as_float(im[q]))
-                           : make_float2(0.f, 0.f);
+                for (int q = 0; q < 32; ++q) re[q] = im[q] = 0u;
+            }
             if (lower) {  // rows gg of L21: consecutive lanes, coalesced per column t
                 if (okr) {
-#pragma unroll 8
-                    for (int q = 0; q < 32; ++q) M[(k0 + half * 32 + q) * n + gg] = v[q];
+#pragma unroll
+                    for (int q = 0; q < 32; ++q)  // unrolled: re and im stay in registers
+                        M[(k0 + half * 32 + q) * n + gg] = make_float2(__uint_as_float(re[q]), __uint_as_float(im[q]));
                 }
             } else {  // columns gg of U12: transposed through shared memory (the operands are
                       // consumed), then one warp writes 32 contiguous entries of a column
                 auto st = reinterpret_cast<float2 (*)[33]>(tc_smem);
 #pragma unroll
-                for (int q = 0; q < 32; ++q) st[row][q] = v[q];
+                for (int q = 0; q < 32; ++q) st[row][q] = make_float2(__uint_as_float(re[q]), __uint_as_float(im[q]));
                 __syncthreads();
 #pragma unroll 4
                 for (int i = 0; i < 32; ++i) {
@@ -305,15 +315,15 @@ k_lu_trsm_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
 #pragma unroll
             for (int c4 = 0; c4 < 4; ++c4) {
                 const int c = half * 4 + c4;
-                const float2* w8 = v + 8 * c4;
+                const uint4 pr = pack8u(re, 8 * c4, 1.f), pi = pack8u(im, 8 * c4, 1.f);
                 if (lower) {
-                    *reinterpret_cast<uint4*>(panel + core_off(row, c, TC_TM)) = pack8(w8, false, 1.f);
-                    *reinterpret_cast<uint4*>(panel + core_off(row, 8 + c, TC_TM)) = pack8(w8, true, 1.f);
+                    *reinterpret_cast<uint4*>(panel + core_off(row, c, TC_TM)) = pr;
+                    *reinterpret_cast<uint4*>(panel + core_off(row, 8 + c, TC_TM)) = pi;
                 } else {
-                    *reinterpret_cast<uint4*>(panel + core_off(row, c, 2 * TC_TN)) = pack8(w8, false, 1.f);
-                    *reinterpret_cast<uint4*>(panel + core_off(row, 8 + c, 2 * TC_TN)) = pack8(w8, true, -1.f);
-                    *reinterpret_cast<uint4*>(panel + core_off(TC_TN + row, c, 2 * TC_TN)) = pack8(w8, true, 1.f);
-                    *reinterpret_cast<uint4*>(panel + core_off(TC_TN + row, 8 + c, 2 * TC_TN)) = pack8(w8, false, 1.f);
+                    *reinterpret_cast<uint4*>(panel + core_off(row, c, 2 * TC_TN)) = pr;
+                    *reinterpret_cast<uint4*>(panel + core_off(row, 8 + c, 2 * TC_TN)) = pack8u(im, 8 * c4, -1.f);
+                    *reinterpret_cast<uint4*>(panel + core_off(TC_TN + row, c, 2 * TC_TN)) = pi;
+                    *reinterpret_cast<uint4*>(panel + core_off(TC_TN + row, 8 + c, 2 * TC_TN)) = pr;
                 }
             }
         }
