@@ -1514,7 +1514,7 @@ constexpr uint32_t kSsStageBytes = kSsTileBytes + kSsYBytes;
 constexpr int kSsConsumers = 256;
 constexpr int kSsThreads = kSsConsumers + 64;  // eight consumer warps, the tile warp and the y warp
 constexpr size_t kSsSmemBytes = (size_t)kSsStages * kSsStageBytes + kSsYBytes;  // + x_i of the block being solved
-constexpr uint64_t kSsWaitNs = 50000000;   // bounded stage waits: 50 ms of the global timer (a poll may
+constexpr uint32_t kSsWaitNs = 50000000;   // bounded stage waits: 50 ms of the global timer (a poll may
 constexpr uint32_t kSsWaitHintNs = 1000;    // return before its suspend hint, so the bound is in time) ...
 constexpr int kSsFlagPolls = 1 << 17;     // ... and flag waits (> 8 ms), as long as k_lu_solve_flags' flag waits
 
@@ -1526,8 +1526,8 @@ __device__ __forceinline__ void ss_bar_init(uint64_t* bar, int count)
 __device__ __forceinline__ bool ss_wait(uint64_t* bar, uint32_t phase)
 {
     const uint32_t a = smem_u32(bar);
-    uint64_t t0;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    uint32_t t0;  // the timer's low word: differences are exact across its 4.3 s wrap
+    asm volatile("mov.u32 %0, %%globaltimer_lo;" : "=r"(t0));
     for (;;) {
         uint32_t ok;
         asm volatile(
@@ -1538,8 +1538,8 @@ __device__ __forceinline__ bool ss_wait(uint64_t* bar, uint32_t phase)
             : "r"(a), "r"(phase), "r"(kSsWaitHintNs)
             : "memory");
         if (ok) return true;
-        uint64_t t;
-        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        uint32_t t;
+        asm volatile("mov.u32 %0, %%globaltimer_lo;" : "=r"(t));
         if (t - t0 > kSsWaitNs) return false;
     }
 }
@@ -1591,21 +1591,18 @@ template <bool kCT, int NQ, bool kMask>
 __device__ inline void ss_tile(const float2* __restrict__ st, const float2 (*__restrict__ ys)[64], int r,
                                         int tq, bool rok, int jlim, float (&ax)[4], float (&ay)[4])
 {
-    float2 m[kFsPer];
-#pragma unroll
-    for (int e = 0; e < kFsPer; ++e) {
-        const int c = fs_t(e, tq);
-        m[e] = kCT ? fs_conj(st[r * kSsLd + c]) : st[c * kSsLd + r];
-        if (kMask && !(rok && c < jlim)) m[e] = make_float2(0.f, 0.f);
-    }
+    // one pair of tile entries at a time (columns c, c + 1): few registers
+    // live, so the consumer warps fit the two-CTA register budget unspilled
 #pragma unroll
     for (int e = 0; e < kFsPer; e += 2) {
         const int c = fs_t(e, tq);
+        float2 a = kCT ? fs_conj(st[r * kSsLd + c]) : st[c * kSsLd + r];
+        float2 a2 = kCT ? fs_conj(st[r * kSsLd + c + 1]) : st[(c + 1) * kSsLd + r];
+        if (kMask && !(rok && c < jlim)) a = a2 = make_float2(0.f, 0.f);  // n even: c, c + 1 together
 #pragma unroll
         for (int qq = 0; qq < NQ; ++qq) {
             float4 v = fs_lds4(&ys[qq][c]);  // volatile: the loads stay in the loop, beside their FMAs
             if (kMask && c >= jlim) v = make_float4(0.f, 0.f, 0.f, 0.f);
-            const float2 a = m[e], a2 = m[e + 1];
             ax[qq] = fmaf(a.x, v.x, ax[qq]);
             ax[qq] = fmaf(-a.y, v.y, ax[qq]);
             ay[qq] = fmaf(a.x, v.y, ay[qq]);
@@ -1807,11 +1804,17 @@ k_lu_solve_stream(const float2* __restrict__ A, int64_t n, int64_t stride, const
             // y_i = inv(T_ii) x_i, over x_i; then publish
             const int s = t % kSsStages;
             take(s);
-            float2 iv[kFsPer];
-            fs_from_stage<kCT, kSsLd>(stage(s), iv);
-            float bx[4], by[4];
-            fs_rowdot(iv, xs, 0, NQ, bx, by);
+            float bx[4] = {0.f, 0.f, 0.f, 0.f}, by[4] = {0.f, 0.f, 0.f, 0.f};
+            ss_tile<kCT, NQ, false>(stage(s), xs, r, tq, true, NB, bx, by);  // the inverse block: a whole tile
             give(s);
+#pragma unroll
+            for (int qq = 0; qq < NQ; ++qq) {
+#pragma unroll
+                for (int o = 1; o < kFsLanes; o <<= 1) {
+                    bx[qq] += __shfl_xor_sync(0xffffffffu, bx[qq], o);
+                    by[qq] += __shfl_xor_sync(0xffffffffu, by[qq], o);
+                }
+            }
             if (tq == 0 && rok) {
 #pragma unroll
                 for (int qq = 0; qq < NQ; ++qq) x[(int64_t)qq * n + i0 + r] = make_float2(bx[qq], by[qq]);
