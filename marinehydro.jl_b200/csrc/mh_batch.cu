@@ -140,7 +140,7 @@ k_wave_batch(const double* __restrict__ geom, int64_t n, int direct, const doubl
 // (G, G_r, G_z) in o3.
 struct AllwPair {
     double dx, dy, rho, inv_rho, area, sr, dr;
-    const double* nn3;  // the normal of D (source panel when direct)
+    double n0, n1, n2;  // the normal of D (source panel when direct), held in registers
     int64_t o;          // pair offset j * n + i
     bool wrt_first;
 };
@@ -160,8 +160,8 @@ __device__ __forceinline__ void allw_emit(const AllwPair& q, int z, double k, co
     const cplx s = ka * o3[0];
     const cplx g0 = (ka * d1) * o3[1], g1 = (ka * d2) * o3[1], g2 = (ka * k) * o3[2];
     const double Sr = q.sr - kInv4Pi * s.re, Si = -kInv4Pi * s.im;
-    const double Dr = q.dr - kInv4Pi * (q.nn3[0] * g0.re + q.nn3[1] * g1.re + q.nn3[2] * g2.re);
-    const double Di = -kInv4Pi * (q.nn3[0] * g0.im + q.nn3[1] * g1.im + q.nn3[2] * g2.im);
+    const double Dr = q.dr - kInv4Pi * (q.n0 * g0.re + q.n1 * g1.re + q.n2 * g2.re);
+    const double Di = -kInv4Pi * (q.n0 * g0.im + q.n1 * g1.im + q.n2 * g2.im);
     const int64_t m = (int64_t)z * nn + q.o;
     S64[m] = make_double2(Sr, Si);
     D64[m] = make_double2(Dr, Di);
@@ -246,7 +246,6 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
         const Panel& p = sp[jj];
         const int64_t j = j0 + jj;
         const int64_t o = j * n + i;
-        const double* nn3 = direct ? p.n : ni;
         // pair geometry (abstract_greens_function.jl:111-131 at k = 1)
         const double dx = x[0] - p.c[0], dy = x[1] - p.c[1];
         const double dis2 = dx * dx + dy * dy;
@@ -284,7 +283,8 @@ k_wave_delh_allw(const double* __restrict__ geom, int64_t n, int direct, const d
                     w[(q * kTabNU + row) * kWT + tid] = (HT)hfma(vc, b1[q], polar_coef<CT>(cr + q * kTabPolarFn) - b2[q]);
             }
         }
-        const AllwPair q{dx, dy, rho, inv_rho, p.area, sr, dr, nn3, o, wrt_first};
+        const AllwPair q{dx, dy, rho, inv_rho, p.area, sr, dr, direct ? p.n[0] : ni[0], direct ? p.n[1] : ni[1],
+                         direct ? p.n[2] : ni[2], o, wrt_first};
         // four frequencies per Horner pass: each coefficient read from shared
         // memory feeds four recurrences.  Frequencies off the polar patch are
         // only counted here: k_wave_delh_allw_rest evaluates them with the
@@ -380,7 +380,8 @@ k_wave_delh_allw_rest(const int* __restrict__ fall, const double* __restrict__ g
         const double zeta = x[2] + p.c[2];
         const double d = hypot(rho, zeta);
         const bool polar_ok = -zeta >= 0.0;
-        const AllwPair q{dx, dy, rho, rho > 0.0 ? 1.0 / rho : 0.0, p.area, SR[o], DR[o], direct ? p.n : ni, o,
+        const double* nn3 = direct ? p.n : ni;
+        const AllwPair q{dx, dy, rho, rho > 0.0 ? 1.0 / rho : 0.0, p.area, SR[o], DR[o], nn3[0], nn3[1], nn3[2], o,
                          !direct};
 #pragma unroll 1
         for (int z = 0; z < nb; ++z) {
