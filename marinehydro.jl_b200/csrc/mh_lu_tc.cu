@@ -10,22 +10,24 @@
 //                      factors into the matrix and the FP16 operand panels of
 //                      the update, pre-packed as their shared-memory images
 //                      at absolute 128-row (column) tile slots;
-//   k_lu_update_tc     A22 -= sum_p L21_p U12_p over one or two panel pairs:
-//                      the packed panels arrive by cp.async.bulk (no register
-//                      staging), eight MMAs per pair accumulate in TMEM.
+//   k_lu_update_tc     A22 -= sum_p L21_p U12_p over panel pairs: the
+//                      packed panels arrive by cp.async.bulk (no register
+//                      staging), sixteen MMAs per pair accumulate in TMEM.
 //
-// The trailing update is one real GEMM per 128 x 128 complex tile of A22:
-// with A = [Re L21 | Im L21] (128 x 128) and
-//   B = [ Re U12^T  -Im U12^T ]   (rows 0..127: real part of the product)
-//       [ Im U12^T   Re U12^T ]   (rows 128..255: imaginary part)
-// D = A B^T (128 x 256) holds Re(L21 U12) in columns 0..127 and Im in
-// 128..255.  Operands are rounded to FP16 and staged in shared memory in the
-// UMMA K-major no-swizzle layout (8-row x 16-byte core matrices; SBO = 128 B
-// between 8-row groups, LBO = one K chunk of 8 elements); one thread issues
-// eight tcgen05.mma.kind::f16 (M=128, N=256, K=16) per panel pair into a
-// 256-column FP32 accumulator in tensor memory and commits them to an
-// mbarrier; the four warps read their 32 TMEM lanes back with tcgen05.ld and
-// subtract from A22 in FP32.  Every wait is bounded: a timeout marks the
+// The trailing update of a 128 x 128 complex tile of A22 is two real GEMMs
+// over the FP16 images A = [Re L21 | Im L21] and B = [Re U12^T | Im U12^T]
+// (128 rows each, K = 128: the 64 complex K entries' real parts, then their
+// imaginary parts): Re(L21 U12) = A_re B_re - A_im B_im into tensor-memory
+// columns 0..127 (the K steps of the imaginary half with A negated by the
+// instruction descriptor) and Im(L21 U12) = A_re B_im + A_im B_re into
+// columns 128..255 (B's K halves swapped through the descriptors' start
+// addresses).  Each operand holds each real and imaginary part once: 64 KB
+// per panel pair.  Operands are rounded to FP16 and staged in shared memory
+// in the UMMA K-major no-swizzle layout (8-row x 16-byte core matrices; SBO =
+// 128 B between 8-row groups, LBO = one K chunk of 8 elements); one thread
+// issues sixteen tcgen05.mma.kind::f16 (M=128, N=128, K=16) per panel pair
+// and commits them to an mbarrier; the four warps read their 32 TMEM lanes
+// back with tcgen05.ld and subtract from A22 in FP32.  Every wait is bounded: a timeout marks the
 // matrix bad (the host then re-solves it with the FP64 pivoted LU) instead
 // of spinning.
 #include <cuda_fp16.h>
@@ -42,23 +44,22 @@ constexpr int TC_TM = 128;                // C rows per CTA (UMMA M)
 constexpr int TC_TN = 128;                // C complex columns per CTA (UMMA N = 256)
 constexpr int TC_KR = 2 * TC_NB;          // real K = 128 (8 UMMA K-steps of 16)
 constexpr uint32_t kSmemA = TC_TM * TC_KR * 2;          // 32 KiB of FP16
-constexpr uint32_t kSmemB = 2 * TC_TN * TC_KR * 2;      // 64 KiB of FP16
+constexpr uint32_t kSmemB = 2 * TC_TN * TC_KR * 2;      // 64 KiB: the B operand (32 KiB) and room after it
 constexpr uint32_t kTmemCols = 2 * TC_TN;               // 256 FP32 columns
 constexpr uint32_t kLboA = (TC_TM / 8) * 128;           // bytes between K chunks of A
-constexpr uint32_t kLboB = (2 * TC_TN / 8) * 128;       // bytes between K chunks of B
 constexpr uint32_t kSbo = 128;                          // bytes between 8-row groups
 // Instruction descriptor: F32 accumulator (bits 4-5 = 1), A and B F16
 // (bits 7-9, 10-12 = 0), both K-major (bits 15, 16 = 0), N >> 3 at bit 17,
 // M >> 4 at bit 24.
-constexpr uint32_t kIdesc = (1u << 4) | ((uint32_t)(2 * TC_TN) >> 3 << 17) | ((uint32_t)TC_TM >> 4 << 24);
 constexpr uint32_t kIdescN128 = (1u << 4) | (128u >> 3 << 17) | ((uint32_t)TC_TM >> 4 << 24);
 constexpr uint32_t kLboB128 = (128 / 8) * 128;          // B of the TRSM GEMM: 128 rows
 constexpr uint32_t kPanelL = kSmemA;                    // packed L21 tile (A image), bytes
-constexpr uint32_t kPanelU = kSmemB;                    // packed U12 tile (B image), bytes
+constexpr uint32_t kPanelU = kSmemA;                    // packed U12 tile (B image, 128 rows), bytes
 constexpr int kWaitPolls = 4096;          // bounded mbarrier polls ...
 constexpr uint32_t kWaitHintNs = 1000;    // ... each suspending at most ~1 us
 
-// Dynamic shared memory of k_lu_update_tc: the two operand tiles (96 KiB), so
+// Dynamic shared memory of k_lu_update_tc: the two operand tiles (64 KiB) and
+// the room the epilogue's three 32 KiB chunks of C need (96 KiB in all), so
 // two CTAs share an SM and its 512 TMEM columns.
 constexpr uint32_t kTcSmemBytes = kSmemA + kSmemB;
 
@@ -174,6 +175,39 @@ __device__ __forceinline__ void mma_k128(uint32_t tmem, uint32_t a0, uint32_t lb
                  :: "r"(bar) : "memory");
 }
 
+// The complex product of one panel pair, C += L21 U12, from the FP16 images
+// A = [Re L21 | Im L21] (128 rows, K = 128) and B = [Re U12^T | Im U12^T]
+// (128 rows, K = 128): sixteen K=16 MMAs of N = 128, the real part into
+// tensor-memory columns 0..127 as A_s B_s over the K steps s (A negated by
+// the instruction descriptor for s >= 4: - Im L Im U), the imaginary part into
+// columns 128..255 as A_s B_(s+4 mod 8) (Re L Im U + Im L Re U); then commit
+// to `bar`.  The first MMAs overwrite the accumulator unless `accumulate`.
+// B holds each of Re U12, Im U12 once: 32 KB per pair instead of the 64 KB
+// of a [Re -Im; Im Re] image.
+__device__ __forceinline__ void mma_cplx(uint32_t tmem, uint32_t a0, uint32_t b0, uint32_t bar, bool accumulate)
+{
+    constexpr uint32_t kNegA = 1u << 13;
+#pragma unroll
+    for (int s = 0; s < TC_KR / 16; ++s) {
+        const uint64_t da = umma_desc(a0 + 2 * s * kLboA, kLboA, kSbo);
+        const uint64_t dre = umma_desc(b0 + 2 * s * kLboB128, kLboB128, kSbo);
+        const uint64_t dim = umma_desc(b0 + 2 * ((s + 4) & 7) * kLboB128, kLboB128, kSbo);
+        const uint32_t acc = (s > 0 || accumulate) ? 1u : 0u;
+        const uint32_t idre = kIdescN128 | (s >= 4 ? kNegA : 0u);
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+            :: "r"(tmem), "l"(da), "l"(dre), "r"(idre), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+            :: "r"(tmem + (uint32_t)TC_TN), "l"(da), "l"(dim), "r"(kIdescN128), "r"(acc), "r"(0u), "r"(0u),
+               "r"(0u), "r"(0u));
+    }
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :: "r"(bar) : "memory");
+}
+
 // Eight consecutive FP32 words of a TMEM read-back (x[o .. o + 7], o a
 // compile-time offset after unrolling) as FP16, times sign.
 __device__ __forceinline__ uint4 pack8u(const uint32_t (&x)[32], int o, float sign)
@@ -199,8 +233,8 @@ __device__ __forceinline__ uint4 pack8(const float2* v, bool imag, float sign)
 // absolute (tile T holds rows, or columns, 128 T .. 128 T + 127), starting
 // at the tile of row k0 + 64; the rows (columns) of that tile above k0 + 64
 // are zero in the images and are not written back.  Writes the FP32 factors
-// back and the packed FP16 panels Lp (A image of the update) and Up (B
-// image: rows j = [Re U12(:, j) | -Im], rows 128 + j = [Im | Re]), each at
+// back and the packed FP16 panels Lp (A image of the update: rows i =
+// [Re L21(i, :) | Im]) and Up (B image: rows j = [Re U12(:, j) | Im]), each at
 // its absolute tile slot.
 __global__ void __launch_bounds__(128, 2)
 k_lu_trsm_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
@@ -315,16 +349,9 @@ k_lu_trsm_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int64_t k0,
 #pragma unroll
             for (int c4 = 0; c4 < 4; ++c4) {
                 const int c = half * 4 + c4;
-                const uint4 pr = pack8u(re, 8 * c4, 1.f), pi = pack8u(im, 8 * c4, 1.f);
-                if (lower) {
-                    *reinterpret_cast<uint4*>(panel + core_off(row, c, TC_TM)) = pr;
-                    *reinterpret_cast<uint4*>(panel + core_off(row, 8 + c, TC_TM)) = pi;
-                } else {
-                    *reinterpret_cast<uint4*>(panel + core_off(row, c, 2 * TC_TN)) = pr;
-                    *reinterpret_cast<uint4*>(panel + core_off(row, 8 + c, 2 * TC_TN)) = pack8u(im, 8 * c4, -1.f);
-                    *reinterpret_cast<uint4*>(panel + core_off(TC_TN + row, c, 2 * TC_TN)) = pi;
-                    *reinterpret_cast<uint4*>(panel + core_off(TC_TN + row, 8 + c, 2 * TC_TN)) = pr;
-                }
+                // both images [Re | Im] by rows (L21 rows; U12 columns = U12^T rows)
+                *reinterpret_cast<uint4*>(panel + core_off(row, c, TC_TM)) = pack8u(re, 8 * c4, 1.f);
+                *reinterpret_cast<uint4*>(panel + core_off(row, 8 + c, TC_TM)) = pack8u(im, 8 * c4, 1.f);
             }
         }
     } else {
@@ -511,7 +538,7 @@ k_lu_update_tc(float2* __restrict__ Ab, int64_t n, int64_t stride, int t0, int n
         if (!ok) break;
         pend_ld = -1;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        if (tid == 0) mma_k128(tmem, smem_u32(sA), kLboA, smem_u32(sB), kLboB, kIdesc, bar_mma, p > 0);
+        if (tid == 0) mma_cplx(tmem, smem_u32(sA), smem_u32(sB), bar_mma, p > 0);
         // the next pair's copies overwrite the operands: wait for these MMAs
         pend_mma = p;
         ok = __syncthreads_and(mbar_wait(bar_mma, (uint32_t)(p & 1))) != 0;
@@ -660,7 +687,7 @@ k_lu_update_tc_acc(float2* __restrict__ Ab, int64_t n, int64_t stride, int t0, i
         if (!ok) break;
         pend_ld = -1;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        if (tid == 0) mma_k128(tmem, smem_u32(sA), kLboA, smem_u32(sB), kLboB, kIdesc, bar_mma, true);
+        if (tid == 0) mma_cplx(tmem, smem_u32(sA), smem_u32(sB), bar_mma, true);
         // the next pair's copies overwrite the operands: wait for these MMAs
         pend_mma = p;
         ok = __syncthreads_and(mbar_wait(bar_mma, (uint32_t)(p & 1))) != 0;
