@@ -674,6 +674,8 @@ WAVE_FP32_FLOPS_PER_PAIR_FREQ = 112.0
 # complement re-read once per 512-column outer step, the left-looking tile
 # updates, panels and diagonal blocks): 3.677 GB / 16 = 229.8 MB per matrix
 # (14.7 GB per 64; 16.7 GB with 256-column steps and right-looking strips).
+# Captured with the 64 KB U12 operand images; their halving since cuts
+# mostly L2 traffic (the images are re-read from L2 by every update CTA).
 LU_DRAM_BYTES_PER_MATRIX_2048 = 3.677e9 / 16
 
 
